@@ -1,0 +1,55 @@
+/*
+ * Extensions of the B200 build of libmaze_poisson.so. None of these has a counterpart
+ * in the reference's ctypes binding; they serve parity tests (kernel-level entry points
+ * on plain host arrays) and callers that want several MD steps per call.
+ *
+ * Grid arrays are plain n^3 C-contiguous doubles, idx = (i*n + j)*n + k, periodic in all
+ * axes (the reference's (n+2)-plane halo layout is not used). Every entry point needs
+ * solver_initialize() first; the kernel-level ones allocate and free device work
+ * buffers per call.
+ */
+#ifndef MAZE_POISSON_B200_H
+#define MAZE_POISSON_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* n_steps x SolverMD.md_loop_iter (maze_poisson/solver.py:483-492) with electrostatic
+   and non-electrostatic forces; cf. the reference's commented-out solver_md_loop_iter /
+   solver_run_n_steps (library/src/solver_md.c:202-228). Returns the last
+   solver_update_field value. */
+int solver_md_step(int n_steps);
+
+/* kernel-level entry points (reference semantics on plain n^3 arrays) */
+void mzb_laplace(const double *u, double *out, int n);                     /* laplace.c:24-75 */
+int mzb_conj_grad(const double *b, const double *x0, double *x, double tol, int n,
+                  int precond);  /* plcg.c:28-90 (precond 0), plcg.c:104-166 (1 JACOBI, 2 MG) */
+void mzb_smooth_rbgs(const double *rhs, double *x, int n, int iters);      /* multigrid.c:636-729 */
+void mzb_restrict27(const double *fine, double *coarse, int n);            /* multigrid.c:523-594 */
+void mzb_prolong_trilinear(const double *coarse, double *fine, int nc);    /* multigrid.c:393-463 */
+int mzb_cg_coarse(const double *b, double *x, int n, int maxit, double rtol); /* multigrid.c:13-96 */
+void mzb_mg_apply(const double *rhs, double *x, int n, int sm);            /* multigrid.c:99-168 */
+void mzb_fft_poisson(const double *q, double *phi, int n, double L, double h); /* fftw_wrap.c:166-189 */
+
+/* state accessors of the current system */
+void mzb_get_cic_neighbors(int64_t *out);  /* (n_p,8,3) CIC corners, particles.c:297-346 */
+void mzb_set_cell_grid(int nc);            /* linked cells per side for the pair forces */
+int mzb_get_cells(int32_t *start, int32_t *ions); /* CSR linked cells; returns nc */
+void mzb_philox_normals(uint64_t call, double *out); /* O-block draws of call `call` (n_p,3) */
+void mzb_set_seed(uint64_t seed);          /* O-block Philox key */
+uint64_t mzb_get_ocalls(void);             /* O-blocks applied so far */
+
+/* instrumentation */
+void *mzb_get_stream(void);                /* cudaStream_t of the current system */
+double mzb_last_solve_ms(void);            /* device ms of the last field-solver launch */
+int mzb_last_solve_result(void);           /* its return value (iterations or -1) */
+uint64_t mzb_kernel_launches(void);        /* kernels this library has launched */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAZE_POISSON_B200_H */

@@ -1,0 +1,562 @@
+// Persistent solver engine (see engine.cuh).
+//
+// Work decomposition: one warp per grid row (fixed i,j; lanes stride over k), rows
+// distributed grid-stride over all warps of the cooperative grid. Every sweep keeps the
+// reference's per-point arithmetic (order of the sums, products rounded before adds) so
+// single sweeps are bit-identical to the reference; only the global dot products are
+// summed in a different (fixed, deterministic) order.
+#include "engine.cuh"
+
+namespace mzb {
+namespace {
+
+constexpr int kThreads = 512;
+constexpr int kMinBlocksPerSM = 1;
+
+struct Team {
+    int lane;
+    long gw;
+    long nw;
+};
+__device__ __forceinline__ Team make_team() {
+    Team t;
+    t.lane = threadIdx.x & 31;
+    t.gw = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    t.nw = (long)gridDim.x * (blockDim.x >> 5);
+    return t;
+}
+
+// Visit every point of an n^3 grid once: warp per (i,j) row, lanes over k.
+template <class F>
+__device__ __forceinline__ void for_points(const Team& t, int n, F&& f) {
+    const long rows = (long)n * n;
+    for (long row = t.gw; row < rows; row += t.nw) {
+        const int i = (int)(row / n), j = (int)(row - (long)i * n);
+        for (int k = t.lane; k < n; k += 32) f(i, j, k);
+    }
+}
+// Visit the points of one colour ((i+j+k) % 2 == colour) of an n^3 grid (n even).
+template <class F>
+__device__ __forceinline__ void for_colour(const Team& t, int n, int colour, F&& f) {
+    const long rows = (long)n * n;
+    for (long row = t.gw; row < rows; row += t.nw) {
+        const int i = (int)(row / n), j = (int)(row - (long)i * n);
+        for (int k = ((i + j + colour) & 1) + 2 * t.lane; k < n; k += 64) f(i, j, k);
+    }
+}
+
+struct Nb {
+    long c, ip, im, jp, jm, kp, km;
+};
+__device__ __forceinline__ Nb neighbours(int n, int i, int j, int k) {
+    const long n2 = (long)n * n;
+    Nb o;
+    o.c = ((long)i * n + j) * n + k;
+    o.ip = o.c + (i + 1 == n ? -(long)(n - 1) * n2 : n2);
+    o.im = o.c + (i == 0 ? (long)(n - 1) * n2 : -n2);
+    o.jp = o.c + (j + 1 == n ? -(long)(n - 1) * n : (long)n);
+    o.jm = o.c + (j == 0 ? (long)(n - 1) * n : -(long)n);
+    o.kp = o.c + (k + 1 == n ? -(long)(n - 1) : 1L);
+    o.km = o.c + (k == 0 ? (long)(n - 1) : -1L);
+    return o;
+}
+
+// 7-point Laplacian in the reference's order: x+1, x-1, y+1, y-1, z+1, z-1, - 6 c
+// (library/src/laplace.c:208-216). `f(idx)` yields the operand at a flat index.
+template <class F>
+__device__ __forceinline__ double lap7(const Nb& o, F&& f) {
+    double s = f(o.ip) + f(o.im);
+    s = s + f(o.jp);
+    s = s + f(o.jm);
+    s = s + f(o.kp);
+    s = s + f(o.km);
+    return s - f(o.c) * 6.0;
+}
+
+// ------------------------------------------------------------------------------------
+// Grid-wide reductions: NS sums followed by NM maxima. Results land in every thread.
+// Partials are double-buffered by a sequence number so a fast block writing reduction
+// k+1 never overwrites values a slow block is still gathering for reduction k.
+// ------------------------------------------------------------------------------------
+template <int NS, int NM>
+__device__ bool grid_reduce(double* s, double* mx, const EngineArgs& a, int& seq) {
+    __shared__ double sh[8 * 32];
+    __shared__ double res[8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const long G = gridDim.x;
+#pragma unroll
+    for (int q = 0; q < NS; q++) s[q] = warp_sum(s[q]);
+#pragma unroll
+    for (int q = 0; q < NM; q++) mx[q] = warp_max(mx[q]);
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NS; q++) sh[q * 32 + w] = s[q];
+#pragma unroll
+        for (int q = 0; q < NM; q++) sh[(NS + q) * 32 + w] = mx[q];
+    }
+    __syncthreads();
+    double* part = a.partials + (long)(seq & 1) * 8 * G;
+    if (w == 0) {
+#pragma unroll
+        for (int q = 0; q < NS + NM; q++) {
+            double v = lane < nwarp ? sh[q * 32 + lane] : 0.0;
+            v = q < NS ? warp_sum(v) : warp_max(v);
+            if (lane == 0) part[q * G + blockIdx.x] = v;
+        }
+    }
+    const bool ok = grid_sync(a.bar);
+    if (w == 0) {
+#pragma unroll
+        for (int q = 0; q < NS + NM; q++) {
+            double v = 0.0;
+            for (long b = lane; b < G; b += 32) {
+                const double e = __ldcg(part + q * G + b);
+                v = q < NS ? v + e : fmax(v, e);
+            }
+            v = q < NS ? warp_sum(v) : warp_max(v);
+            if (lane == 0) res[q] = v;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NS; q++) s[q] = res[q];
+#pragma unroll
+    for (int q = 0; q < NM; q++) mx[q] = res[NS + q];
+    __syncthreads();
+    seq++;
+    return ok;
+}
+
+// ------------------------------------------------------------------------------------
+// Multigrid sweeps (library/src/multigrid.c)
+// ------------------------------------------------------------------------------------
+
+// One red-black Gauss-Seidel iteration: red ((i+j+k) even) then black
+// (multigrid.c:636-729). Neighbour sum order i-1, i+1, j-1, j+1, k-1, k+1.
+__device__ bool rbgs(const Team& t, const double* rhs, double* x, int n, const EngineArgs& a) {
+    const double inv_diag = -1.0 / 6.0;
+    for (int colour = 0; colour < 2; colour++) {
+        for_colour(t, n, colour, [&](int i, int j, int k) {
+            const Nb o = neighbours(n, i, j, k);
+            double s = x[o.im] + x[o.ip];
+            s = s + x[o.jm];
+            s = s + x[o.jp];
+            s = s + x[o.km];
+            s = s + x[o.kp];
+            x[o.c] = (rhs[o.c] - s) * inv_diag;
+        });
+        if (!grid_sync(a.bar)) return false;
+    }
+    return true;
+}
+
+// 27-point full weighting, coarse (I,J,K) <- fine (2I,2J,2K) (multigrid.c:523-594).
+__device__ void restrict27(const Team& t, const double* in, double* out, int n) {
+    const int nc = n / 2;
+    const long n2 = (long)n * n;
+    for_points(t, nc, [&](int I, int J, int K) {
+        const int i = 2 * I, j = 2 * J, k = 2 * K;
+        const long i0 = (long)i * n2, i1 = (long)(i + 1 == n ? 0 : i + 1) * n2,
+                   i2 = (long)(i == 0 ? n - 1 : i - 1) * n2;
+        const long j0 = (long)j * n, j1 = (long)(j + 1 == n ? 0 : j + 1) * n,
+                   j2 = (long)(j == 0 ? n - 1 : j - 1) * n;
+        const long k0 = k, k1 = (k + 1 == n ? 0 : k + 1), k2 = (k == 0 ? n - 1 : k - 1);
+        double f = in[i2 + j0 + k0] + in[i1 + j0 + k0];
+        f = f + in[i0 + j2 + k0];
+        f = f + in[i0 + j1 + k0];
+        f = f + in[i0 + j0 + k2];
+        f = f + in[i0 + j0 + k1];
+        double e = in[i1 + j0 + k2] + in[i1 + j0 + k1];
+        e = e + in[i2 + j0 + k2];
+        e = e + in[i2 + j0 + k1];
+        e = e + in[i1 + j2 + k0];
+        e = e + in[i1 + j1 + k0];
+        e = e + in[i2 + j2 + k0];
+        e = e + in[i2 + j1 + k0];
+        e = e + in[i0 + j2 + k2];
+        e = e + in[i0 + j2 + k1];
+        e = e + in[i0 + j1 + k2];
+        e = e + in[i0 + j1 + k1];
+        double c = in[i1 + j1 + k2] + in[i1 + j1 + k1];
+        c = c + in[i1 + j2 + k2];
+        c = c + in[i1 + j2 + k1];
+        c = c + in[i2 + j1 + k2];
+        c = c + in[i2 + j1 + k1];
+        c = c + in[i2 + j2 + k2];
+        c = c + in[i2 + j2 + k1];
+        double v = 8.0 * in[i0 + j0 + k0] + 4.0 * f;
+        v = v + 2.0 * e;
+        v = v + c;
+        out[((long)I * nc + J) * nc + K] = v * (1.0 / 64.0);
+    });
+}
+
+// Trilinear prolongation value at fine (i,j,k) from an nc^3 coarse grid
+// (multigrid.c:393-463): weights (1,0) on even fine indices, (0.5,0.5) on odd.
+__device__ __forceinline__ double prolong_at(const double* in, int nc, int i, int j, int k) {
+    const double wi0 = (i & 1) ? 0.5 : 1.0, wi1 = (i & 1) ? 0.5 : 0.0;
+    const double wj0 = (j & 1) ? 0.5 : 1.0, wj1 = (j & 1) ? 0.5 : 0.0;
+    const double wk0 = (k & 1) ? 0.5 : 1.0, wk1 = (k & 1) ? 0.5 : 0.0;
+    const long n2 = (long)nc * nc;
+    const int ci = i >> 1, cj = j >> 1, ck = k >> 1;
+    const long i0 = (long)ci * n2, i1 = (long)(ci + 1 == nc ? 0 : ci + 1) * n2;
+    const long j0 = (long)cj * nc, j1 = (long)(cj + 1 == nc ? 0 : cj + 1) * nc;
+    const long k0 = ck, k1 = (ck + 1 == nc ? 0 : ck + 1);
+    double s = in[i0 + j0 + k0] * wi0 * wj0 * wk0 + in[i1 + j0 + k0] * wi1 * wj0 * wk0;
+    s = s + in[i0 + j1 + k0] * wi0 * wj1 * wk0;
+    s = s + in[i1 + j1 + k0] * wi1 * wj1 * wk0;
+    s = s + in[i0 + j0 + k1] * wi0 * wj0 * wk1;
+    s = s + in[i1 + j0 + k1] * wi1 * wj0 * wk1;
+    s = s + in[i0 + j1 + k1] * wi0 * wj1 * wk1;
+    s = s + in[i1 + j1 + k1] * wi1 * wj1 * wk1;
+    return s;
+}
+
+// ------------------------------------------------------------------------------------
+// Conjugate gradients on L x = b (plcg.c:28-166, multigrid.c:13-96).
+// ------------------------------------------------------------------------------------
+struct CgSpec {
+    int n;
+    const double* b;
+    const double* x0;
+    double* x;
+    double* r;
+    double* p0;
+    double* p1;
+    double* Ap;
+    double* v;      // PC_MG: preconditioner output (warm-started)
+    int kind;       // PrecondKind
+    bool coarse;    // cg_coarse semantics (relative stop, denominator guard, count)
+    double tol;     // absolute stop (conj_grad*)
+    double rtol;    // relative stop (cg_coarse)
+    long limit;     // iteration cap
+};
+
+__device__ bool vcycle(const Team& t, const double* rhs, double* x, int n, int sm, const EngineArgs& a,
+                       int& seq);
+
+// Returns the reference's value: conj_grad* -> 0-based iteration at convergence or -1;
+// cg_coarse -> number of iterations run. `ok` turns false on a barrier failure.
+// KIND is the PrecondKind; COARSE selects the cg_coarse variant (never preconditioned, so
+// the V-cycle -> coarse CG call chain is not recursive).
+template <int KIND, bool COARSE>
+__device__ int cg_run(const Team& t, const CgSpec& s, const EngineArgs& a, int& seq, bool& ok) {
+    static_assert(!(COARSE && KIND != PC_IMPLICIT), "coarse CG is unpreconditioned");
+    const int n = s.n;
+    // r = L x0 - b; x = x0; v = 0 (PC_MG)
+    double acc[2] = {0.0, 0.0}, mx[1] = {0.0};
+    for_points(t, n, [&](int i, int j, int k) {
+        const Nb o = neighbours(n, i, j, k);
+        const double x0c = s.x0[o.c];
+        const double rr = lap7(o, [&](long q) { return s.x0[q]; }) + -1.0 * s.b[o.c];
+        if (s.x != s.x0) s.x[o.c] = x0c;
+        s.r[o.c] = rr;
+        if (KIND == PC_IMPLICIT) acc[0] += rr * (rr * (1.0 / 6.0));
+        else if (KIND == PC_JACOBI) acc[0] += rr * (-rr / 6.0);
+        else s.v[o.c] = 0.0;
+        mx[0] = fmax(mx[0], fabs(rr));
+    });
+    ok = grid_reduce<1, 1>(acc, mx, a, seq);
+    if (!ok) return -1;
+    double rv;
+    if (KIND == PC_IMPLICIT) rv = -acc[0];
+    else if (KIND == PC_JACOBI) rv = acc[0];
+    else {
+        ok = vcycle(t, s.r, s.v, n, 5, a, seq);
+        if (!ok) return -1;
+        double d[1] = {0.0}, m0[1];
+        for_points(t, n, [&](int i, int j, int k) {
+            const long c = ((long)i * n + j) * n + k;
+            d[0] += s.r[c] * s.v[c];
+        });
+        ok = grid_reduce<1, 0>(d, m0, a, seq);
+        if (!ok) return -1;
+        rv = d[0];
+    }
+    const double r0 = mx[0];
+    if (COARSE && r0 == 0.0) return 0;
+
+    long iter = 0;
+    int res = COARSE ? (int)s.limit : -1;
+    double beta = 0.0;
+    const double* pold = s.p1;
+    double* pnew = s.p0;
+    while (iter < s.limit) {
+        const bool first = (iter == 0);
+        // phase A: p <- beta p + z(r); Ap = L p; <p, Ap>
+        auto zf = [&](long q) {
+            if (KIND == PC_IMPLICIT) return (1.0 / 6.0) * s.r[q];
+            if (KIND == PC_JACOBI) return -1.0 * (-s.r[q] / 6.0);
+            return -1.0 * s.v[q];
+        };
+        auto pf = [&](long q) { return first ? zf(q) : pold[q] * beta + zf(q); };
+        double pap[1] = {0.0}, m0[1];
+        for_points(t, n, [&](int i, int j, int k) {
+            const Nb o = neighbours(n, i, j, k);
+            const double pc = pf(o.c);
+            const double ap = lap7(o, pf);
+            pnew[o.c] = pc;
+            s.Ap[o.c] = ap;
+            pap[0] += pc * ap;
+        });
+        ok = grid_reduce<1, 0>(pap, m0, a, seq);
+        if (!ok) return -1;
+        if (COARSE && fabs(pap[0]) < 1e-300) { res = (int)iter; break; }
+        const double alpha = rv / pap[0];
+        // phase B: x += alpha p; r += alpha Ap; <r,r>, |r|_inf (+ <r, P r> for Jacobi)
+        double sums[2] = {0.0, 0.0}, rmax[1] = {0.0};
+        for_points(t, n, [&](int i, int j, int k) {
+            const long c = ((long)i * n + j) * n + k;
+            s.x[c] = s.x[c] + alpha * pnew[c];
+            const double rn = s.r[c] + alpha * s.Ap[c];
+            s.r[c] = rn;
+            sums[0] += rn * rn;
+            if (KIND == PC_JACOBI) sums[1] += rn * (-rn / 6.0);
+            rmax[0] = fmax(rmax[0], fabs(rn));
+        });
+        ok = grid_reduce<2, 1>(sums, rmax, a, seq);
+        if (!ok) return -1;
+        if (COARSE) {
+            if (rmax[0] <= s.rtol * r0) { res = (int)iter + 1; break; }
+        } else if (rmax[0] <= s.tol) {
+            res = (int)iter;
+            break;
+        }
+        double rnv;
+        if (KIND == PC_IMPLICIT) rnv = -sums[0] / 6.0;
+        else if (KIND == PC_JACOBI) rnv = sums[1];
+        else {
+            ok = vcycle(t, s.r, s.v, n, 5, a, seq);
+            if (!ok) return -1;
+            double d[1] = {0.0}, m1[1];
+            for_points(t, n, [&](int i, int j, int k) {
+                const long c = ((long)i * n + j) * n + k;
+                d[0] += s.r[c] * s.v[c];
+            });
+            ok = grid_reduce<1, 0>(d, m1, a, seq);
+            if (!ok) return -1;
+            rnv = d[0];
+        }
+        beta = rnv / rv;
+        rv = rnv;
+        iter++;
+        pold = pnew;
+        pnew = (pnew == s.p0) ? s.p1 : s.p0;
+    }
+    return res;
+}
+
+// One V-cycle as the reference runs it (recursion bottoms out at depth 1): sm RBGS
+// iterations, residual rf = -(L x) + rhs, 27-pt restriction, coarse CG (50 it, rtol
+// 1e-5) from zero, x += P e, sm RBGS iterations (multigrid.c:99-168).
+__device__ bool vcycle(const Team& t, const double* rhs, double* x, int n, int sm, const EngineArgs& a,
+                       int& seq) {
+    const int nc = n / 2;
+    for (int it = 0; it < sm; it++)
+        if (!rbgs(t, rhs, x, n, a)) return false;
+    for_points(t, n, [&](int i, int j, int k) {
+        const Nb o = neighbours(n, i, j, k);
+        const double lx = lap7(o, [&](long q) { return x[q]; });
+        a.rf[o.c] = -lx + 1.0 * rhs[o.c];
+    });
+    if (!grid_sync(a.bar)) return false;
+    restrict27(t, a.rf, a.rc, n);
+    for_points(t, nc, [&](int i, int j, int k) { a.ec[((long)i * nc + j) * nc + k] = 0.0; });
+    if (!grid_sync(a.bar)) return false;
+    CgSpec cs;
+    cs.n = nc; cs.b = a.rc; cs.x0 = a.ec; cs.x = a.ec; cs.r = a.cr; cs.p0 = a.cp0; cs.p1 = a.cp1;
+    cs.Ap = a.cAp; cs.v = nullptr; cs.kind = PC_IMPLICIT; cs.coarse = true; cs.tol = 0.0;
+    cs.rtol = 1e-5; cs.limit = 50;
+    bool ok = true;
+    cg_run<PC_IMPLICIT, true>(t, cs, a, seq, ok);
+    if (!ok) return false;
+    for_points(t, n, [&](int i, int j, int k) {
+        const long c = ((long)i * n + j) * n + k;
+        x[c] = x[c] + 1.0 * prolong_at(a.ec, nc, i, j, k);
+    });
+    if (!grid_sync(a.bar)) return false;
+    for (int it = 0; it < sm; it++)
+        if (!rbgs(t, rhs, x, n, a)) return false;
+    return true;
+}
+
+// max |L x - b| over the grid (the reference's residual check after each V-cycle).
+__device__ bool resid_max(const Team& t, const double* x, const double* b, int n, const EngineArgs& a,
+                          int& seq, double& out) {
+    double s0[1], mx[1] = {0.0};
+    for_points(t, n, [&](int i, int j, int k) {
+        const Nb o = neighbours(n, i, j, k);
+        const double lx = lap7(o, [&](long q) { return x[q]; });
+        mx[0] = fmax(mx[0], fabs(lx + -1.0 * b[o.c]));
+    });
+    const bool ok = grid_reduce<0, 1>(s0, mx, a, seq);
+    out = mx[0];
+    return ok;
+}
+
+__global__ void __launch_bounds__(kThreads, kMinBlocksPerSM) engine_kernel(EngineArgs a) {
+    const Team t = make_team();
+    int seq = 0;
+    bool ok = true;
+    int result = 0;
+    const int n = a.n;
+
+    switch (a.prog) {
+    case PROG_LAPLACE:
+        for_points(t, n, [&](int i, int j, int k) {
+            const Nb o = neighbours(n, i, j, k);
+            a.out[o.c] = lap7(o, [&](long q) { return a.u[q]; });
+        });
+        break;
+
+    case PROG_CG:
+    case PROG_PCG:
+    case PROG_CG_COARSE: {
+        CgSpec s;
+        s.n = n; s.b = a.b; s.x0 = a.x0; s.x = a.x; s.r = a.r; s.p0 = a.p0; s.p1 = a.p1; s.Ap = a.Ap;
+        s.v = a.v; s.kind = a.prog == PROG_PCG ? a.precond : PC_IMPLICIT;
+        s.coarse = a.prog == PROG_CG_COARSE; s.tol = a.tol; s.rtol = a.rtol;
+        s.limit = s.coarse ? a.maxit : (long)n * n;
+        if (s.coarse) result = cg_run<PC_IMPLICIT, true>(t, s, a, seq, ok);
+        else if (s.kind == PC_JACOBI) result = cg_run<PC_JACOBI, false>(t, s, a, seq, ok);
+        else if (s.kind == PC_MG) result = cg_run<PC_MG, false>(t, s, a, seq, ok);
+        else result = cg_run<PC_IMPLICIT, false>(t, s, a, seq, ok);
+        break;
+    }
+
+    case PROG_SMOOTH:
+        for (int it = 0; it < a.sm && ok; it++) ok = rbgs(t, a.b, a.x, n, a);
+        break;
+
+    case PROG_RESTRICT:
+        restrict27(t, a.u, a.out, n);
+        break;
+
+    case PROG_PROLONG:  // n is the coarse size here
+        for_points(t, 2 * n, [&](int i, int j, int k) {
+            a.out[((long)i * 2 * n + j) * 2 * n + k] = prolong_at(a.u, n, i, j, k);
+        });
+        break;
+
+    case PROG_MG_APPLY:
+        ok = vcycle(t, a.b, a.x, n, a.sm, a, seq);
+        break;
+
+    case PROG_INIT_FIELD:
+    case PROG_LCG_UPDATE: {
+        // INIT:   y = 0; phi = c q; CG(b = phi, x0 = y, x = phi)   (grid_lcg.c:100-124)
+        // UPDATE: y = c q; CG(b = y, x0 = phi_prev, x = phi)      (grid_lcg.c:126-149)
+        const bool init = a.prog == PROG_INIT_FIELD;
+        for_points(t, n, [&](int i, int j, int k) {
+            const long c = ((long)i * n + j) * n + k;
+            const double bq = a.q[c] * a.c;
+            if (init) { a.y[c] = 0.0; a.phi_new[c] = bq; }
+            else a.y[c] = bq;
+        });
+        ok = grid_sync(a.bar);
+        if (!ok) break;
+        CgSpec s;
+        s.n = n; s.b = init ? a.phi_new : a.y; s.x0 = init ? a.y : a.phi_old; s.x = a.phi_new;
+        s.r = a.r; s.p0 = a.p0; s.p1 = a.p1; s.Ap = a.Ap; s.v = a.v; s.kind = PC_IMPLICIT;
+        s.coarse = false; s.tol = a.tol; s.rtol = 0.0; s.limit = (long)n * n;
+        result = cg_run<PC_IMPLICIT, false>(t, s, a, seq, ok);
+        break;
+    }
+
+    case PROG_MAZE_LCG:
+    case PROG_MAZE_MG:
+    case PROG_MG_UPDATE: {
+        // phi_new = 2 phi - phi_prev (verlet.c:46-51). MaZe: tmp = L phi_new + c q,
+        // the constraint sigma_p (verlet.c:54-55,108-110). MULTIGRID: tmp = c q.
+        const bool maze = a.prog != PROG_MG_UPDATE;
+        for_points(t, n, [&](int i, int j, int k) {
+            const Nb o = neighbours(n, i, j, k);
+            auto ex = [&](long q) { return 2 * a.phi_old[q] - a.phi_prev[q]; };
+            const double pc = ex(o.c);
+            a.phi_new[o.c] = pc;
+            if (maze) a.tmp[o.c] = lap7(o, ex) + a.c * a.q[o.c];
+            else a.tmp[o.c] = a.q[o.c] * a.c;
+        });
+        ok = grid_sync(a.bar);
+        if (!ok) break;
+        double* sol = maze ? a.y : a.phi_new;
+        if (a.prog == PROG_MAZE_LCG) {
+            CgSpec s;
+            s.n = n; s.b = a.tmp; s.x0 = a.y; s.x = a.y; s.r = a.r; s.p0 = a.p0; s.p1 = a.p1;
+            s.Ap = a.Ap; s.v = a.v; s.kind = a.precond; s.coarse = false; s.tol = a.tol;
+            s.rtol = 0.0; s.limit = (long)n * n;
+            if (a.precond == PC_JACOBI) result = cg_run<PC_JACOBI, false>(t, s, a, seq, ok);
+            else if (a.precond == PC_MG) result = cg_run<PC_MG, false>(t, s, a, seq, ok);
+            else result = cg_run<PC_IMPLICIT, false>(t, s, a, seq, ok);
+            if (!ok) break;
+        } else {
+            // repeat V-cycles until |L sol - tmp|_inf <= tol, at most 1000
+            // (grid_multigrid.c:185-206, verlet.c:121-136)
+            result = -1;
+            int it = 0;
+            while (it < 1000) {
+                ok = vcycle(t, a.tmp, sol, n, 3, a, seq);
+                if (!ok) break;
+                double rmax;
+                ok = resid_max(t, sol, a.tmp, n, a, seq, rmax);
+                if (!ok) break;
+                it++;
+                if (rmax <= a.tol) { result = it; break; }
+            }
+            if (!ok) break;
+        }
+        if (maze) {
+            for_points(t, n, [&](int i, int j, int k) {
+                const long c = ((long)i * n + j) * n + k;
+                a.phi_new[c] = a.phi_new[c] + -1.0 * a.y[c];
+            });
+        }
+        break;
+    }
+    default:
+        ok = false;
+        break;
+    }
+
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.result[0] = result;
+        a.result[1] = ok ? 0 : 1;
+    }
+}
+
+struct EngineShape {
+    int device = -1;
+    int blocks = 0;
+};
+EngineShape g_shape;
+
+void ensure_shape() {
+    int dev;
+    MZB_CHECK(cudaGetDevice(&dev));
+    if (g_shape.device == dev) return;
+    int sms = 0, per_sm = 0;
+    MZB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MZB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, engine_kernel, kThreads, 0));
+    if (per_sm < 1) fatal("solver engine: kernel cannot be resident on this device");
+    g_shape.device = dev;
+    g_shape.blocks = sms * (per_sm < kMinBlocksPerSM ? per_sm : kMinBlocksPerSM);
+}
+
+}  // namespace
+
+int engine_grid_blocks() {
+    ensure_shape();
+    return g_shape.blocks;
+}
+
+void engine_launch(const EngineArgs& a, cudaStream_t stream) {
+    ensure_shape();
+    MZB_CHECK(cudaMemsetAsync(a.bar, 0, sizeof(GridBarrier), stream));
+    EngineArgs copy = a;
+    void* params[] = {&copy};
+    count_launch();
+    MZB_CHECK(cudaLaunchCooperativeKernel((const void*)engine_kernel, dim3(g_shape.blocks),
+                                          dim3(kThreads), params, 0, stream));
+}
+
+}  // namespace mzb

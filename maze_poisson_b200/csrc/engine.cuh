@@ -1,0 +1,78 @@
+// Persistent "solver engine": one cooperative launch runs a whole field solve (CG, PCG,
+// V-cycles, MaZe constraint solve) with grid barriers between the sweeps, so no solve
+// pays a launch or a host round trip per iteration.
+#pragma once
+
+#include "mzb_common.cuh"
+
+namespace mzb {
+
+enum EngineProg : int {
+    PROG_LAPLACE = 1,     // out = L u
+    PROG_CG = 2,          // conj_grad(b, x0 -> x)                      plcg.c:28-90
+    PROG_PCG = 3,         // conj_grad_precond(b, x0 -> x, precond)     plcg.c:104-166
+    PROG_SMOOTH = 4,      // x <- RBGS^sm (rhs=b, x)                    multigrid.c:636-729
+    PROG_RESTRICT = 5,    // out(coarse) = R27 u(fine)                  multigrid.c:523-594
+    PROG_PROLONG = 6,     // out(fine) = P u(coarse)                    multigrid.c:393-463
+    PROG_CG_COARSE = 7,   // cg_coarse(b, x) on n^3                     multigrid.c:13-96
+    PROG_MG_APPLY = 8,    // one V-cycle: x <- MG(b, x)                 multigrid.c:99-168
+    PROG_INIT_FIELD = 9,  // y=0; phi_prev=phi; phi = CG(c*q, 0)        grid_lcg.c:100-124
+    PROG_LCG_UPDATE = 10, // phi_prev=phi; phi = CG(c*q, phi_prev)      grid_lcg.c:126-149
+    PROG_MAZE_LCG = 11,   // verlet_poisson                             verlet.c:31-71
+    PROG_MG_UPDATE = 12,  // multigrid_grid_update_field                grid_multigrid.c:110-212
+    PROG_MAZE_MG = 13,    // verlet_poisson_multigrid                   verlet.c:86-149
+};
+
+enum PrecondKind : int { PC_IMPLICIT = 0, PC_JACOBI = 1, PC_MG = 2 };
+
+struct EngineArgs {
+    int prog;
+    int n;          // fine grid points per side
+    int precond;    // PrecondKind for PROG_PCG / PROG_MAZE_LCG
+    int sm;         // RBGS sweeps per V-cycle half (PROG_SMOOTH / PROG_MG_APPLY)
+    int maxit;      // PROG_CG_COARSE
+    double tol;     // absolute inf-norm tolerance
+    double rtol;    // PROG_CG_COARSE
+    double c;       // right-hand-side constant applied to q
+
+    // field state (PROG_INIT_FIELD .. PROG_MAZE_MG)
+    const double* q;
+    const double* phi_old;   // phi at entry
+    const double* phi_prev;  // phi_prev at entry
+    double* phi_new;         // phi at exit (never aliases phi_old / phi_prev)
+    double* y;
+
+    // kernel-level programs
+    const double* b;
+    const double* x0;
+    double* x;
+    const double* u;
+    double* out;
+
+    // fine work arrays (n^3)
+    double* r;
+    double* p0;
+    double* p1;
+    double* Ap;
+    double* v;
+    double* rf;
+    double* tmp;
+    // coarse work arrays ((n/2)^3)
+    double* rc;
+    double* ec;
+    double* cr;
+    double* cp0;
+    double* cp1;
+    double* cAp;
+
+    double* partials;  // 2 sets x 8 values x gridDim.x
+    GridBarrier* bar;
+    int* result;       // [0] program return value, [1] engine status (0 ok)
+};
+
+// Launch the engine for `a` on `stream` (cooperative; shapes chosen once per device).
+void engine_launch(const EngineArgs& a, cudaStream_t stream);
+// Bytes of partials the engine needs and its grid size on this device.
+int engine_grid_blocks();
+
+}  // namespace mzb

@@ -1,0 +1,932 @@
+// C-ABI facade of libmaze_poisson.so for B200: the symbols, argument meanings and error
+// behaviour of the reference's library/src/solver_md.c (plus the enum/string getters of
+// grid_general.c, particles.c, integrator_general.c and the serial MPI stubs of
+// mpi_base.c), so that maze_poisson/c_api (ctypes) loads it unchanged.
+//
+// One global system lives on the GPU. Host<->device traffic happens only where the ABI
+// moves data: the initialisers and setters (H2D), the getters (D2H) and the scalar
+// returns of solver_update_charges / solver_update_field / solver_compute_forces_noel.
+// Fatal conditions print a message and exit(1) exactly where the reference does.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.cuh"
+#include "fft.cuh"
+#include "particles.cuh"
+
+namespace mzb {
+
+void fatal_cuda(cudaError_t e, const char* what, const char* file, int line) {
+    fprintf(stderr, "maze_poisson_b200: CUDA error '%s' in %s (%s:%d)\n", cudaGetErrorString(e), what,
+            file, line);
+    exit(1);
+}
+void fatal(const char* msg) {
+    fprintf(stderr, "maze_poisson_b200: %s\n", msg);
+    exit(1);
+}
+unsigned long long g_kernel_launches = 0;
+
+namespace {
+
+enum GridType { G_LCG = 0, G_FFT = 1, G_MG = 2, G_MAZE_LCG = 3, G_MAZE_MG = 4 };
+enum Precond { P_NONE = 0, P_JACOBI = 1, P_MG = 2, P_SSOR = 3, P_BLOCKJACOBI = 4 };
+
+const char* kGridNames[5] = {"LCG", "FFT", "MULTIGRID", "MAZE-LCG", "MAZE-MULTIGRID"};
+const char* kPrecondNames[5] = {"NONE", "JACOBI", "MG", "SSOR", "BLOCKJACOBI"};
+const char* kPotentialNames[3] = {"TF", "LJ", "SC"};
+const char* kCasNames[3] = {"CIC", "SPL_QUADR", "SPL_CUBIC"};
+const char* kIntegratorNames[2] = {"OVRVO", "VERLET"};
+
+template <class T>
+T* dalloc(size_t count) {
+    T* p = nullptr;
+    if (count == 0) count = 1;
+    MZB_CHECK(cudaMalloc(&p, sizeof(T) * count));
+    MZB_CHECK(cudaMemset(p, 0, sizeof(T) * count));
+    return p;
+}
+template <class T>
+void dfree(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+struct GridState {
+    bool ready = false;
+    int type = 0, precond = 0, n = 0;
+    double L = 0, h = 0, tol = 0, eps_s = 1, eps_int = 1;
+    long m = 0;
+    double* q = nullptr;
+    double* buf[3] = {nullptr, nullptr, nullptr};  // phi / phi_prev / spare (renamed)
+    int iphi = 0, iprev = 1, ispare = 2;
+    double* y = nullptr;
+    double *r = nullptr, *p0 = nullptr, *p1 = nullptr, *Ap = nullptr, *v = nullptr, *rf = nullptr,
+           *tmp = nullptr;
+    double *rc = nullptr, *ec = nullptr, *cr = nullptr, *cp0 = nullptr, *cp1 = nullptr, *cAp = nullptr;
+    FftPoisson fft;
+
+    double* phi() const { return buf[iphi]; }
+    double* phi_prev() const { return buf[iprev]; }
+};
+
+struct System {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    GridState G;
+    ParticleDev P;
+    IntegratorDev I;
+    bool parts_ready = false, integ_ready = false;
+    double* partials = nullptr;
+    GridBarrier* bar = nullptr;
+    int* result = nullptr;       // device
+    int* result_h = nullptr;     // pinned
+    double* red_h = nullptr;     // pinned copy of P.red
+    double* scratch_d = nullptr; // small device scratch (energies, reductions)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the last solver-engine launch
+    float last_solve_ms = 0.f;
+    int last_solve_iters = 0;
+};
+
+System* g = nullptr;
+double g_q_tot = 0.0;  // persists across systems like solver_md.c:16
+bool g_quiet = false;
+
+System& sys() {
+    if (!g) fatal("solver_initialize() has not been called");
+    return *g;
+}
+GridState& grid() {
+    System& s = sys();
+    if (!s.G.ready) fatal("solver_initialize_grid() has not been called");
+    return s.G;
+}
+ParticleDev& parts() {
+    System& s = sys();
+    if (!s.parts_ready) fatal("solver_initialize_particles() has not been called");
+    return s.P;
+}
+
+void sync() { MZB_CHECK(cudaStreamSynchronize(sys().stream)); }
+
+void free_grid(GridState& G) {
+    dfree(G.q);
+    for (auto& b : G.buf) dfree(b);
+    dfree(G.y);
+    dfree(G.r); dfree(G.p0); dfree(G.p1); dfree(G.Ap); dfree(G.v); dfree(G.rf); dfree(G.tmp);
+    dfree(G.rc); dfree(G.ec); dfree(G.cr); dfree(G.cp0); dfree(G.cp1); dfree(G.cAp);
+    G.fft.release();
+    G.ready = false;
+}
+
+void free_particles(ParticleDev& P) {
+    dfree(P.types); dfree(P.pos); dfree(P.vel); dfree(P.fe); dfree(P.fn); dfree(P.ft);
+    dfree(P.mass); dfree(P.chg); dfree(P.tab); dfree(P.base);
+    dfree(P.tile_count); dfree(P.tile_start); dfree(P.tile_fill); dfree(P.tile_ions);
+    dfree(P.cell_of); dfree(P.cell_count); dfree(P.cell_start); dfree(P.cell_fill);
+    dfree(P.cell_ions); dfree(P.srank); dfree(P.spos); dfree(P.stype); dfree(P.fpart);
+    dfree(P.epart); dfree(P.red); dfree(P.flags); dfree(P.partial);
+    P = ParticleDev{};
+}
+
+// Linked-cell geometry for the Tosi-Fumi kernel: about 16 ions per cell, at least one
+// cell per side; warps split the partner cells so that ~12k warps are in flight.
+void set_cells(ParticleDev& P, int nc) {
+    dfree(P.cell_count); dfree(P.cell_start); dfree(P.cell_fill); dfree(P.fpart); dfree(P.epart);
+    P.nc = nc < 1 ? 1 : nc;
+    P.ncell = P.nc * P.nc * P.nc;
+    int split = (12000 + P.ncell - 1) / P.ncell;
+    P.tf_split = split < 1 ? 1 : (split > P.ncell ? P.ncell : split);
+    P.cell_count = dalloc<int32_t>(P.ncell);
+    P.cell_start = dalloc<int32_t>(P.ncell + 1);
+    P.cell_fill = dalloc<int32_t>(P.ncell);
+    P.fpart = dalloc<double>((size_t)P.tf_split * P.np * 3);
+    P.epart = dalloc<double>((size_t)P.ncell * P.tf_split);
+}
+
+EngineArgs engine_base(System& s) {
+    GridState& G = s.G;
+    EngineArgs a{};
+    a.n = G.n;
+    a.tol = G.tol;
+    a.r = G.r; a.p0 = G.p0; a.p1 = G.p1; a.Ap = G.Ap; a.v = G.v; a.rf = G.rf; a.tmp = G.tmp;
+    a.rc = G.rc; a.ec = G.ec; a.cr = G.cr; a.cp0 = G.cp0; a.cp1 = G.cp1; a.cAp = G.cAp;
+    a.partials = s.partials;
+    a.bar = s.bar;
+    a.result = s.result;
+    a.q = G.q;
+    a.y = G.y;
+    return a;
+}
+
+// Run the engine and return its result; an engine failure (a barrier that timed out)
+// is reported and turned into -1 ("not converged").
+int run_engine(System& s, const EngineArgs& a) {
+    MZB_CHECK(cudaEventRecord(s.ev0, s.stream));
+    engine_launch(a, s.stream);
+    MZB_CHECK(cudaEventRecord(s.ev1, s.stream));
+    MZB_CHECK(cudaMemcpyAsync(s.result_h, s.result, 2 * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    MZB_CHECK(cudaStreamSynchronize(s.stream));
+    MZB_CHECK(cudaEventElapsedTime(&s.last_solve_ms, s.ev0, s.ev1));
+    s.last_solve_iters = s.result_h[0];
+    if (s.result_h[1] != 0) {
+        fprintf(stderr, "maze_poisson_b200: solver engine aborted (grid barrier timeout)\n");
+        return -1;
+    }
+    return s.result_h[0];
+}
+
+void require_mg_size(int n) {
+    // multigrid.c:114-121: at least one level of recursion, n/2 >= 16
+    if (n / 2 < 16 || n % 2) fatal("Multigrid: requires an even grid with n/2 >= 16");
+}
+
+double rhs_const(const GridState& G) {
+    double c = -4 * kPi / G.h;  // grid_lcg.c:418-422
+    return c / G.eps_s;
+}
+
+}  // namespace
+}  // namespace mzb
+
+using namespace mzb;
+
+extern "C" {
+
+// ---------------------------------------------------------------- serial MPI stubs
+int init_mpi(void) { return 0; }  // mpi_base.c:169-177 (serial build)
+int get_rank(void) { return 0; }
+
+// ---------------------------------------------------------------- enum tables
+int get_grid_type_num(void) { return 5; }
+char* get_grid_type_str(int i) { return (char*)kGridNames[i]; }
+int get_precond_type_num(void) { return 5; }
+char* get_precond_type_str(int i) { return (char*)kPrecondNames[i]; }
+int get_potential_type_num(void) { return 3; }
+char* get_potential_type_str(int i) { return (char*)kPotentialNames[i]; }
+int get_ca_scheme_type_num(void) { return 3; }
+char* get_ca_scheme_type_str(int i) { return (char*)kCasNames[i]; }
+int get_integrator_type_num(void) { return 2; }
+char* get_integrator_type_str(int i) { return (char*)kIntegratorNames[i]; }
+
+// ---------------------------------------------------------------- lifecycle
+void solver_initialize(void) {
+    if (!g) g = new System();
+    const char* dev = getenv("MZB_DEVICE");
+    g->device = dev ? atoi(dev) : 0;
+    g_quiet = getenv("MZB_QUIET") != nullptr;
+    MZB_CHECK(cudaSetDevice(g->device));
+    if (!g->stream) MZB_CHECK(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    if (!g->partials) {
+        const int blocks = engine_grid_blocks();
+        g->partials = dalloc<double>((size_t)2 * 8 * blocks);
+        g->bar = dalloc<GridBarrier>(1);
+        g->result = dalloc<int>(2);
+        MZB_CHECK(cudaMallocHost(&g->result_h, 2 * sizeof(int)));
+        MZB_CHECK(cudaMallocHost(&g->red_h, 8 * sizeof(double)));
+        g->scratch_d = dalloc<double>(4096);
+        MZB_CHECK(cudaEventCreate(&g->ev0));
+        MZB_CHECK(cudaEventCreate(&g->ev1));
+    }
+    if (!g_quiet) {
+        cudaDeviceProp prop;
+        MZB_CHECK(cudaGetDeviceProperties(&prop, g->device));
+        printf("******************************************************\n");
+        printf("* MAZE_POISSON (B200 CUDA build)\n");
+        printf("*   GPU     %s, %d SMs\n", prop.name, prop.multiProcessorCount);
+        printf("******************************************************\n");
+    }
+}
+
+void solver_initialize_grid(int n, double L, double h, double tol, double eps, double eps_int,
+                            int grid_type, int precond_type) {
+    System& s = sys();
+    GridState& G = s.G;
+    if (G.ready) free_grid(G);
+    if (grid_type < 0 || grid_type > 4) fatal("invalid grid type");
+    if (n < 2) fatal("grid size must be at least 2");
+    G.type = grid_type;
+    G.precond = precond_type;
+    G.n = n;
+    G.L = L;
+    G.h = h;
+    G.tol = tol;
+    G.eps_s = eps;
+    G.eps_int = eps_int;
+    G.m = (long)n * n * n;
+    G.iphi = 0; G.iprev = 1; G.ispare = 2;
+    G.q = dalloc<double>(G.m);
+    G.buf[0] = dalloc<double>(G.m);
+    if (grid_type == G_FFT) {
+        G.fft.init(n, L, h);
+    } else {
+        if (grid_type == G_MG || grid_type == G_MAZE_MG) require_mg_size(n);
+        if (n % 2) fatal("this build requires an even grid size (red-black smoothing, multigrid)");
+        G.buf[1] = dalloc<double>(G.m);
+        G.buf[2] = dalloc<double>(G.m);
+        G.y = dalloc<double>(G.m);
+        G.r = dalloc<double>(G.m); G.p0 = dalloc<double>(G.m); G.p1 = dalloc<double>(G.m);
+        G.Ap = dalloc<double>(G.m); G.tmp = dalloc<double>(G.m);
+        const bool mg = grid_type == G_MG || grid_type == G_MAZE_MG ||
+                        (grid_type == G_MAZE_LCG && precond_type == P_MG);
+        if (mg) {
+            require_mg_size(n);
+            const long mc = G.m / 8;
+            G.v = dalloc<double>(G.m); G.rf = dalloc<double>(G.m);
+            G.rc = dalloc<double>(mc); G.ec = dalloc<double>(mc); G.cr = dalloc<double>(mc);
+            G.cp0 = dalloc<double>(mc); G.cp1 = dalloc<double>(mc); G.cAp = dalloc<double>(mc);
+        }
+    }
+    G.ready = true;
+}
+
+void solver_initialize_grid_pois_boltz(double, double, int) {
+    fatal("Poisson-Boltzmann is not supported by this build");
+}
+
+void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, int pot_type, int cas_type,
+                                 int* types, double* pos, double* vel, double* mass, double* charges,
+                                 double* pot_params) {
+    System& s = sys();
+    if (pot_type != 0) fatal("only the Tosi-Fumi potential (TF) is supported by this build");
+    if (cas_type != 0) fatal("only CIC charge assignment is supported by this build");
+    if (n_typ < 1 || n_typ > 8) fatal("between 1 and 8 particle types are supported");
+    if (s.parts_ready) free_particles(s.P);
+    ParticleDev& P = s.P;
+    P.np = n_p;
+    P.ntyp = n_typ;
+    P.n = n;
+    P.L = L;
+    P.h = h;
+    P.rcut = L / 2.0;  // particles.c:189
+    const size_t v3 = (size_t)3 * n_p;
+    P.types = dalloc<int32_t>(n_p);
+    P.pos = dalloc<double>(v3);
+    P.vel = dalloc<double>(v3);
+    P.fe = dalloc<double>(v3);
+    P.fn = dalloc<double>(v3);
+    P.ft = dalloc<double>(v3);
+    P.mass = dalloc<double>(n_p);
+    P.chg = dalloc<double>(n_p);
+    P.base = dalloc<int32_t>(v3);
+    if (n_p > 0) {
+        MZB_CHECK(cudaMemcpy(P.types, types, sizeof(int32_t) * n_p, cudaMemcpyHostToDevice));
+        MZB_CHECK(cudaMemcpy(P.pos, pos, sizeof(double) * v3, cudaMemcpyHostToDevice));
+        MZB_CHECK(cudaMemcpy(P.vel, vel, sizeof(double) * v3, cudaMemcpyHostToDevice));
+        MZB_CHECK(cudaMemcpy(P.mass, mass, sizeof(double) * n_p, cudaMemcpyHostToDevice));
+        MZB_CHECK(cudaMemcpy(P.chg, charges, sizeof(double) * n_p, cudaMemcpyHostToDevice));
+    }
+    // Tosi-Fumi constants per type pair (particles.c:181-228)
+    std::vector<double> tab((size_t)n_typ * n_typ * 7);
+    const double rc = L / 2.0, rc6 = pow(rc, 6), rc7 = rc6 * rc, rc8 = rc7 * rc, rc9 = rc8 * rc;
+    for (int t = 0; t < n_typ * n_typ; t++) {
+        const double A = pot_params[5 * t], B = pot_params[5 * t + 1], C = pot_params[5 * t + 2],
+                     D = pot_params[5 * t + 3], sg = pot_params[5 * t + 4];
+        const double ea = exp(B * (sg - rc));
+        const double vs = A * ea - C / rc6 - D / rc8;
+        const double al = A * B * ea - 6 * C / rc7 - 8 * D / rc9;
+        const double be = -vs - al * rc;
+        double* o = &tab[7 * t];
+        o[0] = A; o[1] = B; o[2] = C; o[3] = D; o[4] = sg; o[5] = al; o[6] = be;
+    }
+    P.tab = dalloc<double>(tab.size());
+    MZB_CHECK(cudaMemcpy(P.tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+    // spreading tiles over the grid
+    P.nti = (n + kTileI - 1) / kTileI;
+    P.ntj = (n + kTileJ - 1) / kTileJ;
+    P.ntk = (n + kTileK - 1) / kTileK;
+    P.ntiles = P.nti * P.ntj * P.ntk;
+    P.tile_count = dalloc<int32_t>(P.ntiles);
+    P.tile_start = dalloc<int32_t>(P.ntiles + 1);
+    P.tile_fill = dalloc<int32_t>(P.ntiles);
+    P.tile_ions = dalloc<int32_t>(n_p);
+    // linked cells
+    P.cell_of = dalloc<int32_t>(n_p);
+    P.cell_ions = dalloc<int32_t>(n_p);
+    P.srank = dalloc<int32_t>(n_p);
+    P.spos = dalloc<double>(v3);
+    P.stype = dalloc<int32_t>(n_p);
+    const int nc = (int)std::lround(std::cbrt(n_p / 16.0));
+    set_cells(P, nc < 1 ? 1 : nc);
+    P.red = dalloc<double>(16);
+    P.flags = dalloc<int>(4);
+    P.partial = dalloc<double>((size_t)4 * ((n_p + 127) / 128) + 64);
+    s.parts_ready = true;
+}
+
+void solver_initialize_particles_pois_boltz(double, double, double*) {
+    fatal("Poisson-Boltzmann is not supported by this build");
+}
+
+void solver_initialize_integrator(int n_p, double dt, double T, double gamma, int itg_type, int itg_enabled) {
+    System& s = sys();
+    (void)n_p;
+    IntegratorDev& I = s.I;
+    const uint64_t seed = I.seed;
+    I = IntegratorDev{};
+    I.seed = seed;
+    I.type = itg_type;
+    I.dt = dt;
+    if (itg_enabled == 1) {  // *_integrator_init_thermostat
+        I.T = T;
+        I.enabled = 1;
+        if (itg_type == 0) {
+            I.c1 = exp(-gamma * dt);
+            I.c2 = sqrt(2 / (gamma * dt) * tanh(0.5 * gamma * dt));
+        }
+    }
+    s.integ_ready = true;
+}
+
+// solver_md.c:91-107
+int solver_update_charges(void) {
+    System& s = sys();
+    GridState& G = grid();
+    ParticleDev& P = parts();
+    spread_charges(P, G.q, G.n, G.h, s.stream);
+    MZB_CHECK(cudaMemcpyAsync(s.red_h, P.red, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    int flag = 0;
+    MZB_CHECK(cudaMemcpyAsync(s.result_h, P.flags, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    sync();
+    flag = s.result_h[0];
+    if (flag) fatal("charge spreading: more than 2048 ions reach one 4x4x32 grid tile");
+    const double q_loc = s.red_h[0];
+    int res = 0;
+    if (fabs(g_q_tot - q_loc) > 1e-6) {
+        res = 1;
+        printf("Charge conservation error: q_tot = %.6f, q_tot_loc = %.6f\n", g_q_tot, q_loc);
+        exit(1);
+    }
+    g_q_tot = q_loc;
+    return res;
+}
+
+void solver_init_field(void) {
+    System& s = sys();
+    GridState& G = grid();
+    if (G.type == G_FFT) {  // grid_fft.c:135-137
+        G.fft.solve(G.q, G.phi(), s.stream);
+        sync();
+        return;
+    }
+    EngineArgs a = engine_base(s);
+    a.prog = PROG_INIT_FIELD;
+    a.c = rhs_const(G);
+    a.phi_old = G.phi();
+    a.phi_prev = G.phi_prev();
+    a.phi_new = G.buf[G.ispare];
+    run_engine(s, a);
+    // phi_prev <- old phi, phi <- solution
+    const int old = G.iphi;
+    G.iphi = G.ispare;
+    G.ispare = G.iprev;
+    G.iprev = old;
+}
+
+int solver_update_field(void) {
+    System& s = sys();
+    GridState& G = grid();
+    if (G.type == G_FFT) {  // grid_fft.c:139-143
+        G.fft.solve(G.q, G.phi(), s.stream);
+        sync();
+        return 0;
+    }
+    EngineArgs a = engine_base(s);
+    a.phi_old = G.phi();
+    a.phi_prev = G.phi_prev();
+    a.phi_new = G.buf[G.ispare];
+    switch (G.type) {
+    case G_LCG:
+        a.prog = PROG_LCG_UPDATE;
+        a.c = rhs_const(G);
+        break;
+    case G_MAZE_LCG:
+        a.prog = PROG_MAZE_LCG;
+        a.c = (4 * kPi) / (G.h * G.eps_s);  // verlet.c:55 with h <- h*eps (grid_maze_lcg.c:158)
+        if (G.precond == P_NONE) a.precond = PC_IMPLICIT;
+        else if (G.precond == P_JACOBI) a.precond = PC_JACOBI;
+        else if (G.precond == P_MG) a.precond = PC_MG;
+        else fatal("SSOR and BLOCKJACOBI preconditioners are not supported by this build");
+        break;
+    case G_MG:
+        a.prog = PROG_MG_UPDATE;
+        a.c = rhs_const(G);
+        break;
+    case G_MAZE_MG:
+        a.prog = PROG_MAZE_MG;
+        a.c = (4 * kPi) / (G.h * G.eps_s);
+        break;
+    }
+    const int res = run_engine(s, a);
+    const int old = G.iphi;
+    G.iphi = G.ispare;
+    G.ispare = G.iprev;
+    G.iprev = old;
+    if (G.type == G_MAZE_MG) {
+        if (res == -1) fprintf(stderr, "Warning: Multigrid did not converge after 1000 iterations.\n");
+        if (G.precond != P_NONE) {  // grid_maze_multigrid.c:138-141
+            fprintf(stderr, "Maze Multigrid with preconditioner not implemented yet.\n");
+            exit(1);
+        }
+    }
+    return res;
+}
+
+void solver_set_field(double* phi) {
+    System& s = sys();
+    GridState& G = grid();
+    MZB_CHECK(cudaMemcpyAsync(G.phi(), phi, sizeof(double) * G.m, cudaMemcpyHostToDevice, s.stream));
+    sync();
+}
+
+void solver_set_field_prev(double* phi) {
+    System& s = sys();
+    GridState& G = grid();
+    if (G.type == G_FFT) return;  // no phi_prev (solver_md.c:119-129)
+    MZB_CHECK(cudaMemcpyAsync(G.phi_prev(), phi, sizeof(double) * G.m, cudaMemcpyHostToDevice, s.stream));
+    sync();
+}
+
+void solver_update_eps_k2(void) { fatal("Poisson-Boltzmann is not supported by this build"); }
+
+void solver_compute_forces_elec(void) {
+    System& s = sys();
+    GridState& G = grid();
+    field_forces(parts(), G.phi(), G.n, G.h, s.stream);
+}
+
+double solver_compute_forces_noel(void) {
+    System& s = sys();
+    ParticleDev& P = parts();
+    build_cells(P, s.stream);
+    tf_forces(P, s.stream);
+    MZB_CHECK(cudaMemcpyAsync(s.red_h + 1, P.red + 1, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    sync();
+    return s.red_h[1];
+}
+
+double solver_compute_forces_pb(void) {
+    fatal("Poisson-Boltzmann is not supported by this build");
+}
+
+void solver_compute_forces_tot(void) { total_forces(parts(), sys().stream); }
+
+void integrator_part_1(void) {
+    System& s = sys();
+    if (!s.integ_ready) fatal("solver_initialize_integrator() has not been called");
+    mzb::integrator_part1(parts(), s.I, s.stream);
+}
+
+void integrator_part_2(void) {
+    System& s = sys();
+    if (!s.integ_ready) fatal("solver_initialize_integrator() has not been called");
+    mzb::integrator_part2(parts(), s.I, s.stream);
+}
+
+double get_temperature(void);
+
+int solver_check_thermostat(void) {  // solver_md.c:210-221
+    System& s = sys();
+    int res = 0;
+    if (s.I.enabled == 1) {
+        const double temp = get_temperature();
+        if (fabs(temp - s.I.T) < 100) {
+            res = 1;
+            s.I.enabled = 0;
+            if (s.I.type == 0) {
+                s.I.c1 = 1.0;
+                s.I.c2 = 1.0;
+            }
+        }
+    }
+    return res;
+}
+
+void solver_rescale_velocities(void) { mzb::rescale_velocities(parts(), sys().stream); }
+
+void solver_finalize(void) {
+    if (!g) return;
+    if (g->stream) cudaStreamSynchronize(g->stream);
+    if (g->G.ready) free_grid(g->G);
+    if (g->parts_ready) free_particles(g->P);
+    g->parts_ready = false;
+    g->integ_ready = false;
+}
+
+// ---------------------------------------------------------------- getters (solver_md.c:247-354)
+static void d2h(void* dst, const void* src, size_t bytes) {
+    System& s = sys();
+    if (bytes == 0) return;
+    MZB_CHECK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s.stream));
+    sync();
+}
+
+void get_pos(double* recv) { ParticleDev& P = parts(); d2h(recv, P.pos, sizeof(double) * 3 * P.np); }
+void get_vel(double* recv) { ParticleDev& P = parts(); d2h(recv, P.vel, sizeof(double) * 3 * P.np); }
+void get_fcs_elec(double* recv) { ParticleDev& P = parts(); d2h(recv, P.fe, sizeof(double) * 3 * P.np); }
+void get_fcs_noel(double* recv) { ParticleDev& P = parts(); d2h(recv, P.fn, sizeof(double) * 3 * P.np); }
+void get_fcs_tot(double* recv) { ParticleDev& P = parts(); d2h(recv, P.ft, sizeof(double) * 3 * P.np); }
+void get_fcs_db(double* recv) { memset(recv, 0, sizeof(double) * 3 * parts().np); }
+void get_fcs_ib(double* recv) { memset(recv, 0, sizeof(double) * 3 * parts().np); }
+void get_fcs_np(double* recv) { memset(recv, 0, sizeof(double) * 3 * parts().np); }
+void get_types(int* recv) { ParticleDev& P = parts(); d2h(recv, P.types, sizeof(int32_t) * P.np); }
+void get_charges(double* recv) { ParticleDev& P = parts(); d2h(recv, P.chg, sizeof(double) * P.np); }
+void get_masses(double* recv) { ParticleDev& P = parts(); d2h(recv, P.mass, sizeof(double) * P.np); }
+void get_radii(double* recv) { memset(recv, 0, sizeof(double) * parts().np); }
+void get_field(double* recv) { GridState& G = grid(); d2h(recv, G.phi(), sizeof(double) * G.m); }
+void get_field_prev(double* recv) {
+    GridState& G = grid();
+    d2h(recv, G.type == G_FFT ? G.phi() : G.phi_prev(), sizeof(double) * G.m);
+}
+void get_q(double* recv) { GridState& G = grid(); d2h(recv, G.q, sizeof(double) * G.m); }
+
+double get_kinetic_energy(void) {
+    System& s = sys();
+    ParticleDev& P = parts();
+    kinetic_and_momentum(P, s.stream);
+    d2h(s.red_h, P.red, sizeof(double) * 8);
+    return s.red_h[2];
+}
+
+double get_temperature(void) {  // particles.c:798-800
+    System& s = sys();
+    ParticleDev& P = parts();
+    kinetic_and_momentum(P, s.stream);
+    d2h(s.red_h, P.red, sizeof(double) * 8);
+    return s.red_h[6];
+}
+
+void get_momentum(double* recv) {
+    System& s = sys();
+    ParticleDev& P = parts();
+    kinetic_and_momentum(P, s.stream);
+    d2h(s.red_h, P.red, sizeof(double) * 8);
+    recv[0] = s.red_h[3];
+    recv[1] = s.red_h[4];
+    recv[2] = s.red_h[5];
+}
+
+
+// grid_general.c:304-315: sum of 0.5*phi over the grid (what the reference computes)
+double get_energy_elec(void);
+
+}  // extern "C"
+
+// ====================================================================================
+// Extensions (no reference counterpart): kernel-level entry points on plain n^3 host
+// arrays for parity tests, accessors for the linked cells / CIC corners / O-block noise,
+// and a multi-step driver.
+// ====================================================================================
+namespace mzb {
+namespace {
+
+__global__ void k_half_sum(const double* __restrict__ phi, long m, double* __restrict__ part) {
+    double v[1] = {0.0};
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < m; t += (long)gridDim.x * blockDim.x)
+        v[0] += 0.5 * phi[t];
+    __shared__ double sh[4 * 32];
+    block_sum<1>(v, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+__global__ void k_sum_parts(const double* __restrict__ part, int nb, double* __restrict__ out) {
+    double s = 0.0;
+    for (int b = 0; b < nb; b++) s += part[b];
+    *out = s;
+}
+
+__global__ void k_cic_neighbors(const int32_t* __restrict__ base, int np, int n, int64_t* __restrict__ out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+    for (int c = 0; c < 8; c++)
+        for (int d = 0; d < 3; d++) {
+            const int b = base[3 * p + d];
+            out[(p * 8 + c) * 3 + d] = off[c][d] ? wrap_inc(b, n) : b;
+        }
+}
+
+// Temporary device work set for the kernel-level entry points.
+struct Work {
+    std::vector<double*> bufs;
+    double* get(size_t count) {
+        double* p = dalloc<double>(count);
+        bufs.push_back(p);
+        return p;
+    }
+    ~Work() {
+        for (double* p : bufs) cudaFree(p);
+    }
+};
+
+EngineArgs scratch_engine(System& s, Work& w, int n) {
+    const long m = (long)n * n * n, mc = m / 8 > 0 ? m / 8 : 1;
+    EngineArgs a{};
+    a.n = n;
+    a.r = w.get(m); a.p0 = w.get(m); a.p1 = w.get(m); a.Ap = w.get(m); a.v = w.get(m); a.rf = w.get(m);
+    a.tmp = w.get(m);
+    a.rc = w.get(mc); a.ec = w.get(mc); a.cr = w.get(mc); a.cp0 = w.get(mc); a.cp1 = w.get(mc);
+    a.cAp = w.get(mc);
+    a.partials = s.partials;
+    a.bar = s.bar;
+    a.result = s.result;
+    return a;
+}
+
+void h2d(double* d, const double* h, long m) {
+    MZB_CHECK(cudaMemcpy(d, h, sizeof(double) * m, cudaMemcpyHostToDevice));
+}
+void d2h_sync(double* h, const double* d, long m) {
+    MZB_CHECK(cudaMemcpy(h, d, sizeof(double) * m, cudaMemcpyDeviceToHost));
+}
+
+}  // namespace
+}  // namespace mzb
+
+extern "C" {
+
+double get_energy_elec(void) {
+    System& s = sys();
+    GridState& G = grid();
+    const int nb = 256;
+    count_launch();
+    k_half_sum<<<nb, 256, 0, s.stream>>>(G.phi(), G.m, s.scratch_d);
+    count_launch();
+    k_sum_parts<<<1, 1, 0, s.stream>>>(s.scratch_d, nb, s.scratch_d + nb);
+    MZB_CHECK(cudaGetLastError());
+    double out = 0.0;
+    MZB_CHECK(cudaMemcpyAsync(s.red_h, s.scratch_d + nb, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    sync();
+    out = s.red_h[0];
+    return out;
+}
+
+// out = L u (laplace.c:24-75) on plain n^3 arrays
+void mzb_laplace(const double* u, double* out, int n) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    EngineArgs a = scratch_engine(s, w, n);
+    double* du = w.get(m);
+    double* dout = w.get(m);
+    h2d(du, u, m);
+    a.prog = PROG_LAPLACE;
+    a.u = du;
+    a.out = dout;
+    run_engine(s, a);
+    d2h_sync(out, dout, m);
+}
+
+// conj_grad (plcg.c:28-90) and conj_grad_precond (plcg.c:104-166, precond 1 = JACOBI,
+// 2 = MG); returns the reference's return value.
+int mzb_conj_grad(const double* b, const double* x0, double* x, double tol, int n, int precond) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    if (precond == 2) require_mg_size(n);
+    EngineArgs a = scratch_engine(s, w, n);
+    double* db = w.get(m);
+    double* dx0 = w.get(m);
+    double* dx = w.get(m);
+    h2d(db, b, m);
+    h2d(dx0, x0, m);
+    a.prog = precond == 0 ? PROG_CG : PROG_PCG;
+    a.precond = precond;
+    a.tol = tol;
+    a.b = db;
+    a.x0 = dx0;
+    a.x = dx;
+    const int res = run_engine(s, a);
+    d2h_sync(x, dx, m);
+    return res;
+}
+
+// smooth_rbgs (multigrid.c:636-729): `iters` red-black iterations on x in place
+void mzb_smooth_rbgs(const double* rhs, double* x, int n, int iters) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    EngineArgs a = scratch_engine(s, w, n);
+    double* db = w.get(m);
+    double* dx = w.get(m);
+    h2d(db, rhs, m);
+    h2d(dx, x, m);
+    a.prog = PROG_SMOOTH;
+    a.sm = iters;
+    a.b = db;
+    a.x = dx;
+    run_engine(s, a);
+    d2h_sync(x, dx, m);
+}
+
+// restriction_27pt (multigrid.c:523-594): fine n^3 -> coarse (n/2)^3
+void mzb_restrict27(const double* fine, double* coarse, int n) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    EngineArgs a = scratch_engine(s, w, n);
+    double* du = w.get(m);
+    double* dout = w.get(m / 8);
+    h2d(du, fine, m);
+    a.prog = PROG_RESTRICT;
+    a.u = du;
+    a.out = dout;
+    run_engine(s, a);
+    d2h_sync(coarse, dout, m / 8);
+}
+
+// prolong_trilinear (multigrid.c:393-463): coarse nc^3 -> fine (2nc)^3
+void mzb_prolong_trilinear(const double* coarse, double* fine, int nc) {
+    System& s = sys();
+    Work w;
+    const long mc = (long)nc * nc * nc;
+    EngineArgs a = scratch_engine(s, w, nc);
+    double* du = w.get(mc);
+    double* dout = w.get(mc * 8);
+    h2d(du, coarse, mc);
+    a.prog = PROG_PROLONG;
+    a.u = du;
+    a.out = dout;
+    run_engine(s, a);
+    d2h_sync(fine, dout, mc * 8);
+}
+
+// cg_coarse (multigrid.c:13-96); x holds the initial guess and receives the result
+int mzb_cg_coarse(const double* b, double* x, int n, int maxit, double rtol) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    EngineArgs a = scratch_engine(s, w, n);
+    double* db = w.get(m);
+    double* dx = w.get(m);
+    h2d(db, b, m);
+    h2d(dx, x, m);
+    a.prog = PROG_CG_COARSE;
+    a.maxit = maxit;
+    a.rtol = rtol;
+    a.b = db;
+    a.x0 = dx;
+    a.x = dx;
+    const int res = run_engine(s, a);
+    d2h_sync(x, dx, m);
+    return res;
+}
+
+// one V-cycle (multigrid.c:99-168) with `sm` RBGS iterations per half; x in place
+void mzb_mg_apply(const double* rhs, double* x, int n, int sm) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    require_mg_size(n);
+    EngineArgs a = scratch_engine(s, w, n);
+    double* db = w.get(m);
+    double* dx = w.get(m);
+    h2d(db, rhs, m);
+    h2d(dx, x, m);
+    a.prog = PROG_MG_APPLY;
+    a.sm = sm;
+    a.b = db;
+    a.x = dx;
+    run_engine(s, a);
+    d2h_sync(x, dx, m);
+}
+
+// rfft_solve with the reference's ig2 (grid_fft.c:65-125, fftw_wrap.c:166-189)
+void mzb_fft_poisson(const double* q, double* phi, int n, double L, double h) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    double* dq = w.get(m);
+    double* dphi = w.get(m);
+    h2d(dq, q, m);
+    FftPoisson f;
+    f.init(n, L, h);
+    f.solve(dq, dphi, s.stream);
+    sync();
+    f.release();
+    d2h_sync(phi, dphi, m);
+}
+
+// CIC corner indices of the current system, (n_p, 8, 3) int64 in the reference's layout
+// (particles.c:297-346); valid after solver_update_charges.
+void mzb_get_cic_neighbors(int64_t* out) {
+    System& s = sys();
+    ParticleDev& P = parts();
+    if (P.np == 0) return;
+    int64_t* d = nullptr;
+    MZB_CHECK(cudaMalloc(&d, sizeof(int64_t) * 24 * P.np));
+    count_launch();
+    k_cic_neighbors<<<(P.np + 127) / 128, 128, 0, s.stream>>>(P.base, P.np, grid().n, d);
+    MZB_CHECK(cudaMemcpyAsync(out, d, sizeof(int64_t) * 24 * P.np, cudaMemcpyDeviceToHost, s.stream));
+    sync();
+    cudaFree(d);
+}
+
+// Linked cells per side used by the pair-force kernel (default ~16 ions per cell).
+void mzb_set_cell_grid(int nc) {
+    ParticleDev& P = parts();
+    sync();
+    set_cells(P, nc);
+}
+
+// Build the linked cells for the current positions and copy them out: start has
+// nc^3 + 1 entries, ions n_p. Returns nc.
+int mzb_get_cells(int32_t* start, int32_t* ions) {
+    System& s = sys();
+    ParticleDev& P = parts();
+    build_cells(P, s.stream);
+    MZB_CHECK(cudaMemcpyAsync(start, P.cell_start, sizeof(int32_t) * (P.ncell + 1), cudaMemcpyDeviceToHost,
+                              s.stream));
+    if (P.np > 0)
+        MZB_CHECK(cudaMemcpyAsync(ions, P.cell_ions, sizeof(int32_t) * P.np, cudaMemcpyDeviceToHost, s.stream));
+    sync();
+    return P.nc;
+}
+
+// O-block noise: the N(0,1) draws the O-block applies on its `call`-th application
+// (integrator_ovrvo.c:45-78 draws them from glibc rand()), 3*n_p values.
+void mzb_philox_normals(uint64_t call, double* out) {
+    System& s = sys();
+    ParticleDev& P = parts();
+    if (P.np == 0) return;
+    double* d = nullptr;
+    MZB_CHECK(cudaMalloc(&d, sizeof(double) * 3 * P.np));
+    philox_normals(s.I.seed, call, P.np, d, s.stream);
+    MZB_CHECK(cudaMemcpyAsync(out, d, sizeof(double) * 3 * P.np, cudaMemcpyDeviceToHost, s.stream));
+    sync();
+    cudaFree(d);
+}
+
+void mzb_set_seed(uint64_t seed) { sys().I.seed = seed; }
+
+// The CUDA stream all work of the current system is queued on (for callers that time
+// it with their own events or order their own kernels against it).
+void* mzb_get_stream(void) { return (void*)sys().stream; }
+
+// Device time (CUDA events on the library stream) and return value of the last
+// field-solver launch (one solver_update_field / solver_init_field).
+double mzb_last_solve_ms(void) { return (double)sys().last_solve_ms; }
+int mzb_last_solve_result(void) { return sys().last_solve_iters; }
+
+// Kernels launched by this library since it was loaded.
+uint64_t mzb_kernel_launches(void) { return g_kernel_launches; }
+uint64_t mzb_get_ocalls(void) { return sys().I.ocalls; }
+
+// n_steps iterations of SolverMD.md_loop_iter (maze_poisson/solver.py:483-492) with both
+// electrostatic and non-electrostatic forces; returns the last solver_update_field value.
+int solver_md_step(int n_steps) {
+    int res = 0;
+    for (int i = 0; i < n_steps; i++) {
+        integrator_part_1();
+        solver_update_charges();
+        res = solver_update_field();
+        solver_compute_forces_elec();
+        solver_compute_forces_noel();
+        solver_compute_forces_tot();
+        integrator_part_2();
+    }
+    sync();
+    return res;
+}
+
+}  // extern "C"

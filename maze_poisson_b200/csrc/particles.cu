@@ -1,0 +1,561 @@
+// Particle-side kernels (see particles.cuh). FP64, compiled with --fmad=false.
+#include "particles.cuh"
+
+namespace mzb {
+
+__device__ __forceinline__ int wrapi(int a, int n) {
+    a %= n;
+    return a < 0 ? a + n : a;
+}
+
+// CIC weight with the minimum image over L = n*h (library/src/charges.c:8-14).
+__device__ __forceinline__ double w_cic(double x, double L, double h) {
+    x = fabs(x - round(x / L) * L);
+    if (x >= h) return 0.0;
+    return 1.0 - x / h;
+}
+
+// CIC corner c (0..7) in the reference's order (particles.c:323-344):
+// (0,0,0) (1,0,0) (0,1,0) (0,0,1) (1,1,0) (1,0,1) (0,1,1) (1,1,1)
+__device__ __forceinline__ void corner_offsets(int c, int& di, int& dj, int& dk) {
+    di = (c == 1 || c == 4 || c == 5 || c == 7);
+    dj = (c == 2 || c == 4 || c == 6 || c == 7);
+    dk = (c == 3 || c == 5 || c == 6 || c == 7);
+}
+
+// ------------------------------------------------------------------------------------
+// Exclusive scan of count[0..m) into start[0..m] (start[m] = total); start is also copied
+// into fill[0..m) as a scatter cursor. One block of 1024 threads. Optionally sums
+// `part[0..np_part)` in index order into *sum_out.
+// ------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_scan(const int32_t* __restrict__ count, int m,
+                                               int32_t* __restrict__ start, int32_t* __restrict__ fill,
+                                               const double* __restrict__ part, int np_part,
+                                               double* __restrict__ sum_out) {
+    __shared__ int32_t wsum[32];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int chunk = (m + blockDim.x - 1) / blockDim.x;
+    const int b = t * chunk, e = min(m, b + chunk);
+    int32_t local = 0;
+    for (int x = b; x < e; x++) local += count[x];
+    // inclusive warp scan
+    int32_t incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int32_t v = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t u = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += u;
+        }
+        wsum[lane] = v;
+    }
+    __syncthreads();
+    int32_t run = incl - local + (w > 0 ? wsum[w - 1] : 0);
+    for (int x = b; x < e; x++) {
+        start[x] = run;
+        fill[x] = run;
+        run += count[x];
+    }
+    if (t == blockDim.x - 1) start[m] = wsum[(blockDim.x >> 5) - 1];
+    if (sum_out != nullptr && t == 0) {
+        double s = 0.0;
+        for (int x = 0; x < np_part; x++) s += part[x];
+        *sum_out = s;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Charge spreading
+// ------------------------------------------------------------------------------------
+
+// Per ion: base cell floor(pos/h) (wrapped), tile histogram and the ion's total spread
+// charge (block partial, summed later in block order).
+__global__ void k_spread_bin(ParticleDev P, int n, double h, double* __restrict__ part) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double u = 0.0;
+    if (p < P.np) {
+        int b[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            b[d] = wrapi((int)floor(P.pos[3 * p + d] / h), n);
+            P.base[3 * p + d] = b[d];
+        }
+        const int tile = ((b[0] / kTileI) * P.ntj + b[1] / kTileJ) * P.ntk + b[2] / kTileK;
+        atomicAdd(&P.tile_count[tile], 1);
+        const double L = n * h, q = P.chg[p];
+        for (int c = 0; c < 8; c++) {
+            int di, dj, dk;
+            corner_offsets(c, di, dj, dk);
+            const int a = di ? wrap_inc(b[0], n) : b[0];
+            const int bb = dj ? wrap_inc(b[1], n) : b[1];
+            const int e = dk ? wrap_inc(b[2], n) : b[2];
+            double w = w_cic(P.pos[3 * p] - a * h, L, h) * w_cic(P.pos[3 * p + 1] - bb * h, L, h);
+            w = w * w_cic(P.pos[3 * p + 2] - e * h, L, h);
+            u += q * w;
+        }
+    }
+    __shared__ double sh[4 * 32];
+    double v[1] = {u};
+    block_sum<1>(v, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+__global__ void k_spread_fill(ParticleDev P) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.np) return;
+    const int* b = P.base + 3 * p;
+    const int tile = ((b[0] / kTileI) * P.ntj + b[1] / kTileJ) * P.ntk + b[2] / kTileK;
+    const int slot = atomicAdd(&P.tile_fill[tile], 1);
+    P.tile_ions[slot] = p;
+}
+
+// One CTA per tile (grid-stride): gather the ions whose base cell lies in this tile or
+// in the 7 tiles below it (their +1 corners can reach this tile), sort them by ion index,
+// accumulate chg*w into a shared-memory tile in ascending ion order -- exactly the order
+// of the reference's serial scatter (charges.c:123-141) -- and flush the whole tile,
+// zeros included, with coalesced stores. q is written once; no atomics touch it.
+__global__ void __launch_bounds__(128) k_spread_tiles(ParticleDev P, double* __restrict__ q, int n,
+                                                      double h) {
+    __shared__ double acc[kTileI * kTileJ * kTileK];
+    __shared__ int cand[kTileCap];
+    __shared__ int sorted[kTileCap];
+    __shared__ int ncand;
+    __shared__ int srcs[8];
+    const double L = n * h;
+    const long n2 = (long)n * n;
+    for (int tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
+        const int ti = tile / (P.ntj * P.ntk), tj = (tile / P.ntk) % P.ntj, tk = tile % P.ntk;
+        for (int e = threadIdx.x; e < kTileI * kTileJ * kTileK; e += blockDim.x) acc[e] = 0.0;
+        if (threadIdx.x < 8) {
+            const int c = threadIdx.x;
+            const int si = wrapi(ti - ((c >> 2) & 1), P.nti), sj = wrapi(tj - ((c >> 1) & 1), P.ntj),
+                      sk = wrapi(tk - (c & 1), P.ntk);
+            srcs[c] = (si * P.ntj + sj) * P.ntk + sk;
+        }
+        if (threadIdx.x == 0) ncand = 0;
+        __syncthreads();
+        if (threadIdx.x < 8) {
+            const int c = threadIdx.x, s = srcs[c];
+            bool dup = false;
+            for (int d = 0; d < c; d++) dup |= (srcs[d] == s);
+            if (!dup) {
+                for (int x = P.tile_start[s]; x < P.tile_start[s + 1]; x++) {
+                    const int slot = atomicAdd(&ncand, 1);
+                    if (slot < kTileCap) cand[slot] = P.tile_ions[x];
+                }
+            }
+        }
+        __syncthreads();
+        const int nc = ncand;
+        if (nc > kTileCap) {
+            if (threadIdx.x == 0) atomicOr(&P.flags[0], 1);
+        } else {
+            for (int x = threadIdx.x; x < nc; x += blockDim.x) {
+                const int me = cand[x];
+                int rank = 0;
+                for (int y = 0; y < nc; y++) rank += (cand[y] < me);
+                sorted[rank] = me;
+            }
+            __syncthreads();
+            if (threadIdx.x < 8) {
+                const int c = threadIdx.x;
+                int di, dj, dk;
+                corner_offsets(c, di, dj, dk);
+                for (int x = 0; x < nc; x++) {
+                    const int p = sorted[x];
+                    const int* b = P.base + 3 * p;
+                    const int a = di ? wrap_inc(b[0], n) : b[0];
+                    const int bb = dj ? wrap_inc(b[1], n) : b[1];
+                    const int e = dk ? wrap_inc(b[2], n) : b[2];
+                    const int li = a - ti * kTileI, lj = bb - tj * kTileJ, lk = e - tk * kTileK;
+                    if (li >= 0 && li < kTileI && lj >= 0 && lj < kTileJ && lk >= 0 && lk < kTileK) {
+                        double w = w_cic(P.pos[3 * p] - a * h, L, h) * w_cic(P.pos[3 * p + 1] - bb * h, L, h);
+                        w = w * w_cic(P.pos[3 * p + 2] - e * h, L, h);
+                        acc[(li * kTileJ + lj) * kTileK + lk] += P.chg[p] * w;
+                    }
+                    __syncwarp(0xffu);
+                }
+            }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < kTileI * kTileJ * kTileK; e += blockDim.x) {
+            const int li = e / (kTileJ * kTileK), lj = (e / kTileK) % kTileJ, lk = e % kTileK;
+            const int i = ti * kTileI + li, j = tj * kTileJ + lj, k = tk * kTileK + lk;
+            if (i < n && j < n && k < n) q[(long)i * n2 + (long)j * n + k] = acc[e];
+        }
+        __syncthreads();
+    }
+}
+
+void spread_charges(ParticleDev& P, double* q, int n, double h, cudaStream_t s) {
+    const int nb = (P.np + 127) / 128;
+    MZB_CHECK(cudaMemsetAsync(P.tile_count, 0, sizeof(int32_t) * P.ntiles, s));
+    count_launch();
+    k_spread_bin<<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial);
+    count_launch();
+    k_scan<<<1, 1024, 0, s>>>(P.tile_count, P.ntiles, P.tile_start, P.tile_fill, P.partial,
+                              nb > 0 ? nb : 1, P.red + 0);
+    if (nb > 0) count_launch();
+    if (nb > 0) k_spread_fill<<<nb, 128, 0, s>>>(P);
+    int dev, sms;
+    MZB_CHECK(cudaGetDevice(&dev));
+    MZB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int grid = P.ntiles < sms * 16 ? P.ntiles : sms * 16;
+    count_launch();
+    k_spread_tiles<<<grid, 128, 0, s>>>(P, q, n, h);
+    MZB_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// Field forces: central differences of phi at the 8 CIC corners (forces.c:26-100).
+// ------------------------------------------------------------------------------------
+__global__ void k_field_forces(ParticleDev P, const double* __restrict__ phi, int n, double h) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.np) return;
+    const double L = n * h, h2 = 2.0 * h;
+    const long n2 = (long)n * n;
+    const int* b = P.base + 3 * p;
+    const double px = P.pos[3 * p], py = P.pos[3 * p + 1], pz = P.pos[3 * p + 2], chg = P.chg[p];
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int c = 0; c < 8; c++) {
+        int di, dj, dk;
+        corner_offsets(c, di, dj, dk);
+        const int i = di ? wrap_inc(b[0], n) : b[0];
+        const int j = dj ? wrap_inc(b[1], n) : b[1];
+        const int k = dk ? wrap_inc(b[2], n) : b[2];
+        double qc = chg * w_cic(px - i * h, L, h);
+        qc = qc * w_cic(py - j * h, L, h);
+        qc = qc * w_cic(pz - k * h, L, h);
+        const long i0 = i * n2, j0 = (long)j * n;
+        const long ip = (long)wrap_inc(i, n) * n2, im = (long)wrap_dec(i, n) * n2;
+        const long jp = (long)wrap_inc(j, n) * n, jm = (long)wrap_dec(j, n) * n;
+        const int kp = wrap_inc(k, n), km = wrap_dec(k, n);
+        fx += qc * ((phi[im + j0 + k] - phi[ip + j0 + k]) / h2);
+        fy += qc * ((phi[i0 + jm + k] - phi[i0 + jp + k]) / h2);
+        fz += qc * ((phi[i0 + j0 + km] - phi[i0 + j0 + kp]) / h2);
+    }
+    P.fe[3 * p] = fx;
+    P.fe[3 * p + 1] = fy;
+    P.fe[3 * p + 2] = fz;
+}
+
+void field_forces(ParticleDev& P, const double* phi, int n, double h, cudaStream_t s) {
+    if (P.np == 0) return;
+    count_launch();
+    k_field_forces<<<(P.np + 127) / 128, 128, 0, s>>>(P, phi, n, h);
+    MZB_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// Linked cells by counting sort, stable in ion index: cell (IX,IY,IZ) with
+// IX = int((nc/L) * x) (maze_poisson/linkedcell.py:18-26), clamped into the box.
+// ------------------------------------------------------------------------------------
+__global__ void k_cell_count(ParticleDev P) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.np) return;
+    const double rel = P.nc / P.L;
+    int c[3];
+    bool inside = true;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const double x = P.pos[3 * p + d];
+        inside &= (x >= 0.0 && x < P.L);
+        int v = (int)(rel * x);
+        if (!(rel * x >= 0.0)) v = 0;
+        c[d] = v < 0 ? 0 : (v >= P.nc ? P.nc - 1 : v);
+    }
+    if (!inside) atomicOr(&P.flags[1], 1);
+    const int cell = (c[0] * P.nc + c[1]) * P.nc + c[2];
+    P.cell_of[p] = cell;
+    atomicAdd(&P.cell_count[cell], 1);
+}
+
+__global__ void k_cell_fill(ParticleDev P) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.np) return;
+    const int slot = atomicAdd(&P.cell_fill[P.cell_of[p]], 1);
+    P.cell_ions[slot] = p;
+}
+
+// One thread per cell: restore ascending ion order inside the cell (the scatter above is
+// unordered), then gather positions/types into cell order and record each ion's rank.
+__global__ void k_cell_sort_gather(ParticleDev P) {
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+    if (cell >= P.ncell) return;
+    const int b = P.cell_start[cell], e = P.cell_start[cell + 1];
+    for (int x = b + 1; x < e; x++) {
+        const int v = P.cell_ions[x];
+        int y = x - 1;
+        while (y >= b && P.cell_ions[y] > v) {
+            P.cell_ions[y + 1] = P.cell_ions[y];
+            y--;
+        }
+        P.cell_ions[y + 1] = v;
+    }
+    for (int x = b; x < e; x++) {
+        const int p = P.cell_ions[x];
+        P.spos[3 * x] = P.pos[3 * p];
+        P.spos[3 * x + 1] = P.pos[3 * p + 1];
+        P.spos[3 * x + 2] = P.pos[3 * p + 2];
+        P.stype[x] = P.types[p];
+        P.srank[p] = x;
+    }
+}
+
+void build_cells(ParticleDev& P, cudaStream_t s) {
+    MZB_CHECK(cudaMemsetAsync(P.cell_count, 0, sizeof(int32_t) * P.ncell, s));
+    MZB_CHECK(cudaMemsetAsync(P.flags + 1, 0, sizeof(int), s));
+    if (P.np > 0) count_launch();
+    if (P.np > 0) k_cell_count<<<(P.np + 127) / 128, 128, 0, s>>>(P);
+    count_launch();
+    k_scan<<<1, 1024, 0, s>>>(P.cell_count, P.ncell, P.cell_start, P.cell_fill, nullptr, 0, nullptr);
+    if (P.np > 0) count_launch();
+    if (P.np > 0) k_cell_fill<<<(P.np + 127) / 128, 128, 0, s>>>(P);
+    count_launch();
+    k_cell_sort_gather<<<(P.ncell + 127) / 128, 128, 0, s>>>(P);
+    MZB_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// fcs_tot = (0 + 1*fcs_elec) + 1*fcs_noel (particles.c:777-795)
+// ------------------------------------------------------------------------------------
+__global__ void k_total_forces(ParticleDev P) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * P.np) return;
+    double v = 0.0;
+    v += 1.0 * P.fe[t];
+    v += 1.0 * P.fn[t];
+    P.ft[t] = v;
+}
+
+void total_forces(ParticleDev& P, cudaStream_t s) {
+    if (P.np == 0) return;
+    count_launch();
+    k_total_forces<<<(3 * P.np + 255) / 256, 256, 0, s>>>(P);
+    MZB_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// Kinetic energy, momentum, temperature (particles.c:798-839). Block partials are summed
+// in block order by one thread: deterministic for a given N.
+// ------------------------------------------------------------------------------------
+__global__ void k_ke_partial(ParticleDev P) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    if (p < P.np) {
+        const double m = P.mass[p], vx = P.vel[3 * p], vy = P.vel[3 * p + 1], vz = P.vel[3 * p + 2];
+        double a = 0.0;
+        a += vx * vx;
+        a += vy * vy;
+        a += vz * vz;
+        v[0] = m * a;
+        v[1] = m * vx;
+        v[2] = m * vy;
+        v[3] = m * vz;
+    }
+    __shared__ double sh[4 * 32];
+    block_sum<4>(v, sh);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 4; q++) P.partial[4 * blockIdx.x + q] = v[q];
+}
+
+// red[2] = KE, red[3..5] = momentum, red[6] = T, red[7] = sqrt(T_target / T)
+__global__ void k_ke_final(ParticleDev P, int nblocks, double T_target) {
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = 0; b < nblocks; b++)
+        for (int q = 0; q < 4; q++) s[q] += P.partial[4 * b + q];
+    const double ke = 0.5 * s[0];
+    P.red[2] = ke;
+    P.red[3] = s[1];
+    P.red[4] = s[2];
+    P.red[5] = s[3];
+    const double T = 2 * ke / (3 * P.np * kBoltzmannHartree);
+    P.red[6] = T;
+    P.red[7] = sqrt(T_target / T);
+}
+
+static void ke_reduce(ParticleDev& P, double T_target, cudaStream_t s) {
+    const int nb = P.np > 0 ? (P.np + 255) / 256 : 1;
+    count_launch();
+    k_ke_partial<<<nb, 256, 0, s>>>(P);
+    count_launch();
+    k_ke_final<<<1, 1, 0, s>>>(P, nb, T_target);
+    MZB_CHECK(cudaGetLastError());
+}
+
+void kinetic_and_momentum(ParticleDev& P, cudaStream_t s) { ke_reduce(P, 1.0, s); }
+
+// ------------------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) and Box-Muller normals.
+// Counter = (ion, draw, call_lo, call_hi), key = (seed_lo, seed_hi); each draw gives two
+// normals from two 53-bit uniforms in (0,1).
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        const uint32_t lo0 = 0xD2511F53u * c[0], hi0 = __umulhi(0xD2511F53u, c[0]);
+        const uint32_t lo1 = 0xCD9E8D57u * c[2], hi1 = __umulhi(0xCD9E8D57u, c[2]);
+        const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = lo1;
+        c[2] = n2;
+        c[3] = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+__device__ __forceinline__ double u53(uint32_t hi, uint32_t lo) {
+    const uint64_t a = ((uint64_t)hi << 32) | lo;
+    return ((double)(a >> 11) + 0.5) * 0x1.0p-53;
+}
+
+__device__ void philox_normal3(uint64_t seed, uint64_t call, uint32_t ion, double z[3]) {
+    for (uint32_t draw = 0; draw < 2; draw++) {
+        uint32_t c[4] = {ion, draw, (uint32_t)call, (uint32_t)(call >> 32)};
+        philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+        const double u1 = u53(c[0], c[1]), u2 = u53(c[2], c[3]);
+        const double rad = sqrt(-2.0 * log(u1));
+        double sn, cs;
+        sincospi(2.0 * u2, &sn, &cs);
+        z[2 * draw] = rad * cs;
+        if (draw == 0) z[1] = rad * sn;
+    }
+}
+
+__global__ void k_philox(uint64_t seed, uint64_t call, int np, double* out) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    double z[3];
+    philox_normal3(seed, call, (uint32_t)p, z);
+    out[3 * p] = z[0];
+    out[3 * p + 1] = z[1];
+    out[3 * p + 2] = z[2];
+}
+
+void philox_normals(uint64_t seed, uint64_t call, int np, double* out, cudaStream_t s) {
+    if (np == 0) return;
+    count_launch();
+    k_philox<<<(np + 127) / 128, 128, 0, s>>>(seed, call, np, out);
+    MZB_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// Integrators (integrator_verlet.c, integrator_ovrvo.c)
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ double wrap_box(double a, double L) {
+    if (a < 0) return a + L;
+    if (a >= L) return a - L;
+    return a;
+}
+
+// Velocity Verlet part 1: optional rescale to the target T, half kick, drift, wrap.
+__global__ void k_verlet1(ParticleDev P, double dt, int rescale) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * P.np) return;
+    const int p = t / 3;
+    double v = P.vel[t];
+    if (rescale) v *= P.red[7];
+    v += 0.5 * dt * P.ft[t] / P.mass[p];
+    P.vel[t] = v;
+    P.pos[t] = wrap_box(P.pos[t] + dt * v, P.L);
+}
+__global__ void k_verlet2(ParticleDev P, double dt) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * P.np) return;
+    P.vel[t] += 0.5 * dt * P.ft[t] / P.mass[t / 3];
+}
+
+// OVRVO: part1 = [O] V R, part2 = V [O]; O uses Philox normals for call `call`.
+__global__ void k_ovrvo(ParticleDev P, IntegratorDev I, int part, uint64_t call) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.np) return;
+    const double m = P.mass[p];
+    double v[3] = {P.vel[3 * p], P.vel[3 * p + 1], P.vel[3 * p + 2]};
+    auto o_block = [&]() {
+        const double c1s = sqrt(I.c1), var2 = (1 - I.c1) * kBoltzmannHartree * I.T;
+        const double var1 = sqrt(var2 / m);
+        double z[3];
+        philox_normal3(I.seed, call, (uint32_t)p, z);
+        for (int d = 0; d < 3; d++) {
+            v[d] *= c1s;
+            v[d] += var1 * z[d];
+        }
+    };
+    auto v_block = [&]() {
+        for (int d = 0; d < 3; d++) v[d] += 0.5 * I.dt * I.c2 * P.ft[3 * p + d] / m;
+    };
+    if (part == 1) {
+        if (I.enabled) o_block();
+        v_block();
+        for (int d = 0; d < 3; d++) P.pos[3 * p + d] = wrap_box(P.pos[3 * p + d] + I.c2 * I.dt * v[d], P.L);
+    } else {
+        v_block();
+        if (I.enabled) o_block();
+    }
+    for (int d = 0; d < 3; d++) P.vel[3 * p + d] = v[d];
+}
+
+void integrator_part1(ParticleDev& P, IntegratorDev& I, cudaStream_t s) {
+    if (P.np == 0) return;
+    if (I.type == 1) {
+        if (I.enabled) ke_reduce(P, I.T, s);
+        count_launch();
+        k_verlet1<<<(3 * P.np + 255) / 256, 256, 0, s>>>(P, I.dt, I.enabled);
+    } else {
+        count_launch();
+        k_ovrvo<<<(P.np + 127) / 128, 128, 0, s>>>(P, I, 1, I.ocalls);
+        if (I.enabled) I.ocalls++;
+    }
+    MZB_CHECK(cudaGetLastError());
+}
+
+void integrator_part2(ParticleDev& P, IntegratorDev& I, cudaStream_t s) {
+    if (P.np == 0) return;
+    if (I.type == 1) {
+        count_launch();
+        k_verlet2<<<(3 * P.np + 255) / 256, 256, 0, s>>>(P, I.dt);
+    } else {
+        count_launch();
+        k_ovrvo<<<(P.np + 127) / 128, 128, 0, s>>>(P, I, 2, I.ocalls);
+        if (I.enabled) I.ocalls++;
+    }
+    MZB_CHECK(cudaGetLastError());
+}
+
+// rescale_velocities (particles.c:841-857): per-type velocity sums accumulated serially
+// in ion order (one thread per type and component), then v -= 2*sum/N.
+__global__ void k_rescale_sum(ParticleDev P, double* iv) {
+    const int t = threadIdx.x;
+    if (t >= 3 * P.ntyp) return;
+    const int typ = t / 3, d = t % 3;
+    double s = 0.0;
+    for (int p = 0; p < P.np; p++)
+        if (P.types[p] == typ) s += P.vel[3 * p + d];
+    iv[t] = s;
+}
+__global__ void k_rescale_apply(ParticleDev P, const double* iv) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * P.np) return;
+    const int p = t / 3, d = t % 3;
+    P.vel[t] -= 2 * iv[P.types[p] * 3 + d] / P.np;
+}
+
+void rescale_velocities(ParticleDev& P, cudaStream_t s) {
+    if (P.np == 0) return;
+    if (3 * P.ntyp > 1024) fatal("rescale_velocities: too many particle types");
+    count_launch();
+    k_rescale_sum<<<1, 3 * P.ntyp, 0, s>>>(P, P.partial);
+    count_launch();
+    k_rescale_apply<<<(3 * P.np + 255) / 256, 256, 0, s>>>(P, P.partial);
+    MZB_CHECK(cudaGetLastError());
+}
+
+}  // namespace mzb

@@ -1,0 +1,84 @@
+// Particle-side kernels of the MD step: CIC charge spreading, linked cells, field-force
+// interpolation, Tosi-Fumi pair forces, integrators and reductions.
+#pragma once
+
+#include "mzb_common.cuh"
+
+namespace mzb {
+
+// Spreading tile: TI x TJ x TK grid points accumulated in shared memory by one CTA.
+constexpr int kTileI = 4, kTileJ = 4, kTileK = 32;
+constexpr int kTileCap = 2048;  // candidate ions one tile CTA can hold (see spread_tiles)
+
+struct ParticleDev {
+    int np = 0, ntyp = 0, n = 0;
+    double L = 0, h = 0, rcut = 0;
+    int32_t* types = nullptr;
+    double* pos = nullptr;
+    double* vel = nullptr;
+    double* fe = nullptr;
+    double* fn = nullptr;
+    double* ft = nullptr;
+    double* mass = nullptr;
+    double* chg = nullptr;
+    double* tab = nullptr;   // [ntyp*ntyp][7] Tosi-Fumi table
+    int32_t* base = nullptr; // [np][3] CIC base cell (wrapped)
+
+    // spreading bins
+    int ntiles = 0, nti = 0, ntj = 0, ntk = 0;
+    int32_t* tile_count = nullptr;   // [ntiles]
+    int32_t* tile_start = nullptr;   // [ntiles+1]
+    int32_t* tile_fill = nullptr;    // [ntiles]
+    int32_t* tile_ions = nullptr;    // [np]
+
+    // linked cells (Tosi-Fumi)
+    int nc = 0, ncell = 0;
+    int32_t* cell_of = nullptr;      // [np]
+    int32_t* cell_count = nullptr;   // [ncell]
+    int32_t* cell_start = nullptr;   // [ncell+1]
+    int32_t* cell_fill = nullptr;    // [ncell]
+    int32_t* cell_ions = nullptr;    // [np]
+    int32_t* srank = nullptr;        // [np] position of ion p in cell order
+    double* spos = nullptr;          // [np][3] positions in cell order
+    int32_t* stype = nullptr;        // [np]
+    int tf_split = 1;                // cell-pair chunks per cell
+    double* fpart = nullptr;         // [tf_split][np][3]
+    double* epart = nullptr;         // [ncell * tf_split]
+
+    // scalars
+    double* red = nullptr;           // reduction outputs (device)
+    int* flags = nullptr;            // [0] spread overflow, [1] bad cell index
+    double* partial = nullptr;       // block partials
+};
+
+// Build the CIC base cells, the tile bins and q (bit-identical to the reference's serial
+// update_charges). Writes the spread total charge to red[0].
+void spread_charges(ParticleDev& P, double* q, int n, double h, cudaStream_t s);
+// Forces from -grad(phi) at the 8 CIC corners (forces.c:26-100) into P.fe.
+void field_forces(ParticleDev& P, const double* phi, int n, double h, cudaStream_t s);
+// Linked cells (counting sort, stable by ion index) + Tosi-Fumi forces into P.fn;
+// pair energy / 2 into red[1].
+void build_cells(ParticleDev& P, cudaStream_t s);
+void tf_forces(ParticleDev& P, cudaStream_t s);
+// fcs_tot = fcs_elec + fcs_noel (particles.c:777-795)
+void total_forces(ParticleDev& P, cudaStream_t s);
+// Kinetic energy into red[2] and momentum into red[3..5] (particles.c:798-839).
+void kinetic_and_momentum(ParticleDev& P, cudaStream_t s);
+
+struct IntegratorDev {
+    int type = 1;      // 0 OVRVO, 1 VERLET
+    int enabled = 0;
+    double dt = 0, T = 0, c1 = 1, c2 = 1;
+    uint64_t seed = 0x5eedULL;
+    uint64_t ocalls = 0;  // O-blocks applied so far (Philox counter)
+};
+
+void integrator_part1(ParticleDev& P, IntegratorDev& I, cudaStream_t s);
+void integrator_part2(ParticleDev& P, IntegratorDev& I, cudaStream_t s);
+void rescale_velocities(ParticleDev& P, cudaStream_t s);
+
+// Philox4x32-10 standard normals of the O-block (O-block call `call`, ion `ion`,
+// components 0..2) written to out[3*ion + d] for ion < np.
+void philox_normals(uint64_t seed, uint64_t call, int np, double* out, cudaStream_t s);
+
+}  // namespace mzb

@@ -1,0 +1,109 @@
+"""MD driver over the C ABI, mirroring the reference's SolverMD call sequence.
+
+`MDRun` makes the same ctypes calls, in the same order, as maze_poisson/solver.py:
+initialize (96-108), the two bootstrap Verlet steps of initialize_md (371-409) and
+md_loop_iter (483-492) -- so it drives this build's libmaze_poisson.so exactly the way
+the reference's solver.py would, without the reference's file I/O.
+"""
+import numpy as np
+
+from .systems import T_AU_FS
+
+
+def gamma_au(gamma_per_ps):
+    """Langevin friction in a.u.^-1 from ps^-1 (the reference takes `gamma` in a.u.)."""
+    return gamma_per_ps * 1e-3 * T_AU_FS
+
+
+class MDRun:
+    def __init__(self, capi, system, method="LCG", precond="NONE", tol=1e-7, integrator="VERLET",
+                 thermostat=False, T=1200.0, gamma_per_ps=1.0, dt_fs=1.0, eps_s=1.0, eps_int=1.0,
+                 rescale=False):
+        self.capi = capi
+        self.sys = system
+        self.method = method.upper()
+        self.precond = precond.upper()
+        self.tol = tol
+        self.integrator = integrator.upper()
+        self.thermostat = thermostat
+        self.T = T
+        self.gamma = gamma_au(gamma_per_ps)
+        self.dt = dt_fs / T_AU_FS
+        self.eps_s = eps_s
+        self.eps_int = eps_int
+        self.rescale = rescale
+        self.n_iters = None
+        self.potential_notelec = None
+
+    # -- solver.py:96-108 + initialize_md 371-409 -------------------------------------
+    def initialize(self):
+        c = self.capi
+        s = self.sys
+        c.solver_initialize()
+        maps = c.type_maps()
+        c.solver_initialize_grid(s.n_grid, s.L, s.h, self.tol, self.eps_s, self.eps_int,
+                                 maps["method"][self.method], maps["precond"][self.precond])
+        c.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, maps["potential"]["TF"],
+                                      maps["cas"]["CIC"], s.types, s.pos, s.vel, s.mass, s.charges,
+                                      s.pot_params)
+        c.solver_initialize_integrator(s.n_ions, self.dt, self.T, self.gamma,
+                                       maps["integrator"][self.integrator], 1 if self.thermostat else 0)
+        # step 0
+        self.update_charges()
+        c.solver_init_field()
+        self.compute_forces()
+        # step 1
+        c.integrator_part_1()
+        self.update_charges()
+        c.solver_init_field()
+        self.compute_forces()
+        c.integrator_part_2()
+        if self.rescale:
+            c.solver_rescale_velocities()
+
+    def update_charges(self):
+        if self.capi.solver_update_charges() != 0:
+            raise RuntimeError("charge is not preserved")
+
+    def compute_forces(self):
+        c = self.capi
+        c.solver_compute_forces_elec()
+        self.potential_notelec = c.solver_compute_forces_noel()
+        c.solver_compute_forces_tot()
+
+    # -- solver.py:483-492 --------------------------------------------------------------
+    def step(self):
+        c = self.capi
+        c.integrator_part_1()
+        self.update_charges()
+        self.n_iters = c.solver_update_field()
+        self.compute_forces()
+        c.integrator_part_2()
+        return self.n_iters
+
+    def run(self, n_steps):
+        for _ in range(n_steps):
+            self.step()
+
+    # -- getters (solver_md.c:247-354) ---------------------------------------------------
+    def state(self, fields=True):
+        c = self.capi
+        n = self.sys.n_ions
+        out = {}
+        for name in ("pos", "vel", "fcs_elec", "fcs_noel", "fcs_tot"):
+            a = np.empty((n, 3), dtype=np.float64)
+            getattr(c, "get_" + name)(a)
+            out[name] = a
+        if fields:
+            g = self.sys.n_grid
+            for name in ("field", "field_prev", "q"):
+                a = np.empty((g, g, g), dtype=np.float64)
+                getattr(c, "get_" + name)(a)
+                out[name] = a
+        out["kinetic"] = c.get_kinetic_energy()
+        out["potential_notelec"] = self.potential_notelec
+        out["n_iters"] = self.n_iters
+        return out
+
+    def finalize(self):
+        self.capi.solver_finalize()

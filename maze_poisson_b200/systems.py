@@ -1,0 +1,141 @@
+"""Seeded synthetic molten-salt (Na+/Cl-) systems.
+
+The reference measures on no public dataset; its runs start from lattice or restart
+files (examples/). These systems follow that recipe:
+
+* ncell^3 cubic cells of side a = L/ncell, each with a Na+ at the corner and a Cl- at
+  the body centre (the 2-ion cell of maze_poisson/cli/utilities/bcc_generate.py:17-32),
+  so N = 2 ncell^3 (250 / 2000 / 16000 for ncell = 5 / 10 / 20);
+* uniform jitter U(-0.1 a, 0.1 a) per coordinate from numpy.random.default_rng(seed),
+  wrapped into [0, L);
+* L from the mass density: L[A] = ((N/2) * 58.443 / N_A / rho)^(1/3) * 1e8;
+* Maxwell-Boltzmann velocities at T (a.u.), centre-of-mass drift removed;
+* Tosi-Fumi NaCl parameters (kJ/mol, A) converted to atomic units exactly as
+  maze_poisson/solver.py:198-202 does.
+
+Units are atomic (bohr, Hartree, electron mass, a.u. of time), constants from
+maze_poisson/constants.py.
+"""
+import dataclasses
+import os
+
+import numpy as np
+
+A0 = 0.529177210903            # A per bohr
+T_AU_FS = 2.4188843265857e-2   # fs per a.u. of time
+AMU_TO_KG = 1.66054e-27
+M_E = 9.1093837e-31
+CONV_MASS = AMU_TO_KG / M_E
+KB = 3.1668e-6                 # Hartree / K
+KJMOL_TO_HARTREE = 0.0003808798
+N_AVOGADRO = 6.02214076e23
+NACL_MOLAR_MASS = 58.443       # g/mol
+
+SPECIES = (("Na", 1.0, 22.99), ("Cl", -1.0, 35.453))  # type, charge, mass [amu]
+# Tosi-Fumi NaCl: (type1, type2, A [kJ/mol], B [1/A], C [kJ/mol A^6], D [kJ/mol A^8], sigma [A])
+TOSI_FUMI = (
+    ("Na", "Na", 25.4435, 3.1546, 101.1719, 48.1771, 2.340),
+    ("Na", "Cl", 20.3548, 3.1546, 674.4793, 837.0770, 2.755),
+    ("Cl", "Cl", 15.2661, 3.1546, 6985.6786, 14031.5785, 3.170),
+)
+
+
+def box_length_ang(n_ions, density):
+    """Cubic box side [A] holding n_ions/2 NaCl formula units at `density` g/cm^3."""
+    return ((n_ions / 2) * NACL_MOLAR_MASS / N_AVOGADRO / density) ** (1.0 / 3.0) * 1e8
+
+
+def tf_params_au():
+    """[2][2][A,B,C,D,sigma] in a.u., flattened (the pot_params of solver_initialize_particles)."""
+    names = [s[0] for s in SPECIES]
+    arr = np.full((2, 2, 5), np.nan)
+    for t1, t2, A, B, C, D, s in TOSI_FUMI:
+        v = np.array([A, B, C, D, s], dtype=np.float64)
+        i, j = names.index(t1), names.index(t2)
+        arr[i, j] = v
+        arr[j, i] = v
+    arr[:, :, 0] *= KJMOL_TO_HARTREE
+    arr[:, :, 1] *= A0
+    arr[:, :, 2] *= KJMOL_TO_HARTREE / A0 ** 6
+    arr[:, :, 3] *= KJMOL_TO_HARTREE / A0 ** 8
+    arr[:, :, 4] /= A0
+    return np.ascontiguousarray(arr.reshape(-1), dtype=np.float64)
+
+
+@dataclasses.dataclass
+class MoltenSalt:
+    ncell: int
+    n_grid: int
+    density: float
+    T: float
+    seed: int
+    L: float                 # bohr
+    h: float                 # bohr
+    types: np.ndarray        # int32 [N]
+    pos: np.ndarray          # float64 [N, 3] bohr
+    vel: np.ndarray          # float64 [N, 3] a.u.
+    mass: np.ndarray         # float64 [N] a.u.
+    charges: np.ndarray      # float64 [N]
+    pot_params: np.ndarray   # float64 [2*2*5]
+
+    @property
+    def n_ions(self):
+        return len(self.types)
+
+    def copy(self):
+        return dataclasses.replace(self, types=self.types.copy(), pos=self.pos.copy(),
+                                   vel=self.vel.copy(), mass=self.mass.copy(),
+                                   charges=self.charges.copy(), pot_params=self.pot_params.copy())
+
+
+def make_system(ncell, n_grid, density=1.379, T=1200.0, seed=0, jitter=0.1):
+    """Build the jittered 2-ion-cell NaCl lattice with MB velocities (see module doc)."""
+    rng = np.random.default_rng(seed)
+    n = 2 * ncell ** 3
+    L = box_length_ang(n, density) / A0
+    a = L / ncell
+    cells = np.stack(np.meshgrid(np.arange(ncell), np.arange(ncell), np.arange(ncell),
+                                 indexing="ij"), axis=-1).reshape(-1, 3).astype(np.float64)
+    pos = np.empty((n, 3))
+    pos[0::2] = cells * a
+    pos[1::2] = (cells + 0.5) * a
+    pos += rng.uniform(-jitter * a, jitter * a, size=pos.shape)
+    pos = np.mod(pos, L)
+    pos = np.where(pos >= L, pos - L, pos)
+    types = np.tile(np.array([0, 1], dtype=np.int32), ncell ** 3)
+    charges = np.array([SPECIES[t][1] for t in types], dtype=np.float64)
+    mass = np.array([SPECIES[t][2] for t in types], dtype=np.float64) * CONV_MASS
+    vel = rng.normal(0.0, 1.0, size=(n, 3)) * np.sqrt(KB * T / mass)[:, None]
+    vel -= (mass[:, None] * vel).sum(axis=0) / mass.sum()
+    return MoltenSalt(ncell=ncell, n_grid=n_grid, density=density, T=T, seed=seed, L=L,
+                      h=L / n_grid, types=np.ascontiguousarray(types),
+                      pos=np.ascontiguousarray(pos), vel=np.ascontiguousarray(vel),
+                      mass=np.ascontiguousarray(mass), charges=np.ascontiguousarray(charges),
+                      pot_params=tf_params_au())
+
+
+# Workloads of the reference's configurations (sizes only; solver settings in md.py)
+WORKLOADS = {
+    "nacl250_64": dict(ncell=5, n_grid=64, density=1.379),
+    "nacl2000_128": dict(ncell=10, n_grid=128, density=1.329),
+    "nacl16000_256": dict(ncell=20, n_grid=256, density=1.379),
+}
+
+
+def write_reference_inputs(system, directory, name="input.csv"):
+    """Write species.csv, tosi_fumi.csv and a positions/velocities CSV (A, a.u.) that the
+    reference's SolverMD reads (maze_poisson/solver.py:165-205, 276-330)."""
+    os.makedirs(directory, exist_ok=True)
+    with open(os.path.join(directory, "species.csv"), "w") as f:
+        f.write("type,charge,mass,radius\n")
+        for t, q, m in SPECIES:
+            f.write(f"{t},{q},{m},1.0\n")
+    with open(os.path.join(directory, "tosi_fumi.csv"), "w") as f:
+        f.write("type1,type2,A,B,C,D,sigma\n")
+        for row in TOSI_FUMI:
+            f.write(",".join(str(x) for x in row) + "\n")
+    names = [s[0] for s in SPECIES]
+    with open(os.path.join(directory, name), "w") as f:
+        f.write("type,x,y,z,vx,vy,vz\n")
+        for t, p, v in zip(system.types, system.pos * A0, system.vel):
+            f.write(f"{names[t]},{p[0]!r},{p[1]!r},{p[2]!r},{v[0]!r},{v[1]!r},{v[2]!r}\n")

@@ -1,0 +1,743 @@
+/*
+ * CPU oracle for the MaZe_Poisson per-step MD hot path -- TEST INFRASTRUCTURE ONLY.
+ * See oracle.h for the contract.  Citations are to the reference project
+ * (Crivella/MaZe_Poisson) by path within that project.
+ *
+ * Conventions kept from the reference so results match bit for bit:
+ *  - grids are n^3, idx = (i*n + j)*n + k, periodic in all three axes (the reference's
+ *    x-halo slabs filled by mpi_grid_exchange_bot_top, library/src/mpi_base.c:186-197,
+ *    are the same as wrapping i);
+ *  - every sum is accumulated in the reference's order, products are rounded before they
+ *    are added (built with -ffp-contract=off, see Makefile);
+ *  - reductions are serial, i.e. the reference run with OMP_NUM_THREADS=1.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "oracle.h"
+
+#define PI_D 3.14159265358979323846
+#define KB_HARTREE 3.1668e-6 /* library/include/constants.h:10 */
+
+static inline long wrap(long a, long n) { a %= n; return a < 0 ? a + n : a; }
+static inline long gidx(long i, long j, long k, long n) {
+    return (wrap(i, n) * n + wrap(j, n)) * n + wrap(k, n);
+}
+
+/* ------------------------------------------------------------------------------------
+ * BLAS-1 helpers (library/src/linalg.c:105-212, serial no-BLAS build)
+ * ---------------------------------------------------------------------------------- */
+static double dot(const double *a, const double *b, long m) {
+    double s = 0.0;
+    for (long t = 0; t < m; t++) s += a[t] * b[t];
+    return s;
+}
+static double amax(const double *a, long m) {
+    double s = 0.0;
+    for (long t = 0; t < m; t++) { double v = fabs(a[t]); if (v > s) s = v; }
+    return s;
+}
+/* u += alpha * v  (linalg.c:153-159) */
+static void axpy(double *u, const double *v, double alpha, long m) {
+    for (long t = 0; t < m; t++) u[t] += alpha * v[t];
+}
+static void scal(double *x, double alpha, long m) {
+    for (long t = 0; t < m; t++) x[t] *= alpha;
+}
+
+/* ------------------------------------------------------------------------------------
+ * 7-point Laplacian, no 1/h^2 (library/src/laplace.c:24-75).
+ * Sum order: x+1, x-1, y+1, y-1, z+1, z-1, then minus 6*centre.
+ * ---------------------------------------------------------------------------------- */
+void orc_laplace(const double *u, double *out, int n) {
+    for (long i = 0; i < n; i++)
+        for (long j = 0; j < n; j++)
+            for (long k = 0; k < n; k++) {
+                double s = u[gidx(i + 1, j, k, n)] + u[gidx(i - 1, j, k, n)];
+                s = s + u[gidx(i, j + 1, k, n)];
+                s = s + u[gidx(i, j - 1, k, n)];
+                s = s + u[gidx(i, j, k + 1, n)];
+                s = s + u[gidx(i, j, k - 1, n)];
+                out[(i * n + j) * n + k] = s - u[(i * n + j) * n + k] * 6.0;
+            }
+}
+
+/* ------------------------------------------------------------------------------------
+ * CG with implicit Jacobi preconditioner (library/src/plcg.c:28-90).
+ * Stops when ||r||_inf <= tol (absolute) after the x/r update; at most n^2 iterations;
+ * returns the 0-based iteration index at convergence or -1.  x may alias b.
+ * ---------------------------------------------------------------------------------- */
+int orc_conj_grad(const double *b, const double *x0, double *x, double tol, int n) {
+    long m = (long)n * n * n, limit = (long)n * n, iter = 0;
+    int res = -1;
+    double *r = malloc(m * sizeof(double)), *p = malloc(m * sizeof(double));
+    double *Ap = malloc(m * sizeof(double));
+    orc_laplace(x0, r, n);
+    axpy(r, b, -1.0, m);                       /* r = A x0 - b */
+    if (x != x0) memcpy(x, x0, m * sizeof(double));
+    for (long t = 0; t < m; t++) p[t] = r[t] * (1.0 / 6.0);
+    double rv = -dot(r, p, m);
+    while (iter < limit) {
+        orc_laplace(p, Ap, n);
+        double alpha = rv / dot(p, Ap, m);
+        axpy(x, p, alpha, m);
+        axpy(r, Ap, alpha, m);
+        double rr = dot(r, r, m);
+        if (amax(r, m) <= tol) { res = (int)iter; break; }
+        double rnv = -rr / 6.0, beta = rnv / rv;
+        rv = rnv;
+        scal(p, beta, m);
+        axpy(p, r, 1.0 / 6.0, m);
+        iter++;
+    }
+    free(r); free(p); free(Ap);
+    return res;
+}
+
+/* ------------------------------------------------------------------------------------
+ * Multigrid pieces (library/src/multigrid.c)
+ * ---------------------------------------------------------------------------------- */
+
+/* Red-black Gauss-Seidel, red = (i+j+k) even first (multigrid.c:636-729). */
+void orc_smooth_rbgs(const double *rhs, double *x, int n, int iters) {
+    const double inv_diag = -1.0 / 6.0;
+    for (int it = 0; it < iters; it++)
+        for (int colour = 0; colour < 2; colour++)
+            for (long i = 0; i < n; i++)
+                for (long j = 0; j < n; j++)
+                    for (long k = (i + j + colour) & 1; k < n; k += 2) {
+                        double s = x[gidx(i - 1, j, k, n)] + x[gidx(i + 1, j, k, n)];
+                        s = s + x[gidx(i, j - 1, k, n)];
+                        s = s + x[gidx(i, j + 1, k, n)];
+                        s = s + x[gidx(i, j, k - 1, n)];
+                        s = s + x[gidx(i, j, k + 1, n)];
+                        long c = (i * n + j) * n + k;
+                        x[c] = (rhs[c] - s) * inv_diag;
+                    }
+}
+
+/* 27-point full weighting onto (n/2)^3, coarse (I,J,K) <- fine (2I,2J,2K)
+   (multigrid.c:523-594); centre 8, faces 4, edges 2, corners 1, /64. */
+void orc_restrict27(const double *in, double *out, int n) {
+    int nc = n / 2;
+#define F(a, b, c) in[gidx(i + (a), j + (b), k + (c), n)]
+    for (long I = 0; I < nc; I++)
+        for (long J = 0; J < nc; J++)
+            for (long K = 0; K < nc; K++) {
+                long i = 2 * I, j = 2 * J, k = 2 * K;
+                double f = F(-1, 0, 0) + F(1, 0, 0);
+                f = f + F(0, -1, 0); f = f + F(0, 1, 0);
+                f = f + F(0, 0, -1); f = f + F(0, 0, 1);
+                double e = F(1, 0, -1) + F(1, 0, 1);
+                e = e + F(-1, 0, -1); e = e + F(-1, 0, 1);
+                e = e + F(1, -1, 0);  e = e + F(1, 1, 0);
+                e = e + F(-1, -1, 0); e = e + F(-1, 1, 0);
+                e = e + F(0, -1, -1); e = e + F(0, -1, 1);
+                e = e + F(0, 1, -1);  e = e + F(0, 1, 1);
+                double c = F(1, 1, -1) + F(1, 1, 1);
+                c = c + F(1, -1, -1);  c = c + F(1, -1, 1);
+                c = c + F(-1, 1, -1);  c = c + F(-1, 1, 1);
+                c = c + F(-1, -1, -1); c = c + F(-1, -1, 1);
+                double v = 8.0 * F(0, 0, 0) + 4.0 * f;
+                v = v + 2.0 * e;
+                v = v + c;
+                out[(I * nc + J) * nc + K] = v * (1.0 / 64.0);
+            }
+#undef F
+}
+
+/* Trilinear prolongation from nc^3 onto (2nc)^3 (multigrid.c:393-463). Weights are
+   (1,0) on even fine indices and (0.5,0.5) on odd ones; 8 terms summed in the
+   reference's order. */
+void orc_prolong_trilinear(const double *in, double *out, int nc) {
+    long nf = 2L * nc;
+    for (long i = 0; i < nf; i++) {
+        double wi0 = (i & 1) ? 0.5 : 1.0, wi1 = (i & 1) ? 0.5 : 0.0;
+        long i0 = i / 2, i1 = i0 + 1;
+        for (long j = 0; j < nf; j++) {
+            double wj0 = (j & 1) ? 0.5 : 1.0, wj1 = (j & 1) ? 0.5 : 0.0;
+            long j0 = (j / 2) % nc, j1 = j0 + 1;
+            for (long k = 0; k < nf; k++) {
+                double wk0 = (k & 1) ? 0.5 : 1.0, wk1 = (k & 1) ? 0.5 : 0.0;
+                long k0 = (k / 2) % nc, k1 = k0 + 1;
+#define C(a, b, c) in[gidx(a, b, c, nc)]
+                double s = C(i0, j0, k0) * wi0 * wj0 * wk0 + C(i1, j0, k0) * wi1 * wj0 * wk0;
+                s = s + C(i0, j1, k0) * wi0 * wj1 * wk0;
+                s = s + C(i1, j1, k0) * wi1 * wj1 * wk0;
+                s = s + C(i0, j0, k1) * wi0 * wj0 * wk1;
+                s = s + C(i1, j0, k1) * wi1 * wj0 * wk1;
+                s = s + C(i0, j1, k1) * wi0 * wj1 * wk1;
+                s = s + C(i1, j1, k1) * wi1 * wj1 * wk1;
+#undef C
+                out[(i * nf + j) * nf + k] = s;
+            }
+        }
+    }
+}
+
+/* Coarse-level CG with a relative inf-norm stop (multigrid.c:13-96). */
+int orc_cg_coarse(const double *b, double *x, int n, int maxit, double rtol) {
+    long m = (long)n * n * n;
+    double *r = malloc(m * sizeof(double)), *p = malloc(m * sizeof(double));
+    double *Ap = malloc(m * sizeof(double));
+    int k;
+    orc_laplace(x, r, n);
+    axpy(r, b, -1.0, m);
+    for (long t = 0; t < m; t++) p[t] = r[t] * (1.0 / 6.0);
+    double r0 = amax(r, m);
+    if (r0 == 0.0) { free(r); free(p); free(Ap); return 0; }
+    double rv = -dot(r, p, m);
+    for (k = 0; k < maxit; ++k) {
+        orc_laplace(p, Ap, n);
+        double den = dot(p, Ap, m);
+        if (fabs(den) < 1e-300) break;
+        double alpha = rv / den;
+        axpy(x, p, alpha, m);
+        axpy(r, Ap, alpha, m);
+        if (amax(r, m) <= rtol * r0) { ++k; break; }
+        double rr = dot(r, r, m);
+        double rnv = -rr / 6.0, beta = rnv / rv;
+        rv = rnv;
+        scal(p, beta, m);
+        axpy(p, r, 1.0 / 6.0, m);
+    }
+    free(r); free(p); free(Ap);
+    return k;
+}
+
+/* One V-cycle as the reference runs it: the recursion bottoms out at depth 1, so this is
+   a two-level cycle -- sm RBGS sweeps, residual, 27-pt restriction, coarse CG (50 it,
+   rtol 1e-5) from zero, trilinear prolongation, correction, sm RBGS sweeps
+   (multigrid.c:99-168, 743-765; multigrid.h:4-7). Requires n/2 >= 16. */
+void orc_mg_apply(const double *rhs, double *x, int n, int sm) {
+    long m = (long)n * n * n;
+    int nc = n / 2;
+    long mc = (long)nc * nc * nc;
+    if (nc < 16) { fprintf(stderr, "oracle multigrid: requires n/2 >= 16\n"); exit(1); }
+    double *r = malloc(m * sizeof(double));
+    double *rc = malloc(mc * sizeof(double)), *ec = calloc(mc, sizeof(double));
+    orc_smooth_rbgs(rhs, x, n, sm);
+    orc_laplace(x, r, n);
+    scal(r, -1.0, m);
+    axpy(r, rhs, 1.0, m);
+    orc_restrict27(r, rc, n);
+    orc_cg_coarse(rc, ec, nc, 50, 1e-5);
+    orc_prolong_trilinear(ec, r, nc);
+    axpy(x, r, 1.0, m);
+    orc_smooth_rbgs(rhs, x, n, sm);
+    free(r); free(rc); free(ec);
+}
+
+/* ------------------------------------------------------------------------------------
+ * Preconditioned CG (library/src/plcg.c:104-166) with the two explicit preconditioners
+ * in scope: Jacobi, out = -in/6 (precond_jacobi.c:8-14), and one V-cycle with 5 sweeps
+ * warm-started from the previous output (precond_mg.c:3-5).  The preconditioner output
+ * buffer starts at zero.
+ * ---------------------------------------------------------------------------------- */
+static void apply_precond(int kind, const double *in, double *out, int n) {
+    long m = (long)n * n * n;
+    if (kind == 1) { for (long t = 0; t < m; t++) out[t] = -in[t] / 6.0; }
+    else orc_mg_apply(in, out, n, 5);
+}
+
+static int conj_grad_precond(const double *b, const double *x0, double *x, double tol, int n,
+                             int kind) {
+    long m = (long)n * n * n, limit = (long)n * n, iter = 0;
+    int res = -1;
+    double *r = malloc(m * sizeof(double)), *Ap = malloc(m * sizeof(double));
+    double *v = calloc(m, sizeof(double)), *p = malloc(m * sizeof(double));
+    orc_laplace(x0, r, n);
+    axpy(r, b, -1.0, m);
+    if (x != x0) memcpy(x, x0, m * sizeof(double));
+    apply_precond(kind, r, v, n);
+    for (long t = 0; t < m; t++) p[t] = v[t] * -1.0;
+    double rv = dot(r, v, m);
+    while (iter < limit) {
+        orc_laplace(p, Ap, n);
+        double alpha = rv / dot(p, Ap, m);
+        axpy(x, p, alpha, m);
+        axpy(r, Ap, alpha, m);
+        if (amax(r, m) <= tol) { res = (int)iter; break; }
+        apply_precond(kind, r, v, n);
+        double rnv = dot(r, v, m), beta = rnv / rv;
+        rv = rnv;
+        scal(p, beta, m);
+        axpy(p, v, -1.0, m);
+        iter++;
+    }
+    free(r); free(Ap); free(v); free(p);
+    return res;
+}
+
+/* ------------------------------------------------------------------------------------
+ * Particle kernels
+ * ---------------------------------------------------------------------------------- */
+
+/* CIC weight (charges.c:8-14) with the minimum image over L = n*h. */
+static inline double w_cic(double x, double L, double h) {
+    x = fabs(x - round(x / L) * L);
+    if (x >= h) return 0.0;
+    return 1.0 - x / h;
+}
+
+/* Base cell floor(pos/h) and its 8 wrapped corners in the reference's order
+   (particles.c:297-346). A base index outside [0,n) (a position at or beyond the box
+   edge, where the reference indexes out of bounds) is wrapped. */
+void orc_cic_neighbors(const double *pos, int np, int n, double h, int64_t *nbr) {
+    static const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1},
+                                  {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+    for (long p = 0; p < np; p++) {
+        long b[3];
+        for (int d = 0; d < 3; d++) b[d] = wrap((long)(int)floor(pos[3 * p + d] / h), n);
+        for (int c = 0; c < 8; c++)
+            for (int d = 0; d < 3; d++)
+                nbr[(p * 8 + c) * 3 + d] = off[c][d] ? (b[d] + 1) % n : b[d];
+    }
+}
+
+/* Zero q, then scatter chg*w over the 8 corners in ion order (charges.c:100-144).
+   Returns the total spread charge. */
+double orc_spread_cic(const double *pos, const double *chg, const int64_t *nbr, int np, int n,
+                      double h, double *q) {
+    double L = n * h, tot = 0.0;
+    memset(q, 0, (size_t)n * n * n * sizeof(double));
+    for (long p = 0; p < np; p++) {
+        const int64_t *nb = nbr + p * 24;
+        for (int c = 0; c < 8; c++) {
+            long a = nb[3 * c], b = nb[3 * c + 1], e = nb[3 * c + 2];
+            double w = w_cic(pos[3 * p] - a * h, L, h) * w_cic(pos[3 * p + 1] - b * h, L, h);
+            w = w * w_cic(pos[3 * p + 2] - e * h, L, h);
+            double u = chg[p] * w;
+            tot += u;
+            q[(a * n + b) * n + e] += u;
+        }
+    }
+    return tot;
+}
+
+/* Field force by central differences of phi at the 8 CIC corners (forces.c:26-100). */
+double orc_force_fd(const double *phi, const int64_t *nbr, const double *chg, const double *pos,
+                    int np, int n, double h, double *f) {
+    double L = n * h, h2 = 2.0 * h, sq = 0.0;
+    for (long p = 0; p < np; p++) {
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        const int64_t *nb = nbr + p * 24;
+        for (int c = 0; c < 8; c++) {
+            long i = nb[3 * c], j = nb[3 * c + 1], k = nb[3 * c + 2];
+            double qc = chg[p] * w_cic(pos[3 * p] - i * h, L, h);
+            qc = qc * w_cic(pos[3 * p + 1] - j * h, L, h);
+            qc = qc * w_cic(pos[3 * p + 2] - k * h, L, h);
+            sq += qc;
+            fx += qc * ((phi[gidx(i - 1, j, k, n)] - phi[gidx(i + 1, j, k, n)]) / h2);
+            fy += qc * ((phi[gidx(i, j - 1, k, n)] - phi[gidx(i, j + 1, k, n)]) / h2);
+            fz += qc * ((phi[gidx(i, j, k - 1, n)] - phi[gidx(i, j, k + 1, n)]) / h2);
+        }
+        f[3 * p] = fx; f[3 * p + 1] = fy; f[3 * p + 2] = fz;
+    }
+    return sq;
+}
+
+/* Per type-pair Tosi-Fumi table [A,B,C,D,sigma,alpha,beta] with the shifted-force
+   constants at r_cut = L/2 (particles.c:181-228). The reference stores the same seven
+   numbers per ion pair (7*N^2 doubles); they depend only on the two types. */
+void orc_tf_table(const double *pp, int ntyp, double L, double *tab) {
+    double rc = L / 2.0, rc6 = pow(rc, 6), rc7 = rc6 * rc, rc8 = rc7 * rc, rc9 = rc8 * rc;
+    for (int t = 0; t < ntyp * ntyp; t++) {
+        double A = pp[5 * t], B = pp[5 * t + 1], C = pp[5 * t + 2], D = pp[5 * t + 3],
+               s = pp[5 * t + 4];
+        double vs = A * exp(B * (s - rc)) - C / rc6 - D / rc8;
+        double al = A * B * exp(B * (s - rc)) - 6 * C / rc7 - 8 * D / rc9;
+        double be = -vs - al * rc;
+        double *o = tab + 7 * t;
+        o[0] = A; o[1] = B; o[2] = C; o[3] = D; o[4] = s; o[5] = al; o[6] = be;
+    }
+}
+
+/* All-pairs shifted-force Tosi-Fumi, minimum image, skip r > r_cut, both orders summed
+   over j ascending (forces.c:112-186). Returns half the summed pair energy. */
+double orc_tf_forces(const double *pos, const int32_t *types, const double *tab, int ntyp, int np,
+                     double L, double rcut, double *f) {
+    double en = 0.0;
+    for (long i = 0; i < np; i++) {
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (long j = 0; j < np; j++) {
+            if (i == j) continue;
+            double d[3], r = 0.0;
+            for (int a = 0; a < 3; a++) {
+                double x = pos[3 * i + a] - pos[3 * j + a];
+                x -= L * round(x / L);
+                d[a] = x;
+                r = (a == 0) ? x * x : r + x * x;
+            }
+            r = sqrt(r);
+            if (r > rcut) continue;
+            const double *t = tab + 7 * (types[i] * ntyp + types[j]);
+            double a = t[0], b = t[1], c = t[2], dd = t[3], s = t[4], al = t[5], be = t[6];
+            double fm = b * a * exp(b * (s - r)) - 6 * c / pow(r, 7) - 8 * dd / pow(r, 9) - al;
+            double vm = a * exp(b * (s - r)) - c / pow(r, 6) - dd / pow(r, 8) + al * r + be;
+            fx += fm * (d[0] / r);
+            fy += fm * (d[1] / r);
+            fz += fm * (d[2] / r);
+            en += vm;
+        }
+        f[3 * i] = fx; f[3 * i + 1] = fy; f[3 * i + 2] = fz;
+    }
+    return en / 2;
+}
+
+/* Linked cells as a CSR list: cell (IX,IY,IZ) with IX = int((nc/L) * x)
+   (maze_poisson/linkedcell.py:18-26), ions of a cell in ascending index (the reverse of
+   the reference's header/link chain). Out-of-range coordinates are clamped. */
+void orc_cell_list(const double *pos, int np, double L, int nc, int32_t *start, int32_t *ions) {
+    long ncell = (long)nc * nc * nc;
+    double rel = nc / L;
+    int32_t *cell = malloc((size_t)(np > 0 ? np : 1) * sizeof(int32_t));
+    memset(start, 0, (ncell + 1) * sizeof(int32_t));
+    for (long p = 0; p < np; p++) {
+        long c[3];
+        for (int d = 0; d < 3; d++) {
+            long v = (long)(rel * pos[3 * p + d]);
+            c[d] = v < 0 ? 0 : (v >= nc ? nc - 1 : v);
+        }
+        cell[p] = (int32_t)((c[0] * nc + c[1]) * nc + c[2]);
+        start[cell[p] + 1]++;
+    }
+    for (long c = 0; c < ncell; c++) start[c + 1] += start[c];
+    int32_t *fill = malloc((size_t)ncell * sizeof(int32_t));
+    memcpy(fill, start, ncell * sizeof(int32_t));
+    for (long p = 0; p < np; p++) ions[fill[cell[p]]++] = (int32_t)p;
+    free(fill); free(cell);
+}
+
+/* ------------------------------------------------------------------------------------
+ * Facade (library/src/solver_md.c) over one global system.
+ * ---------------------------------------------------------------------------------- */
+enum { G_LCG = 0, G_FFT = 1, G_MG = 2, G_MAZE_LCG = 3, G_MAZE_MG = 4 };
+enum { P_NONE = 0, P_JACOBI = 1, P_MG = 2 };
+
+static struct {
+    int type, precond, n;
+    double L, h, tol, eps_s;
+    long m;
+    double *q, *phi, *phi_prev, *y;
+} G;
+static struct {
+    int np, ntyp, n;
+    double L, h, rcut;
+    int32_t *types;
+    double *pos, *vel, *fe, *fn, *ft, *mass, *chg, *tab;
+    int64_t *nbr;
+} P;
+static struct {
+    int type, enabled;
+    double dt, T, c1, c2;
+} I;
+static double q_tot_prev = 0.0; /* persists across systems, solver_md.c:16 */
+static double *noise = NULL;
+static long noise_len = 0, noise_pos = 0;
+
+static void die(const char *msg) { fprintf(stderr, "oracle: %s\n", msg); exit(1); }
+
+void solver_initialize(void) {}
+
+void solver_initialize_grid(int n, double L, double h, double tol, double eps_s, double eps_int,
+                            int grid_type, int precond_type) {
+    (void)eps_int;
+    if (grid_type == G_FFT) die("FFT is restated in numpy (oracle/fft_oracle.py)");
+    if (grid_type < 0 || grid_type > 4) die("bad grid type");
+    if (precond_type > P_MG) die("SSOR / BLOCKJACOBI are outside the oracle");
+    G.type = grid_type; G.precond = precond_type; G.n = n;
+    G.L = L; G.h = h; G.tol = tol; G.eps_s = eps_s;
+    G.m = (long)n * n * n;
+    G.q = calloc(G.m, sizeof(double)); G.phi = calloc(G.m, sizeof(double));
+    G.phi_prev = calloc(G.m, sizeof(double)); G.y = calloc(G.m, sizeof(double));
+}
+
+void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, int pot_type,
+                                 int cas_type, int *types, double *pos, double *vel, double *mass,
+                                 double *charges, double *pot_params) {
+    if (pot_type != 0) die("only the Tosi-Fumi potential is restated");
+    if (cas_type != 0) die("only CIC charge assignment is restated");
+    P.np = n_p; P.ntyp = n_typ; P.n = n; P.L = L; P.h = h; P.rcut = L / 2.0;
+    size_t v3 = (size_t)3 * n_p * sizeof(double);
+    P.types = malloc(n_p * sizeof(int32_t)); memcpy(P.types, types, n_p * sizeof(int32_t));
+    P.pos = malloc(v3); memcpy(P.pos, pos, v3);
+    P.vel = malloc(v3); memcpy(P.vel, vel, v3);
+    P.mass = malloc(n_p * sizeof(double)); memcpy(P.mass, mass, n_p * sizeof(double));
+    P.chg = malloc(n_p * sizeof(double)); memcpy(P.chg, charges, n_p * sizeof(double));
+    P.fe = calloc(3 * n_p, sizeof(double)); P.fn = calloc(3 * n_p, sizeof(double));
+    P.ft = calloc(3 * n_p, sizeof(double));
+    P.nbr = malloc((size_t)n_p * 24 * sizeof(int64_t));
+    P.tab = malloc((size_t)n_typ * n_typ * 7 * sizeof(double));
+    orc_tf_table(pot_params, n_typ, L, P.tab);
+}
+
+void solver_initialize_integrator(int n_p, double dt, double T, double gamma, int itg_type,
+                                  int itg_enabled) {
+    (void)n_p;
+    I.type = itg_type; I.dt = dt; I.enabled = 0; I.c1 = 1.0; I.c2 = 1.0; I.T = 0.0;
+    if (itg_enabled == 1) {                 /* integrator_{ovrvo,verlet}.c init_thermostat */
+        I.T = T; I.enabled = 1;
+        if (itg_type == 0) {
+            I.c1 = exp(-gamma * dt);
+            I.c2 = sqrt(2 / (gamma * dt) * tanh(0.5 * gamma * dt));
+        }
+    }
+}
+
+int solver_update_charges(void) {
+    orc_cic_neighbors(P.pos, P.np, P.n, P.h, P.nbr);
+    double qt = orc_spread_cic(P.pos, P.chg, P.nbr, P.np, G.n, G.h, G.q);
+    if (fabs(q_tot_prev - qt) > 1e-6) {
+        printf("Charge conservation error: q_tot = %.6f, q_tot_loc = %.6f\n", q_tot_prev, qt);
+        exit(1);
+    }
+    q_tot_prev = qt;
+    return 0;
+}
+
+static double rhs_const(void) { double c = -4 * PI_D / G.h; return c / G.eps_s; }
+
+/* grid_lcg.c:100-124, grid_maze_lcg.c:107-126, grid_multigrid.c:86-108,
+   grid_maze_multigrid.c:86-112: all four solve L phi = -4 pi q/(h eps) by CG from 0. */
+void solver_init_field(void) {
+    double c = rhs_const();
+    memset(G.y, 0, G.m * sizeof(double));
+    memcpy(G.phi_prev, G.phi, G.m * sizeof(double));
+    for (long t = 0; t < G.m; t++) G.phi[t] = G.q[t] * c;
+    orc_conj_grad(G.phi, G.y, G.phi, G.tol, G.n);
+}
+
+/* phi <- 2 phi - phi_prev, phi_prev <- old phi (verlet.c:46-51, grid_multigrid.c:124-129) */
+static void extrapolate(void) {
+    for (long t = 0; t < G.m; t++) {
+        double a = G.phi[t];
+        G.phi[t] = 2 * a - G.phi_prev[t];
+        G.phi_prev[t] = a;
+    }
+}
+
+int solver_update_field(void) {
+    long m = G.m;
+    int n = G.n, res = -1;
+    if (G.type == G_LCG) {                                 /* grid_lcg.c:126-149 */
+        double c = rhs_const();
+        memcpy(G.phi_prev, G.phi, m * sizeof(double));
+        for (long t = 0; t < m; t++) G.y[t] = G.q[t] * c;
+        return orc_conj_grad(G.y, G.phi_prev, G.phi, G.tol, n);
+    }
+    if (G.type == G_MAZE_LCG) {                            /* verlet.c:31-71 */
+        double hh = G.h * G.eps_s;
+        double *tmp = malloc(m * sizeof(double));
+        extrapolate();
+        orc_laplace(G.phi, tmp, n);
+        axpy(tmp, G.q, (4 * PI_D) / hh, m);
+        if (G.precond == P_NONE) res = orc_conj_grad(tmp, G.y, G.y, G.tol, n);
+        else res = conj_grad_precond(tmp, G.y, G.y, G.tol, n, G.precond);
+        axpy(G.phi, G.y, -1.0, m);
+        free(tmp);
+        return res;
+    }
+    double *tmp = malloc(m * sizeof(double)), *tmp2 = malloc(m * sizeof(double));
+    int it = 0;
+    if (G.type == G_MG) {                                  /* grid_multigrid.c:110-212 */
+        extrapolate();
+        double c = rhs_const();
+        for (long t = 0; t < m; t++) tmp[t] = G.q[t] * c;
+        while (it < 1000) {
+            orc_mg_apply(tmp, G.phi, n, 3);
+            orc_laplace(G.phi, tmp2, n);
+            axpy(tmp2, tmp, -1.0, m);
+            double a = amax(tmp2, m);
+            it++;
+            if (a <= G.tol) { res = it; break; }
+        }
+    } else {                                               /* verlet.c:86-149 */
+        double hh = G.h * G.eps_s;
+        extrapolate();
+        orc_laplace(G.phi, tmp2, n);
+        axpy(tmp2, G.q, (4 * PI_D) / hh, m);
+        while (it < 1000) {
+            orc_mg_apply(tmp2, G.y, n, 3);
+            orc_laplace(G.y, tmp, n);
+            axpy(tmp, tmp2, -1., m);
+            double a = amax(tmp, m);
+            it++;
+            if (a <= G.tol) { res = it; break; }
+        }
+        axpy(G.phi, G.y, -1.0, m);
+        if (G.precond != P_NONE) die("Maze Multigrid with preconditioner not implemented");
+    }
+    free(tmp); free(tmp2);
+    return res;
+}
+
+void solver_set_field(double *phi) { memcpy(G.phi, phi, G.m * sizeof(double)); }
+void solver_set_field_prev(double *phi) { memcpy(G.phi_prev, phi, G.m * sizeof(double)); }
+
+void solver_compute_forces_elec(void) {
+    orc_force_fd(G.phi, P.nbr, P.chg, P.pos, P.np, P.n, P.h, P.fe);
+}
+double solver_compute_forces_noel(void) {
+    return orc_tf_forces(P.pos, P.types, P.tab, P.ntyp, P.np, P.L, P.rcut, P.fn);
+}
+void solver_compute_forces_tot(void) {                     /* particles.c:777-795 */
+    for (long t = 0; t < 3L * P.np; t++) { double v = 0.0; v += 1.0 * P.fe[t]; v += 1.0 * P.fn[t]; P.ft[t] = v; }
+}
+
+double get_kinetic_energy(void) {                          /* particles.c:802-820 */
+    double kin = 0.0;
+    for (long p = 0; p < P.np; p++) {
+        double a = 0.0;
+        for (int d = 0; d < 3; d++) a += pow(P.vel[3 * p + d], 2);
+        kin += P.mass[p] * a;
+    }
+    return 0.5 * kin;
+}
+double get_temperature(void) { return 2 * get_kinetic_energy() / (3 * P.np * KB_HARTREE); }
+
+static double next_noise(void) {
+    if (noise_pos >= noise_len) die("injected noise exhausted");
+    return noise[noise_pos++];
+}
+void orc_set_noise(const double *z, int64_t count) {
+    free(noise);
+    noise = malloc((size_t)(count > 0 ? count : 1) * sizeof(double));
+    memcpy(noise, z, (size_t)count * sizeof(double));
+    noise_len = count; noise_pos = 0;
+}
+
+static inline double wrap_box(double a, double L) {
+    if (a < 0) return a + L;
+    if (a >= L) return a - L;
+    return a;
+}
+
+/* integrator_ovrvo.c:45-78 with injected N(0,1) draws */
+static void o_block(void) {
+    double c1s = sqrt(I.c1), var2 = (1 - I.c1) * KB_HARTREE * I.T;
+    for (long p = 0; p < P.np; p++) {
+        double var1 = sqrt(var2 / P.mass[p]);
+        for (int d = 0; d < 3; d++) {
+            P.vel[3 * p + d] *= c1s;
+            P.vel[3 * p + d] += var1 * next_noise();
+        }
+    }
+}
+static void v_block(void) {                                /* integrator_ovrvo.c:80-96 */
+    for (long p = 0; p < P.np; p++)
+        for (int d = 0; d < 3; d++)
+            P.vel[3 * p + d] += 0.5 * I.dt * I.c2 * P.ft[3 * p + d] / P.mass[p];
+}
+static void r_block(void) {                                /* integrator_ovrvo.c:98-123 */
+    for (long p = 0; p < P.np; p++)
+        for (int d = 0; d < 3; d++)
+            P.pos[3 * p + d] = wrap_box(P.pos[3 * p + d] + I.c2 * I.dt * P.vel[3 * p + d], P.L);
+}
+
+void integrator_part_1(void) {
+    if (I.type == 0) {                                     /* integrator_ovrvo.c:125-131 */
+        if (I.enabled) o_block();
+        v_block();
+        r_block();
+        return;
+    }
+    if (I.enabled) {                                       /* integrator_verlet.c:12-53 */
+        double s = sqrt(I.T / get_temperature());
+        for (long t = 0; t < 3L * P.np; t++) P.vel[t] *= s;
+    }
+    for (long p = 0; p < P.np; p++)
+        for (int d = 0; d < 3; d++) {
+            long t = 3 * p + d;
+            P.vel[t] += 0.5 * I.dt * P.ft[t] / P.mass[p];
+            P.pos[t] = wrap_box(P.pos[t] + I.dt * P.vel[t], P.L);
+        }
+}
+
+void integrator_part_2(void) {
+    if (I.type == 0) {
+        v_block();
+        if (I.enabled) o_block();
+        return;
+    }
+    for (long p = 0; p < P.np; p++)
+        for (int d = 0; d < 3; d++)
+            P.vel[3 * p + d] += 0.5 * I.dt * P.ft[3 * p + d] / P.mass[p];
+}
+
+int solver_check_thermostat(void) {                        /* solver_md.c:210-221 */
+    if (I.enabled == 1 && fabs(get_temperature() - I.T) < 100) {
+        I.enabled = 0;
+        if (I.type == 0) { I.c1 = 1.0; I.c2 = 1.0; }
+        return 1;
+    }
+    return 0;
+}
+
+void solver_rescale_velocities(void) {                     /* particles.c:841-857 */
+    double *iv = calloc((size_t)P.ntyp * 3, sizeof(double));
+    for (long p = 0; p < P.np; p++)
+        for (int d = 0; d < 3; d++) iv[P.types[p] * 3 + d] += P.vel[3 * p + d];
+    for (long p = 0; p < P.np; p++)
+        for (int d = 0; d < 3; d++) P.vel[3 * p + d] -= 2 * iv[P.types[p] * 3 + d] / P.np;
+    free(iv);
+}
+
+void solver_finalize(void) {
+    free(G.q); free(G.phi); free(G.phi_prev); free(G.y);
+    free(P.types); free(P.pos); free(P.vel); free(P.mass); free(P.chg);
+    free(P.fe); free(P.fn); free(P.ft); free(P.nbr); free(P.tab);
+    memset(&G, 0, sizeof(G)); memset(&P, 0, sizeof(P));
+}
+
+void get_pos(double *o) { memcpy(o, P.pos, 3 * (size_t)P.np * sizeof(double)); }
+void get_vel(double *o) { memcpy(o, P.vel, 3 * (size_t)P.np * sizeof(double)); }
+void get_fcs_elec(double *o) { memcpy(o, P.fe, 3 * (size_t)P.np * sizeof(double)); }
+void get_fcs_noel(double *o) { memcpy(o, P.fn, 3 * (size_t)P.np * sizeof(double)); }
+void get_fcs_tot(double *o) { memcpy(o, P.ft, 3 * (size_t)P.np * sizeof(double)); }
+void get_field(double *o) { memcpy(o, G.phi, G.m * sizeof(double)); }
+void get_field_prev(double *o) { memcpy(o, G.phi_prev, G.m * sizeof(double)); }
+void get_q(double *o) { memcpy(o, G.q, G.m * sizeof(double)); }
+void get_momentum(double *o) {                             /* particles.c:822-839 */
+    double s[3] = {0.0, 0.0, 0.0};
+    for (long p = 0; p < P.np; p++)
+        for (int d = 0; d < 3; d++) s[d] += P.mass[p] * P.vel[3 * p + d];
+    o[0] = s[0]; o[1] = s[1]; o[2] = s[2];
+}
+
+/* ---- remaining facade symbols (enum tables, serial MPI stubs, trivial getters) ---- */
+static char grid_names[5][16] = {"LCG", "FFT", "MULTIGRID", "MAZE-LCG", "MAZE-MULTIGRID"};
+static char precond_names[5][16] = {"NONE", "JACOBI", "MG", "SSOR", "BLOCKJACOBI"};
+static char pot_names[3][16] = {"TF", "LJ", "SC"};
+static char cas_names[3][16] = {"CIC", "SPL_QUADR", "SPL_CUBIC"};
+static char itg_names[2][16] = {"OVRVO", "VERLET"};
+int init_mpi(void) { return 0; }
+int get_rank(void) { return 0; }
+int get_grid_type_num(void) { return 5; }
+char *get_grid_type_str(int i) { return grid_names[i]; }
+int get_precond_type_num(void) { return 5; }
+char *get_precond_type_str(int i) { return precond_names[i]; }
+int get_potential_type_num(void) { return 3; }
+char *get_potential_type_str(int i) { return pot_names[i]; }
+int get_ca_scheme_type_num(void) { return 3; }
+char *get_ca_scheme_type_str(int i) { return cas_names[i]; }
+int get_integrator_type_num(void) { return 2; }
+char *get_integrator_type_str(int i) { return itg_names[i]; }
+void solver_initialize_grid_pois_boltz(double w, double k, int e) { (void)w; (void)k; (void)e; die("PB is outside the oracle"); }
+void solver_initialize_particles_pois_boltz(double a, double b, double *r) { (void)a; (void)b; (void)r; die("PB is outside the oracle"); }
+void solver_update_eps_k2(void) { die("PB is outside the oracle"); }
+double solver_compute_forces_pb(void) { die("PB is outside the oracle"); return 0.0; }
+void get_fcs_db(double *o) { memset(o, 0, 3 * (size_t)P.np * sizeof(double)); }
+void get_fcs_ib(double *o) { memset(o, 0, 3 * (size_t)P.np * sizeof(double)); }
+void get_fcs_np(double *o) { memset(o, 0, 3 * (size_t)P.np * sizeof(double)); }
+void get_charges(double *o) { memcpy(o, P.chg, (size_t)P.np * sizeof(double)); }
+void get_masses(double *o) { memcpy(o, P.mass, (size_t)P.np * sizeof(double)); }
+void get_types(int *o) { memcpy(o, P.types, (size_t)P.np * sizeof(int32_t)); }
+void get_radii(double *o) { memset(o, 0, (size_t)P.np * sizeof(double)); }
+double get_energy_elec(void) {                             /* grid_general.c:304-315 */
+    double e = 0.0;
+    for (long t = 0; t < G.m; t++) e += 0.5 * G.phi[t];
+    return e;
+}

@@ -1,0 +1,260 @@
+"""MD-level parity of the CUDA path against the CPU oracle, through the reference's C ABI.
+
+Both libraries are driven by the same MDRun call sequence (the reference's SolverMD).
+Tolerances (FP64 mode):
+  * bit-exact: CIC corner indices, the charge grid q, linked cells, the field force of a
+    given phi, every per-ion integrator update;
+  * 1e-10 relative (max-norm ratio): fields, forces, energies, positions and velocities
+    after each step -- the only differences come from the dot-product order inside the
+    iterative solves and from exp/pow in the pair forces.
+"""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, ROOT
+from maze_poisson_b200.c_api import CAPI
+from maze_poisson_b200.md import MDRun
+from maze_poisson_b200.systems import make_system
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def rel(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def prod(product_path):
+    return CAPI(product_path)
+
+
+@pytest.fixture(scope="module")
+def orc(oracle_path):
+    return CAPI(oracle_path, extensions=False)
+
+
+def run_pair(prod, orc, system, steps, check_each=True, noise=False, **kw):
+    """Run the same MD on product and oracle; compare after init and every step."""
+    a = MDRun(prod, system.copy(), **kw)
+    b = MDRun(orc, system.copy(), **kw)
+    a.initialize()
+    if noise:
+        from oracle.loader import load_kernels
+        ok = load_kernels()
+        calls = 2 + 2 * steps
+        z = np.empty((calls, system.n_ions, 3))
+        for c in range(calls):
+            prod.mzb_philox_normals(c, z[c])
+        ok.orc_set_noise(np.ascontiguousarray(z.reshape(-1)), z.size)
+    b.initialize()
+    try:
+        sa, sb = a.state(), b.state()
+        assert np.array_equal(sa["q"], sb["q"])
+        assert rel(sa["field"], sb["field"]) < TOL
+        for key in ("fcs_elec", "fcs_noel", "fcs_tot", "pos", "vel"):
+            assert rel(sa[key], sb[key]) < TOL, key
+        assert abs(sa["potential_notelec"] - sb["potential_notelec"]) <= TOL * abs(sb["potential_notelec"])
+        for s in range(steps):
+            a.step()
+            b.step()
+            if check_each or s == steps - 1:
+                sa, sb = a.state(), b.state()
+                assert abs(sa["n_iters"] - sb["n_iters"]) <= 1, (s, sa["n_iters"], sb["n_iters"])
+                for key in ("field", "fcs_tot", "pos", "vel"):
+                    assert rel(sa[key], sb[key]) < TOL, (s, key, rel(sa[key], sb[key]))
+                assert abs(sa["kinetic"] - sb["kinetic"]) <= TOL * sb["kinetic"]
+        return sa, sb
+    finally:
+        a.finalize()
+        b.finalize()
+
+
+SCEN = json.load(open(os.path.join(GOLDEN, "scenarios.json")))
+
+
+@pytest.mark.parametrize("name", sorted(SCEN))
+def test_golden_scenarios(prod, name):
+    """Product against the reference's own trajectories (tests/golden)."""
+    ncell, ng, method, precond, tol, itg, thermo, steps = SCEN[name]
+    g = np.load(os.path.join(GOLDEN, f"md_{name}.npz"))
+    system = make_system(ncell, ng, density=1.379, T=1200.0, seed=7)
+    run = MDRun(prod, system, method=method, precond=precond, tol=tol, integrator=itg,
+                thermostat=thermo)
+    run.initialize()
+    try:
+        st = run.state()
+        for key in ("fcs_tot", "fcs_elec", "fcs_noel", "pos", "vel"):
+            assert rel(st[key], g["init_" + key]) < TOL, key
+        if "init_q" in g:
+            assert np.array_equal(st["q"], g["init_q"])
+        for s in range(steps):
+            run.step()
+            st = run.state()
+            assert abs(st["n_iters"] - int(g[f"s{s}_iters"])) <= 1
+            for key in ("pos", "vel", "fcs_tot"):
+                assert rel(st[key], g[f"s{s}_{key}"]) < TOL, (s, key)
+            assert rel(st["field"].reshape(-1)[::101], g[f"s{s}_field_sample"]) < TOL
+    finally:
+        run.finalize()
+
+
+def test_lcg_verlet_250(prod, orc):
+    run_pair(prod, orc, make_system(5, 64, seed=3), 6, method="LCG", tol=1e-7)
+
+
+def test_maze_lcg_250(prod, orc):
+    run_pair(prod, orc, make_system(5, 64, seed=4), 4, method="MAZE-LCG", tol=1e-7)
+
+
+def test_maze_lcg_jacobi_250(prod, orc):
+    run_pair(prod, orc, make_system(5, 64, seed=5), 3, method="MAZE-LCG", precond="JACOBI", tol=1e-7)
+
+
+def test_multigrid_250(prod, orc):
+    run_pair(prod, orc, make_system(5, 64, seed=6), 2, method="MULTIGRID", tol=1e-7)
+
+
+def test_maze_multigrid_250(prod, orc):
+    run_pair(prod, orc, make_system(5, 64, seed=8), 2, method="MAZE-MULTIGRID", tol=1e-7)
+
+
+def test_ovrvo_thermostat_injected_noise(prod, orc):
+    """OVRVO with the thermostat on: the oracle's O-block is fed the GPU's Philox draws."""
+    run_pair(prod, orc, make_system(3, 32, seed=9), 4, noise=True, method="LCG", tol=1e-9,
+             integrator="OVRVO", thermostat=True, gamma_per_ps=1.0)
+
+
+def test_fft_path(prod, oracle_lib):
+    """FFT method: q bit-exact, phi = numpy oracle of the same q, forces bit-exact."""
+    from oracle.fft_oracle import fft_poisson
+    system = make_system(5, 64, seed=10)
+    run = MDRun(prod, system.copy(), method="FFT")
+    run.initialize()
+    try:
+        for _ in range(2):
+            run.step()
+        st = run.state()
+        s = run.sys
+        assert rel(st["field"], fft_poisson(st["q"], s.L, s.h)) < 1e-12
+        # the last forces were computed from the current positions (part 2 only kicks)
+        nbr = np.empty((s.n_ions, 8, 3), dtype=np.int64)
+        oracle_lib.orc_cic_neighbors(st["pos"], s.n_ions, s.n_grid, s.h, nbr)
+        f = np.empty((s.n_ions, 3))
+        oracle_lib.orc_force_fd(st["field"], nbr, s.charges, st["pos"], s.n_ions, s.n_grid, s.h, f)
+        assert np.array_equal(st["fcs_elec"], f)
+        # FFT keeps no previous field: get_field_prev returns phi (solver_md.c:289-292)
+        assert np.array_equal(st["field_prev"], st["field"])
+    finally:
+        run.finalize()
+
+
+def test_particle_kernels_bitexact(prod, oracle_lib):
+    """CIC corners, q, field force of a given phi, linked cells, and the Tosi-Fumi forces."""
+    s = make_system(10, 64, density=1.329, seed=12)
+    # exercise the box edges: ions at 0, at L - tiny, and a dense cluster in one tile
+    s.pos[0] = [0.0, 0.0, 0.0]
+    s.pos[1] = [s.L * (1 - 1e-16), s.L * 0.5, s.L * (1 - 1e-15)]
+    s.pos[2:40] = s.pos[2] * 0 + np.array([1.0, 1.0, 1.0]) * s.h * 0.25 + \
+        np.random.default_rng(0).uniform(0, s.h * 3.5, (38, 3))
+    run = MDRun(prod, s, method="LCG", tol=1e-6)
+    prod.solver_initialize()
+    maps = prod.type_maps()
+    prod.solver_initialize_grid(s.n_grid, s.L, s.h, 1e-6, 1.0, 1.0, maps["method"]["LCG"], 0)
+    prod.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, 0, 0, s.types, s.pos, s.vel,
+                                     s.mass, s.charges, s.pot_params)
+    prod.solver_initialize_integrator(s.n_ions, 1.0, 1200.0, 0.0, 1, 0)
+    try:
+        # charges: 38 clustered ions make the grid non-neutral locally but the total stays 0
+        assert prod.solver_update_charges() == 0
+        nbr = np.empty((s.n_ions, 8, 3), dtype=np.int64)
+        prod.mzb_get_cic_neighbors(nbr)
+        nbo = np.empty_like(nbr)
+        oracle_lib.orc_cic_neighbors(s.pos, s.n_ions, s.n_grid, s.h, nbo)
+        assert np.array_equal(nbr, nbo)
+        q = np.empty((64, 64, 64))
+        prod.get_q(q)
+        qo = np.empty_like(q)
+        oracle_lib.orc_spread_cic(s.pos, s.charges, nbo, s.n_ions, 64, s.h, qo)
+        assert np.array_equal(q, qo)
+        # field force on an arbitrary phi
+        phi = np.random.default_rng(1).standard_normal((64, 64, 64))
+        prod.solver_set_field(phi)
+        prod.solver_compute_forces_elec()
+        fe = np.empty((s.n_ions, 3))
+        prod.get_fcs_elec(fe)
+        feo = np.empty_like(fe)
+        oracle_lib.orc_force_fd(phi, nbo, s.charges, s.pos, s.n_ions, 64, s.h, feo)
+        assert np.array_equal(fe, feo)
+        # linked cells
+        for nc in (3, 4, 7):
+            prod.mzb_set_cell_grid(nc)
+            st = np.empty(nc ** 3 + 1, dtype=np.int32)
+            io = np.empty(s.n_ions, dtype=np.int32)
+            assert prod.mzb_get_cells(st, io) == nc
+            sto, ioo = np.empty_like(st), np.empty_like(io)
+            oracle_lib.orc_cell_list(s.pos, s.n_ions, s.L, nc, sto, ioo)
+            assert np.array_equal(st, sto) and np.array_equal(io, ioo)
+        # Tosi-Fumi forces and energy
+        tab = np.empty(28)
+        oracle_lib.orc_tf_table(s.pot_params, 2, s.L, tab)
+        for nc in (1, 4):
+            prod.mzb_set_cell_grid(nc)
+            e = prod.solver_compute_forces_noel()
+            fn = np.empty((s.n_ions, 3))
+            prod.get_fcs_noel(fn)
+            fno = np.empty_like(fn)
+            eo = oracle_lib.orc_tf_forces(s.pos, s.types, tab, 2, s.n_ions, s.L, s.L / 2, fno)
+            assert rel(fn, fno) < 1e-12
+            assert abs(e - eo) < 1e-12 * abs(eo)
+    finally:
+        prod.solver_finalize()
+
+
+def test_philox_matches_restatement(prod):
+    from oracle.philox import normals
+    s = make_system(3, 32, seed=1)
+    run = MDRun(prod, s, integrator="OVRVO", thermostat=True)
+    prod.solver_initialize()
+    prod.solver_initialize_grid(32, s.L, s.h, 1e-7, 1.0, 1.0, 0, 0)
+    prod.solver_initialize_particles(32, 2, s.L, s.h, s.n_ions, 0, 0, s.types, s.pos, s.vel, s.mass,
+                                     s.charges, s.pot_params)
+    try:
+        for seed, call in [(0x5eed, 0), (0x5eed, 7), (2 ** 40 + 3, 2 ** 33 + 1)]:
+            prod.mzb_set_seed(seed)
+            z = np.empty((s.n_ions, 3))
+            prod.mzb_philox_normals(call, z)
+            assert np.max(np.abs(z - normals(seed, call, s.n_ions))) < 1e-13
+        prod.mzb_set_seed(0x5eed)
+    finally:
+        prod.solver_finalize()
+    del run
+
+
+def test_charge_conservation_failure_exits():
+    """A non-neutral system makes solver_update_charges print and exit(1), as the
+    reference does (library/src/solver_md.c:91-107)."""
+    code = f"""
+import sys; sys.path.insert(0, {ROOT!r})
+import numpy as np
+from maze_poisson_b200.c_api import CAPI
+from maze_poisson_b200.systems import make_system
+s = make_system(2, 16, seed=1)
+s.charges[0] = 3.0
+c = CAPI(); c.solver_initialize()
+c.solver_initialize_grid(16, s.L, s.h, 1e-7, 1.0, 1.0, 0, 0)
+c.solver_initialize_particles(16, 2, s.L, s.h, s.n_ions, 0, 0, s.types, s.pos, s.vel, s.mass, s.charges, s.pot_params)
+c.solver_update_charges()
+print("not reached")
+"""
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300,
+                       env=dict(os.environ, MZB_QUIET="1"))
+    assert r.returncode == 1
+    assert "Charge conservation error" in r.stdout
+    assert "not reached" not in r.stdout
