@@ -43,4 +43,4 @@ def fft_poisson(q, L, h):
     dc = X[0, 0, 0]
     X = X * g
     X[0, 0, 0] = dc
-    return np.fft.irfftn(X, s=q.shape) * float(n * n * n)
+    return np.fft.irfftn(X, s=q.shape, axes=(0, 1, 2)) * float(n * n * n)
