@@ -22,12 +22,13 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
 # source -> extra flags
 SOURCES = {
     "engine.cu": ["--fmad=false"],
+    "cg_fast.cu": ["--fmad=false"],
     "particles.cu": ["--fmad=false"],
     "tf_forces.cu": ["--fmad=true"],
     "fft.cu": ["--fmad=false"],
     "facade.cu": ["--fmad=false"],
 }
-HEADERS = ["mzb_common.cuh", "engine.cuh", "particles.cuh", "fft.cuh"]
+HEADERS = ["mzb_common.cuh", "engine.cuh", "particles.cuh", "fft.cuh", "tma.cuh"]
 
 
 def _nvcc():

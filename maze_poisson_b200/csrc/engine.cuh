@@ -68,10 +68,16 @@ struct EngineArgs {
     double* partials;  // 2 sets x 8 values x gridDim.x
     GridBarrier* bar;
     int* result;       // [0] program return value, [1] engine status (0 ok)
+    unsigned long long* stamps;  // optional phase timestamps of the CG kernel (or null)
 };
 
 // Launch the engine for `a` on `stream` (cooperative; shapes chosen once per device).
 void engine_launch(const EngineArgs& a, cudaStream_t stream);
+// Launch a CG program (PROG_CG, PROG_PCG with Jacobi, PROG_INIT_FIELD, PROG_LCG_UPDATE,
+// PROG_MAZE_LCG without MG) on the TMA-staged kernel of cg_fast.cu; false when the grid
+// size or device does not allow it (the caller then uses engine_launch).
+bool cg_fast_launch(const EngineArgs& a, cudaStream_t stream);
+int cg_fast_stamp_slots();
 // Bytes of partials the engine needs and its grid size on this device.
 int engine_grid_blocks();
 

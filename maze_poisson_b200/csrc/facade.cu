@@ -164,7 +164,39 @@ EngineArgs engine_base(System& s) {
 // is reported and turned into -1 ("not converged").
 int run_engine(System& s, const EngineArgs& a) {
     MZB_CHECK(cudaEventRecord(s.ev0, s.stream));
-    engine_launch(a, s.stream);
+    static const bool generic_only = getenv("MZB_ENGINE") && strcmp(getenv("MZB_ENGINE"), "generic") == 0;
+    // MZB_PHASE_TIMING=1: time-stamp the phases of the CG kernel and print them (debug aid)
+    static const bool stamps_on = getenv("MZB_PHASE_TIMING") != nullptr;
+    static unsigned long long* stamps_d = nullptr;
+    EngineArgs b = a;
+    if (stamps_on) {
+        if (!stamps_d) MZB_CHECK(cudaMalloc(&stamps_d, sizeof(unsigned long long) * 96));
+        MZB_CHECK(cudaMemsetAsync(stamps_d, 0, sizeof(unsigned long long) * 96, s.stream));
+        b.stamps = stamps_d;
+    }
+    if (generic_only || !cg_fast_launch(b, s.stream)) engine_launch(a, s.stream);
+    if (stamps_on) {
+        unsigned long long h[96];
+        MZB_CHECK(cudaMemcpyAsync(h, stamps_d, sizeof(h), cudaMemcpyDeviceToHost, s.stream));
+        MZB_CHECK(cudaStreamSynchronize(s.stream));
+        if (h[0]) {
+            fprintf(stderr, "[cg phases us] pre %.2f sync %.2f init %.2f |", (h[1] - h[0]) * 1e-3,
+                    (h[2] - h[1]) * 1e-3, 0.0);
+            for (int it = 0; it + 1 < (cg_fast_stamp_slots() - 4) / 4; it++) {
+                const unsigned long long* t = h + 4 + 4 * it;
+                if (!t[0] || !t[4]) break;
+                fprintf(stderr, " A %.2f redA %.2f B %.2f redB %.2f |", (t[0] - (it ? t[-1] : h[2])) * 1e-3,
+                        (t[1] - t[0]) * 1e-3, (t[2] - t[1]) * 1e-3, (t[3] - t[2]) * 1e-3);
+            }
+            fprintf(stderr, "\n[cg phase A slabs us: sync+issue, p_new, stencil]");
+            for (int e = 0; e < 18 && h[40 + 3 * e]; e++) {
+                const unsigned long long prev = e ? h[39 + 3 * e] : h[2];
+                fprintf(stderr, " %.2f,%.2f,%.2f", (h[40 + 3 * e] - prev) * 1e-3, (h[41 + 3 * e] - h[40 + 3 * e]) * 1e-3,
+                        (h[42 + 3 * e] - h[41 + 3 * e]) * 1e-3);
+            }
+            fprintf(stderr, "\n");
+        }
+    }
     MZB_CHECK(cudaEventRecord(s.ev1, s.stream));
     MZB_CHECK(cudaMemcpyAsync(s.result_h, s.result, 2 * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
     MZB_CHECK(cudaStreamSynchronize(s.stream));

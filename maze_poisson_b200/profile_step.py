@@ -1,0 +1,38 @@
+"""Run a few MD steps of a named workload through the C ABI -- the command the committed
+ncu summaries (profiles/) profile.
+
+    python -m maze_poisson_b200.profile_step --workload nacl2000_128 --method LCG --steps 1
+
+Launch order of the field-solver kernels: two solves from zero (the two bootstrap steps of
+SolverMD.initialize_md) then one warm-started solve per step.
+"""
+import argparse
+import os
+
+from .c_api import CAPI
+from .md import MDRun
+from .systems import WORKLOADS, make_system
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="nacl2000_128", choices=sorted(WORKLOADS))
+    ap.add_argument("--method", default="LCG")
+    ap.add_argument("--precond", default="NONE")
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--integrator", default="OVRVO")
+    ap.add_argument("--steps", type=int, default=1)
+    args = ap.parse_args()
+    os.environ.setdefault("MZB_QUIET", "1")
+    run = MDRun(CAPI(), make_system(seed=1, **WORKLOADS[args.workload]), method=args.method,
+                precond=args.precond, tol=args.tol, integrator=args.integrator,
+                thermostat=args.integrator.upper() == "OVRVO")
+    run.initialize()
+    for _ in range(args.steps):
+        run.step()
+    run.finalize()
+    print("ok")
+
+
+if __name__ == "__main__":
+    main()
