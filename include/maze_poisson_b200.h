@@ -42,6 +42,18 @@ void mzb_philox_normals(uint64_t call, double *out); /* O-block draws of call `c
 void mzb_set_seed(uint64_t seed);          /* O-block Philox key */
 uint64_t mzb_get_ocalls(void);             /* O-blocks applied so far */
 
+/* CG solve that allocates no device memory, for callers that cannot call cudaMalloc
+   (a host framework that owns all device allocations, a loop that must not take an
+   allocation's implicit synchronisation). No counterpart in the reference. b, x0, x are
+   caller-owned device buffers of n^3 doubles, 2 <= n <= 64; the work arrays live in a
+   static ~8.4 MB device array that every GPU loading this library holds until exit and
+   that all calls share (overlapping calls race). The first call per device looks up that
+   array's address; make it before any stream capture. Returns iterations or -1 as
+   conj_grad does, -2 for unsupported arguments, -3 if the solver aborted, -4 if the work
+   area's address is unavailable. precond: 0 implicit Jacobi, 1 Jacobi. */
+int mzb_conj_grad_noalloc(const double *b, const double *x0, double *x, double tol, int n,
+                          int precond, void *stream);
+
 /* instrumentation */
 void *mzb_get_stream(void);                /* cudaStream_t of the current system */
 double mzb_last_solve_ms(void);            /* device ms of the last field-solver launch */

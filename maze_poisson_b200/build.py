@@ -27,6 +27,7 @@ SOURCES = {
     "tf_forces.cu": ["--fmad=true"],
     "fft.cu": ["--fmad=false"],
     "facade.cu": ["--fmad=false"],
+    "noalloc.cu": ["--fmad=false"],
 }
 HEADERS = ["mzb_common.cuh", "engine.cuh", "particles.cuh", "fft.cuh", "tma.cuh"]
 
