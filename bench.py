@@ -19,6 +19,8 @@ charge spreading, field solve, field + pair + total forces, integrator part 2.
           steps, then K steps of the reference's per-call sequence, each followed by the
           output getters get_pos/get_vel/get_fcs_tot (D2H into pinned host memory);
           wall-clock over the whole job / K.
+  modes : the same steps with the field solve in FP32 multigrid + FP64 refinement
+          (same FP64 residual tolerance), its steps/s and force RMS error against FP64.
   roofline : the solver-engine launch (one field solve per step) against the measured
           HBM copy bandwidth; algorithmic bytes per launch = (5 + 8 (it+1)) * 8 B * n^3
           (CG: x, r, p read+write and Ap write+read per iteration; set-up 5 passes).
@@ -120,11 +122,30 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_run(capi, rank):
+def make_run(capi, rank, precision=0):
     from maze_poisson_b200.md import MDRun
     from maze_poisson_b200.systems import make_system
     system = make_system(seed=1000 + rank, T=SOLVER["T"], **WORKLOAD)
-    return MDRun(capi, system, **{k: v for k, v in SOLVER.items()})
+    return MDRun(capi, system, precision=precision, **{k: v for k, v in SOLVER.items()})
+
+
+def timed_steps(capi, stream, flush, steps):
+    """Device time of `steps` MD steps (CUDA events on the library stream, L2 flushed
+    before each), the mean solve time and the solver's return values."""
+    import torch
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    solve_ms, iters = [], []
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+            ev[k][0].record(stream)
+        capi.solver_md_step(1)
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+        solve_ms.append(capi.mzb_last_solve_ms())
+        iters.append(capi.mzb_last_solve_result())
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in ev), solve_ms, iters
 
 
 def bench_b200(args, rank, world, dist):
@@ -149,29 +170,43 @@ def bench_b200(args, rank, world, dist):
     clocks = ClockSampler(local)
     clocks.start()
     launches0 = capi.mzb_kernel_launches()
-    total_ms, solve_ms, iters = 0.0, [], []
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(float(k))
-            ev[k][0].record(stream)
-        capi.solver_md_step(1)
-        with torch.cuda.stream(stream):
-            ev[k][1].record(stream)
-        solve_ms.append(capi.mzb_last_solve_ms())
-        iters.append(capi.mzb_last_solve_result())
-    torch.cuda.synchronize()
+    total_ms, solve_ms, iters = timed_steps(capi, stream, flush, args.steps)
     launches = capi.mzb_kernel_launches() - launches0
-    total_ms = sum(a.elapsed_time(b) for a, b in ev)
     clk = clocks.stop()
     t = torch.tensor([total_ms], dtype=torch.float64, device=f"cuda:{local}")
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     max_ms = float(t.item())
     run.finalize()
-    del flush
 
+    # FP32+refine form on the same workload and tolerance: steps/s and its force error
+    # against the FP64 form at the same initial state (after the two bootstrap steps)
+    mixed = None
+    if not args.fp64_only:
+        ref = make_run(capi, rank)
+        ref.initialize()
+        f_ref = ref.state(fields=False)["fcs_tot"]
+        ref.finalize()
+        mrun = make_run(capi, rank, precision=1)
+        mrun.initialize()
+        f_mix = mrun.state(fields=False)["fcs_tot"]
+        stream = torch.cuda.ExternalStream(capi.mzb_get_stream(), device=local)
+        for _ in range(args.warmup):
+            capi.solver_md_step(1)
+        torch.cuda.synchronize()
+        m_ms, m_solve, m_iters = timed_steps(capi, stream, flush, args.steps)
+        mrun.finalize()
+        tm = torch.tensor([m_ms], dtype=torch.float64, device=f"cuda:{local}")
+        if dist is not None:
+            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        rms = float(np.sqrt(np.mean((f_mix - f_ref) ** 2)) / np.sqrt(np.mean(f_ref ** 2)))
+        mixed = {"value": round(args.steps * world / (float(tm.item()) / 1e3), 3), "unit": "steps/s",
+                 "ms_per_step": round(float(tm.item()) / args.steps, 4),
+                 "solve_ms": round(statistics.mean(m_solve), 4),
+                 "refinement_steps": statistics.mean(m_iters),
+                 "force_rms_rel_err_vs_fp64": rms,
+                 "dtype": "f32 multigrid + f64 refinement"}
+    del flush
     # end to end through the reference ABI from pinned host buffers
     e2e = bench_e2e(args, capi, rank)
     if dist is not None:
@@ -211,6 +246,10 @@ def bench_b200(args, rank, world, dist):
                      "traffic_source": (traffic or {}).get("source")},
         "gpu_launches": int(launches),
         "clocks": clk,
+        "modes": {"fp64": {"value": round(args.steps * world / (max_ms / 1e3), 3), "unit": "steps/s",
+                           "solve_ms": round(mean_solve_s * 1e3, 4), "cg_iterations": mean_iters,
+                           "dtype": "f64 (reference algorithms)"},
+                  "fp32_refine": mixed},
     }
     return line
 
@@ -316,6 +355,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp64-only", action="store_true", help="skip the FP32+refine measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))

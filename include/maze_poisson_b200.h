@@ -34,6 +34,13 @@ int mzb_cg_coarse(const double *b, double *x, int n, int maxit, double rtol); /*
 void mzb_mg_apply(const double *rhs, double *x, int n, int sm);            /* multigrid.c:99-168 */
 void mzb_fft_poisson(const double *q, double *phi, int n, double L, double h); /* fftw_wrap.c:166-189 */
 
+/* precision of the field solve: 0 = the reference's FP64 algorithms (default), 1 = FP32
+   multigrid V-cycles with FP64 iterative refinement until the FP64 residual meets the
+   grid's tol (or tol_override when > 0). Also selected by MZB_PRECISION=mixed at
+   solver_initialize_grid. FFT grids and grids that cannot be halved twice stay FP64. */
+void mzb_set_precision(int mode, double tol_override);
+int mzb_get_precision(void);      /* precision in effect for the current grid */
+
 /* state accessors of the current system */
 void mzb_get_cic_neighbors(int64_t *out);  /* (n_p,8,3) CIC corners, particles.c:297-346 */
 void mzb_set_cell_grid(int nc);            /* linked cells per side for the pair forces */

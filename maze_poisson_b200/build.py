@@ -28,8 +28,9 @@ SOURCES = {
     "fft.cu": ["--fmad=false"],
     "facade.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
+    "mixed.cu": ["--fmad=true"],
 }
-HEADERS = ["mzb_common.cuh", "engine.cuh", "particles.cuh", "fft.cuh", "tma.cuh"]
+HEADERS = ["mzb_common.cuh", "engine.cuh", "particles.cuh", "fft.cuh", "tma.cuh", "mixed.cuh"]
 
 
 def _nvcc():

@@ -164,42 +164,6 @@ __device__ __forceinline__ double zf(double r) {
     return -1.0 * (-r / 6.0);
 }
 
-// Sequence of plane slabs the CTA streams in phase A: for every run of items with the
-// same j-block, planes ia-1, ia, ..., ib+1 (wrapped).
-struct Plan {
-    long w0, w1;
-    int n;
-    // element e -> (jb, plane, position in run: 0 = ia-1, 1 = ia, ...), run length
-    __device__ bool at(long e, int& jb, int& plane, int& pos, int& len) const {
-        long w = w0;
-        while (w < w1) {
-            const int b = (int)(w / n);
-            const long wend = min(w1, (long)(b + 1) * n);
-            const int L = (int)(wend - w) + 2;
-            if (e < L) {
-                jb = b;
-                pos = (int)e;
-                len = L;
-                const int ia = (int)(w - (long)b * n);
-                plane = ((ia - 1 + (int)e) % n + n) % n;
-                return true;
-            }
-            e -= L;
-            w = wend;
-        }
-        return false;
-    }
-    __device__ long total() const {
-        long t = 0, w = w0;
-        while (w < w1) {
-            const int b = (int)(w / n);
-            const long wend = min(w1, (long)(b + 1) * n);
-            t += (wend - w) + 2;
-            w = wend;
-        }
-        return t;
-    }
-};
 
 // KIND: PrecondKind; PPT: column pairs per compute thread (1 for n <= 128, else 2). With
 // 17 warps one SM sub-partition holds 5 of them, so 96 registers is the most a thread may

@@ -13,6 +13,7 @@
 
 #include "engine.cuh"
 #include "fft.cuh"
+#include "mixed.cuh"
 #include "particles.cuh"
 
 namespace mzb {
@@ -66,6 +67,14 @@ struct GridState {
            *tmp = nullptr;
     double *rc = nullptr, *ec = nullptr, *cr = nullptr, *cp0 = nullptr, *cp1 = nullptr, *cAp = nullptr;
     FftPoisson fft;
+    // mixed precision (FP32 multigrid + FP64 refinement)
+    int precision = 0;        // 0: FP64 reference algorithms, 1: mixed
+    double mixed_tol = 0.0;   // > 0 overrides tol for the mixed solve
+    int nlev = 0;
+    int lev_n[kMixedMaxLevels] = {};
+    float* lev_x[kMixedMaxLevels] = {};
+    float* lev_b[kMixedMaxLevels] = {};
+    float* lev_r[kMixedMaxLevels] = {};
 
     double* phi() const { return buf[iphi]; }
     double* phi_prev() const { return buf[iprev]; }
@@ -117,7 +126,32 @@ void free_grid(GridState& G) {
     dfree(G.r); dfree(G.p0); dfree(G.p1); dfree(G.Ap); dfree(G.v); dfree(G.rf); dfree(G.tmp);
     dfree(G.rc); dfree(G.ec); dfree(G.cr); dfree(G.cp0); dfree(G.cp1); dfree(G.cAp);
     G.fft.release();
+    for (int l = 0; l < kMixedMaxLevels; l++) {
+        if (G.lev_x[l]) cudaFree(G.lev_x[l]);
+        if (G.lev_b[l]) cudaFree(G.lev_b[l]);
+        if (G.lev_r[l]) cudaFree(G.lev_r[l]);
+        G.lev_x[l] = G.lev_b[l] = G.lev_r[l] = nullptr;
+    }
+    G.nlev = 0;
     G.ready = false;
+}
+
+// Mixed precision needs at least three multigrid levels (n, n/2, n/4 even).
+bool mixed_supported(const GridState& G) {
+    int sizes[kMixedMaxLevels];
+    return G.type != 1 && mixed_levels(G.n, sizes) >= 3;
+}
+
+void ensure_mixed_levels(GridState& G) {
+    if (G.nlev) return;
+    G.nlev = mixed_levels(G.n, G.lev_n);
+    for (int l = 0; l < G.nlev; l++) {
+        const size_t m = (size_t)G.lev_n[l] * G.lev_n[l] * G.lev_n[l];
+        MZB_CHECK(cudaMalloc(&G.lev_x[l], m * sizeof(float)));
+        MZB_CHECK(cudaMalloc(&G.lev_b[l], m * sizeof(float)));
+        MZB_CHECK(cudaMalloc(&G.lev_r[l], m * sizeof(float)));
+        MZB_CHECK(cudaMemset(G.lev_x[l], 0, m * sizeof(float)));
+    }
 }
 
 void free_particles(ParticleDev& P) {
@@ -209,6 +243,55 @@ int run_engine(System& s, const EngineArgs& a) {
     return s.result_h[0];
 }
 
+// Mixed-precision solve of program `prog` (see mixed.cu); returns refinement steps or -1.
+int run_mixed(System& s, int prog, double cst) {
+    GridState& G = s.G;
+    ensure_mixed_levels(G);
+    MixedArgs m{};
+    m.prog = prog;
+    m.n = G.n;
+    m.tol = G.mixed_tol > 0 ? G.mixed_tol : G.tol;
+    m.c = cst;
+    m.max_outer = 100;
+    m.cycles = 1;
+    m.nu1 = 2;
+    m.nu2 = 2;
+    m.coarse_sweeps = 40;
+    m.nlev = G.nlev;
+    for (int l = 0; l < G.nlev; l++) {
+        m.lev_n[l] = G.lev_n[l];
+        m.lev_x[l] = G.lev_x[l];
+        m.lev_b[l] = G.lev_b[l];
+        m.lev_r[l] = G.lev_r[l];
+    }
+    m.q = G.q;
+    m.phi_old = G.phi();
+    m.phi_prev = G.phi_prev();
+    m.phi_new = G.buf[G.ispare];
+    m.y = G.y;
+    m.tmp = G.tmp;
+    m.partials = s.partials;
+    m.bar = s.bar;
+    m.result = s.result;
+    MZB_CHECK(cudaEventRecord(s.ev0, s.stream));
+    mixed_launch(m, s.stream);
+    MZB_CHECK(cudaEventRecord(s.ev1, s.stream));
+    MZB_CHECK(cudaMemcpyAsync(s.result_h, s.result, 2 * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    MZB_CHECK(cudaStreamSynchronize(s.stream));
+    MZB_CHECK(cudaEventElapsedTime(&s.last_solve_ms, s.ev0, s.ev1));
+    s.last_solve_iters = s.result_h[0];
+    if (s.result_h[1] != 0) {
+        fprintf(stderr, "maze_poisson_b200: mixed solver aborted (grid barrier timeout)\n");
+        return -1;
+    }
+    // phi_prev <- old phi, phi <- new
+    const int old = G.iphi;
+    G.iphi = G.ispare;
+    G.ispare = G.iprev;
+    G.iprev = old;
+    return s.result_h[0];
+}
+
 void require_mg_size(int n) {
     // multigrid.c:114-121: at least one level of recursion, n/2 >= 16
     if (n / 2 < 16 || n % 2) fatal("Multigrid: requires an even grid with n/2 >= 16");
@@ -288,6 +371,10 @@ void solver_initialize_grid(int n, double L, double h, double tol, double eps, d
     G.eps_int = eps_int;
     G.m = (long)n * n * n;
     G.iphi = 0; G.iprev = 1; G.ispare = 2;
+    {
+        const char* pm = getenv("MZB_PRECISION");
+        G.precision = (pm && strcmp(pm, "mixed") == 0) ? 1 : 0;
+    }
     G.q = dalloc<double>(G.m);
     G.buf[0] = dalloc<double>(G.m);
     if (grid_type == G_FFT) {
@@ -442,6 +529,10 @@ void solver_init_field(void) {
         sync();
         return;
     }
+    if (G.precision == 1 && mixed_supported(G)) {
+        run_mixed(s, PROG_INIT_FIELD, rhs_const(G));
+        return;
+    }
     EngineArgs a = engine_base(s);
     a.prog = PROG_INIT_FIELD;
     a.c = rhs_const(G);
@@ -463,6 +554,15 @@ int solver_update_field(void) {
         G.fft.solve(G.q, G.phi(), s.stream);
         sync();
         return 0;
+    }
+    if (G.precision == 1 && mixed_supported(G)) {
+        if (G.type == G_MAZE_MG && G.precond != P_NONE) {  // grid_maze_multigrid.c:138-141
+            fprintf(stderr, "Maze Multigrid with preconditioner not implemented yet.\n");
+            exit(1);
+        }
+        if (G.type == G_LCG) return run_mixed(s, PROG_LCG_UPDATE, rhs_const(G));
+        if (G.type == G_MG) return run_mixed(s, PROG_MG_UPDATE, rhs_const(G));
+        return run_mixed(s, G.type == G_MAZE_LCG ? PROG_MAZE_LCG : PROG_MAZE_MG, (4 * kPi) / (G.h * G.eps_s));
     }
     EngineArgs a = engine_base(s);
     a.phi_old = G.phi();
@@ -930,6 +1030,19 @@ void mzb_philox_normals(uint64_t call, double* out) {
 }
 
 void mzb_set_seed(uint64_t seed) { sys().I.seed = seed; }
+
+// Field-solve precision of the current grid: 0 = the reference's FP64 algorithms,
+// 1 = FP32 multigrid with FP64 iterative refinement to the same (or an overriding)
+// tolerance. Grids that cannot be coarsened three times, and FFT, stay FP64.
+void mzb_set_precision(int mode, double tol_override) {
+    GridState& G = grid();
+    G.precision = mode == 1 ? 1 : 0;
+    G.mixed_tol = tol_override;
+}
+int mzb_get_precision(void) {
+    GridState& G = grid();
+    return (G.precision == 1 && mixed_supported(G)) ? 1 : 0;
+}
 
 // The CUDA stream all work of the current system is queued on (for callers that time
 // it with their own events or order their own kernels against it).

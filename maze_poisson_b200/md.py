@@ -18,7 +18,7 @@ def gamma_au(gamma_per_ps):
 class MDRun:
     def __init__(self, capi, system, method="LCG", precond="NONE", tol=1e-7, integrator="VERLET",
                  thermostat=False, T=1200.0, gamma_per_ps=1.0, dt_fs=1.0, eps_s=1.0, eps_int=1.0,
-                 rescale=False):
+                 rescale=False, precision=0, mixed_tol=0.0):
         self.capi = capi
         self.sys = system
         self.method = method.upper()
@@ -32,6 +32,10 @@ class MDRun:
         self.eps_s = eps_s
         self.eps_int = eps_int
         self.rescale = rescale
+        # field-solve precision (this build's extension): 0 FP64 reference algorithms,
+        # 1 FP32 multigrid + FP64 refinement to mixed_tol (or tol when 0)
+        self.precision = precision
+        self.mixed_tol = mixed_tol
         self.n_iters = None
         self.potential_notelec = None
 
@@ -43,6 +47,8 @@ class MDRun:
         maps = c.type_maps()
         c.solver_initialize_grid(s.n_grid, s.L, s.h, self.tol, self.eps_s, self.eps_int,
                                  maps["method"][self.method], maps["precond"][self.precond])
+        if self.precision:
+            c.mzb_set_precision(int(self.precision), float(self.mixed_tol))
         c.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, maps["potential"]["TF"],
                                       maps["cas"]["CIC"], s.types, s.pos, s.vel, s.mass, s.charges,
                                       s.pot_params)
