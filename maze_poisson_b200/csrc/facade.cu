@@ -75,6 +75,7 @@ struct GridState {
     float* lev_x[kMixedMaxLevels] = {};
     float* lev_b[kMixedMaxLevels] = {};
     float* lev_r[kMixedMaxLevels] = {};
+    float* lev_g = nullptr;   // Green's function of the coarsest level (direct solve) or null
 
     double* phi() const { return buf[iphi]; }
     double* phi_prev() const { return buf[iprev]; }
@@ -132,6 +133,10 @@ void free_grid(GridState& G) {
         if (G.lev_r[l]) cudaFree(G.lev_r[l]);
         G.lev_x[l] = G.lev_b[l] = G.lev_r[l] = nullptr;
     }
+    if (G.lev_g) {
+        cudaFree(G.lev_g);
+        G.lev_g = nullptr;
+    }
     G.nlev = 0;
     G.ready = false;
 }
@@ -139,7 +144,8 @@ void free_grid(GridState& G) {
 // Mixed precision needs at least three multigrid levels (n, n/2, n/4 even).
 bool mixed_supported(const GridState& G) {
     int sizes[kMixedMaxLevels];
-    return G.type != 1 && mixed_levels(G.n, sizes) >= 3;
+    const int L = mixed_levels(G.n, sizes);
+    return G.type != 1 && L >= 3 && mixed_small_level(L, sizes) >= 1;
 }
 
 void ensure_mixed_levels(GridState& G) {
@@ -151,6 +157,13 @@ void ensure_mixed_levels(GridState& G) {
         MZB_CHECK(cudaMalloc(&G.lev_b[l], m * sizeof(float)));
         MZB_CHECK(cudaMalloc(&G.lev_r[l], m * sizeof(float)));
         MZB_CHECK(cudaMemset(G.lev_x[l], 0, m * sizeof(float)));
+    }
+    const int nc = G.lev_n[G.nlev - 1];
+    if (nc <= kMixedDirectN && mixed_small_level(G.nlev, G.lev_n) < G.nlev) {
+        std::vector<float> g((size_t)nc * nc * nc);
+        mixed_coarse_green(nc, g.data());
+        MZB_CHECK(cudaMalloc(&G.lev_g, g.size() * sizeof(float)));
+        MZB_CHECK(cudaMemcpy(G.lev_g, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
 }
 
@@ -253,11 +266,12 @@ int run_mixed(System& s, int prog, double cst) {
     m.tol = G.mixed_tol > 0 ? G.mixed_tol : G.tol;
     m.c = cst;
     m.max_outer = 100;
-    m.cycles = 1;
     m.nu1 = 2;
     m.nu2 = 2;
-    m.coarse_sweeps = 40;
+    m.coarse_sweeps = 16;
     m.nlev = G.nlev;
+    m.lsmall = mixed_small_level(G.nlev, G.lev_n);
+    m.coarse_g = G.lev_g;
     for (int l = 0; l < G.nlev; l++) {
         m.lev_n[l] = G.lev_n[l];
         m.lev_x[l] = G.lev_x[l];
@@ -273,9 +287,34 @@ int run_mixed(System& s, int prog, double cst) {
     m.partials = s.partials;
     m.bar = s.bar;
     m.result = s.result;
+    // MZB_PHASE_TIMING=1: time-stamp the phases of each refinement step and print them
+    static const bool stamps_on = getenv("MZB_PHASE_TIMING") != nullptr;
+    static unsigned long long* stamps_d = nullptr;
+    if (stamps_on) {
+        if (!stamps_d) MZB_CHECK(cudaMalloc(&stamps_d, sizeof(unsigned long long) * kMixedStampSlots));
+        MZB_CHECK(cudaMemsetAsync(stamps_d, 0, sizeof(unsigned long long) * kMixedStampSlots, s.stream));
+        m.stamps = stamps_d;
+    }
     MZB_CHECK(cudaEventRecord(s.ev0, s.stream));
     mixed_launch(m, s.stream);
     MZB_CHECK(cudaEventRecord(s.ev1, s.stream));
+    if (stamps_on) {
+        unsigned long long h[kMixedStampSlots];
+        MZB_CHECK(cudaMemcpyAsync(h, stamps_d, sizeof(h), cudaMemcpyDeviceToHost, s.stream));
+        MZB_CHECK(cudaStreamSynchronize(s.stream));
+        fprintf(stderr, "[mixed phases us] setup %.2f |", (h[1] - h[0]) * 1e-3);
+        for (int o = 0; o < 8; o++) {
+            const unsigned long long* t = h + 2 + 8 * o;
+            if (!t[0] || !t[1]) break;
+            double rmax;
+            memcpy(&rmax, &t[7], sizeof(double));
+            fprintf(stderr, " r=%.2e resid %.2f", rmax, (t[1] - t[0]) * 1e-3);
+            if (!t[6]) break;
+            fprintf(stderr, " down %.2f small %.2f up %.2f esum %.2f upd %.2f |", (t[2] - t[1]) * 1e-3,
+                    (t[3] - t[2]) * 1e-3, (t[4] - t[3]) * 1e-3, (t[5] - t[4]) * 1e-3, (t[6] - t[5]) * 1e-3);
+        }
+        fprintf(stderr, "\n");
+    }
     MZB_CHECK(cudaMemcpyAsync(s.result_h, s.result, 2 * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
     MZB_CHECK(cudaStreamSynchronize(s.stream));
     MZB_CHECK(cudaEventElapsedTime(&s.last_solve_ms, s.ev0, s.ev1));

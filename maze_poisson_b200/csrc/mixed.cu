@@ -10,14 +10,20 @@
 //           e = V-cycle(r)         (FP32: red-black GS V(nu1,nu2), 27-point full
 //                                   weighting scaled by 4 = (2h/h)^2 for the unscaled
 //                                   Laplacian, trilinear prolongation, levels down to
-//                                   4^3, coarse levels <= 32^3 worked by one CTA)
+//                                   4^3)
 //           x += e - mean(e)       (FP64; the periodic Laplacian's null space is the
 //                                   constants, and dropping e's mean keeps x's mean
 //                                   where it started, as CG does)
 //
-// Each V-cycle moves ~10 FP64-equivalent passes of the fine grid instead of the ~10 per
-// CG iteration of the reference's solver, and a warm-started MD step needs a few cycles
-// where CG needs hundreds of iterations.
+// Work placement. Levels with n > 16 are swept by every CTA with a grid barrier between
+// passes. Levels with n <= 16 (at most 3 x 4 x (16^3 + 8^3 + 4^3) B = 55 KB) are loaded
+// into CTA 0's shared memory and worked there while the other CTAs wait at the next grid
+// barrier; a coarsest level of at most 6^3 points is solved exactly by a convolution with
+// its Green's function instead of by sweeps. Every V-cycle starts a level from
+// x = 0, so the first red half-sweep (x_red = -b/6, no neighbour reads) is folded into the
+// pass that writes the level's right-hand side (the FP64 residual pass, the
+// restrictions), and the sum of the finest correction, whose mean is removed, is taken in
+// the last two half-sweeps instead of by another pass.
 #include "engine.cuh"
 #include "mixed.cuh"
 #include "tma.cuh"
@@ -26,21 +32,23 @@ namespace mzb {
 namespace {
 
 constexpr int kThreads = 1024;
-constexpr int kSmallN = 32;  // levels with n <= kSmallN are worked by CTA 0 alone
 
-// warp-per-row point loops over an n^3 grid, either over the whole grid (all CTAs) or
-// inside CTA 0 only (small levels)
+__device__ __forceinline__ void stamp(const MixedArgs& a, int slot) {
+    if (a.stamps != nullptr && blockIdx.x == 0 && threadIdx.x == 0 && slot < kMixedStampSlots)
+        a.stamps[slot] = global_ns();
+}
+__device__ __forceinline__ void stamp_outer(const MixedArgs& a, int outer, int k) {
+    if (outer < 8) stamp(a, 2 + 8 * outer + k);
+}
+
+// ---- loops ----
+
+// whole-grid loops (all CTAs): a warp per row of k
 template <class F>
-__device__ __forceinline__ void for_pts(bool single, int n, F&& f) {
+__device__ __forceinline__ void grid_pts(int n, F&& f) {
     const int lane = threadIdx.x & 31;
-    long gw, nw;
-    if (single) {
-        gw = threadIdx.x >> 5;
-        nw = blockDim.x >> 5;
-    } else {
-        gw = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-        nw = (long)gridDim.x * (blockDim.x >> 5);
-    }
+    const long gw = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const long nw = (long)gridDim.x * (blockDim.x >> 5);
     const long rows = (long)n * n;
     for (long row = gw; row < rows; row += nw) {
         const int i = (int)(row / n), j = (int)(row - (long)i * n);
@@ -48,20 +56,32 @@ __device__ __forceinline__ void for_pts(bool single, int n, F&& f) {
     }
 }
 template <class F>
-__device__ __forceinline__ void for_col(bool single, int n, int colour, F&& f) {
+__device__ __forceinline__ void grid_col(int n, int colour, F&& f) {
     const int lane = threadIdx.x & 31;
-    long gw, nw;
-    if (single) {
-        gw = threadIdx.x >> 5;
-        nw = blockDim.x >> 5;
-    } else {
-        gw = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-        nw = (long)gridDim.x * (blockDim.x >> 5);
-    }
+    const long gw = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const long nw = (long)gridDim.x * (blockDim.x >> 5);
     const long rows = (long)n * n;
     for (long row = gw; row < rows; row += nw) {
         const int i = (int)(row / n), j = (int)(row - (long)i * n);
         for (int k = ((i + j + colour) & 1) + 2 * lane; k < n; k += 64) f(i, j, k);
+    }
+}
+
+// CTA-0 loops (shared-memory levels): a thread per point
+template <class F>
+__device__ __forceinline__ void cta_pts(int n, F&& f) {
+    const int n2 = n * n, tot = n2 * n;
+    for (int p = threadIdx.x; p < tot; p += blockDim.x) {
+        const int i = p / n2, rem = p - i * n2, j = rem / n;
+        f(i, j, rem - j * n);
+    }
+}
+template <class F>
+__device__ __forceinline__ void cta_col(int n, int colour, F&& f) {
+    const int h = n >> 1, hn = h * n, tot = hn * n;
+    for (int p = threadIdx.x; p < tot; p += blockDim.x) {
+        const int i = p / hn, rem = p - i * hn, j = rem / h, kk = rem - j * h;
+        f(i, j, 2 * kk + ((i + j + colour) & 1));
     }
 }
 
@@ -79,15 +99,6 @@ __device__ __forceinline__ Nb nb_of(int n, int i, int j, int k) {
     o.kp = o.c + (k + 1 == n ? -(long)(n - 1) : 1L);
     o.km = o.c + (k == 0 ? (long)(n - 1) : -1L);
     return o;
-}
-
-// block-level barrier for single-CTA work, grid barrier otherwise
-__device__ __forceinline__ bool sync_level(bool single, GridBarrier* bar, unsigned& epoch) {
-    if (single) {
-        __syncthreads();
-        return true;
-    }
-    return grid_sync_mono(bar, epoch);
 }
 
 // Grid reduction of one sum and one max (deterministic fixed-order gather).
@@ -135,147 +146,236 @@ __device__ bool reduce_sum_max(double& s, double& mx, const MixedArgs& a, unsign
     return ok;
 }
 
-// ---- FP32 multigrid pieces ----
+// ---- FP32 multigrid point operations (pointers may be global or shared) ----
 
-__device__ void rbgs32(bool single, int n, const float* b, float* x, int colour) {
-    for_col(single, n, colour, [&](int i, int j, int k) {
-        const Nb o = nb_of(n, i, j, k);
-        float s = x[o.im] + x[o.ip];
-        s += x[o.jm];
-        s += x[o.jp];
-        s += x[o.km];
-        s += x[o.kp];
-        x[o.c] = (b[o.c] - s) * (-1.0f / 6.0f);
-    });
+// red-black Gauss-Seidel update of one point; returns the new value
+__device__ __forceinline__ float gs_point(int n, const float* b, float* x, int i, int j, int k) {
+    const Nb o = nb_of(n, i, j, k);
+    float s = x[o.im] + x[o.ip];
+    s += x[o.jm];
+    s += x[o.jp];
+    s += x[o.km];
+    s += x[o.kp];
+    const float v = (b[o.c] - s) * (-1.0f / 6.0f);
+    x[o.c] = v;
+    return v;
 }
 
-__device__ void resid32(bool single, int n, const float* b, const float* x, float* r) {
-    for_pts(single, n, [&](int i, int j, int k) {
-        const Nb o = nb_of(n, i, j, k);
-        float s = x[o.ip] + x[o.im];
-        s += x[o.jp];
-        s += x[o.jm];
-        s += x[o.kp];
-        s += x[o.km];
-        r[o.c] = b[o.c] - (s - 6.0f * x[o.c]);
-    });
+__device__ __forceinline__ void resid_point(int n, const float* b, const float* x, float* r, int i, int j, int k) {
+    const Nb o = nb_of(n, i, j, k);
+    float s = x[o.ip] + x[o.im];
+    s += x[o.jp];
+    s += x[o.jm];
+    s += x[o.kp];
+    s += x[o.km];
+    r[o.c] = b[o.c] - (s - 6.0f * x[o.c]);
 }
 
-// coarse b = 4 * R27(r), coarse x = 0
-__device__ void restrict32(bool single, int n, const float* r, float* bc, float* xc) {
+// Coarse point (I,J,K) of bc = 4 * R27(r) with its first red half-sweep from x = 0:
+// xc = -bc/6 on red (I+J+K even) points, 0 on black ones.
+__device__ __forceinline__ void restrict_point(int n, const float* r, float* bc, float* xc, int I, int J, int K) {
     const int nc = n / 2;
     const long n2 = (long)n * n;
-    for_pts(single, nc, [&](int I, int J, int K) {
-        const int i = 2 * I, j = 2 * J, k = 2 * K;
-        const long i0 = (long)i * n2, i1 = (long)(i + 1 == n ? 0 : i + 1) * n2, i2 = (long)(i == 0 ? n - 1 : i - 1) * n2;
-        const long j0 = (long)j * n, j1 = (long)(j + 1 == n ? 0 : j + 1) * n, j2 = (long)(j == 0 ? n - 1 : j - 1) * n;
-        const long k0 = k, k1 = (k + 1 == n ? 0 : k + 1), k2 = (k == 0 ? n - 1 : k - 1);
-        const float f = r[i2 + j0 + k0] + r[i1 + j0 + k0] + r[i0 + j2 + k0] + r[i0 + j1 + k0] + r[i0 + j0 + k2] +
-                        r[i0 + j0 + k1];
-        const float e = r[i1 + j0 + k2] + r[i1 + j0 + k1] + r[i2 + j0 + k2] + r[i2 + j0 + k1] + r[i1 + j2 + k0] +
-                        r[i1 + j1 + k0] + r[i2 + j2 + k0] + r[i2 + j1 + k0] + r[i0 + j2 + k2] + r[i0 + j2 + k1] +
-                        r[i0 + j1 + k2] + r[i0 + j1 + k1];
-        const float c = r[i1 + j1 + k2] + r[i1 + j1 + k1] + r[i1 + j2 + k2] + r[i1 + j2 + k1] + r[i2 + j1 + k2] +
-                        r[i2 + j1 + k1] + r[i2 + j2 + k2] + r[i2 + j2 + k1];
-        const long cc = ((long)I * nc + J) * nc + K;
-        bc[cc] = (8.0f * r[i0 + j0 + k0] + 4.0f * f + 2.0f * e + c) * (4.0f / 64.0f);
-        xc[cc] = 0.0f;
-    });
+    const int i = 2 * I, j = 2 * J, k = 2 * K;
+    const long i0 = (long)i * n2, i1 = (long)(i + 1 == n ? 0 : i + 1) * n2, i2 = (long)(i == 0 ? n - 1 : i - 1) * n2;
+    const long j0 = (long)j * n, j1 = (long)(j + 1 == n ? 0 : j + 1) * n, j2 = (long)(j == 0 ? n - 1 : j - 1) * n;
+    const long k0 = k, k1 = (k + 1 == n ? 0 : k + 1), k2 = (k == 0 ? n - 1 : k - 1);
+    const float f = r[i2 + j0 + k0] + r[i1 + j0 + k0] + r[i0 + j2 + k0] + r[i0 + j1 + k0] + r[i0 + j0 + k2] +
+                    r[i0 + j0 + k1];
+    const float e = r[i1 + j0 + k2] + r[i1 + j0 + k1] + r[i2 + j0 + k2] + r[i2 + j0 + k1] + r[i1 + j2 + k0] +
+                    r[i1 + j1 + k0] + r[i2 + j2 + k0] + r[i2 + j1 + k0] + r[i0 + j2 + k2] + r[i0 + j2 + k1] +
+                    r[i0 + j1 + k2] + r[i0 + j1 + k1];
+    const float c = r[i1 + j1 + k2] + r[i1 + j1 + k1] + r[i1 + j2 + k2] + r[i1 + j2 + k1] + r[i2 + j1 + k2] +
+                    r[i2 + j1 + k1] + r[i2 + j2 + k2] + r[i2 + j2 + k1];
+    const long cc = ((long)I * nc + J) * nc + K;
+    const float bv = (8.0f * r[i0 + j0 + k0] + 4.0f * f + 2.0f * e + c) * (4.0f / 64.0f);
+    bc[cc] = bv;
+    xc[cc] = ((I + J + K) & 1) == 0 ? bv * (-1.0f / 6.0f) : 0.0f;
 }
 
-// fine x += P(coarse x), trilinear
-__device__ void prolong32(bool single, int n, const float* xc, float* x) {
+// fine x += P(coarse x) at (i,j,k), trilinear
+__device__ __forceinline__ void prolong_point(int n, const float* xc, float* x, int i, int j, int k) {
     const int nc = n / 2;
     const long n2c = (long)nc * nc;
-    for_pts(single, n, [&](int i, int j, int k) {
-        const int ci = i >> 1, cj = j >> 1, ck = k >> 1;
-        const long i0 = (long)ci * n2c, i1 = (long)(ci + 1 == nc ? 0 : ci + 1) * n2c;
-        const long j0 = (long)cj * nc, j1 = (long)(cj + 1 == nc ? 0 : cj + 1) * nc;
-        const long k0 = ck, k1 = (ck + 1 == nc ? 0 : ck + 1);
-        const float wi = (i & 1) ? 0.5f : 0.0f, wj = (j & 1) ? 0.5f : 0.0f, wk = (k & 1) ? 0.5f : 0.0f;
-        const float a00 = xc[i0 + j0 + k0] * (1.0f - wk) + xc[i0 + j0 + k1] * wk;
-        const float a01 = xc[i0 + j1 + k0] * (1.0f - wk) + xc[i0 + j1 + k1] * wk;
-        const float a10 = xc[i1 + j0 + k0] * (1.0f - wk) + xc[i1 + j0 + k1] * wk;
-        const float a11 = xc[i1 + j1 + k0] * (1.0f - wk) + xc[i1 + j1 + k1] * wk;
-        const float b0 = a00 * (1.0f - wj) + a01 * wj, b1 = a10 * (1.0f - wj) + a11 * wj;
-        x[((long)i * n + j) * n + k] += b0 * (1.0f - wi) + b1 * wi;
-    });
+    const int ci = i >> 1, cj = j >> 1, ck = k >> 1;
+    const long i0 = (long)ci * n2c, i1 = (long)(ci + 1 == nc ? 0 : ci + 1) * n2c;
+    const long j0 = (long)cj * nc, j1 = (long)(cj + 1 == nc ? 0 : cj + 1) * nc;
+    const long k0 = ck, k1 = (ck + 1 == nc ? 0 : ck + 1);
+    const float wi = (i & 1) ? 0.5f : 0.0f, wj = (j & 1) ? 0.5f : 0.0f, wk = (k & 1) ? 0.5f : 0.0f;
+    const float a00 = xc[i0 + j0 + k0] * (1.0f - wk) + xc[i0 + j0 + k1] * wk;
+    const float a01 = xc[i0 + j1 + k0] * (1.0f - wk) + xc[i0 + j1 + k1] * wk;
+    const float a10 = xc[i1 + j0 + k0] * (1.0f - wk) + xc[i1 + j0 + k1] * wk;
+    const float a11 = xc[i1 + j1 + k0] * (1.0f - wk) + xc[i1 + j1 + k1] * wk;
+    const float b0 = a00 * (1.0f - wj) + a01 * wj, b1 = a10 * (1.0f - wj) + a11 * wj;
+    x[((long)i * n + j) * n + k] += b0 * (1.0f - wi) + b1 * wi;
 }
 
-// One V-cycle: x[0] improved in place for rhs b[0]. Levels with n > kSmallN use all
-// CTAs with grid barriers between sweeps; the smaller ones, and the coarsest solve, run
-// in CTA 0 with block barriers while the other CTAs wait at the next grid barrier.
-__device__ bool vcycle32(const MixedArgs& a, unsigned& epoch) {
-    const int L = a.nlev;
-    int lsmall = L;
-    for (int l = 0; l < L; l++)
-        if (a.lev_n[l] <= kSmallN) {
-            lsmall = l;
-            break;
+// ---- the shared-memory part of the V-cycle (CTA 0) ----
+//
+// Shared memory holds x, b, r of levels lsmall..nlev-1 back to back, then (when the
+// coarsest level is solved directly) the coarsest level's Green's function.
+__device__ __forceinline__ float* small_arr(const MixedArgs& a, float* sm, int m, int which) {
+    int off = 0;
+    for (int l = a.lsmall; l < m; l++) off += 3 * a.lev_n[l] * a.lev_n[l] * a.lev_n[l];
+    return sm + off + which * a.lev_n[m] * a.lev_n[m] * a.lev_n[m];
+}
+
+// Coarsest level solved exactly: x = G * b (circular convolution with the pseudo-inverse
+// of the unscaled periodic 7-point Laplacian, precomputed on the host), i.e. the
+// zero-mean solution of L x = b - mean(b). S lanes share one output point.
+__device__ void coarse_direct(int n, const float* g, const float* b, float* x) {
+    const int N = n * n * n;
+    int S = 1;
+    while (S < 32 && 2 * S * N <= (int)blockDim.x) S *= 2;
+    const int p = threadIdx.x / S, sub = threadIdx.x % S;
+    float acc = 0.0f;
+    if (p < N) {
+        const int pi = p / (n * n), pj = (p / n) % n, pk = p % n;
+        for (int q = sub; q < N; q += S) {
+            const int qi = q / (n * n), qj = (q / n) % n, qk = q % n;
+            const int d = (((pi - qi + n) % n) * n + ((pj - qj + n) % n)) * n + ((pk - qk + n) % n);
+            acc += g[d] * b[q];
         }
-    const int lbig = lsmall < L - 1 ? lsmall : L - 1;  // big levels below the coarsest
-    auto smooth = [&](bool single, int l, int sweeps) -> bool {
-        for (int s = 0; s < sweeps; s++)
-            for (int c = 0; c < 2; c++) {
-                rbgs32(single, a.lev_n[l], a.lev_b[l], a.lev_x[l], c);
-                if (!sync_level(single, a.bar, epoch)) return false;
-            }
-        return true;
+    }
+    for (int o = S >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (p < N && sub == 0) x[p] = acc;
+}
+
+// Restricts the residual of level lsmall-1 (global) into shared memory, runs the rest of
+// the V-cycle there and writes level lsmall's correction back to lev_x[lsmall].
+__device__ void small_vcycle(const MixedArgs& a, float* sm) {
+    const int L = a.nlev, ls = a.lsmall;
+    auto smooth = [&](int m, int first_colour, int half_sweeps) {
+        const int n = a.lev_n[m];
+        float* x = small_arr(a, sm, m, 0);
+        const float* b = small_arr(a, sm, m, 1);
+        for (int h = 0; h < half_sweeps; h++) {
+            cta_col(n, (first_colour + h) & 1, [&](int i, int j, int k) { gs_point(n, b, x, i, j, k); });
+            __syncthreads();
+        }
     };
-    for (int l = 0; l < lbig; l++) {
-        if (!smooth(false, l, a.nu1)) return false;
-        resid32(false, a.lev_n[l], a.lev_b[l], a.lev_x[l], a.lev_r[l]);
-        if (!grid_sync_mono(a.bar, epoch)) return false;
-        restrict32(false, a.lev_n[l], a.lev_r[l], a.lev_b[l + 1], a.lev_x[l + 1]);
+    float* gsm = small_arr(a, sm, L, 0);  // just past the last level
+    if (a.coarse_g != nullptr) {
+        const int N = a.lev_n[L - 1] * a.lev_n[L - 1] * a.lev_n[L - 1];
+        for (int p = threadIdx.x; p < N; p += blockDim.x) gsm[p] = a.coarse_g[p];
+    }
+    {
+        const float* r = a.lev_r[ls - 1];
+        const int nf = a.lev_n[ls - 1];
+        float* bs = small_arr(a, sm, ls, 1);
+        float* xs = small_arr(a, sm, ls, 0);
+        cta_pts(a.lev_n[ls], [&](int I, int J, int K) { restrict_point(nf, r, bs, xs, I, J, K); });
+        __syncthreads();
+    }
+    for (int m = ls; m < L - 1; m++) {
+        const int n = a.lev_n[m];
+        smooth(m, 1, 2 * a.nu1 - 1);
+        float* x = small_arr(a, sm, m, 0);
+        float* b = small_arr(a, sm, m, 1);
+        float* r = small_arr(a, sm, m, 2);
+        cta_pts(n, [&](int i, int j, int k) { resid_point(n, b, x, r, i, j, k); });
+        __syncthreads();
+        float* bc = small_arr(a, sm, m + 1, 1);
+        float* xc = small_arr(a, sm, m + 1, 0);
+        cta_pts(a.lev_n[m + 1], [&](int I, int J, int K) { restrict_point(n, r, bc, xc, I, J, K); });
+        __syncthreads();
+    }
+    if (a.coarse_g != nullptr) {
+        coarse_direct(a.lev_n[L - 1], gsm, small_arr(a, sm, L - 1, 1), small_arr(a, sm, L - 1, 0));
+        __syncthreads();
+    } else {
+        smooth(L - 1, 1, 2 * a.coarse_sweeps - 1);
+    }
+    for (int m = L - 2; m >= ls; m--) {
+        const int n = a.lev_n[m];
+        const float* xc = small_arr(a, sm, m + 1, 0);
+        float* x = small_arr(a, sm, m, 0);
+        cta_pts(n, [&](int i, int j, int k) { prolong_point(n, xc, x, i, j, k); });
+        __syncthreads();
+        smooth(m, 0, 2 * a.nu2);
+    }
+    const int v = a.lev_n[ls] * a.lev_n[ls] * a.lev_n[ls];
+    const float* xs = small_arr(a, sm, ls, 0);
+    float* dst = a.lev_x[ls];
+    for (int p = threadIdx.x; p < v; p += blockDim.x) dst[p] = xs[p];
+}
+
+// Grid-wide red-black sweeps of level l: `half_sweeps` colours starting at first_colour,
+// a grid barrier after each except (when skip_last_barrier) the last. When esum is not
+// null the values written in the last two half-sweeps are summed into it.
+__device__ bool grid_smooth(const MixedArgs& a, int l, float* x, int first_colour, int half_sweeps, unsigned& epoch,
+                            double* esum, bool skip_last_barrier) {
+    const int n = a.lev_n[l];
+    const float* b = a.lev_b[l];
+    for (int h = 0; h < half_sweeps; h++) {
+        const bool acc = esum != nullptr && h >= half_sweeps - 2;
+        double s = 0.0;
+        grid_col(n, (first_colour + h) & 1, [&](int i, int j, int k) {
+            const float v = gs_point(n, b, x, i, j, k);
+            if (acc) s += (double)v;
+        });
+        if (acc) *esum += s;
+        if (h == half_sweeps - 1 && skip_last_barrier) break;
         if (!grid_sync_mono(a.bar, epoch)) return false;
     }
-    if (lsmall < L) {
-        if (blockIdx.x == 0) {
-            for (int m = lsmall; m < L - 1; m++) {
-                smooth(true, m, a.nu1);
-                resid32(true, a.lev_n[m], a.lev_b[m], a.lev_x[m], a.lev_r[m]);
-                __syncthreads();
-                restrict32(true, a.lev_n[m], a.lev_r[m], a.lev_b[m + 1], a.lev_x[m + 1]);
-                __syncthreads();
-            }
-            smooth(true, L - 1, a.coarse_sweeps);
-            for (int m = L - 2; m >= lsmall; m--) {
-                prolong32(true, a.lev_n[m], a.lev_x[m + 1], a.lev_x[m]);
-                __syncthreads();
-                smooth(true, m, a.nu2);
-            }
+    return true;
+}
+
+// One V-cycle for the correction e = lev_x[0] of rhs lev_b[0], whose first red half-sweep
+// has been done by the residual pass. Ends after the last half-sweep of level 0 without a
+// barrier, with this thread's share of sum(e) in esum.
+__device__ bool vcycle(const MixedArgs& a, float* sm, unsigned& epoch, double& esum, int outer) {
+    const int L = a.nlev, ls = a.lsmall;
+    const int lg = ls < L ? ls : L - 1;  // levels 0..lg-1 are smoothed and restricted on the grid
+    for (int l = 0; l < lg; l++) {
+        if (!grid_smooth(a, l, a.lev_x[l], 1, 2 * a.nu1 - 1, epoch, nullptr, false)) return false;
+        grid_pts(a.lev_n[l],
+                 [&](int i, int j, int k) { resid_point(a.lev_n[l], a.lev_b[l], a.lev_x[l], a.lev_r[l], i, j, k); });
+        if (!grid_sync_mono(a.bar, epoch)) return false;
+        if (l + 1 < ls) {
+            grid_pts(a.lev_n[l + 1], [&](int I, int J, int K) {
+                restrict_point(a.lev_n[l], a.lev_r[l], a.lev_b[l + 1], a.lev_x[l + 1], I, J, K);
+            });
+            if (!grid_sync_mono(a.bar, epoch)) return false;
         }
+    }
+    stamp_outer(a, outer, 2);
+    if (ls < L) {
+        if (blockIdx.x == 0) small_vcycle(a, sm);
         if (!grid_sync_mono(a.bar, epoch)) return false;
     } else {
-        if (!smooth(false, L - 1, a.coarse_sweeps)) return false;
+        if (!grid_smooth(a, L - 1, a.lev_x[L - 1], 1, 2 * a.coarse_sweeps - 1, epoch, nullptr, false)) return false;
     }
-    for (int l = lbig - 1; l >= 0; l--) {
-        prolong32(false, a.lev_n[l], a.lev_x[l + 1], a.lev_x[l]);
+    stamp_outer(a, outer, 3);
+    for (int l = lg - 1; l >= 0; l--) {
+        grid_pts(a.lev_n[l], [&](int i, int j, int k) { prolong_point(a.lev_n[l], a.lev_x[l + 1], a.lev_x[l], i, j, k); });
         if (!grid_sync_mono(a.bar, epoch)) return false;
-        if (!smooth(false, l, a.nu2)) return false;
+        if (!grid_smooth(a, l, a.lev_x[l], 0, 2 * a.nu2, epoch, l == 0 ? &esum : nullptr, l == 0)) return false;
     }
     return true;
 }
 
 __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
+    extern __shared__ float sm[];
     const int n = a.n;
     unsigned epoch = 0;
     int seq = 0;
     bool ok = true;
     int result = -1;
+    stamp(a, 0);
 
     // ---- set-up: right-hand side B and solution X (FP64), as the FP64 programs ----
     double* X = a.phi_new;
     const double* B = a.tmp;
     if (a.prog == PROG_INIT_FIELD) {         // y = 0, phi = 0 start, b = c q
-        for_pts(false, n, [&](int i, int j, int k) {
+        grid_pts(n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             a.y[c] = 0.0;
             a.phi_new[c] = 0.0;
             a.tmp[c] = a.q[c] * a.c;
         });
     } else if (a.prog == PROG_LCG_UPDATE) {  // y = c q; start from phi_prev (old phi)
-        for_pts(false, n, [&](int i, int j, int k) {
+        grid_pts(n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             const double bq = a.q[c] * a.c;
             a.y[c] = bq;
@@ -283,14 +383,14 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
             a.phi_new[c] = a.phi_old[c];
         });
     } else if (a.prog == PROG_MG_UPDATE) {   // phi = 2 phi - phi_prev (start), b = c q
-        for_pts(false, n, [&](int i, int j, int k) {
+        grid_pts(n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             a.phi_new[c] = 2 * a.phi_old[c] - a.phi_prev[c];
             a.tmp[c] = a.q[c] * a.c;
         });
     } else {                                 // MaZe: phi = 2 phi - phi_prev; sigma = L phi + c q
         X = a.y;
-        for_pts(false, n, [&](int i, int j, int k) {
+        grid_pts(n, [&](int i, int j, int k) {
             const Nb o = nb_of(n, i, j, k);
             auto ex = [&](long q) { return 2 * a.phi_old[q] - a.phi_prev[q]; };
             double s = ex(o.ip) + ex(o.im);
@@ -303,14 +403,17 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
         });
     }
     ok = grid_sync_mono(a.bar, epoch);
+    stamp(a, 1);
 
     float* e = a.lev_x[0];
     float* rb = a.lev_b[0];
     int outer = 0;
     while (ok) {
-        // r = B - L X in FP64 -> FP32 rhs of the inner solve; |r|_inf
+        // r = B - L X in FP64 -> FP32 rhs of the inner solve, with the correction's first
+        // red half-sweep from e = 0; |r|_inf
+        stamp_outer(a, outer, 0);
         double s0 = 0.0, rmax = 0.0;
-        for_pts(false, n, [&](int i, int j, int k) {
+        grid_pts(n, [&](int i, int j, int k) {
             const Nb o = nb_of(n, i, j, k);
             double s = X[o.ip] + X[o.im];
             s = s + X[o.jp];
@@ -318,37 +421,40 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
             s = s + X[o.kp];
             s = s + X[o.km];
             const double r = B[o.c] - (s - X[o.c] * 6.0);
-            rb[o.c] = (float)r;
-            e[o.c] = 0.0f;
+            const float rf = (float)r;
+            rb[o.c] = rf;
+            e[o.c] = ((i + j + k) & 1) == 0 ? rf * (-1.0f / 6.0f) : 0.0f;
             rmax = fmax(rmax, fabs(r));
         });
         ok = reduce_sum_max(s0, rmax, a, epoch, seq);
+        stamp_outer(a, outer, 1);
+        if (a.stamps != nullptr && outer < 8 && blockIdx.x == 0 && threadIdx.x == 0)
+            a.stamps[2 + 8 * outer + 7] = (unsigned long long)__double_as_longlong(rmax);
         if (!ok) break;
         if (rmax <= a.tol) {
             result = outer;
             break;
         }
         if (outer >= a.max_outer) break;
-        for (int c = 0; c < a.cycles; c++) {
-            ok = vcycle32(a, epoch);
-            if (!ok) break;
-        }
-        if (!ok) break;
-        // mean of the correction (the periodic Laplacian's null space)
         double esum = 0.0, m0 = 0.0;
-        for_pts(false, n, [&](int i, int j, int k) { esum += (double)e[((long)i * n + j) * n + k]; });
+        ok = vcycle(a, sm, epoch, esum, outer);
+        if (!ok) break;
+        stamp_outer(a, outer, 4);
+        // mean of the correction (the periodic Laplacian's null space)
         ok = reduce_sum_max(esum, m0, a, epoch, seq);
         if (!ok) break;
+        stamp_outer(a, outer, 5);
         const double emean = esum / ((double)n * n * n);
-        for_pts(false, n, [&](int i, int j, int k) {
+        grid_pts(n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             X[c] = X[c] + ((double)e[c] - emean);
         });
         ok = grid_sync_mono(a.bar, epoch);
+        stamp_outer(a, outer, 6);
         outer++;
     }
     if (ok && (a.prog == PROG_MAZE_LCG || a.prog == PROG_MAZE_MG)) {  // phi -= y
-        for_pts(false, n, [&](int i, int j, int k) {
+        grid_pts(n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             a.phi_new[c] = a.phi_new[c] + -1.0 * a.y[c];
         });
@@ -361,6 +467,14 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
 
 int g_mixed_device = -1;
 int g_mixed_blocks = 0;
+size_t g_mixed_smem_set = 0;
+
+size_t small_smem_bytes(const MixedArgs& a) {
+    size_t v = 0;
+    for (int m = a.lsmall; m < a.nlev; m++) v += 3 * (size_t)a.lev_n[m] * a.lev_n[m] * a.lev_n[m];
+    if (a.coarse_g != nullptr) v += (size_t)a.lev_n[a.nlev - 1] * a.lev_n[a.nlev - 1] * a.lev_n[a.nlev - 1];
+    return v * sizeof(float);
+}
 
 }  // namespace
 
@@ -375,23 +489,50 @@ int mixed_levels(int n, int* sizes) {
     return L;
 }
 
+void mixed_coarse_green(int n, float* g) {
+    const int N = n * n * n;
+    const double w = 2.0 * 3.14159265358979323846 / n;
+    for (int d = 0; d < N; d++) {
+        const int di = d / (n * n), dj = (d / n) % n, dk = d % n;
+        double s = 0.0;
+        for (int k = 1; k < N; k++) {
+            const int ki = k / (n * n), kj = (k / n) % n, kk = k % n;
+            const double lam = 2 * cos(w * ki) + 2 * cos(w * kj) + 2 * cos(w * kk) - 6.0;
+            s += cos(w * (ki * di + kj * dj + kk * dk)) / lam;
+        }
+        g[d] = (float)(s / N);
+    }
+}
+
+int mixed_small_level(int nlev, const int* sizes) {
+    for (int l = 0; l < nlev; l++)
+        if (sizes[l] <= kMixedSmallN) return l;
+    return nlev;
+}
+
 void mixed_launch(const MixedArgs& a, cudaStream_t stream) {
+    if (a.lsmall < 1 || a.lsmall > a.nlev || a.nlev < 2 || a.nu1 < 1 || a.nu2 < 1 || a.coarse_sweeps < 1)
+        fatal("mixed solver: invalid level plan");
+    const size_t smem = small_smem_bytes(a);
     int dev;
     MZB_CHECK(cudaGetDevice(&dev));
-    if (g_mixed_device != dev) {
+    if (g_mixed_device != dev || smem > g_mixed_smem_set) {
         int sms = 0, per_sm = 0;
+        if (smem > 48 * 1024)
+            MZB_CHECK(cudaFuncSetAttribute(mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         MZB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        MZB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_kernel, kThreads, 0));
+        MZB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_kernel, kThreads, smem));
         if (per_sm < 1) fatal("mixed solver: kernel cannot be resident on this device");
         g_mixed_device = dev;
         g_mixed_blocks = sms;
+        g_mixed_smem_set = smem > g_mixed_smem_set ? smem : g_mixed_smem_set;
     }
     MZB_CHECK(cudaMemsetAsync(a.bar, 0, sizeof(GridBarrier), stream));
     MixedArgs copy = a;
     void* params[] = {&copy};
     count_launch();
     MZB_CHECK(cudaLaunchCooperativeKernel((const void*)mixed_kernel, dim3(g_mixed_blocks), dim3(kThreads), params,
-                                          0, stream));
+                                          smem, stream));
 }
 
 }  // namespace mzb

@@ -6,6 +6,8 @@
 namespace mzb {
 
 constexpr int kMixedMaxLevels = 10;
+constexpr int kMixedSmallN = 16;     // levels with n <= this live in CTA 0's shared memory
+constexpr int kMixedStampSlots = 2 + 8 * 8;
 
 struct MixedArgs {
     int prog;           // PROG_INIT_FIELD, PROG_LCG_UPDATE, PROG_MAZE_LCG, PROG_MG_UPDATE, PROG_MAZE_MG
@@ -13,10 +15,11 @@ struct MixedArgs {
     double tol;         // absolute inf-norm tolerance on the FP64 residual
     double c;           // right-hand-side constant (as the FP64 programs)
     int max_outer;      // refinement steps before giving up (-1 returned)
-    int cycles;         // V-cycles per refinement step
-    int nu1, nu2;       // red-black GS sweeps before / after the coarse correction
-    int coarse_sweeps;  // sweeps on the coarsest level
+    int nu1, nu2;       // red-black GS sweeps before / after the coarse correction (>= 1)
+    int coarse_sweeps;  // sweeps on the coarsest level (>= 1) when coarse_g is null
+    const float* coarse_g;  // Green's function of the coarsest level (mixed_coarse_green) or null
     int nlev;
+    int lsmall;         // first level held in shared memory (nlev if none; >= 1)
     int lev_n[kMixedMaxLevels];
     float* lev_x[kMixedMaxLevels];
     float* lev_b[kMixedMaxLevels];
@@ -30,10 +33,19 @@ struct MixedArgs {
     double* partials;   // >= 4 x gridDim.x doubles
     GridBarrier* bar;
     int* result;        // [0] refinement steps taken or -1, [1] status (0 ok)
+    unsigned long long* stamps;  // optional phase time stamps (kMixedStampSlots) or null
 };
 
 // Level sizes n, n/2, ... while the next size is even and >= 4; returns the count.
 int mixed_levels(int n, int* sizes);
+// First level with n <= kMixedSmallN (nlev if none).
+int mixed_small_level(int nlev, const int* sizes);
+// Largest coarsest level solved directly (n^3 values of its Green's function).
+constexpr int kMixedDirectN = 6;
+// Pseudo-inverse kernel of the unscaled periodic 7-point Laplacian on an n^3 grid:
+// g[d] = (1/n^3) sum_{k != 0} cos(2 pi k.d / n) / lambda(k),
+// lambda(k) = 2 cos(2 pi k1/n) + 2 cos(2 pi k2/n) + 2 cos(2 pi k3/n) - 6.
+void mixed_coarse_green(int n, float* g);
 void mixed_launch(const MixedArgs& a, cudaStream_t stream);
 
 }  // namespace mzb

@@ -22,14 +22,17 @@ def main():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--integrator", default="OVRVO")
     ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 FP32 multigrid + FP64 refinement")
     args = ap.parse_args()
     os.environ.setdefault("MZB_QUIET", "1")
     run = MDRun(CAPI(), make_system(seed=1, **WORKLOADS[args.workload]), method=args.method,
                 precond=args.precond, tol=args.tol, integrator=args.integrator,
-                thermostat=args.integrator.upper() == "OVRVO")
+                thermostat=args.integrator.upper() == "OVRVO", precision=args.precision)
+    capi = run.capi
     run.initialize()
-    for _ in range(args.steps):
-        run.step()
+    for k in range(args.steps):
+        it = run.step()
+        print(f"step {k}: solve {capi.mzb_last_solve_ms():.4f} ms, solver returned {it}")
     run.finalize()
     print("ok")
 
