@@ -145,7 +145,7 @@ void free_grid(GridState& G) {
 bool mixed_supported(const GridState& G) {
     int sizes[kMixedMaxLevels];
     const int L = mixed_levels(G.n, sizes);
-    return G.type != 1 && L >= 3 && mixed_small_level(L, sizes) >= 1;
+    return G.type != 1 && G.n <= kMixedMaxN && L >= 3 && mixed_small_level(L, sizes) >= 1;
 }
 
 void ensure_mixed_levels(GridState& G) {

@@ -31,7 +31,16 @@
 namespace mzb {
 namespace {
 
-constexpr int kThreads = 1024;
+#ifndef MZB_MIXED_THREADS
+#define MZB_MIXED_THREADS 1024
+#endif
+#ifndef MZB_MIXED_SWEEP_BATCH
+#define MZB_MIXED_SWEEP_BATCH 2
+#endif
+#ifndef MZB_MIXED_BATCH
+#define MZB_MIXED_BATCH 2
+#endif
+constexpr int kThreads = MZB_MIXED_THREADS;
 
 __device__ __forceinline__ void stamp(const MixedArgs& a, int slot) {
     if (a.stamps != nullptr && blockIdx.x == 0 && threadIdx.x == 0 && slot < kMixedStampSlots)
@@ -55,18 +64,6 @@ __device__ __forceinline__ void grid_pts(int n, F&& f) {
         for (int k = lane; k < n; k += 32) f(i, j, k);
     }
 }
-template <class F>
-__device__ __forceinline__ void grid_col(int n, int colour, F&& f) {
-    const int lane = threadIdx.x & 31;
-    const long gw = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const long nw = (long)gridDim.x * (blockDim.x >> 5);
-    const long rows = (long)n * n;
-    for (long row = gw; row < rows; row += nw) {
-        const int i = (int)(row / n), j = (int)(row - (long)i * n);
-        for (int k = ((i + j + colour) & 1) + 2 * lane; k < n; k += 64) f(i, j, k);
-    }
-}
-
 // CTA-0 loops (shared-memory levels): a thread per point
 template <class F>
 __device__ __forceinline__ void cta_pts(int n, F&& f) {
@@ -210,6 +207,257 @@ __device__ __forceinline__ void prolong_point(int n, const float* xc, float* x, 
     x[((long)i * n + j) * n + k] += b0 * (1.0f - wi) + b1 * wi;
 }
 
+// ---- grid levels: red-black split layout ----
+//
+// On the levels worked by the whole grid, point (i,j,k) of colour c = (i+j+k) & 1 is
+// stored at c n^3/2 + (i n + j) n/2 + (k >> 1): each colour is a contiguous half, and a
+// row (i,j) of one colour is n/2 consecutive values. A half-sweep of colour c then reads
+// the other colour and writes its own with unit-stride, fully coalesced accesses; in row
+// (i,j) the points of colour c sit at k = 2 kk + s, s = (i+j+c) & 1, and their k-1 / k+1
+// neighbours are the other colour's kk-1+s / kk+s, while their i+-1 / j+-1 neighbours are
+// the other colour's kk in those rows.
+//
+// After a pre-smoothing that ends with a black half-sweep, the residual of every black
+// point is zero (each black point satisfies its own equation exactly), so only the red
+// residual is formed, the 27-point restriction keeps its 13 red taps (centre weight 8,
+// the 12 edge points weight 2), and a prolongation that is followed by a red half-sweep
+// only updates the black points (the red half-sweep overwrites the red ones without
+// reading them).
+
+constexpr int kBatch = MZB_MIXED_BATCH;  // points per lane whose loads are issued before any store
+constexpr int kBatchSweep = MZB_MIXED_SWEEP_BATCH;  // the same for the red-black half-sweeps and red residuals
+
+// Offsets within a level are 32-bit: the mixed solver takes n <= kMixedMaxN (n^3 < 2^31).
+__device__ __forceinline__ int split_idx(int n, int i, int j, int k) {
+    const int h = n >> 1;
+    return ((i + j + k) & 1) * h * n * n + (i * n + j) * h + (k >> 1);
+}
+
+struct Rows {
+    int c, im, ip, jm, jp;  // offsets of rows (i,j), (i-1,j), (i+1,j), (i,j-1), (i,j+1) in one colour
+};
+__device__ __forceinline__ Rows rows_of(int n, int i, int j) {
+    const int h = n >> 1;
+    const int ip = i + 1 == n ? 0 : i + 1, im = i == 0 ? n - 1 : i - 1;
+    const int jp = j + 1 == n ? 0 : j + 1, jm = j == 0 ? n - 1 : j - 1;
+    return Rows{(i * n + j) * h, (im * n + j) * h, (ip * n + j) * h, (i * n + jm) * h, (i * n + jp) * h};
+}
+
+// warp per row (i,j) of an n x n set of rows, over all CTAs
+template <class F>
+__device__ __forceinline__ void grid_rows(int n, F&& f) {
+    const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    const int rows = n * n;
+    for (int row = gw; row < rows; row += nw) {
+        const int i = row / n;
+        f(i, row - i * n);
+    }
+}
+
+// Sums of the six other-colour neighbours of the T chunks kk = k0 + lane + 32 t of the
+// colour in row o whose points sit at k = 2 kk + s. The four off-row neighbours and the
+// in-row value at kk are loaded for all chunks first; the in-row neighbour on the other
+// side (kk - 1 for s = 0, kk + 1 for s = 1) comes from the adjacent lane by a shuffle,
+// and only at a chunk or row boundary from memory.
+template <int T>
+__device__ __forceinline__ void split_nb_sums(const float* xo, const Rows& o, int h, int s, int k0, float (&sum)[T]) {
+    const int lane = threadIdx.x & 31;
+    float cen[T];
+#pragma unroll
+    for (int t = 0; t < T; t++) {
+        const int kk = k0 + lane + 32 * t;
+        sum[t] = 0.0f;
+        cen[t] = 0.0f;
+        if (kk < h) {
+            const float a0 = xo[o.im + kk], a1 = xo[o.ip + kk], a2 = xo[o.jm + kk], a3 = xo[o.jp + kk];
+            cen[t] = xo[o.c + kk];
+            sum[t] = ((a0 + a1) + a2) + a3;
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < T; t++) {
+        const int kk = k0 + lane + 32 * t;
+        const float up = __shfl_up_sync(0xffffffffu, cen[t], 1);
+        const float dn = __shfl_down_sync(0xffffffffu, cen[t], 1);
+        const float last_prev = __shfl_sync(0xffffffffu, cen[t > 0 ? t - 1 : 0], 31);
+        const float first_next = __shfl_sync(0xffffffffu, cen[t + 1 < T ? t + 1 : t], 0);
+        if (kk < h) {
+            float side;
+            if (s == 0) {
+                if (lane > 0)
+                    side = up;
+                else if (t > 0)
+                    side = last_prev;
+                else
+                    side = xo[o.c + (kk == 0 ? h - 1 : kk - 1)];
+            } else {
+                if (kk + 1 == h)
+                    side = xo[o.c];
+                else if (lane < 31)
+                    side = dn;
+                else if (t + 1 < T)
+                    side = first_next;
+                else
+                    side = xo[o.c + kk + 1];
+            }
+            sum[t] = (sum[t] + cen[t]) + side;
+        }
+    }
+}
+
+// half-sweep of colour c; when acc is not null the new values are summed into it
+__device__ void split_gs(int n, int c, const float* b, float* x, double* acc) {
+    const int lane = threadIdx.x & 31, h = n >> 1;
+    const int hp = h * n * n;
+    const float* xo = x + (1 - c) * hp;
+    float* xc = x + c * hp;
+    const float* bc = b + c * hp;
+    double s_acc = 0.0;
+    grid_rows(n, [&](int i, int j) {
+        const Rows o = rows_of(n, i, j);
+        const int s = (i + j + c) & 1;
+        for (int k0 = 0; k0 < h; k0 += 32 * kBatchSweep) {
+            float bv[kBatchSweep], sum[kBatchSweep];
+#pragma unroll
+            for (int t = 0; t < kBatchSweep; t++) {
+                const int kk = k0 + lane + 32 * t;
+                bv[t] = kk < h ? bc[o.c + kk] : 0.0f;
+            }
+            split_nb_sums<kBatchSweep>(xo, o, h, s, k0, sum);
+#pragma unroll
+            for (int t = 0; t < kBatchSweep; t++) {
+                const int kk = k0 + lane + 32 * t;
+                if (kk < h) {
+                    const float v = (bv[t] - sum[t]) * (-1.0f / 6.0f);
+                    xc[o.c + kk] = v;
+                    s_acc += (double)v;
+                }
+            }
+        }
+    });
+    if (acc != nullptr) *acc += s_acc;
+}
+
+// red residual r_red = b_red - L x at the red points (black residuals are zero)
+__device__ void split_resid_red(int n, const float* b, const float* x, float* r) {
+    const int lane = threadIdx.x & 31, h = n >> 1;
+    const int hp = h * n * n;
+    const float* x1 = x + hp;
+    grid_rows(n, [&](int i, int j) {
+        const Rows o = rows_of(n, i, j);
+        const int s = (i + j) & 1;
+        for (int k0 = 0; k0 < h; k0 += 32 * kBatchSweep) {
+            float bv[kBatchSweep], xv[kBatchSweep], sum[kBatchSweep];
+#pragma unroll
+            for (int t = 0; t < kBatchSweep; t++) {
+                const int kk = k0 + lane + 32 * t;
+                bv[t] = kk < h ? b[o.c + kk] : 0.0f;
+                xv[t] = kk < h ? x[o.c + kk] : 0.0f;
+            }
+            split_nb_sums<kBatchSweep>(x1, o, h, s, k0, sum);
+#pragma unroll
+            for (int t = 0; t < kBatchSweep; t++) {
+                const int kk = k0 + lane + 32 * t;
+                if (kk < h) r[o.c + kk] = bv[t] - (sum[t] - 6.0f * xv[t]);
+            }
+        }
+    });
+}
+
+// 4 x R27(r) at coarse point (I,J,K) from the red residual half of a split level n
+// (the 13 red taps of the 27-point full weighting)
+__device__ __forceinline__ float split_restrict_value(int n, const float* r, int I, int J, int K) {
+    const int h = n >> 1;
+    const int i = 2 * I, j = 2 * J;
+    const int ip = i + 1, im = i == 0 ? n - 1 : i - 1, jp = j + 1, jm = j == 0 ? n - 1 : j - 1;
+    auto R = [&](int fi, int fj) { return (fi * n + fj) * h; };
+    const int Km = K == 0 ? h - 1 : K - 1;
+    float e = r[R(ip, jp) + K] + r[R(ip, jm) + K];
+    e += r[R(im, jp) + K];
+    e += r[R(im, jm) + K];
+    e += r[R(ip, j) + K];
+    e += r[R(ip, j) + Km];
+    e += r[R(im, j) + K];
+    e += r[R(im, j) + Km];
+    e += r[R(i, jp) + K];
+    e += r[R(i, jp) + Km];
+    e += r[R(i, jm) + K];
+    e += r[R(i, jm) + Km];
+    return (8.0f * r[R(i, j) + K] + 2.0f * e) * (4.0f / 64.0f);
+}
+
+// coarse b = 4 R27(r), coarse x = its first red half-sweep from 0 (both split layout)
+__device__ void split_restrict(int n, const float* r, float* bc, float* xc) {
+    const int lane = threadIdx.x & 31, nc = n / 2, hc = nc >> 1;
+    const int hpc = hc * nc * nc;
+    grid_rows(nc, [&](int I, int J) {
+        for (int k0 = 0; k0 < nc; k0 += 32 * kBatch) {
+            float v[kBatch];
+#pragma unroll
+            for (int t = 0; t < kBatch; t++) {
+                const int K = k0 + lane + 32 * t;
+                if (K < nc) v[t] = split_restrict_value(n, r, I, J, K);
+            }
+#pragma unroll
+            for (int t = 0; t < kBatch; t++) {
+                const int K = k0 + lane + 32 * t;
+                if (K < nc) {
+                    const int C = (I + J + K) & 1;
+                    const int idx = C * hpc + (I * nc + J) * hc + (K >> 1);
+                    bc[idx] = v[t];
+                    xc[idx] = C == 0 ? v[t] * (-1.0f / 6.0f) : 0.0f;
+                }
+            }
+        }
+    });
+}
+
+// fine black x += P(coarse x), trilinear (both split layout)
+__device__ void split_prolong_black(int n, const float* xc, float* x) {
+    const int lane = threadIdx.x & 31, h = n >> 1, nc = n / 2, hc = nc >> 1;
+    const int hp = h * n * n, hpc = hc * nc * nc;
+    float* x1 = x + hp;
+    grid_rows(n, [&](int i, int j) {
+        const int s1 = (i + j + 1) & 1;  // black points of row (i,j) sit at k = 2 kk + s1
+        const int ci = i >> 1, cj = j >> 1;
+        const int ci1 = ci + 1 == nc ? 0 : ci + 1, cj1 = cj + 1 == nc ? 0 : cj + 1;
+        const bool oi = i & 1, oj = j & 1, ok = s1;
+        auto C = [&](int CI, int CJ, int CK) {
+            return ((CI + CJ + CK) & 1) * hpc + (CI * nc + CJ) * hc + (CK >> 1);
+        };
+        auto line = [&](int CI, int CJ, int ck, int ck1) {
+            const float a = xc[C(CI, CJ, ck)];
+            return ok ? 0.5f * (a + xc[C(CI, CJ, ck1)]) : a;
+        };
+        const int rowx = (i * n + j) * h;
+        for (int k0 = 0; k0 < h; k0 += 32 * kBatch) {
+            float v[kBatch], old[kBatch];
+#pragma unroll
+            for (int t = 0; t < kBatch; t++) {
+                const int kk = k0 + lane + 32 * t;
+                if (kk < h) {
+                    const int ck = kk, ck1 = kk + 1 == nc ? 0 : kk + 1;
+                    float p = line(ci, cj, ck, ck1);
+                    if (oj) p = 0.5f * (p + line(ci, cj1, ck, ck1));
+                    if (oi) {
+                        float q = line(ci1, cj, ck, ck1);
+                        if (oj) q = 0.5f * (q + line(ci1, cj1, ck, ck1));
+                        p = 0.5f * (p + q);
+                    }
+                    v[t] = p;
+                    old[t] = x1[rowx + kk];
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < kBatch; t++) {
+                const int kk = k0 + lane + 32 * t;
+                if (kk < h) x1[rowx + kk] = old[t] + v[t];
+            }
+        }
+    });
+}
+
 // ---- the shared-memory part of the V-cycle (CTA 0) ----
 //
 // Shared memory holds x, b, r of levels lsmall..nlev-1 back to back, then (when the
@@ -260,11 +508,16 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm) {
         for (int p = threadIdx.x; p < N; p += blockDim.x) gsm[p] = a.coarse_g[p];
     }
     {
-        const float* r = a.lev_r[ls - 1];
-        const int nf = a.lev_n[ls - 1];
+        const float* r = a.lev_r[ls - 1];  // red residual, split layout
+        const int nf = a.lev_n[ls - 1], nc = a.lev_n[ls];
         float* bs = small_arr(a, sm, ls, 1);
         float* xs = small_arr(a, sm, ls, 0);
-        cta_pts(a.lev_n[ls], [&](int I, int J, int K) { restrict_point(nf, r, bs, xs, I, J, K); });
+        cta_pts(nc, [&](int I, int J, int K) {
+            const float bv = split_restrict_value(nf, r, I, J, K);
+            const int cc = (I * nc + J) * nc + K;
+            bs[cc] = bv;
+            xs[cc] = ((I + J + K) & 1) == 0 ? bv * (-1.0f / 6.0f) : 0.0f;
+        });
         __syncthreads();
     }
     for (int m = ls; m < L - 1; m++) {
@@ -294,27 +547,20 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm) {
         __syncthreads();
         smooth(m, 0, 2 * a.nu2);
     }
-    const int v = a.lev_n[ls] * a.lev_n[ls] * a.lev_n[ls];
+    const int nl = a.lev_n[ls];
     const float* xs = small_arr(a, sm, ls, 0);
-    float* dst = a.lev_x[ls];
-    for (int p = threadIdx.x; p < v; p += blockDim.x) dst[p] = xs[p];
+    float* dst = a.lev_x[ls];  // split layout
+    cta_pts(nl, [&](int i, int j, int k) { dst[split_idx(nl, i, j, k)] = xs[(i * nl + j) * nl + k]; });
 }
 
 // Grid-wide red-black sweeps of level l: `half_sweeps` colours starting at first_colour,
 // a grid barrier after each except (when skip_last_barrier) the last. When esum is not
 // null the values written in the last two half-sweeps are summed into it.
-__device__ bool grid_smooth(const MixedArgs& a, int l, float* x, int first_colour, int half_sweeps, unsigned& epoch,
+__device__ bool grid_smooth(const MixedArgs& a, int l, int first_colour, int half_sweeps, unsigned& epoch,
                             double* esum, bool skip_last_barrier) {
-    const int n = a.lev_n[l];
-    const float* b = a.lev_b[l];
     for (int h = 0; h < half_sweeps; h++) {
-        const bool acc = esum != nullptr && h >= half_sweeps - 2;
-        double s = 0.0;
-        grid_col(n, (first_colour + h) & 1, [&](int i, int j, int k) {
-            const float v = gs_point(n, b, x, i, j, k);
-            if (acc) s += (double)v;
-        });
-        if (acc) *esum += s;
+        split_gs(a.lev_n[l], (first_colour + h) & 1, a.lev_b[l], a.lev_x[l],
+                 esum != nullptr && h >= half_sweeps - 2 ? esum : nullptr);
         if (h == half_sweeps - 1 && skip_last_barrier) break;
         if (!grid_sync_mono(a.bar, epoch)) return false;
     }
@@ -328,14 +574,11 @@ __device__ bool vcycle(const MixedArgs& a, float* sm, unsigned& epoch, double& e
     const int L = a.nlev, ls = a.lsmall;
     const int lg = ls < L ? ls : L - 1;  // levels 0..lg-1 are smoothed and restricted on the grid
     for (int l = 0; l < lg; l++) {
-        if (!grid_smooth(a, l, a.lev_x[l], 1, 2 * a.nu1 - 1, epoch, nullptr, false)) return false;
-        grid_pts(a.lev_n[l],
-                 [&](int i, int j, int k) { resid_point(a.lev_n[l], a.lev_b[l], a.lev_x[l], a.lev_r[l], i, j, k); });
+        if (!grid_smooth(a, l, 1, 2 * a.nu1 - 1, epoch, nullptr, false)) return false;
+        split_resid_red(a.lev_n[l], a.lev_b[l], a.lev_x[l], a.lev_r[l]);
         if (!grid_sync_mono(a.bar, epoch)) return false;
         if (l + 1 < ls) {
-            grid_pts(a.lev_n[l + 1], [&](int I, int J, int K) {
-                restrict_point(a.lev_n[l], a.lev_r[l], a.lev_b[l + 1], a.lev_x[l + 1], I, J, K);
-            });
+            split_restrict(a.lev_n[l], a.lev_r[l], a.lev_b[l + 1], a.lev_x[l + 1]);
             if (!grid_sync_mono(a.bar, epoch)) return false;
         }
     }
@@ -344,13 +587,13 @@ __device__ bool vcycle(const MixedArgs& a, float* sm, unsigned& epoch, double& e
         if (blockIdx.x == 0) small_vcycle(a, sm);
         if (!grid_sync_mono(a.bar, epoch)) return false;
     } else {
-        if (!grid_smooth(a, L - 1, a.lev_x[L - 1], 1, 2 * a.coarse_sweeps - 1, epoch, nullptr, false)) return false;
+        if (!grid_smooth(a, L - 1, 1, 2 * a.coarse_sweeps - 1, epoch, nullptr, false)) return false;
     }
     stamp_outer(a, outer, 3);
     for (int l = lg - 1; l >= 0; l--) {
-        grid_pts(a.lev_n[l], [&](int i, int j, int k) { prolong_point(a.lev_n[l], a.lev_x[l + 1], a.lev_x[l], i, j, k); });
+        split_prolong_black(a.lev_n[l], a.lev_x[l + 1], a.lev_x[l]);
         if (!grid_sync_mono(a.bar, epoch)) return false;
-        if (!grid_smooth(a, l, a.lev_x[l], 0, 2 * a.nu2, epoch, l == 0 ? &esum : nullptr, l == 0)) return false;
+        if (!grid_smooth(a, l, 0, 2 * a.nu2, epoch, l == 0 ? &esum : nullptr, l == 0)) return false;
     }
     return true;
 }
@@ -422,8 +665,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
             s = s + X[o.km];
             const double r = B[o.c] - (s - X[o.c] * 6.0);
             const float rf = (float)r;
-            rb[o.c] = rf;
-            e[o.c] = ((i + j + k) & 1) == 0 ? rf * (-1.0f / 6.0f) : 0.0f;
+            const int sx = split_idx(n, i, j, k);
+            rb[sx] = rf;
+            e[sx] = ((i + j + k) & 1) == 0 ? rf * (-1.0f / 6.0f) : 0.0f;
             rmax = fmax(rmax, fabs(r));
         });
         ok = reduce_sum_max(s0, rmax, a, epoch, seq);
@@ -447,7 +691,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
         const double emean = esum / ((double)n * n * n);
         grid_pts(n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
-            X[c] = X[c] + ((double)e[c] - emean);
+            X[c] = X[c] + ((double)e[split_idx(n, i, j, k)] - emean);
         });
         ok = grid_sync_mono(a.bar, epoch);
         stamp_outer(a, outer, 6);

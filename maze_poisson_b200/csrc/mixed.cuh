@@ -7,6 +7,7 @@ namespace mzb {
 
 constexpr int kMixedMaxLevels = 10;
 constexpr int kMixedSmallN = 16;     // levels with n <= this live in CTA 0's shared memory
+constexpr int kMixedMaxN = 1024;     // largest grid of the mixed solver (32-bit offsets in a level)
 constexpr int kMixedStampSlots = 2 + 8 * 8;
 
 struct MixedArgs {
