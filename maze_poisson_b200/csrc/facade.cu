@@ -178,18 +178,20 @@ void free_particles(ParticleDev& P) {
 }
 
 // Linked-cell geometry for the Tosi-Fumi kernel: about 16 ions per cell, at least one
-// cell per side; warps split the partner cells so that ~12k warps are in flight.
+// cell per side; the warps (one per 32 ions in cell order) split the partner cells so
+// that ~12k warps are in flight.
 void set_cells(ParticleDev& P, int nc) {
     dfree(P.cell_count); dfree(P.cell_start); dfree(P.cell_fill); dfree(P.fpart); dfree(P.epart);
     P.nc = nc < 1 ? 1 : nc;
     P.ncell = P.nc * P.nc * P.nc;
-    int split = (12000 + P.ncell - 1) / P.ncell;
+    const int nblk = (P.np + 31) / 32 > 0 ? (P.np + 31) / 32 : 1;
+    int split = (12000 + nblk - 1) / nblk;
     P.tf_split = split < 1 ? 1 : (split > P.ncell ? P.ncell : split);
     P.cell_count = dalloc<int32_t>(P.ncell);
     P.cell_start = dalloc<int32_t>(P.ncell + 1);
     P.cell_fill = dalloc<int32_t>(P.ncell);
     P.fpart = dalloc<double>((size_t)P.tf_split * P.np * 3);
-    P.epart = dalloc<double>((size_t)P.ncell * P.tf_split);
+    P.epart = dalloc<double>((size_t)nblk * P.tf_split);
 }
 
 EngineArgs engine_base(System& s) {

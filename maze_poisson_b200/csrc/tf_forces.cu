@@ -1,21 +1,35 @@
-// Shifted-force Tosi-Fumi (Born-Mayer-Huggins) pair forces, warp per linked cell
+// Shifted-force Tosi-Fumi (Born-Mayer-Huggins) pair forces, warp per 32 cell-sorted ions
 // (reference: library/src/forces.c:112-186, parameters particles.c:181-228).
 //
 // Compiled with --fmad=true: this kernel is bound by the FP64 pipe, and its results are
 // already ulp-level (exp and inverse powers) rather than bit-level equal to the
 // reference, which uses glibc exp/pow.
 //
-// Layout: ions are sorted by cell (linked cells, particles.cu). Warp w handles cell
-// ci = w / split and the w % split-th contiguous chunk of partner cells; lanes hold up to
-// 32 ions of ci (looping if a cell has more), partner ions are broadcast loads. Partner
-// cells whose minimum-image distance exceeds r_cut = L/2 are skipped (with a 1e-9
-// relative margin), which removes ~40% of the N^2 pair work; pruning is turned off when
-// any coordinate lies outside [0, L). Partial forces per chunk are summed in chunk order.
+// Layout: ions are sorted by cell (linked cells, particles.cu). Warp w takes the 32
+// consecutive ions of block w / split in that order (every lane holds an ion) and the
+// w % split-th contiguous chunk of partner cells; partner ions are broadcast loads.
+// Partner cells whose minimum-image distance to the bounding box of the warp's ions
+// exceeds r_cut = L/2 are skipped (with a 1e-9 relative margin), which removes ~40% of
+// the N^2 pair work; pruning is turned off when any coordinate lies outside [0, L).
+// 1/r comes from one FP64 rsqrt and r = r2 (1/r); the cutoff is tested on r^2. Partial
+// forces per chunk are summed in chunk order.
 #include "particles.cuh"
 
 namespace mzb {
 
 constexpr int kTfWarps = 4;
+
+// min-image gap along one axis between the interval [lo, hi] and the cell [c0, c0 + cl]
+__device__ __forceinline__ double axis_gap(double lo, double hi, double c0, double cl, double L) {
+    double best = 1e300;
+#pragma unroll
+    for (int s = -1; s <= 1; s++) {
+        const double a = c0 + s * L, b = a + cl;
+        const double g = fmax(0.0, fmax(a - hi, lo - b));
+        best = fmin(best, g);
+    }
+    return best;
+}
 
 __global__ void __launch_bounds__(kTfWarps * 32) k_tf(ParticleDev P) {
     __shared__ double tab[64 * 7];
@@ -23,76 +37,73 @@ __global__ void __launch_bounds__(kTfWarps * 32) k_tf(ParticleDev P) {
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const long gw = (long)blockIdx.x * kTfWarps + (threadIdx.x >> 5);
-    const long total = (long)P.ncell * P.tf_split;
+    const int nblk = (P.np + 31) / 32;
+    const long total = (long)nblk * P.tf_split;
     if (gw >= total) return;
-    const int ci = (int)(gw / P.tf_split), chunk = (int)(gw % P.tf_split);
+    const int blk = (int)(gw / P.tf_split), chunk = (int)(gw % P.tf_split);
     const int cj0 = (int)((long)chunk * P.ncell / P.tf_split);
     const int cj1 = (int)((long)(chunk + 1) * P.ncell / P.tf_split);
     const int nc = P.nc;
-    const int cix = ci / (nc * nc), ciy = (ci / nc) % nc, ciz = ci % nc;
     const double L = P.L, invL = 1.0 / L, rcut = P.rcut;
     const double cl = L / nc;
     const double prune2 = rcut * rcut * (1.0 + 1e-9);
-    const double pre2 = rcut * rcut * (1.0 + 1e-12);
+    const double rc2 = rcut * rcut;
     const bool prune = P.flags[1] == 0;
     const int ntyp = P.ntyp;
-    double e_acc = 0.0;
-    const int cb = P.cell_start[ci], ce = P.cell_start[ci + 1];
-    for (int s0 = cb; s0 < ce; s0 += 32) {
-        const int si = s0 + lane;
-        const bool valid = si < ce;
-        double xi = 0, yi = 0, zi = 0;
-        int ti = 0;
-        if (valid) {
-            xi = P.spos[3 * si];
-            yi = P.spos[3 * si + 1];
-            zi = P.spos[3 * si + 2];
-            ti = P.stype[si];
+
+    const int si = blk * 32 + lane;
+    const bool valid = si < P.np;
+    const int sl = valid ? si : blk * 32;  // invalid lanes mirror lane 0 for the bounding box
+    const double xi = P.spos[3 * sl], yi = P.spos[3 * sl + 1], zi = P.spos[3 * sl + 2];
+    const int ti = P.stype[sl];
+    double lx = xi, hx = xi, ly = yi, hy = yi, lz = zi, hz = zi;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lx = fmin(lx, __shfl_xor_sync(0xffffffffu, lx, o));
+        hx = fmax(hx, __shfl_xor_sync(0xffffffffu, hx, o));
+        ly = fmin(ly, __shfl_xor_sync(0xffffffffu, ly, o));
+        hy = fmax(hy, __shfl_xor_sync(0xffffffffu, hy, o));
+        lz = fmin(lz, __shfl_xor_sync(0xffffffffu, lz, o));
+        hz = fmax(hz, __shfl_xor_sync(0xffffffffu, hz, o));
+    }
+    double fx = 0.0, fy = 0.0, fz = 0.0, e_acc = 0.0;
+    for (int cj = cj0; cj < cj1; cj++) {
+        if (prune) {
+            const int cjx = cj / (nc * nc), cjy = (cj / nc) % nc, cjz = cj % nc;
+            const double gx = axis_gap(lx, hx, cjx * cl, cl, L), gy = axis_gap(ly, hy, cjy * cl, cl, L);
+            const double gz = axis_gap(lz, hz, cjz * cl, cl, L);
+            if (gx * gx + gy * gy + gz * gz > prune2) continue;
         }
-        double fx = 0.0, fy = 0.0, fz = 0.0;
-        for (int cj = cj0; cj < cj1; cj++) {
-            if (prune) {
-                const int cjx = cj / (nc * nc), cjy = (cj / nc) % nc, cjz = cj % nc;
-                int dx = abs(cix - cjx), dy = abs(ciy - cjy), dz = abs(ciz - cjz);
-                dx = min(dx, nc - dx);
-                dy = min(dy, nc - dy);
-                dz = min(dz, nc - dz);
-                const double gx = max(dx - 1, 0) * cl, gy = max(dy - 1, 0) * cl, gz = max(dz - 1, 0) * cl;
-                if (gx * gx + gy * gy + gz * gz > prune2) continue;
-            }
-            const int jb = P.cell_start[cj], je = P.cell_start[cj + 1];
-            for (int sj = jb; sj < je; sj++) {
-                const double xj = P.spos[3 * sj], yj = P.spos[3 * sj + 1], zj = P.spos[3 * sj + 2];
-                const int tj = P.stype[sj];
-                if (!valid || sj == si) continue;
-                double dx = xi - xj, dy = yi - yj, dz = zi - zj;
-                dx -= L * round(dx * invL);
-                dy -= L * round(dy * invL);
-                dz -= L * round(dz * invL);
-                const double r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 > pre2) continue;
-                const double r = sqrt(r2);
-                if (r > rcut) continue;
-                const double* t = tab + 7 * (ti * ntyp + tj);
-                const double a = t[0], b = t[1], c = t[2], d = t[3], sg = t[4], al = t[5], be = t[6];
-                const double ir = 1.0 / r, ir2 = ir * ir, ir6 = ir2 * ir2 * ir2;
-                const double ir7 = ir6 * ir, ir8 = ir6 * ir2, ir9 = ir8 * ir;
-                const double ex = exp(b * (sg - r));
-                const double fm = b * a * ex - 6 * c * ir7 - 8 * d * ir9 - al;
-                const double vm = a * ex - c * ir6 - d * ir8 + al * r + be;
-                const double fr = fm * ir;
-                fx += fr * dx;
-                fy += fr * dy;
-                fz += fr * dz;
-                e_acc += vm;
-            }
+        const int jb = P.cell_start[cj], je = P.cell_start[cj + 1];
+        for (int sj = jb; sj < je; sj++) {
+            const double xj = P.spos[3 * sj], yj = P.spos[3 * sj + 1], zj = P.spos[3 * sj + 2];
+            const int tj = P.stype[sj];
+            if (!valid || sj == si) continue;
+            double dx = xi - xj, dy = yi - yj, dz = zi - zj;
+            dx -= L * round(dx * invL);
+            dy -= L * round(dy * invL);
+            dz -= L * round(dz * invL);
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 > rc2) continue;
+            const double* t = tab + 7 * (ti * ntyp + tj);
+            const double a = t[0], b = t[1], c = t[2], d = t[3], sg = t[4], al = t[5], be = t[6];
+            const double ir = rsqrt(r2), r = r2 * ir, ir2 = ir * ir, ir6 = ir2 * ir2 * ir2;
+            const double ir7 = ir6 * ir, ir8 = ir6 * ir2, ir9 = ir8 * ir;
+            const double ex = exp(b * (sg - r));
+            const double fm = b * a * ex - 6 * c * ir7 - 8 * d * ir9 - al;
+            const double vm = a * ex - c * ir6 - d * ir8 + al * r + be;
+            const double fr = fm * ir;
+            fx += fr * dx;
+            fy += fr * dy;
+            fz += fr * dz;
+            e_acc += vm;
         }
-        if (valid) {
-            double* o = P.fpart + ((long)chunk * P.np + si) * 3;
-            o[0] = fx;
-            o[1] = fy;
-            o[2] = fz;
-        }
+    }
+    if (valid) {
+        double* o = P.fpart + ((long)chunk * P.np + si) * 3;
+        o[0] = fx;
+        o[1] = fy;
+        o[2] = fz;
     }
     e_acc = warp_sum(e_acc);
     if (lane == 0) P.epart[gw] = e_acc;
@@ -116,7 +127,7 @@ __global__ void k_tf_gather(ParticleDev P) {
 }
 
 __global__ void k_tf_energy(ParticleDev P) {
-    const long m = (long)P.ncell * P.tf_split;
+    const long m = (long)((P.np + 31) / 32) * P.tf_split;
     double v[1] = {0.0};
     for (long x = threadIdx.x; x < m; x += blockDim.x) v[0] += P.epart[x];
     __shared__ double sh[4 * 32];
@@ -130,7 +141,7 @@ void tf_forces(ParticleDev& P, cudaStream_t s) {
         return;
     }
     if (P.ntyp * P.ntyp > 64) fatal("Tosi-Fumi: more than 8 particle types");
-    const long warps = (long)P.ncell * P.tf_split;
+    const long warps = (long)((P.np + 31) / 32) * P.tf_split;
     count_launch();
     k_tf<<<(unsigned)((warps + kTfWarps - 1) / kTfWarps), kTfWarps * 32, 0, s>>>(P);
     count_launch();
