@@ -61,6 +61,34 @@ uint64_t mzb_get_ocalls(void);             /* O-blocks applied so far */
 int mzb_conj_grad_noalloc(const double *b, const double *x0, double *x, double tol, int n,
                           int precond, void *stream);
 
+/* Several resident systems. No counterpart in the reference, which holds one global
+   system per process (library/src/solver_md.c:12-14); every reference call above acts on
+   the selected system. mzb_system_create makes a new empty system and selects it
+   (initialise it with solver_initialize, solver_initialize_grid, ...); select/destroy
+   return -1 for an unknown handle. */
+int mzb_system_create(void);
+int mzb_system_select(int handle);
+int mzb_system_current(void);
+int mzb_system_destroy(int handle);
+
+/* Advance the listed systems by n_steps MD steps (solver.py:483-492 each) together: one
+   CUDA graph per step, whose branches run each system's integrator, charge spreading and
+   forces, and one cooperative launch that runs every system's field solve on its own
+   range of CTAs. Every system must be initialised, bootstrapped and use the FP32+refine
+   field solve (mzb_set_precision(1, ...)). Charge errors exit as solver_update_charges
+   does, after the call. Returns 0, or -1 if a field solve did not converge. No
+   counterpart in the reference. */
+int mzb_batch_step(const int *handles, int nsys, int n_steps);
+
+/* Time candidate team partitions of the batched field solve and warp targets of the pair
+   forces on the listed systems and keep the fastest; out[0..3] = {partition exponent,
+   warps, solve ms, forces ms}. Leaves the systems' state unchanged. */
+int mzb_batch_autotune(const int *handles, int nsys, double *out);
+
+/* Device bytes one FP32+refine system with an n^3 grid and n_p ions holds (admission
+   against an HBM budget). */
+double mzb_system_footprint(int n, int n_p);
+
 /* instrumentation */
 void *mzb_get_stream(void);                /* cudaStream_t of the current system */
 double mzb_last_solve_ms(void);            /* device ms of the last field-solver launch */

@@ -111,6 +111,13 @@ EXTENSION_SYMBOLS = {
     "mzb_get_precision": (_c.c_int, []),
     "mzb_conj_grad_noalloc": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_double, _c.c_int,
                                          _c.c_int, _c.c_void_p]),
+    "mzb_system_create": (_c.c_int, []),
+    "mzb_system_select": (_c.c_int, [_c.c_int]),
+    "mzb_system_current": (_c.c_int, []),
+    "mzb_system_destroy": (_c.c_int, [_c.c_int]),
+    "mzb_batch_step": (_c.c_int, [_i32_1, _c.c_int, _c.c_int]),
+    "mzb_batch_autotune": (_c.c_int, [_i32_1, _c.c_int, _f64_1]),
+    "mzb_system_footprint": (_c.c_double, [_c.c_int, _c.c_int]),
 }
 
 
@@ -119,7 +126,8 @@ class CAPI:
 
     `CAPI()` loads this build's libmaze_poisson.so; `CAPI(path, extensions=False)` loads
     any other library with the reference's ABI (only the reference symbols are bound).
-    Each library holds one global MD system, as in the reference.
+    The reference holds one global MD system; this build holds several (mzb_system_*),
+    and the reference calls act on the selected one.
     """
 
     def __init__(self, path=None, extensions=True, mode=ctypes.RTLD_LOCAL):

@@ -9,6 +9,7 @@
 // Fatal conditions print a message and exit(1) exactly where the reference does.
 #include <cmath>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "engine.cuh"
@@ -97,11 +98,18 @@ struct System {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the last solver-engine launch
     float last_solve_ms = 0.f;
     int last_solve_iters = 0;
+    double q_tot = 0.0;           // charge of the last spreading; persists like solver_md.c:16
+    uint64_t epoch = 0;           // bumped by host-side changes that batched-step graphs bake in
+    double* qtot_d = nullptr;     // device copy of q_tot (batched steps check charge on the device)
+    int* err_d = nullptr;         // batched steps: [0] charge error, [1] spread overflow, [2] solve failure
 };
 
-System* g = nullptr;
-double g_q_tot = 0.0;  // persists across systems like solver_md.c:16
+System* g = nullptr;             // the selected system
+std::vector<System*> g_systems;  // handle -> system (null once destroyed)
+int g_current = -1;
 bool g_quiet = false;
+
+void touch(System& s) { s.epoch++; }
 
 System& sys() {
     if (!g) fatal("solver_initialize() has not been called");
@@ -179,13 +187,14 @@ void free_particles(ParticleDev& P) {
 
 // Linked-cell geometry for the Tosi-Fumi kernel: about 16 ions per cell, at least one
 // cell per side; the warps (one per 32 ions in cell order) split the partner cells so
-// that ~12k warps are in flight.
+// that ~P.tf_warps (default 12k) warps are in flight.
 void set_cells(ParticleDev& P, int nc) {
     dfree(P.cell_count); dfree(P.cell_start); dfree(P.cell_fill); dfree(P.fpart); dfree(P.epart);
     P.nc = nc < 1 ? 1 : nc;
     P.ncell = P.nc * P.nc * P.nc;
     const int nblk = (P.np + 31) / 32 > 0 ? (P.np + 31) / 32 : 1;
-    int split = (12000 + nblk - 1) / nblk;
+    const int target = P.tf_warps > 0 ? P.tf_warps : 12000;
+    int split = (target + nblk - 1) / nblk;
     P.tf_split = split < 1 ? 1 : (split > P.ncell ? P.ncell : split);
     P.cell_count = dalloc<int32_t>(P.ncell);
     P.cell_start = dalloc<int32_t>(P.ncell + 1);
@@ -259,7 +268,9 @@ int run_engine(System& s, const EngineArgs& a) {
 }
 
 // Mixed-precision solve of program `prog` (see mixed.cu); returns refinement steps or -1.
-int run_mixed(System& s, int prog, double cst) {
+// Arguments of the mixed-precision solve of program `prog` for system s (writes the new
+// field into the spare buffer; the caller rotates the buffers afterwards).
+MixedArgs mixed_args(System& s, int prog, double cst) {
     GridState& G = s.G;
     ensure_mixed_levels(G);
     MixedArgs m{};
@@ -289,6 +300,23 @@ int run_mixed(System& s, int prog, double cst) {
     m.partials = s.partials;
     m.bar = s.bar;
     m.result = s.result;
+    return m;
+}
+
+// The mixed-precision program of an MD-step field update for the grid's method and its
+// right-hand-side constant (the mixed branch of solver_update_field).
+int mixed_update_prog(const GridState& G, double& cst) {
+    if (G.type == G_LCG || G.type == G_MG) {
+        cst = -4 * kPi / G.h / G.eps_s;
+        return G.type == G_LCG ? PROG_LCG_UPDATE : PROG_MG_UPDATE;
+    }
+    cst = (4 * kPi) / (G.h * G.eps_s);
+    return G.type == G_MAZE_LCG ? PROG_MAZE_LCG : PROG_MAZE_MG;
+}
+
+int run_mixed(System& s, int prog, double cst) {
+    GridState& G = s.G;
+    MixedArgs m = mixed_args(s, prog, cst);
     // MZB_PHASE_TIMING=1: time-stamp the phases of each refinement step and print them
     static const bool stamps_on = getenv("MZB_PHASE_TIMING") != nullptr;
     static unsigned long long* stamps_d = nullptr;
@@ -368,7 +396,11 @@ char* get_integrator_type_str(int i) { return (char*)kIntegratorNames[i]; }
 
 // ---------------------------------------------------------------- lifecycle
 void solver_initialize(void) {
-    if (!g) g = new System();
+    if (!g) {
+        g = new System();
+        g_systems.push_back(g);
+        g_current = (int)g_systems.size() - 1;
+    }
     const char* dev = getenv("MZB_DEVICE");
     g->device = dev ? atoi(dev) : 0;
     g_quiet = getenv("MZB_QUIET") != nullptr;
@@ -399,6 +431,7 @@ void solver_initialize_grid(int n, double L, double h, double tol, double eps, d
                             int grid_type, int precond_type) {
     System& s = sys();
     GridState& G = s.G;
+    touch(s);
     if (G.ready) free_grid(G);
     if (grid_type < 0 || grid_type > 4) fatal("invalid grid type");
     if (n < 2) fatal("grid size must be at least 2");
@@ -449,6 +482,7 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
                                  int* types, double* pos, double* vel, double* mass, double* charges,
                                  double* pot_params) {
     System& s = sys();
+    touch(s);
     if (pot_type != 0) fatal("only the Tosi-Fumi potential (TF) is supported by this build");
     if (cas_type != 0) fatal("only CIC charge assignment is supported by this build");
     if (n_typ < 1 || n_typ > 8) fatal("between 1 and 8 particle types are supported");
@@ -521,6 +555,7 @@ void solver_initialize_particles_pois_boltz(double, double, double*) {
 
 void solver_initialize_integrator(int n_p, double dt, double T, double gamma, int itg_type, int itg_enabled) {
     System& s = sys();
+    touch(s);
     (void)n_p;
     IntegratorDev& I = s.I;
     const uint64_t seed = I.seed;
@@ -553,12 +588,12 @@ int solver_update_charges(void) {
     if (flag) fatal("charge spreading: more than 2048 ions reach one 4x4x32 grid tile");
     const double q_loc = s.red_h[0];
     int res = 0;
-    if (fabs(g_q_tot - q_loc) > 1e-6) {
+    if (fabs(s.q_tot - q_loc) > 1e-6) {
         res = 1;
-        printf("Charge conservation error: q_tot = %.6f, q_tot_loc = %.6f\n", g_q_tot, q_loc);
+        printf("Charge conservation error: q_tot = %.6f, q_tot_loc = %.6f\n", s.q_tot, q_loc);
         exit(1);
     }
-    g_q_tot = q_loc;
+    s.q_tot = q_loc;
     return res;
 }
 
@@ -707,6 +742,7 @@ int solver_check_thermostat(void) {  // solver_md.c:210-221
         if (fabs(temp - s.I.T) < 100) {
             res = 1;
             s.I.enabled = 0;
+            touch(s);
             if (s.I.type == 0) {
                 s.I.c1 = 1.0;
                 s.I.c2 = 1.0;
@@ -720,6 +756,7 @@ void solver_rescale_velocities(void) { mzb::rescale_velocities(parts(), sys().st
 
 void solver_finalize(void) {
     if (!g) return;
+    touch(*g);
     if (g->stream) cudaStreamSynchronize(g->stream);
     if (g->G.ready) free_grid(g->G);
     if (g->parts_ready) free_particles(g->P);
@@ -1040,6 +1077,7 @@ void mzb_set_cell_grid(int nc) {
     ParticleDev& P = parts();
     sync();
     set_cells(P, nc);
+    touch(sys());
 }
 
 // Build the linked cells for the current positions and copy them out: start has
@@ -1070,13 +1108,17 @@ void mzb_philox_normals(uint64_t call, double* out) {
     cudaFree(d);
 }
 
-void mzb_set_seed(uint64_t seed) { sys().I.seed = seed; }
+void mzb_set_seed(uint64_t seed) {
+    sys().I.seed = seed;
+    touch(sys());
+}
 
 // Field-solve precision of the current grid: 0 = the reference's FP64 algorithms,
 // 1 = FP32 multigrid with FP64 iterative refinement to the same (or an overriding)
 // tolerance. Grids that cannot be coarsened three times, and FFT, stay FP64.
 void mzb_set_precision(int mode, double tol_override) {
     GridState& G = grid();
+    touch(sys());
     G.precision = mode == 1 ? 1 : 0;
     G.mixed_tol = tol_override;
 }
@@ -1113,6 +1155,473 @@ int solver_md_step(int n_steps) {
     }
     sync();
     return res;
+}
+
+}  // extern "C"
+
+// ====================================================================================
+// Several resident systems and the batched step (this build's extension; the reference
+// holds one system per process, solver_md.c:12-14).
+//
+// A system handle selects which system the reference-ABI calls act on. mzb_batch_step
+// advances a set of systems together: per MD step one CUDA graph forks a branch per
+// system for integrator part 1 + charge spreading (+ a device-side charge check), joins
+// into ONE cooperative launch that runs every system's mixed-precision field solve on its
+// own range of CTAs (mixed_batch_kernel), and forks again for field + pair + total forces
+// and integrator part 2. The graph bakes in each system's buffer pointers, which rotate
+// with period 3 after every solve, so up to three graphs per membership are cached.
+// ====================================================================================
+namespace mzb {
+namespace {
+
+__global__ void k_charge_check(const double* red, double* qtot, int* err, const int* flags) {
+    const double q = red[0];
+    if (fabs(*qtot - q) > 1e-6) err[0] = 1;  // solver_md.c:98-102
+    *qtot = q;
+    if (flags[0]) err[1] = 1;
+}
+__global__ void k_solve_check(const int* result, int* err) {
+    if (result[0] < 0 || result[1] != 0) err[2] = 1;
+}
+
+struct BatchGraph {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec = nullptr;
+    MixedArgs* list_d = nullptr;
+    int* start_d = nullptr;
+    unsigned long long launches = 0;
+};
+
+struct Batch {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork1 = nullptr, fork2 = nullptr, t0 = nullptr, t1 = nullptr;
+    std::vector<cudaEvent_t> join1, join2;
+    std::vector<BatchGraph> graphs;
+    double alpha = 1.0;  // team size ~ (grid points)^alpha (autotuned)
+};
+Batch g_batchst;
+
+void release_graph(BatchGraph& bg) {
+    if (bg.exec) cudaGraphExecDestroy(bg.exec);
+    if (bg.list_d) cudaFree(bg.list_d);
+    if (bg.start_d) cudaFree(bg.start_d);
+    bg = BatchGraph{};
+}
+
+void batch_clear_graphs() {
+    for (auto& bg : g_batchst.graphs) release_graph(bg);
+    g_batchst.graphs.clear();
+}
+
+void batch_events(int nsys) {
+    Batch& B = g_batchst;
+    int dev;
+    MZB_CHECK(cudaGetDevice(&dev));
+    if (B.device != dev) {
+        MZB_CHECK(cudaStreamCreateWithFlags(&B.stream, cudaStreamNonBlocking));
+        MZB_CHECK(cudaEventCreateWithFlags(&B.fork1, cudaEventDisableTiming));
+        MZB_CHECK(cudaEventCreateWithFlags(&B.fork2, cudaEventDisableTiming));
+        MZB_CHECK(cudaEventCreate(&B.t0));
+        MZB_CHECK(cudaEventCreate(&B.t1));
+        B.device = dev;
+    }
+    while ((int)B.join1.size() < nsys) {
+        cudaEvent_t e1, e2;
+        MZB_CHECK(cudaEventCreateWithFlags(&e1, cudaEventDisableTiming));
+        MZB_CHECK(cudaEventCreateWithFlags(&e2, cudaEventDisableTiming));
+        B.join1.push_back(e1);
+        B.join2.push_back(e2);
+    }
+}
+
+System& checked_system(int h) {
+    if (h < 0 || h >= (int)g_systems.size() || !g_systems[h]) fatal("batched step: invalid system handle");
+    System& s = *g_systems[h];
+    if (!s.G.ready || !s.parts_ready || !s.integ_ready) fatal("batched step: system is not fully initialised");
+    if (s.G.type == G_FFT || s.G.precision != 1 || !mixed_supported(s.G))
+        fatal("batched step: every system must use the mixed-precision (FP32+refine) field solve");
+    return s;
+}
+
+// Device-side state a batched step needs (charge total, error flags, Philox counter).
+void batch_prepare(System& s) {
+    if (!s.qtot_d) {
+        s.qtot_d = dalloc<double>(1);
+        s.err_d = dalloc<int>(4);
+        MZB_CHECK(cudaMemset(s.err_d, 0, 4 * sizeof(int)));
+    }
+    if (!s.I.ocalls_d) {
+        s.I.ocalls_d = dalloc<uint64_t>(1);
+        touch(s);
+    }
+    MZB_CHECK(cudaMemcpy(s.qtot_d, &s.q_tot, sizeof(double), cudaMemcpyHostToDevice));
+    MZB_CHECK(cudaMemcpy(s.I.ocalls_d, &s.I.ocalls, sizeof(uint64_t), cudaMemcpyHostToDevice));
+}
+
+// Team partition of nblocks CTAs: at least one per system, the rest in proportion to
+// (grid points)^alpha by largest remainder.
+std::vector<int> team_starts(const std::vector<System*>& ss, int nblocks, double alpha) {
+    const int n = (int)ss.size();
+    std::vector<double> w(n);
+    double tot = 0.0;
+    for (int r = 0; r < n; r++) {
+        w[r] = pow((double)ss[r]->G.m, alpha);
+        tot += w[r];
+    }
+    const int rem = nblocks - n;
+    std::vector<int> cnt(n, 1);
+    std::vector<std::pair<double, int>> frac(n);
+    int used = 0;
+    for (int r = 0; r < n; r++) {
+        const double share = rem * w[r] / tot;
+        const int f = (int)floor(share);
+        cnt[r] += f;
+        used += f;
+        frac[r] = {share - f, r};
+    }
+    std::sort(frac.begin(), frac.end(), [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+        return a.first > b.first || (a.first == b.first && a.second < b.second);
+    });
+    for (int k = 0; used < rem; k++, used++) cnt[frac[k % n].second]++;
+    std::vector<int> start(n + 1, 0);
+    for (int r = 0; r < n; r++) start[r + 1] = start[r] + cnt[r];
+    return start;
+}
+
+void stage_particles_before_solve(System& s) {
+    ParticleDev& P = s.P;
+    integrator_part1(P, s.I, s.stream);
+    spread_charges(P, s.G.q, s.G.n, s.G.h, s.stream);
+    count_launch();
+    k_charge_check<<<1, 1, 0, s.stream>>>(P.red, s.qtot_d, s.err_d, P.flags);
+}
+
+void stage_particles_after_solve(System& s) {
+    ParticleDev& P = s.P;
+    count_launch();
+    k_solve_check<<<1, 1, 0, s.stream>>>(s.result, s.err_d);
+    field_forces(P, s.G.buf[s.G.ispare], s.G.n, s.G.h, s.stream);  // the field the solve wrote
+    build_cells(P, s.stream);
+    tf_forces(P, s.stream);
+    total_forces(P, s.stream);
+    integrator_part2(P, s.I, s.stream);
+}
+
+// Build (or find) the graph of one batched MD step for the systems' current state.
+BatchGraph& batch_graph(const std::vector<int>& handles, const std::vector<System*>& ss) {
+    Batch& B = g_batchst;
+    std::vector<uint64_t> key;
+    key.push_back((uint64_t)(B.alpha * 1e6));
+    for (size_t r = 0; r < ss.size(); r++) {
+        key.push_back((uint64_t)handles[r]);
+        key.push_back(ss[r]->epoch);
+        key.push_back((uint64_t)ss[r]->G.iphi);
+    }
+    for (auto& bg : B.graphs)
+        if (bg.key == key) return bg;
+    if (B.graphs.size() >= 6) {
+        release_graph(B.graphs.front());
+        B.graphs.erase(B.graphs.begin());
+    }
+    const int nsys = (int)ss.size();
+    std::vector<MixedArgs> list(nsys);
+    size_t smem = 0;
+    for (int r = 0; r < nsys; r++) {
+        double cst = 0.0;
+        const int prog = mixed_update_prog(ss[r]->G, cst);
+        list[r] = mixed_args(*ss[r], prog, cst);
+        smem = std::max(smem, mixed_smem_bytes(list[r]));
+    }
+    const int nblocks = mixed_grid_blocks();
+    const std::vector<int> start = team_starts(ss, nblocks, B.alpha);
+    BatchGraph bg;
+    bg.key = key;
+    MZB_CHECK(cudaMalloc(&bg.list_d, sizeof(MixedArgs) * nsys));
+    MZB_CHECK(cudaMalloc(&bg.start_d, sizeof(int) * (nsys + 1)));
+    MZB_CHECK(cudaMemcpy(bg.list_d, list.data(), sizeof(MixedArgs) * nsys, cudaMemcpyHostToDevice));
+    MZB_CHECK(cudaMemcpy(bg.start_d, start.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice));
+
+    const unsigned long long l0 = g_kernel_launches;
+    cudaGraph_t graph = nullptr;
+    MZB_CHECK(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
+    MZB_CHECK(cudaEventRecord(B.fork1, B.stream));
+    for (int r = 0; r < nsys; r++) {
+        MZB_CHECK(cudaStreamWaitEvent(ss[r]->stream, B.fork1, 0));
+        stage_particles_before_solve(*ss[r]);
+        MZB_CHECK(cudaEventRecord(B.join1[r], ss[r]->stream));
+        MZB_CHECK(cudaStreamWaitEvent(B.stream, B.join1[r], 0));
+    }
+    for (int r = 0; r < nsys; r++) MZB_CHECK(cudaMemsetAsync(ss[r]->bar, 0, sizeof(GridBarrier), B.stream));
+    mixed_batch_launch(bg.list_d, bg.start_d, nsys, nblocks, smem, B.stream);
+    MZB_CHECK(cudaEventRecord(B.fork2, B.stream));
+    for (int r = 0; r < nsys; r++) {
+        MZB_CHECK(cudaStreamWaitEvent(ss[r]->stream, B.fork2, 0));
+        stage_particles_after_solve(*ss[r]);
+        MZB_CHECK(cudaEventRecord(B.join2[r], ss[r]->stream));
+        MZB_CHECK(cudaStreamWaitEvent(B.stream, B.join2[r], 0));
+    }
+    MZB_CHECK(cudaStreamEndCapture(B.stream, &graph));
+    bg.launches = g_kernel_launches - l0;
+    g_kernel_launches = l0;  // counted when the graph runs
+    MZB_CHECK(cudaGraphInstantiate(&bg.exec, graph, 0));
+    MZB_CHECK(cudaGraphDestroy(graph));
+    B.graphs.push_back(bg);
+    return B.graphs.back();
+}
+
+std::vector<System*> batch_systems(const int* handles, int nsys) {
+    if (nsys < 1) fatal("batched step: no systems");
+    std::vector<System*> ss;
+    for (int r = 0; r < nsys; r++) {
+        System& s = checked_system(handles[r]);
+        for (System* o : ss)
+            if (o == &s) fatal("batched step: a system is listed twice");
+        ss.push_back(&s);
+    }
+    if (nsys > mixed_grid_blocks()) fatal("batched step: more systems than SMs");
+    return ss;
+}
+
+// Wait for the systems' own streams, set up their device-side state.
+void batch_begin(std::vector<System*>& ss) {
+    batch_events((int)ss.size());
+    for (System* s : ss) {
+        MZB_CHECK(cudaStreamSynchronize(s->stream));
+        batch_prepare(*s);
+    }
+}
+
+// Wait for the batch, copy the device-side state back and report errors the way the
+// per-call path does (solver_md.c:98-102 exits on a charge error).
+int batch_end(std::vector<System*>& ss, const int* handles) {
+    MZB_CHECK(cudaStreamSynchronize(g_batchst.stream));
+    int status = 0;
+    for (size_t r = 0; r < ss.size(); r++) {
+        System& s = *ss[r];
+        int err[4];
+        double q = 0.0;
+        MZB_CHECK(cudaMemcpy(err, s.err_d, sizeof(err), cudaMemcpyDeviceToHost));
+        MZB_CHECK(cudaMemcpy(&q, s.qtot_d, sizeof(double), cudaMemcpyDeviceToHost));
+        MZB_CHECK(cudaMemcpy(&s.I.ocalls, s.I.ocalls_d, sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        if (err[1]) fatal("charge spreading: more than 2048 ions reach one 4x4x32 grid tile");
+        if (err[0]) {
+            printf("Charge conservation error in system %d: q_tot = %.6f\n", handles[r], s.q_tot);
+            exit(1);
+        }
+        if (err[2]) status = -1;
+        s.q_tot = q;
+        MZB_CHECK(cudaMemset(s.err_d, 0, 4 * sizeof(int)));
+    }
+    return status;
+}
+
+}  // namespace
+}  // namespace mzb
+
+extern "C" {
+
+// Create an empty system and select it; returns its handle. Initialise it with the
+// reference calls (solver_initialize, solver_initialize_grid, ...).
+int mzb_system_create(void) {
+    System* s = new System();
+    g_systems.push_back(s);
+    g_current = (int)g_systems.size() - 1;
+    g = s;
+    return g_current;
+}
+
+// Make `handle` the system the reference-ABI calls act on; -1 if it does not exist.
+int mzb_system_select(int handle) {
+    if (handle < 0 || handle >= (int)g_systems.size() || !g_systems[handle]) return -1;
+    g_current = handle;
+    g = g_systems[handle];
+    return 0;
+}
+
+int mzb_system_current(void) { return g_current; }
+
+// Free a system and everything it holds on the device; -1 if it does not exist.
+int mzb_system_destroy(int handle) {
+    if (handle < 0 || handle >= (int)g_systems.size() || !g_systems[handle]) return -1;
+    System* prev = g;
+    const int prev_h = g_current;
+    g = g_systems[handle];
+    solver_finalize();
+    System& s = *g;
+    batch_clear_graphs();
+    if (s.stream) cudaStreamDestroy(s.stream);
+    if (s.ev0) cudaEventDestroy(s.ev0);
+    if (s.ev1) cudaEventDestroy(s.ev1);
+    dfree(s.partials);
+    dfree(s.bar);
+    dfree(s.result);
+    dfree(s.scratch_d);
+    dfree(s.qtot_d);
+    dfree(s.err_d);
+    dfree(s.I.ocalls_d);
+    if (s.result_h) cudaFreeHost(s.result_h);
+    if (s.red_h) cudaFreeHost(s.red_h);
+    delete g_systems[handle];
+    g_systems[handle] = nullptr;
+    if (prev_h == handle) {
+        g = nullptr;
+        g_current = -1;
+    } else {
+        g = prev;
+        g_current = prev_h;
+    }
+    return 0;
+}
+
+// Advance the listed systems (FP32+refine field solve, set up and bootstrapped through
+// the reference calls) by n_steps MD steps together, one CUDA graph per step (see the
+// section comment). Returns 0, or -1 if any field solve did not converge.
+int mzb_batch_step(const int* handles, int nsys, int n_steps) {
+    std::vector<System*> ss = batch_systems(handles, nsys);
+    batch_begin(ss);
+    std::vector<int> hv(handles, handles + nsys);
+    for (int k = 0; k < n_steps; k++) {
+        BatchGraph& bg = batch_graph(hv, ss);
+        MZB_CHECK(cudaGraphLaunch(bg.exec, g_batchst.stream));
+        g_kernel_launches += bg.launches;
+        for (System* s : ss) {  // phi_prev <- old phi, phi <- the solve's output
+            GridState& G = s->G;
+            const int old = G.iphi;
+            G.iphi = G.ispare;
+            G.ispare = G.iprev;
+            G.iprev = old;
+        }
+    }
+    return batch_end(ss, handles);
+}
+
+// Choose the batched step's team partition exponent (CTAs per system ~ points^alpha)
+// and the pair-force kernel's warp target by timing candidates on the listed systems:
+// the field solves alone (their inputs are left unchanged; the MaZe unknown y is saved
+// and restored) and the force stages alone (they only rewrite forces). Writes
+// {alpha, warps, solve ms, forces ms} into out[0..3] and keeps the choice.
+int mzb_batch_autotune(const int* handles, int nsys, double* out) {
+    std::vector<System*> ss = batch_systems(handles, nsys);
+    batch_begin(ss);
+    Batch& B = g_batchst;
+    const int nblocks = mixed_grid_blocks();
+    std::vector<MixedArgs> list(nsys);
+    size_t smem = 0;
+    for (int r = 0; r < nsys; r++) {
+        double cst = 0.0;
+        const int prog = mixed_update_prog(ss[r]->G, cst);
+        list[r] = mixed_args(*ss[r], prog, cst);
+        smem = std::max(smem, mixed_smem_bytes(list[r]));
+    }
+    MixedArgs* list_d = nullptr;
+    int* start_d = nullptr;
+    MZB_CHECK(cudaMalloc(&list_d, sizeof(MixedArgs) * nsys));
+    MZB_CHECK(cudaMalloc(&start_d, sizeof(int) * (nsys + 1)));
+    MZB_CHECK(cudaMemcpy(list_d, list.data(), sizeof(MixedArgs) * nsys, cudaMemcpyHostToDevice));
+    std::vector<double*> ysave(nsys, nullptr);
+    for (int r = 0; r < nsys; r++) {
+        const int t = ss[r]->G.type;
+        if (t == G_MAZE_LCG || t == G_MAZE_MG) {
+            ysave[r] = dalloc<double>(ss[r]->G.m);
+            MZB_CHECK(cudaMemcpy(ysave[r], ss[r]->G.y, sizeof(double) * ss[r]->G.m, cudaMemcpyDeviceToDevice));
+        }
+    }
+    auto restore_y = [&]() {
+        for (int r = 0; r < nsys; r++)
+            if (ysave[r])
+                MZB_CHECK(cudaMemcpyAsync(ss[r]->G.y, ysave[r], sizeof(double) * ss[r]->G.m, cudaMemcpyDeviceToDevice,
+                                          B.stream));
+    };
+    const double alphas[] = {1.0, 0.8, 0.6, 0.4};
+    double best_alpha = B.alpha, best_solve = 1e30;
+    for (double alpha : alphas) {
+        const std::vector<int> start = team_starts(ss, nblocks, alpha);
+        MZB_CHECK(cudaMemcpy(start_d, start.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice));
+        float tot = 0.f;
+        for (int rep = 0; rep < 3; rep++) {
+            restore_y();
+            for (int r = 0; r < nsys; r++) MZB_CHECK(cudaMemsetAsync(ss[r]->bar, 0, sizeof(GridBarrier), B.stream));
+            MZB_CHECK(cudaEventRecord(B.t0, B.stream));
+            mixed_batch_launch(list_d, start_d, nsys, nblocks, smem, B.stream);
+            MZB_CHECK(cudaEventRecord(B.t1, B.stream));
+            MZB_CHECK(cudaStreamSynchronize(B.stream));
+            float ms = 0.f;
+            MZB_CHECK(cudaEventElapsedTime(&ms, B.t0, B.t1));
+            if (rep > 0) tot += ms;
+        }
+        if (tot / 2 < best_solve) {
+            best_solve = tot / 2;
+            best_alpha = alpha;
+        }
+    }
+    restore_y();
+    MZB_CHECK(cudaStreamSynchronize(B.stream));
+    for (double* p : ysave)
+        if (p) cudaFree(p);
+    cudaFree(list_d);
+    cudaFree(start_d);
+    B.alpha = best_alpha;
+
+    const int targets[] = {2000, 4000, 8000, 12000, 24000};
+    int best_target = 12000;
+    double best_forces = 1e30;
+    for (int target : targets) {
+        for (System* s : ss) {
+            s->P.tf_warps = target;
+            set_cells(s->P, s->P.nc);
+        }
+        float tot = 0.f;
+        for (int rep = 0; rep < 3; rep++) {
+            MZB_CHECK(cudaEventRecord(B.t0, B.stream));
+            MZB_CHECK(cudaEventRecord(B.fork1, B.stream));
+            for (int r = 0; r < nsys; r++) {
+                MZB_CHECK(cudaStreamWaitEvent(ss[r]->stream, B.fork1, 0));
+                build_cells(ss[r]->P, ss[r]->stream);
+                tf_forces(ss[r]->P, ss[r]->stream);
+                MZB_CHECK(cudaEventRecord(B.join1[r], ss[r]->stream));
+                MZB_CHECK(cudaStreamWaitEvent(B.stream, B.join1[r], 0));
+            }
+            MZB_CHECK(cudaEventRecord(B.t1, B.stream));
+            MZB_CHECK(cudaStreamSynchronize(B.stream));
+            float ms = 0.f;
+            MZB_CHECK(cudaEventElapsedTime(&ms, B.t0, B.t1));
+            if (rep > 0) tot += ms;
+        }
+        if (tot / 2 < best_forces) {
+            best_forces = tot / 2;
+            best_target = target;
+        }
+    }
+    for (System* s : ss) {
+        s->P.tf_warps = best_target;
+        set_cells(s->P, s->P.nc);
+        touch(*s);
+    }
+    batch_clear_graphs();
+    if (out) {
+        out[0] = best_alpha;
+        out[1] = best_target;
+        out[2] = best_solve;
+        out[3] = best_forces;
+    }
+    return 0;
+}
+
+// Bytes of device memory one system of n^3 grid points and n_p ions holds with the
+// FP32+refine field solve (fields, multigrid levels, particle and pair-force arrays);
+// the request loop admits jobs against an HBM budget with it.
+double mzb_system_footprint(int n, int n_p) {
+    const double m = (double)n * n * n;
+    double levels = 0.0;
+    int sizes[kMixedMaxLevels];
+    const int L = mixed_levels(n, sizes);
+    for (int l = 0; l < L; l++) levels += 3.0 * 4.0 * (double)sizes[l] * sizes[l] * sizes[l];
+    const double grid = 8.0 * m * 10.0;  // q, phi x3, y, r, p0, p1, Ap, tmp
+    const int nblk = (n_p + 31) / 32 > 0 ? (n_p + 31) / 32 : 1;
+    const double split = std::min(12000.0 / nblk + 1.0, 4096.0);
+    const double parts = (double)n_p * (8.0 * 3 * 7 + 4.0 * 8) + split * n_p * 3 * 8.0;
+    return grid + levels + parts + 64.0 * 1024 * 1024;
 }
 
 }  // extern "C"

@@ -50,14 +50,54 @@ __device__ __forceinline__ void stamp_outer(const MixedArgs& a, int outer, int k
     if (outer < 8) stamp(a, 2 + 8 * outer + k);
 }
 
+// The CTAs that work one system: every CTA of a single-system launch, or one system's
+// contiguous range of CTAs in a batched launch (mixed_batch_kernel).
+struct Team {
+    int nblk, b;        // CTAs in the team, this CTA's index in it
+    GridBarrier* bar;   // the team's barrier (zeroed before the launch)
+    double* partials;   // >= 4 nblk doubles
+};
+
+// Barrier over the team's CTAs (the monotonic barrier of tma.cuh with the team's count).
+__device__ __forceinline__ bool team_sync(const Team& t, unsigned int& epoch) {
+    __shared__ int ok_sh;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(&t.bar->count) : "memory");
+        const unsigned int target = (epoch + 1u) * (unsigned)t.nblk;
+        const unsigned long long t0 = global_ns();
+        unsigned int polls = 0;
+        while (ld_relaxed_u32(&t.bar->count) < target) {
+            if ((++polls & 255u) == 0u) {
+                if (ld_relaxed_u32(&t.bar->err) != 0u) {
+                    ok = 0;
+                    break;
+                }
+                if (global_ns() - t0 > kBarrierTimeoutNs) {
+                    atomicOr(&t.bar->err, 1u);
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        asm volatile("fence.acq_rel.gpu;" ::: "memory");
+        if (ok && ld_relaxed_u32(&t.bar->err) != 0u) ok = 0;
+        ok_sh = ok;
+    }
+    epoch++;
+    __syncthreads();
+    return ok_sh != 0;
+}
+
 // ---- loops ----
 
-// whole-grid loops (all CTAs): a warp per row of k
+// whole-team loops: a warp per row of k
 template <class F>
-__device__ __forceinline__ void grid_pts(int n, F&& f) {
+__device__ __forceinline__ void grid_pts(const Team& tm, int n, F&& f) {
     const int lane = threadIdx.x & 31;
-    const long gw = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const long nw = (long)gridDim.x * (blockDim.x >> 5);
+    const long gw = (long)tm.b * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const long nw = (long)tm.nblk * (blockDim.x >> 5);
     const long rows = (long)n * n;
     for (long row = gw; row < rows; row += nw) {
         const int i = (int)(row / n), j = (int)(row - (long)i * n);
@@ -99,11 +139,11 @@ __device__ __forceinline__ Nb nb_of(int n, int i, int j, int k) {
 }
 
 // Grid reduction of one sum and one max (deterministic fixed-order gather).
-__device__ bool reduce_sum_max(double& s, double& mx, const MixedArgs& a, unsigned& epoch, int& seq) {
+__device__ bool reduce_sum_max(double& s, double& mx, const Team& tm, unsigned& epoch, int& seq) {
     __shared__ double sh[2][32];
     __shared__ double res[2];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const long G = gridDim.x;
+    const long G = tm.nblk;
     s = warp_sum(s);
     mx = warp_max(mx);
     if (lane == 0) {
@@ -111,17 +151,17 @@ __device__ bool reduce_sum_max(double& s, double& mx, const MixedArgs& a, unsign
         sh[1][w] = mx;
     }
     __syncthreads();
-    double* part = a.partials + (long)(seq & 1) * 2 * G;
+    double* part = tm.partials + (long)(seq & 1) * 2 * G;
     if (w == 0) {
         double v0 = lane < nwarp ? sh[0][lane] : 0.0, v1 = lane < nwarp ? sh[1][lane] : 0.0;
         v0 = warp_sum(v0);
         v1 = warp_max(v1);
         if (lane == 0) {
-            part[blockIdx.x] = v0;
-            part[G + blockIdx.x] = v1;
+            part[tm.b] = v0;
+            part[G + tm.b] = v1;
         }
     }
-    const bool ok = grid_sync_mono(a.bar, epoch);
+    const bool ok = team_sync(tm, epoch);
     if (w == 0) {
         double v0 = 0.0, v1 = 0.0;
         for (long b = lane; b < G; b += 32) {
@@ -243,11 +283,11 @@ __device__ __forceinline__ Rows rows_of(int n, int i, int j) {
     return Rows{(i * n + j) * h, (im * n + j) * h, (ip * n + j) * h, (i * n + jm) * h, (i * n + jp) * h};
 }
 
-// warp per row (i,j) of an n x n set of rows, over all CTAs
+// warp per row (i,j) of an n x n set of rows, over the team's CTAs
 template <class F>
-__device__ __forceinline__ void grid_rows(int n, F&& f) {
-    const int gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int nw = gridDim.x * (blockDim.x >> 5);
+__device__ __forceinline__ void grid_rows(const Team& tm, int n, F&& f) {
+    const int gw = tm.b * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nw = tm.nblk * (blockDim.x >> 5);
     const int rows = n * n;
     for (int row = gw; row < rows; row += nw) {
         const int i = row / n;
@@ -307,14 +347,14 @@ __device__ __forceinline__ void split_nb_sums(const float* xo, const Rows& o, in
 }
 
 // half-sweep of colour c; when acc is not null the new values are summed into it
-__device__ void split_gs(int n, int c, const float* b, float* x, double* acc) {
+__device__ void split_gs(const Team& tm, int n, int c, const float* b, float* x, double* acc) {
     const int lane = threadIdx.x & 31, h = n >> 1;
     const int hp = h * n * n;
     const float* xo = x + (1 - c) * hp;
     float* xc = x + c * hp;
     const float* bc = b + c * hp;
     double s_acc = 0.0;
-    grid_rows(n, [&](int i, int j) {
+    grid_rows(tm, n, [&](int i, int j) {
         const Rows o = rows_of(n, i, j);
         const int s = (i + j + c) & 1;
         for (int k0 = 0; k0 < h; k0 += 32 * kBatchSweep) {
@@ -340,11 +380,11 @@ __device__ void split_gs(int n, int c, const float* b, float* x, double* acc) {
 }
 
 // red residual r_red = b_red - L x at the red points (black residuals are zero)
-__device__ void split_resid_red(int n, const float* b, const float* x, float* r) {
+__device__ void split_resid_red(const Team& tm, int n, const float* b, const float* x, float* r) {
     const int lane = threadIdx.x & 31, h = n >> 1;
     const int hp = h * n * n;
     const float* x1 = x + hp;
-    grid_rows(n, [&](int i, int j) {
+    grid_rows(tm, n, [&](int i, int j) {
         const Rows o = rows_of(n, i, j);
         const int s = (i + j) & 1;
         for (int k0 = 0; k0 < h; k0 += 32 * kBatchSweep) {
@@ -388,10 +428,10 @@ __device__ __forceinline__ float split_restrict_value(int n, const float* r, int
 }
 
 // coarse b = 4 R27(r), coarse x = its first red half-sweep from 0 (both split layout)
-__device__ void split_restrict(int n, const float* r, float* bc, float* xc) {
+__device__ void split_restrict(const Team& tm, int n, const float* r, float* bc, float* xc) {
     const int lane = threadIdx.x & 31, nc = n / 2, hc = nc >> 1;
     const int hpc = hc * nc * nc;
-    grid_rows(nc, [&](int I, int J) {
+    grid_rows(tm, nc, [&](int I, int J) {
         for (int k0 = 0; k0 < nc; k0 += 32 * kBatch) {
             float v[kBatch];
 #pragma unroll
@@ -414,11 +454,11 @@ __device__ void split_restrict(int n, const float* r, float* bc, float* xc) {
 }
 
 // fine black x += P(coarse x), trilinear (both split layout)
-__device__ void split_prolong_black(int n, const float* xc, float* x) {
+__device__ void split_prolong_black(const Team& tm, int n, const float* xc, float* x) {
     const int lane = threadIdx.x & 31, h = n >> 1, nc = n / 2, hc = nc >> 1;
     const int hp = h * n * n, hpc = hc * nc * nc;
     float* x1 = x + hp;
-    grid_rows(n, [&](int i, int j) {
+    grid_rows(tm, n, [&](int i, int j) {
         const int s1 = (i + j + 1) & 1;  // black points of row (i,j) sit at k = 2 kk + s1
         const int ci = i >> 1, cj = j >> 1;
         const int ci1 = ci + 1 == nc ? 0 : ci + 1, cj1 = cj + 1 == nc ? 0 : cj + 1;
@@ -556,13 +596,13 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm) {
 // Grid-wide red-black sweeps of level l: `half_sweeps` colours starting at first_colour,
 // a grid barrier after each except (when skip_last_barrier) the last. When esum is not
 // null the values written in the last two half-sweeps are summed into it.
-__device__ bool grid_smooth(const MixedArgs& a, int l, int first_colour, int half_sweeps, unsigned& epoch,
-                            double* esum, bool skip_last_barrier) {
+__device__ bool grid_smooth(const MixedArgs& a, const Team& tm, int l, int first_colour, int half_sweeps,
+                            unsigned& epoch, double* esum, bool skip_last_barrier) {
     for (int h = 0; h < half_sweeps; h++) {
-        split_gs(a.lev_n[l], (first_colour + h) & 1, a.lev_b[l], a.lev_x[l],
+        split_gs(tm, a.lev_n[l], (first_colour + h) & 1, a.lev_b[l], a.lev_x[l],
                  esum != nullptr && h >= half_sweeps - 2 ? esum : nullptr);
         if (h == half_sweeps - 1 && skip_last_barrier) break;
-        if (!grid_sync_mono(a.bar, epoch)) return false;
+        if (!team_sync(tm, epoch)) return false;
     }
     return true;
 }
@@ -570,55 +610,55 @@ __device__ bool grid_smooth(const MixedArgs& a, int l, int first_colour, int hal
 // One V-cycle for the correction e = lev_x[0] of rhs lev_b[0], whose first red half-sweep
 // has been done by the residual pass. Ends after the last half-sweep of level 0 without a
 // barrier, with this thread's share of sum(e) in esum.
-__device__ bool vcycle(const MixedArgs& a, float* sm, unsigned& epoch, double& esum, int outer) {
+__device__ bool vcycle(const MixedArgs& a, const Team& tm, float* sm, unsigned& epoch, double& esum, int outer) {
     const int L = a.nlev, ls = a.lsmall;
     const int lg = ls < L ? ls : L - 1;  // levels 0..lg-1 are smoothed and restricted on the grid
     for (int l = 0; l < lg; l++) {
-        if (!grid_smooth(a, l, 1, 2 * a.nu1 - 1, epoch, nullptr, false)) return false;
-        split_resid_red(a.lev_n[l], a.lev_b[l], a.lev_x[l], a.lev_r[l]);
-        if (!grid_sync_mono(a.bar, epoch)) return false;
+        if (!grid_smooth(a, tm, l, 1, 2 * a.nu1 - 1, epoch, nullptr, false)) return false;
+        split_resid_red(tm, a.lev_n[l], a.lev_b[l], a.lev_x[l], a.lev_r[l]);
+        if (!team_sync(tm, epoch)) return false;
         if (l + 1 < ls) {
-            split_restrict(a.lev_n[l], a.lev_r[l], a.lev_b[l + 1], a.lev_x[l + 1]);
-            if (!grid_sync_mono(a.bar, epoch)) return false;
+            split_restrict(tm, a.lev_n[l], a.lev_r[l], a.lev_b[l + 1], a.lev_x[l + 1]);
+            if (!team_sync(tm, epoch)) return false;
         }
     }
     stamp_outer(a, outer, 2);
     if (ls < L) {
-        if (blockIdx.x == 0) small_vcycle(a, sm);
-        if (!grid_sync_mono(a.bar, epoch)) return false;
+        if (tm.b == 0) small_vcycle(a, sm);
+        if (!team_sync(tm, epoch)) return false;
     } else {
-        if (!grid_smooth(a, L - 1, 1, 2 * a.coarse_sweeps - 1, epoch, nullptr, false)) return false;
+        if (!grid_smooth(a, tm, L - 1, 1, 2 * a.coarse_sweeps - 1, epoch, nullptr, false)) return false;
     }
     stamp_outer(a, outer, 3);
     for (int l = lg - 1; l >= 0; l--) {
-        split_prolong_black(a.lev_n[l], a.lev_x[l + 1], a.lev_x[l]);
-        if (!grid_sync_mono(a.bar, epoch)) return false;
-        if (!grid_smooth(a, l, 0, 2 * a.nu2, epoch, l == 0 ? &esum : nullptr, l == 0)) return false;
+        split_prolong_black(tm, a.lev_n[l], a.lev_x[l + 1], a.lev_x[l]);
+        if (!team_sync(tm, epoch)) return false;
+        if (!grid_smooth(a, tm, l, 0, 2 * a.nu2, epoch, l == 0 ? &esum : nullptr, l == 0)) return false;
     }
     return true;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
-    extern __shared__ float sm[];
+// The solve of one system by one team of CTAs.
+__device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, float* sm) {
     const int n = a.n;
     unsigned epoch = 0;
     int seq = 0;
     bool ok = true;
     int result = -1;
-    stamp(a, 0);
+    if (tm.b == 0) stamp(a, 0);
 
     // ---- set-up: right-hand side B and solution X (FP64), as the FP64 programs ----
     double* X = a.phi_new;
     const double* B = a.tmp;
     if (a.prog == PROG_INIT_FIELD) {         // y = 0, phi = 0 start, b = c q
-        grid_pts(n, [&](int i, int j, int k) {
+        grid_pts(tm, n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             a.y[c] = 0.0;
             a.phi_new[c] = 0.0;
             a.tmp[c] = a.q[c] * a.c;
         });
     } else if (a.prog == PROG_LCG_UPDATE) {  // y = c q; start from phi_prev (old phi)
-        grid_pts(n, [&](int i, int j, int k) {
+        grid_pts(tm, n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             const double bq = a.q[c] * a.c;
             a.y[c] = bq;
@@ -626,14 +666,14 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
             a.phi_new[c] = a.phi_old[c];
         });
     } else if (a.prog == PROG_MG_UPDATE) {   // phi = 2 phi - phi_prev (start), b = c q
-        grid_pts(n, [&](int i, int j, int k) {
+        grid_pts(tm, n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             a.phi_new[c] = 2 * a.phi_old[c] - a.phi_prev[c];
             a.tmp[c] = a.q[c] * a.c;
         });
     } else {                                 // MaZe: phi = 2 phi - phi_prev; sigma = L phi + c q
         X = a.y;
-        grid_pts(n, [&](int i, int j, int k) {
+        grid_pts(tm, n, [&](int i, int j, int k) {
             const Nb o = nb_of(n, i, j, k);
             auto ex = [&](long q) { return 2 * a.phi_old[q] - a.phi_prev[q]; };
             double s = ex(o.ip) + ex(o.im);
@@ -645,7 +685,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
             a.tmp[o.c] = (s - ex(o.c) * 6.0) + a.c * a.q[o.c];
         });
     }
-    ok = grid_sync_mono(a.bar, epoch);
+    ok = team_sync(tm, epoch);
     stamp(a, 1);
 
     float* e = a.lev_x[0];
@@ -656,7 +696,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
         // red half-sweep from e = 0; |r|_inf
         stamp_outer(a, outer, 0);
         double s0 = 0.0, rmax = 0.0;
-        grid_pts(n, [&](int i, int j, int k) {
+        grid_pts(tm, n, [&](int i, int j, int k) {
             const Nb o = nb_of(n, i, j, k);
             double s = X[o.ip] + X[o.im];
             s = s + X[o.jp];
@@ -670,9 +710,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
             e[sx] = ((i + j + k) & 1) == 0 ? rf * (-1.0f / 6.0f) : 0.0f;
             rmax = fmax(rmax, fabs(r));
         });
-        ok = reduce_sum_max(s0, rmax, a, epoch, seq);
+        ok = reduce_sum_max(s0, rmax, tm, epoch, seq);
         stamp_outer(a, outer, 1);
-        if (a.stamps != nullptr && outer < 8 && blockIdx.x == 0 && threadIdx.x == 0)
+        if (a.stamps != nullptr && outer < 8 && tm.b == 0 && threadIdx.x == 0)
             a.stamps[2 + 8 * outer + 7] = (unsigned long long)__double_as_longlong(rmax);
         if (!ok) break;
         if (rmax <= a.tol) {
@@ -681,37 +721,65 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
         }
         if (outer >= a.max_outer) break;
         double esum = 0.0, m0 = 0.0;
-        ok = vcycle(a, sm, epoch, esum, outer);
+        ok = vcycle(a, tm, sm, epoch, esum, outer);
         if (!ok) break;
         stamp_outer(a, outer, 4);
         // mean of the correction (the periodic Laplacian's null space)
-        ok = reduce_sum_max(esum, m0, a, epoch, seq);
+        ok = reduce_sum_max(esum, m0, tm, epoch, seq);
         if (!ok) break;
         stamp_outer(a, outer, 5);
         const double emean = esum / ((double)n * n * n);
-        grid_pts(n, [&](int i, int j, int k) {
+        grid_pts(tm, n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             X[c] = X[c] + ((double)e[split_idx(n, i, j, k)] - emean);
         });
-        ok = grid_sync_mono(a.bar, epoch);
+        ok = team_sync(tm, epoch);
         stamp_outer(a, outer, 6);
         outer++;
     }
     if (ok && (a.prog == PROG_MAZE_LCG || a.prog == PROG_MAZE_MG)) {  // phi -= y
-        grid_pts(n, [&](int i, int j, int k) {
+        grid_pts(tm, n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             a.phi_new[c] = a.phi_new[c] + -1.0 * a.y[c];
         });
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (tm.b == 0 && threadIdx.x == 0) {
         a.result[0] = result;
         a.result[1] = ok ? 0 : 1;
     }
 }
 
+__global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
+    extern __shared__ float sm[];
+    const Team tm{(int)gridDim.x, (int)blockIdx.x, a.bar, a.partials};
+    mixed_body(a, tm, sm);
+}
+
+// Many systems in one launch: system r is worked by CTAs [start[r], start[r+1]).
+__global__ void __launch_bounds__(kThreads, 1)
+    mixed_batch_kernel(const MixedArgs* __restrict__ list, const int* __restrict__ start, int nsys) {
+    extern __shared__ float sm[];
+    int lo = 0, hi = nsys - 1;  // last r with start[r] <= blockIdx.x
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= (int)blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const int b0 = start[lo], b1 = start[lo + 1];
+    if ((int)blockIdx.x >= b1) return;  // CTAs past the last team (none when start[nsys] = gridDim.x)
+    __shared__ MixedArgs a;  // this system's arguments, read from shared memory
+    for (int w = threadIdx.x; w < (int)(sizeof(MixedArgs) / sizeof(int)); w += blockDim.x)
+        reinterpret_cast<int*>(&a)[w] = reinterpret_cast<const int*>(list + lo)[w];
+    __syncthreads();
+    const Team tm{b1 - b0, (int)blockIdx.x - b0, a.bar, a.partials};
+    mixed_body(a, tm, sm);
+}
+
 int g_mixed_device = -1;
 int g_mixed_blocks = 0;
 size_t g_mixed_smem_set = 0;
+int g_batch_device = -1;
+size_t g_batch_smem_set = 0;
 
 size_t small_smem_bytes(const MixedArgs& a) {
     size_t v = 0;
@@ -752,6 +820,35 @@ int mixed_small_level(int nlev, const int* sizes) {
     for (int l = 0; l < nlev; l++)
         if (sizes[l] <= kMixedSmallN) return l;
     return nlev;
+}
+
+size_t mixed_smem_bytes(const MixedArgs& a) { return small_smem_bytes(a); }
+
+int mixed_grid_blocks() {
+    int dev = 0, sms = 0;
+    MZB_CHECK(cudaGetDevice(&dev));
+    MZB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return sms;
+}
+
+void mixed_batch_launch(const MixedArgs* list, const int* start, int nsys, int nblocks, size_t smem,
+                        cudaStream_t stream) {
+    int dev;
+    MZB_CHECK(cudaGetDevice(&dev));
+    if (g_batch_device != dev || smem > g_batch_smem_set) {
+        int per_sm = 0, sms = 0;
+        if (smem > 48 * 1024)
+            MZB_CHECK(cudaFuncSetAttribute(mixed_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MZB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_batch_kernel, kThreads, smem));
+        MZB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        if (per_sm < 1 || nblocks > per_sm * sms) fatal("batched mixed solver: CTAs cannot be co-resident");
+        g_batch_device = dev;
+        g_batch_smem_set = smem > g_batch_smem_set ? smem : g_batch_smem_set;
+    }
+    void* params[] = {(void*)&list, (void*)&start, (void*)&nsys};
+    count_launch();
+    MZB_CHECK(cudaLaunchCooperativeKernel((const void*)mixed_batch_kernel, dim3(nblocks), dim3(kThreads), params, smem,
+                                          stream));
 }
 
 void mixed_launch(const MixedArgs& a, cudaStream_t stream) {

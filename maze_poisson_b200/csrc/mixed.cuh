@@ -48,5 +48,15 @@ constexpr int kMixedDirectN = 6;
 // lambda(k) = 2 cos(2 pi k1/n) + 2 cos(2 pi k2/n) + 2 cos(2 pi k3/n) - 6.
 void mixed_coarse_green(int n, float* g);
 void mixed_launch(const MixedArgs& a, cudaStream_t stream);
+// Dynamic shared memory one system's solve needs.
+size_t mixed_smem_bytes(const MixedArgs& a);
+// CTAs of a full (one per SM) launch on the current device.
+int mixed_grid_blocks();
+// Solve nsys systems in one cooperative launch of nblocks CTAs: system r (list[r], in
+// device memory) is worked by CTAs [start[r], start[r+1]), start[nsys] = nblocks, each
+// team on its own barrier (zeroed by the caller) and partials. smem is the largest
+// mixed_smem_bytes of the list.
+void mixed_batch_launch(const MixedArgs* list, const int* start, int nsys, int nblocks, size_t smem,
+                        cudaStream_t stream);
 
 }  // namespace mzb

@@ -477,6 +477,7 @@ __global__ void k_verlet2(ParticleDev P, double dt) {
 __global__ void k_ovrvo(ParticleDev P, IntegratorDev I, int part, uint64_t call) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P.np) return;
+    if (I.ocalls_d != nullptr) call = *I.ocalls_d;
     const double m = P.mass[p];
     double v[3] = {P.vel[3 * p], P.vel[3 * p + 1], P.vel[3 * p + 2]};
     auto o_block = [&]() {
@@ -503,6 +504,17 @@ __global__ void k_ovrvo(ParticleDev P, IntegratorDev I, int part, uint64_t call)
     for (int d = 0; d < 3; d++) P.vel[3 * p + d] = v[d];
 }
 
+__global__ void k_advance_counter(uint64_t* c) { *c += 1; }
+
+static void advance_ocalls(IntegratorDev& I, cudaStream_t s) {
+    if (!I.enabled) return;
+    I.ocalls++;
+    if (I.ocalls_d != nullptr) {
+        count_launch();
+        k_advance_counter<<<1, 1, 0, s>>>(I.ocalls_d);
+    }
+}
+
 void integrator_part1(ParticleDev& P, IntegratorDev& I, cudaStream_t s) {
     if (P.np == 0) return;
     if (I.type == 1) {
@@ -512,7 +524,7 @@ void integrator_part1(ParticleDev& P, IntegratorDev& I, cudaStream_t s) {
     } else {
         count_launch();
         k_ovrvo<<<(P.np + 127) / 128, 128, 0, s>>>(P, I, 1, I.ocalls);
-        if (I.enabled) I.ocalls++;
+        advance_ocalls(I, s);
     }
     MZB_CHECK(cudaGetLastError());
 }
@@ -525,7 +537,7 @@ void integrator_part2(ParticleDev& P, IntegratorDev& I, cudaStream_t s) {
     } else {
         count_launch();
         k_ovrvo<<<(P.np + 127) / 128, 128, 0, s>>>(P, I, 2, I.ocalls);
-        if (I.enabled) I.ocalls++;
+        advance_ocalls(I, s);
     }
     MZB_CHECK(cudaGetLastError());
 }

@@ -41,7 +41,8 @@ struct ParticleDev {
     int32_t* srank = nullptr;        // [np] position of ion p in cell order
     double* spos = nullptr;          // [np][3] positions in cell order
     int32_t* stype = nullptr;        // [np]
-    int tf_split = 1;                // cell-pair chunks per cell
+    int tf_split = 1;                // partner-cell chunks per block of 32 ions
+    int tf_warps = 0;                // warps the split aims at (0: 12000)
     double* fpart = nullptr;         // [tf_split][np][3]
     double* epart = nullptr;         // [ncell * tf_split]
 
@@ -71,6 +72,9 @@ struct IntegratorDev {
     double dt = 0, T = 0, c1 = 1, c2 = 1;
     uint64_t seed = 0x5eedULL;
     uint64_t ocalls = 0;  // O-blocks applied so far (Philox counter)
+    // When set (batched steps replayed from a CUDA graph), the Philox counter lives in
+    // device memory: k_ovrvo reads it and a one-thread kernel advances it.
+    uint64_t* ocalls_d = nullptr;
 };
 
 void integrator_part1(ParticleDev& P, IntegratorDev& I, cudaStream_t s);
