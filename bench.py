@@ -87,16 +87,20 @@ def level_sizes(n):
 
 def mixed_solve_bytes(n, refinements, nu1=2, nu2=2, small_n=16):
     """Algorithmic HBM bytes of one mixed solve (MD update, LCG form) that took
-    `refinements` V-cycles, with b = 8 (FP64) and 4 (FP32) bytes per value:
-      set-up          read q, phi_old; write y, rhs, phi            5 x 8 B per point
-      residual check  read X, rhs (FP64); write FP32 rhs, e       (8+8+4+4) B, refinements+1 times
-      V-cycle, per level worked by the whole grid (n > small_n), per point of that level:
-        (2 nu1 - 1)/2 + nu2 red-black sweeps x 3 x 4 B, residual 3 x 4 B,
-        restriction 4 B + 4 B/8, prolongation 4 B/8 + 2 x 4 B
-      update          read X, e; write X                          (8+4+8) B
+    `refinements` V-cycles, with 8 B per FP64 and 4 B per FP32 value, per grid point:
+      set-up          read q, phi_old; write y, rhs, phi                     40 B
+      residual check  read X, rhs; write FP32 rhs, e            24 B, refinements + 1 times
+      update          read X, e; write X                                     20 B
+      V-cycle, per point of each level worked by the whole grid (n > small_n), with the
+      red-black split layout (a half-sweep reads the other colour, this colour's rhs and
+      writes this colour: 3 x 4 B x 1/2):
+        2 nu1 - 1 + 2 nu2 half-sweeps                                   6 B each
+        red residual: read both colours of x, red rhs; write red r       8 B
+        restriction (13 red taps): read red r; write coarse rhs, x       2 + 1 B
+        prolongation into black points: read coarse x; read/write black  0.5 + 4 B
     Levels of at most small_n^3 points live in shared memory and move no HBM bytes."""
     P = n ** 3
-    per_level = ((2 * nu1 - 1) / 2 + nu2) * 12 + 12 + 4.5 + 8.5
+    per_level = (2 * nu1 - 1 + 2 * nu2) * 6 + 8 + 3 + 4.5
     grid_levels = [m for m in level_sizes(n) if m > small_n]
     vcycle = sum(m ** 3 * per_level for m in grid_levels)
     return P * 40 + (refinements + 1) * P * 24 + refinements * (vcycle + P * 20)
