@@ -531,7 +531,7 @@ __device__ void coarse_direct(int n, const float* g, const float* b, float* x) {
 
 // Restricts the residual of level lsmall-1 (global) into shared memory, runs the rest of
 // the V-cycle there and writes level lsmall's correction back to lev_x[lsmall].
-__device__ void small_vcycle(const MixedArgs& a, float* sm) {
+__device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above) {
     const int L = a.nlev, ls = a.lsmall;
     auto smooth = [&](int m, int first_colour, int half_sweeps) {
         const int n = a.lev_n[m];
@@ -548,7 +548,7 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm) {
         for (int p = threadIdx.x; p < N; p += blockDim.x) gsm[p] = a.coarse_g[p];
     }
     {
-        const float* r = a.lev_r[ls - 1];  // red residual, split layout
+        const float* r = r_above;  // red residual of level ls - 1, split layout
         const int nf = a.lev_n[ls - 1], nc = a.lev_n[ls];
         float* bs = small_arr(a, sm, ls, 1);
         float* xs = small_arr(a, sm, ls, 0);
@@ -596,10 +596,10 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm) {
 // Grid-wide red-black sweeps of level l: `half_sweeps` colours starting at first_colour,
 // a grid barrier after each except (when skip_last_barrier) the last. When esum is not
 // null the values written in the last two half-sweeps are summed into it.
-__device__ bool grid_smooth(const MixedArgs& a, const Team& tm, int l, int first_colour, int half_sweeps,
+__device__ bool grid_smooth(const MixedArgs& a, const Team& tm, int l, float* x, int first_colour, int half_sweeps,
                             unsigned& epoch, double* esum, bool skip_last_barrier) {
     for (int h = 0; h < half_sweeps; h++) {
-        split_gs(tm, a.lev_n[l], (first_colour + h) & 1, a.lev_b[l], a.lev_x[l],
+        split_gs(tm, a.lev_n[l], (first_colour + h) & 1, a.lev_b[l], x,
                  esum != nullptr && h >= half_sweeps - 2 ? esum : nullptr);
         if (h == half_sweeps - 1 && skip_last_barrier) break;
         if (!team_sync(tm, epoch)) return false;
@@ -607,35 +607,69 @@ __device__ bool grid_smooth(const MixedArgs& a, const Team& tm, int l, int first
     return true;
 }
 
-// One V-cycle for the correction e = lev_x[0] of rhs lev_b[0], whose first red half-sweep
-// has been done by the residual pass. Ends after the last half-sweep of level 0 without a
-// barrier, with this thread's share of sum(e) in esum.
-__device__ bool vcycle(const MixedArgs& a, const Team& tm, float* sm, unsigned& epoch, double& esum, int outer) {
+// One V-cycle for the correction x0 (level 0's x; r0 is level 0's residual buffer) of rhs
+// lev_b[0], whose first red half-sweep has been done by the residual pass. Ends after
+// the last half-sweep of level 0 without a barrier, with this thread's share of sum(x0)
+// in esum.
+__device__ bool vcycle(const MixedArgs& a, const Team& tm, float* sm, unsigned& epoch, double& esum, int outer,
+                       float* x0, float* r0) {
     const int L = a.nlev, ls = a.lsmall;
     const int lg = ls < L ? ls : L - 1;  // levels 0..lg-1 are smoothed and restricted on the grid
+    auto X = [&](int l) { return l == 0 ? x0 : a.lev_x[l]; };
+    auto R = [&](int l) { return l == 0 ? r0 : a.lev_r[l]; };
     for (int l = 0; l < lg; l++) {
-        if (!grid_smooth(a, tm, l, 1, 2 * a.nu1 - 1, epoch, nullptr, false)) return false;
-        split_resid_red(tm, a.lev_n[l], a.lev_b[l], a.lev_x[l], a.lev_r[l]);
+        if (!grid_smooth(a, tm, l, X(l), 1, 2 * a.nu1 - 1, epoch, nullptr, false)) return false;
+        split_resid_red(tm, a.lev_n[l], a.lev_b[l], X(l), R(l));
         if (!team_sync(tm, epoch)) return false;
         if (l + 1 < ls) {
-            split_restrict(tm, a.lev_n[l], a.lev_r[l], a.lev_b[l + 1], a.lev_x[l + 1]);
+            split_restrict(tm, a.lev_n[l], R(l), a.lev_b[l + 1], X(l + 1));
             if (!team_sync(tm, epoch)) return false;
         }
     }
     stamp_outer(a, outer, 2);
     if (ls < L) {
-        if (tm.b == 0) small_vcycle(a, sm);
+        if (tm.b == 0) small_vcycle(a, sm, R(ls - 1));
         if (!team_sync(tm, epoch)) return false;
     } else {
-        if (!grid_smooth(a, tm, L - 1, 1, 2 * a.coarse_sweeps - 1, epoch, nullptr, false)) return false;
+        if (!grid_smooth(a, tm, L - 1, X(L - 1), 1, 2 * a.coarse_sweeps - 1, epoch, nullptr, false)) return false;
     }
     stamp_outer(a, outer, 3);
     for (int l = lg - 1; l >= 0; l--) {
-        split_prolong_black(tm, a.lev_n[l], a.lev_x[l + 1], a.lev_x[l]);
+        split_prolong_black(tm, a.lev_n[l], X(l + 1), X(l));
         if (!team_sync(tm, epoch)) return false;
-        if (!grid_smooth(a, tm, l, 0, 2 * a.nu2, epoch, l == 0 ? &esum : nullptr, l == 0)) return false;
+        if (!grid_smooth(a, tm, l, X(l), 0, 2 * a.nu2, epoch, l == 0 ? &esum : nullptr, l == 0)) return false;
     }
     return true;
+}
+
+// FP64 residual r = B - L X (X = 0 when ZERO; B = c q when RHS_Q, else tmp) written as
+// the FP32 rhs of the inner solve together with that solve's first red half-sweep from
+// e = 0; returns this thread's max |r|.
+template <bool ZERO, bool RHS_Q>
+__device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs& a, const double* X, float* e,
+                                                float* rb) {
+    const int n = a.n;
+    double rmax = 0.0;
+    grid_pts(tm, n, [&](int i, int j, int k) {
+        const Nb o = nb_of(n, i, j, k);
+        double r;
+        if (ZERO) {
+            r = RHS_Q ? a.q[o.c] * a.c : a.tmp[o.c];
+        } else {
+            double s = X[o.ip] + X[o.im];
+            s = s + X[o.jp];
+            s = s + X[o.jm];
+            s = s + X[o.kp];
+            s = s + X[o.km];
+            r = (RHS_Q ? a.q[o.c] * a.c : a.tmp[o.c]) - (s - X[o.c] * 6.0);
+        }
+        const float rf = (float)r;
+        const int sx = split_idx(n, i, j, k);
+        rb[sx] = rf;
+        e[sx] = ((i + j + k) & 1) == 0 ? rf * (-1.0f / 6.0f) : 0.0f;
+        rmax = fmax(rmax, fabs(r));
+    });
+    return rmax;
 }
 
 // The solve of one system by one team of CTAs.
@@ -647,32 +681,26 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
     int result = -1;
     if (tm.b == 0) stamp(a, 0);
 
-    // ---- set-up: right-hand side B and solution X (FP64), as the FP64 programs ----
-    double* X = a.phi_new;
-    const double* B = a.tmp;
-    if (a.prog == PROG_INIT_FIELD) {         // y = 0, phi = 0 start, b = c q
-        grid_pts(tm, n, [&](int i, int j, int k) {
-            const long c = ((long)i * n + j) * n + k;
-            a.y[c] = 0.0;
-            a.phi_new[c] = 0.0;
-            a.tmp[c] = a.q[c] * a.c;
-        });
-    } else if (a.prog == PROG_LCG_UPDATE) {  // y = c q; start from phi_prev (old phi)
-        grid_pts(tm, n, [&](int i, int j, int k) {
-            const long c = ((long)i * n + j) * n + k;
-            const double bq = a.q[c] * a.c;
-            a.y[c] = bq;
-            a.tmp[c] = bq;
-            a.phi_new[c] = a.phi_old[c];
-        });
-    } else if (a.prog == PROG_MG_UPDATE) {   // phi = 2 phi - phi_prev (start), b = c q
+    // ---- set-up, as the FP64 programs (the unknown X, its start X0, the rhs B) ----
+    // LCG and INIT read the rhs c q on the fly and start from the old field (or 0) without
+    // a set-up pass; the MaZe programs keep sigma = L(2 phi - phi_prev) + c q in tmp.
+    double* home = a.phi_new;        // where the solution must end
+    const double* X0 = a.phi_old;    // the start (read-only)
+    bool zero_start = false, rhs_q = true;
+    if (a.prog == PROG_INIT_FIELD) {         // y = 0 (later MaZe warm starts), phi = 0 start
+        zero_start = true;
+        grid_pts(tm, n, [&](int i, int j, int k) { a.y[((long)i * n + j) * n + k] = 0.0; });
+    } else if (a.prog == PROG_LCG_UPDATE) {  // start from the old phi
+    } else if (a.prog == PROG_MG_UPDATE) {   // start from 2 phi - phi_prev
+        X0 = a.phi_new;
         grid_pts(tm, n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
             a.phi_new[c] = 2 * a.phi_old[c] - a.phi_prev[c];
-            a.tmp[c] = a.q[c] * a.c;
         });
-    } else {                                 // MaZe: phi = 2 phi - phi_prev; sigma = L phi + c q
-        X = a.y;
+    } else {                                 // MaZe: phi = 2 phi - phi_prev; solve L y = sigma
+        home = a.y;
+        X0 = a.y;
+        rhs_q = false;
         grid_pts(tm, n, [&](int i, int j, int k) {
             const Nb o = nb_of(n, i, j, k);
             auto ex = [&](long q) { return 2 * a.phi_old[q] - a.phi_prev[q]; };
@@ -685,31 +713,26 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
             a.tmp[o.c] = (s - ex(o.c) * 6.0) + a.c * a.q[o.c];
         });
     }
-    ok = team_sync(tm, epoch);
+    if (a.prog != PROG_LCG_UPDATE) ok = team_sync(tm, epoch);
     stamp(a, 1);
 
+    // Refinement: r = B - L X in FP64 (checked against tol) -> FP32 rhs of the inner solve
+    // with the correction's first red half-sweep from e = 0; e = V-cycle; X += e - mean(e).
+    // X starts as X0 (read-only; zero for INIT) and lives in `home` from the first update.
+    const double* Xs = X0;
     float* e = a.lev_x[0];
     float* rb = a.lev_b[0];
     int outer = 0;
     while (ok) {
-        // r = B - L X in FP64 -> FP32 rhs of the inner solve, with the correction's first
-        // red half-sweep from e = 0; |r|_inf
         stamp_outer(a, outer, 0);
+        const bool zero = zero_start && outer == 0;
         double s0 = 0.0, rmax = 0.0;
-        grid_pts(tm, n, [&](int i, int j, int k) {
-            const Nb o = nb_of(n, i, j, k);
-            double s = X[o.ip] + X[o.im];
-            s = s + X[o.jp];
-            s = s + X[o.jm];
-            s = s + X[o.kp];
-            s = s + X[o.km];
-            const double r = B[o.c] - (s - X[o.c] * 6.0);
-            const float rf = (float)r;
-            const int sx = split_idx(n, i, j, k);
-            rb[sx] = rf;
-            e[sx] = ((i + j + k) & 1) == 0 ? rf * (-1.0f / 6.0f) : 0.0f;
-            rmax = fmax(rmax, fabs(r));
-        });
+        if (zero)
+            rmax = residual_pass<true, true>(tm, a, Xs, e, rb);
+        else if (rhs_q)
+            rmax = residual_pass<false, true>(tm, a, Xs, e, rb);
+        else
+            rmax = residual_pass<false, false>(tm, a, Xs, e, rb);
         ok = reduce_sum_max(s0, rmax, tm, epoch, seq);
         stamp_outer(a, outer, 1);
         if (a.stamps != nullptr && outer < 8 && tm.b == 0 && threadIdx.x == 0)
@@ -721,7 +744,7 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
         }
         if (outer >= a.max_outer) break;
         double esum = 0.0, m0 = 0.0;
-        ok = vcycle(a, tm, sm, epoch, esum, outer);
+        ok = vcycle(a, tm, sm, epoch, esum, outer, e, a.lev_r[0]);
         if (!ok) break;
         stamp_outer(a, outer, 4);
         // mean of the correction (the periodic Laplacian's null space)
@@ -731,11 +754,21 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
         const double emean = esum / ((double)n * n * n);
         grid_pts(tm, n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
-            X[c] = X[c] + ((double)e[split_idx(n, i, j, k)] - emean);
+            const double xo = zero ? 0.0 : Xs[c];
+            home[c] = xo + ((double)e[split_idx(n, i, j, k)] - emean);
         });
+        Xs = home;
         ok = team_sync(tm, epoch);
         stamp_outer(a, outer, 6);
         outer++;
+    }
+    // converged before any update: the solution is the start itself
+    if (ok && Xs != home) {
+        grid_pts(tm, n, [&](int i, int j, int k) {
+            const long c = ((long)i * n + j) * n + k;
+            home[c] = zero_start ? 0.0 : Xs[c];
+        });
+        ok = team_sync(tm, epoch);
     }
     if (ok && (a.prog == PROG_MAZE_LCG || a.prog == PROG_MAZE_MG)) {  // phi -= y
         grid_pts(tm, n, [&](int i, int j, int k) {

@@ -30,7 +30,7 @@ struct MixedArgs {
     const double* phi_prev;
     double* phi_new;
     double* y;
-    double* tmp;        // FP64 right-hand side
+    double* tmp;        // FP64 right-hand side (MaZe programs)
     double* partials;   // >= 4 x gridDim.x doubles
     GridBarrier* bar;
     int* result;        // [0] refinement steps taken or -1, [1] status (0 ok)
