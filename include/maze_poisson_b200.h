@@ -89,6 +89,23 @@ int mzb_batch_autotune(const int *handles, int nsys, double *out);
    against an HBM budget). */
 double mzb_system_footprint(int n, int n_p);
 
+/* Asynchronous output snapshots of the selected system (the reference's output path,
+   maze_poisson/myio/output/csv.py:45-183, calls the blocking getters every stride).
+   begin stages the requested arrays on the system's stream and copies them to pinned
+   host memory on a copy stream, overlapping the next MD steps; it returns the slot (0 or
+   1), or -1 when both slots hold unfetched snapshots. what: 1 positions, 2 velocities,
+   4 forces (elec, noel, tot), 8 scalars {q total, V_notelec, K, Px, Py, Pz, T, 0},
+   16 fields (phi, phi_prev). fetch waits for the slot, copies into the given arrays
+   (null skips one) and frees the slot; it returns the captured mask or -1. */
+int mzb_snapshot_begin(int what);
+int mzb_snapshot_fetch(int slot, double *pos, double *vel, double *fcs_elec, double *fcs_noel,
+                       double *fcs_tot, double *scalars, double *phi, double *phi_prev);
+/* The slot's pinned host buffer, read in place without a copy (layout: pos, vel,
+   fcs_elec, fcs_noel, fcs_tot as n_p*3 doubles each, 8 scalars, then phi, phi_prev as
+   n^3 each when captured), after waiting for it; valid until mzb_snapshot_fetch releases
+   the slot. Null if the slot holds no snapshot. */
+double *mzb_snapshot_host(int slot);
+
 /* instrumentation */
 void *mzb_get_stream(void);                /* cudaStream_t of the current system */
 double mzb_last_solve_ms(void);            /* device ms of the last field-solver launch */

@@ -118,6 +118,9 @@ EXTENSION_SYMBOLS = {
     "mzb_batch_step": (_c.c_int, [_i32_1, _c.c_int, _c.c_int]),
     "mzb_batch_autotune": (_c.c_int, [_i32_1, _c.c_int, _f64_1]),
     "mzb_system_footprint": (_c.c_double, [_c.c_int, _c.c_int]),
+    "mzb_snapshot_begin": (_c.c_int, [_c.c_int]),
+    "mzb_snapshot_fetch": (_c.c_int, [_c.c_int] + [_c.c_void_p] * 8),
+    "mzb_snapshot_host": (_c.POINTER(_c.c_double), [_c.c_int]),
 }
 
 

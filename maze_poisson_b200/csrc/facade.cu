@@ -1416,6 +1416,8 @@ int batch_end(std::vector<System*>& ss, const int* handles) {
     return status;
 }
 
+void release_snapshots(int handle);  // output snapshots of a system (defined below)
+
 }  // namespace
 }  // namespace mzb
 
@@ -1462,6 +1464,7 @@ int mzb_system_destroy(int handle) {
     dfree(s.I.ocalls_d);
     if (s.result_h) cudaFreeHost(s.result_h);
     if (s.red_h) cudaFreeHost(s.red_h);
+    release_snapshots(handle);
     delete g_systems[handle];
     g_systems[handle] = nullptr;
     if (prev_h == handle) {
@@ -1622,6 +1625,178 @@ double mzb_system_footprint(int n, int n_p) {
     const double split = std::min(12000.0 / nblk + 1.0, 4096.0);
     const double parts = (double)n_p * (8.0 * 3 * 7 + 4.0 * 8) + split * n_p * 3 * 8.0;
     return grid + levels + parts + 64.0 * 1024 * 1024;
+}
+
+}  // extern "C"
+
+// ====================================================================================
+// Output snapshots (this build's extension). The reference's output path calls the
+// synchronous getters every `stride` steps (maze_poisson/myio/output/csv.py:45-183,
+// solver.py:461-464). A snapshot instead stages the requested arrays with
+// device-to-device copies on the system's stream (ordered after the last step and before
+// the next one), then copies the staging area to pinned host memory on a separate copy
+// stream, so the transfer overlaps the following MD steps. Two slots per system.
+// ====================================================================================
+namespace mzb {
+namespace {
+
+enum SnapBits { SNAP_POS = 1, SNAP_VEL = 2, SNAP_FORCES = 4, SNAP_SCALARS = 8, SNAP_FIELDS = 16 };
+
+struct SnapSlot {
+    int what = 0;
+    bool busy = false;
+    long np = 0, m = 0;
+    cudaEvent_t staged = nullptr, done = nullptr;
+    double* d_buf = nullptr;
+    double* h_buf = nullptr;
+    size_t cap = 0;  // doubles
+};
+
+struct SnapState {
+    cudaStream_t copy = nullptr;
+    SnapSlot slot[2];
+};
+
+std::vector<SnapState*> g_snaps;  // per system handle
+
+SnapState& snap_state() {
+    if (g_current < 0) fatal("no system selected");
+    if ((int)g_snaps.size() <= g_current) g_snaps.resize(g_current + 1, nullptr);
+    SnapState*& st = g_snaps[g_current];
+    if (!st) {
+        st = new SnapState();
+        MZB_CHECK(cudaStreamCreateWithFlags(&st->copy, cudaStreamNonBlocking));
+        for (auto& sl : st->slot) {
+            MZB_CHECK(cudaEventCreateWithFlags(&sl.staged, cudaEventDisableTiming));
+            MZB_CHECK(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+        }
+    }
+    return *st;
+}
+
+// Layout of a slot's buffer: pos, vel (np*3 each), fcs_elec, fcs_noel, fcs_tot (np*3
+// each), scalars (8: q total, V_notelec, K, Px, Py, Pz, T, spare), phi, phi_prev (m each).
+size_t snap_size(long np, long m, int what) {
+    size_t s = 5 * 3 * (size_t)np + 8;
+    if (what & SNAP_FIELDS) s += 2 * (size_t)m;
+    return s;
+}
+
+}  // namespace
+
+namespace {
+void release_snapshots(int handle) {
+    if (handle < 0 || handle >= (int)g_snaps.size() || !g_snaps[handle]) return;
+    SnapState* st = g_snaps[handle];
+    cudaStreamSynchronize(st->copy);
+    for (auto& sl : st->slot) {
+        if (sl.d_buf) cudaFree(sl.d_buf);
+        if (sl.h_buf) cudaFreeHost(sl.h_buf);
+        cudaEventDestroy(sl.staged);
+        cudaEventDestroy(sl.done);
+    }
+    cudaStreamDestroy(st->copy);
+    delete st;
+    g_snaps[handle] = nullptr;
+}
+}  // namespace
+}  // namespace mzb
+
+extern "C" {
+
+// Queue a snapshot of the selected system (what: 1 positions, 2 velocities, 4 forces
+// (elec, noel, tot), 8 scalars (V_notelec, K, momentum, T), 16 fields (phi, phi_prev)).
+// Returns the slot (0 or 1) to fetch, or -1 if both slots hold unfetched snapshots.
+int mzb_snapshot_begin(int what) {
+    System& s = sys();
+    ParticleDev& P = parts();
+    SnapState& st = snap_state();
+    int k = !st.slot[0].busy ? 0 : (!st.slot[1].busy ? 1 : -1);
+    if (k < 0) return -1;
+    SnapSlot& sl = st.slot[k];
+    const bool fields = (what & SNAP_FIELDS) && s.G.ready;
+    const long m = fields ? s.G.m : 0;
+    const size_t need = snap_size(P.np, m, fields ? what : what & ~SNAP_FIELDS);
+    if (need > sl.cap) {
+        if (sl.d_buf) cudaFree(sl.d_buf);
+        if (sl.h_buf) cudaFreeHost(sl.h_buf);
+        MZB_CHECK(cudaMalloc(&sl.d_buf, need * sizeof(double)));
+        MZB_CHECK(cudaMallocHost(&sl.h_buf, need * sizeof(double)));
+        sl.cap = need;
+    }
+    sl.what = fields ? what : what & ~SNAP_FIELDS;
+    sl.np = P.np;
+    sl.m = m;
+    const size_t v = 3 * (size_t)P.np * sizeof(double);
+    double* d = sl.d_buf;
+    if (what & SNAP_SCALARS) kinetic_and_momentum(P, s.stream);
+    if (P.np > 0) {
+        if (what & SNAP_POS) MZB_CHECK(cudaMemcpyAsync(d, P.pos, v, cudaMemcpyDeviceToDevice, s.stream));
+        if (what & SNAP_VEL) MZB_CHECK(cudaMemcpyAsync(d + 3 * P.np, P.vel, v, cudaMemcpyDeviceToDevice, s.stream));
+        if (what & SNAP_FORCES) {
+            MZB_CHECK(cudaMemcpyAsync(d + 6 * P.np, P.fe, v, cudaMemcpyDeviceToDevice, s.stream));
+            MZB_CHECK(cudaMemcpyAsync(d + 9 * P.np, P.fn, v, cudaMemcpyDeviceToDevice, s.stream));
+            MZB_CHECK(cudaMemcpyAsync(d + 12 * P.np, P.ft, v, cudaMemcpyDeviceToDevice, s.stream));
+        }
+    }
+    if (what & SNAP_SCALARS)
+        MZB_CHECK(cudaMemcpyAsync(d + 15 * P.np, P.red, 8 * sizeof(double), cudaMemcpyDeviceToDevice, s.stream));
+    if (fields) {
+        double* f = d + 15 * P.np + 8;
+        MZB_CHECK(cudaMemcpyAsync(f, s.G.phi(), sizeof(double) * m, cudaMemcpyDeviceToDevice, s.stream));
+        if (s.G.type != G_FFT)
+            MZB_CHECK(cudaMemcpyAsync(f + m, s.G.phi_prev(), sizeof(double) * m, cudaMemcpyDeviceToDevice, s.stream));
+    }
+    MZB_CHECK(cudaEventRecord(sl.staged, s.stream));
+    MZB_CHECK(cudaStreamWaitEvent(st.copy, sl.staged, 0));
+    MZB_CHECK(cudaMemcpyAsync(sl.h_buf, sl.d_buf, need * sizeof(double), cudaMemcpyDeviceToHost, st.copy));
+    MZB_CHECK(cudaEventRecord(sl.done, st.copy));
+    sl.busy = true;
+    return k;
+}
+
+// Wait for snapshot `slot` of the selected system and return its pinned host buffer
+// (read in place, no copy): pos, vel, fcs_elec, fcs_noel, fcs_tot (n_p*3 doubles each),
+// 8 scalars, then phi and phi_prev (n^3 each) if captured. The buffer stays valid until
+// the slot is released by mzb_snapshot_fetch. Null if the slot holds no snapshot.
+double* mzb_snapshot_host(int slot) {
+    if (slot < 0 || slot > 1) return nullptr;
+    SnapState& st = snap_state();
+    SnapSlot& sl = st.slot[slot];
+    if (!sl.busy) return nullptr;
+    MZB_CHECK(cudaEventSynchronize(sl.done));
+    return sl.h_buf;
+}
+
+// Wait for snapshot `slot` of the selected system and copy it out; null pointers skip an
+// array. scalars[8] = {q total, V_notelec, K, Px, Py, Pz, T, 0}. Returns the mask that
+// was captured, or -1 if the slot holds no snapshot.
+int mzb_snapshot_fetch(int slot, double* pos, double* vel, double* fcs_elec, double* fcs_noel, double* fcs_tot,
+                       double* scalars, double* phi, double* phi_prev) {
+    if (slot < 0 || slot > 1) return -1;
+    SnapState& st = snap_state();
+    SnapSlot& sl = st.slot[slot];
+    if (!sl.busy) return -1;
+    MZB_CHECK(cudaEventSynchronize(sl.done));
+    const size_t v = 3 * (size_t)sl.np * sizeof(double);
+    const double* h = sl.h_buf;
+    if ((sl.what & SNAP_POS) && pos) memcpy(pos, h, v);
+    if ((sl.what & SNAP_VEL) && vel) memcpy(vel, h + 3 * sl.np, v);
+    if (sl.what & SNAP_FORCES) {
+        if (fcs_elec) memcpy(fcs_elec, h + 6 * sl.np, v);
+        if (fcs_noel) memcpy(fcs_noel, h + 9 * sl.np, v);
+        if (fcs_tot) memcpy(fcs_tot, h + 12 * sl.np, v);
+    }
+    if ((sl.what & SNAP_SCALARS) && scalars) {
+        memcpy(scalars, h + 15 * sl.np, 8 * sizeof(double));
+        scalars[7] = 0.0;
+    }
+    if (sl.what & SNAP_FIELDS) {
+        if (phi) memcpy(phi, h + 15 * sl.np + 8, sizeof(double) * sl.m);
+        if (phi_prev) memcpy(phi_prev, h + 15 * sl.np + 8 + sl.m, sizeof(double) * sl.m);
+    }
+    sl.busy = false;
+    return sl.what;
 }
 
 }  // extern "C"

@@ -23,6 +23,11 @@ def main():
     ap.add_argument("--integrator", default="OVRVO")
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--precision", type=int, default=0, help="0 FP64, 1 FP32 multigrid + FP64 refinement")
+    ap.add_argument("--outputs", type=int, default=0,
+                    help="take the reference's per-stride outputs every N steps (0: none), both ways")
+    ap.add_argument("--restart-every", action="store_true",
+                    help="with --outputs: the restart outputs (both fields) at every output step")
+    ap.add_argument("--no-write", action="store_true", help="with --outputs: transfer only, write no file")
     args = ap.parse_args()
     os.environ.setdefault("MZB_QUIET", "1")
     run = MDRun(CAPI(), make_system(seed=1, **WORKLOADS[args.workload]), method=args.method,
@@ -30,9 +35,29 @@ def main():
                 thermostat=args.integrator.upper() == "OVRVO", precision=args.precision)
     capi = run.capi
     run.initialize()
-    for k in range(args.steps):
-        it = run.step()
-        print(f"step {k}: solve {capi.mzb_last_solve_ms():.4f} ms, solver returned {it}")
+    if args.outputs:
+        import tempfile
+        import time
+        from .output import Outputs
+        for mode in (False, True, False, True):
+            with tempfile.TemporaryDirectory() as d:
+                out = Outputs(capi, d, ["Na", "Cl"], run.sys.n_grid, stride=args.outputs,
+                              use_snapshots=mode, write=not args.no_write).bind(run.sys.n_ions)
+                t0 = time.perf_counter()
+                for k in range(args.steps):
+                    run.step()
+                    if args.restart_every and k % args.outputs == 0:
+                        out.restart_step = k
+                    out.output(k, run.potential_notelec)
+                out.close()
+                dt = (time.perf_counter() - t0) / args.steps
+            what = "per-stride + restart" if args.restart_every else "per-stride"
+            print(f"{what} outputs every {args.outputs} steps via {'snapshots' if mode else 'getters'}"
+                  f"{' (no files)' if args.no_write else ''}: {dt * 1e3:.3f} ms per step")
+    else:
+        for k in range(args.steps):
+            it = run.step()
+            print(f"step {k}: solve {capi.mzb_last_solve_ms():.4f} ms, solver returned {it}")
     run.finalize()
     print("ok")
 
