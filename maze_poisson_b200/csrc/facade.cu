@@ -484,10 +484,13 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
     System& s = sys();
     touch(s);
     if (pot_type != 0) fatal("only the Tosi-Fumi potential (TF) is supported by this build");
-    if (cas_type != 0) fatal("only CIC charge assignment is supported by this build");
+    if (cas_type < 0 || cas_type > 2) fatal("invalid charge assignment scheme");
+    if (cas_type != CAS_CIC && n < 4)  // offsets -1..2 would wrap onto the same point
+        fatal("B-spline charge assignment needs a grid of at least 4 points per side");
     if (n_typ < 1 || n_typ > 8) fatal("between 1 and 8 particle types are supported");
     if (s.parts_ready) free_particles(s.P);
     ParticleDev& P = s.P;
+    P.cas = cas_type;
     P.np = n_p;
     P.ntyp = n_typ;
     P.n = n;
@@ -845,15 +848,24 @@ __global__ void k_sum_parts(const double* __restrict__ part, int nb, double* __r
     *out = s;
 }
 
-__global__ void k_cic_neighbors(const int32_t* __restrict__ base, int np, int n, int64_t* __restrict__ out) {
+// Stencil points of every ion in the reference's neighbour layout: CIC corners
+// (particles.c:297-346) or the 64 B-spline points (particles.c:348-385).
+__global__ void k_stencil_points(const int32_t* __restrict__ base, int np, int n, int cas,
+                                 int64_t* __restrict__ out) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= np) return;
-    const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
-    for (int c = 0; c < 8; c++)
-        for (int d = 0; d < 3; d++) {
-            const int b = base[3 * p + d];
-            out[(p * 8 + c) * 3 + d] = off[c][d] ? wrap_inc(b, n) : b;
+    const int* b = base + 3 * p;
+    if (cas == CAS_CIC) {
+        const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+        for (int c = 0; c < 8; c++)
+            for (int d = 0; d < 3; d++) out[(p * 8 + c) * 3 + d] = off[c][d] ? wrap_inc(b[d], n) : b[d];
+    } else {
+        for (int o = 0; o < 64; o++) {
+            out[(p * 64 + o) * 3 + 0] = (b[0] + o / 16 - 1 + n) % n;
+            out[(p * 64 + o) * 3 + 1] = (b[1] + (o / 4) % 4 - 1 + n) % n;
+            out[(p * 64 + o) * 3 + 2] = (b[2] + o % 4 - 1 + n) % n;
         }
+    }
 }
 
 // Temporary device work set for the kernel-level entry points.
@@ -1057,17 +1069,19 @@ void mzb_fft_poisson(const double* q, double* phi, int n, double L, double h) {
     d2h_sync(phi, dphi, m);
 }
 
-// CIC corner indices of the current system, (n_p, 8, 3) int64 in the reference's layout
-// (particles.c:297-346); valid after solver_update_charges.
+// Stencil (neighbour) indices of the current system in the reference's layout: (n_p, 8, 3)
+// int64 for CIC (particles.c:297-346), (n_p, 64, 3) for the B-splines
+// (particles.c:348-385); valid after solver_update_charges.
 void mzb_get_cic_neighbors(int64_t* out) {
     System& s = sys();
     ParticleDev& P = parts();
     if (P.np == 0) return;
+    const int nnb = P.cas == CAS_CIC ? 8 : 64;
     int64_t* d = nullptr;
-    MZB_CHECK(cudaMalloc(&d, sizeof(int64_t) * 24 * P.np));
+    MZB_CHECK(cudaMalloc(&d, sizeof(int64_t) * 3 * nnb * P.np));
     count_launch();
-    k_cic_neighbors<<<(P.np + 127) / 128, 128, 0, s.stream>>>(P.base, P.np, grid().n, d);
-    MZB_CHECK(cudaMemcpyAsync(out, d, sizeof(int64_t) * 24 * P.np, cudaMemcpyDeviceToHost, s.stream));
+    k_stencil_points<<<(P.np + 127) / 128, 128, 0, s.stream>>>(P.base, P.np, grid().n, P.cas, d);
+    MZB_CHECK(cudaMemcpyAsync(out, d, sizeof(int64_t) * 3 * nnb * P.np, cudaMemcpyDeviceToHost, s.stream));
     sync();
     cudaFree(d);
 }

@@ -15,6 +15,54 @@ __device__ __forceinline__ double w_cic(double x, double L, double h) {
     return 1.0 - x / h;
 }
 
+// Correctly rounded x^3: x^2 = p + e exactly, p x = hi + lo exactly, one final rounding
+// of hi + (lo + e x) (Dekker's exact product via FMA). glibc's pow(x, 3), which the
+// reference's cubic spline calls, returns this value except in ~0.08 % of inputs where
+// it is one ulp off.
+__device__ __forceinline__ double cube_rn(double x) {
+    const double p = x * x, e = fma(x, x, -p);
+    const double hi = p * x, lo = fma(p, x, -hi);
+    return hi + (lo + e * x);
+}
+
+// Assignment weight of scheme CAS with the minimum image over L (charges.c:8-38).
+template <int CAS>
+__device__ __forceinline__ double w_cas(double x, double L, double h) {
+    if (CAS == CAS_CIC) return w_cic(x, L, h);
+    x = fabs(x - round(x / L) * L) / h;
+    if (CAS == CAS_SPL_QUADR) {
+        if (x < 0.5) return 0.75 - x * x;
+        if (x < 1.5) {
+            const double y = 1.5 - x;
+            return 0.5 * (y * y);
+        }
+        return 0.0;
+    }
+    if (x < 1) return (4.0 - 6.0 * (x * x) + 3.0 * cube_rn(x)) / 6.0;
+    if (x < 2) return cube_rn(2 - x) / 6.0;
+    return 0.0;
+}
+
+// Stencil point o of scheme CAS around base cell b, in the reference's neighbour order
+// (CIC: particles.c:323-344; splines: particles.c:366-381, a/b/c = -1..2 nested).
+template <int CAS>
+__device__ __forceinline__ void stencil_point(int o, const int* b, int n, int& i, int& j, int& k) {
+    if (CAS == CAS_CIC) {
+        const int di = (o == 1 || o == 4 || o == 5 || o == 7);
+        const int dj = (o == 2 || o == 4 || o == 6 || o == 7);
+        const int dk = (o == 3 || o == 5 || o == 6 || o == 7);
+        i = di ? (b[0] + 1 == n ? 0 : b[0] + 1) : b[0];
+        j = dj ? (b[1] + 1 == n ? 0 : b[1] + 1) : b[1];
+        k = dk ? (b[2] + 1 == n ? 0 : b[2] + 1) : b[2];
+    } else {
+        i = (b[0] + o / 16 - 1 + n) % n;
+        j = (b[1] + (o / 4) % 4 - 1 + n) % n;
+        k = (b[2] + o % 4 - 1 + n) % n;
+    }
+}
+template <int CAS>
+constexpr int stencil_size() { return CAS == CAS_CIC ? 8 : 64; }
+
 // CIC corner c (0..7) in the reference's order (particles.c:323-344):
 // (0,0,0) (1,0,0) (0,1,0) (0,0,1) (1,1,0) (1,0,1) (0,1,1) (1,1,1)
 __device__ __forceinline__ void corner_offsets(int c, int& di, int& dj, int& dk) {
@@ -77,6 +125,7 @@ __global__ void __launch_bounds__(1024) k_scan(const int32_t* __restrict__ count
 
 // Per ion: base cell floor(pos/h) (wrapped), tile histogram and the ion's total spread
 // charge (block partial, summed later in block order).
+template <int CAS>
 __global__ void k_spread_bin(ParticleDev P, int n, double h, double* __restrict__ part) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     double u = 0.0;
@@ -90,14 +139,11 @@ __global__ void k_spread_bin(ParticleDev P, int n, double h, double* __restrict_
         const int tile = ((b[0] / kTileI) * P.ntj + b[1] / kTileJ) * P.ntk + b[2] / kTileK;
         atomicAdd(&P.tile_count[tile], 1);
         const double L = n * h, q = P.chg[p];
-        for (int c = 0; c < 8; c++) {
-            int di, dj, dk;
-            corner_offsets(c, di, dj, dk);
-            const int a = di ? wrap_inc(b[0], n) : b[0];
-            const int bb = dj ? wrap_inc(b[1], n) : b[1];
-            const int e = dk ? wrap_inc(b[2], n) : b[2];
-            double w = w_cic(P.pos[3 * p] - a * h, L, h) * w_cic(P.pos[3 * p + 1] - bb * h, L, h);
-            w = w * w_cic(P.pos[3 * p + 2] - e * h, L, h);
+        for (int o = 0; o < stencil_size<CAS>(); o++) {
+            int a, bb, e;
+            stencil_point<CAS>(o, b, n, a, bb, e);
+            double w = w_cas<CAS>(P.pos[3 * p] - a * h, L, h) * w_cas<CAS>(P.pos[3 * p + 1] - bb * h, L, h);
+            w = w * w_cas<CAS>(P.pos[3 * p + 2] - e * h, L, h);
             u += q * w;
         }
     }
@@ -116,32 +162,47 @@ __global__ void k_spread_fill(ParticleDev P) {
     P.tile_ions[slot] = p;
 }
 
-// One CTA per tile (grid-stride): gather the ions whose base cell lies in this tile or
-// in the 7 tiles below it (their +1 corners can reach this tile), sort them by ion index,
+// One CTA per tile (grid-stride): gather the ions whose stencil can reach this tile (base
+// cell in this tile or the 7 tiles below it for CIC, whose +1 corners reach up; in the 27
+// tiles around it for the splines, whose offsets run -1..2), sort them by ion index,
 // accumulate chg*w into a shared-memory tile in ascending ion order -- exactly the order
 // of the reference's serial scatter (charges.c:123-141) -- and flush the whole tile,
-// zeros included, with coalesced stores. q is written once; no atomics touch it.
+// zeros included, with coalesced stores. q is written once; no atomics touch it. One
+// thread per stencil point; the stencil's threads step through the ions together (a warp
+// barrier for CIC's 8, a named barrier for the splines' 64), so each point receives its
+// contributions in ion order.
+template <int CAS>
 __global__ void __launch_bounds__(128) k_spread_tiles(ParticleDev P, double* __restrict__ q, int n,
                                                       double h) {
+    constexpr int NS = stencil_size<CAS>();
+    constexpr int NSRC = CAS == CAS_CIC ? 8 : 27;
     __shared__ double acc[kTileI * kTileJ * kTileK];
     __shared__ int cand[kTileCap];
     __shared__ int sorted[kTileCap];
     __shared__ int ncand;
-    __shared__ int srcs[8];
+    __shared__ int srcs[NSRC];
     const double L = n * h;
     const long n2 = (long)n * n;
     for (int tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
         const int ti = tile / (P.ntj * P.ntk), tj = (tile / P.ntk) % P.ntj, tk = tile % P.ntk;
         for (int e = threadIdx.x; e < kTileI * kTileJ * kTileK; e += blockDim.x) acc[e] = 0.0;
-        if (threadIdx.x < 8) {
+        if (threadIdx.x < NSRC) {
             const int c = threadIdx.x;
-            const int si = wrapi(ti - ((c >> 2) & 1), P.nti), sj = wrapi(tj - ((c >> 1) & 1), P.ntj),
-                      sk = wrapi(tk - (c & 1), P.ntk);
+            int si, sj, sk;
+            if (CAS == CAS_CIC) {
+                si = wrapi(ti - ((c >> 2) & 1), P.nti);
+                sj = wrapi(tj - ((c >> 1) & 1), P.ntj);
+                sk = wrapi(tk - (c & 1), P.ntk);
+            } else {
+                si = wrapi(ti + c / 9 - 1, P.nti);
+                sj = wrapi(tj + (c / 3) % 3 - 1, P.ntj);
+                sk = wrapi(tk + c % 3 - 1, P.ntk);
+            }
             srcs[c] = (si * P.ntj + sj) * P.ntk + sk;
         }
         if (threadIdx.x == 0) ncand = 0;
         __syncthreads();
-        if (threadIdx.x < 8) {
+        if (threadIdx.x < NSRC) {
             const int c = threadIdx.x, s = srcs[c];
             bool dup = false;
             for (int d = 0; d < c; d++) dup |= (srcs[d] == s);
@@ -164,23 +225,22 @@ __global__ void __launch_bounds__(128) k_spread_tiles(ParticleDev P, double* __r
                 sorted[rank] = me;
             }
             __syncthreads();
-            if (threadIdx.x < 8) {
-                const int c = threadIdx.x;
-                int di, dj, dk;
-                corner_offsets(c, di, dj, dk);
+            if (threadIdx.x < NS) {
+                const int o = threadIdx.x;
                 for (int x = 0; x < nc; x++) {
                     const int p = sorted[x];
-                    const int* b = P.base + 3 * p;
-                    const int a = di ? wrap_inc(b[0], n) : b[0];
-                    const int bb = dj ? wrap_inc(b[1], n) : b[1];
-                    const int e = dk ? wrap_inc(b[2], n) : b[2];
+                    int a, bb, e;
+                    stencil_point<CAS>(o, P.base + 3 * p, n, a, bb, e);
                     const int li = a - ti * kTileI, lj = bb - tj * kTileJ, lk = e - tk * kTileK;
                     if (li >= 0 && li < kTileI && lj >= 0 && lj < kTileJ && lk >= 0 && lk < kTileK) {
-                        double w = w_cic(P.pos[3 * p] - a * h, L, h) * w_cic(P.pos[3 * p + 1] - bb * h, L, h);
-                        w = w * w_cic(P.pos[3 * p + 2] - e * h, L, h);
+                        double w = w_cas<CAS>(P.pos[3 * p] - a * h, L, h) * w_cas<CAS>(P.pos[3 * p + 1] - bb * h, L, h);
+                        w = w * w_cas<CAS>(P.pos[3 * p + 2] - e * h, L, h);
                         acc[(li * kTileJ + lj) * kTileK + lk] += P.chg[p] * w;
                     }
-                    __syncwarp(0xffu);
+                    if (CAS == CAS_CIC)
+                        __syncwarp(0xffu);
+                    else
+                        asm volatile("bar.sync 1, 64;" ::: "memory");
                 }
             }
         }
@@ -198,7 +258,12 @@ void spread_charges(ParticleDev& P, double* q, int n, double h, cudaStream_t s) 
     const int nb = (P.np + 127) / 128;
     MZB_CHECK(cudaMemsetAsync(P.tile_count, 0, sizeof(int32_t) * P.ntiles, s));
     count_launch();
-    k_spread_bin<<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial);
+    if (P.cas == CAS_CIC)
+        k_spread_bin<CAS_CIC><<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial);
+    else if (P.cas == CAS_SPL_QUADR)
+        k_spread_bin<CAS_SPL_QUADR><<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial);
+    else
+        k_spread_bin<CAS_SPL_CUBIC><<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial);
     count_launch();
     k_scan<<<1, 1024, 0, s>>>(P.tile_count, P.ntiles, P.tile_start, P.tile_fill, P.partial,
                               nb > 0 ? nb : 1, P.red + 0);
@@ -209,13 +274,19 @@ void spread_charges(ParticleDev& P, double* q, int n, double h, cudaStream_t s) 
     MZB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int grid = P.ntiles < sms * 16 ? P.ntiles : sms * 16;
     count_launch();
-    k_spread_tiles<<<grid, 128, 0, s>>>(P, q, n, h);
+    if (P.cas == CAS_CIC)
+        k_spread_tiles<CAS_CIC><<<grid, 128, 0, s>>>(P, q, n, h);
+    else if (P.cas == CAS_SPL_QUADR)
+        k_spread_tiles<CAS_SPL_QUADR><<<grid, 128, 0, s>>>(P, q, n, h);
+    else
+        k_spread_tiles<CAS_SPL_CUBIC><<<grid, 128, 0, s>>>(P, q, n, h);
     MZB_CHECK(cudaGetLastError());
 }
 
 // ------------------------------------------------------------------------------------
-// Field forces: central differences of phi at the 8 CIC corners (forces.c:26-100).
+// Field forces: central differences of phi at the stencil points (forces.c:26-100).
 // ------------------------------------------------------------------------------------
+template <int CAS>
 __global__ void k_field_forces(ParticleDev P, const double* __restrict__ phi, int n, double h) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P.np) return;
@@ -224,15 +295,12 @@ __global__ void k_field_forces(ParticleDev P, const double* __restrict__ phi, in
     const int* b = P.base + 3 * p;
     const double px = P.pos[3 * p], py = P.pos[3 * p + 1], pz = P.pos[3 * p + 2], chg = P.chg[p];
     double fx = 0.0, fy = 0.0, fz = 0.0;
-    for (int c = 0; c < 8; c++) {
-        int di, dj, dk;
-        corner_offsets(c, di, dj, dk);
-        const int i = di ? wrap_inc(b[0], n) : b[0];
-        const int j = dj ? wrap_inc(b[1], n) : b[1];
-        const int k = dk ? wrap_inc(b[2], n) : b[2];
-        double qc = chg * w_cic(px - i * h, L, h);
-        qc = qc * w_cic(py - j * h, L, h);
-        qc = qc * w_cic(pz - k * h, L, h);
+    for (int c = 0; c < stencil_size<CAS>(); c++) {
+        int i, j, k;
+        stencil_point<CAS>(c, b, n, i, j, k);
+        double qc = chg * w_cas<CAS>(px - i * h, L, h);
+        qc = qc * w_cas<CAS>(py - j * h, L, h);
+        qc = qc * w_cas<CAS>(pz - k * h, L, h);
         const long i0 = i * n2, j0 = (long)j * n;
         const long ip = (long)wrap_inc(i, n) * n2, im = (long)wrap_dec(i, n) * n2;
         const long jp = (long)wrap_inc(j, n) * n, jm = (long)wrap_dec(j, n) * n;
@@ -249,7 +317,13 @@ __global__ void k_field_forces(ParticleDev P, const double* __restrict__ phi, in
 void field_forces(ParticleDev& P, const double* phi, int n, double h, cudaStream_t s) {
     if (P.np == 0) return;
     count_launch();
-    k_field_forces<<<(P.np + 127) / 128, 128, 0, s>>>(P, phi, n, h);
+    const int nb = (P.np + 127) / 128;
+    if (P.cas == CAS_CIC)
+        k_field_forces<CAS_CIC><<<nb, 128, 0, s>>>(P, phi, n, h);
+    else if (P.cas == CAS_SPL_QUADR)
+        k_field_forces<CAS_SPL_QUADR><<<nb, 128, 0, s>>>(P, phi, n, h);
+    else
+        k_field_forces<CAS_SPL_CUBIC><<<nb, 128, 0, s>>>(P, phi, n, h);
     MZB_CHECK(cudaGetLastError());
 }
 

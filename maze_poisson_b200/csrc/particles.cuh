@@ -10,6 +10,10 @@ namespace mzb {
 constexpr int kTileI = 4, kTileJ = 4, kTileK = 32;
 constexpr int kTileCap = 2048;  // candidate ions one tile CTA can hold (see spread_tiles)
 
+// Charge assignment schemes (particles.c:28): CIC (8 points), quadratic and cubic
+// B-splines (4 x 4 x 4 = 64 points, offsets -1..2 around floor(pos/h)).
+enum CasType { CAS_CIC = 0, CAS_SPL_QUADR = 1, CAS_SPL_CUBIC = 2 };
+
 struct ParticleDev {
     int np = 0, ntyp = 0, n = 0;
     double L = 0, h = 0, rcut = 0;
@@ -22,7 +26,8 @@ struct ParticleDev {
     double* mass = nullptr;
     double* chg = nullptr;
     double* tab = nullptr;   // [ntyp*ntyp][7] Tosi-Fumi table
-    int32_t* base = nullptr; // [np][3] CIC base cell (wrapped)
+    int32_t* base = nullptr; // [np][3] base cell floor(pos/h) (wrapped)
+    int cas = CAS_CIC;       // charge assignment scheme
 
     // spreading bins
     int ntiles = 0, nti = 0, ntj = 0, ntk = 0;

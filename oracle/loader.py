@@ -48,6 +48,9 @@ KERNELS = {
     "orc_cic_neighbors": (None, [_f, _c.c_int, _c.c_int, _c.c_double, _i64]),
     "orc_spread_cic": (_c.c_double, [_f, _f, _i64, _c.c_int, _c.c_int, _c.c_double, _f]),
     "orc_force_fd": (_c.c_double, [_f, _i64, _f, _f, _c.c_int, _c.c_int, _c.c_double, _f]),
+    "orc_spline_neighbors": (None, [_f, _c.c_int, _c.c_int, _c.c_double, _i64]),
+    "orc_spread_scheme": (_c.c_double, [_f, _f, _c.c_int, _c.c_int, _c.c_double, _c.c_int, _f, _c.c_void_p]),
+    "orc_force_scheme": (_c.c_double, [_f, _f, _f, _c.c_int, _c.c_int, _c.c_double, _c.c_int, _f]),
     "orc_tf_forces": (_c.c_double, [_f, _i32, _f, _c.c_int, _c.c_int, _c.c_double, _c.c_double, _f]),
     "orc_tf_table": (None, [_f, _c.c_int, _c.c_double, _f]),
     "orc_cell_list": (None, [_f, _c.c_int, _c.c_double, _c.c_int, _i32, _i32]),

@@ -282,6 +282,113 @@ static inline double w_cic(double x, double L, double h) {
     return 1.0 - x / h;
 }
 
+void orc_cic_neighbors(const double *pos, int np, int n, double h, int64_t *nbr);
+
+/* Quadratic and cubic B-spline weights (charges.c:16-38), with the reference's own pow()
+   calls so that the oracle reproduces glibc's rounding. */
+static double w_spl_quadr(double x, double L, double h) {
+    x = fabs(x - round(x / L) * L) / h;
+    if (x < 0.5) return 0.75 - x * x;
+    if (x < 1.5) return 0.5 * pow((1.5 - x), 2);
+    return 0.0;
+}
+static double w_spl_cubic(double x, double L, double h) {
+    x = fabs(x - round(x / L) * L) / h;
+    if (x < 1) return (4.0 - 6.0 * pow(x, 2) + 3.0 * pow(x, 3)) / 6.0;
+    if (x < 2) return pow(2 - x, 3) / 6.0;
+    return 0.0;
+}
+static double w_cic_fn(double x, double L, double h) { return w_cic(x, L, h); }
+
+typedef double (*weight_fn)(double, double, double);
+static weight_fn scheme_weight(int cas) {
+    return cas == 1 ? w_spl_quadr : (cas == 2 ? w_spl_cubic : w_cic_fn);
+}
+static int scheme_points(int cas) { return cas == 0 ? 8 : 64; }
+
+/* 4 x 4 x 4 points around floor(pos/h), offsets -1..2 nested a (x), b (y), c (z), each
+   wrapped as (base + off + n) % n (particles.c:348-385). */
+void orc_spline_neighbors(const double *pos, int np, int n, double h, int64_t *nbr) {
+    for (long p = 0; p < np; p++) {
+        long b[3];
+        for (int d = 0; d < 3; d++) b[d] = (long)(int)floor(pos[3 * p + d] / h);
+        long o = p * 64 * 3;
+        for (int a = -1; a <= 2; a++)
+            for (int bb = -1; bb <= 2; bb++)
+                for (int cc = -1; cc <= 2; cc++) {
+                    nbr[o++] = wrap(b[0] + a + n, n);
+                    nbr[o++] = wrap(b[1] + bb + n, n);
+                    nbr[o++] = wrap(b[2] + cc + n, n);
+                }
+    }
+}
+
+/* Zero q, then scatter chg*w over each ion's `nnb` stencil points in ion order
+   (charges.c:100-144). Returns the total spread charge. */
+static double spread_scheme(const double *pos, const double *chg, const int64_t *nbr, int nnb, int np,
+                            int n, double h, double *q, weight_fn g) {
+    double L = n * h, tot = 0.0;
+    memset(q, 0, (size_t)n * n * n * sizeof(double));
+    for (long p = 0; p < np; p++) {
+        const int64_t *nb = nbr + p * nnb * 3;
+        for (int c = 0; c < nnb; c++) {
+            long a = nb[3 * c], b = nb[3 * c + 1], e = nb[3 * c + 2];
+            double w = g(pos[3 * p] - a * h, L, h) * g(pos[3 * p + 1] - b * h, L, h);
+            w = w * g(pos[3 * p + 2] - e * h, L, h);
+            double u = chg[p] * w;
+            tot += u;
+            q[(a * n + b) * n + e] += u;
+        }
+    }
+    return tot;
+}
+
+/* Field force by central differences of phi at each ion's stencil points
+   (forces.c:26-100). Returns the sum of the stencil charges. */
+static double force_scheme(const double *phi, const int64_t *nbr, int nnb, const double *chg,
+                           const double *pos, int np, int n, double h, double *f, weight_fn g) {
+    double L = n * h, h2 = 2.0 * h, sq = 0.0;
+    for (long p = 0; p < np; p++) {
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        const int64_t *nb = nbr + p * nnb * 3;
+        for (int c = 0; c < nnb; c++) {
+            long i = nb[3 * c], j = nb[3 * c + 1], k = nb[3 * c + 2];
+            double qc = chg[p] * g(pos[3 * p] - i * h, L, h);
+            qc = qc * g(pos[3 * p + 1] - j * h, L, h);
+            qc = qc * g(pos[3 * p + 2] - k * h, L, h);
+            sq += qc;
+            fx += qc * ((phi[gidx(i - 1, j, k, n)] - phi[gidx(i + 1, j, k, n)]) / h2);
+            fy += qc * ((phi[gidx(i, j - 1, k, n)] - phi[gidx(i, j + 1, k, n)]) / h2);
+            fz += qc * ((phi[gidx(i, j, k - 1, n)] - phi[gidx(i, j, k + 1, n)]) / h2);
+        }
+        f[3 * p] = fx; f[3 * p + 1] = fy; f[3 * p + 2] = fz;
+    }
+    return sq;
+}
+
+/* Spreading / field force for scheme cas (0 CIC, 1 SPL_QUADR, 2 SPL_CUBIC) with the
+   scheme's neighbour list built inside; nbr (np * points * 3) receives it if not null. */
+double orc_spread_scheme(const double *pos, const double *chg, int np, int n, double h, int cas,
+                         double *q, int64_t *nbr_out) {
+    int nnb = scheme_points(cas);
+    int64_t *nbr = nbr_out ? nbr_out : malloc((size_t)np * nnb * 3 * sizeof(int64_t));
+    if (cas == 0) orc_cic_neighbors(pos, np, n, h, nbr);
+    else orc_spline_neighbors(pos, np, n, h, nbr);
+    double t = spread_scheme(pos, chg, nbr, nnb, np, n, h, q, scheme_weight(cas));
+    if (!nbr_out) free(nbr);
+    return t;
+}
+double orc_force_scheme(const double *phi, const double *chg, const double *pos, int np, int n, double h,
+                        int cas, double *f) {
+    int nnb = scheme_points(cas);
+    int64_t *nbr = malloc((size_t)np * nnb * 3 * sizeof(int64_t));
+    if (cas == 0) orc_cic_neighbors(pos, np, n, h, nbr);
+    else orc_spline_neighbors(pos, np, n, h, nbr);
+    double s = force_scheme(phi, nbr, nnb, chg, pos, np, n, h, f, scheme_weight(cas));
+    free(nbr);
+    return s;
+}
+
 /* Base cell floor(pos/h) and its 8 wrapped corners in the reference's order
    (particles.c:297-346). A base index outside [0,n) (a position at or beyond the box
    edge, where the reference indexes out of bounds) is wrapped. */
@@ -429,6 +536,7 @@ static struct {
     int32_t *types;
     double *pos, *vel, *fe, *fn, *ft, *mass, *chg, *tab;
     int64_t *nbr;
+    int cas, nnb;
 } P;
 static struct {
     int type, enabled;
@@ -459,8 +567,9 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
                                  int cas_type, int *types, double *pos, double *vel, double *mass,
                                  double *charges, double *pot_params) {
     if (pot_type != 0) die("only the Tosi-Fumi potential is restated");
-    if (cas_type != 0) die("only CIC charge assignment is restated");
+    if (cas_type < 0 || cas_type > 2) die("bad charge assignment scheme");
     P.np = n_p; P.ntyp = n_typ; P.n = n; P.L = L; P.h = h; P.rcut = L / 2.0;
+    P.cas = cas_type; P.nnb = scheme_points(cas_type);
     size_t v3 = (size_t)3 * n_p * sizeof(double);
     P.types = malloc(n_p * sizeof(int32_t)); memcpy(P.types, types, n_p * sizeof(int32_t));
     P.pos = malloc(v3); memcpy(P.pos, pos, v3);
@@ -469,7 +578,7 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
     P.chg = malloc(n_p * sizeof(double)); memcpy(P.chg, charges, n_p * sizeof(double));
     P.fe = calloc(3 * n_p, sizeof(double)); P.fn = calloc(3 * n_p, sizeof(double));
     P.ft = calloc(3 * n_p, sizeof(double));
-    P.nbr = malloc((size_t)n_p * 24 * sizeof(int64_t));
+    P.nbr = malloc((size_t)n_p * P.nnb * 3 * sizeof(int64_t));
     P.tab = malloc((size_t)n_typ * n_typ * 7 * sizeof(double));
     orc_tf_table(pot_params, n_typ, L, P.tab);
 }
@@ -488,8 +597,9 @@ void solver_initialize_integrator(int n_p, double dt, double T, double gamma, in
 }
 
 int solver_update_charges(void) {
-    orc_cic_neighbors(P.pos, P.np, P.n, P.h, P.nbr);
-    double qt = orc_spread_cic(P.pos, P.chg, P.nbr, P.np, G.n, G.h, G.q);
+    if (P.cas == 0) orc_cic_neighbors(P.pos, P.np, P.n, P.h, P.nbr);
+    else orc_spline_neighbors(P.pos, P.np, P.n, P.h, P.nbr);
+    double qt = spread_scheme(P.pos, P.chg, P.nbr, P.nnb, P.np, G.n, G.h, G.q, scheme_weight(P.cas));
     if (fabs(q_tot_prev - qt) > 1e-6) {
         printf("Charge conservation error: q_tot = %.6f, q_tot_loc = %.6f\n", q_tot_prev, qt);
         exit(1);
@@ -578,7 +688,7 @@ void solver_set_field(double *phi) { memcpy(G.phi, phi, G.m * sizeof(double)); }
 void solver_set_field_prev(double *phi) { memcpy(G.phi_prev, phi, G.m * sizeof(double)); }
 
 void solver_compute_forces_elec(void) {
-    orc_force_fd(G.phi, P.nbr, P.chg, P.pos, P.np, P.n, P.h, P.fe);
+    force_scheme(G.phi, P.nbr, P.nnb, P.chg, P.pos, P.np, P.n, P.h, P.fe, scheme_weight(P.cas));
 }
 double solver_compute_forces_noel(void) {
     return orc_tf_forces(P.pos, P.types, P.tab, P.ntyp, P.np, P.L, P.rcut, P.fn);

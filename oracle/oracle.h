@@ -33,6 +33,13 @@ void orc_mg_apply(const double *rhs, double *x, int n, int sm);                /
 
 /* particle kernels */
 void orc_cic_neighbors(const double *pos, int np, int n, double h, int64_t *nbr);      /* particles.c:297-346 */
+void orc_spline_neighbors(const double *pos, int np, int n, double h, int64_t *nbr);   /* particles.c:348-385 */
+/* spreading / field force for scheme cas (0 CIC, 1 SPL_QUADR, 2 SPL_CUBIC; charges.c:8-38,
+   100-144, forces.c:26-100); nbr_out (np * points * 3) receives the neighbour list if set */
+double orc_spread_scheme(const double *pos, const double *chg, int np, int n, double h, int cas,
+                         double *q, int64_t *nbr_out);
+double orc_force_scheme(const double *phi, const double *chg, const double *pos, int np, int n,
+                        double h, int cas, double *f);
 double orc_spread_cic(const double *pos, const double *chg, const int64_t *nbr, int np,
                       int n, double h, double *q);                                       /* charges.c:100-144 */
 double orc_force_fd(const double *phi, const int64_t *nbr, const double *chg,

@@ -125,14 +125,18 @@ SCENARIOS = {
     "maze_multigrid": (2, 32, "MAZE-MULTIGRID", "NONE", 1e-8, "VERLET", False, 3),
     "ovrvo_nothermo": (2, 16, "LCG", "NONE", 1e-10, "OVRVO", False, 5),
     "verlet_thermo": (2, 16, "LCG", "NONE", 1e-10, "VERLET", True, 3),
+    # B-spline charge assignment (charges.c:16-38, particles.c:348-385)
+    "spl_quadr": (2, 16, "LCG", "NONE", 1e-10, "VERLET", False, 3, "SPL_QUADR"),
+    "spl_cubic": (2, 16, "LCG", "NONE", 1e-10, "VERLET", False, 3, "SPL_CUBIC"),
 }
 
 
 def scenario(ref_path, name, spec):
-    ncell, ng, method, precond, tol, itg, thermo, steps = spec
+    ncell, ng, method, precond, tol, itg, thermo, steps = spec[:8]
+    cas = spec[8] if len(spec) > 8 else "CIC"
     system = make_system(ncell, ng, density=1.379, T=1200.0, seed=7)
     run = MDRun(CAPI(ref_path, extensions=False), system, method=method, precond=precond, tol=tol,
-                integrator=itg, thermostat=thermo)
+                integrator=itg, thermostat=thermo, cas=cas)
     run.initialize()
     st = run.state()
     rec = {"init_q_sha": np.array(sha(st["q"])), "init_field_sha": np.array(sha(st["field"])),
@@ -176,15 +180,22 @@ def linked_cells():
 
 
 def main():
+    only = None
+    if "--only" in sys.argv:  # regenerate just these scenarios (comma-separated)
+        only = set(sys.argv[sys.argv.index("--only") + 1].split(","))
     loader.build(ref=True)
-    ref = ctypes.CDLL(loader.REF_SO, mode=ctypes.RTLD_LOCAL)
-    data = kernel_cases(ref)
-    np.savez_compressed(os.path.join(OUT, "kernels.npz"), **data)
+    if only is None:
+        ref = ctypes.CDLL(loader.REF_SO, mode=ctypes.RTLD_LOCAL)
+        data = kernel_cases(ref)
+        np.savez_compressed(os.path.join(OUT, "kernels.npz"), **data)
     for name, spec in SCENARIOS.items():
+        if only is not None and name not in only:
+            continue
         rec = scenario(loader.REF_SO, name, spec)
         np.savez_compressed(os.path.join(OUT, f"md_{name}.npz"), **rec)
         print(name, "done", flush=True)
-    np.savez_compressed(os.path.join(OUT, "linked_cells.npz"), **linked_cells())
+    if only is None:
+        np.savez_compressed(os.path.join(OUT, "linked_cells.npz"), **linked_cells())
     with open(os.path.join(OUT, "scenarios.json"), "w") as f:
         json.dump({k: list(v) for k, v in SCENARIOS.items()}, f, indent=1)
 

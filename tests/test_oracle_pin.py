@@ -71,11 +71,12 @@ SCEN = json.load(open(os.path.join(GOLDEN, "scenarios.json")))
 
 @pytest.mark.parametrize("name", sorted(SCEN))
 def test_md_scenario_bitexact(oracle_path, name):
-    ncell, ng, method, precond, tol, itg, thermo, steps = SCEN[name]
+    ncell, ng, method, precond, tol, itg, thermo, steps = SCEN[name][:8]
+    cas = SCEN[name][8] if len(SCEN[name]) > 8 else "CIC"
     g = np.load(os.path.join(GOLDEN, f"md_{name}.npz"))
     system = make_system(ncell, ng, density=1.379, T=1200.0, seed=7)
     run = MDRun(CAPI(oracle_path, extensions=False), system, method=method, precond=precond, tol=tol,
-                integrator=itg, thermostat=thermo)
+                integrator=itg, thermostat=thermo, cas=cas)
     run.initialize()
     try:
         st = run.state()
