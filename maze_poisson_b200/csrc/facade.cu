@@ -483,7 +483,7 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
                                  double* pot_params) {
     System& s = sys();
     touch(s);
-    if (pot_type != 0) fatal("only the Tosi-Fumi potential (TF) is supported by this build");
+    if (pot_type < 0 || pot_type > 2) fatal("invalid potential type");
     if (cas_type < 0 || cas_type > 2) fatal("invalid charge assignment scheme");
     if (cas_type != CAS_CIC && n < 4)  // offsets -1..2 would wrap onto the same point
         fatal("B-spline charge assignment needs a grid of at least 4 points per side");
@@ -514,18 +514,36 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
         MZB_CHECK(cudaMemcpy(P.mass, mass, sizeof(double) * n_p, cudaMemcpyHostToDevice));
         MZB_CHECK(cudaMemcpy(P.chg, charges, sizeof(double) * n_p, cudaMemcpyHostToDevice));
     }
-    // Tosi-Fumi constants per type pair (particles.c:181-228)
-    std::vector<double> tab((size_t)n_typ * n_typ * 7);
+    // pair-potential constants per type pair, 7 doubles each, with the shifted-force
+    // constants at r_cut = L/2
+    P.pot = pot_type;
+    std::vector<double> tab((size_t)n_typ * n_typ * 7, 0.0);
     const double rc = L / 2.0, rc6 = pow(rc, 6), rc7 = rc6 * rc, rc8 = rc7 * rc, rc9 = rc8 * rc;
     for (int t = 0; t < n_typ * n_typ; t++) {
-        const double A = pot_params[5 * t], B = pot_params[5 * t + 1], C = pot_params[5 * t + 2],
-                     D = pot_params[5 * t + 3], sg = pot_params[5 * t + 4];
-        const double ea = exp(B * (sg - rc));
-        const double vs = A * ea - C / rc6 - D / rc8;
-        const double al = A * B * ea - 6 * C / rc7 - 8 * D / rc9;
-        const double be = -vs - al * rc;
         double* o = &tab[7 * t];
-        o[0] = A; o[1] = B; o[2] = C; o[3] = D; o[4] = sg; o[5] = al; o[6] = be;
+        if (pot_type == POT_TF) {  // particles.c:181-228: [A, B, C, D, sigma, alpha, beta]
+            const double A = pot_params[5 * t], B = pot_params[5 * t + 1], C = pot_params[5 * t + 2],
+                         D = pot_params[5 * t + 3], sg = pot_params[5 * t + 4];
+            const double ea = exp(B * (sg - rc));
+            const double vs = A * ea - C / rc6 - D / rc8;
+            const double al = A * B * ea - 6 * C / rc7 - 8 * D / rc9;
+            const double be = -vs - al * rc;
+            o[0] = A; o[1] = B; o[2] = C; o[3] = D; o[4] = sg; o[5] = al; o[6] = be;
+        } else if (pot_type == POT_LJ) {
+            // particles.c:230-266: [sigma, epsilon, alpha, beta]. pot_params holds [sigma,
+            // epsilon] per type pair as solver.py:241-270 passes it; the reference reads
+            // it with a stride of 4 (particles.c:241), past the array for two or more
+            // types -- with one type both agree.
+            const double sg = pot_params[2 * t], ep = pot_params[2 * t + 1];
+            const double vs = 4 * ep * (pow(sg / rc, 12) - pow(sg / rc, 6));
+            const double al = 4 * (12 * ep * pow(sg / rc, 12) - 6 * ep * pow(sg / rc, 6)) / rc;
+            o[0] = sg; o[1] = ep; o[2] = al; o[3] = -vs - al * rc;
+        } else {  // particles.c:268-295: [nu, d, B, alpha, beta], shared by every pair
+            const double nu = pot_params[0], d = pot_params[1], B = pot_params[2];
+            const double drp = pow(d / rc, nu);
+            const double al = B * nu * drp / rc;
+            o[0] = nu; o[1] = d; o[2] = B; o[3] = al; o[4] = -B * drp - al * rc;
+        }
     }
     P.tab = dalloc<double>(tab.size());
     MZB_CHECK(cudaMemcpy(P.tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));

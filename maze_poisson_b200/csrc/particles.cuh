@@ -13,6 +13,8 @@ constexpr int kTileCap = 2048;  // candidate ions one tile CTA can hold (see spr
 // Charge assignment schemes (particles.c:28): CIC (8 points), quadratic and cubic
 // B-splines (4 x 4 x 4 = 64 points, offsets -1..2 around floor(pos/h)).
 enum CasType { CAS_CIC = 0, CAS_SPL_QUADR = 1, CAS_SPL_CUBIC = 2 };
+// Pair potentials (particles.c:17): Tosi-Fumi, Lennard-Jones, soft-core repulsion.
+enum PotType { POT_TF = 0, POT_LJ = 1, POT_SC = 2 };
 
 struct ParticleDev {
     int np = 0, ntyp = 0, n = 0;
@@ -25,9 +27,10 @@ struct ParticleDev {
     double* ft = nullptr;
     double* mass = nullptr;
     double* chg = nullptr;
-    double* tab = nullptr;   // [ntyp*ntyp][7] Tosi-Fumi table
+    double* tab = nullptr;   // [ntyp*ntyp][7] pair-potential constants per type pair
     int32_t* base = nullptr; // [np][3] base cell floor(pos/h) (wrapped)
     int cas = CAS_CIC;       // charge assignment scheme
+    int pot = POT_TF;        // pair potential
 
     // spreading bins
     int ntiles = 0, nti = 0, ntj = 0, ntk = 0;

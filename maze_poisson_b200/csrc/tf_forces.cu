@@ -1,5 +1,8 @@
-// Shifted-force Tosi-Fumi (Born-Mayer-Huggins) pair forces, warp per 32 cell-sorted ions
-// (reference: library/src/forces.c:112-186, parameters particles.c:181-228).
+// Shifted-force pair forces -- Tosi-Fumi (Born-Mayer-Huggins), Lennard-Jones and soft-core
+// repulsion -- warp per 32 cell-sorted ions (reference: library/src/forces.c:112-337,
+// parameters particles.c:181-295). Every potential is summed over both orders of each
+// pair and the energy halved, which for the soft-core potential equals the reference's
+// sum over i < j with Newton's third law.
 //
 // Compiled with --fmad=true: this kernel is bound by the FP64 pipe, and its results are
 // already ulp-level (exp and inverse powers) rather than bit-level equal to the
@@ -31,6 +34,35 @@ __device__ __forceinline__ double axis_gap(double lo, double hi, double c0, doub
     return best;
 }
 
+// Shifted-force pair force (times 1/r, to be multiplied by the separation vector) and
+// pair energy of one pair at r^2 with 1/r = ir, from the type pair's constants t.
+template <int POT>
+__device__ __forceinline__ void pair_terms(const double* t, double r2, double ir, double& fr, double& vm) {
+    const double r = r2 * ir;
+    if (POT == POT_TF) {  // forces.c:112-186
+        const double a = t[0], b = t[1], c = t[2], d = t[3], sg = t[4], al = t[5], be = t[6];
+        const double ir2 = ir * ir, ir6 = ir2 * ir2 * ir2;
+        const double ir7 = ir6 * ir, ir8 = ir6 * ir2, ir9 = ir8 * ir;
+        const double ex = exp(b * (sg - r));
+        const double fm = b * a * ex - 6 * c * ir7 - 8 * d * ir9 - al;
+        vm = a * ex - c * ir6 - d * ir8 + al * r + be;
+        fr = fm * ir;
+    } else if (POT == POT_LJ) {  // forces.c:199-271
+        const double sg = t[0], ep = t[1], al = t[2], be = t[3];
+        const double s = sg * ir, s2 = s * s, s6 = s2 * s2 * s2, s12 = s6 * s6;
+        const double fm = 4 * ep * (12 * s12 - 6 * s6) * ir - al;
+        vm = 4 * ep * (s12 - s6) + al * r + be;
+        fr = fm * ir;
+    } else {  // forces.c:283-337
+        const double nu = t[0], d = t[1], B = t[2], al = t[3], be = t[4];
+        const double p = pow(d * ir, nu);
+        const double fm = B * nu * p * ir - al;
+        vm = B * p + al * r + be;
+        fr = fm * ir;
+    }
+}
+
+template <int POT>
 __global__ void __launch_bounds__(kTfWarps * 32) k_tf(ParticleDev P) {
     __shared__ double tab[64 * 7];
     for (int x = threadIdx.x; x < P.ntyp * P.ntyp * 7; x += blockDim.x) tab[x] = P.tab[x];
@@ -85,14 +117,8 @@ __global__ void __launch_bounds__(kTfWarps * 32) k_tf(ParticleDev P) {
             dz -= L * round(dz * invL);
             const double r2 = dx * dx + dy * dy + dz * dz;
             if (r2 > rc2) continue;
-            const double* t = tab + 7 * (ti * ntyp + tj);
-            const double a = t[0], b = t[1], c = t[2], d = t[3], sg = t[4], al = t[5], be = t[6];
-            const double ir = rsqrt(r2), r = r2 * ir, ir2 = ir * ir, ir6 = ir2 * ir2 * ir2;
-            const double ir7 = ir6 * ir, ir8 = ir6 * ir2, ir9 = ir8 * ir;
-            const double ex = exp(b * (sg - r));
-            const double fm = b * a * ex - 6 * c * ir7 - 8 * d * ir9 - al;
-            const double vm = a * ex - c * ir6 - d * ir8 + al * r + be;
-            const double fr = fm * ir;
+            double fr, vm;
+            pair_terms<POT>(tab + 7 * (ti * ntyp + tj), r2, rsqrt(r2), fr, vm);
             fx += fr * dx;
             fy += fr * dy;
             fz += fr * dz;
@@ -140,10 +166,16 @@ void tf_forces(ParticleDev& P, cudaStream_t s) {
         MZB_CHECK(cudaMemsetAsync(P.red + 1, 0, sizeof(double), s));
         return;
     }
-    if (P.ntyp * P.ntyp > 64) fatal("Tosi-Fumi: more than 8 particle types");
+    if (P.ntyp * P.ntyp > 64) fatal("pair forces: more than 8 particle types");
     const long warps = (long)((P.np + 31) / 32) * P.tf_split;
     count_launch();
-    k_tf<<<(unsigned)((warps + kTfWarps - 1) / kTfWarps), kTfWarps * 32, 0, s>>>(P);
+    const unsigned nb = (unsigned)((warps + kTfWarps - 1) / kTfWarps);
+    if (P.pot == POT_LJ)
+        k_tf<POT_LJ><<<nb, kTfWarps * 32, 0, s>>>(P);
+    else if (P.pot == POT_SC)
+        k_tf<POT_SC><<<nb, kTfWarps * 32, 0, s>>>(P);
+    else
+        k_tf<POT_TF><<<nb, kTfWarps * 32, 0, s>>>(P);
     count_launch();
     k_tf_gather<<<(P.np + 127) / 128, 128, 0, s>>>(P);
     count_launch();

@@ -18,7 +18,7 @@ def gamma_au(gamma_per_ps):
 class MDRun:
     def __init__(self, capi, system, method="LCG", precond="NONE", tol=1e-7, integrator="VERLET",
                  thermostat=False, T=1200.0, gamma_per_ps=1.0, dt_fs=1.0, eps_s=1.0, eps_int=1.0,
-                 rescale=False, precision=0, mixed_tol=0.0, cas="CIC"):
+                 rescale=False, precision=0, mixed_tol=0.0, cas="CIC", pot="TF"):
         self.capi = capi
         self.sys = system
         self.method = method.upper()
@@ -33,6 +33,7 @@ class MDRun:
         self.eps_int = eps_int
         self.rescale = rescale
         self.cas = cas.upper()  # charge assignment: CIC, SPL_QUADR, SPL_CUBIC
+        self.pot = pot.upper()  # pair potential: TF, LJ, SC (system.pot_params to match)
         # field-solve precision (this build's extension): 0 FP64 reference algorithms,
         # 1 FP32 multigrid + FP64 refinement to mixed_tol (or tol when 0)
         self.precision = precision
@@ -50,7 +51,7 @@ class MDRun:
                                  maps["method"][self.method], maps["precond"][self.precond])
         if self.precision:
             c.mzb_set_precision(int(self.precision), float(self.mixed_tol))
-        c.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, maps["potential"]["TF"],
+        c.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, maps["potential"][self.pot],
                                       maps["cas"][self.cas], s.types, s.pos, s.vel, s.mass, s.charges,
                                       s.pot_params)
         c.solver_initialize_integrator(s.n_ions, self.dt, self.T, self.gamma,

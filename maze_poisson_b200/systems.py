@@ -114,6 +114,59 @@ def make_system(ncell, n_grid, density=1.379, T=1200.0, seed=0, jitter=0.1):
                       pot_params=tf_params_au())
 
 
+# Lennard-Jones Na+/Cl- pairs: (type1, type2, sigma [A], epsilon [kJ/mol])
+LENNARD_JONES = (("Na", "Na", 2.350, 0.544), ("Na", "Cl", 3.370, 0.477), ("Cl", "Cl", 4.400, 0.418))
+
+
+def lj_params_au():
+    """[sigma, epsilon] per type pair in a.u. (the conversion of solver.py:266-269), laid out
+    so that both readers see the same table: the pairs (0,0), (0,1), (1,0), (1,1) sit at
+    doubles 0, 2, 4, 6 (stride 2, the layout solver.py passes and this build reads) and at
+    doubles 0, 4, 8, 12 (stride 4, the reference's read, particles.c:241)."""
+    names = [s[0] for s in SPECIES]
+    tab = {}
+    for t1, t2, sg, ep in LENNARD_JONES:
+        v = (sg / A0, ep * KJMOL_TO_HARTREE)
+        tab[(names.index(t1), names.index(t2))] = v
+        tab[(names.index(t2), names.index(t1))] = v
+    out = np.zeros(14)
+    for k, pair in enumerate([(0, 0), (0, 1), (1, 0), (1, 1)]):
+        out[2 * k:2 * k + 2] = tab[pair]
+        out[4 * k:4 * k + 2] = tab[pair]
+    assert np.array_equal(out[:8].reshape(4, 2), out[[0, 1, 4, 5, 8, 9, 12, 13]].reshape(4, 2))
+    return np.ascontiguousarray(out, dtype=np.float64)
+
+
+def sc_params_au(nu=8.0, d_ang=2.8):
+    """[nu, d, B] of the soft-core repulsion in a.u., B = 1.74 / (6 nu d) as
+    solver.py:207-233 derives it."""
+    d = d_ang / A0
+    return np.ascontiguousarray([nu, d, 1.74 / (6 * nu * d)], dtype=np.float64)
+
+
+def make_lj_system(ncell, n_grid, density=1.379, T=1200.0, seed=0, jitter=0.1):
+    """The NaCl melt of make_system with Lennard-Jones pairs instead of Tosi-Fumi."""
+    s = make_system(ncell, n_grid, density=density, T=T, seed=seed, jitter=jitter)
+    s.pot_params = lj_params_au()
+    return s
+
+
+def make_sc_system(ncell, n_grid, density=1.379, T=1200.0, seed=0, jitter=0.1):
+    """The NaCl melt of make_system with the soft-core repulsion instead of Tosi-Fumi."""
+    s = make_system(ncell, n_grid, density=density, T=T, seed=seed, jitter=jitter)
+    s.pot_params = sc_params_au()
+    return s
+
+
+def pair_system(ncell, n_grid, pot="TF", density=1.379, T=1200.0, seed=0):
+    """make_system with the pair potential's parameters (TF, LJ or SC)."""
+    if pot == "LJ":
+        return make_lj_system(ncell, n_grid, density=density, T=T, seed=seed)
+    if pot == "SC":
+        return make_sc_system(ncell, n_grid, density=density, T=T, seed=seed)
+    return make_system(ncell, n_grid, density=density, T=T, seed=seed)
+
+
 # Workloads of the reference's configurations (sizes only; solver settings in md.py)
 WORKLOADS = {
     "nacl250_64": dict(ncell=5, n_grid=64, density=1.379),

@@ -494,6 +494,107 @@ double orc_tf_forces(const double *pos, const int32_t *types, const double *tab,
     return en / 2;
 }
 
+/* Lennard-Jones table per type pair [sigma, epsilon, alpha, beta, 0, 0, 0] with the
+   shifted-force constants at r_cut = L/2 (particles.c:230-266). pot_params holds
+   [sigma, epsilon] per type pair, the layout solver.py:241-270 passes; the reference
+   indexes it with a stride of 4 (particles.c:241), which reads past the array for two
+   or more types -- with one type both agree. */
+void orc_lj_table(const double *pp, int ntyp, double L, double *tab) {
+    double rc = L / 2.0;
+    for (int t = 0; t < ntyp * ntyp; t++) {
+        double sigma = pp[2 * t], eps = pp[2 * t + 1];
+        double vs = 4 * eps * (pow(sigma / rc, 12) - pow(sigma / rc, 6));
+        double al = 4 * (12 * eps * pow(sigma / rc, 12) - 6 * eps * pow(sigma / rc, 6)) / rc;
+        double be = -vs - al * rc;
+        double *o = tab + 7 * t;
+        o[0] = sigma; o[1] = eps; o[2] = al; o[3] = be; o[4] = 0; o[5] = 0; o[6] = 0;
+    }
+}
+
+/* All-pairs shifted-force Lennard-Jones, both orders, j ascending (forces.c:199-271).
+   Returns half the summed pair energy. */
+double orc_lj_forces(const double *pos, const int32_t *types, const double *tab, int ntyp, int np,
+                     double L, double rcut, double *f) {
+    double en = 0.0;
+    for (long i = 0; i < np; i++) {
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (long j = 0; j < np; j++) {
+            if (i == j) continue;
+            double d[3], r;
+            double x = pos[3 * i] - pos[3 * j];
+            x -= L * round(x / L);
+            r = x * x;
+            d[0] = x;
+            x = pos[3 * i + 1] - pos[3 * j + 1];
+            x -= L * round(x / L);
+            d[1] = x;
+            r += x * x;
+            x = pos[3 * i + 2] - pos[3 * j + 2];
+            x -= L * round(x / L);
+            d[2] = x;
+            r += x * x;
+            r = sqrt(r);
+            if (r > rcut) continue;
+            d[0] /= r; d[1] /= r; d[2] /= r;
+            const double *t = tab + 7 * (types[i] * ntyp + types[j]);
+            double sigma = t[0], eps = t[1], al = t[2], be = t[3];
+            double fm = 4 * eps * (12 * pow(sigma / r, 12) - 6 * pow(sigma / r, 6)) / r - al;
+            double vm = 4 * eps * (pow(sigma / r, 12) - pow(sigma / r, 6)) + al * r + be;
+            fx += fm * d[0];
+            fy += fm * d[1];
+            fz += fm * d[2];
+            en += vm;
+        }
+        f[3 * i] = fx; f[3 * i + 1] = fy; f[3 * i + 2] = fz;
+    }
+    return en / 2;
+}
+
+/* Soft-core repulsion table [nu, d, B, alpha, beta, 0, 0] (particles.c:268-295; the same
+   for every type pair). */
+void orc_sc_table(const double *pp, int ntyp, double L, double *tab) {
+    double nu = pp[0], d = pp[1], B = pp[2], rc = 0.5 * L;
+    double dr = d / rc, drp = pow(dr, nu);
+    double al = B * nu * drp / rc;
+    double be = -B * drp - al * rc;
+    for (int t = 0; t < ntyp * ntyp; t++) {
+        double *o = tab + 7 * t;
+        o[0] = nu; o[1] = d; o[2] = B; o[3] = al; o[4] = be; o[5] = 0; o[6] = 0;
+    }
+}
+
+/* Soft-core forces over pairs i < j with Newton's third law (forces.c:283-337), serial
+   semantics: the reference's `omp parallel` without `for` runs the whole loop on every
+   thread, which multiplies forces and energy by the thread count above one thread.
+   Returns the summed pair energy. */
+double orc_sc_forces(const double *pos, const double *tab, int np, double L, double rcut, double *f) {
+    double nu = tab[0], d = tab[1], B = tab[2], al = tab[3], be = tab[4], en = 0.0;
+    memset(f, 0, (size_t)3 * np * sizeof(double));
+    for (long i = 0; i < np; i++) {
+        for (long j = i + 1; j < np; j++) {
+            double rd[3], r = 0.0;
+            for (int k = 0; k < 3; k++) {
+                double x = pos[3 * i + k] - pos[3 * j + k];
+                x -= L * round(x / L);
+                r += x * x;
+                rd[k] = x;
+            }
+            r = sqrt(r);
+            if (r > rcut) continue;
+            double p = pow(d / r, nu);
+            double vm = B * p + al * r + be;
+            double fm = B * nu * p / r - al;
+            for (int k = 0; k < 3; k++) {
+                double fk = fm * rd[k] / r;
+                f[3 * i + k] += fk;
+                f[3 * j + k] -= fk;
+            }
+            en += vm;
+        }
+    }
+    return en;
+}
+
 /* Linked cells as a CSR list: cell (IX,IY,IZ) with IX = int((nc/L) * x)
    (maze_poisson/linkedcell.py:18-26), ions of a cell in ascending index (the reverse of
    the reference's header/link chain). Out-of-range coordinates are clamped. */
@@ -536,7 +637,7 @@ static struct {
     int32_t *types;
     double *pos, *vel, *fe, *fn, *ft, *mass, *chg, *tab;
     int64_t *nbr;
-    int cas, nnb;
+    int cas, nnb, pot;
 } P;
 static struct {
     int type, enabled;
@@ -566,7 +667,7 @@ void solver_initialize_grid(int n, double L, double h, double tol, double eps_s,
 void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, int pot_type,
                                  int cas_type, int *types, double *pos, double *vel, double *mass,
                                  double *charges, double *pot_params) {
-    if (pot_type != 0) die("only the Tosi-Fumi potential is restated");
+    if (pot_type < 0 || pot_type > 2) die("bad potential type");
     if (cas_type < 0 || cas_type > 2) die("bad charge assignment scheme");
     P.np = n_p; P.ntyp = n_typ; P.n = n; P.L = L; P.h = h; P.rcut = L / 2.0;
     P.cas = cas_type; P.nnb = scheme_points(cas_type);
@@ -580,7 +681,10 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
     P.ft = calloc(3 * n_p, sizeof(double));
     P.nbr = malloc((size_t)n_p * P.nnb * 3 * sizeof(int64_t));
     P.tab = malloc((size_t)n_typ * n_typ * 7 * sizeof(double));
-    orc_tf_table(pot_params, n_typ, L, P.tab);
+    P.pot = pot_type;
+    if (pot_type == 0) orc_tf_table(pot_params, n_typ, L, P.tab);
+    else if (pot_type == 1) orc_lj_table(pot_params, n_typ, L, P.tab);
+    else orc_sc_table(pot_params, n_typ, L, P.tab);
 }
 
 void solver_initialize_integrator(int n_p, double dt, double T, double gamma, int itg_type,
@@ -691,6 +795,8 @@ void solver_compute_forces_elec(void) {
     force_scheme(G.phi, P.nbr, P.nnb, P.chg, P.pos, P.np, P.n, P.h, P.fe, scheme_weight(P.cas));
 }
 double solver_compute_forces_noel(void) {
+    if (P.pot == 1) return orc_lj_forces(P.pos, P.types, P.tab, P.ntyp, P.np, P.L, P.rcut, P.fn);
+    if (P.pot == 2) return orc_sc_forces(P.pos, P.tab, P.np, P.L, P.rcut, P.fn);
     return orc_tf_forces(P.pos, P.types, P.tab, P.ntyp, P.np, P.L, P.rcut, P.fn);
 }
 void solver_compute_forces_tot(void) {                     /* particles.c:777-795 */

@@ -47,6 +47,12 @@ double orc_force_fd(const double *phi, const int64_t *nbr, const double *chg,
 double orc_tf_forces(const double *pos, const int32_t *types, const double *tab, int ntyp,
                      int np, double L, double rcut, double *f);                           /* forces.c:112-186 */
 void orc_tf_table(const double *pot_params, int ntyp, double L, double *tab);             /* particles.c:181-228 */
+void orc_lj_table(const double *pot_params, int ntyp, double L, double *tab);             /* particles.c:230-266 */
+double orc_lj_forces(const double *pos, const int32_t *types, const double *tab, int ntyp, int np,
+                     double L, double rcut, double *f);                                    /* forces.c:199-271 */
+void orc_sc_table(const double *pot_params, int ntyp, double L, double *tab);             /* particles.c:268-295 */
+double orc_sc_forces(const double *pos, const double *tab, int np, double L, double rcut,
+                     double *f);                                                           /* forces.c:283-337 */
 void orc_cell_list(const double *pos, int np, double L, int nc, int32_t *cell_start,
                    int32_t *cell_ions);                                                   /* linkedcell.py:4-53 */
 

@@ -24,7 +24,7 @@ sys.path.insert(0, ROOT)
 
 from maze_poisson_b200.c_api import CAPI  # noqa: E402
 from maze_poisson_b200.md import MDRun  # noqa: E402
-from maze_poisson_b200.systems import make_system  # noqa: E402
+from maze_poisson_b200.systems import make_system, pair_system  # noqa: E402
 from oracle import loader  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
@@ -128,15 +128,21 @@ SCENARIOS = {
     # B-spline charge assignment (charges.c:16-38, particles.c:348-385)
     "spl_quadr": (2, 16, "LCG", "NONE", 1e-10, "VERLET", False, 3, "SPL_QUADR"),
     "spl_cubic": (2, 16, "LCG", "NONE", 1e-10, "VERLET", False, 3, "SPL_CUBIC"),
+    # Lennard-Jones (parameters laid out so that the reference's stride-4 read sees the
+    # same table as the stride-2 layout, systems.lj_params_au) and soft-core pair
+    # potentials (forces.c:199-337)
+    "lj_fluid": (2, 16, "LCG", "NONE", 1e-10, "VERLET", False, 4, "CIC", "LJ"),
+    "sc_melt": (2, 16, "LCG", "NONE", 1e-10, "VERLET", False, 4, "CIC", "SC"),
 }
 
 
 def scenario(ref_path, name, spec):
     ncell, ng, method, precond, tol, itg, thermo, steps = spec[:8]
     cas = spec[8] if len(spec) > 8 else "CIC"
-    system = make_system(ncell, ng, density=1.379, T=1200.0, seed=7)
+    pot = spec[9] if len(spec) > 9 else "TF"
+    system = pair_system(ncell, ng, pot, density=1.379, T=1200.0, seed=7)
     run = MDRun(CAPI(ref_path, extensions=False), system, method=method, precond=precond, tol=tol,
-                integrator=itg, thermostat=thermo, cas=cas)
+                integrator=itg, thermostat=thermo, cas=cas, pot=pot)
     run.initialize()
     st = run.state()
     rec = {"init_q_sha": np.array(sha(st["q"])), "init_field_sha": np.array(sha(st["field"])),

@@ -19,7 +19,7 @@ import pytest
 from conftest import GOLDEN, ROOT
 from maze_poisson_b200.c_api import CAPI
 from maze_poisson_b200.md import MDRun
-from maze_poisson_b200.systems import make_system
+from maze_poisson_b200.systems import make_system, pair_system
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-10
@@ -86,10 +86,11 @@ def test_golden_scenarios(prod, name):
     """Product against the reference's own trajectories (tests/golden)."""
     ncell, ng, method, precond, tol, itg, thermo, steps = SCEN[name][:8]
     cas = SCEN[name][8] if len(SCEN[name]) > 8 else "CIC"
+    pot = SCEN[name][9] if len(SCEN[name]) > 9 else "TF"
     g = np.load(os.path.join(GOLDEN, f"md_{name}.npz"))
-    system = make_system(ncell, ng, density=1.379, T=1200.0, seed=7)
+    system = pair_system(ncell, ng, pot, density=1.379, T=1200.0, seed=7)
     run = MDRun(prod, system, method=method, precond=precond, tol=tol, integrator=itg,
-                thermostat=thermo, cas=cas)
+                thermostat=thermo, cas=cas, pot=pot)
     run.initialize()
     try:
         st = run.state()
@@ -250,7 +251,7 @@ def test_charge_conservation_failure_exits():
 import sys; sys.path.insert(0, {ROOT!r})
 import numpy as np
 from maze_poisson_b200.c_api import CAPI
-from maze_poisson_b200.systems import make_system
+from maze_poisson_b200.systems import make_system, pair_system
 s = make_system(2, 16, seed=1)
 s.charges[0] = 3.0
 c = CAPI(); c.solver_initialize()
@@ -317,3 +318,9 @@ def test_spline_kernels(prod, oracle_lib, cas):
 @pytest.mark.parametrize("cas", ["SPL_QUADR", "SPL_CUBIC"])
 def test_spline_md_250(prod, orc, cas):
     run_pair(prod, orc, make_system(5, 64, seed=13), 4, method="LCG", tol=1e-7, cas=cas)
+
+
+@pytest.mark.parametrize("pot", ["LJ", "SC"])
+def test_pair_potentials_250(prod, orc, pot):
+    """Lennard-Jones and soft-core pair forces (forces.c:199-337) through MD steps."""
+    run_pair(prod, orc, pair_system(5, 64, pot, seed=17), 4, method="LCG", tol=1e-7, pot=pot)

@@ -11,7 +11,7 @@ import pytest
 from conftest import GOLDEN
 from maze_poisson_b200.c_api import CAPI
 from maze_poisson_b200.md import MDRun
-from maze_poisson_b200.systems import make_system
+from maze_poisson_b200.systems import make_system, pair_system
 
 
 def sha(a):
@@ -73,10 +73,11 @@ SCEN = json.load(open(os.path.join(GOLDEN, "scenarios.json")))
 def test_md_scenario_bitexact(oracle_path, name):
     ncell, ng, method, precond, tol, itg, thermo, steps = SCEN[name][:8]
     cas = SCEN[name][8] if len(SCEN[name]) > 8 else "CIC"
+    pot = SCEN[name][9] if len(SCEN[name]) > 9 else "TF"
     g = np.load(os.path.join(GOLDEN, f"md_{name}.npz"))
-    system = make_system(ncell, ng, density=1.379, T=1200.0, seed=7)
+    system = pair_system(ncell, ng, pot, density=1.379, T=1200.0, seed=7)
     run = MDRun(CAPI(oracle_path, extensions=False), system, method=method, precond=precond, tol=tol,
-                integrator=itg, thermostat=thermo, cas=cas)
+                integrator=itg, thermostat=thermo, cas=cas, pot=pot)
     run.initialize()
     try:
         st = run.state()
