@@ -642,26 +642,29 @@ __device__ bool vcycle(const MixedArgs& a, const Team& tm, float* sm, unsigned& 
     return true;
 }
 
-// FP64 residual r = B - L X (X = 0 when ZERO; B = c q when RHS_Q, else tmp) written as
-// the FP32 rhs of the inner solve together with that solve's first red half-sweep from
-// e = 0; returns this thread's max |r|.
-template <bool ZERO, bool RHS_Q>
-__device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs& a, const double* X, float* e,
-                                                float* rb) {
+// FP64 residual r = B - L X written as the FP32 rhs of the inner solve together with that
+// solve's first red half-sweep from e = 0; returns this thread's max |r|. X is 0
+// (START_ZERO), X[] (START_X) or the extrapolation 2 X[] - Xp[] (START_EXTRAP); B is c q
+// when RHS_Q, else tmp.
+enum StartKind { START_ZERO, START_X, START_EXTRAP };
+template <int START, bool RHS_Q>
+__device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs& a, const double* X,
+                                                const double* Xp, float* e, float* rb) {
     const int n = a.n;
     double rmax = 0.0;
     grid_pts(tm, n, [&](int i, int j, int k) {
         const Nb o = nb_of(n, i, j, k);
+        auto x = [&](long q) { return START == START_EXTRAP ? 2 * X[q] - Xp[q] : X[q]; };
         double r;
-        if (ZERO) {
+        if (START == START_ZERO) {
             r = RHS_Q ? a.q[o.c] * a.c : a.tmp[o.c];
         } else {
-            double s = X[o.ip] + X[o.im];
-            s = s + X[o.jp];
-            s = s + X[o.jm];
-            s = s + X[o.kp];
-            s = s + X[o.km];
-            r = (RHS_Q ? a.q[o.c] * a.c : a.tmp[o.c]) - (s - X[o.c] * 6.0);
+            double s = x(o.ip) + x(o.im);
+            s = s + x(o.jp);
+            s = s + x(o.jm);
+            s = s + x(o.kp);
+            s = s + x(o.km);
+            r = (RHS_Q ? a.q[o.c] * a.c : a.tmp[o.c]) - (s - x(o.c) * 6.0);
         }
         const float rf = (float)r;
         const int sx = split_idx(n, i, j, k);
@@ -670,6 +673,18 @@ __device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs&
         rmax = fmax(rmax, fabs(r));
     });
     return rmax;
+}
+
+// home = X + (e - emean) with X as residual_pass reads it (0, X[], 2 X[] - phi_prev[]).
+template <int START>
+__device__ __forceinline__ void update_pass(const Team& tm, const MixedArgs& a, const double* X, double* home,
+                                            const float* e, double emean) {
+    const int n = a.n;
+    grid_pts(tm, n, [&](int i, int j, int k) {
+        const long c = ((long)i * n + j) * n + k;
+        const double xo = START == START_ZERO ? 0.0 : (START == START_EXTRAP ? 2 * X[c] - a.phi_prev[c] : X[c]);
+        home[c] = xo + ((double)e[split_idx(n, i, j, k)] - emean);
+    });
 }
 
 // The solve of one system by one team of CTAs.
@@ -681,14 +696,17 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
     int result = -1;
     if (tm.b == 0) stamp(a, 0);
 
-    // ---- set-up, as the FP64 programs (the unknown X, its start X0, the rhs B) ----
+    // ---- set-up, as the FP64 programs (the unknown X, its start, the rhs B) ----
     // LCG and INIT read the rhs c q on the fly and start from the old field (or 0) without
     // a set-up pass; the MaZe programs keep sigma = L(2 phi - phi_prev) + c q in tmp.
+    // (Starting the LCG update from 2 phi - phi_prev instead does not lower the first
+    // residual: it is dominated by the local change of the spread charge.)
     double* home = a.phi_new;        // where the solution must end
     const double* X0 = a.phi_old;    // the start (read-only)
-    bool zero_start = false, rhs_q = true;
+    int start = START_X;
+    bool rhs_q = true;
     if (a.prog == PROG_INIT_FIELD) {         // y = 0 (later MaZe warm starts), phi = 0 start
-        zero_start = true;
+        start = START_ZERO;
         grid_pts(tm, n, [&](int i, int j, int k) { a.y[((long)i * n + j) * n + k] = 0.0; });
     } else if (a.prog == PROG_LCG_UPDATE) {  // start from the old phi
     } else if (a.prog == PROG_MG_UPDATE) {   // start from 2 phi - phi_prev
@@ -725,14 +743,16 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
     int outer = 0;
     while (ok) {
         stamp_outer(a, outer, 0);
-        const bool zero = zero_start && outer == 0;
+        const int st = outer == 0 ? start : START_X;
         double s0 = 0.0, rmax = 0.0;
-        if (zero)
-            rmax = residual_pass<true, true>(tm, a, Xs, e, rb);
+        if (st == START_ZERO)
+            rmax = residual_pass<START_ZERO, true>(tm, a, Xs, a.phi_prev, e, rb);
+        else if (st == START_EXTRAP)
+            rmax = residual_pass<START_EXTRAP, true>(tm, a, Xs, a.phi_prev, e, rb);
         else if (rhs_q)
-            rmax = residual_pass<false, true>(tm, a, Xs, e, rb);
+            rmax = residual_pass<START_X, true>(tm, a, Xs, a.phi_prev, e, rb);
         else
-            rmax = residual_pass<false, false>(tm, a, Xs, e, rb);
+            rmax = residual_pass<START_X, false>(tm, a, Xs, a.phi_prev, e, rb);
         ok = reduce_sum_max(s0, rmax, tm, epoch, seq);
         stamp_outer(a, outer, 1);
         if (a.stamps != nullptr && outer < 8 && tm.b == 0 && threadIdx.x == 0)
@@ -752,11 +772,12 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
         if (!ok) break;
         stamp_outer(a, outer, 5);
         const double emean = esum / ((double)n * n * n);
-        grid_pts(tm, n, [&](int i, int j, int k) {
-            const long c = ((long)i * n + j) * n + k;
-            const double xo = zero ? 0.0 : Xs[c];
-            home[c] = xo + ((double)e[split_idx(n, i, j, k)] - emean);
-        });
+        if (st == START_ZERO)
+            update_pass<START_ZERO>(tm, a, Xs, home, e, emean);
+        else if (st == START_EXTRAP)
+            update_pass<START_EXTRAP>(tm, a, Xs, home, e, emean);
+        else
+            update_pass<START_X>(tm, a, Xs, home, e, emean);
         Xs = home;
         ok = team_sync(tm, epoch);
         stamp_outer(a, outer, 6);
@@ -766,7 +787,7 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
     if (ok && Xs != home) {
         grid_pts(tm, n, [&](int i, int j, int k) {
             const long c = ((long)i * n + j) * n + k;
-            home[c] = zero_start ? 0.0 : Xs[c];
+            home[c] = start == START_ZERO ? 0.0 : (start == START_EXTRAP ? 2 * Xs[c] - a.phi_prev[c] : Xs[c]);
         });
         ok = team_sync(tm, epoch);
     }
