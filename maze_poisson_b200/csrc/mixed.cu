@@ -347,7 +347,7 @@ __device__ __forceinline__ void split_nb_sums(const float* xo, const Rows& o, in
 }
 
 // half-sweep of colour c; when acc is not null the new values are summed into it
-__device__ void split_gs(const Team& tm, int n, int c, const float* b, float* x, double* acc) {
+__device__ void split_gs_scalar(const Team& tm, int n, int c, const float* b, float* x, double* acc) {
     const int lane = threadIdx.x & 31, h = n >> 1;
     const int hp = h * n * n;
     const float* xo = x + (1 - c) * hp;
@@ -380,7 +380,7 @@ __device__ void split_gs(const Team& tm, int n, int c, const float* b, float* x,
 }
 
 // red residual r_red = b_red - L x at the red points (black residuals are zero)
-__device__ void split_resid_red(const Team& tm, int n, const float* b, const float* x, float* r) {
+__device__ void split_resid_red_scalar(const Team& tm, int n, const float* b, const float* x, float* r) {
     const int lane = threadIdx.x & 31, h = n >> 1;
     const int hp = h * n * n;
     const float* x1 = x + hp;
@@ -428,7 +428,7 @@ __device__ __forceinline__ float split_restrict_value(int n, const float* r, int
 }
 
 // coarse b = 4 R27(r), coarse x = its first red half-sweep from 0 (both split layout)
-__device__ void split_restrict(const Team& tm, int n, const float* r, float* bc, float* xc) {
+__device__ void split_restrict_scalar(const Team& tm, int n, const float* r, float* bc, float* xc) {
     const int lane = threadIdx.x & 31, nc = n / 2, hc = nc >> 1;
     const int hpc = hc * nc * nc;
     grid_rows(tm, nc, [&](int I, int J) {
@@ -454,7 +454,7 @@ __device__ void split_restrict(const Team& tm, int n, const float* r, float* bc,
 }
 
 // fine black x += P(coarse x), trilinear (both split layout)
-__device__ void split_prolong_black(const Team& tm, int n, const float* xc, float* x) {
+__device__ void split_prolong_black_scalar(const Team& tm, int n, const float* xc, float* x) {
     const int lane = threadIdx.x & 31, h = n >> 1, nc = n / 2, hc = nc >> 1;
     const int hp = h * n * n, hpc = hc * nc * nc;
     float* x1 = x + hp;
@@ -496,6 +496,206 @@ __device__ void split_prolong_black(const Team& tm, int n, const float* xc, floa
             }
         }
     });
+}
+
+// ---- vectorised split-layout passes (rows of h = 32 V floats, V = 2 or 4) ----
+//
+// A warp reads a whole row of one colour with one V-wide access per lane (lane l holds
+// kk = V l .. V l + V - 1), so each lane keeps several independent 8- or 16-byte loads in
+// flight; the scalar versions, one 4-byte value per access, reach only about a third of
+// the HBM bandwidth. The in-row neighbour at either end of a lane's V values comes from
+// the adjacent lane by a shuffle, wrapping from lane 0 to lane 31 as the periodic row
+// does. Every sum keeps the scalar versions' order, so results are identical.
+
+template <int V>
+__device__ __forceinline__ void ldv(const float* p, float (&v)[V]) {
+    if constexpr (V == 4) {
+        const float4 t = *reinterpret_cast<const float4*>(p);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else {
+        const float2 t = *reinterpret_cast<const float2*>(p);
+        v[0] = t.x; v[1] = t.y;
+    }
+}
+template <int V>
+__device__ __forceinline__ void stv(float* p, const float (&v)[V]) {
+    if constexpr (V == 4)
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    else
+        *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+}
+
+// sum of the six other-colour neighbours of the lane's V points in row o (s as in
+// split_nb_sums), from full-row vector loads
+template <int V>
+__device__ __forceinline__ void vec_nb_sums(const float* xo, const Rows& o, int s, float (&sum)[V]) {
+    const int lane = threadIdx.x & 31;
+    float a0[V], a1[V], a2[V], a3[V], cen[V];
+    ldv<V>(xo + o.im + V * lane, a0);
+    ldv<V>(xo + o.ip + V * lane, a1);
+    ldv<V>(xo + o.jm + V * lane, a2);
+    ldv<V>(xo + o.jp + V * lane, a3);
+    ldv<V>(xo + o.c + V * lane, cen);
+    const float prev = __shfl_sync(0xffffffffu, cen[V - 1], (lane + 31) & 31);
+    const float next = __shfl_sync(0xffffffffu, cen[0], (lane + 1) & 31);
+#pragma unroll
+    for (int e = 0; e < V; e++) {
+        const float side = s == 0 ? (e == 0 ? prev : cen[e - 1]) : (e == V - 1 ? next : cen[e + 1]);
+        float t = ((a0[e] + a1[e]) + a2[e]) + a3[e];
+        sum[e] = (t + cen[e]) + side;
+    }
+}
+
+template <int V>
+__device__ void split_gs_vec(const Team& tm, int n, int c, const float* b, float* x, double* acc) {
+    const int lane = threadIdx.x & 31, h = n >> 1;
+    const int hp = h * n * n;
+    const float* xo = x + (1 - c) * hp;
+    float* xc = x + c * hp;
+    const float* bc = b + c * hp;
+    double s_acc = 0.0;
+    grid_rows(tm, n, [&](int i, int j) {
+        const Rows o = rows_of(n, i, j);
+        float bv[V], sum[V], v[V];
+        ldv<V>(bc + o.c + V * lane, bv);
+        vec_nb_sums<V>(xo, o, (i + j + c) & 1, sum);
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            v[e] = (bv[e] - sum[e]) * (-1.0f / 6.0f);
+            s_acc += (double)v[e];
+        }
+        stv<V>(xc + o.c + V * lane, v);
+    });
+    if (acc != nullptr) *acc += s_acc;
+}
+
+template <int V>
+__device__ void split_resid_red_vec(const Team& tm, int n, const float* b, const float* x, float* r) {
+    const int lane = threadIdx.x & 31, h = n >> 1;
+    const int hp = h * n * n;
+    const float* x1 = x + hp;
+    grid_rows(tm, n, [&](int i, int j) {
+        const Rows o = rows_of(n, i, j);
+        float bv[V], xv[V], sum[V], v[V];
+        ldv<V>(b + o.c + V * lane, bv);
+        ldv<V>(x + o.c + V * lane, xv);
+        vec_nb_sums<V>(x1, o, (i + j) & 1, sum);
+#pragma unroll
+        for (int e = 0; e < V; e++) v[e] = bv[e] - (sum[e] - 6.0f * xv[e]);
+        stv<V>(r + o.c + V * lane, v);
+    });
+}
+
+// restriction with coarse rows of nc = h = 32 V points: lane l computes K = V l .. V l + V - 1
+template <int V>
+__device__ void split_restrict_vec(const Team& tm, int n, const float* r, float* bc, float* xc) {
+    const int lane = threadIdx.x & 31, nc = n / 2, hc = nc >> 1, h = n >> 1;
+    const int hpc = hc * nc * nc;
+    grid_rows(tm, nc, [&](int I, int J) {
+        const int i = 2 * I, j = 2 * J;
+        const int ip = i + 1, im = i == 0 ? n - 1 : i - 1, jp = j + 1, jm = j == 0 ? n - 1 : j - 1;
+        auto R = [&](int fi, int fj) { return r + (fi * n + fj) * h + V * lane; };
+        float dpp[V], dpm[V], dmp[V], dmm[V], p0[V], m0[V], q0p[V], q0m[V], cc[V];
+        ldv<V>(R(ip, jp), dpp);
+        ldv<V>(R(ip, jm), dpm);
+        ldv<V>(R(im, jp), dmp);
+        ldv<V>(R(im, jm), dmm);
+        ldv<V>(R(ip, j), p0);
+        ldv<V>(R(im, j), m0);
+        ldv<V>(R(i, jp), q0p);
+        ldv<V>(R(i, jm), q0m);
+        ldv<V>(R(i, j), cc);
+        // values at K - 1: the previous element, or the previous lane's last one
+        const float p0m = __shfl_sync(0xffffffffu, p0[V - 1], (lane + 31) & 31);
+        const float m0m = __shfl_sync(0xffffffffu, m0[V - 1], (lane + 31) & 31);
+        const float q0pm = __shfl_sync(0xffffffffu, q0p[V - 1], (lane + 31) & 31);
+        const float q0mm = __shfl_sync(0xffffffffu, q0m[V - 1], (lane + 31) & 31);
+        float bv[V];
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            float ee = dpp[e] + dpm[e];
+            ee += dmp[e];
+            ee += dmm[e];
+            ee += p0[e];
+            ee += e == 0 ? p0m : p0[e - 1];
+            ee += m0[e];
+            ee += e == 0 ? m0m : m0[e - 1];
+            ee += q0p[e];
+            ee += e == 0 ? q0pm : q0p[e - 1];
+            ee += q0m[e];
+            ee += e == 0 ? q0mm : q0m[e - 1];
+            bv[e] = (8.0f * cc[e] + 2.0f * ee) * (4.0f / 64.0f);
+        }
+        // K = V lane + e has colour (I + J + e) & 1 and sits at K >> 1 of its half
+        const int rowc = (I * nc + J) * hc;
+        const int c0 = (I + J) & 1;
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            const int C = (c0 + e) & 1;
+            const int idx = C * hpc + rowc + ((V * lane + e) >> 1);
+            bc[idx] = bv[e];
+            xc[idx] = C == 0 ? bv[e] * (-1.0f / 6.0f) : 0.0f;
+        }
+    });
+}
+
+template <int V>
+__device__ void split_prolong_black_vec(const Team& tm, int n, const float* xc, float* x) {
+    const int lane = threadIdx.x & 31, h = n >> 1, nc = n / 2, hc = nc >> 1;
+    const int hp = h * n * n, hpc = hc * nc * nc;
+    float* x1 = x + hp;
+    grid_rows(tm, n, [&](int i, int j) {
+        const int s1 = (i + j + 1) & 1;
+        const int ci = i >> 1, cj = j >> 1;
+        const int ci1 = ci + 1 == nc ? 0 : ci + 1, cj1 = cj + 1 == nc ? 0 : cj + 1;
+        const bool oi = i & 1, oj = j & 1, ok = s1;
+        auto C = [&](int CI, int CJ, int CK) {
+            return ((CI + CJ + CK) & 1) * hpc + (CI * nc + CJ) * hc + (CK >> 1);
+        };
+        auto line = [&](int CI, int CJ, int ck, int ck1) {
+            const float a = xc[C(CI, CJ, ck)];
+            return ok ? 0.5f * (a + xc[C(CI, CJ, ck1)]) : a;
+        };
+        const int rowx = (i * n + j) * h + V * lane;
+        float old[V], v[V];
+        ldv<V>(x1 + rowx, old);
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            const int kk = V * lane + e;
+            const int ck = kk, ck1 = kk + 1 == nc ? 0 : kk + 1;
+            float p = line(ci, cj, ck, ck1);
+            if (oj) p = 0.5f * (p + line(ci, cj1, ck, ck1));
+            if (oi) {
+                float q = line(ci1, cj, ck, ck1);
+                if (oj) q = 0.5f * (q + line(ci1, cj1, ck, ck1));
+                p = 0.5f * (p + q);
+            }
+            v[e] = old[e] + p;
+        }
+        stv<V>(x1 + rowx, v);
+    });
+}
+
+// dispatch: rows of 128 floats (n = 256) as float4, of 64 (n = 128) as float2
+__device__ __forceinline__ void split_gs(const Team& tm, int n, int c, const float* b, float* x, double* acc) {
+    if (n == 256) split_gs_vec<4>(tm, n, c, b, x, acc);
+    else if (n == 128) split_gs_vec<2>(tm, n, c, b, x, acc);
+    else split_gs_scalar(tm, n, c, b, x, acc);
+}
+__device__ __forceinline__ void split_resid_red(const Team& tm, int n, const float* b, const float* x, float* r) {
+    if (n == 256) split_resid_red_vec<4>(tm, n, b, x, r);
+    else if (n == 128) split_resid_red_vec<2>(tm, n, b, x, r);
+    else split_resid_red_scalar(tm, n, b, x, r);
+}
+__device__ __forceinline__ void split_restrict(const Team& tm, int n, const float* r, float* bc, float* xc) {
+    if (n == 256) split_restrict_vec<4>(tm, n, r, bc, xc);
+    else if (n == 128) split_restrict_vec<2>(tm, n, r, bc, xc);
+    else split_restrict_scalar(tm, n, r, bc, xc);
+}
+__device__ __forceinline__ void split_prolong_black(const Team& tm, int n, const float* xc, float* x) {
+    if (n == 256) split_prolong_black_vec<4>(tm, n, xc, x);
+    else if (n == 128) split_prolong_black_vec<2>(tm, n, xc, x);
+    else split_prolong_black_scalar(tm, n, xc, x);
 }
 
 // ---- the shared-memory part of the V-cycle (CTA 0) ----
@@ -675,11 +875,113 @@ __device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs&
     return rmax;
 }
 
+// Vectorised residual pass for n % 64 == 0: a warp covers 64 consecutive k of a row with
+// one double2 per lane; k - 1 / k + 1 come from the adjacent lane by a shuffle, from memory
+// at the ends of the 64. Same sums, in the same order, as residual_pass.
+template <int START, bool RHS_Q>
+__device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedArgs& a, const double* X,
+                                                    const double* Xp, float* e, float* rb) {
+    const int n = a.n, h = n >> 1, lane = threadIdx.x & 31;
+    const int hp = h * n * n;
+    double rmax = 0.0;
+    auto x1 = [&](int q) { return START == START_EXTRAP ? 2 * X[q] - Xp[q] : X[q]; };
+    auto x2 = [&](int q) {
+        double2 v = *reinterpret_cast<const double2*>(X + q);
+        if (START == START_EXTRAP) {
+            const double2 p = *reinterpret_cast<const double2*>(Xp + q);
+            v.x = 2 * v.x - p.x;
+            v.y = 2 * v.y - p.y;
+        }
+        return v;
+    };
+    grid_rows(tm, n, [&](int i, int j) {
+        const int ip = i + 1 == n ? 0 : i + 1, im = i == 0 ? n - 1 : i - 1;
+        const int jp = j + 1 == n ? 0 : j + 1, jm = j == 0 ? n - 1 : j - 1;
+        // 32-bit offsets: the mixed solver takes n <= kMixedMaxN (n^3 < 2^31)
+        const int row = (i * n + j) * n;
+        const int rip = (ip * n + j) * n, rim = (im * n + j) * n;
+        const int rjp = (i * n + jp) * n, rjm = (i * n + jm) * n;
+        const int cA = (i + j) & 1;  // colour of even k in this row
+        const int srow = (i * n + j) * h;
+        for (int k0 = 0; k0 < n; k0 += 64) {
+            const int k = k0 + 2 * lane;
+            double r0, r1;
+            double2 bq;
+            if (RHS_Q) {
+                bq = *reinterpret_cast<const double2*>(a.q + row + k);
+                bq.x = bq.x * a.c;
+                bq.y = bq.y * a.c;
+            } else {
+                bq = *reinterpret_cast<const double2*>(a.tmp + row + k);
+            }
+            if (START == START_ZERO) {
+                r0 = bq.x;
+                r1 = bq.y;
+            } else {
+                const double2 xip = x2(rip + k), xim = x2(rim + k), xjp = x2(rjp + k), xjm = x2(rjm + k);
+                const double2 xc = x2(row + k);
+                double km0 = __shfl_sync(0xffffffffu, xc.y, (lane + 31) & 31);
+                double kp1 = __shfl_sync(0xffffffffu, xc.x, (lane + 1) & 31);
+                if (lane == 0) km0 = x1(row + (k0 == 0 ? n - 1 : k0 - 1));
+                if (lane == 31) kp1 = x1(row + (k0 + 64 == n ? 0 : k0 + 64));
+                double s0 = xip.x + xim.x;
+                s0 = s0 + xjp.x;
+                s0 = s0 + xjm.x;
+                s0 = s0 + xc.y;
+                s0 = s0 + km0;
+                double s1 = xip.y + xim.y;
+                s1 = s1 + xjp.y;
+                s1 = s1 + xjm.y;
+                s1 = s1 + kp1;
+                s1 = s1 + xc.x;
+                r0 = bq.x - (s0 - xc.x * 6.0);
+                r1 = bq.y - (s1 - xc.y * 6.0);
+            }
+            const float rf0 = (float)r0, rf1 = (float)r1;
+            const int p0 = cA * hp + srow + (k >> 1), p1 = (cA ^ 1) * hp + srow + (k >> 1);
+            rb[p0] = rf0;
+            rb[p1] = rf1;
+            e[p0] = cA == 0 ? rf0 * (-1.0f / 6.0f) : 0.0f;
+            e[p1] = cA == 1 ? rf1 * (-1.0f / 6.0f) : 0.0f;
+            rmax = fmax(rmax, fmax(fabs(r0), fabs(r1)));
+        }
+    });
+    return rmax;
+}
+
+template <int START, bool RHS_Q>
+__device__ __forceinline__ double residual_any(const Team& tm, const MixedArgs& a, const double* X,
+                                               const double* Xp, float* e, float* rb) {
+    if (a.n % 64 == 0) return residual_pass_vec<START, RHS_Q>(tm, a, X, Xp, e, rb);
+    return residual_pass<START, RHS_Q>(tm, a, X, Xp, e, rb);
+}
+
 // home = X + (e - emean) with X as residual_pass reads it (0, X[], 2 X[] - phi_prev[]).
 template <int START>
 __device__ __forceinline__ void update_pass(const Team& tm, const MixedArgs& a, const double* X, double* home,
                                             const float* e, double emean) {
     const int n = a.n;
+    if (n % 64 == 0) {  // double2 per lane, e from both colour halves
+        const int h = n >> 1, lane = threadIdx.x & 31, hp = h * n * n;
+        grid_rows(tm, n, [&](int i, int j) {
+            const int row = (i * n + j) * n, srow = (i * n + j) * h;
+            const int cA = (i + j) & 1;
+            for (int k0 = 0; k0 < n; k0 += 64) {
+                const int k = k0 + 2 * lane;
+                double2 xo = make_double2(0.0, 0.0);
+                if (START != START_ZERO) xo = *reinterpret_cast<const double2*>(X + row + k);
+                if (START == START_EXTRAP) {
+                    const double2 p = *reinterpret_cast<const double2*>(a.phi_prev + row + k);
+                    xo.x = 2 * xo.x - p.x;
+                    xo.y = 2 * xo.y - p.y;
+                }
+                const float e0 = e[cA * hp + srow + (k >> 1)], e1 = e[(cA ^ 1) * hp + srow + (k >> 1)];
+                *reinterpret_cast<double2*>(home + row + k) =
+                    make_double2(xo.x + ((double)e0 - emean), xo.y + ((double)e1 - emean));
+            }
+        });
+        return;
+    }
     grid_pts(tm, n, [&](int i, int j, int k) {
         const long c = ((long)i * n + j) * n + k;
         const double xo = START == START_ZERO ? 0.0 : (START == START_EXTRAP ? 2 * X[c] - a.phi_prev[c] : X[c]);
@@ -746,13 +1048,13 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
         const int st = outer == 0 ? start : START_X;
         double s0 = 0.0, rmax = 0.0;
         if (st == START_ZERO)
-            rmax = residual_pass<START_ZERO, true>(tm, a, Xs, a.phi_prev, e, rb);
+            rmax = residual_any<START_ZERO, true>(tm, a, Xs, a.phi_prev, e, rb);
         else if (st == START_EXTRAP)
-            rmax = residual_pass<START_EXTRAP, true>(tm, a, Xs, a.phi_prev, e, rb);
+            rmax = residual_any<START_EXTRAP, true>(tm, a, Xs, a.phi_prev, e, rb);
         else if (rhs_q)
-            rmax = residual_pass<START_X, true>(tm, a, Xs, a.phi_prev, e, rb);
+            rmax = residual_any<START_X, true>(tm, a, Xs, a.phi_prev, e, rb);
         else
-            rmax = residual_pass<START_X, false>(tm, a, Xs, a.phi_prev, e, rb);
+            rmax = residual_any<START_X, false>(tm, a, Xs, a.phi_prev, e, rb);
         ok = reduce_sum_max(s0, rmax, tm, epoch, seq);
         stamp_outer(a, outer, 1);
         if (a.stamps != nullptr && outer < 8 && tm.b == 0 && threadIdx.x == 0)
