@@ -18,7 +18,7 @@ def gamma_au(gamma_per_ps):
 class MDRun:
     def __init__(self, capi, system, method="LCG", precond="NONE", tol=1e-7, integrator="VERLET",
                  thermostat=False, T=1200.0, gamma_per_ps=1.0, dt_fs=1.0, eps_s=1.0, eps_int=1.0,
-                 rescale=False, precision=0, mixed_tol=0.0, cas="CIC", pot="TF"):
+                 rescale=False, precision=0, mixed_tol=0.0, cas="CIC", pot="TF", pb=None):
         self.capi = capi
         self.sys = system
         self.method = method.upper()
@@ -38,6 +38,8 @@ class MDRun:
         # 1 FP32 multigrid + FP64 refinement to mixed_tol (or tol when 0)
         self.precision = precision
         self.mixed_tol = mixed_tol
+        # Poisson-Boltzmann implicit solvent (systems.PBSettings) or None
+        self.pb = pb
         self.n_iters = None
         self.potential_notelec = None
 
@@ -49,11 +51,15 @@ class MDRun:
         maps = c.type_maps()
         c.solver_initialize_grid(s.n_grid, s.L, s.h, self.tol, self.eps_s, self.eps_int,
                                  maps["method"][self.method], maps["precond"][self.precond])
+        if self.pb is not None:  # solver.py:145-163
+            c.solver_initialize_grid_pois_boltz(self.pb.w, self.pb.kbar2, int(self.pb.nonpolar))
         if self.precision:
             c.mzb_set_precision(int(self.precision), float(self.mixed_tol))
         c.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, maps["potential"][self.pot],
                                       maps["cas"][self.cas], s.types, s.pos, s.vel, s.mass, s.charges,
                                       s.pot_params)
+        if self.pb is not None:  # solver.py:346-356
+            c.solver_initialize_particles_pois_boltz(self.pb.gamma_np, self.pb.beta_np, self.pb.radii)
         c.solver_initialize_integrator(s.n_ions, self.dt, self.T, self.gamma,
                                        maps["integrator"][self.integrator], 1 if self.thermostat else 0)
         # step 0
@@ -72,11 +78,15 @@ class MDRun:
     def update_charges(self):
         if self.capi.solver_update_charges() != 0:
             raise RuntimeError("charge is not preserved")
+        if self.pb is not None:  # solver.py:411-415, called after every charge update
+            self.capi.solver_update_eps_k2()
 
     def compute_forces(self):
         c = self.capi
         c.solver_compute_forces_elec()
         self.potential_notelec = c.solver_compute_forces_noel()
+        if self.pb is not None:
+            self.energy_nonpolar = c.solver_compute_forces_pb()
         c.solver_compute_forces_tot()
 
     # -- solver.py:483-492 --------------------------------------------------------------
@@ -98,7 +108,10 @@ class MDRun:
         c = self.capi
         n = self.sys.n_ions
         out = {}
-        for name in ("pos", "vel", "fcs_elec", "fcs_noel", "fcs_tot"):
+        names = ("pos", "vel", "fcs_elec", "fcs_noel", "fcs_tot")
+        if self.pb is not None:
+            names += ("fcs_db", "fcs_ib", "fcs_np")
+        for name in names:
             a = np.empty((n, 3), dtype=np.float64)
             getattr(c, "get_" + name)(a)
             out[name] = a

@@ -167,6 +167,68 @@ def pair_system(ncell, n_grid, pot="TF", density=1.379, T=1200.0, seed=0):
     return make_system(ncell, n_grid, density=density, T=T, seed=seed)
 
 
+# Poisson-Boltzmann implicit solvent (maze_poisson/solver.py:145-163, 346-356). The
+# reference passes each ion's solvation radius (its species radius plus the probe radius,
+# in bohr), the shell half-width w and the screening term kbar^2 h^2 to the library.
+ION_RADII_ANG = (1.02, 1.81)     # Na+, Cl- ionic radii [A]
+PROBE_RADIUS_ANG = 1.4           # maze_poisson/myio/input/base_file_input.py:129
+EC_SI, EPS0_SI, KB_SI, BOHR_M = 1.602176634e-19, 8.854187817e-12, 1.380649e-23, 5.29177210903e-11
+
+
+@dataclasses.dataclass
+class PBSettings:
+    """Arguments of solver_initialize_grid_pois_boltz / _particles_pois_boltz."""
+    w: float                 # shell half-width [bohr]
+    kbar2: float             # kbar^2 h^2
+    nonpolar: int            # 1: non-polar forces on
+    gamma_np: float          # a.u.
+    beta_np: float
+    radii: np.ndarray        # float64 [N] solvation radii [bohr]
+
+
+def pb_kbar2(ionic_strength, T, eps_s, h):
+    """kbar^2 h^2 of the linearised screening term, formed as solver.py:149-153 does
+    (ionic strength in mol/L, h in bohr)."""
+    return ((8 * np.pi * N_AVOGADRO * EC_SI ** 2 * ionic_strength * 1e3)
+            / (eps_s * EPS0_SI * KB_SI * T) * BOHR_M ** 2 * h ** 2)
+
+
+def pb_settings(system, eps_s=78.4, ionic_strength=0.15, w=1.0, nonpolar=1, gamma_np=0.005,
+                beta_np=0.0):
+    """PB arguments for `system`: solvation radius = ionic radius + probe (as solver.py:349-352
+    forms it), gamma_np in kcal/mol/A^2 converted as base_file_input.py:145-147 does."""
+    radii = (np.array([ION_RADII_ANG[t] for t in system.types]) + PROBE_RADIUS_ANG) / A0
+    return PBSettings(w=w, kbar2=pb_kbar2(ionic_strength, system.T, eps_s, system.h),
+                      nonpolar=nonpolar, gamma_np=gamma_np * 0.0065934, beta_np=beta_np,
+                      radii=np.ascontiguousarray(radii, dtype=np.float64))
+
+
+def make_pb_system(n_ions, n_grid, box_ang, T=300.0, seed=0, cluster_ang=None, min_sep_ang=2.7):
+    """A solute of n_ions alternating Na+/Cl- ions at random positions inside a sphere of
+    radius cluster_ang (default a quarter of the box) around the box centre, at least
+    min_sep_ang apart, in implicit solvent; MB velocities at T, Tosi-Fumi pairs."""
+    rng = np.random.default_rng(seed)
+    L = box_ang / A0
+    R = (cluster_ang if cluster_ang is not None else box_ang / 4) / A0
+    sep = min_sep_ang / A0
+    pos = []
+    while len(pos) < n_ions:
+        p = rng.uniform(-R, R, size=3)
+        if np.linalg.norm(p) > R:
+            continue
+        if all(np.linalg.norm(p - q) >= sep for q in pos):
+            pos.append(p)
+    pos = np.mod(np.array(pos) + L / 2, L)
+    types = np.array([k % 2 for k in range(n_ions)], dtype=np.int32)
+    charges = np.array([SPECIES[t][1] for t in types], dtype=np.float64)
+    mass = np.array([SPECIES[t][2] for t in types], dtype=np.float64) * CONV_MASS
+    vel = rng.normal(0.0, 1.0, size=(n_ions, 3)) * np.sqrt(KB * T / mass)[:, None]
+    return MoltenSalt(ncell=0, n_grid=n_grid, density=0.0, T=T, seed=seed, L=L, h=L / n_grid,
+                      types=types, pos=np.ascontiguousarray(pos), vel=np.ascontiguousarray(vel),
+                      mass=np.ascontiguousarray(mass), charges=np.ascontiguousarray(charges),
+                      pot_params=tf_params_au())
+
+
 # Workloads of the reference's configurations (sizes only; solver settings in md.py)
 WORKLOADS = {
     "nacl250_64": dict(ncell=5, n_grid=64, density=1.379),

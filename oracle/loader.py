@@ -55,6 +55,18 @@ KERNELS = {
     "orc_tf_table": (None, [_f, _c.c_int, _c.c_double, _f]),
     "orc_cell_list": (None, [_f, _c.c_int, _c.c_double, _c.c_int, _i32, _i32]),
     "orc_set_noise": (None, [_f, _c.c_int64]),
+    "orc_update_eps_k2": (None, [_f, _f, _c.c_int, _c.c_int, _c.c_double, _c.c_double, _c.c_double,
+                                 _c.c_double, _c.c_double, _f, _f, _f, _f]),
+    "orc_laplace_pb": (None, [_f, _f, _f, _f, _f, _f, _c.c_int]),
+    "orc_conj_grad_pb": (_c.c_int, [_f, _f, _f, _c.c_double, _c.c_int, _f, _f, _f, _f]),
+    "orc_smooth_pb": (None, [_f, _f, _c.c_int, _c.c_int, _f, _f, _f, _f]),
+    "orc_restrict_eps": (None, [_f, _f, _c.c_int, _c.c_int]),
+    "orc_restrict_k2": (None, [_f, _f, _c.c_int]),
+    "orc_cg_coarse_pb": (_c.c_int, [_f, _f, _c.c_int, _c.c_int, _c.c_double, _f, _f, _f, _f]),
+    "orc_mg_pb_apply": (None, [_f, _f, _c.c_int, _c.c_int, _f, _f, _f, _f]),
+    "orc_forces_pb": (None, [_f, _f, _c.c_int, _c.c_int, _c.c_double, _c.c_double, _c.c_double,
+                             _c.c_double, _c.c_double, _c.c_int, _f, _f, _f, _f, _f, _f, _f, _f]),
+    "orc_get_pb_grids": (None, [_f, _f, _f, _f]),
 }
 
 

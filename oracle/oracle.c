@@ -272,6 +272,331 @@ static int conj_grad_precond(const double *b, const double *x0, double *x, doubl
 }
 
 /* ------------------------------------------------------------------------------------
+ * Poisson-Boltzmann variant: face dielectric arrays eps_x/y/z (eps_x[c] sits on the
+ * face between point c and its +x neighbour), cell screening k2, the variable-
+ * coefficient operator and its solvers, and the boundary forces.
+ * ---------------------------------------------------------------------------------- */
+
+/* Smooth switch across the transition shell, a in [0, 2w] (grid_general.c:213-216). */
+static double pb_switch(double a, double w2, double w3) {
+    return -(1 / (4 * w3)) * pow(a, 3) + (3 / (4 * w2)) * pow(a, 2);
+}
+/* d(switch)/da / switch (particles.c:407-418). */
+static double pb_h_ratio(double rad, double w2, double w3) {
+    return (-(3 / (4 * w3)) * pow(rad, 2) + (3 / (2 * w2)) * rad) /
+           (-(1 / (4 * w3)) * pow(rad, 3) + (3 / (4 * w2)) * pow(rad, 2));
+}
+/* One coefficient at squared distance r2 from an ion: untouched outside r_s + w, scaled
+   by the switch inside the shell, zero inside r_s - w (grid_general.c:207-222). */
+static void pb_scale(double *v, double r2, double rp2, double rm2, double rs, double w, double w2,
+                     double w3) {
+    if (r2 >= rp2) return;
+    if (r2 > rm2) *v *= pb_switch(sqrt(r2) - rs + w, w2, w3);
+    else *v = 0.0;
+}
+
+/* grid_update_eps_and_k2 (grid_general.c:138-301): eps = eps_s - eps_int and k2 = kbar2,
+   scaled ion by ion (in ion order) over each ion's box of +-(floor((r_s+w)/h)+1) points,
+   then eps += eps_int. */
+void orc_update_eps_k2(const double *pos, const double *radii, int np, int n, double h, double w,
+                       double eps_s, double eps_int, double kbar2, double *eps_x, double *eps_y,
+                       double *eps_z, double *k2) {
+    long m = (long)n * n * n, n2 = (long)n * n;
+    double w2 = w * w, w3 = w2 * w, hd2 = h / 2.0;
+    for (long t = 0; t < m; t++) {
+        eps_x[t] = (eps_s - eps_int); eps_y[t] = (eps_s - eps_int); eps_z[t] = (eps_s - eps_int);
+        k2[t] = kbar2;
+    }
+    for (int p = 0; p < np; p++) {
+        double rs = radii[p], px = pos[3 * p], py = pos[3 * p + 1], pz = pos[3 * p + 2];
+        double rp2 = pow(rs + w, 2), rm2 = pow(rs - w, 2);
+        int range = (int)floor((rs + w) / h) + 1;
+        int ix = (int)floor(px / h), iy = (int)floor(py / h), iz = (int)floor(pz / h);
+        if (range >= n) { fprintf(stderr, "oracle: PB ion box wider than the grid\n"); exit(1); }
+        for (int di = -range; di <= range; di++) {
+            int i0 = ix + di;
+            double dx = px - i0 * h, dx2 = dx * dx;
+            i0 = (i0 + n) % n;
+            if (i0 < 0 || i0 >= n) continue;
+            long ib = (long)i0 * n2;
+            for (int dj = -range; dj <= range; dj++) {
+                int j0 = iy + dj;
+                double dy = py - j0 * h, dy2 = dy * dy;
+                long jb = (long)((j0 + n) % n) * n;
+                for (int dk = -range; dk <= range; dk++) {
+                    int k0 = iz + dk;
+                    double dz = pz - k0 * h, dz2 = dz * dz;
+                    long c = ib + jb + (k0 + n) % n;
+                    pb_scale(&k2[c], dx2 + dy2 + dz2, rp2, rm2, rs, w, w2, w3);
+                    double a = dx - hd2;
+                    pb_scale(&eps_x[c], a * a + dy2 + dz2, rp2, rm2, rs, w, w2, w3);
+                    a = dy - hd2;
+                    pb_scale(&eps_y[c], dx2 + a * a + dz2, rp2, rm2, rs, w, w2, w3);
+                    a = dz - hd2;
+                    pb_scale(&eps_z[c], dx2 + dy2 + a * a, rp2, rm2, rs, w, w2, w3);
+                }
+            }
+        }
+    }
+    for (long t = 0; t < m; t++) { eps_x[t] += eps_int; eps_y[t] += eps_int; eps_z[t] += eps_int; }
+}
+
+/* Variable-coefficient operator (laplace.c:77-145): faces x+, x-, y+, y-, z+, z- times
+   their neighbours, minus centre times (sum of the six faces + k2). */
+void orc_laplace_pb(const double *u, double *out, const double *ex, const double *ey,
+                    const double *ez, const double *k2, int n) {
+    for (long i = 0; i < n; i++)
+        for (long j = 0; j < n; j++)
+            for (long k = 0; k < n; k++) {
+                long c = (i * n + j) * n + k;
+                long xm = gidx(i - 1, j, k, n), ym = gidx(i, j - 1, k, n), zm = gidx(i, j, k - 1, n);
+                double s = u[gidx(i + 1, j, k, n)] * ex[c] + u[xm] * ex[xm];
+                s = s + u[gidx(i, j + 1, k, n)] * ey[c];
+                s = s + u[ym] * ey[ym];
+                s = s + u[gidx(i, j, k + 1, n)] * ez[c];
+                s = s + u[zm] * ez[zm];
+                double d = ex[c] + ex[xm];
+                d = d + ey[c]; d = d + ey[ym]; d = d + ez[c]; d = d + ez[zm]; d = d + k2[c];
+                out[c] = s - u[c] * d;
+            }
+}
+
+/* conj_grad_pb (plcg.c:169-238): conj_grad with the PB operator, still the implicit
+   1/6 Jacobi scaling. */
+int orc_conj_grad_pb(const double *b, const double *x0, double *x, double tol, int n,
+                     const double *ex, const double *ey, const double *ez, const double *k2) {
+    long m = (long)n * n * n, limit = (long)n * n, iter = 0;
+    int res = -1;
+    double *r = malloc(m * sizeof(double)), *p = malloc(m * sizeof(double));
+    double *Ap = malloc(m * sizeof(double));
+    orc_laplace_pb(x0, r, ex, ey, ez, k2, n);
+    axpy(r, b, -1.0, m);
+    if (x != x0) memcpy(x, x0, m * sizeof(double));
+    for (long t = 0; t < m; t++) p[t] = r[t] * (1.0 / 6.0);
+    double rv = -dot(r, p, m);
+    while (iter < limit) {
+        orc_laplace_pb(p, Ap, ex, ey, ez, k2, n);
+        double alpha = rv / dot(p, Ap, m);
+        axpy(x, p, alpha, m);
+        axpy(r, Ap, alpha, m);
+        double rr = dot(r, r, m);
+        if (amax(r, m) <= tol) { res = (int)iter; break; }
+        double rnv = -rr / 6.0, beta = rnv / rv;
+        rv = rnv;
+        scal(p, beta, m);
+        axpy(p, r, 1.0 / 6.0, m);
+        iter++;
+    }
+    free(r); free(p); free(Ap);
+    return res;
+}
+
+/* smooth_pb_rbgs (multigrid_pb.c:544-640): red ((i+j+k) even) then black; x = (sum of
+   face * neighbour - rhs) / max(diag, 1e-14). */
+void orc_smooth_pb(const double *rhs, double *x, int n, int iters, const double *ex,
+                   const double *ey, const double *ez, const double *k2) {
+    for (int it = 0; it < iters; it++)
+        for (int colour = 0; colour < 2; colour++)
+            for (long i = 0; i < n; i++)
+                for (long j = 0; j < n; j++)
+                    for (long k = (i + j + colour) & 1; k < n; k += 2) {
+                        long c = (i * n + j) * n + k;
+                        long xm = gidx(i - 1, j, k, n), ym = gidx(i, j - 1, k, n), zm = gidx(i, j, k - 1, n);
+                        double d = ex[c] + ex[xm];
+                        d = d + ey[c]; d = d + ey[ym]; d = d + ez[c]; d = d + ez[zm]; d = d + k2[c];
+                        if (d < 1e-14) d = 1e-14;
+                        double s = ex[c] * x[gidx(i + 1, j, k, n)] + ex[xm] * x[xm];
+                        s = s + ey[c] * x[gidx(i, j + 1, k, n)];
+                        s = s + ey[ym] * x[ym];
+                        s = s + ez[c] * x[gidx(i, j, k + 1, n)];
+                        s = s + ez[zm] * x[zm];
+                        s = s - rhs[c];
+                        x[c] = s / d;
+                    }
+}
+
+/* restriction_eps (multigrid_pb.c:330-447): the coarse +axis face is the mean of the 2x2
+   fine faces of that axis around it; axis 0 = x, 1 = y, 2 = z. */
+void orc_restrict_eps(const double *in, double *out, int n, int axis) {
+    int nc = n / 2;
+    for (long I = 0; I < nc; I++)
+        for (long J = 0; J < nc; J++)
+            for (long K = 0; K < nc; K++) {
+                long i = 2 * I, j = 2 * J, k = 2 * K;
+                double s;
+                if (axis == 0)
+                    s = in[gidx(i, j, k, n)] + in[gidx(i, j, k + 1, n)] + in[gidx(i, j + 1, k, n)] +
+                        in[gidx(i, j + 1, k + 1, n)];
+                else if (axis == 1)
+                    s = in[gidx(i, j, k, n)] + in[gidx(i, j, k + 1, n)] + in[gidx(i + 1, j, k, n)] +
+                        in[gidx(i + 1, j, k + 1, n)];
+                else
+                    s = in[gidx(i, j, k, n)] + in[gidx(i + 1, j, k, n)] + in[gidx(i, j + 1, k, n)] +
+                        in[gidx(i + 1, j + 1, k, n)];
+                out[(I * nc + J) * nc + K] = s * 0.25;
+            }
+}
+
+/* restriction_k2screen (multigrid_pb.c:459-527) on one process (n_start = 0): coarse
+   (I,J,K) is the mean of the fine cube at i in {2I+1, 2I+2}, j in {2J, 2J+1},
+   k in {2K, 2K+1}. */
+void orc_restrict_k2(const double *in, double *out, int n) {
+    int nc = n / 2;
+    for (long I = 0; I < nc; I++)
+        for (long J = 0; J < nc; J++)
+            for (long K = 0; K < nc; K++) {
+                long i = 2 * I + 1, j = 2 * J, k = 2 * K;
+                double s = in[gidx(i, j, k, n)] + in[gidx(i, j, k + 1, n)] + in[gidx(i, j + 1, k, n)] +
+                           in[gidx(i, j + 1, k + 1, n)] + in[gidx(i + 1, j, k, n)] +
+                           in[gidx(i + 1, j, k + 1, n)] + in[gidx(i + 1, j + 1, k, n)] +
+                           in[gidx(i + 1, j + 1, k + 1, n)];
+                out[(I * nc + J) * nc + K] = (1.0 / 8.0) * s;
+            }
+}
+
+/* cg_coarse_pb (multigrid_pb.c:16-97): unpreconditioned CG, relative inf-norm stop. */
+int orc_cg_coarse_pb(const double *b, double *x, int n, int maxit, double rtol, const double *ex,
+                     const double *ey, const double *ez, const double *k2) {
+    long m = (long)n * n * n;
+    double *r = malloc(m * sizeof(double)), *p = malloc(m * sizeof(double));
+    double *Ap = malloc(m * sizeof(double));
+    int k;
+    orc_laplace_pb(x, r, ex, ey, ez, k2, n);
+    axpy(r, b, -1.0, m);
+    for (long t = 0; t < m; t++) p[t] = r[t] * -1.0;
+    double r0 = amax(r, m);
+    if (r0 == 0.0) { free(r); free(p); free(Ap); return 0; }
+    double rr = dot(r, r, m);
+    for (k = 0; k < maxit; ++k) {
+        orc_laplace_pb(p, Ap, ex, ey, ez, k2, n);
+        double den = dot(p, Ap, m);
+        if (fabs(den) < 1e-300) break;
+        double alpha = rr / den;
+        axpy(x, p, alpha, m);
+        axpy(r, Ap, alpha, m);
+        if (amax(r, m) <= rtol * r0) { ++k; break; }
+        double rn = dot(r, r, m), beta = rn / rr;
+        rr = rn;
+        scal(p, beta, m);
+        axpy(p, r, -1.0, m);
+    }
+    free(r); free(p); free(Ap);
+    return k;
+}
+
+/* v_cycle_pb at depth 0 (multigrid_pb.c:270-328): sm PB-RBGS iterations, residual,
+   27-pt restriction, face / cell restrictions of eps and k2, coarse PB CG (50 it, rtol
+   1e-5) from zero, trilinear prolongation, correction, sm iterations. n/2 >= 16. */
+void orc_mg_pb_apply(const double *rhs, double *x, int n, int sm, const double *ex,
+                     const double *ey, const double *ez, const double *k2) {
+    long m = (long)n * n * n;
+    int nc = n / 2;
+    long mc = (long)nc * nc * nc;
+    if (nc < 16) { fprintf(stderr, "oracle multigrid: requires n/2 >= 16\n"); exit(1); }
+    double *r = malloc(m * sizeof(double));
+    double *rc = malloc(mc * sizeof(double)), *ec = calloc(mc, sizeof(double));
+    double *cx = malloc(mc * sizeof(double)), *cy = malloc(mc * sizeof(double));
+    double *cz = malloc(mc * sizeof(double)), *ck = malloc(mc * sizeof(double));
+    orc_smooth_pb(rhs, x, n, sm, ex, ey, ez, k2);
+    orc_laplace_pb(x, r, ex, ey, ez, k2, n);
+    scal(r, -1.0, m);
+    axpy(r, rhs, 1.0, m);
+    orc_restrict27(r, rc, n);
+    orc_restrict_eps(ex, cx, n, 0);
+    orc_restrict_eps(ey, cy, n, 1);
+    orc_restrict_eps(ez, cz, n, 2);
+    orc_restrict_k2(k2, ck, n);
+    orc_cg_coarse_pb(rc, ec, nc, 50, 1e-5, cx, cy, cz, ck);
+    orc_prolong_trilinear(ec, r, nc);
+    axpy(x, r, 1.0, m);
+    orc_smooth_pb(rhs, x, n, sm, ex, ey, ez, k2);
+    free(r); free(rc); free(ec); free(cx); free(cy); free(cz); free(ck);
+}
+
+/* particles_compute_forces_pb (particles.c:420-775): over each ion's box of
+   +-(floor((r_s+w)/h)+2) points, in the shell r_s - w < r < r_s + w around the point
+   (ionic boundary, k2 phi^2) and around each of its six faces (dielectric boundary,
+   (eps_face - eps_int) * dphi * phi, and non-polar, eps gradient direction), summed
+   ion by ion in loop order; then scaled by h/(8 pi), h/(8 pi) and
+   -gamma_np h / (eps_s - eps_int). */
+void orc_forces_pb(const double *pos, const double *radii, int np, int n, double h, double w,
+                   double eps_s, double eps_int, double gamma_np, int nonpolar, const double *phi,
+                   const double *ex, const double *ey, const double *ez, const double *k2,
+                   double *fdb, double *fib, double *fnp) {
+    double w2 = w * w, w3 = w2 * w, hd2 = h / 2.0;
+    long v = 3L * np;
+    memset(fdb, 0, v * sizeof(double)); memset(fib, 0, v * sizeof(double));
+    memset(fnp, 0, v * sizeof(double));
+    for (int p = 0; p < np; p++) {
+        double *db = fdb + 3 * p, *ib = fib + 3 * p, *nq = fnp + 3 * p;
+        double rs = radii[p], px = pos[3 * p], py = pos[3 * p + 1], pz = pos[3 * p + 2];
+        double rp2 = pow(rs + w, 2), rm2 = pow(rs - w, 2);
+        int range = (int)floor((rs + w) / h) + 2;
+        int ix = (int)floor(px / h), iy = (int)floor(py / h), iz = (int)floor(pz / h);
+        if (range >= n) { fprintf(stderr, "oracle: PB ion box wider than the grid\n"); exit(1); }
+        for (int di = -range; di <= range; di++) {
+            int i = ix + di;
+            double dx = px - i * h, dx2 = dx * dx;
+            i = (i + n) % n;
+            for (int dj = -range; dj <= range; dj++) {
+                int j = iy + dj;
+                double dy = py - j * h, dy2 = dy * dy;
+                j = (j + n) % n;
+                for (int dk = -range; dk <= range; dk++) {
+                    int k = iz + dk;
+                    double dz = pz - k * h, dz2 = dz * dz;
+                    k = (k + n) % n;
+                    long c = gidx(i, j, k, n);
+                    long fx = gidx(i + 1, j, k, n), fy = gidx(i, j + 1, k, n), fz = gidx(i, j, k + 1, n);
+                    long bx = gidx(i - 1, j, k, n), by = gidx(i, j - 1, k, n), bz = gidx(i, j, k - 1, n);
+                    double exc = ex[c], eyc = ey[c], ezc = ez[c];
+                    double exb = ex[bx], eyb = ey[by], ezb = ez[bz];
+                    double ddx = exc - exb, ddy = eyc - eyb, ddz = ezc - ezb;
+                    double dn = sqrt(ddx * ddx + ddy * ddy + ddz * ddz) / h;
+                    double ig = (dn > 0.0) ? 1.0 / dn : 0.0;
+                    double pc = phi[c];
+                    double r2 = dx2 + dy2 + dz2, r1, rx, ry, rz, hr, a, g, dphi;
+                    if (r2 < rp2 && r2 > rm2) {                      /* centre: ionic boundary */
+                        r1 = sqrt(r2) + 1E-12;
+                        rx = dx / r1; ry = dy / r1; rz = dz / r1;
+                        hr = pb_h_ratio(r1 - rs + w, w2, w3);
+                        a = k2[c] * pc * pc * hr;
+                        ib[0] += a * rx; ib[1] += a * ry; ib[2] += a * rz;
+                    }
+                    /* six faces: (offset along the axis, sign of the non-polar term,
+                       face coefficient, neighbour, gradient component) */
+                    for (int f = 0; f < 6; f++) {
+                        int axis = f / 2, fwd = f & 1;
+                        double o = fwd ? -hd2 : hd2;
+                        double ux = dx, uy = dy, uz = dz;
+                        if (axis == 0) { ux = dx + o; r2 = ux * ux + dy2 + dz2; g = ig * ddx; }
+                        else if (axis == 1) { uy = dy + o; r2 = dx2 + uy * uy + dz2; g = ig * ddy; }
+                        else { uz = dz + o; r2 = dx2 + dy2 + uz * uz; g = ig * ddz; }
+                        if (!(r2 < rp2 && r2 > rm2)) continue;
+                        r1 = sqrt(r2) + 1E-12;
+                        rx = ux / r1; ry = uy / r1; rz = uz / r1;
+                        hr = pb_h_ratio(r1 - rs + w, w2, w3);
+                        double ef = axis == 0 ? (fwd ? exc : exb) : axis == 1 ? (fwd ? eyc : eyb) : (fwd ? ezc : ezb);
+                        long nb = axis == 0 ? (fwd ? fx : bx) : axis == 1 ? (fwd ? fy : by) : (fwd ? fz : bz);
+                        a = (ef - eps_int) * hr;
+                        dphi = phi[nb] - pc;
+                        db[0] -= a * dphi * pc * rx; db[1] -= a * dphi * pc * ry; db[2] -= a * dphi * pc * rz;
+                        if (nonpolar) {
+                            if (fwd) { nq[0] += a * g * rx; nq[1] += a * g * ry; nq[2] += a * g * rz; }
+                            else { nq[0] -= a * g * rx; nq[1] -= a * g * ry; nq[2] -= a * g * rz; }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    double cdb = h / (8.0 * PI_D), cnp = -gamma_np * h / (eps_s - eps_int);
+    scal(fdb, cdb, v);
+    scal(fib, cdb, v);
+    scal(fnp, cnp, v);
+}
+
+/* ------------------------------------------------------------------------------------
  * Particle kernels
  * ---------------------------------------------------------------------------------- */
 
@@ -627,9 +952,12 @@ enum { P_NONE = 0, P_JACOBI = 1, P_MG = 2 };
 
 static struct {
     int type, precond, n;
-    double L, h, tol, eps_s;
+    double L, h, tol, eps_s, eps_int;
     long m;
     double *q, *phi, *phi_prev, *y;
+    int pb, nonpolar;                    /* grid_general.c:84-100 */
+    double w, kbar2;
+    double *ex, *ey, *ez, *k2;
 } G;
 static struct {
     int np, ntyp, n;
@@ -638,6 +966,9 @@ static struct {
     double *pos, *vel, *fe, *fn, *ft, *mass, *chg, *tab;
     int64_t *nbr;
     int cas, nnb, pot;
+    int pb;                              /* particles.c:111-127 */
+    double gamma_np, beta_np;
+    double *radii, *fdb, *fib, *fnp;
 } P;
 static struct {
     int type, enabled;
@@ -653,13 +984,13 @@ void solver_initialize(void) {}
 
 void solver_initialize_grid(int n, double L, double h, double tol, double eps_s, double eps_int,
                             int grid_type, int precond_type) {
-    (void)eps_int;
     if (grid_type == G_FFT) die("FFT is restated in numpy (oracle/fft_oracle.py)");
     if (grid_type < 0 || grid_type > 4) die("bad grid type");
     if (precond_type > P_MG) die("SSOR / BLOCKJACOBI are outside the oracle");
     G.type = grid_type; G.precond = precond_type; G.n = n;
-    G.L = L; G.h = h; G.tol = tol; G.eps_s = eps_s;
+    G.L = L; G.h = h; G.tol = tol; G.eps_s = eps_s; G.eps_int = eps_int;
     G.m = (long)n * n * n;
+    G.pb = 0; G.nonpolar = 0;
     G.q = calloc(G.m, sizeof(double)); G.phi = calloc(G.m, sizeof(double));
     G.phi_prev = calloc(G.m, sizeof(double)); G.y = calloc(G.m, sizeof(double));
 }
@@ -682,6 +1013,7 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
     P.nbr = malloc((size_t)n_p * P.nnb * 3 * sizeof(int64_t));
     P.tab = malloc((size_t)n_typ * n_typ * 7 * sizeof(double));
     P.pot = pot_type;
+    P.pb = 0;
     if (pot_type == 0) orc_tf_table(pot_params, n_typ, L, P.tab);
     else if (pot_type == 1) orc_lj_table(pot_params, n_typ, L, P.tab);
     else orc_sc_table(pot_params, n_typ, L, P.tab);
@@ -712,7 +1044,14 @@ int solver_update_charges(void) {
     return 0;
 }
 
-static double rhs_const(void) { double c = -4 * PI_D / G.h; return c / G.eps_s; }
+/* -4 pi / h, divided by eps_s unless PB carries the dielectric in the operator
+   (grid_lcg.c:100-110) */
+static double rhs_const(void) {
+    double c = -4 * PI_D / G.h;
+    if (!G.pb) c /= G.eps_s;
+    return c;
+}
+static void lap_pb(const double *u, double *out) { orc_laplace_pb(u, out, G.ex, G.ey, G.ez, G.k2, G.n); }
 
 /* grid_lcg.c:100-124, grid_maze_lcg.c:107-126, grid_multigrid.c:86-108,
    grid_maze_multigrid.c:86-112: all four solve L phi = -4 pi q/(h eps) by CG from 0. */
@@ -721,7 +1060,8 @@ void solver_init_field(void) {
     memset(G.y, 0, G.m * sizeof(double));
     memcpy(G.phi_prev, G.phi, G.m * sizeof(double));
     for (long t = 0; t < G.m; t++) G.phi[t] = G.q[t] * c;
-    orc_conj_grad(G.phi, G.y, G.phi, G.tol, G.n);
+    if (G.pb) orc_conj_grad_pb(G.phi, G.y, G.phi, G.tol, G.n, G.ex, G.ey, G.ez, G.k2);
+    else orc_conj_grad(G.phi, G.y, G.phi, G.tol, G.n);
 }
 
 /* phi <- 2 phi - phi_prev, phi_prev <- old phi (verlet.c:46-51, grid_multigrid.c:124-129) */
@@ -740,7 +1080,50 @@ int solver_update_field(void) {
         double c = rhs_const();
         memcpy(G.phi_prev, G.phi, m * sizeof(double));
         for (long t = 0; t < m; t++) G.y[t] = G.q[t] * c;
+        if (G.pb) return orc_conj_grad_pb(G.y, G.phi_prev, G.phi, G.tol, n, G.ex, G.ey, G.ez, G.k2);
         return orc_conj_grad(G.y, G.phi_prev, G.phi, G.tol, n);
+    }
+    if (G.pb && G.type == G_MAZE_LCG) {                    /* verlet.c:152-193 */
+        double *tmp = malloc(m * sizeof(double));
+        extrapolate();
+        lap_pb(G.phi, tmp);
+        axpy(tmp, G.q, (4 * PI_D) / G.h, m);
+        res = orc_conj_grad_pb(tmp, G.y, G.y, G.tol, n, G.ex, G.ey, G.ez, G.k2);
+        axpy(G.phi, G.y, -1.0, m);
+        free(tmp);
+        return res;
+    }
+    if (G.pb) {                                            /* grid_multigrid.c:151-177, verlet.c:212-271 */
+        double *tmp = malloc(m * sizeof(double)), *tmp2 = malloc(m * sizeof(double));
+        int it = 0;
+        extrapolate();
+        if (G.type == G_MG) {
+            double c = rhs_const();
+            for (long t = 0; t < m; t++) tmp[t] = G.q[t] * c;
+            while (it < 1000) {
+                orc_mg_pb_apply(tmp, G.phi, n, 4, G.ex, G.ey, G.ez, G.k2);
+                lap_pb(G.phi, tmp2);
+                axpy(tmp2, tmp, -1.0, m);
+                double a = amax(tmp2, m);
+                it++;
+                if (a <= G.tol) { res = it; break; }
+            }
+        } else {
+            lap_pb(G.phi, tmp2);
+            axpy(tmp2, G.q, (4 * PI_D) / G.h, m);
+            while (it < 1000) {
+                orc_mg_pb_apply(tmp2, G.y, n, 4, G.ex, G.ey, G.ez, G.k2);
+                lap_pb(G.y, tmp);
+                axpy(tmp, tmp2, -1., m);
+                double a = amax(tmp, m);
+                it++;
+                if (a <= G.tol) { res = it; break; }
+            }
+            axpy(G.phi, G.y, -1.0, m);
+            if (G.precond != P_NONE) die("Maze Multigrid with preconditioner not implemented");
+        }
+        free(tmp); free(tmp2);
+        return res;
     }
     if (G.type == G_MAZE_LCG) {                            /* verlet.c:31-71 */
         double hh = G.h * G.eps_s;
@@ -800,7 +1183,13 @@ double solver_compute_forces_noel(void) {
     return orc_tf_forces(P.pos, P.types, P.tab, P.ntyp, P.np, P.L, P.rcut, P.fn);
 }
 void solver_compute_forces_tot(void) {                     /* particles.c:777-795 */
-    for (long t = 0; t < 3L * P.np; t++) { double v = 0.0; v += 1.0 * P.fe[t]; v += 1.0 * P.fn[t]; P.ft[t] = v; }
+    for (long t = 0; t < 3L * P.np; t++) {
+        double v = 0.0;
+        v += 1.0 * P.fe[t];
+        v += 1.0 * P.fn[t];
+        if (P.pb) { v += 1.0 * P.fdb[t]; v += 1.0 * P.fib[t]; v += 1.0 * P.fnp[t]; }
+        P.ft[t] = v;
+    }
 }
 
 double get_kinetic_energy(void) {                          /* particles.c:802-820 */
@@ -905,6 +1294,8 @@ void solver_finalize(void) {
     free(G.q); free(G.phi); free(G.phi_prev); free(G.y);
     free(P.types); free(P.pos); free(P.vel); free(P.mass); free(P.chg);
     free(P.fe); free(P.fn); free(P.ft); free(P.nbr); free(P.tab);
+    free(G.ex); free(G.ey); free(G.ez); free(G.k2);
+    free(P.radii); free(P.fdb); free(P.fib); free(P.fnp);
     memset(&G, 0, sizeof(G)); memset(&P, 0, sizeof(P));
 }
 
@@ -941,17 +1332,52 @@ int get_ca_scheme_type_num(void) { return 3; }
 char *get_ca_scheme_type_str(int i) { return cas_names[i]; }
 int get_integrator_type_num(void) { return 2; }
 char *get_integrator_type_str(int i) { return itg_names[i]; }
-void solver_initialize_grid_pois_boltz(double w, double k, int e) { (void)w; (void)k; (void)e; die("PB is outside the oracle"); }
-void solver_initialize_particles_pois_boltz(double a, double b, double *r) { (void)a; (void)b; (void)r; die("PB is outside the oracle"); }
-void solver_update_eps_k2(void) { die("PB is outside the oracle"); }
-double solver_compute_forces_pb(void) { die("PB is outside the oracle"); return 0.0; }
-void get_fcs_db(double *o) { memset(o, 0, 3 * (size_t)P.np * sizeof(double)); }
-void get_fcs_ib(double *o) { memset(o, 0, 3 * (size_t)P.np * sizeof(double)); }
-void get_fcs_np(double *o) { memset(o, 0, 3 * (size_t)P.np * sizeof(double)); }
+void solver_initialize_grid_pois_boltz(double w, double kbar2, int nonpolar) {  /* grid_general.c:84-100 */
+    G.pb = 1; G.nonpolar = nonpolar; G.w = w; G.kbar2 = kbar2;
+    G.ex = calloc(G.m, sizeof(double)); G.ey = calloc(G.m, sizeof(double));
+    G.ez = calloc(G.m, sizeof(double)); G.k2 = calloc(G.m, sizeof(double));
+}
+void solver_initialize_particles_pois_boltz(double gamma_np, double beta_np, double *radii) {
+    P.pb = 1; P.gamma_np = gamma_np; P.beta_np = beta_np;   /* particles.c:111-127 */
+    P.radii = malloc((size_t)P.np * sizeof(double));
+    memcpy(P.radii, radii, (size_t)P.np * sizeof(double));
+    P.fdb = calloc(3 * (size_t)P.np, sizeof(double)); P.fib = calloc(3 * (size_t)P.np, sizeof(double));
+    P.fnp = calloc(3 * (size_t)P.np, sizeof(double));
+}
+void solver_update_eps_k2(void) {                           /* solver_md.c:131-133 */
+    orc_update_eps_k2(P.pos, P.radii, P.np, G.n, G.h, G.w, G.eps_s, G.eps_int, G.kbar2, G.ex, G.ey,
+                      G.ez, G.k2);
+}
+double solver_compute_forces_pb(void) {                     /* particles.c:420-775 */
+    if (!G.pb) die("Poisson-Boltzmann forces are not enabled in the grid.");
+    orc_forces_pb(P.pos, P.radii, P.np, G.n, G.h, G.w, G.eps_s, G.eps_int, P.gamma_np, G.nonpolar, G.phi,
+                  G.ex, G.ey, G.ez, G.k2, P.fdb, P.fib, P.fnp);
+    return 0.0;  /* the reference's non_polar_energy is never accumulated */
+}
+void get_fcs_db(double *o) {
+    if (P.pb) memcpy(o, P.fdb, 3 * (size_t)P.np * sizeof(double));
+    else memset(o, 0, 3 * (size_t)P.np * sizeof(double));
+}
+void get_fcs_ib(double *o) {
+    if (P.pb) memcpy(o, P.fib, 3 * (size_t)P.np * sizeof(double));
+    else memset(o, 0, 3 * (size_t)P.np * sizeof(double));
+}
+void get_fcs_np(double *o) {
+    if (P.pb) memcpy(o, P.fnp, 3 * (size_t)P.np * sizeof(double));
+    else memset(o, 0, 3 * (size_t)P.np * sizeof(double));
+}
+/* the PB face / cell coefficients of the current grid (no reference getter) */
+void orc_get_pb_grids(double *ex, double *ey, double *ez, double *k2) {
+    size_t b = G.m * sizeof(double);
+    memcpy(ex, G.ex, b); memcpy(ey, G.ey, b); memcpy(ez, G.ez, b); memcpy(k2, G.k2, b);
+}
 void get_charges(double *o) { memcpy(o, P.chg, (size_t)P.np * sizeof(double)); }
 void get_masses(double *o) { memcpy(o, P.mass, (size_t)P.np * sizeof(double)); }
 void get_types(int *o) { memcpy(o, P.types, (size_t)P.np * sizeof(int32_t)); }
-void get_radii(double *o) { memset(o, 0, (size_t)P.np * sizeof(double)); }
+void get_radii(double *o) {
+    if (P.pb) memcpy(o, P.radii, (size_t)P.np * sizeof(double));
+    else memset(o, 0, (size_t)P.np * sizeof(double));
+}
 double get_energy_elec(void) {                             /* grid_general.c:304-315 */
     double e = 0.0;
     for (long t = 0; t < G.m; t++) e += 0.5 * G.phi[t];

@@ -31,6 +31,29 @@ void orc_prolong_trilinear(const double *coarse, double *fine, int nc);        /
 int orc_cg_coarse(const double *b, double *x, int n, int maxit, double rtol);  /* multigrid.c:13-96 */
 void orc_mg_apply(const double *rhs, double *x, int n, int sm);                /* multigrid.c:99-168,743 */
 
+/* Poisson-Boltzmann kernels on n^3 arrays: ex/ey/ez are the +x/+y/+z face dielectric
+   coefficients of each point, k2 its screening term */
+void orc_update_eps_k2(const double *pos, const double *radii, int np, int n, double h, double w,
+                       double eps_s, double eps_int, double kbar2, double *eps_x, double *eps_y,
+                       double *eps_z, double *k2);                                     /* grid_general.c:138-301 */
+void orc_laplace_pb(const double *u, double *out, const double *ex, const double *ey,
+                    const double *ez, const double *k2, int n);                        /* laplace.c:77-145 */
+int orc_conj_grad_pb(const double *b, const double *x0, double *x, double tol, int n,
+                     const double *ex, const double *ey, const double *ez, const double *k2); /* plcg.c:169-238 */
+void orc_smooth_pb(const double *rhs, double *x, int n, int iters, const double *ex,
+                   const double *ey, const double *ez, const double *k2);          /* multigrid_pb.c:544-640 */
+void orc_restrict_eps(const double *in, double *out, int n, int axis);              /* multigrid_pb.c:330-447 */
+void orc_restrict_k2(const double *in, double *out, int n);                         /* multigrid_pb.c:459-527 */
+int orc_cg_coarse_pb(const double *b, double *x, int n, int maxit, double rtol, const double *ex,
+                     const double *ey, const double *ez, const double *k2);        /* multigrid_pb.c:16-97 */
+void orc_mg_pb_apply(const double *rhs, double *x, int n, int sm, const double *ex,
+                     const double *ey, const double *ez, const double *k2);        /* multigrid_pb.c:270-328 */
+void orc_forces_pb(const double *pos, const double *radii, int np, int n, double h, double w,
+                   double eps_s, double eps_int, double gamma_np, int nonpolar, const double *phi,
+                   const double *ex, const double *ey, const double *ez, const double *k2,
+                   double *fdb, double *fib, double *fnp);                          /* particles.c:420-775 */
+void orc_get_pb_grids(double *ex, double *ey, double *ez, double *k2);
+
 /* particle kernels */
 void orc_cic_neighbors(const double *pos, int np, int n, double h, int64_t *nbr);      /* particles.c:297-346 */
 void orc_spline_neighbors(const double *pos, int np, int n, double h, int64_t *nbr);   /* particles.c:348-385 */
@@ -78,6 +101,14 @@ void integrator_part_2(void);
 int solver_check_thermostat(void);
 void solver_rescale_velocities(void);
 void solver_finalize(void);
+void solver_initialize_grid_pois_boltz(double w, double kbar2, int nonpolar);
+void solver_initialize_particles_pois_boltz(double gamma_np, double beta_np, double *radii);
+void solver_update_eps_k2(void);
+double solver_compute_forces_pb(void);
+void get_fcs_db(double *o);
+void get_fcs_ib(double *o);
+void get_fcs_np(double *o);
+void get_radii(double *o);
 
 void get_pos(double *o);
 void get_vel(double *o);

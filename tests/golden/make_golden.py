@@ -6,7 +6,8 @@ single-threaded, through its exported functions and its facade, on seeded inputs
 imports the reference's maze_poisson/linkedcell.py for the linked-cell layout. Small
 arrays are stored whole; large fields as SHA-256 of their bytes plus samples.
 
-    OMP_NUM_THREADS=1 python tests/golden/make_golden.py
+    OMP_NUM_THREADS=1 python tests/golden/make_golden.py          # all fixtures
+    OMP_NUM_THREADS=1 python tests/golden/make_golden.py --pb     # Poisson-Boltzmann ones
 """
 import ctypes
 import hashlib
@@ -24,7 +25,7 @@ sys.path.insert(0, ROOT)
 
 from maze_poisson_b200.c_api import CAPI  # noqa: E402
 from maze_poisson_b200.md import MDRun  # noqa: E402
-from maze_poisson_b200.systems import make_system, pair_system  # noqa: E402
+from maze_poisson_b200.systems import make_pb_system, make_system, pair_system, pb_settings  # noqa: E402
 from oracle import loader  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
@@ -164,6 +165,106 @@ def scenario(ref_path, name, spec):
     return rec
 
 
+def pb_inputs(n, seed):
+    """Seeded PB kernel inputs: face coefficients in [1, 78), screening in [0, 0.05), a
+    field xt (tests/test_oracle_pin.py regenerates them the same way)."""
+    rng = np.random.default_rng(seed)
+    ex, ey, ez = (1.0 + 77.0 * rng.random((n, n, n)) for _ in range(3))
+    k2 = 0.05 * rng.random((n, n, n))
+    xt = rng.standard_normal((n, n, n))
+    return ex, ey, ez, k2, xt
+
+
+def pb_kernel_cases(ref):
+    """The Poisson-Boltzmann grid kernels (laplace.c:77-145, plcg.c:169-238,
+    multigrid_pb.c) on seeded positive face coefficients and screening terms."""
+    P = ctypes.c_void_p
+    D, I = ctypes.c_double, ctypes.c_int
+    ref.laplace_filter_pb.argtypes = [P, P, I, I, P, P, P, P]
+    ref.smooth_pb_rbgs.argtypes = [P, P, I, I, D, P, P, P, P]
+    ref.restriction_eps.argtypes = [P, P, I, I, I]
+    ref.restriction_k2screen.argtypes = [P, P, I, I, I]
+    ref.conj_grad_pb.argtypes = [P, P, P, D, I, I, P, P, P, P]
+    ref.conj_grad_pb.restype = I
+    ref.multigrid_pb_apply.argtypes = [P, P, I, I, I, I, P, P, P, P]
+    ref.solver_initialize_grid.argtypes = [I, D, D, D, D, D, I, I]
+    out = {}
+    for n, seed in ((16, 4321), (32, 4322)):
+        ref.solver_initialize()
+        ref.solver_initialize_grid(n, 1.0, 1.0 / n, 1e-7, 1.0, 1.0, 2 if n == 32 else 0, 0)
+        ex, ey, ez, k2, xt = pb_inputs(n, seed)
+        keep = [halo(a) for a in (ex, ey, ez)]
+        cp = [k[1] for k in keep] + [k2.ctypes.data]
+        xtb, xtp = halo(xt)
+        b = np.zeros((n, n, n))
+        ref.laplace_filter_pb(xtp, b.ctypes.data, n, n, *cp)
+        out[f"n{n}_seed"] = np.array(seed)
+        if n == 16:
+            out["n16_b"] = b.copy()
+            rng = np.random.default_rng(99)
+            rhs = rng.standard_normal((n, n, n))
+            x0 = rng.standard_normal((n, n, n))
+            xb, xp = halo(x0)
+            ref.smooth_pb_rbgs(rhs.ctypes.data, xp, n, n, 3.0, *cp)
+            out["rbgs_out"] = xb[1:-1].copy()
+            for axis, (name, arr) in enumerate((("ex", ex), ("ey", ey), ("ez", ez))):
+                ab, ap = halo(arr)
+                c = np.zeros((n // 2,) * 3)
+                ref.restriction_eps(ap, c.ctypes.data, n, n, axis)
+                out[f"restrict_{name}"] = c
+            c = np.zeros((n // 2,) * 3)
+            ref.restriction_k2screen(k2.ctypes.data, c.ctypes.data, n, n, 0)
+            out["restrict_k2"] = c
+            zb, zp = halo(np.zeros((n, n, n)))
+            x = np.zeros((n, n, n))
+            it = ref.conj_grad_pb(b.ctypes.data, zp, x.ctypes.data, 1e-9, n, n, *cp)
+            out["cg_x"], out["cg_iters"] = x, np.array(it)
+        else:
+            out["n32_b_sha"] = np.array(sha(b))
+            xb, xp = halo(np.zeros((n, n, n)))
+            ref.multigrid_pb_apply(b.ctypes.data, xp, n, n, 0, 4, *cp)
+            out["mg_x_sha"] = np.array(sha(xb[1:-1]))
+            out["mg_x_sample"] = xb[1:-1].reshape(-1)[::997].copy()
+        ref.solver_finalize()
+        del keep
+    return out
+
+
+PB_SCENARIOS = {
+    # name: (n_ions, n_grid, box [A], seed, method, tol, steps, nonpolar, eps_s)
+    "pb_lcg": (8, 32, 16.0, 3, "LCG", 1e-10, 2, 1, 78.4),
+    "pb_maze_lcg": (8, 32, 16.0, 3, "MAZE-LCG", 1e-10, 2, 0, 78.4),
+    "pb_multigrid": (8, 32, 16.0, 3, "MULTIGRID", 1e-8, 2, 1, 78.4),
+    "pb_maze_multigrid": (8, 32, 16.0, 3, "MAZE-MULTIGRID", 1e-8, 2, 1, 78.4),
+}
+
+
+def pb_run(capi, spec):
+    """The MD run of a PB scenario (implicit solvent, Tosi-Fumi pairs, Verlet at 300 K)."""
+    n_ions, ng, box, seed, method, tol, steps, nonpolar, eps_s = spec
+    system = make_pb_system(n_ions, ng, box, T=300.0, seed=seed)
+    return MDRun(capi, system, method=method, tol=tol, integrator="VERLET", T=300.0, eps_s=eps_s,
+                 eps_int=1.0, pb=pb_settings(system, eps_s=eps_s, nonpolar=nonpolar))
+
+
+def pb_scenario(ref_path, spec):
+    run = pb_run(CAPI(ref_path, extensions=False), spec)
+    run.initialize()
+    rec = {}
+    for s in range(-1, spec[6]):
+        if s >= 0:
+            run.step()
+        st = run.state()
+        tag = "init" if s < 0 else f"s{s}"
+        for key in ("pos", "vel", "fcs_tot", "fcs_elec", "fcs_noel", "fcs_db", "fcs_ib", "fcs_np"):
+            rec[f"{tag}_{key}"] = st[key]
+        rec[f"{tag}_iters"] = np.array(-2 if st["n_iters"] is None else st["n_iters"])
+        rec[f"{tag}_field_sha"] = np.array(sha(st["field"]))
+        rec[f"{tag}_field_sample"] = st["field"].reshape(-1)[::101].copy()
+    run.finalize()
+    return rec
+
+
 def linked_cells():
     spec = importlib.util.spec_from_file_location(
         "ref_linkedcell", os.path.join(REF_TREE, "maze_poisson", "linkedcell.py"))
@@ -186,6 +287,16 @@ def linked_cells():
 
 
 def main():
+    if "--pb" in sys.argv:
+        loader.build(ref=True)
+        ref = ctypes.CDLL(loader.REF_SO, mode=ctypes.RTLD_LOCAL)
+        np.savez_compressed(os.path.join(OUT, "pb_kernels.npz"), **pb_kernel_cases(ref))
+        for name, spec in PB_SCENARIOS.items():
+            np.savez_compressed(os.path.join(OUT, f"md_{name}.npz"), **pb_scenario(loader.REF_SO, spec))
+            print(name, "done", flush=True)
+        with open(os.path.join(OUT, "pb_scenarios.json"), "w") as f:
+            json.dump({k: list(v) for k, v in PB_SCENARIOS.items()}, f, indent=1)
+        return
     only = None
     if "--only" in sys.argv:  # regenerate just these scenarios (comma-separated)
         only = set(sys.argv[sys.argv.index("--only") + 1].split(","))

@@ -11,7 +11,7 @@ import pytest
 from conftest import GOLDEN
 from maze_poisson_b200.c_api import CAPI
 from maze_poisson_b200.md import MDRun
-from maze_poisson_b200.systems import make_system, pair_system
+from maze_poisson_b200.systems import make_pb_system, make_system, pair_system, pb_settings
 
 
 def sha(a):
@@ -118,3 +118,86 @@ def test_linked_cells_match_reference_chain(oracle_lib):
                 chain.append(int(p))
                 p = link[p]
             assert list(ions[start[c]:start[c + 1]]) == chain[::-1]
+
+
+# ---------------------------------------------------------------- Poisson-Boltzmann
+def pb_inputs(n, seed):
+    """The seeded inputs make_golden.py gave the reference's PB kernels."""
+    rng = np.random.default_rng(seed)
+    ex, ey, ez = (1.0 + 77.0 * rng.random((n, n, n)) for _ in range(3))
+    k2 = 0.05 * rng.random((n, n, n))
+    xt = rng.standard_normal((n, n, n))
+    return ex, ey, ez, k2, xt
+
+
+@pytest.fixture(scope="module")
+def PBK():
+    return np.load(os.path.join(GOLDEN, "pb_kernels.npz"))
+
+
+def test_pb_grid_kernels_bitexact(oracle_lib, PBK):
+    n = 16
+    ex, ey, ez, k2, xt = pb_inputs(n, int(PBK["n16_seed"]))
+    b = np.empty_like(xt)
+    oracle_lib.orc_laplace_pb(xt, b, ex, ey, ez, k2, n)
+    assert np.array_equal(b, PBK["n16_b"])
+    rng = np.random.default_rng(99)
+    rhs = rng.standard_normal((n, n, n))
+    x = rng.standard_normal((n, n, n))
+    oracle_lib.orc_smooth_pb(rhs, x, n, 3, ex, ey, ez, k2)
+    assert np.array_equal(x, PBK["rbgs_out"])
+    for axis, (name, arr) in enumerate((("ex", ex), ("ey", ey), ("ez", ez))):
+        c = np.empty((8, 8, 8))
+        oracle_lib.orc_restrict_eps(arr, c, n, axis)
+        assert np.array_equal(c, PBK[f"restrict_{name}"]), name
+    c = np.empty((8, 8, 8))
+    oracle_lib.orc_restrict_k2(k2, c, n)
+    assert np.array_equal(c, PBK["restrict_k2"])
+    x = np.empty_like(b)
+    it = oracle_lib.orc_conj_grad_pb(b, np.zeros_like(b), x, 1e-9, n, ex, ey, ez, k2)
+    assert it == int(PBK["cg_iters"])
+    assert np.array_equal(x, PBK["cg_x"])
+
+
+def test_pb_vcycle_bitexact(oracle_lib, PBK):
+    n = 32
+    ex, ey, ez, k2, xt = pb_inputs(n, int(PBK["n32_seed"]))
+    b = np.empty_like(xt)
+    oracle_lib.orc_laplace_pb(xt, b, ex, ey, ez, k2, n)
+    assert sha(b) == str(PBK["n32_b_sha"])
+    x = np.zeros_like(xt)
+    oracle_lib.orc_mg_pb_apply(b, x, n, 4, ex, ey, ez, k2)
+    assert np.array_equal(x.reshape(-1)[::997], PBK["mg_x_sample"])
+    assert sha(x) == str(PBK["mg_x_sha"])
+
+
+PB_SCEN = json.load(open(os.path.join(GOLDEN, "pb_scenarios.json")))
+
+
+def pb_run(capi, spec):
+    """The MD run of a PB scenario, built as make_golden.py builds it."""
+    n_ions, ng, box, seed, method, tol, steps, nonpolar, eps_s = spec
+    system = make_pb_system(n_ions, ng, box, T=300.0, seed=seed)
+    return MDRun(capi, system, method=method, tol=tol, integrator="VERLET", T=300.0, eps_s=eps_s,
+                 eps_int=1.0, pb=pb_settings(system, eps_s=eps_s, nonpolar=nonpolar))
+
+
+@pytest.mark.parametrize("name", sorted(PB_SCEN))
+def test_pb_md_scenario_bitexact(oracle_path, name):
+    spec = PB_SCEN[name]
+    g = np.load(os.path.join(GOLDEN, f"md_{name}.npz"))
+    run = pb_run(CAPI(oracle_path, extensions=False), spec)
+    run.initialize()
+    try:
+        for s in range(-1, spec[6]):
+            if s >= 0:
+                run.step()
+            st = run.state()
+            tag = "init" if s < 0 else f"s{s}"
+            iters = -2 if st["n_iters"] is None else st["n_iters"]
+            assert iters == int(g[f"{tag}_iters"]), tag
+            for key in ("pos", "vel", "fcs_tot", "fcs_elec", "fcs_noel", "fcs_db", "fcs_ib", "fcs_np"):
+                assert np.array_equal(st[key], g[f"{tag}_{key}"]), (tag, key)
+            assert sha(st["field"]) == str(g[f"{tag}_field_sha"]), tag
+    finally:
+        run.finalize()
