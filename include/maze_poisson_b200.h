@@ -34,6 +34,22 @@ int mzb_cg_coarse(const double *b, double *x, int n, int maxit, double rtol); /*
 void mzb_mg_apply(const double *rhs, double *x, int n, int sm);            /* multigrid.c:99-168 */
 void mzb_fft_poisson(const double *q, double *phi, int n, double L, double h); /* fftw_wrap.c:166-189 */
 
+/* Poisson-Boltzmann kernel-level entry points; ex/ey/ez/k2 are n^3 arrays of each point's
+   +x/+y/+z face dielectric coefficients and screening term (grid_general.c:138-301) */
+void mzb_laplace_pb(const double *u, double *out, const double *ex, const double *ey,
+                    const double *ez, const double *k2, int n);                 /* laplace.c:77-145 */
+int mzb_conj_grad_pb(const double *b, const double *x0, double *x, double tol, int n,
+                     const double *ex, const double *ey, const double *ez,
+                     const double *k2);                                          /* plcg.c:169-238 */
+void mzb_smooth_pb(const double *rhs, double *x, int n, int iters, const double *ex,
+                   const double *ey, const double *ez, const double *k2);   /* multigrid_pb.c:544-640 */
+void mzb_mg_pb_apply(const double *rhs, double *x, int n, int sm, const double *ex,
+                     const double *ey, const double *ez, const double *k2); /* multigrid_pb.c:270-328 */
+void mzb_restrict_pb(const double *ex, const double *ey, const double *ez, const double *k2,
+                     double *cex, double *cey, double *cez, double *ck2, int n); /* multigrid_pb.c:330-527 */
+/* the PB coefficients of the current grid after solver_update_eps_k2 (no reference getter) */
+void mzb_get_pb_grids(double *ex, double *ey, double *ez, double *k2);
+
 /* precision of the field solve: 0 = the reference's FP64 algorithms (default), 1 = FP32
    multigrid V-cycles with FP64 iterative refinement until the FP64 residual meets the
    grid's tol (or tol_override when > 0). Also selected by MZB_PRECISION=mixed at

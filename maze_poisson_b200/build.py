@@ -29,8 +29,9 @@ SOURCES = {
     "facade.cu": ["--fmad=false"],
     "noalloc.cu": ["--fmad=false"],
     "mixed.cu": ["--fmad=true"],
+    "pb.cu": ["--fmad=false"],
 }
-HEADERS = ["mzb_common.cuh", "engine.cuh", "particles.cuh", "fft.cuh", "tma.cuh", "mixed.cuh"]
+HEADERS = ["mzb_common.cuh", "engine.cuh", "particles.cuh", "fft.cuh", "tma.cuh", "mixed.cuh", "pb.cuh"]
 
 
 def _nvcc():

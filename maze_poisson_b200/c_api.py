@@ -96,6 +96,12 @@ EXTENSION_SYMBOLS = {
     "mzb_prolong_trilinear": (None, [_f64_any, _f64_any, _c.c_int]),
     "mzb_cg_coarse": (_c.c_int, [_f64_any, _f64_any, _c.c_int, _c.c_int, _c.c_double]),
     "mzb_mg_apply": (None, [_f64_any, _f64_any, _c.c_int, _c.c_int]),
+    "mzb_laplace_pb": (None, [_f64_any] * 6 + [_c.c_int]),
+    "mzb_conj_grad_pb": (_c.c_int, [_f64_any, _f64_any, _f64_any, _c.c_double, _c.c_int] + [_f64_any] * 4),
+    "mzb_smooth_pb": (None, [_f64_any, _f64_any, _c.c_int, _c.c_int] + [_f64_any] * 4),
+    "mzb_mg_pb_apply": (None, [_f64_any, _f64_any, _c.c_int, _c.c_int] + [_f64_any] * 4),
+    "mzb_restrict_pb": (None, [_f64_any] * 8 + [_c.c_int]),
+    "mzb_get_pb_grids": (None, [_f64_any] * 4),
     "mzb_fft_poisson": (None, [_f64_any, _f64_any, _c.c_int, _c.c_double, _c.c_double]),
     "mzb_get_cic_neighbors": (None, [_i64_3]),
     "mzb_set_cell_grid": (None, [_c.c_int]),

@@ -609,6 +609,7 @@ bool cg_fast_launch(const EngineArgs& e, cudaStream_t stream) {
         return false;
     };
     const int n = e.n;
+    if (e.pb) return no("Poisson-Boltzmann operator");
     if (!cg_fast_supported(n)) return no("grid size");
     const bool cg_prog = e.prog == PROG_CG || e.prog == PROG_PCG || e.prog == PROG_INIT_FIELD ||
                          e.prog == PROG_LCG_UPDATE || e.prog == PROG_MAZE_LCG;

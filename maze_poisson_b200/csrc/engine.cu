@@ -5,6 +5,8 @@
 // reference's per-point arithmetic (order of the sums, products rounded before adds) so
 // single sweeps are bit-identical to the reference; only the global dot products are
 // summed in a different (fixed, deterministic) order.
+#include <type_traits>
+
 #include "engine.cuh"
 
 namespace mzb {
@@ -72,6 +74,28 @@ __device__ __forceinline__ double lap7(const Nb& o, F&& f) {
     s = s + f(o.km);
     return s - f(o.c) * 6.0;
 }
+
+// The field operators the programs are written over: the reference's Laplacian
+// (laplace.c:24-75) and the Poisson-Boltzmann operator (laplace.c:77-145), whose faces
+// x+, x-, y+, y-, z+, z- multiply their neighbours in that order before the centre term
+// u_c * dg_c, dg = ex_c + ex_{x-1} + ey_c + ey_{y-1} + ez_c + ez_{z-1} + k2_c (the
+// reference's inline diagonal, precomputed with the same additions).
+struct LapOp {
+    template <class F>
+    __device__ __forceinline__ double apply(const Nb& o, F&& f) const { return lap7(o, f); }
+};
+struct PbOp {
+    const double *ex, *ey, *ez, *dg;
+    template <class F>
+    __device__ __forceinline__ double apply(const Nb& o, F&& f) const {
+        double s = f(o.ip) * ex[o.c] + f(o.im) * ex[o.im];
+        s = s + f(o.jp) * ey[o.c];
+        s = s + f(o.jm) * ey[o.jm];
+        s = s + f(o.kp) * ez[o.c];
+        s = s + f(o.km) * ez[o.km];
+        return s - f(o.c) * dg[o.c];
+    }
+};
 
 // ------------------------------------------------------------------------------------
 // Grid-wide reductions: NS sums followed by NM maxima. Results land in every thread.
@@ -150,6 +174,28 @@ __device__ bool rbgs(const Team& t, const double* rhs, double* x, int n, const E
     return true;
 }
 
+// One red-black iteration of the PB smoother (multigrid_pb.c:544-640): x_c = (faces x+,
+// x-, y+, y-, z+, z- times their neighbours, minus rhs_c) / max(dg_c, 1e-14).
+__device__ bool rbgs_pb(const Team& t, const double* rhs, double* x, int n, const PbOp& op,
+                        const EngineArgs& a) {
+    for (int colour = 0; colour < 2; colour++) {
+        for_colour(t, n, colour, [&](int i, int j, int k) {
+            const Nb o = neighbours(n, i, j, k);
+            double d = op.dg[o.c];
+            if (d < 1e-14) d = 1e-14;
+            double s = op.ex[o.c] * x[o.ip] + op.ex[o.im] * x[o.im];
+            s = s + op.ey[o.c] * x[o.jp];
+            s = s + op.ey[o.jm] * x[o.jm];
+            s = s + op.ez[o.c] * x[o.kp];
+            s = s + op.ez[o.km] * x[o.km];
+            s = s - rhs[o.c];
+            x[o.c] = s / d;
+        });
+        if (!grid_sync(a.bar)) return false;
+    }
+    return true;
+}
+
 // 27-point full weighting, coarse (I,J,K) <- fine (2I,2J,2K) (multigrid.c:523-594).
 __device__ void restrict27(const Team& t, const double* in, double* out, int n) {
     const int nc = n / 2;
@@ -213,7 +259,7 @@ __device__ __forceinline__ double prolong_at(const double* in, int nc, int i, in
 }
 
 // ------------------------------------------------------------------------------------
-// Conjugate gradients on L x = b (plcg.c:28-166, multigrid.c:13-96).
+// Conjugate gradients on A x = b (plcg.c:28-238, multigrid.c:13-96, multigrid_pb.c:16-97).
 // ------------------------------------------------------------------------------------
 struct CgSpec {
     int n;
@@ -236,23 +282,25 @@ __device__ bool vcycle(const Team& t, const double* rhs, double* x, int n, int s
                        int& seq);
 
 // Returns the reference's value: conj_grad* -> 0-based iteration at convergence or -1;
-// cg_coarse -> number of iterations run. `ok` turns false on a barrier failure.
-// KIND is the PrecondKind; COARSE selects the cg_coarse variant (never preconditioned, so
-// the V-cycle -> coarse CG call chain is not recursive).
-template <int KIND, bool COARSE>
-__device__ int cg_run(const Team& t, const CgSpec& s, const EngineArgs& a, int& seq, bool& ok) {
-    static_assert(!(COARSE && KIND != PC_IMPLICIT), "coarse CG is unpreconditioned");
+// cg_coarse* -> number of iterations run. `ok` turns false on a barrier failure.
+// KIND is the PrecondKind; COARSE selects the cg_coarse variant (implicit Jacobi for the
+// Laplacian, none for PB; never an MG preconditioner, so the V-cycle -> coarse CG call
+// chain is not recursive). OP is the operator A (LapOp or PbOp).
+template <int KIND, bool COARSE, class OP>
+__device__ int cg_run(const Team& t, const CgSpec& s, const OP& op, const EngineArgs& a, int& seq, bool& ok) {
+    static_assert(!(COARSE && KIND != PC_IMPLICIT && KIND != PC_NONE), "coarse CG has no MG preconditioner");
     const int n = s.n;
     // r = L x0 - b; x = x0; v = 0 (PC_MG)
     double acc[2] = {0.0, 0.0}, mx[1] = {0.0};
     for_points(t, n, [&](int i, int j, int k) {
         const Nb o = neighbours(n, i, j, k);
         const double x0c = s.x0[o.c];
-        const double rr = lap7(o, [&](long q) { return s.x0[q]; }) + -1.0 * s.b[o.c];
+        const double rr = op.apply(o, [&](long q) { return s.x0[q]; }) + -1.0 * s.b[o.c];
         if (s.x != s.x0) s.x[o.c] = x0c;
         s.r[o.c] = rr;
         if (KIND == PC_IMPLICIT) acc[0] += rr * (rr * (1.0 / 6.0));
         else if (KIND == PC_JACOBI) acc[0] += rr * (-rr / 6.0);
+        else if (KIND == PC_NONE) acc[0] += rr * rr;
         else s.v[o.c] = 0.0;
         mx[0] = fmax(mx[0], fabs(rr));
     });
@@ -260,7 +308,7 @@ __device__ int cg_run(const Team& t, const CgSpec& s, const EngineArgs& a, int& 
     if (!ok) return -1;
     double rv;
     if (KIND == PC_IMPLICIT) rv = -acc[0];
-    else if (KIND == PC_JACOBI) rv = acc[0];
+    else if (KIND == PC_JACOBI || KIND == PC_NONE) rv = acc[0];
     else {
         ok = vcycle(t, s.r, s.v, n, 5, a, seq);
         if (!ok) return -1;
@@ -287,6 +335,7 @@ __device__ int cg_run(const Team& t, const CgSpec& s, const EngineArgs& a, int& 
         auto zf = [&](long q) {
             if (KIND == PC_IMPLICIT) return (1.0 / 6.0) * s.r[q];
             if (KIND == PC_JACOBI) return -1.0 * (-s.r[q] / 6.0);
+            if (KIND == PC_NONE) return -1.0 * s.r[q];
             return -1.0 * s.v[q];
         };
         auto pf = [&](long q) { return first ? zf(q) : pold[q] * beta + zf(q); };
@@ -294,7 +343,7 @@ __device__ int cg_run(const Team& t, const CgSpec& s, const EngineArgs& a, int& 
         for_points(t, n, [&](int i, int j, int k) {
             const Nb o = neighbours(n, i, j, k);
             const double pc = pf(o.c);
-            const double ap = lap7(o, pf);
+            const double ap = op.apply(o, pf);
             pnew[o.c] = pc;
             s.Ap[o.c] = ap;
             pap[0] += pc * ap;
@@ -325,6 +374,7 @@ __device__ int cg_run(const Team& t, const CgSpec& s, const EngineArgs& a, int& 
         double rnv;
         if (KIND == PC_IMPLICIT) rnv = -sums[0] / 6.0;
         else if (KIND == PC_JACOBI) rnv = sums[1];
+        else if (KIND == PC_NONE) rnv = sums[0];
         else {
             ok = vcycle(t, s.r, s.v, n, 5, a, seq);
             if (!ok) return -1;
@@ -368,7 +418,7 @@ __device__ bool vcycle(const Team& t, const double* rhs, double* x, int n, int s
     cs.Ap = a.cAp; cs.v = nullptr; cs.kind = PC_IMPLICIT; cs.coarse = true; cs.tol = 0.0;
     cs.rtol = 1e-5; cs.limit = 50;
     bool ok = true;
-    cg_run<PC_IMPLICIT, true>(t, cs, a, seq, ok);
+    cg_run<PC_IMPLICIT, true>(t, cs, LapOp{}, a, seq, ok);
     if (!ok) return false;
     for_points(t, n, [&](int i, int j, int k) {
         const long c = ((long)i * n + j) * n + k;
@@ -380,13 +430,49 @@ __device__ bool vcycle(const Team& t, const double* rhs, double* x, int n, int s
     return true;
 }
 
-// max |L x - b| over the grid (the reference's residual check after each V-cycle).
-__device__ bool resid_max(const Team& t, const double* x, const double* b, int n, const EngineArgs& a,
-                          int& seq, double& out) {
+// One PB V-cycle (multigrid_pb.c:270-328): sm PB smoother iterations, residual
+// rf = -(A x) + rhs, 27-pt restriction, coarse PB CG (unpreconditioned, 50 it, rtol
+// 1e-5) from zero on the restricted coefficients, x += P e, sm iterations.
+__device__ bool vcycle_pb(const Team& t, const double* rhs, double* x, int n, int sm, const EngineArgs& a,
+                          int& seq) {
+    const int nc = n / 2;
+    const PbOp fine{a.ex, a.ey, a.ez, a.dg}, coarse{a.cex, a.cey, a.cez, a.cdg};
+    for (int it = 0; it < sm; it++)
+        if (!rbgs_pb(t, rhs, x, n, fine, a)) return false;
+    for_points(t, n, [&](int i, int j, int k) {
+        const Nb o = neighbours(n, i, j, k);
+        const double lx = fine.apply(o, [&](long q) { return x[q]; });
+        a.rf[o.c] = -lx + 1.0 * rhs[o.c];
+    });
+    if (!grid_sync(a.bar)) return false;
+    restrict27(t, a.rf, a.rc, n);
+    for_points(t, nc, [&](int i, int j, int k) { a.ec[((long)i * nc + j) * nc + k] = 0.0; });
+    if (!grid_sync(a.bar)) return false;
+    CgSpec cs;
+    cs.n = nc; cs.b = a.rc; cs.x0 = a.ec; cs.x = a.ec; cs.r = a.cr; cs.p0 = a.cp0; cs.p1 = a.cp1;
+    cs.Ap = a.cAp; cs.v = nullptr; cs.kind = PC_NONE; cs.coarse = true; cs.tol = 0.0;
+    cs.rtol = 1e-5; cs.limit = 50;
+    bool ok = true;
+    cg_run<PC_NONE, true>(t, cs, coarse, a, seq, ok);
+    if (!ok) return false;
+    for_points(t, n, [&](int i, int j, int k) {
+        const long c = ((long)i * n + j) * n + k;
+        x[c] = x[c] + 1.0 * prolong_at(a.ec, nc, i, j, k);
+    });
+    if (!grid_sync(a.bar)) return false;
+    for (int it = 0; it < sm; it++)
+        if (!rbgs_pb(t, rhs, x, n, fine, a)) return false;
+    return true;
+}
+
+// max |A x - b| over the grid (the reference's residual check after each V-cycle).
+template <class OP>
+__device__ bool resid_max(const Team& t, const double* x, const double* b, int n, const OP& op,
+                          const EngineArgs& a, int& seq, double& out) {
     double s0[1], mx[1] = {0.0};
     for_points(t, n, [&](int i, int j, int k) {
         const Nb o = neighbours(n, i, j, k);
-        const double lx = lap7(o, [&](long q) { return x[q]; });
+        const double lx = op.apply(o, [&](long q) { return x[q]; });
         mx[0] = fmax(mx[0], fabs(lx + -1.0 * b[o.c]));
     });
     const bool ok = grid_reduce<0, 1>(s0, mx, a, seq);
@@ -394,18 +480,25 @@ __device__ bool resid_max(const Team& t, const double* x, const double* b, int n
     return ok;
 }
 
-__global__ void __launch_bounds__(kThreads, kMinBlocksPerSM) engine_kernel(EngineArgs a) {
-    const Team t = make_team();
+// The programs over operator OP. With the PB operator the solves follow the reference's
+// PB branches: conj_grad_pb (plcg.c:169-238, implicit Jacobi whatever the grid's
+// preconditioner), verlet_poisson_pb (verlet.c:152-193), and the PB V-cycle with 4
+// smoother iterations (MG_SOLVE_SM_PB, grid_multigrid.c:151-177, verlet.c:212-271).
+template <class OP>
+__device__ void engine_body(const Team& t, const EngineArgs& a, const OP& op, int& result, bool& ok) {
+    constexpr bool PB = !std::is_same<OP, LapOp>::value;
     int seq = 0;
-    bool ok = true;
-    int result = 0;
     const int n = a.n;
+    auto mg_cycle = [&](const double* rhs, double* x, int sm) {
+        if constexpr (PB) return vcycle_pb(t, rhs, x, n, sm, a, seq);
+        else return vcycle(t, rhs, x, n, sm, a, seq);
+    };
 
     switch (a.prog) {
     case PROG_LAPLACE:
         for_points(t, n, [&](int i, int j, int k) {
             const Nb o = neighbours(n, i, j, k);
-            a.out[o.c] = lap7(o, [&](long q) { return a.u[q]; });
+            a.out[o.c] = op.apply(o, [&](long q) { return a.u[q]; });
         });
         break;
 
@@ -417,15 +510,23 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksPerSM) engine_kernel(Engin
         s.v = a.v; s.kind = a.prog == PROG_PCG ? a.precond : PC_IMPLICIT;
         s.coarse = a.prog == PROG_CG_COARSE; s.tol = a.tol; s.rtol = a.rtol;
         s.limit = s.coarse ? a.maxit : (long)n * n;
-        if (s.coarse) result = cg_run<PC_IMPLICIT, true>(t, s, a, seq, ok);
-        else if (s.kind == PC_JACOBI) result = cg_run<PC_JACOBI, false>(t, s, a, seq, ok);
-        else if (s.kind == PC_MG) result = cg_run<PC_MG, false>(t, s, a, seq, ok);
-        else result = cg_run<PC_IMPLICIT, false>(t, s, a, seq, ok);
+        if constexpr (PB) {
+            if (s.coarse) result = cg_run<PC_NONE, true>(t, s, op, a, seq, ok);
+            else result = cg_run<PC_IMPLICIT, false>(t, s, op, a, seq, ok);
+        } else {
+            if (s.coarse) result = cg_run<PC_IMPLICIT, true>(t, s, op, a, seq, ok);
+            else if (s.kind == PC_JACOBI) result = cg_run<PC_JACOBI, false>(t, s, op, a, seq, ok);
+            else if (s.kind == PC_MG) result = cg_run<PC_MG, false>(t, s, op, a, seq, ok);
+            else result = cg_run<PC_IMPLICIT, false>(t, s, op, a, seq, ok);
+        }
         break;
     }
 
     case PROG_SMOOTH:
-        for (int it = 0; it < a.sm && ok; it++) ok = rbgs(t, a.b, a.x, n, a);
+        for (int it = 0; it < a.sm && ok; it++) {
+            if constexpr (PB) ok = rbgs_pb(t, a.b, a.x, n, op, a);
+            else ok = rbgs(t, a.b, a.x, n, a);
+        }
         break;
 
     case PROG_RESTRICT:
@@ -439,7 +540,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksPerSM) engine_kernel(Engin
         break;
 
     case PROG_MG_APPLY:
-        ok = vcycle(t, a.b, a.x, n, a.sm, a, seq);
+        ok = mg_cycle(a.b, a.x, a.sm);
         break;
 
     case PROG_INIT_FIELD:
@@ -459,22 +560,22 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksPerSM) engine_kernel(Engin
         s.n = n; s.b = init ? a.phi_new : a.y; s.x0 = init ? a.y : a.phi_old; s.x = a.phi_new;
         s.r = a.r; s.p0 = a.p0; s.p1 = a.p1; s.Ap = a.Ap; s.v = a.v; s.kind = PC_IMPLICIT;
         s.coarse = false; s.tol = a.tol; s.rtol = 0.0; s.limit = (long)n * n;
-        result = cg_run<PC_IMPLICIT, false>(t, s, a, seq, ok);
+        result = cg_run<PC_IMPLICIT, false>(t, s, op, a, seq, ok);
         break;
     }
 
     case PROG_MAZE_LCG:
     case PROG_MAZE_MG:
     case PROG_MG_UPDATE: {
-        // phi_new = 2 phi - phi_prev (verlet.c:46-51). MaZe: tmp = L phi_new + c q,
-        // the constraint sigma_p (verlet.c:54-55,108-110). MULTIGRID: tmp = c q.
+        // phi_new = 2 phi - phi_prev (verlet.c:46-51). MaZe: tmp = A phi_new + c q,
+        // the constraint sigma_p (verlet.c:54-55,108-110,174-179). MULTIGRID: tmp = c q.
         const bool maze = a.prog != PROG_MG_UPDATE;
         for_points(t, n, [&](int i, int j, int k) {
             const Nb o = neighbours(n, i, j, k);
             auto ex = [&](long q) { return 2 * a.phi_old[q] - a.phi_prev[q]; };
             const double pc = ex(o.c);
             a.phi_new[o.c] = pc;
-            if (maze) a.tmp[o.c] = lap7(o, ex) + a.c * a.q[o.c];
+            if (maze) a.tmp[o.c] = op.apply(o, ex) + a.c * a.q[o.c];
             else a.tmp[o.c] = a.q[o.c] * a.c;
         });
         ok = grid_sync(a.bar);
@@ -483,22 +584,24 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksPerSM) engine_kernel(Engin
         if (a.prog == PROG_MAZE_LCG) {
             CgSpec s;
             s.n = n; s.b = a.tmp; s.x0 = a.y; s.x = a.y; s.r = a.r; s.p0 = a.p0; s.p1 = a.p1;
-            s.Ap = a.Ap; s.v = a.v; s.kind = a.precond; s.coarse = false; s.tol = a.tol;
+            s.Ap = a.Ap; s.v = a.v; s.kind = PB ? PC_IMPLICIT : a.precond; s.coarse = false; s.tol = a.tol;
             s.rtol = 0.0; s.limit = (long)n * n;
-            if (a.precond == PC_JACOBI) result = cg_run<PC_JACOBI, false>(t, s, a, seq, ok);
-            else if (a.precond == PC_MG) result = cg_run<PC_MG, false>(t, s, a, seq, ok);
-            else result = cg_run<PC_IMPLICIT, false>(t, s, a, seq, ok);
+            if (PB || s.kind == PC_IMPLICIT) result = cg_run<PC_IMPLICIT, false>(t, s, op, a, seq, ok);
+            else if constexpr (!PB) {
+                if (s.kind == PC_JACOBI) result = cg_run<PC_JACOBI, false>(t, s, op, a, seq, ok);
+                else result = cg_run<PC_MG, false>(t, s, op, a, seq, ok);
+            }
             if (!ok) break;
         } else {
-            // repeat V-cycles until |L sol - tmp|_inf <= tol, at most 1000
-            // (grid_multigrid.c:185-206, verlet.c:121-136)
+            // repeat V-cycles until |A sol - tmp|_inf <= tol, at most 1000
+            // (grid_multigrid.c:151-206, verlet.c:121-136, 236-262)
             result = -1;
             int it = 0;
             while (it < 1000) {
-                ok = vcycle(t, a.tmp, sol, n, 3, a, seq);
+                ok = mg_cycle(a.tmp, sol, PB ? 4 : 3);
                 if (!ok) break;
                 double rmax;
-                ok = resid_max(t, sol, a.tmp, n, a, seq, rmax);
+                ok = resid_max(t, sol, a.tmp, n, op, a, seq, rmax);
                 if (!ok) break;
                 it++;
                 if (rmax <= a.tol) { result = it; break; }
@@ -517,7 +620,14 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksPerSM) engine_kernel(Engin
         ok = false;
         break;
     }
+}
 
+__global__ void __launch_bounds__(kThreads, kMinBlocksPerSM) engine_kernel(EngineArgs a) {
+    const Team t = make_team();
+    bool ok = true;
+    int result = 0;
+    if (a.pb) engine_body(t, a, PbOp{a.ex, a.ey, a.ez, a.dg}, result, ok);
+    else engine_body(t, a, LapOp{}, result, ok);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         a.result[0] = result;
         a.result[1] = ok ? 0 : 1;

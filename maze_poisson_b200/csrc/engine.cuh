@@ -23,7 +23,8 @@ enum EngineProg : int {
     PROG_MAZE_MG = 13,    // verlet_poisson_multigrid                   verlet.c:86-149
 };
 
-enum PrecondKind : int { PC_IMPLICIT = 0, PC_JACOBI = 1, PC_MG = 2 };
+// PC_NONE: unpreconditioned CG, p = -r (the PB coarse solve, multigrid_pb.c:16-97)
+enum PrecondKind : int { PC_IMPLICIT = 0, PC_JACOBI = 1, PC_MG = 2, PC_NONE = 3 };
 
 struct EngineArgs {
     int prog;
@@ -64,6 +65,13 @@ struct EngineArgs {
     double* cp0;
     double* cp1;
     double* cAp;
+
+    // Poisson-Boltzmann operator (pb != 0, laplace.c:77-145): +x/+y/+z face coefficients
+    // and the diagonal (six faces + k2) of the n^3 grid, and the same for the (n/2)^3
+    // grid of the PB V-cycle (multigrid_pb.c:270-328)
+    int pb;
+    const double *ex, *ey, *ez, *dg;
+    const double *cex, *cey, *cez, *cdg;
 
     double* partials;  // 2 sets x 8 values x gridDim.x
     GridBarrier* bar;

@@ -16,6 +16,7 @@
 #include "fft.cuh"
 #include "mixed.cuh"
 #include "particles.cuh"
+#include "pb.cuh"
 
 namespace mzb {
 
@@ -77,6 +78,9 @@ struct GridState {
     float* lev_b[kMixedMaxLevels] = {};
     float* lev_r[kMixedMaxLevels] = {};
     float* lev_g = nullptr;   // Green's function of the coarsest level (direct solve) or null
+    // Poisson-Boltzmann (solver_initialize_grid_pois_boltz, grid_general.c:84-100)
+    bool pb = false;
+    PbGrid pbg;
 
     double* phi() const { return buf[iphi]; }
     double* phi_prev() const { return buf[iprev]; }
@@ -101,6 +105,7 @@ struct System {
     double q_tot = 0.0;           // charge of the last spreading; persists like solver_md.c:16
     uint64_t epoch = 0;           // bumped by host-side changes that batched-step graphs bake in
     double* qtot_d = nullptr;     // device copy of q_tot (batched steps check charge on the device)
+    std::vector<double> pb_radii; // host copy of the PB solvation radii
     int* err_d = nullptr;         // batched steps: [0] charge error, [1] spread overflow, [2] solve failure
 };
 
@@ -135,6 +140,10 @@ void free_grid(GridState& G) {
     dfree(G.r); dfree(G.p0); dfree(G.p1); dfree(G.Ap); dfree(G.v); dfree(G.rf); dfree(G.tmp);
     dfree(G.rc); dfree(G.ec); dfree(G.cr); dfree(G.cp0); dfree(G.cp1); dfree(G.cAp);
     G.fft.release();
+    dfree(G.pbg.ex); dfree(G.pbg.ey); dfree(G.pbg.ez); dfree(G.pbg.k2); dfree(G.pbg.dg);
+    dfree(G.pbg.cex); dfree(G.pbg.cey); dfree(G.pbg.cez); dfree(G.pbg.ck2); dfree(G.pbg.cdg);
+    G.pbg = PbGrid{};
+    G.pb = false;
     for (int l = 0; l < kMixedMaxLevels; l++) {
         if (G.lev_x[l]) cudaFree(G.lev_x[l]);
         if (G.lev_b[l]) cudaFree(G.lev_b[l]);
@@ -149,11 +158,12 @@ void free_grid(GridState& G) {
     G.ready = false;
 }
 
-// Mixed precision needs at least three multigrid levels (n, n/2, n/4 even).
+// Mixed precision needs at least three multigrid levels (n, n/2, n/4 even) and the
+// plain Laplacian (Poisson-Boltzmann grids stay on the FP64 solvers).
 bool mixed_supported(const GridState& G) {
     int sizes[kMixedMaxLevels];
     const int L = mixed_levels(G.n, sizes);
-    return G.type != 1 && G.n <= kMixedMaxN && L >= 3 && mixed_small_level(L, sizes) >= 1;
+    return G.type != 1 && !G.pb && G.n <= kMixedMaxN && L >= 3 && mixed_small_level(L, sizes) >= 1;
 }
 
 void ensure_mixed_levels(GridState& G) {
@@ -182,6 +192,7 @@ void free_particles(ParticleDev& P) {
     dfree(P.cell_of); dfree(P.cell_count); dfree(P.cell_start); dfree(P.cell_fill);
     dfree(P.cell_ions); dfree(P.srank); dfree(P.spos); dfree(P.stype); dfree(P.fpart);
     dfree(P.epart); dfree(P.red); dfree(P.flags); dfree(P.partial);
+    dfree(P.radii); dfree(P.fdb); dfree(P.fib); dfree(P.fnp); dfree(P.pb_part);
     P = ParticleDev{};
 }
 
@@ -203,6 +214,13 @@ void set_cells(ParticleDev& P, int nc) {
     P.epart = dalloc<double>((size_t)nblk * P.tf_split);
 }
 
+// Point the engine's PB operator at the coefficients of g.
+void set_pb_operator(EngineArgs& a, const PbGrid& g) {
+    a.pb = 1;
+    a.ex = g.ex; a.ey = g.ey; a.ez = g.ez; a.dg = g.dg;
+    a.cex = g.cex; a.cey = g.cey; a.cez = g.cez; a.cdg = g.cdg;
+}
+
 EngineArgs engine_base(System& s) {
     GridState& G = s.G;
     EngineArgs a{};
@@ -215,6 +233,7 @@ EngineArgs engine_base(System& s) {
     a.result = s.result;
     a.q = G.q;
     a.y = G.y;
+    if (G.pb) set_pb_operator(a, G.pbg);
     return a;
 }
 
@@ -366,9 +385,32 @@ void require_mg_size(int n) {
     if (n / 2 < 16 || n % 2) fatal("Multigrid: requires an even grid with n/2 >= 16");
 }
 
+// -4 pi / h, divided by eps_s unless the PB operator carries the dielectric
+// (grid_lcg.c:100-110)
 double rhs_const(const GridState& G) {
-    double c = -4 * kPi / G.h;  // grid_lcg.c:418-422
-    return c / G.eps_s;
+    double c = -4 * kPi / G.h;
+    if (!G.pb) c /= G.eps_s;
+    return c;
+}
+
+// (4 pi) / h of the MaZe constraint: h <- h * eps_s on Poisson grids (grid_maze_lcg.c:158,
+// grid_maze_multigrid.c:133), plain h with PB (verlet.c:178, 232)
+double maze_const(const GridState& G) { return G.pb ? (4 * kPi) / G.h : (4 * kPi) / (G.h * G.eps_s); }
+
+// Check the PB boxes fit the grid and size the force partials (the reference writes out of
+// bounds when a box of +-(floor((r_s+w)/h)+2) points is wider than the grid).
+void ensure_pb_forces(System& s) {
+    GridState& G = s.G;
+    ParticleDev& P = s.P;
+    if (P.pb_range > 0) return;
+    int rmax = 0;
+    for (double r : s.pb_radii) {
+        const int rg = (int)floor((r + G.pbg.w) / G.h) + 2;
+        rmax = rg > rmax ? rg : rmax;
+    }
+    if (rmax >= G.n) fatal("Poisson-Boltzmann: an ion's solvation box is wider than the grid");
+    P.pb_range = rmax;
+    P.pb_part = dalloc<double>((size_t)P.np * (2 * rmax + 1) * 9);
 }
 
 }  // namespace
@@ -474,8 +516,35 @@ void solver_initialize_grid(int n, double L, double h, double tol, double eps, d
     G.ready = true;
 }
 
-void solver_initialize_grid_pois_boltz(double, double, int) {
-    fatal("Poisson-Boltzmann is not supported by this build");
+// grid_pb_init (grid_general.c:84-100): face coefficients, screening term and the PB
+// operator's diagonal on the grid (and the coarse grid of the PB V-cycle on MULTIGRID and
+// MAZE-MULTIGRID grids); filled by solver_update_eps_k2.
+void solver_initialize_grid_pois_boltz(double w, double kbar2, int nonpolar_enabled) {
+    System& s = sys();
+    GridState& G = grid();
+    touch(s);
+    PbGrid& g = G.pbg;
+    if (!G.pb) {
+        g.ex = dalloc<double>(G.m); g.ey = dalloc<double>(G.m); g.ez = dalloc<double>(G.m);
+        g.k2 = dalloc<double>(G.m); g.dg = dalloc<double>(G.m);
+        if (G.type == G_MG || G.type == G_MAZE_MG) {
+            const long mc = G.m / 8;
+            g.cex = dalloc<double>(mc); g.cey = dalloc<double>(mc); g.cez = dalloc<double>(mc);
+            g.ck2 = dalloc<double>(mc); g.cdg = dalloc<double>(mc);
+        }
+    }
+    G.pb = true;
+    g.n = G.n;
+    g.h = G.h;
+    g.w = w;
+    g.eps_s = G.eps_s;
+    g.eps_int = G.eps_int;
+    g.kbar2 = kbar2;
+    g.nonpolar = nonpolar_enabled;
+    if (s.parts_ready) {  // the force boxes depend on w
+        dfree(s.P.pb_part);
+        s.P.pb_range = 0;
+    }
 }
 
 void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, int pot_type, int cas_type,
@@ -489,6 +558,7 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
         fatal("B-spline charge assignment needs a grid of at least 4 points per side");
     if (n_typ < 1 || n_typ > 8) fatal("between 1 and 8 particle types are supported");
     if (s.parts_ready) free_particles(s.P);
+    s.pb_radii.clear();
     ParticleDev& P = s.P;
     P.cas = cas_type;
     P.np = n_p;
@@ -570,8 +640,23 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
     s.parts_ready = true;
 }
 
-void solver_initialize_particles_pois_boltz(double, double, double*) {
-    fatal("Poisson-Boltzmann is not supported by this build");
+// particles_pb_init (particles.c:111-127): solvation radii and the three PB force arrays.
+void solver_initialize_particles_pois_boltz(double gamma_np, double beta_np, double* solv_radii) {
+    System& s = sys();
+    ParticleDev& P = parts();
+    touch(s);
+    P.gamma_np = gamma_np;
+    P.beta_np = beta_np;
+    if (!P.fdb) {
+        P.radii = dalloc<double>(P.np);
+        P.fdb = dalloc<double>((size_t)3 * P.np);
+        P.fib = dalloc<double>((size_t)3 * P.np);
+        P.fnp = dalloc<double>((size_t)3 * P.np);
+    }
+    if (P.np > 0) MZB_CHECK(cudaMemcpy(P.radii, solv_radii, sizeof(double) * P.np, cudaMemcpyHostToDevice));
+    s.pb_radii.assign(solv_radii, solv_radii + P.np);
+    dfree(P.pb_part);
+    P.pb_range = 0;
 }
 
 void solver_initialize_integrator(int n_p, double dt, double T, double gamma, int itg_type, int itg_enabled) {
@@ -659,7 +744,7 @@ int solver_update_field(void) {
         }
         if (G.type == G_LCG) return run_mixed(s, PROG_LCG_UPDATE, rhs_const(G));
         if (G.type == G_MG) return run_mixed(s, PROG_MG_UPDATE, rhs_const(G));
-        return run_mixed(s, G.type == G_MAZE_LCG ? PROG_MAZE_LCG : PROG_MAZE_MG, (4 * kPi) / (G.h * G.eps_s));
+        return run_mixed(s, G.type == G_MAZE_LCG ? PROG_MAZE_LCG : PROG_MAZE_MG, maze_const(G));
     }
     EngineArgs a = engine_base(s);
     a.phi_old = G.phi();
@@ -672,8 +757,8 @@ int solver_update_field(void) {
         break;
     case G_MAZE_LCG:
         a.prog = PROG_MAZE_LCG;
-        a.c = (4 * kPi) / (G.h * G.eps_s);  // verlet.c:55 with h <- h*eps (grid_maze_lcg.c:158)
-        if (G.precond == P_NONE) a.precond = PC_IMPLICIT;
+        a.c = maze_const(G);  // verlet.c:55 with h <- h*eps (grid_maze_lcg.c:158); PB verlet.c:178
+        if (G.precond == P_NONE || G.pb) a.precond = PC_IMPLICIT;  // PB ignores it (grid_maze_lcg.c:150-156)
         else if (G.precond == P_JACOBI) a.precond = PC_JACOBI;
         else if (G.precond == P_MG) a.precond = PC_MG;
         else fatal("SSOR and BLOCKJACOBI preconditioners are not supported by this build");
@@ -684,7 +769,7 @@ int solver_update_field(void) {
         break;
     case G_MAZE_MG:
         a.prog = PROG_MAZE_MG;
-        a.c = (4 * kPi) / (G.h * G.eps_s);
+        a.c = maze_const(G);
         break;
     }
     const int res = run_engine(s, a);
@@ -717,7 +802,16 @@ void solver_set_field_prev(double* phi) {
     sync();
 }
 
-void solver_update_eps_k2(void) { fatal("Poisson-Boltzmann is not supported by this build"); }
+// grid_update_eps_and_k2 (grid_general.c:138-301) from the current positions.
+void solver_update_eps_k2(void) {
+    System& s = sys();
+    GridState& G = grid();
+    ParticleDev& P = parts();
+    if (!G.pb || !P.fdb)
+        fatal("solver_update_eps_k2: Poisson-Boltzmann is not initialised for the grid and the particles");
+    ensure_pb_forces(s);
+    pb_update_coefficients(G.pbg, P.pos, P.radii, P.np, s.stream);
+}
 
 void solver_compute_forces_elec(void) {
     System& s = sys();
@@ -735,8 +829,23 @@ double solver_compute_forces_noel(void) {
     return s.red_h[1];
 }
 
+// particles_compute_forces_pb (particles.c:420-775); returns the non-polar energy, which
+// the reference never accumulates (always 0).
 double solver_compute_forces_pb(void) {
-    fatal("Poisson-Boltzmann is not supported by this build");
+    System& s = sys();
+    GridState& G = grid();
+    ParticleDev& P = parts();
+    if (!G.pb) {
+        fprintf(stderr, "Poisson-Boltzmann forces are not enabled in the grid.\n");
+        exit(1);
+    }
+    if (!P.fdb) fatal("solver_compute_forces_pb: solver_initialize_particles_pois_boltz() has not been called");
+    ensure_pb_forces(s);
+    const double cdb = G.h / (8.0 * kPi);
+    const double cnp = -P.gamma_np * G.h / (G.eps_s - G.eps_int);
+    pb_forces(G.pbg, G.phi(), P.pos, P.radii, P.np, P.pb_range, cdb, cnp, P.pb_part, P.fdb, P.fib, P.fnp,
+              s.stream);
+    return 0.0;
 }
 
 void solver_compute_forces_tot(void) { total_forces(parts(), sys().stream); }
@@ -798,13 +907,17 @@ void get_vel(double* recv) { ParticleDev& P = parts(); d2h(recv, P.vel, sizeof(d
 void get_fcs_elec(double* recv) { ParticleDev& P = parts(); d2h(recv, P.fe, sizeof(double) * 3 * P.np); }
 void get_fcs_noel(double* recv) { ParticleDev& P = parts(); d2h(recv, P.fn, sizeof(double) * 3 * P.np); }
 void get_fcs_tot(double* recv) { ParticleDev& P = parts(); d2h(recv, P.ft, sizeof(double) * 3 * P.np); }
-void get_fcs_db(double* recv) { memset(recv, 0, sizeof(double) * 3 * parts().np); }
-void get_fcs_ib(double* recv) { memset(recv, 0, sizeof(double) * 3 * parts().np); }
-void get_fcs_np(double* recv) { memset(recv, 0, sizeof(double) * 3 * parts().np); }
+static void get_or_zero(double* recv, const double* d, size_t count) {
+    if (d) d2h(recv, d, sizeof(double) * count);
+    else memset(recv, 0, sizeof(double) * count);
+}
+void get_fcs_db(double* recv) { ParticleDev& P = parts(); get_or_zero(recv, P.fdb, (size_t)3 * P.np); }
+void get_fcs_ib(double* recv) { ParticleDev& P = parts(); get_or_zero(recv, P.fib, (size_t)3 * P.np); }
+void get_fcs_np(double* recv) { ParticleDev& P = parts(); get_or_zero(recv, P.fnp, (size_t)3 * P.np); }
 void get_types(int* recv) { ParticleDev& P = parts(); d2h(recv, P.types, sizeof(int32_t) * P.np); }
 void get_charges(double* recv) { ParticleDev& P = parts(); d2h(recv, P.chg, sizeof(double) * P.np); }
 void get_masses(double* recv) { ParticleDev& P = parts(); d2h(recv, P.mass, sizeof(double) * P.np); }
-void get_radii(double* recv) { memset(recv, 0, sizeof(double) * parts().np); }
+void get_radii(double* recv) { ParticleDev& P = parts(); get_or_zero(recv, P.radii, (size_t)P.np); }
 void get_field(double* recv) { GridState& G = grid(); d2h(recv, G.phi(), sizeof(double) * G.m); }
 void get_field_prev(double* recv) {
     GridState& G = grid();
@@ -1071,6 +1184,138 @@ void mzb_mg_apply(const double* rhs, double* x, int n, int sm) {
     d2h_sync(x, dx, m);
 }
 
+// ---- Poisson-Boltzmann kernel-level entry points: ex/ey/ez/k2 are host n^3 arrays of the
+// +x/+y/+z face coefficients and screening term of each point.
+}  // extern "C"
+namespace mzb {
+namespace {
+PbGrid scratch_pb(System& s, Work& w, int n, const double* ex, const double* ey, const double* ez,
+                  const double* k2, bool coarse) {
+    const long m = (long)n * n * n;
+    PbGrid g;
+    g.n = n;
+    g.ex = w.get(m); g.ey = w.get(m); g.ez = w.get(m); g.k2 = w.get(m); g.dg = w.get(m);
+    h2d(g.ex, ex, m); h2d(g.ey, ey, m); h2d(g.ez, ez, m); h2d(g.k2, k2, m);
+    if (coarse) {
+        const long mc = m / 8;
+        g.cex = w.get(mc); g.cey = w.get(mc); g.cez = w.get(mc); g.ck2 = w.get(mc); g.cdg = w.get(mc);
+    }
+    pb_derive(g, s.stream);
+    return g;
+}
+}  // namespace
+}  // namespace mzb
+extern "C" {
+
+// out = A_pb u (laplace.c:77-145)
+void mzb_laplace_pb(const double* u, double* out, const double* ex, const double* ey, const double* ez,
+                    const double* k2, int n) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    EngineArgs a = scratch_engine(s, w, n);
+    set_pb_operator(a, scratch_pb(s, w, n, ex, ey, ez, k2, false));
+    double* du = w.get(m);
+    double* dout = w.get(m);
+    h2d(du, u, m);
+    a.prog = PROG_LAPLACE;
+    a.u = du;
+    a.out = dout;
+    run_engine(s, a);
+    d2h_sync(out, dout, m);
+}
+
+// conj_grad_pb (plcg.c:169-238); returns the reference's return value
+int mzb_conj_grad_pb(const double* b, const double* x0, double* x, double tol, int n, const double* ex,
+                     const double* ey, const double* ez, const double* k2) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    EngineArgs a = scratch_engine(s, w, n);
+    set_pb_operator(a, scratch_pb(s, w, n, ex, ey, ez, k2, false));
+    double* db = w.get(m);
+    double* dx0 = w.get(m);
+    double* dx = w.get(m);
+    h2d(db, b, m);
+    h2d(dx0, x0, m);
+    a.prog = PROG_CG;
+    a.tol = tol;
+    a.b = db;
+    a.x0 = dx0;
+    a.x = dx;
+    const int res = run_engine(s, a);
+    d2h_sync(x, dx, m);
+    return res;
+}
+
+// smooth_pb_rbgs (multigrid_pb.c:544-640): `iters` red-black iterations on x in place
+void mzb_smooth_pb(const double* rhs, double* x, int n, int iters, const double* ex, const double* ey,
+                   const double* ez, const double* k2) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    EngineArgs a = scratch_engine(s, w, n);
+    set_pb_operator(a, scratch_pb(s, w, n, ex, ey, ez, k2, false));
+    double* db = w.get(m);
+    double* dx = w.get(m);
+    h2d(db, rhs, m);
+    h2d(dx, x, m);
+    a.prog = PROG_SMOOTH;
+    a.sm = iters;
+    a.b = db;
+    a.x = dx;
+    run_engine(s, a);
+    d2h_sync(x, dx, m);
+}
+
+// one PB V-cycle (multigrid_pb.c:270-328) with `sm` smoother iterations per half; x in place
+void mzb_mg_pb_apply(const double* rhs, double* x, int n, int sm, const double* ex, const double* ey,
+                     const double* ez, const double* k2) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    require_mg_size(n);
+    EngineArgs a = scratch_engine(s, w, n);
+    set_pb_operator(a, scratch_pb(s, w, n, ex, ey, ez, k2, true));
+    double* db = w.get(m);
+    double* dx = w.get(m);
+    h2d(db, rhs, m);
+    h2d(dx, x, m);
+    a.prog = PROG_MG_APPLY;
+    a.sm = sm;
+    a.b = db;
+    a.x = dx;
+    run_engine(s, a);
+    d2h_sync(x, dx, m);
+}
+
+// coarse coefficients of the PB V-cycle (restriction_eps, restriction_k2screen,
+// multigrid_pb.c:330-527): (n/2)^3 outputs
+void mzb_restrict_pb(const double* ex, const double* ey, const double* ez, const double* k2, double* cex,
+                     double* cey, double* cez, double* ck2, int n) {
+    System& s = sys();
+    Work w;
+    const PbGrid g = scratch_pb(s, w, n, ex, ey, ez, k2, true);
+    MZB_CHECK(cudaStreamSynchronize(s.stream));
+    const long mc = (long)(n / 2) * (n / 2) * (n / 2);
+    d2h_sync(cex, g.cex, mc);
+    d2h_sync(cey, g.cey, mc);
+    d2h_sync(cez, g.cez, mc);
+    d2h_sync(ck2, g.ck2, mc);
+}
+
+// The PB coefficients of the current grid (after solver_update_eps_k2).
+void mzb_get_pb_grids(double* ex, double* ey, double* ez, double* k2) {
+    System& s = sys();
+    GridState& G = grid();
+    if (!G.pb) fatal("mzb_get_pb_grids: the grid has no Poisson-Boltzmann coefficients");
+    MZB_CHECK(cudaStreamSynchronize(s.stream));
+    d2h_sync(ex, G.pbg.ex, G.m);
+    d2h_sync(ey, G.pbg.ey, G.m);
+    d2h_sync(ez, G.pbg.ez, G.m);
+    d2h_sync(k2, G.pbg.k2, G.m);
+}
+
 // rfft_solve with the reference's ig2 (grid_fft.c:65-125, fftw_wrap.c:166-189)
 void mzb_fft_poisson(const double* q, double* phi, int n, double L, double h) {
     System& s = sys();
@@ -1173,15 +1418,19 @@ uint64_t mzb_kernel_launches(void) { return g_kernel_launches; }
 uint64_t mzb_get_ocalls(void) { return sys().I.ocalls; }
 
 // n_steps iterations of SolverMD.md_loop_iter (maze_poisson/solver.py:483-492) with both
-// electrostatic and non-electrostatic forces; returns the last solver_update_field value.
+// electrostatic and non-electrostatic forces (and the PB coefficient update and forces on
+// a Poisson-Boltzmann grid); returns the last solver_update_field value.
 int solver_md_step(int n_steps) {
     int res = 0;
     for (int i = 0; i < n_steps; i++) {
+        const bool pb = grid().pb;
         integrator_part_1();
         solver_update_charges();
+        if (pb) solver_update_eps_k2();
         res = solver_update_field();
         solver_compute_forces_elec();
         solver_compute_forces_noel();
+        if (pb) solver_compute_forces_pb();
         solver_compute_forces_tot();
         integrator_part_2();
     }

@@ -39,6 +39,16 @@ namespace mzb {
 __host__ __device__ __forceinline__ int wrap_inc(int a, int n) { return a + 1 == n ? 0 : a + 1; }
 __host__ __device__ __forceinline__ int wrap_dec(int a, int n) { return a == 0 ? n - 1 : a - 1; }
 
+// Correctly rounded x^3: x^2 = p + e exactly, p x = hi + lo exactly, one final rounding
+// of hi + (lo + e x) (Dekker's exact product via FMA). glibc's pow(x, 3), which the
+// reference calls for cubes (cubic spline weights, the PB transition switch), returns
+// this value except in ~0.08 % of inputs where it is one ulp off.
+__device__ __forceinline__ double cube_rn(double x) {
+    const double p = x * x, e = fma(x, x, -p);
+    const double hi = p * x, lo = fma(p, x, -hi);
+    return hi + (lo + e * x);
+}
+
 // ------------------------------------------------------------------------------------
 // Warp / block reductions (fixed trees: deterministic for a given launch shape; the xor
 // butterfly leaves the identical value in every lane because IEEE addition commutes).

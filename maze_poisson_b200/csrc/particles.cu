@@ -15,16 +15,6 @@ __device__ __forceinline__ double w_cic(double x, double L, double h) {
     return 1.0 - x / h;
 }
 
-// Correctly rounded x^3: x^2 = p + e exactly, p x = hi + lo exactly, one final rounding
-// of hi + (lo + e x) (Dekker's exact product via FMA). glibc's pow(x, 3), which the
-// reference's cubic spline calls, returns this value except in ~0.08 % of inputs where
-// it is one ulp off.
-__device__ __forceinline__ double cube_rn(double x) {
-    const double p = x * x, e = fma(x, x, -p);
-    const double hi = p * x, lo = fma(p, x, -hi);
-    return hi + (lo + e * x);
-}
-
 // Assignment weight of scheme CAS with the minimum image over L (charges.c:8-38).
 template <int CAS>
 __device__ __forceinline__ double w_cas(double x, double L, double h) {
@@ -406,6 +396,11 @@ __global__ void k_total_forces(ParticleDev P) {
     double v = 0.0;
     v += 1.0 * P.fe[t];
     v += 1.0 * P.fn[t];
+    if (P.fdb) {
+        v += 1.0 * P.fdb[t];
+        v += 1.0 * P.fib[t];
+        v += 1.0 * P.fnp[t];
+    }
     P.ft[t] = v;
 }
 

@@ -54,6 +54,16 @@ struct ParticleDev {
     double* fpart = nullptr;         // [tf_split][np][3]
     double* epart = nullptr;         // [ncell * tf_split]
 
+    // Poisson-Boltzmann (solver_initialize_particles_pois_boltz, particles.c:111-127);
+    // fdb/fib/fnp are null unless it was called
+    double* radii = nullptr;         // [np] solvation radii
+    double* fdb = nullptr;           // [np][3] dielectric-boundary forces
+    double* fib = nullptr;           // [np][3] ionic-boundary forces
+    double* fnp = nullptr;           // [np][3] non-polar forces
+    double* pb_part = nullptr;       // [np][2 pb_range + 1][9] force partials
+    int pb_range = 0;                // largest floor((r_s + w)/h) + 2 (0: not sized yet)
+    double gamma_np = 0, beta_np = 0;
+
     // scalars
     double* red = nullptr;           // reduction outputs (device)
     int* flags = nullptr;            // [0] spread overflow, [1] bad cell index
@@ -69,7 +79,7 @@ void field_forces(ParticleDev& P, const double* phi, int n, double h, cudaStream
 // pair energy / 2 into red[1].
 void build_cells(ParticleDev& P, cudaStream_t s);
 void tf_forces(ParticleDev& P, cudaStream_t s);
-// fcs_tot = fcs_elec + fcs_noel (particles.c:777-795)
+// fcs_tot = fcs_elec + fcs_noel (+ fcs_db + fcs_ib + fcs_np when set; particles.c:777-795)
 void total_forces(ParticleDev& P, cudaStream_t s);
 // Kinetic energy into red[2] and momentum into red[3..5] (particles.c:798-839).
 void kinetic_and_momentum(ParticleDev& P, cudaStream_t s);
