@@ -374,7 +374,7 @@ sys.path.insert(0, {root!r})
 from maze_poisson_b200.c_api import CAPI
 import bench
 capi = CAPI({lib!r}, extensions=False)
-run = bench.make_run(capi, 0)
+run = {make_run}
 d = {fields!r}
 s = run.sys
 s.pos = np.ascontiguousarray(np.load(os.path.join(d, "pos.npy")))
@@ -384,8 +384,12 @@ maps = c.type_maps()
 c.solver_initialize()
 c.solver_initialize_grid(s.n_grid, s.L, s.h, run.tol, run.eps_s, run.eps_int, maps["method"][run.method],
                          maps["precond"][run.precond])
+if run.pb is not None:
+    c.solver_initialize_grid_pois_boltz(run.pb.w, run.pb.kbar2, int(run.pb.nonpolar))
 c.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, maps["potential"]["TF"], maps["cas"]["CIC"],
                               s.types, s.pos, s.vel, s.mass, s.charges, s.pot_params)
+if run.pb is not None:
+    c.solver_initialize_particles_pois_boltz(run.pb.gamma_np, run.pb.beta_np, run.pb.radii)
 c.solver_initialize_integrator(s.n_ions, run.dt, run.T, run.gamma, maps["integrator"][run.integrator], 0)
 run.update_charges()
 c.solver_set_field(np.load(os.path.join(d, "field.npy")))
@@ -404,7 +408,8 @@ def cpu_baseline_sample(fields_dir, steps=1):
     workload, restarted (solver_set_field / solver_set_field_prev) from the FP64 GPU
     form's state after its timed steps, as the reference's restart path does."""
     cores = os.cpu_count() or 1
-    code = CPU_SAMPLE.format(root=ROOT, lib=reference_lib(), fields=fields_dir, steps=steps)
+    code = CPU_SAMPLE.format(root=ROOT, lib=reference_lib(), fields=fields_dir, steps=steps,
+                             make_run="bench.make_run(capi, 0)")
     env = dict(os.environ, OMP_NUM_THREADS=str(cores))
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=1800)
     if r.returncode != 0:
@@ -414,6 +419,126 @@ def cpu_baseline_sample(fields_dir, steps=1):
             "sample": f"{steps} MD step(s) of nacl16000_256 (LCG, tol 1e-10, {out['iters']} CG iterations), "
                       f"restarted from the FP64 GPU state; reference C (-O3 --fast-math -mavx2, OpenMP {cores} "
                       f"threads)"}
+
+
+# Poisson-Boltzmann workload (--workload pb_solute32_128): a 32-ion Na+/Cl- solute (a
+# cluster of radius 10 A, ions >= 2.7 A apart) at the centre of a 40 A box of implicit
+# water (eps_s 78.4, eps_int 1, 0.15 M ionic strength, shell half-width 1 bohr, non-polar
+# forces on), 128^3 grid (h = 0.3125 A), Tosi-Fumi pairs, Verlet at 300 K, dt 1 fs.
+PB_WORKLOAD = dict(n_ions=32, n_grid=128, box_ang=40.0, cluster_ang=10.0, seed=11)
+PB_SOLVER = dict(tol=1e-10, integrator="VERLET", T=300.0, eps_s=78.4, eps_int=1.0, dt_fs=1.0)
+
+
+def make_pb_run(capi, method):
+    from maze_poisson_b200.md import MDRun
+    from maze_poisson_b200.systems import make_pb_system, pb_settings
+    w = PB_WORKLOAD
+    s = make_pb_system(w["n_ions"], w["n_grid"], w["box_ang"], T=PB_SOLVER["T"], seed=w["seed"],
+                       cluster_ang=w["cluster_ang"])
+    return MDRun(capi, s, method=method, pb=pb_settings(s, eps_s=PB_SOLVER["eps_s"]), **PB_SOLVER)
+
+
+def pb_cg_bytes(n, iterations):
+    """Algorithmic bytes of one PB CG solve: per iteration 8 values of the Poisson CG
+    (x, r, p read + write; Ap write + read) plus the 4 operator coefficients (ex, ey, ez,
+    dg) read once, 8 bytes each per point; set-up: b, x0, the 4 coefficients read, r and x
+    written."""
+    P = n ** 3
+    return P * 8 * (12 * iterations + 8)
+
+
+def bench_pb(args):
+    """One JSON line: GPU steps/s of the PB workload (FP64, the reference's PB algorithms)
+    with per-phase device times, the solve kernel's roofline (CG methods) and the
+    reference's C on the host cores for one step restarted from the GPU state."""
+    import numpy as np
+    import torch
+    from maze_poisson_b200.c_api import CAPI
+    os.environ.setdefault("MZB_QUIET", "1")
+    torch.cuda.set_device(0)
+    capi = CAPI()
+    run = make_pb_run(capi, args.method)
+    run.initialize()
+    stream = torch.cuda.ExternalStream(capi.mzb_get_stream(), device=0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
+    for _ in range(args.warmup):
+        capi.solver_md_step(1)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    l0 = capi.mzb_kernel_launches()
+    total_ms, solve_ms, iters = timed_steps(capi, stream, flush, args.steps)
+    launches = capi.mzb_kernel_launches() - l0
+    clk = clocks.stop()
+    # phase split: the same calls as solver_md_step, each bracketed by events
+    names = ("integrator_part_1", "solver_update_charges", "solver_update_eps_k2", "solver_update_field",
+             "solver_compute_forces_elec", "solver_compute_forces_noel", "solver_compute_forces_pb",
+             "solver_compute_forces_tot", "integrator_part_2")
+    phase = {k: 0.0 for k in names}
+    for _ in range(args.steps):
+        for k in names:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                e0.record(stream)
+            getattr(capi, k)()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            torch.cuda.synchronize()
+            phase[k] += e0.elapsed_time(e1)
+    want_cpu = not args.no_cpu_baseline and reference_lib() is not None
+    cpu = None
+    if want_cpu:
+        with tempfile.TemporaryDirectory() as d:
+            g = run.sys.n_grid
+            for name in ("field", "field_prev"):
+                a = np.empty((g, g, g))
+                getattr(capi, "get_" + name)(a)
+                np.save(os.path.join(d, f"{name}.npy"), a)
+            st = run.state(fields=False)
+            np.save(os.path.join(d, "pos.npy"), st["pos"])
+            np.save(os.path.join(d, "vel.npy"), st["vel"])
+            cores = os.cpu_count() or 1
+            code = CPU_SAMPLE.format(root=ROOT, lib=reference_lib(), fields=d, steps=1,
+                                     make_run=f"bench.make_pb_run(capi, {args.method!r})")
+            env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+            r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
+                               timeout=1800)
+            if r.returncode == 0:
+                out = json.loads(r.stdout.strip().splitlines()[-1])
+                cpu = {"value": round(1 / out["seconds"], 5), "unit": "steps/s", "cores": cores,
+                       "kind": "reference",
+                       "sample": f"1 MD step of pb_solute32_128 ({args.method}, tol 1e-10, solver returned "
+                                 f"{out['iters']}), restarted from the GPU state; reference C (-O3 --fast-math "
+                                 f"-mavx2, OpenMP {cores} threads)"}
+            else:
+                cpu = {"unavailable": (r.stderr.strip().splitlines() or ["cpu sample failed"])[-1][:200]}
+    run.finalize()
+    peak, peak_kind = load_peaks()
+    n = PB_WORKLOAD["n_grid"]
+    mean_solve = statistics.mean(solve_ms)
+    line = {
+        "metric": f"PB MD steps/s (FP64, {args.method}), 32-ion solute in implicit water, 128^3",
+        "value": round(args.steps / (total_ms / 1e3), 3), "unit": "steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 32-ion NaCl cluster, 300 K MB velocities)",
+        "config": {"workload": "pb_solute32_128", **PB_WORKLOAD, **PB_SOLVER, "method": args.method,
+                   "l2": "flushed (256 MB write) before every timed step"},
+        "phases_ms": {k: round(v / args.steps, 4) for k, v in phase.items()},
+        "solve_ms": round(mean_solve, 4), "solver_result": iters[-1],
+        "gpu_launches": int(launches), "clocks": clk,
+    }
+    if args.method in ("LCG", "MAZE-LCG") and iters[-1] > 0:
+        it = statistics.mean(iters) + 1
+        achieved = pb_cg_bytes(n, it) / (mean_solve / 1e3) / 1e9
+        line["roofline"] = {"kernel": "engine_kernel (PB CG solve)", "bound": "hbm", "achieved": round(achieved, 1),
+                            "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                            "peak_source": peak_kind, "alg_bytes_per_launch": int(pb_cg_bytes(n, it)),
+                            "cg_iterations": it, "traffic": None}
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
 
 
 def bench_reference(args):
@@ -459,8 +584,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["nacl16000_256", "pb_solute32_128"], default="nacl16000_256",
+                    help="pb_solute32_128: the Poisson-Boltzmann workload (one GPU, its own JSON line)")
+    ap.add_argument("--method", default="MAZE-LCG", help="field method of the PB workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload == "pb_solute32_128":
+        bench_pb(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
 
