@@ -26,7 +26,9 @@ int solver_md_step(int n_steps);
 /* kernel-level entry points (reference semantics on plain n^3 arrays) */
 void mzb_laplace(const double *u, double *out, int n);                     /* laplace.c:24-75 */
 int mzb_conj_grad(const double *b, const double *x0, double *x, double tol, int n,
-                  int precond);  /* plcg.c:28-90 (precond 0), plcg.c:104-166 (1 JACOBI, 2 MG) */
+                  int precond);  /* plcg.c:28-90 (precond 0), plcg.c:104-166 (1 JACOBI, 2 MG, 3 SSOR, 4 BLOCKJACOBI) */
+void mzb_ssor_apply(const double *u, double *out, int n);                  /* precond_ssor.c:1240-1252 */
+void mzb_blockjacobi_apply(const double *u, double *out, int n);    /* precond_blockjacobi.c:173-206; n % 10 == 0 */
 void mzb_smooth_rbgs(const double *rhs, double *x, int n, int iters);      /* multigrid.c:636-729 */
 void mzb_restrict27(const double *fine, double *coarse, int n);            /* multigrid.c:523-594 */
 void mzb_prolong_trilinear(const double *coarse, double *fine, int nc);    /* multigrid.c:393-463 */

@@ -96,6 +96,8 @@ EXTENSION_SYMBOLS = {
     "mzb_prolong_trilinear": (None, [_f64_any, _f64_any, _c.c_int]),
     "mzb_cg_coarse": (_c.c_int, [_f64_any, _f64_any, _c.c_int, _c.c_int, _c.c_double]),
     "mzb_mg_apply": (None, [_f64_any, _f64_any, _c.c_int, _c.c_int]),
+    "mzb_ssor_apply": (None, [_f64_any, _f64_any, _c.c_int]),
+    "mzb_blockjacobi_apply": (None, [_f64_any, _f64_any, _c.c_int]),
     "mzb_laplace_pb": (None, [_f64_any] * 6 + [_c.c_int]),
     "mzb_conj_grad_pb": (_c.c_int, [_f64_any, _f64_any, _f64_any, _c.c_double, _c.c_int] + [_f64_any] * 4),
     "mzb_smooth_pb": (None, [_f64_any, _f64_any, _c.c_int, _c.c_int] + [_f64_any] * 4),

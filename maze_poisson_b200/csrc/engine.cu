@@ -6,6 +6,7 @@
 // single sweeps are bit-identical to the reference; only the global dot products are
 // summed in a different (fixed, deterministic) order.
 #include <type_traits>
+#include <utility>
 
 #include "engine.cuh"
 
@@ -281,6 +282,111 @@ struct CgSpec {
 __device__ bool vcycle(const Team& t, const double* rhs, double* x, int n, int sm, const EngineArgs& a,
                        int& seq);
 
+// Points of the hyperplane i + j + k = s of an n^3 grid, spread over every warp.
+template <class F>
+__device__ __forceinline__ void for_hyperplane(const Team& t, int n, int s, F&& f) {
+    const int ilo = s - 2 * (n - 1) > 0 ? s - 2 * (n - 1) : 0, ihi = s < n - 1 ? s : n - 1;
+    if (ilo > ihi) return;
+    const long pairs = (long)(ihi - ilo + 1) * n;
+    for (long q = t.gw * 32 + t.lane; q < pairs; q += t.nw * 32) {
+        const int i = ilo + (int)(q / n), j = (int)(q % n), k = s - i - j;
+        if (k >= 0 && k < n) f(i, j, k);
+    }
+}
+
+// SSOR preconditioner (precond_ssor.c:1240-1252, omega = 1.75): v = r; a forward solve in
+// index order, v_c = (v_c + the neighbours of smaller flat index in the order x+1, x-1,
+// y+1, y-1, z+1, z-1) / (6/omega); v *= -6; a backward solve in reverse index order over
+// the neighbours of larger index; v *= (2-omega)/omega. Every smaller-index neighbour lies
+// on an earlier hyperplane i+j+k (the periodic x+1 neighbour of i = n-1 sits n-1 planes
+// back), so each solve is a wavefront of 3n-2 hyperplanes with a grid barrier between
+// them. The copy and the -6 scaling are folded into the solves' reads of v_c.
+__device__ bool ssor_apply(const Team& t, const double* r, double* v, int n, const EngineArgs& a) {
+    const double omega = 1.75, dc = 6.0 / omega;
+    for (int dir = 0; dir < 2; dir++) {
+        const bool fwd = dir == 0;
+        for (int h = 0; h <= 3 * (n - 1); h++) {
+            const int s = fwd ? h : 3 * (n - 1) - h;
+            for_hyperplane(t, n, s, [&](int i, int j, int k) {
+                const Nb o = neighbours(n, i, j, k);
+                double x = fwd ? r[o.c] : v[o.c] * -6.0;
+                const long nb[6] = {o.ip, o.im, o.jp, o.jm, o.kp, o.km};
+#pragma unroll
+                for (int q = 0; q < 6; q++)
+                    if (fwd ? nb[q] < o.c : nb[q] > o.c) x = x + v[nb[q]];
+                v[o.c] = x / dc;
+            });
+            if (!grid_sync(a.bar)) return false;
+        }
+    }
+    const double fin = (2 - omega) / omega;
+    for_points(t, n, [&](int i, int j, int k) {
+        const long c = ((long)i * n + j) * n + k;
+        v[c] = v[c] * fin;
+    });
+    return grid_sync(a.bar);
+}
+
+// Block-Jacobi preconditioner (precond_blockjacobi.c:173-206): the (n/10)^3 blocks as
+// rows of 1000 values in (i, j, k) order times the block inverse, C = R Ainv, the
+// reference's dgemm with every output summed over l in increasing order (linalg.c:170-181)
+// and every product rounded. A CTA computes 64 x 64 tiles of C from 8-deep slices of R
+// (gathered straight from the grid, so no reorder pass) and Ainv staged in shared memory;
+// each thread holds a 4 x 2 block of C.
+__device__ __forceinline__ long bj_point(int n, int nb, int blk, int l) {
+    const int bk = blk % nb, bj = (blk / nb) % nb, bi = blk / (nb * nb);
+    const int ii = l / 100, jj = (l / 10) % 10, kk = l % 10;
+    return ((long)(bi * kBlockJacobiB + ii) * n + (bj * kBlockJacobiB + jj)) * n + bk * kBlockJacobiB + kk;
+}
+
+__device__ bool bj_apply(const Team& t, const double* r, double* v, int n, const EngineArgs& a) {
+    constexpr int T = 64, K = 8;
+    static_assert(kThreads == 512, "the tile map assumes 512 threads");
+    __shared__ double As[K][T];
+    __shared__ double Bs[K][T];
+    const int nb = n / kBlockJacobiB, nblk = nb * nb * nb;
+    const int rt = (nblk + T - 1) / T, ct = (kBlockJacobiB3 + T - 1) / T;
+    const int tr = threadIdx.x >> 5, tc = threadIdx.x & 31;       // rows 4 tr.., cols 2 tc..
+    const int lk = threadIdx.x / T, lr = threadIdx.x % T;          // loader slot
+    for (int tile = blockIdx.x; tile < rt * ct; tile += gridDim.x) {
+        const int row0 = (tile / ct) * T, col0 = (tile % ct) * T;
+        double acc[4][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+        for (int k0 = 0; k0 < kBlockJacobiB3; k0 += K) {
+            const int blk = row0 + lr, col = col0 + lr;
+            As[lk][lr] = blk < nblk ? r[bj_point(n, nb, blk, k0 + lk)] : 0.0;
+            Bs[lk][lr] = col < kBlockJacobiB3 ? a.bj_inv[(long)(k0 + lk) * kBlockJacobiB3 + col] : 0.0;
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < K; kk++) {
+                const double b0 = Bs[kk][2 * tc], b1 = Bs[kk][2 * tc + 1];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const double av = As[kk][4 * tr + i];
+                    acc[i][0] = acc[i][0] + av * b0;
+                    acc[i][1] = acc[i][1] + av * b1;
+                }
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const int blk = row0 + 4 * tr + i, col = col0 + 2 * tc + j;
+                if (blk < nblk && col < kBlockJacobiB3) v[bj_point(n, nb, blk, col)] = acc[i][j];
+            }
+    }
+    return grid_sync(a.bar);
+}
+
+// v = M^-1 r for the explicit preconditioners of conj_grad_precond
+template <int KIND>
+__device__ bool precond_apply(const Team& t, const double* r, double* v, int n, const EngineArgs& a, int& seq) {
+    if (KIND == PC_SSOR) return ssor_apply(t, r, v, n, a);
+    if (KIND == PC_BLOCKJACOBI) return bj_apply(t, r, v, n, a);
+    return vcycle(t, r, v, n, 5, a, seq);
+}
+
 // Returns the reference's value: conj_grad* -> 0-based iteration at convergence or -1;
 // cg_coarse* -> number of iterations run. `ok` turns false on a barrier failure.
 // KIND is the PrecondKind; COARSE selects the cg_coarse variant (implicit Jacobi for the
@@ -310,7 +416,7 @@ __device__ int cg_run(const Team& t, const CgSpec& s, const OP& op, const Engine
     if (KIND == PC_IMPLICIT) rv = -acc[0];
     else if (KIND == PC_JACOBI || KIND == PC_NONE) rv = acc[0];
     else {
-        ok = vcycle(t, s.r, s.v, n, 5, a, seq);
+        ok = precond_apply<KIND>(t, s.r, s.v, n, a, seq);
         if (!ok) return -1;
         double d[1] = {0.0}, m0[1];
         for_points(t, n, [&](int i, int j, int k) {
@@ -376,7 +482,7 @@ __device__ int cg_run(const Team& t, const CgSpec& s, const OP& op, const Engine
         else if (KIND == PC_JACOBI) rnv = sums[1];
         else if (KIND == PC_NONE) rnv = sums[0];
         else {
-            ok = vcycle(t, s.r, s.v, n, 5, a, seq);
+            ok = precond_apply<KIND>(t, s.r, s.v, n, a, seq);
             if (!ok) return -1;
             double d[1] = {0.0}, m1[1];
             for_points(t, n, [&](int i, int j, int k) {
@@ -517,6 +623,8 @@ __device__ void engine_body(const Team& t, const EngineArgs& a, const OP& op, in
             if (s.coarse) result = cg_run<PC_IMPLICIT, true>(t, s, op, a, seq, ok);
             else if (s.kind == PC_JACOBI) result = cg_run<PC_JACOBI, false>(t, s, op, a, seq, ok);
             else if (s.kind == PC_MG) result = cg_run<PC_MG, false>(t, s, op, a, seq, ok);
+            else if (s.kind == PC_SSOR) result = cg_run<PC_SSOR, false>(t, s, op, a, seq, ok);
+            else if (s.kind == PC_BLOCKJACOBI) result = cg_run<PC_BLOCKJACOBI, false>(t, s, op, a, seq, ok);
             else result = cg_run<PC_IMPLICIT, false>(t, s, op, a, seq, ok);
         }
         break;
@@ -531,6 +639,14 @@ __device__ void engine_body(const Team& t, const EngineArgs& a, const OP& op, in
 
     case PROG_RESTRICT:
         restrict27(t, a.u, a.out, n);
+        break;
+
+    case PROG_SSOR:
+        ok = ssor_apply(t, a.u, a.out, n, a);
+        break;
+
+    case PROG_BLOCKJACOBI:
+        ok = bj_apply(t, a.u, a.out, n, a);
         break;
 
     case PROG_PROLONG:  // n is the coarse size here
@@ -589,6 +705,8 @@ __device__ void engine_body(const Team& t, const EngineArgs& a, const OP& op, in
             if (PB || s.kind == PC_IMPLICIT) result = cg_run<PC_IMPLICIT, false>(t, s, op, a, seq, ok);
             else if constexpr (!PB) {
                 if (s.kind == PC_JACOBI) result = cg_run<PC_JACOBI, false>(t, s, op, a, seq, ok);
+                else if (s.kind == PC_SSOR) result = cg_run<PC_SSOR, false>(t, s, op, a, seq, ok);
+                else if (s.kind == PC_BLOCKJACOBI) result = cg_run<PC_BLOCKJACOBI, false>(t, s, op, a, seq, ok);
                 else result = cg_run<PC_MG, false>(t, s, op, a, seq, ok);
             }
             if (!ok) break;
@@ -653,6 +771,54 @@ void ensure_shape() {
 }
 
 }  // namespace
+
+// Gauss-Jordan elimination with partial pivoting on the block's Laplacian (the LU-based
+// inverse LAPACK's dgetrf + dgetri give the reference, linalg.c:16-35), in plain FP64 on
+// the host; computed on first use and kept.
+const std::vector<double>& block_jacobi_inverse() {
+    static std::vector<double> inv;
+    if (!inv.empty()) return inv;
+    const int B = kBlockJacobiB, n = kBlockJacobiB3;
+    std::vector<double> m((size_t)n * n, 0.0), x((size_t)n * n, 0.0);
+    for (int i = 0; i < B; i++)
+        for (int j = 0; j < B; j++)
+            for (int k = 0; k < B; k++) {
+                const long r = (i * B + j) * B + k;
+                m[r * n + r] = -6.0;
+                if (i > 0) m[r * n + r - B * B] = 1.0;
+                if (i < B - 1) m[r * n + r + B * B] = 1.0;
+                if (j > 0) m[r * n + r - B] = 1.0;
+                if (j < B - 1) m[r * n + r + B] = 1.0;
+                if (k > 0) m[r * n + r - 1] = 1.0;
+                if (k < B - 1) m[r * n + r + 1] = 1.0;
+            }
+    for (long r = 0; r < n; r++) x[r * n + r] = 1.0;
+    for (long c = 0; c < n; c++) {
+        long piv = c;
+        for (long r = c + 1; r < n; r++)
+            if (fabs(m[r * n + c]) > fabs(m[piv * n + c])) piv = r;
+        if (piv != c)
+            for (long q = 0; q < n; q++) {
+                std::swap(m[c * n + q], m[piv * n + q]);
+                std::swap(x[c * n + q], x[piv * n + q]);
+            }
+        const double d = m[c * n + c];
+        for (long q = 0; q < n; q++) {
+            m[c * n + q] /= d;
+            x[c * n + q] /= d;
+        }
+        for (long r = 0; r < n; r++) {
+            const double f = m[r * n + c];
+            if (r == c || f == 0.0) continue;
+            for (long q = 0; q < n; q++) {
+                m[r * n + q] -= f * m[c * n + q];
+                x[r * n + q] -= f * x[c * n + q];
+            }
+        }
+    }
+    inv.swap(x);
+    return inv;
+}
 
 int engine_grid_blocks() {
     ensure_shape();

@@ -3,6 +3,8 @@
 // pays a launch or a host round trip per iteration.
 #pragma once
 
+#include <vector>
+
 #include "mzb_common.cuh"
 
 namespace mzb {
@@ -21,10 +23,17 @@ enum EngineProg : int {
     PROG_MAZE_LCG = 11,   // verlet_poisson                             verlet.c:31-71
     PROG_MG_UPDATE = 12,  // multigrid_grid_update_field                grid_multigrid.c:110-212
     PROG_MAZE_MG = 13,    // verlet_poisson_multigrid                   verlet.c:86-149
+    PROG_SSOR = 14,       // out = SSOR^-1 u                            precond_ssor.c:1240-1252
+    PROG_BLOCKJACOBI = 15,// out = block-Jacobi^-1 u                    precond_blockjacobi.c:173-206
 };
 
-// PC_NONE: unpreconditioned CG, p = -r (the PB coarse solve, multigrid_pb.c:16-97)
-enum PrecondKind : int { PC_IMPLICIT = 0, PC_JACOBI = 1, PC_MG = 2, PC_NONE = 3 };
+// The reference's preconditioner numbers (grid_general.c:16) for IMPLICIT (its NONE: the
+// implicit 1/6 scaling of conj_grad), JACOBI, MG and SSOR; PC_NONE is an unpreconditioned
+// CG, p = -r (the PB coarse solve, multigrid_pb.c:16-97).
+enum PrecondKind : int { PC_IMPLICIT = 0, PC_JACOBI = 1, PC_MG = 2, PC_SSOR = 3, PC_BLOCKJACOBI = 4, PC_NONE = 5 };
+
+// Block-Jacobi blocks: 10^3 points (precond_blockjacobi.c:10)
+constexpr int kBlockJacobiB = 10, kBlockJacobiB3 = 1000;
 
 struct EngineArgs {
     int prog;
@@ -73,6 +82,9 @@ struct EngineArgs {
     const double *ex, *ey, *ez, *dg;
     const double *cex, *cey, *cez, *cdg;
 
+    // inverse of one 10^3 block's Laplacian (1000 x 1000, row-major), PC_BLOCKJACOBI
+    const double* bj_inv;
+
     double* partials;  // 2 sets x 8 values x gridDim.x
     GridBarrier* bar;
     int* result;       // [0] program return value, [1] engine status (0 ok)
@@ -86,6 +98,9 @@ void engine_launch(const EngineArgs& a, cudaStream_t stream);
 // size or device does not allow it (the caller then uses engine_launch).
 bool cg_fast_launch(const EngineArgs& a, cudaStream_t stream);
 int cg_fast_stamp_slots();
+// The inverse of the 7-point Laplacian of one 10^3 block with Dirichlet edges
+// (precond_blockjacobi.c:14-69), row-major 1000 x 1000, computed once on the host.
+const std::vector<double>& block_jacobi_inverse();
 // Bytes of partials the engine needs and its grid size on this device.
 int engine_grid_blocks();
 

@@ -42,12 +42,31 @@ const char* kPotentialNames[3] = {"TF", "LJ", "SC"};
 const char* kCasNames[3] = {"CIC", "SPL_QUADR", "SPL_CUBIC"};
 const char* kIntegratorNames[2] = {"OVRVO", "VERLET"};
 
+// Host-to-device copies and zero fills that have landed when they return. The blocking
+// cudaMemcpy / cudaMemset run on the legacy default stream, which the library's
+// non-blocking streams do not wait for, and an upload from pageable memory may return
+// before its last DMA completes; waiting on the legacy stream orders them before any
+// kernel launched afterwards.
+void upload(void* d, const void* h, size_t bytes) {
+    if (bytes == 0) return;
+    MZB_CHECK(cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice));
+    MZB_CHECK(cudaStreamSynchronize(cudaStreamLegacy));
+}
+void zero_fill(void* d, size_t bytes) {
+    MZB_CHECK(cudaMemset(d, 0, bytes));
+    MZB_CHECK(cudaStreamSynchronize(cudaStreamLegacy));
+}
+void copy_d2d(void* d, const void* src, size_t bytes) {
+    MZB_CHECK(cudaMemcpy(d, src, bytes, cudaMemcpyDeviceToDevice));
+    MZB_CHECK(cudaStreamSynchronize(cudaStreamLegacy));
+}
+
 template <class T>
 T* dalloc(size_t count) {
     T* p = nullptr;
     if (count == 0) count = 1;
     MZB_CHECK(cudaMalloc(&p, sizeof(T) * count));
-    MZB_CHECK(cudaMemset(p, 0, sizeof(T) * count));
+    zero_fill(p, sizeof(T) * count);
     return p;
 }
 template <class T>
@@ -78,6 +97,7 @@ struct GridState {
     float* lev_b[kMixedMaxLevels] = {};
     float* lev_r[kMixedMaxLevels] = {};
     float* lev_g = nullptr;   // Green's function of the coarsest level (direct solve) or null
+    double* bj_inv = nullptr;  // block-Jacobi block inverse (1000 x 1000) on BLOCKJACOBI grids
     // Poisson-Boltzmann (solver_initialize_grid_pois_boltz, grid_general.c:84-100)
     bool pb = false;
     PbGrid pbg;
@@ -140,6 +160,7 @@ void free_grid(GridState& G) {
     dfree(G.r); dfree(G.p0); dfree(G.p1); dfree(G.Ap); dfree(G.v); dfree(G.rf); dfree(G.tmp);
     dfree(G.rc); dfree(G.ec); dfree(G.cr); dfree(G.cp0); dfree(G.cp1); dfree(G.cAp);
     G.fft.release();
+    dfree(G.bj_inv);
     dfree(G.pbg.ex); dfree(G.pbg.ey); dfree(G.pbg.ez); dfree(G.pbg.k2); dfree(G.pbg.dg);
     dfree(G.pbg.cex); dfree(G.pbg.cey); dfree(G.pbg.cez); dfree(G.pbg.ck2); dfree(G.pbg.cdg);
     G.pbg = PbGrid{};
@@ -174,14 +195,14 @@ void ensure_mixed_levels(GridState& G) {
         MZB_CHECK(cudaMalloc(&G.lev_x[l], m * sizeof(float)));
         MZB_CHECK(cudaMalloc(&G.lev_b[l], m * sizeof(float)));
         MZB_CHECK(cudaMalloc(&G.lev_r[l], m * sizeof(float)));
-        MZB_CHECK(cudaMemset(G.lev_x[l], 0, m * sizeof(float)));
+        zero_fill(G.lev_x[l], m * sizeof(float));
     }
     const int nc = G.lev_n[G.nlev - 1];
     if (nc <= kMixedDirectN && mixed_small_level(G.nlev, G.lev_n) < G.nlev) {
         std::vector<float> g((size_t)nc * nc * nc);
         mixed_coarse_green(nc, g.data());
         MZB_CHECK(cudaMalloc(&G.lev_g, g.size() * sizeof(float)));
-        MZB_CHECK(cudaMemcpy(G.lev_g, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice));
+        upload(G.lev_g, g.data(), g.size() * sizeof(float));
     }
 }
 
@@ -214,6 +235,14 @@ void set_cells(ParticleDev& P, int nc) {
     P.epart = dalloc<double>((size_t)nblk * P.tf_split);
 }
 
+// A device copy of the block-Jacobi block inverse (the caller frees it).
+double* device_block_inverse() {
+    const std::vector<double>& inv = block_jacobi_inverse();
+    double* d = dalloc<double>(inv.size());
+    upload(d, inv.data(), sizeof(double) * inv.size());
+    return d;
+}
+
 // Point the engine's PB operator at the coefficients of g.
 void set_pb_operator(EngineArgs& a, const PbGrid& g) {
     a.pb = 1;
@@ -233,6 +262,7 @@ EngineArgs engine_base(System& s) {
     a.result = s.result;
     a.q = G.q;
     a.y = G.y;
+    a.bj_inv = G.bj_inv;
     if (G.pb) set_pb_operator(a, G.pbg);
     return a;
 }
@@ -512,6 +542,10 @@ void solver_initialize_grid(int n, double L, double h, double tol, double eps, d
             G.rc = dalloc<double>(mc); G.ec = dalloc<double>(mc); G.cr = dalloc<double>(mc);
             G.cp0 = dalloc<double>(mc); G.cp1 = dalloc<double>(mc); G.cAp = dalloc<double>(mc);
         }
+        if (grid_type == G_MAZE_LCG && (precond_type == P_SSOR || precond_type == P_BLOCKJACOBI))
+            G.v = dalloc<double>(G.m);  // v = M^-1 r
+        if ((grid_type == G_LCG || grid_type == G_MAZE_LCG) && precond_type == P_BLOCKJACOBI)
+            G.bj_inv = device_block_inverse();  // precond_blockjacobi_init (grid_lcg.c:75-78)
     }
     G.ready = true;
 }
@@ -578,11 +612,11 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
     P.chg = dalloc<double>(n_p);
     P.base = dalloc<int32_t>(v3);
     if (n_p > 0) {
-        MZB_CHECK(cudaMemcpy(P.types, types, sizeof(int32_t) * n_p, cudaMemcpyHostToDevice));
-        MZB_CHECK(cudaMemcpy(P.pos, pos, sizeof(double) * v3, cudaMemcpyHostToDevice));
-        MZB_CHECK(cudaMemcpy(P.vel, vel, sizeof(double) * v3, cudaMemcpyHostToDevice));
-        MZB_CHECK(cudaMemcpy(P.mass, mass, sizeof(double) * n_p, cudaMemcpyHostToDevice));
-        MZB_CHECK(cudaMemcpy(P.chg, charges, sizeof(double) * n_p, cudaMemcpyHostToDevice));
+        upload(P.types, types, sizeof(int32_t) * n_p);
+        upload(P.pos, pos, sizeof(double) * v3);
+        upload(P.vel, vel, sizeof(double) * v3);
+        upload(P.mass, mass, sizeof(double) * n_p);
+        upload(P.chg, charges, sizeof(double) * n_p);
     }
     // pair-potential constants per type pair, 7 doubles each, with the shifted-force
     // constants at r_cut = L/2
@@ -616,7 +650,7 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
         }
     }
     P.tab = dalloc<double>(tab.size());
-    MZB_CHECK(cudaMemcpy(P.tab, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+    upload(P.tab, tab.data(), sizeof(double) * tab.size());
     // spreading tiles over the grid
     P.nti = (n + kTileI - 1) / kTileI;
     P.ntj = (n + kTileJ - 1) / kTileJ;
@@ -653,7 +687,7 @@ void solver_initialize_particles_pois_boltz(double gamma_np, double beta_np, dou
         P.fib = dalloc<double>((size_t)3 * P.np);
         P.fnp = dalloc<double>((size_t)3 * P.np);
     }
-    if (P.np > 0) MZB_CHECK(cudaMemcpy(P.radii, solv_radii, sizeof(double) * P.np, cudaMemcpyHostToDevice));
+    if (P.np > 0) upload(P.radii, solv_radii, sizeof(double) * P.np);
     s.pb_radii.assign(solv_radii, solv_radii + P.np);
     dfree(P.pb_part);
     P.pb_range = 0;
@@ -761,7 +795,16 @@ int solver_update_field(void) {
         if (G.precond == P_NONE || G.pb) a.precond = PC_IMPLICIT;  // PB ignores it (grid_maze_lcg.c:150-156)
         else if (G.precond == P_JACOBI) a.precond = PC_JACOBI;
         else if (G.precond == P_MG) a.precond = PC_MG;
-        else fatal("SSOR and BLOCKJACOBI preconditioners are not supported by this build");
+        else if (G.precond == P_SSOR) a.precond = PC_SSOR;
+        else {  // precond_blockjacobi.c:192-197
+            if (G.n % kBlockJacobiB) {
+                fprintf(stderr, "Error: The size of the input vector is not a multiple of the block size (%d)\n",
+                        kBlockJacobiB3);
+                fprintf(stderr, "Padding is not implemented yet\n");
+                exit(1);
+            }
+            a.precond = PC_BLOCKJACOBI;
+        }
         break;
     case G_MG:
         a.prog = PROG_MG_UPDATE;
@@ -1027,7 +1070,7 @@ EngineArgs scratch_engine(System& s, Work& w, int n) {
 }
 
 void h2d(double* d, const double* h, long m) {
-    MZB_CHECK(cudaMemcpy(d, h, sizeof(double) * m, cudaMemcpyHostToDevice));
+    upload(d, h, sizeof(double) * m);
 }
 void d2h_sync(double* h, const double* d, long m) {
     MZB_CHECK(cudaMemcpy(h, d, sizeof(double) * m, cudaMemcpyDeviceToHost));
@@ -1071,7 +1114,7 @@ void mzb_laplace(const double* u, double* out, int n) {
 }
 
 // conj_grad (plcg.c:28-90) and conj_grad_precond (plcg.c:104-166, precond 1 = JACOBI,
-// 2 = MG); returns the reference's return value.
+// 2 = MG, 3 = SSOR, 4 = BLOCKJACOBI); returns the reference's return value.
 int mzb_conj_grad(const double* b, const double* x0, double* x, double tol, int n, int precond) {
     System& s = sys();
     Work w;
@@ -1089,8 +1132,14 @@ int mzb_conj_grad(const double* b, const double* x0, double* x, double tol, int 
     a.b = db;
     a.x0 = dx0;
     a.x = dx;
+    double* inv = nullptr;
+    if (precond == PC_BLOCKJACOBI) {
+        if (n % kBlockJacobiB) fatal("mzb_conj_grad: block Jacobi needs n to be a multiple of 10");
+        a.bj_inv = inv = device_block_inverse();
+    }
     const int res = run_engine(s, a);
     d2h_sync(x, dx, m);
+    if (inv) cudaFree(inv);
     return res;
 }
 
@@ -1110,6 +1159,42 @@ void mzb_smooth_rbgs(const double* rhs, double* x, int n, int iters) {
     a.x = dx;
     run_engine(s, a);
     d2h_sync(x, dx, m);
+}
+
+// precond_blockjacobi_apply (precond_blockjacobi.c:173-206), n a multiple of 10
+void mzb_blockjacobi_apply(const double* u, double* out, int n) {
+    System& s = sys();
+    Work w;
+    if (n % kBlockJacobiB) fatal("mzb_blockjacobi_apply: n must be a multiple of 10");
+    const long m = (long)n * n * n;
+    EngineArgs a = scratch_engine(s, w, n);
+    double* du = w.get(m);
+    double* dout = w.get(m);
+    h2d(du, u, m);
+    double* inv = device_block_inverse();
+    a.prog = PROG_BLOCKJACOBI;
+    a.bj_inv = inv;
+    a.u = du;
+    a.out = dout;
+    run_engine(s, a);
+    d2h_sync(out, dout, m);
+    cudaFree(inv);
+}
+
+// precond_ssor_apply (precond_ssor.c:1240-1252): out = SSOR preconditioner applied to u
+void mzb_ssor_apply(const double* u, double* out, int n) {
+    System& s = sys();
+    Work w;
+    const long m = (long)n * n * n;
+    EngineArgs a = scratch_engine(s, w, n);
+    double* du = w.get(m);
+    double* dout = w.get(m);
+    h2d(du, u, m);
+    a.prog = PROG_SSOR;
+    a.u = du;
+    a.out = dout;
+    run_engine(s, a);
+    d2h_sync(out, dout, m);
 }
 
 // restriction_27pt (multigrid.c:523-594): fine n^3 -> coarse (n/2)^3
@@ -1530,14 +1615,14 @@ void batch_prepare(System& s) {
     if (!s.qtot_d) {
         s.qtot_d = dalloc<double>(1);
         s.err_d = dalloc<int>(4);
-        MZB_CHECK(cudaMemset(s.err_d, 0, 4 * sizeof(int)));
+        zero_fill(s.err_d, 4 * sizeof(int));
     }
     if (!s.I.ocalls_d) {
         s.I.ocalls_d = dalloc<uint64_t>(1);
         touch(s);
     }
-    MZB_CHECK(cudaMemcpy(s.qtot_d, &s.q_tot, sizeof(double), cudaMemcpyHostToDevice));
-    MZB_CHECK(cudaMemcpy(s.I.ocalls_d, &s.I.ocalls, sizeof(uint64_t), cudaMemcpyHostToDevice));
+    upload(s.qtot_d, &s.q_tot, sizeof(double));
+    upload(s.I.ocalls_d, &s.I.ocalls, sizeof(uint64_t));
 }
 
 // Team partition of nblocks CTAs: at least one per system, the rest in proportion to
@@ -1620,8 +1705,8 @@ BatchGraph& batch_graph(const std::vector<int>& handles, const std::vector<Syste
     bg.key = key;
     MZB_CHECK(cudaMalloc(&bg.list_d, sizeof(MixedArgs) * nsys));
     MZB_CHECK(cudaMalloc(&bg.start_d, sizeof(int) * (nsys + 1)));
-    MZB_CHECK(cudaMemcpy(bg.list_d, list.data(), sizeof(MixedArgs) * nsys, cudaMemcpyHostToDevice));
-    MZB_CHECK(cudaMemcpy(bg.start_d, start.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice));
+    upload(bg.list_d, list.data(), sizeof(MixedArgs) * nsys);
+    upload(bg.start_d, start.data(), sizeof(int) * (nsys + 1));
 
     const unsigned long long l0 = g_kernel_launches;
     cudaGraph_t graph = nullptr;
@@ -1692,7 +1777,7 @@ int batch_end(std::vector<System*>& ss, const int* handles) {
         }
         if (err[2]) status = -1;
         s.q_tot = q;
-        MZB_CHECK(cudaMemset(s.err_d, 0, 4 * sizeof(int)));
+        zero_fill(s.err_d, 4 * sizeof(int));
     }
     return status;
 }
@@ -1802,13 +1887,14 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
     int* start_d = nullptr;
     MZB_CHECK(cudaMalloc(&list_d, sizeof(MixedArgs) * nsys));
     MZB_CHECK(cudaMalloc(&start_d, sizeof(int) * (nsys + 1)));
-    MZB_CHECK(cudaMemcpy(list_d, list.data(), sizeof(MixedArgs) * nsys, cudaMemcpyHostToDevice));
+    upload(list_d, list.data(), sizeof(MixedArgs) * nsys);
     std::vector<double*> ysave(nsys, nullptr);
+    MZB_CHECK(cudaDeviceSynchronize());  // the systems' streams have written y
     for (int r = 0; r < nsys; r++) {
         const int t = ss[r]->G.type;
         if (t == G_MAZE_LCG || t == G_MAZE_MG) {
             ysave[r] = dalloc<double>(ss[r]->G.m);
-            MZB_CHECK(cudaMemcpy(ysave[r], ss[r]->G.y, sizeof(double) * ss[r]->G.m, cudaMemcpyDeviceToDevice));
+            copy_d2d(ysave[r], ss[r]->G.y, sizeof(double) * ss[r]->G.m);
         }
     }
     auto restore_y = [&]() {
@@ -1821,7 +1907,7 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
     double best_alpha = B.alpha, best_solve = 1e30;
     for (double alpha : alphas) {
         const std::vector<int> start = team_starts(ss, nblocks, alpha);
-        MZB_CHECK(cudaMemcpy(start_d, start.data(), sizeof(int) * (nsys + 1), cudaMemcpyHostToDevice));
+        upload(start_d, start.data(), sizeof(int) * (nsys + 1));
         float tot = 0.f;
         for (int rep = 0; rep < 3; rep++) {
             restore_y();

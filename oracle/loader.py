@@ -67,6 +67,9 @@ KERNELS = {
     "orc_forces_pb": (None, [_f, _f, _c.c_int, _c.c_int, _c.c_double, _c.c_double, _c.c_double,
                              _c.c_double, _c.c_double, _c.c_int, _f, _f, _f, _f, _f, _f, _f, _f]),
     "orc_get_pb_grids": (None, [_f, _f, _f, _f]),
+    "orc_ssor_apply": (None, [_f, _f, _c.c_int]),
+    "orc_blockjacobi_apply": (None, [_f, _f, _c.c_int]),
+    "orc_blockjacobi_inverse": (None, [_f]),
 }
 
 

@@ -231,14 +231,16 @@ void orc_mg_apply(const double *rhs, double *x, int n, int sm) {
 }
 
 /* ------------------------------------------------------------------------------------
- * Preconditioned CG (library/src/plcg.c:104-166) with the two explicit preconditioners
- * in scope: Jacobi, out = -in/6 (precond_jacobi.c:8-14), and one V-cycle with 5 sweeps
- * warm-started from the previous output (precond_mg.c:3-5).  The preconditioner output
- * buffer starts at zero.
+ * Preconditioned CG (library/src/plcg.c:104-166) with the explicit preconditioners:
+ * Jacobi, out = -in/6 (precond_jacobi.c:8-14), one V-cycle with 5 sweeps warm-started from
+ * the previous output (precond_mg.c:3-5), SSOR (orc_ssor_apply) and block Jacobi
+ * (orc_blockjacobi_apply).  The preconditioner output buffer starts at zero.
  * ---------------------------------------------------------------------------------- */
 static void apply_precond(int kind, const double *in, double *out, int n) {
     long m = (long)n * n * n;
     if (kind == 1) { for (long t = 0; t < m; t++) out[t] = -in[t] / 6.0; }
+    else if (kind == 3) orc_ssor_apply(in, out, n);
+    else if (kind == 4) orc_blockjacobi_apply(in, out, n);
     else orc_mg_apply(in, out, n, 5);
 }
 
@@ -269,6 +271,123 @@ static int conj_grad_precond(const double *b, const double *x0, double *x, doubl
     }
     free(r); free(Ap); free(v); free(p);
     return res;
+}
+
+/* ------------------------------------------------------------------------------------
+ * SSOR preconditioner (library/src/precond_ssor.c:1240-1252 with the edge solves of
+ * precond_ssor.c:172-957, omega = 1.75): a forward sweep in index order, each point
+ * b_c = (b_c + its neighbours of smaller flat index, taken in the order x+1, x-1, y+1,
+ * y-1, z+1, z-1) / (6 / omega); b *= -6; a backward sweep in reverse index order over the
+ * neighbours of larger index, same order and divisor; b *= (2 - omega) / omega. The
+ * periodic wrap decides which neighbours count: at i = n-1 the x+1 neighbour (i = 0) has a
+ * smaller index, at i = 0 the x-1 neighbour (i = n-1) a larger one.
+ * ---------------------------------------------------------------------------------- */
+static void ssor_sweep(double *b, int n, int forward, double dc) {
+    long m = (long)n * n * n;
+    for (long t = 0; t < m; t++) {
+        long c = forward ? t : m - 1 - t;
+        long i = c / ((long)n * n), j = (c / n) % n, k = c % n;
+        long nb[6] = {gidx(i + 1, j, k, n), gidx(i - 1, j, k, n), gidx(i, j + 1, k, n),
+                      gidx(i, j - 1, k, n), gidx(i, j, k + 1, n), gidx(i, j, k - 1, n)};
+        double v = b[c];
+        for (int q = 0; q < 6; q++)
+            if (forward ? nb[q] < c : nb[q] > c) v = v + b[nb[q]];
+        b[c] = v / dc;
+    }
+}
+
+void orc_ssor_apply(const double *in, double *out, int n) {
+    const double omega = 1.75, dc = 6.0 / omega;
+    long m = (long)n * n * n;
+    if (out != in) memcpy(out, in, m * sizeof(double));
+    ssor_sweep(out, n, 1, dc);
+    scal(out, -6.0, m);
+    ssor_sweep(out, n, 0, dc);
+    scal(out, (2 - omega) / omega, m);
+}
+
+/* ------------------------------------------------------------------------------------
+ * Block-Jacobi preconditioner (library/src/precond_blockjacobi.c): the grid is cut into
+ * 10^3 blocks; the preconditioner multiplies each block, as a row of 1000 values in
+ * (i, j, k) order, by the inverse of the 7-point Laplacian of one block with Dirichlet
+ * edges (diagonal -6, +1 to the in-block neighbours; precond_blockjacobi.c:14-69). The
+ * reference inverts that matrix with LAPACK's dgetrf + dgetri (linalg.c:16-35), which
+ * this image does not have: here it is Gauss-Jordan elimination with partial pivoting,
+ * the same LU-based inverse up to rounding (parity unpinned). The product is the
+ * reference's non-BLAS dgemm (linalg.c:170-181): every output summed serially over l.
+ * ---------------------------------------------------------------------------------- */
+#define BJ_B 10
+#define BJ_B3 (BJ_B * BJ_B * BJ_B)
+static double *bj_inv = NULL;
+
+static void bj_build(void) {
+    if (bj_inv) return;
+    int n = BJ_B3;
+    double *a = calloc((size_t)n * n, sizeof(double)), *inv = calloc((size_t)n * n, sizeof(double));
+    for (int i = 0; i < BJ_B; i++)
+        for (int j = 0; j < BJ_B; j++)
+            for (int k = 0; k < BJ_B; k++) {
+                long r = (i * BJ_B + j) * BJ_B + k;
+                a[r * n + r] = -6.0;
+                if (i > 0) a[r * n + r - BJ_B * BJ_B] = 1.0;
+                if (i < BJ_B - 1) a[r * n + r + BJ_B * BJ_B] = 1.0;
+                if (j > 0) a[r * n + r - BJ_B] = 1.0;
+                if (j < BJ_B - 1) a[r * n + r + BJ_B] = 1.0;
+                if (k > 0) a[r * n + r - 1] = 1.0;
+                if (k < BJ_B - 1) a[r * n + r + 1] = 1.0;
+            }
+    for (long r = 0; r < n; r++) inv[r * n + r] = 1.0;
+    for (long c = 0; c < n; c++) {
+        long piv = c;
+        for (long r = c + 1; r < n; r++)
+            if (fabs(a[r * n + c]) > fabs(a[piv * n + c])) piv = r;
+        if (piv != c)
+            for (long q = 0; q < n; q++) {
+                double t = a[c * n + q]; a[c * n + q] = a[piv * n + q]; a[piv * n + q] = t;
+                t = inv[c * n + q]; inv[c * n + q] = inv[piv * n + q]; inv[piv * n + q] = t;
+            }
+        double d = a[c * n + c];
+        for (long q = 0; q < n; q++) { a[c * n + q] /= d; inv[c * n + q] /= d; }
+        for (long r = 0; r < n; r++) {
+            double f = a[r * n + c];
+            if (r == c || f == 0.0) continue;
+            for (long q = 0; q < n; q++) {
+                a[r * n + q] -= f * a[c * n + q];
+                inv[r * n + q] -= f * inv[c * n + q];
+            }
+        }
+    }
+    free(a);
+    bj_inv = inv;
+}
+
+/* precond_blockjacobi_apply (precond_blockjacobi.c:173-206): n a multiple of 10 */
+void orc_blockjacobi_apply(const double *in, double *out, int n) {
+    if (n % BJ_B) {
+        fprintf(stderr, "Error: The size of the input vector is not a multiple of the block size (1000)\n");
+        exit(1);
+    }
+    bj_build();
+    int nb = n / BJ_B;
+    double *row = malloc(BJ_B3 * sizeof(double));
+    for (long bi = 0; bi < nb; bi++)
+        for (long bj = 0; bj < nb; bj++)
+            for (long bk = 0; bk < nb; bk++) {
+                for (int l = 0; l < BJ_B3; l++)
+                    row[l] = in[((bi * BJ_B + l / 100) * n + bj * BJ_B + (l / 10) % 10) * n + bk * BJ_B + l % 10];
+                for (int p = 0; p < BJ_B3; p++) {
+                    double c = 0.0;
+                    for (int l = 0; l < BJ_B3; l++) c += row[l] * bj_inv[(long)l * BJ_B3 + p];
+                    out[((bi * BJ_B + p / 100) * n + bj * BJ_B + (p / 10) % 10) * n + bk * BJ_B + p % 10] = c;
+                }
+            }
+    free(row);
+}
+
+/* the block inverse itself (1000 x 1000, row-major), for the tests */
+void orc_blockjacobi_inverse(double *out) {
+    bj_build();
+    memcpy(out, bj_inv, (size_t)BJ_B3 * BJ_B3 * sizeof(double));
 }
 
 /* ------------------------------------------------------------------------------------
@@ -948,7 +1067,7 @@ void orc_cell_list(const double *pos, int np, double L, int nc, int32_t *start, 
  * Facade (library/src/solver_md.c) over one global system.
  * ---------------------------------------------------------------------------------- */
 enum { G_LCG = 0, G_FFT = 1, G_MG = 2, G_MAZE_LCG = 3, G_MAZE_MG = 4 };
-enum { P_NONE = 0, P_JACOBI = 1, P_MG = 2 };
+enum { P_NONE = 0, P_JACOBI = 1, P_MG = 2, P_SSOR = 3, P_BLOCKJACOBI = 4 };
 
 static struct {
     int type, precond, n;
@@ -986,7 +1105,7 @@ void solver_initialize_grid(int n, double L, double h, double tol, double eps_s,
                             int grid_type, int precond_type) {
     if (grid_type == G_FFT) die("FFT is restated in numpy (oracle/fft_oracle.py)");
     if (grid_type < 0 || grid_type > 4) die("bad grid type");
-    if (precond_type > P_MG) die("SSOR / BLOCKJACOBI are outside the oracle");
+    if (precond_type < 0 || precond_type > P_BLOCKJACOBI) die("bad preconditioner type");
     G.type = grid_type; G.precond = precond_type; G.n = n;
     G.L = L; G.h = h; G.tol = tol; G.eps_s = eps_s; G.eps_int = eps_int;
     G.m = (long)n * n * n;

@@ -31,6 +31,10 @@ void orc_prolong_trilinear(const double *coarse, double *fine, int nc);        /
 int orc_cg_coarse(const double *b, double *x, int n, int maxit, double rtol);  /* multigrid.c:13-96 */
 void orc_mg_apply(const double *rhs, double *x, int n, int sm);                /* multigrid.c:99-168,743 */
 
+void orc_ssor_apply(const double *in, double *out, int n);                      /* precond_ssor.c:1240-1252 */
+void orc_blockjacobi_apply(const double *in, double *out, int n);          /* precond_blockjacobi.c:173-206 */
+void orc_blockjacobi_inverse(double *out);                                  /* precond_blockjacobi.c:14-69 */
+
 /* Poisson-Boltzmann kernels on n^3 arrays: ex/ey/ez are the +x/+y/+z face dielectric
    coefficients of each point, k2 its screening term */
 void orc_update_eps_k2(const double *pos, const double *radii, int np, int n, double h, double w,

@@ -122,6 +122,7 @@ SCENARIOS = {
     "maze_lcg": (2, 16, "MAZE-LCG", "NONE", 1e-10, "VERLET", False, 5),
     "maze_lcg_jacobi": (2, 16, "MAZE-LCG", "JACOBI", 1e-10, "VERLET", False, 3),
     "maze_lcg_mg": (2, 32, "MAZE-LCG", "MG", 1e-9, "VERLET", False, 2),
+    "maze_lcg_ssor": (2, 16, "MAZE-LCG", "SSOR", 1e-10, "VERLET", False, 3),
     "multigrid": (2, 32, "MULTIGRID", "NONE", 1e-8, "VERLET", False, 3),
     "maze_multigrid": (2, 32, "MAZE-MULTIGRID", "NONE", 1e-8, "VERLET", False, 3),
     "ovrvo_nothermo": (2, 16, "LCG", "NONE", 1e-10, "OVRVO", False, 5),
@@ -163,6 +164,20 @@ def scenario(ref_path, name, spec):
         rec[f"s{s}_field_sample"] = st["field"].reshape(-1)[::101].copy()
     run.finalize()
     return rec
+
+
+def ssor_kernel_cases(ref):
+    """precond_ssor_apply (precond_ssor.c:1240-1252) on seeded inputs, n = 2..9, 16."""
+    P = ctypes.c_void_p
+    ref.precond_ssor_apply.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    rng = np.random.default_rng(2024)
+    out = {}
+    for n in (2, 3, 4, 5, 6, 7, 8, 9, 16):
+        x = rng.standard_normal((n, n, n))
+        y = np.empty_like(x)
+        ref.precond_ssor_apply(x.ctypes.data, y.ctypes.data, n, n, 0)
+        out[f"n{n}_in"], out[f"n{n}_out"] = x, y
+    return out
 
 
 def pb_inputs(n, seed):
@@ -305,6 +320,9 @@ def main():
         ref = ctypes.CDLL(loader.REF_SO, mode=ctypes.RTLD_LOCAL)
         data = kernel_cases(ref)
         np.savez_compressed(os.path.join(OUT, "kernels.npz"), **data)
+    if only is None or "ssor_kernels" in only:
+        ref = ctypes.CDLL(loader.REF_SO, mode=ctypes.RTLD_LOCAL)
+        np.savez_compressed(os.path.join(OUT, "ssor_kernels.npz"), **ssor_kernel_cases(ref))
     for name, spec in SCENARIOS.items():
         if only is not None and name not in only:
             continue

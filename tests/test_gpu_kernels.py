@@ -144,3 +144,66 @@ def test_fft_poisson_vs_numpy(lib, n):
     lib.mzb_fft_poisson(q, phi, n, L, L / n)
     ref = fft_poisson(q, L, L / n)
     assert rel(phi, ref) < 1e-12
+
+
+def test_ssor_golden_bitexact(lib):
+    """The SSOR preconditioner's two wavefront solves equal the reference's serial ones."""
+    g = np.load(os.path.join(GOLDEN, "ssor_kernels.npz"))
+    for n in (2, 3, 4, 5, 6, 7, 8, 9, 16):
+        x = np.ascontiguousarray(g[f"n{n}_in"])
+        y = np.empty_like(x)
+        lib.mzb_ssor_apply(x, y, n)
+        assert np.array_equal(y, g[f"n{n}_out"]), n
+
+
+@pytest.mark.parametrize("n", [31, 64])
+def test_ssor_bitexact_vs_oracle(lib, oracle_lib, n):
+    x = np.random.default_rng(n).standard_normal((n, n, n))
+    a, b = np.empty_like(x), np.empty_like(x)
+    lib.mzb_ssor_apply(x, a, n)
+    oracle_lib.orc_ssor_apply(x, b, n)
+    assert np.array_equal(a, b)
+
+
+def test_conj_grad_ssor(lib, oracle_lib):
+    """conj_grad_precond with SSOR (plcg.c:104-166): fewer iterations than the implicit
+    Jacobi CG, converged to the absolute tolerance."""
+    n = 32
+    rng = np.random.default_rng(3)
+    xt = rng.standard_normal((n, n, n))
+    b = np.empty_like(xt)
+    oracle_lib.orc_laplace(xt, b, n)
+    x, x0 = np.empty_like(b), np.zeros_like(b)
+    it = lib.mzb_conj_grad(b, x0, x, 1e-9, n, 3)
+    it0 = lib.mzb_conj_grad(b, x0, np.empty_like(b), 1e-9, n, 0)
+    assert 0 < it < it0
+    lx = np.empty_like(x)
+    oracle_lib.orc_laplace(x, lx, n)
+    assert np.max(np.abs(lx - b)) <= 1e-9
+
+
+@pytest.mark.parametrize("n", [10, 20, 40])
+def test_blockjacobi_bitexact_vs_oracle(lib, oracle_lib, n):
+    """The block-Jacobi product (precond_blockjacobi.c:173-206) with the same block inverse
+    (Gauss-Jordan on the host, as the oracle computes it) and the reference's serial
+    summation order is bit-exact; the oracle's inverse agrees with LAPACK's (numpy) to
+    ~4e-15 relative (tests/test_oracle_pin.py)."""
+    x = np.random.default_rng(n).standard_normal((n, n, n))
+    a, b = np.empty_like(x), np.empty_like(x)
+    lib.mzb_blockjacobi_apply(x, a, n)
+    oracle_lib.orc_blockjacobi_apply(x, b, n)
+    assert np.array_equal(a, b)
+
+
+def test_conj_grad_blockjacobi(lib, oracle_lib):
+    n = 20
+    rng = np.random.default_rng(4)
+    xt = rng.standard_normal((n, n, n))
+    b = np.empty_like(xt)
+    oracle_lib.orc_laplace(xt, b, n)
+    x, x0 = np.empty_like(b), np.zeros_like(b)
+    it = lib.mzb_conj_grad(b, x0, x, 1e-9, n, 4)
+    assert it > 0
+    lx = np.empty_like(x)
+    oracle_lib.orc_laplace(x, lx, n)
+    assert np.max(np.abs(lx - b)) <= 1e-9

@@ -324,3 +324,12 @@ def test_spline_md_250(prod, orc, cas):
 def test_pair_potentials_250(prod, orc, pot):
     """Lennard-Jones and soft-core pair forces (forces.c:199-337) through MD steps."""
     run_pair(prod, orc, pair_system(5, 64, pot, seed=17), 4, method="LCG", tol=1e-7, pot=pot)
+
+
+def test_maze_lcg_ssor_250(prod, orc):
+    run_pair(prod, orc, make_system(5, 64, seed=3), 3, method="MAZE-LCG", precond="SSOR", tol=1e-9)
+
+
+def test_maze_lcg_blockjacobi_250(prod, orc):
+    """MAZE-LCG with the block-Jacobi preconditioner (grid 40^3, a multiple of the block)."""
+    run_pair(prod, orc, make_system(5, 40, seed=4), 3, method="MAZE-LCG", precond="BLOCKJACOBI", tol=1e-9)

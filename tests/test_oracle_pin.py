@@ -66,6 +66,15 @@ def test_vcycle_bitexact(oracle_lib, K):
     assert sha(x) == str(K["mg_x_sha"])
 
 
+def test_ssor_bitexact(oracle_lib):
+    g = np.load(os.path.join(GOLDEN, "ssor_kernels.npz"))
+    for n in (2, 3, 4, 5, 6, 7, 8, 9, 16):
+        x = np.ascontiguousarray(g[f"n{n}_in"])
+        y = np.empty_like(x)
+        oracle_lib.orc_ssor_apply(x, y, n)
+        assert np.array_equal(y, g[f"n{n}_out"]), n
+
+
 SCEN = json.load(open(os.path.join(GOLDEN, "scenarios.json")))
 
 
@@ -201,3 +210,32 @@ def test_pb_md_scenario_bitexact(oracle_path, name):
             assert sha(st["field"]) == str(g[f"{tag}_field_sha"]), tag
     finally:
         run.finalize()
+
+
+def test_blockjacobi_inverse_matches_lapack(oracle_lib):
+    """Block-Jacobi parity is unpinned: the reference inverts its block with LAPACK's
+    dgetri, which this image lacks, so its block-Jacobi path cannot run here. The oracle's
+    Gauss-Jordan inverse is checked against LAPACK's (numpy) instead, and its product
+    against a numpy restatement of the reorder + dgemm (precond_blockjacobi.c:79-206)."""
+    B = 10
+    A = np.zeros((1000, 1000))
+    for i in range(B):
+        for j in range(B):
+            for k in range(B):
+                r = (i * B + j) * B + k
+                A[r, r] = -6.0
+                for di, dj, dk in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+                    ii, jj, kk = i + di, j + dj, k + dk
+                    if 0 <= ii < B and 0 <= jj < B and 0 <= kk < B:
+                        A[r, (ii * B + jj) * B + kk] = 1.0
+    inv = np.empty((1000, 1000))
+    oracle_lib.orc_blockjacobi_inverse(inv)
+    ref = np.linalg.inv(A)
+    assert np.max(np.abs(inv - ref)) <= 1e-14 * np.max(np.abs(ref))
+    n = 20
+    x = np.random.default_rng(1).standard_normal((n, n, n))
+    y = np.empty_like(x)
+    oracle_lib.orc_blockjacobi_apply(x, y, n)
+    blocks = x.reshape(2, 10, 2, 10, 2, 10).transpose(0, 2, 4, 1, 3, 5).reshape(8, 1000)
+    yy = (blocks @ ref).reshape(2, 2, 2, 10, 10, 10).transpose(0, 3, 1, 4, 2, 5).reshape(n, n, n)
+    assert np.max(np.abs(y - yy)) <= 1e-13 * np.max(np.abs(yy))
