@@ -98,9 +98,9 @@ int mzb_system_destroy(int handle);
    counterpart in the reference. */
 int mzb_batch_step(const int *handles, int nsys, int n_steps);
 
-/* Time candidate team partitions of the batched field solve and warp targets of the pair
-   forces on the listed systems and keep the fastest; out[0..3] = {partition exponent,
-   warps, solve ms, forces ms}. Leaves the systems' state unchanged. */
+/* Time candidate team partitions of the batched field solve on the listed systems and keep
+   the fastest, and time their pair forces; out[0..3] = {partition exponent, pair-force
+   CTAs, solve ms, forces ms}. Leaves the systems' state unchanged. */
 int mzb_batch_autotune(const int *handles, int nsys, double *out);
 
 /* Device bytes one FP32+refine system with an n^3 grid and n_p ions holds (admission

@@ -213,26 +213,20 @@ void free_particles(ParticleDev& P) {
     dfree(P.cell_of); dfree(P.cell_count); dfree(P.cell_start); dfree(P.cell_fill);
     dfree(P.cell_ions); dfree(P.srank); dfree(P.spos); dfree(P.stype); dfree(P.fpart);
     dfree(P.epart); dfree(P.red); dfree(P.flags); dfree(P.partial);
+    dfree(P.tf_st); dfree(P.tf_gstart); dfree(P.tf_gent); dfree(P.tf_box);
     dfree(P.radii); dfree(P.fdb); dfree(P.fib); dfree(P.fnp); dfree(P.pb_part);
     P = ParticleDev{};
 }
 
-// Linked-cell geometry for the Tosi-Fumi kernel: about 16 ions per cell, at least one
-// cell per side; the warps (one per 32 ions in cell order) split the partner cells so
-// that ~P.tf_warps (default 12k) warps are in flight.
+// Linked cells that order the ions for the pair-force kernel: about 16 ions per cell, at
+// least one cell per side.
 void set_cells(ParticleDev& P, int nc) {
-    dfree(P.cell_count); dfree(P.cell_start); dfree(P.cell_fill); dfree(P.fpart); dfree(P.epart);
+    dfree(P.cell_count); dfree(P.cell_start); dfree(P.cell_fill);
     P.nc = nc < 1 ? 1 : nc;
     P.ncell = P.nc * P.nc * P.nc;
-    const int nblk = (P.np + 31) / 32 > 0 ? (P.np + 31) / 32 : 1;
-    const int target = P.tf_warps > 0 ? P.tf_warps : 12000;
-    int split = (target + nblk - 1) / nblk;
-    P.tf_split = split < 1 ? 1 : (split > P.ncell ? P.ncell : split);
     P.cell_count = dalloc<int32_t>(P.ncell);
     P.cell_start = dalloc<int32_t>(P.ncell + 1);
     P.cell_fill = dalloc<int32_t>(P.ncell);
-    P.fpart = dalloc<double>((size_t)P.tf_split * P.np * 3);
-    P.epart = dalloc<double>((size_t)nblk * P.tf_split);
 }
 
 // A device copy of the block-Jacobi block inverse (the caller frees it).
@@ -668,6 +662,7 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
     P.stype = dalloc<int32_t>(n_p);
     const int nc = (int)std::lround(std::cbrt(n_p / 16.0));
     set_cells(P, nc < 1 ? 1 : nc);
+    tf_plan(P);
     P.red = dalloc<double>(16);
     P.flags = dalloc<int>(4);
     P.partial = dalloc<double>((size_t)4 * ((n_p + 127) / 128) + 64);
@@ -1933,14 +1928,11 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
     cudaFree(start_d);
     B.alpha = best_alpha;
 
-    const int targets[] = {2000, 4000, 8000, 12000, 24000};
-    int best_target = 12000;
-    double best_forces = 1e30;
-    for (int target : targets) {
-        for (System* s : ss) {
-            s->P.tf_warps = target;
-            set_cells(s->P, s->P.nc);
-        }
+    // pair forces of all systems together (their work division is fixed by N; timed only)
+    double best_forces = 0.0;
+    long force_ctas = 0;
+    for (System* s : ss) force_ctas += s->P.tf_nst;
+    {
         float tot = 0.f;
         for (int rep = 0; rep < 3; rep++) {
             MZB_CHECK(cudaEventRecord(B.t0, B.stream));
@@ -1958,20 +1950,13 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
             MZB_CHECK(cudaEventElapsedTime(&ms, B.t0, B.t1));
             if (rep > 0) tot += ms;
         }
-        if (tot / 2 < best_forces) {
-            best_forces = tot / 2;
-            best_target = target;
-        }
+        best_forces = tot / 2;
     }
-    for (System* s : ss) {
-        s->P.tf_warps = best_target;
-        set_cells(s->P, s->P.nc);
-        touch(*s);
-    }
+    for (System* s : ss) touch(*s);
     batch_clear_graphs();
     if (out) {
         out[0] = best_alpha;
-        out[1] = best_target;
+        out[1] = (double)force_ctas;
         out[2] = best_solve;
         out[3] = best_forces;
     }
@@ -1989,8 +1974,9 @@ double mzb_system_footprint(int n, int n_p) {
     for (int l = 0; l < L; l++) levels += 3.0 * 4.0 * (double)sizes[l] * sizes[l] * sizes[l];
     const double grid = 8.0 * m * 10.0;  // q, phi x3, y, r, p0, p1, Ap, tmp
     const int nblk = (n_p + 31) / 32 > 0 ? (n_p + 31) / 32 : 1;
-    const double split = std::min(12000.0 / nblk + 1.0, 4096.0);
-    const double parts = (double)n_p * (8.0 * 3 * 7 + 4.0 * 8) + split * n_p * 3 * 8.0;
+    const double nsb = std::ceil(nblk / 8.0);
+    const double super_tiles = nsb * (std::floor(nsb / 2.0) + 1.0);  // pair-force CTAs
+    const double parts = (double)n_p * (8.0 * 3 * 7 + 4.0 * 8) + super_tiles * 2 * 8 * 32 * 3 * 8.0;
     return grid + levels + parts + 64.0 * 1024 * 1024;
 }
 

@@ -49,10 +49,14 @@ struct ParticleDev {
     int32_t* srank = nullptr;        // [np] position of ion p in cell order
     double* spos = nullptr;          // [np][3] positions in cell order
     int32_t* stype = nullptr;        // [np]
-    int tf_split = 1;                // partner-cell chunks per block of 32 ions
-    int tf_warps = 0;                // warps the split aims at (0: 12000)
-    double* fpart = nullptr;         // [tf_split][np][3]
-    double* epart = nullptr;         // [ncell * tf_split]
+    // pair-force plan (tf_forces.cu): super-tiles of 8 x 8 blocks of 32 cell-ordered ions
+    int tf_nst = 0;                  // super-tiles (CTAs of the pair-force kernel)
+    int* tf_st = nullptr;            // [tf_nst][2] (I super-block, J super-block)
+    int* tf_gstart = nullptr;        // [nblk + 1] gather-list offsets per block
+    int* tf_gent = nullptr;          // gather entries (super-tile << 4 | side << 3 | slot)
+    double* tf_box = nullptr;        // [nblk][6] bounding boxes of the blocks
+    double* fpart = nullptr;         // [tf_nst][2][8][32][3] force partials
+    double* epart = nullptr;         // [tf_nst] energy partials
 
     // Poisson-Boltzmann (solver_initialize_particles_pois_boltz, particles.c:111-127);
     // fdb/fib/fnp are null unless it was called
@@ -78,6 +82,8 @@ void field_forces(ParticleDev& P, const double* phi, int n, double h, cudaStream
 // Linked cells (counting sort, stable by ion index) + Tosi-Fumi forces into P.fn;
 // pair energy / 2 into red[1].
 void build_cells(ParticleDev& P, cudaStream_t s);
+// Super-tile list, gather lists and partial buffers of the pair-force kernel for P.np.
+void tf_plan(ParticleDev& P);
 void tf_forces(ParticleDev& P, cudaStream_t s);
 // fcs_tot = fcs_elec + fcs_noel (+ fcs_db + fcs_ib + fcs_np when set; particles.c:777-795)
 void total_forces(ParticleDev& P, cudaStream_t s);

@@ -1,26 +1,41 @@
 // Shifted-force pair forces -- Tosi-Fumi (Born-Mayer-Huggins), Lennard-Jones and soft-core
-// repulsion -- warp per 32 cell-sorted ions (reference: library/src/forces.c:112-337,
-// parameters particles.c:181-295). Every potential is summed over both orders of each
-// pair and the energy halved, which for the soft-core potential equals the reference's
-// sum over i < j with Newton's third law.
+// repulsion (reference: library/src/forces.c:112-337, parameters particles.c:181-295). The
+// reference sums every potential over both orders of each pair and halves the energy;
+// here each pair inside r_cut = L/2 is evaluated once and its force applied to both ions
+// with opposite signs (for the soft-core potential this is the reference's own i < j
+// loop with Newton's third law).
 //
 // Compiled with --fmad=true: this kernel is bound by the FP64 pipe, and its results are
 // already ulp-level (exp and inverse powers) rather than bit-level equal to the
 // reference, which uses glibc exp/pow.
 //
-// Layout: ions are sorted by cell (linked cells, particles.cu). Warp w takes the 32
-// consecutive ions of block w / split in that order (every lane holds an ion) and the
-// w % split-th contiguous chunk of partner cells; partner ions are broadcast loads.
-// Partner cells whose minimum-image distance to the bounding box of the warp's ions
-// exceeds r_cut = L/2 are skipped (with a 1e-9 relative margin), which removes ~40% of
-// the N^2 pair work; pruning is turned off when any coordinate lies outside [0, L).
-// 1/r comes from one FP64 rsqrt and r = r2 (1/r); the cutoff is tested on r^2. Partial
-// forces per chunk are summed in chunk order.
+// Layout. Ions are sorted by linked cell (particles.cu), cut into blocks of 32 and the
+// blocks into super-blocks of 8 (256 ions). A CTA of 8 warps takes one super-block pair
+// (SI, SJ) of a half shell (SJ = SI + d, d = 0 .. nsb/2, the middle distance only once):
+// warp w owns block I = 8 SI + w -- one ion per lane, its forces in registers -- and
+// walks the J blocks of SJ; in step s lane l pairs its ion with ion (l + s) mod 32 of the
+// J block, so the 32 lanes touch 32 distinct J ions and add the reactions into a
+// warp-private shared array without atomics. On the diagonal super-tile each unordered
+// block pair is taken once (and each pair inside a block once). A tile whose bounding
+// boxes are farther apart than r_cut (minimum image, 1e-9 relative margin) is skipped;
+// pruning is off when a coordinate lies outside [0, L).
+//
+// Determinism. Registers and warp arrays accumulate in step order; the warps' J partials
+// are summed in warp order; each ion's force is the sum of its super-tile partials in a
+// fixed order (k_tf_gather over a host-built list), the energy the sum of the CTAs'
+// energies in CTA order.
+#include <algorithm>
+#include <vector>
+
 #include "particles.cuh"
 
 namespace mzb {
 
-constexpr int kTfWarps = 4;
+constexpr int kTfSb = 8;                  // blocks of 32 ions per super-block
+constexpr int kTfThreads = kTfSb * 32;    // one warp per I block of a super-block
+constexpr int kTfTab = 64 * 7;            // pair-constant table (up to 8 types)
+constexpr size_t kTfSmem =
+    sizeof(double) * (kTfTab + 2 * kTfSb * 32 * 4 + kTfSb * kTfSb * 32 * 3);
 
 // min-image gap along one axis between the interval [lo, hi] and the cell [c0, c0 + cl]
 __device__ __forceinline__ double axis_gap(double lo, double hi, double c0, double cl, double L) {
@@ -62,87 +77,144 @@ __device__ __forceinline__ void pair_terms(const double* t, double r2, double ir
     }
 }
 
-template <int POT>
-__global__ void __launch_bounds__(kTfWarps * 32) k_tf(ParticleDev P) {
-    __shared__ double tab[64 * 7];
-    for (int x = threadIdx.x; x < P.ntyp * P.ntyp * 7; x += blockDim.x) tab[x] = P.tab[x];
-    __syncthreads();
+// Bounding box of each block of 32 cell-ordered ions: [lo x, lo y, lo z, hi x, hi y, hi z].
+__global__ void k_tf_boxes(ParticleDev P) {
     const int lane = threadIdx.x & 31;
-    const long gw = (long)blockIdx.x * kTfWarps + (threadIdx.x >> 5);
+    const int b = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
     const int nblk = (P.np + 31) / 32;
-    const long total = (long)nblk * P.tf_split;
-    if (gw >= total) return;
-    const int blk = (int)(gw / P.tf_split), chunk = (int)(gw % P.tf_split);
-    const int cj0 = (int)((long)chunk * P.ncell / P.tf_split);
-    const int cj1 = (int)((long)(chunk + 1) * P.ncell / P.tf_split);
-    const int nc = P.nc;
-    const double L = P.L, invL = 1.0 / L, rcut = P.rcut;
-    const double cl = L / nc;
-    const double prune2 = rcut * rcut * (1.0 + 1e-9);
-    const double rc2 = rcut * rcut;
-    const bool prune = P.flags[1] == 0;
-    const int ntyp = P.ntyp;
-
-    const int si = blk * 32 + lane;
-    const bool valid = si < P.np;
-    const int sl = valid ? si : blk * 32;  // invalid lanes mirror lane 0 for the bounding box
-    const double xi = P.spos[3 * sl], yi = P.spos[3 * sl + 1], zi = P.spos[3 * sl + 2];
-    const int ti = P.stype[sl];
-    double lx = xi, hx = xi, ly = yi, hy = yi, lz = zi, hz = zi;
+    if (b >= nblk) return;
+    const int s = b * 32 + lane < P.np ? b * 32 + lane : b * 32;  // idle lanes mirror lane 0
+    double lo[3], hi[3];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        lx = fmin(lx, __shfl_xor_sync(0xffffffffu, lx, o));
-        hx = fmax(hx, __shfl_xor_sync(0xffffffffu, hx, o));
-        ly = fmin(ly, __shfl_xor_sync(0xffffffffu, ly, o));
-        hy = fmax(hy, __shfl_xor_sync(0xffffffffu, hy, o));
-        lz = fmin(lz, __shfl_xor_sync(0xffffffffu, lz, o));
-        hz = fmax(hz, __shfl_xor_sync(0xffffffffu, hz, o));
+    for (int d = 0; d < 3; d++) lo[d] = hi[d] = P.spos[3 * s + d];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+            hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+        }
+    if (lane < 3) {
+        P.tf_box[6 * b + lane] = lo[lane];
+        P.tf_box[6 * b + 3 + lane] = hi[lane];
     }
+}
+
+template <int POT>
+__global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
+    extern __shared__ double sm[];
+    double* tab = sm;                              // [64 * 7]
+    double* ipos = tab + kTfTab;                   // [256][4]: x, y, z, type
+    double* jpos = ipos + kTfSb * 32 * 4;          // [256][4]
+    double* fjw = jpos + kTfSb * 32 * 4;           // [8 warps][8 J blocks][32][3]
+    const int st = blockIdx.x;
+    const int SI = P.tf_st[2 * st], SJ = P.tf_st[2 * st + 1];
+    const bool diag = SI == SJ;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int np = P.np, nblk = (np + 31) / 32, ntyp = P.ntyp;
+    const double L = P.L, invL = 1.0 / L, rc2 = P.rcut * P.rcut;
+    const double prune2 = rc2 * (1.0 + 1e-9);
+    const bool prune = P.flags[1] == 0;
+
+    for (int x = threadIdx.x; x < ntyp * ntyp * 7; x += blockDim.x) tab[x] = P.tab[x];
+    for (int q = threadIdx.x; q < kTfSb * 32; q += blockDim.x) {
+        const int gi = SI * kTfSb * 32 + q, gj = SJ * kTfSb * 32 + q;
+        const bool vi = gi < np, vj = gj < np;
+        ipos[4 * q] = vi ? P.spos[3 * gi] : 0.0;
+        ipos[4 * q + 1] = vi ? P.spos[3 * gi + 1] : 0.0;
+        ipos[4 * q + 2] = vi ? P.spos[3 * gi + 2] : 0.0;
+        ipos[4 * q + 3] = vi ? (double)P.stype[gi] : -1.0;
+        jpos[4 * q] = vj ? P.spos[3 * gj] : 0.0;
+        jpos[4 * q + 1] = vj ? P.spos[3 * gj + 1] : 0.0;
+        jpos[4 * q + 2] = vj ? P.spos[3 * gj + 2] : 0.0;
+        jpos[4 * q + 3] = vj ? (double)P.stype[gj] : -1.0;
+    }
+    for (int x = threadIdx.x; x < kTfSb * kTfSb * 32 * 3; x += blockDim.x) fjw[x] = 0.0;
+    __syncthreads();
+
     double fx = 0.0, fy = 0.0, fz = 0.0, e_acc = 0.0;
-    for (int cj = cj0; cj < cj1; cj++) {
-        if (prune) {
-            const int cjx = cj / (nc * nc), cjy = (cj / nc) % nc, cjz = cj % nc;
-            const double gx = axis_gap(lx, hx, cjx * cl, cl, L), gy = axis_gap(ly, hy, cjy * cl, cl, L);
-            const double gz = axis_gap(lz, hz, cjz * cl, cl, L);
-            if (gx * gx + gy * gy + gz * gz > prune2) continue;
-        }
-        const int jb = P.cell_start[cj], je = P.cell_start[cj + 1];
-        for (int sj = jb; sj < je; sj++) {
-            const double xj = P.spos[3 * sj], yj = P.spos[3 * sj + 1], zj = P.spos[3 * sj + 2];
-            const int tj = P.stype[sj];
-            if (!valid || sj == si) continue;
-            double dx = xi - xj, dy = yi - yj, dz = zi - zj;
-            dx -= L * round(dx * invL);
-            dy -= L * round(dy * invL);
-            dz -= L * round(dz * invL);
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            if (r2 > rc2) continue;
-            double fr, vm;
-            pair_terms<POT>(tab + 7 * (ti * ntyp + tj), r2, rsqrt(r2), fr, vm);
-            fx += fr * dx;
-            fy += fr * dy;
-            fz += fr * dz;
-            e_acc += vm;
+    const int I = SI * kTfSb + w;
+    if (I < nblk) {
+        const double* me = ipos + 4 * (w * 32 + lane);
+        const double xi = me[0], yi = me[1], zi = me[2];
+        const int ti = (int)me[3];  // -1: no ion in this lane
+        const double* bI = P.tf_box + 6 * I;
+        for (int t = 0; t < kTfSb; t++) {
+            const int d = (t - w) & (kTfSb - 1);
+            if (diag && (d > kTfSb / 2 || (d == kTfSb / 2 && w >= kTfSb / 2))) continue;
+            const int J = SJ * kTfSb + t;
+            if (J >= nblk) continue;
+            const bool self = diag && d == 0;
+            if (prune && !self) {
+                const double* bJ = P.tf_box + 6 * J;
+                const double gx = axis_gap(bI[0], bI[3], bJ[0], bJ[3] - bJ[0], L);
+                const double gy = axis_gap(bI[1], bI[4], bJ[1], bJ[4] - bJ[1], L);
+                const double gz = axis_gap(bI[2], bI[5], bJ[2], bJ[5] - bJ[2], L);
+                if (gx * gx + gy * gy + gz * gz > prune2) continue;
+            }
+            const double* jb = jpos + 4 * (t * 32);
+            double* fj = fjw + ((w * kTfSb + t) * 32) * 3;
+            // self tile: partners (l + s) mod 32 for s = 1..16, the last step by half the
+            // lanes, so every pair inside the block comes once
+            const int s0 = self ? 1 : 0, s1 = self ? 16 : 31;
+            for (int s = s0; s <= s1; s++) {
+                const int jj = (lane + s) & 31;
+                const double* pj = jb + 4 * jj;
+                const int tj = (int)pj[3];
+                if (ti < 0 || tj < 0 || (self && s == 16 && lane >= 16)) continue;
+                double dx = xi - pj[0], dy = yi - pj[1], dz = zi - pj[2];
+                dx -= L * round(dx * invL);
+                dy -= L * round(dy * invL);
+                dz -= L * round(dz * invL);
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 > rc2) continue;
+                double fr, vm;
+                pair_terms<POT>(tab + 7 * (ti * ntyp + tj), r2, rsqrt(r2), fr, vm);
+                const double ax = fr * dx, ay = fr * dy, az = fr * dz;
+                fx += ax;
+                fy += ay;
+                fz += az;
+                fj[3 * jj] -= ax;
+                fj[3 * jj + 1] -= ay;
+                fj[3 * jj + 2] -= az;
+                e_acc += vm;
+            }
         }
     }
-    if (valid) {
-        double* o = P.fpart + ((long)chunk * P.np + si) * 3;
+    // I side: this warp's block; J side: the warps' arrays summed in warp order
+    double* out = P.fpart + (size_t)st * 2 * kTfSb * 32 * 3;
+    if (I < nblk) {
+        double* o = out + (w * 32 + lane) * 3;
         o[0] = fx;
         o[1] = fy;
         o[2] = fz;
     }
+    __shared__ double esh[kTfSb];
     e_acc = warp_sum(e_acc);
-    if (lane == 0) P.epart[gw] = e_acc;
+    if (lane == 0) esh[w] = e_acc;
+    __syncthreads();
+    for (int x = threadIdx.x; x < kTfSb * 32 * 3; x += blockDim.x) {
+        double v = 0.0;
+        for (int q = 0; q < kTfSb; q++) v += fjw[q * kTfSb * 32 * 3 + x];
+        out[kTfSb * 32 * 3 + x] = v;
+    }
+    if (threadIdx.x == 0) {
+        double e = 0.0;
+        for (int q = 0; q < kTfSb; q++) e += esh[q];
+        P.epart[st] = e;
+    }
 }
 
-// Sum the chunk partials in chunk order, scatter back to ion order.
+// Each ion's force: its super-tile partials in list order, scattered back to ion order.
 __global__ void k_tf_gather(ParticleDev P) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P.np) return;
-    const int s = P.srank[p];
+    const int s = P.srank[p], b = s >> 5, lane = s & 31;
     double f[3] = {0.0, 0.0, 0.0};
-    for (int c = 0; c < P.tf_split; c++) {
-        const double* o = P.fpart + ((long)c * P.np + s) * 3;
+    for (int e = P.tf_gstart[b]; e < P.tf_gstart[b + 1]; e++) {
+        const int ent = P.tf_gent[e];
+        const int st = ent >> 4, side = (ent >> 3) & 1, slot = ent & 7;
+        const double* o = P.fpart + (((size_t)st * 2 + side) * kTfSb + slot) * 32 * 3 + lane * 3;
         f[0] += o[0];
         f[1] += o[1];
         f[2] += o[2];
@@ -153,12 +225,65 @@ __global__ void k_tf_gather(ParticleDev P) {
 }
 
 __global__ void k_tf_energy(ParticleDev P) {
-    const long m = (long)((P.np + 31) / 32) * P.tf_split;
     double v[1] = {0.0};
-    for (long x = threadIdx.x; x < m; x += blockDim.x) v[0] += P.epart[x];
+    for (int x = threadIdx.x; x < P.tf_nst; x += blockDim.x) v[0] += P.epart[x];
     __shared__ double sh[4 * 32];
     block_sum<1>(v, sh);
-    if (threadIdx.x == 0) P.red[1] = v[0] / 2;
+    if (threadIdx.x == 0) P.red[1] = v[0];
+}
+
+void tf_plan(ParticleDev& P) {
+    cudaFree(P.tf_st);
+    cudaFree(P.tf_gstart);
+    cudaFree(P.tf_gent);
+    cudaFree(P.tf_box);
+    cudaFree(P.fpart);
+    cudaFree(P.epart);
+    const int nblk = (P.np + 31) / 32 > 0 ? (P.np + 31) / 32 : 1;
+    const int nsb = (nblk + kTfSb - 1) / kTfSb;
+    std::vector<int> st;
+    for (int si = 0; si < nsb; si++) {
+        st.push_back(si);
+        st.push_back(si);
+        for (int d = 1; 2 * d <= nsb; d++) {
+            if (2 * d == nsb && si >= nsb / 2) continue;  // the middle distance once
+            st.push_back(si);
+            st.push_back((si + d) % nsb);
+        }
+    }
+    P.tf_nst = (int)st.size() / 2;
+    std::vector<std::vector<int>> lists(nblk);
+    for (int k = 0; k < P.tf_nst; k++)
+        for (int side = 0; side < 2; side++)
+            for (int slot = 0; slot < kTfSb; slot++) {
+                const int b = st[2 * k + side] * kTfSb + slot;
+                if (b < nblk) lists[b].push_back((k << 4) | (side << 3) | slot);
+            }
+    std::vector<int> gstart(nblk + 1, 0), gent;
+    for (int b = 0; b < nblk; b++) {
+        gent.insert(gent.end(), lists[b].begin(), lists[b].end());
+        gstart[b + 1] = (int)gent.size();
+    }
+    auto up = [](void** d, const void* h, size_t bytes) {
+        MZB_CHECK(cudaMalloc(d, bytes));
+        MZB_CHECK(cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
+        MZB_CHECK(cudaStreamSynchronize(cudaStreamLegacy));  // landed before any later kernel
+    };
+    up((void**)&P.tf_st, st.data(), sizeof(int) * st.size());
+    up((void**)&P.tf_gstart, gstart.data(), sizeof(int) * gstart.size());
+    up((void**)&P.tf_gent, gent.data(), sizeof(int) * gent.size());
+    MZB_CHECK(cudaMalloc(&P.tf_box, sizeof(double) * 6 * nblk));
+    MZB_CHECK(cudaMalloc(&P.fpart, sizeof(double) * (size_t)P.tf_nst * 2 * kTfSb * 32 * 3));
+    MZB_CHECK(cudaMalloc(&P.epart, sizeof(double) * P.tf_nst));
+    static unsigned long long attr_done = 0;  // devices whose kernels allow kTfSmem
+    int dev = 0;
+    MZB_CHECK(cudaGetDevice(&dev));
+    if (!(attr_done >> (dev & 63) & 1ull)) {
+        MZB_CHECK(cudaFuncSetAttribute(k_tf<POT_TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTfSmem));
+        MZB_CHECK(cudaFuncSetAttribute(k_tf<POT_LJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTfSmem));
+        MZB_CHECK(cudaFuncSetAttribute(k_tf<POT_SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTfSmem));
+        attr_done |= 1ull << (dev & 63);
+    }
 }
 
 void tf_forces(ParticleDev& P, cudaStream_t s) {
@@ -167,15 +292,17 @@ void tf_forces(ParticleDev& P, cudaStream_t s) {
         return;
     }
     if (P.ntyp * P.ntyp > 64) fatal("pair forces: more than 8 particle types");
-    const long warps = (long)((P.np + 31) / 32) * P.tf_split;
+    if (!P.tf_st) fatal("pair forces: no plan (tf_plan)");
+    const int nblk = (P.np + 31) / 32;
     count_launch();
-    const unsigned nb = (unsigned)((warps + kTfWarps - 1) / kTfWarps);
+    k_tf_boxes<<<(nblk * 32 + 255) / 256, 256, 0, s>>>(P);
+    count_launch();
     if (P.pot == POT_LJ)
-        k_tf<POT_LJ><<<nb, kTfWarps * 32, 0, s>>>(P);
+        k_tf<POT_LJ><<<P.tf_nst, kTfThreads, kTfSmem, s>>>(P);
     else if (P.pot == POT_SC)
-        k_tf<POT_SC><<<nb, kTfWarps * 32, 0, s>>>(P);
+        k_tf<POT_SC><<<P.tf_nst, kTfThreads, kTfSmem, s>>>(P);
     else
-        k_tf<POT_TF><<<nb, kTfWarps * 32, 0, s>>>(P);
+        k_tf<POT_TF><<<P.tf_nst, kTfThreads, kTfSmem, s>>>(P);
     count_launch();
     k_tf_gather<<<(P.np + 127) / 128, 128, 0, s>>>(P);
     count_launch();
