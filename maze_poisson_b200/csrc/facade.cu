@@ -720,7 +720,7 @@ int solver_update_charges(void) {
     MZB_CHECK(cudaMemcpyAsync(s.result_h, P.flags, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
     sync();
     flag = s.result_h[0];
-    if (flag) fatal("charge spreading: more than 2048 ions reach one 4x4x32 grid tile");
+    if (flag) fatal("charge spreading: more than 1024 ions reach one 2x8x32 grid tile");
     const double q_loc = s.red_h[0];
     int res = 0;
     if (fabs(s.q_tot - q_loc) > 1e-6) {
@@ -1765,7 +1765,7 @@ int batch_end(std::vector<System*>& ss, const int* handles) {
         MZB_CHECK(cudaMemcpy(err, s.err_d, sizeof(err), cudaMemcpyDeviceToHost));
         MZB_CHECK(cudaMemcpy(&q, s.qtot_d, sizeof(double), cudaMemcpyDeviceToHost));
         MZB_CHECK(cudaMemcpy(&s.I.ocalls, s.I.ocalls_d, sizeof(uint64_t), cudaMemcpyDeviceToHost));
-        if (err[1]) fatal("charge spreading: more than 2048 ions reach one 4x4x32 grid tile");
+        if (err[1]) fatal("charge spreading: more than 1024 ions reach one 2x8x32 grid tile");
         if (err[0]) {
             printf("Charge conservation error in system %d: q_tot = %.6f\n", handles[r], s.q_tot);
             exit(1);

@@ -63,45 +63,47 @@ __device__ __forceinline__ void corner_offsets(int c, int& di, int& dj, int& dk)
 
 // ------------------------------------------------------------------------------------
 // Exclusive scan of count[0..m) into start[0..m] (start[m] = total); start is also copied
-// into fill[0..m) as a scatter cursor. One block of 1024 threads. Optionally sums
-// `part[0..np_part)` in index order into *sum_out.
+// into fill[0..m) as a scatter cursor. One block of 1024 threads taking the counts in
+// coalesced rounds of 1024 with a running carry. Optionally sums `part[0..np_part)` in
+// index order into *sum_out.
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_scan(const int32_t* __restrict__ count, int m,
                                                int32_t* __restrict__ start, int32_t* __restrict__ fill,
                                                const double* __restrict__ part, int np_part,
                                                double* __restrict__ sum_out) {
     __shared__ int32_t wsum[32];
-    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    const int chunk = (m + blockDim.x - 1) / blockDim.x;
-    const int b = t * chunk, e = min(m, b + chunk);
-    int32_t local = 0;
-    for (int x = b; x < e; x++) local += count[x];
-    // inclusive warp scan
-    int32_t incl = local;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    if (lane == 31) wsum[w] = incl;
-    __syncthreads();
-    if (w == 0) {
-        int32_t v = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
+    int32_t carry = 0;
+    for (int base = 0; base < m; base += blockDim.x) {
+        const int x = base + t;
+        const int32_t v = x < m ? count[x] : 0;
+        int32_t incl = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int32_t u = __shfl_up_sync(0xffffffffu, v, o);
-            if (lane >= o) v += u;
+            const int32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
         }
-        wsum[lane] = v;
+        if (lane == 31) wsum[w] = incl;
+        __syncthreads();
+        if (w == 0) {
+            int32_t y = lane < nw ? wsum[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int32_t u = __shfl_up_sync(0xffffffffu, y, o);
+                if (lane >= o) y += u;
+            }
+            wsum[lane] = y;
+        }
+        __syncthreads();
+        const int32_t excl = carry + incl - v + (w > 0 ? wsum[w - 1] : 0);
+        if (x < m) {
+            start[x] = excl;
+            fill[x] = excl;
+        }
+        carry += wsum[nw - 1];
+        __syncthreads();
     }
-    __syncthreads();
-    int32_t run = incl - local + (w > 0 ? wsum[w - 1] : 0);
-    for (int x = b; x < e; x++) {
-        start[x] = run;
-        fill[x] = run;
-        run += count[x];
-    }
-    if (t == blockDim.x - 1) start[m] = wsum[(blockDim.x >> 5) - 1];
+    if (t == 0) start[m] = carry;
     if (sum_out != nullptr && t == 0) {
         double s = 0.0;
         for (int x = 0; x < np_part; x++) s += part[x];
@@ -152,95 +154,144 @@ __global__ void k_spread_fill(ParticleDev P) {
     P.tile_ions[slot] = p;
 }
 
-// One CTA per tile (grid-stride): gather the ions whose stencil can reach this tile (base
-// cell in this tile or the 7 tiles below it for CIC, whose +1 corners reach up; in the 27
-// tiles around it for the splines, whose offsets run -1..2), sort them by ion index,
-// accumulate chg*w into a shared-memory tile in ascending ion order -- exactly the order
-// of the reference's serial scatter (charges.c:123-141) -- and flush the whole tile,
-// zeros included, with coalesced stores. q is written once; no atomics touch it. One
-// thread per stencil point; the stencil's threads step through the ions together (a warp
-// barrier for CIC's 8, a named barrier for the splines' 64), so each point receives its
-// contributions in ion order.
+// Is grid index g one of the stencil's indices along an axis with base index b (wrapped)?
+// CIC: b, b+1; splines: b-1 .. b+2 (particles.c:297-385).
 template <int CAS>
-__global__ void __launch_bounds__(128) k_spread_tiles(ParticleDev P, double* __restrict__ q, int n,
-                                                      double h) {
-    constexpr int NS = stencil_size<CAS>();
+__device__ __forceinline__ bool in_stencil(int g, int b, int n) {
+    if (CAS == CAS_CIC) return g == b || g == (b + 1 == n ? 0 : b + 1);
+    const int d = g - b + 1;
+    return (d >= 0 && d <= 3) || (d + n >= 0 && d + n <= 3) || (d - n >= 0 && d - n <= 3);
+}
+
+// One warp per tile (grid-stride over warps): gather the ions whose stencil can reach the
+// tile (base cell in this tile or the 7 tiles below it for CIC, whose +1 corners reach
+// up; in the 27 tiles around it for the splines, whose offsets run -1..2), sort them by
+// ion index, and let every lane sum the contributions of its TI x TJ points (one k column)
+// over those ions in ascending ion order -- for each point the order of the reference's
+// serial scatter (charges.c:123-141), with the same weight expression -- then write the
+// tile, zeros included, 32 consecutive k per store. q is written once; no atomics touch
+// it, and the warps of a CTA never wait on one another.
+constexpr int kSpreadWarps = 4;
+constexpr int kSpreadStage = 32;  // staged candidates per round (one per lane)
+
+template <int CAS>
+__global__ void __launch_bounds__(kSpreadWarps * 32) k_spread_tiles(ParticleDev P, double* __restrict__ q, int n,
+                                                                    double h) {
     constexpr int NSRC = CAS == CAS_CIC ? 8 : 27;
-    __shared__ double acc[kTileI * kTileJ * kTileK];
-    __shared__ int cand[kTileCap];
-    __shared__ int sorted[kTileCap];
-    __shared__ int ncand;
-    __shared__ int srcs[NSRC];
+    __shared__ int cand_all[kSpreadWarps][kTileCap];
+    __shared__ int sorted_all[kSpreadWarps][kTileCap];
+    __shared__ double spos_all[kSpreadWarps][kSpreadStage][4];  // x, y, z, charge (rank order)
+    __shared__ int sbase_all[kSpreadWarps][kSpreadStage][3];
+    __shared__ int srcs_all[kSpreadWarps][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int* cand = cand_all[w];
+    int* sorted = sorted_all[w];
+    double (*spos)[4] = spos_all[w];
+    int (*sbase)[3] = sbase_all[w];
+    int* srcs = srcs_all[w];
     const double L = n * h;
     const long n2 = (long)n * n;
-    for (int tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
-        const int ti = tile / (P.ntj * P.ntk), tj = (tile / P.ntk) % P.ntj, tk = tile % P.ntk;
-        for (int e = threadIdx.x; e < kTileI * kTileJ * kTileK; e += blockDim.x) acc[e] = 0.0;
-        if (threadIdx.x < NSRC) {
-            const int c = threadIdx.x;
+    const long nwarps = (long)gridDim.x * kSpreadWarps;
+    for (long tile = (long)blockIdx.x * kSpreadWarps + w; tile < P.ntiles; tile += nwarps) {
+        const int ti = (int)(tile / (P.ntj * P.ntk)), tj = (int)((tile / P.ntk) % P.ntj), tk = (int)(tile % P.ntk);
+        int s = -1;
+        if (lane < NSRC) {
             int si, sj, sk;
             if (CAS == CAS_CIC) {
-                si = wrapi(ti - ((c >> 2) & 1), P.nti);
-                sj = wrapi(tj - ((c >> 1) & 1), P.ntj);
-                sk = wrapi(tk - (c & 1), P.ntk);
+                si = wrapi(ti - ((lane >> 2) & 1), P.nti);
+                sj = wrapi(tj - ((lane >> 1) & 1), P.ntj);
+                sk = wrapi(tk - (lane & 1), P.ntk);
             } else {
-                si = wrapi(ti + c / 9 - 1, P.nti);
-                sj = wrapi(tj + (c / 3) % 3 - 1, P.ntj);
-                sk = wrapi(tk + c % 3 - 1, P.ntk);
+                si = wrapi(ti + lane / 9 - 1, P.nti);
+                sj = wrapi(tj + (lane / 3) % 3 - 1, P.ntj);
+                sk = wrapi(tk + lane % 3 - 1, P.ntk);
             }
-            srcs[c] = (si * P.ntj + sj) * P.ntk + sk;
+            s = (si * P.ntj + sj) * P.ntk + sk;
+            srcs[lane] = s;
         }
-        if (threadIdx.x == 0) ncand = 0;
-        __syncthreads();
-        if (threadIdx.x < NSRC) {
-            const int c = threadIdx.x, s = srcs[c];
+        __syncwarp();
+        int cnt = 0, first = 0;
+        if (lane < NSRC) {
             bool dup = false;
-            for (int d = 0; d < c; d++) dup |= (srcs[d] == s);
+            for (int d = 0; d < lane; d++) dup |= (srcs[d] == s);
             if (!dup) {
-                for (int x = P.tile_start[s]; x < P.tile_start[s + 1]; x++) {
-                    const int slot = atomicAdd(&ncand, 1);
-                    if (slot < kTileCap) cand[slot] = P.tile_ions[x];
-                }
+                first = P.tile_start[s];
+                cnt = P.tile_start[s + 1] - first;
             }
         }
-        __syncthreads();
-        const int nc = ncand;
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        const int nc = __shfl_sync(0xffffffffu, incl, 31);
+        const int i0 = ti * kTileI, j0 = tj * kTileJ, k = tk * kTileK + lane;
+        double acc[kTileI][kTileJ];
+#pragma unroll
+        for (int a = 0; a < kTileI; a++)
+#pragma unroll
+            for (int r = 0; r < kTileJ; r++) acc[a][r] = 0.0;
         if (nc > kTileCap) {
-            if (threadIdx.x == 0) atomicOr(&P.flags[0], 1);
+            if (lane == 0) atomicOr(&P.flags[0], 1);
         } else {
-            for (int x = threadIdx.x; x < nc; x += blockDim.x) {
+            for (int x = 0; x < cnt; x++) cand[incl - cnt + x] = P.tile_ions[first + x];
+            __syncwarp();
+            for (int x = lane; x < nc; x += 32) {
                 const int me = cand[x];
                 int rank = 0;
                 for (int y = 0; y < nc; y++) rank += (cand[y] < me);
                 sorted[rank] = me;
             }
-            __syncthreads();
-            if (threadIdx.x < NS) {
-                const int o = threadIdx.x;
-                for (int x = 0; x < nc; x++) {
-                    const int p = sorted[x];
-                    int a, bb, e;
-                    stencil_point<CAS>(o, P.base + 3 * p, n, a, bb, e);
-                    const int li = a - ti * kTileI, lj = bb - tj * kTileJ, lk = e - tk * kTileK;
-                    if (li >= 0 && li < kTileI && lj >= 0 && lj < kTileJ && lk >= 0 && lk < kTileK) {
-                        double w = w_cas<CAS>(P.pos[3 * p] - a * h, L, h) * w_cas<CAS>(P.pos[3 * p + 1] - bb * h, L, h);
-                        w = w * w_cas<CAS>(P.pos[3 * p + 2] - e * h, L, h);
-                        acc[(li * kTileJ + lj) * kTileK + lk] += P.chg[p] * w;
-                    }
-                    if (CAS == CAS_CIC)
-                        __syncwarp(0xffu);
-                    else
-                        asm volatile("bar.sync 1, 64;" ::: "memory");
+            __syncwarp();
+            for (int c0 = 0; c0 < nc; c0 += kSpreadStage) {
+                const int cn = min(kSpreadStage, nc - c0);
+                if (lane < cn) {
+                    const int p = sorted[c0 + lane];
+                    spos[lane][0] = P.pos[3 * p];
+                    spos[lane][1] = P.pos[3 * p + 1];
+                    spos[lane][2] = P.pos[3 * p + 2];
+                    spos[lane][3] = P.chg[p];
+                    sbase[lane][0] = P.base[3 * p];
+                    sbase[lane][1] = P.base[3 * p + 1];
+                    sbase[lane][2] = P.base[3 * p + 2];
                 }
+                __syncwarp();
+                if (k < n) {
+                    for (int x = 0; x < cn; x++) {
+                        if (!in_stencil<CAS>(k, sbase[x][2], n)) continue;
+                        const double zk = w_cas<CAS>(spos[x][2] - k * h, L, h);
+                        const double cq = spos[x][3];
+#pragma unroll
+                        for (int a = 0; a < kTileI; a++) {
+                            const int i = i0 + a;
+                            if (i >= n || !in_stencil<CAS>(i, sbase[x][0], n)) continue;
+                            const double wx = w_cas<CAS>(spos[x][0] - i * h, L, h);
+#pragma unroll
+                            for (int r = 0; r < kTileJ; r++) {
+                                const int j = j0 + r;
+                                if (j < n && in_stencil<CAS>(j, sbase[x][1], n)) {
+                                    double wgt = wx * w_cas<CAS>(spos[x][1] - j * h, L, h);
+                                    wgt = wgt * zk;
+                                    acc[a][r] += cq * wgt;
+                                }
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
             }
         }
-        __syncthreads();
-        for (int e = threadIdx.x; e < kTileI * kTileJ * kTileK; e += blockDim.x) {
-            const int li = e / (kTileJ * kTileK), lj = (e / kTileK) % kTileJ, lk = e % kTileK;
-            const int i = ti * kTileI + li, j = tj * kTileJ + lj, k = tk * kTileK + lk;
-            if (i < n && j < n && k < n) q[(long)i * n2 + (long)j * n + k] = acc[e];
+        if (k < n) {
+#pragma unroll
+            for (int a = 0; a < kTileI; a++)
+#pragma unroll
+                for (int r = 0; r < kTileJ; r++) {
+                    const int i = i0 + a, j = j0 + r;
+                    if (i < n && j < n) q[(long)i * n2 + (long)j * n + k] = acc[a][r];
+                }
         }
-        __syncthreads();
+        __syncwarp();
     }
 }
 
@@ -262,14 +313,15 @@ void spread_charges(ParticleDev& P, double* q, int n, double h, cudaStream_t s) 
     int dev, sms;
     MZB_CHECK(cudaGetDevice(&dev));
     MZB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const int grid = P.ntiles < sms * 16 ? P.ntiles : sms * 16;
+    const int ctas = (P.ntiles + kSpreadWarps - 1) / kSpreadWarps;
+    const int grid = ctas < sms * 12 ? ctas : sms * 12;
     count_launch();
     if (P.cas == CAS_CIC)
-        k_spread_tiles<CAS_CIC><<<grid, 128, 0, s>>>(P, q, n, h);
+        k_spread_tiles<CAS_CIC><<<grid, kSpreadWarps * 32, 0, s>>>(P, q, n, h);
     else if (P.cas == CAS_SPL_QUADR)
-        k_spread_tiles<CAS_SPL_QUADR><<<grid, 128, 0, s>>>(P, q, n, h);
+        k_spread_tiles<CAS_SPL_QUADR><<<grid, kSpreadWarps * 32, 0, s>>>(P, q, n, h);
     else
-        k_spread_tiles<CAS_SPL_CUBIC><<<grid, 128, 0, s>>>(P, q, n, h);
+        k_spread_tiles<CAS_SPL_CUBIC><<<grid, kSpreadWarps * 32, 0, s>>>(P, q, n, h);
     MZB_CHECK(cudaGetLastError());
 }
 

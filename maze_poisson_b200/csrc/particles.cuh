@@ -6,9 +6,11 @@
 
 namespace mzb {
 
-// Spreading tile: TI x TJ x TK grid points accumulated in shared memory by one CTA.
-constexpr int kTileI = 4, kTileJ = 4, kTileK = 32;
-constexpr int kTileCap = 2048;  // candidate ions one tile CTA can hold (see spread_tiles)
+// Spreading tile: TI x TJ x TK grid points written by one warp (one k column of TI x TJ
+// points per lane); TI >= 2 so the splines' -1..2 stencils reach at most one tile either
+// way.
+constexpr int kTileI = 2, kTileJ = 8, kTileK = 32;
+constexpr int kTileCap = 1024;  // candidate ions one tile's warp can hold (see spread_tiles)
 
 // Charge assignment schemes (particles.c:28): CIC (8 points), quadratic and cubic
 // B-splines (4 x 4 x 4 = 64 points, offsets -1..2 around floor(pos/h)).
