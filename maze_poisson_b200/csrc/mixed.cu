@@ -58,7 +58,10 @@ struct Team {
     double* partials;   // >= 4 nblk doubles
 };
 
-// Barrier over the team's CTAs (the monotonic barrier of tma.cuh with the team's count).
+// Barrier over the team's CTAs (the monotonic barrier of tma.cuh with the team's count):
+// each CTA's writes are ordered before its release-add by the entry __syncthreads; the
+// acquire load that sees the final count synchronises with every release of the
+// counter's release sequence, and the exit __syncthreads extends that to the whole CTA.
 __device__ __forceinline__ bool team_sync(const Team& t, unsigned int& epoch) {
     __shared__ int ok_sh;
     __syncthreads();
@@ -68,7 +71,7 @@ __device__ __forceinline__ bool team_sync(const Team& t, unsigned int& epoch) {
         const unsigned int target = (epoch + 1u) * (unsigned)t.nblk;
         const unsigned long long t0 = global_ns();
         unsigned int polls = 0;
-        while (ld_relaxed_u32(&t.bar->count) < target) {
+        while (ld_acquire_u32(&t.bar->count) < target) {
             if ((++polls & 255u) == 0u) {
                 if (ld_relaxed_u32(&t.bar->err) != 0u) {
                     ok = 0;
@@ -81,7 +84,6 @@ __device__ __forceinline__ bool team_sync(const Team& t, unsigned int& epoch) {
                 }
             }
         }
-        asm volatile("fence.acq_rel.gpu;" ::: "memory");
         if (ok && ld_relaxed_u32(&t.bar->err) != 0u) ok = 0;
         ok_sh = ok;
     }

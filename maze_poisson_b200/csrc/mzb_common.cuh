@@ -129,17 +129,18 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
             __threadfence();
             atomicAdd(&bar->gen, 1u);
         } else {
+            // the acquire load that sees the new generation orders this CTA after the last
+            // arriver's fence and, through the counter's RMW chain, after every arrival
             const unsigned long long t0 = global_ns();
+            unsigned int polls = 0;
             while (ld_acquire_u32(&bar->gen) == g) {
-                __nanosleep(32);
-                if (global_ns() - t0 > kBarrierTimeoutNs) {
+                if ((++polls & 255u) == 0u && global_ns() - t0 > kBarrierTimeoutNs) {
                     atomicOr(&bar->err, 1u);
                     ok = 0;
                     break;
                 }
             }
         }
-        __threadfence();
         if (ld_acquire_u32(&bar->err) != 0u) ok = 0;
         ok_sh = ok;
     }

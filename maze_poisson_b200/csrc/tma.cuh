@@ -98,7 +98,7 @@ __device__ __forceinline__ bool grid_sync_mono(GridBarrier* bar, unsigned int& e
         const unsigned int target = (epoch + 1u) * gridDim.x;
         const unsigned long long t0 = global_ns();
         unsigned int polls = 0;
-        while (ld_relaxed_u32(&bar->count) < target) {
+        while (ld_acquire_u32(&bar->count) < target) {
             if ((++polls & 255u) == 0u) {
                 if (ld_relaxed_u32(&bar->err) != 0u) { ok = 0; break; }
                 if (global_ns() - t0 > kBarrierTimeoutNs) {
@@ -108,7 +108,6 @@ __device__ __forceinline__ bool grid_sync_mono(GridBarrier* bar, unsigned int& e
                 }
             }
         }
-        asm volatile("fence.acq_rel.gpu;" ::: "memory");
         if (ok && ld_relaxed_u32(&bar->err) != 0u) ok = 0;
         ok_sh = ok;
     }
