@@ -731,6 +731,87 @@ __device__ void coarse_direct(int n, const float* g, const float* b, float* x) {
     if (p < N && sub == 0) x[p] = acc;
 }
 
+// ---- shared-memory levels of 4, 8 or 16 points per side ----
+// The same point operations (and sums, in the same order) as gs_point, resid_point,
+// restrict_point and prolong_point, with the size known at compile time: 32-bit indices
+// and periodic wraps by masks instead of the general helpers' divisions and 64-bit
+// arithmetic, which on one CTA made each pass of these small levels instruction-bound.
+template <int N>
+__device__ __forceinline__ void sm_smooth(const float* b, float* x, int first_colour, int half_sweeps) {
+    constexpr int H = N / 2, M = N - 1, TOT = N * N * H;
+    for (int hs = 0; hs < half_sweeps; hs++) {
+        const int colour = (first_colour + hs) & 1;
+        for (int p = threadIdx.x; p < TOT; p += blockDim.x) {
+            const int i = p / (N * H), j = (p / H) % N, kk = p % H;
+            const int k = 2 * kk + ((i + j + colour) & 1);
+            const int c = (i * N + j) * N + k;
+            float s = x[(((i - 1) & M) * N + j) * N + k] + x[(((i + 1) & M) * N + j) * N + k];
+            s += x[(i * N + ((j - 1) & M)) * N + k];
+            s += x[(i * N + ((j + 1) & M)) * N + k];
+            s += x[(i * N + j) * N + ((k - 1) & M)];
+            s += x[(i * N + j) * N + ((k + 1) & M)];
+            x[c] = (b[c] - s) * (-1.0f / 6.0f);
+        }
+        __syncthreads();
+    }
+}
+template <int N>
+__device__ __forceinline__ void sm_resid(const float* b, const float* x, float* r) {
+    constexpr int M = N - 1, TOT = N * N * N;
+    for (int p = threadIdx.x; p < TOT; p += blockDim.x) {
+        const int i = p / (N * N), j = (p / N) % N, k = p % N;
+        float s = x[(((i + 1) & M) * N + j) * N + k] + x[(((i - 1) & M) * N + j) * N + k];
+        s += x[(i * N + ((j + 1) & M)) * N + k];
+        s += x[(i * N + ((j - 1) & M)) * N + k];
+        s += x[(i * N + j) * N + ((k + 1) & M)];
+        s += x[(i * N + j) * N + ((k - 1) & M)];
+        r[p] = b[p] - (s - 6.0f * x[p]);
+    }
+    __syncthreads();
+}
+template <int N>
+__device__ __forceinline__ void sm_restrict(const float* r, float* bc, float* xc) {
+    constexpr int NC = N / 2, M = N - 1, N2 = N * N, TOT = NC * NC * NC;
+    for (int p = threadIdx.x; p < TOT; p += blockDim.x) {
+        const int I = p / (NC * NC), J = (p / NC) % NC, K = p % NC;
+        const int i = 2 * I, j = 2 * J, k = 2 * K;
+        const int i0 = i * N2, i1 = ((i + 1) & M) * N2, i2 = ((i - 1) & M) * N2;
+        const int j0 = j * N, j1 = ((j + 1) & M) * N, j2 = ((j - 1) & M) * N;
+        const int k0 = k, k1 = (k + 1) & M, k2 = (k - 1) & M;
+        const float f = r[i2 + j0 + k0] + r[i1 + j0 + k0] + r[i0 + j2 + k0] + r[i0 + j1 + k0] + r[i0 + j0 + k2] +
+                        r[i0 + j0 + k1];
+        const float e = r[i1 + j0 + k2] + r[i1 + j0 + k1] + r[i2 + j0 + k2] + r[i2 + j0 + k1] + r[i1 + j2 + k0] +
+                        r[i1 + j1 + k0] + r[i2 + j2 + k0] + r[i2 + j1 + k0] + r[i0 + j2 + k2] + r[i0 + j2 + k1] +
+                        r[i0 + j1 + k2] + r[i0 + j1 + k1];
+        const float c = r[i1 + j1 + k2] + r[i1 + j1 + k1] + r[i1 + j2 + k2] + r[i1 + j2 + k1] + r[i2 + j1 + k2] +
+                        r[i2 + j1 + k1] + r[i2 + j2 + k2] + r[i2 + j2 + k1];
+        const float bv = (8.0f * r[i0 + j0 + k0] + 4.0f * f + 2.0f * e + c) * (4.0f / 64.0f);
+        bc[p] = bv;
+        xc[p] = ((I + J + K) & 1) == 0 ? bv * (-1.0f / 6.0f) : 0.0f;
+    }
+    __syncthreads();
+}
+template <int N>
+__device__ __forceinline__ void sm_prolong(const float* xc, float* x) {
+    constexpr int NC = N / 2, MC = NC - 1, NC2 = NC * NC, TOT = N * N * N;
+    for (int p = threadIdx.x; p < TOT; p += blockDim.x) {
+        const int i = p / (N * N), j = (p / N) % N, k = p % N;
+        const int ci = i >> 1, cj = j >> 1, ck = k >> 1;
+        const int i0 = ci * NC2, i1 = ((ci + 1) & MC) * NC2;
+        const int j0 = cj * NC, j1 = ((cj + 1) & MC) * NC;
+        const int k0 = ck, k1 = (ck + 1) & MC;
+        const float wi = (i & 1) ? 0.5f : 0.0f, wj = (j & 1) ? 0.5f : 0.0f, wk = (k & 1) ? 0.5f : 0.0f;
+        const float a00 = xc[i0 + j0 + k0] * (1.0f - wk) + xc[i0 + j0 + k1] * wk;
+        const float a01 = xc[i0 + j1 + k0] * (1.0f - wk) + xc[i0 + j1 + k1] * wk;
+        const float a10 = xc[i1 + j0 + k0] * (1.0f - wk) + xc[i1 + j0 + k1] * wk;
+        const float a11 = xc[i1 + j1 + k0] * (1.0f - wk) + xc[i1 + j1 + k1] * wk;
+        const float b0 = a00 * (1.0f - wj) + a01 * wj, b1 = a10 * (1.0f - wj) + a11 * wj;
+        x[p] += b0 * (1.0f - wi) + b1 * wi;
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ bool sm_fixed(int n) { return n == 4 || n == 8 || n == 16; }
+
 // Restricts the residual of level lsmall-1 (global) into shared memory, runs the rest of
 // the V-cycle there and writes level lsmall's correction back to lev_x[lsmall].
 __device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above) {
@@ -739,6 +820,9 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above
         const int n = a.lev_n[m];
         float* x = small_arr(a, sm, m, 0);
         const float* b = small_arr(a, sm, m, 1);
+        if (n == 16) return sm_smooth<16>(b, x, first_colour, half_sweeps);
+        if (n == 8) return sm_smooth<8>(b, x, first_colour, half_sweeps);
+        if (n == 4) return sm_smooth<4>(b, x, first_colour, half_sweeps);
         for (int h = 0; h < half_sweeps; h++) {
             cta_col(n, (first_colour + h) & 1, [&](int i, int j, int k) { gs_point(n, b, x, i, j, k); });
             __syncthreads();
@@ -768,12 +852,18 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above
         float* x = small_arr(a, sm, m, 0);
         float* b = small_arr(a, sm, m, 1);
         float* r = small_arr(a, sm, m, 2);
-        cta_pts(n, [&](int i, int j, int k) { resid_point(n, b, x, r, i, j, k); });
-        __syncthreads();
         float* bc = small_arr(a, sm, m + 1, 1);
         float* xc = small_arr(a, sm, m + 1, 0);
-        cta_pts(a.lev_n[m + 1], [&](int I, int J, int K) { restrict_point(n, r, bc, xc, I, J, K); });
-        __syncthreads();
+        if (sm_fixed(n)) {
+            if (n == 16) { sm_resid<16>(b, x, r); sm_restrict<16>(r, bc, xc); }
+            else if (n == 8) { sm_resid<8>(b, x, r); sm_restrict<8>(r, bc, xc); }
+            else { sm_resid<4>(b, x, r); sm_restrict<4>(r, bc, xc); }
+        } else {
+            cta_pts(n, [&](int i, int j, int k) { resid_point(n, b, x, r, i, j, k); });
+            __syncthreads();
+            cta_pts(a.lev_n[m + 1], [&](int I, int J, int K) { restrict_point(n, r, bc, xc, I, J, K); });
+            __syncthreads();
+        }
     }
     if (a.coarse_g != nullptr) {
         coarse_direct(a.lev_n[L - 1], gsm, small_arr(a, sm, L - 1, 1), small_arr(a, sm, L - 1, 0));
@@ -785,8 +875,12 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above
         const int n = a.lev_n[m];
         const float* xc = small_arr(a, sm, m + 1, 0);
         float* x = small_arr(a, sm, m, 0);
-        cta_pts(n, [&](int i, int j, int k) { prolong_point(n, xc, x, i, j, k); });
-        __syncthreads();
+        if (n == 16) sm_prolong<16>(xc, x);
+        else if (n == 8) sm_prolong<8>(xc, x);
+        else {
+            cta_pts(n, [&](int i, int j, int k) { prolong_point(n, xc, x, i, j, k); });
+            __syncthreads();
+        }
         smooth(m, 0, 2 * a.nu2);
     }
     const int nl = a.lev_n[ls];
