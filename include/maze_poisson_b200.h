@@ -98,6 +98,15 @@ int mzb_system_destroy(int handle);
    counterpart in the reference. */
 int mzb_batch_step(const int *handles, int nsys, int n_steps);
 
+/* Size classes side by side: system r belongs to class cls[r]; class c advances
+   class_steps[c] MD steps on its own stream while the others run, its systems' field
+   solves sharing class_ctas[c] CTAs (at least one per system; the counts add up to at
+   most the SM count). Each class takes the steps of mzb_batch_step, with the same
+   results. Returns when all classes are done: 0, or -1 if a field solve did not
+   converge. No counterpart in the reference. */
+int mzb_batch_classes(const int *handles, const int *cls, int nsys, const int *class_ctas,
+                      const int *class_steps, int nclass);
+
 /* Time candidate team partitions of the batched field solve on the listed systems and keep
    the fastest, and time their pair forces; out[0..3] = {partition exponent, pair-force
    CTAs, solve ms, forces ms}. Leaves the systems' state unchanged. */
@@ -106,6 +115,11 @@ int mzb_batch_autotune(const int *handles, int nsys, double *out);
 /* Device bytes one FP32+refine system with an n^3 grid and n_p ions holds (admission
    against an HBM budget). */
 double mzb_system_footprint(int n, int n_p);
+
+/* Release the device blocks the library keeps for reuse after systems are finalised (a
+   later system of the same sizes takes them instead of new allocations); returns the
+   bytes released. */
+size_t mzb_trim_device_cache(void);
 
 /* Asynchronous output snapshots of the selected system (the reference's output path,
    maze_poisson/myio/output/csv.py:45-183, calls the blocking getters every stride).
@@ -129,6 +143,7 @@ void *mzb_get_stream(void);                /* cudaStream_t of the current system
 double mzb_last_solve_ms(void);            /* device ms of the last field-solver launch */
 int mzb_last_solve_result(void);           /* its return value (iterations or -1) */
 uint64_t mzb_kernel_launches(void);        /* kernels this library has launched */
+int mzb_sm_count(void);                    /* SMs of the current device (CTA shares of the batched step) */
 
 #ifdef __cplusplus
 }

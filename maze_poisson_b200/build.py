@@ -30,6 +30,7 @@ SOURCES = {
     "noalloc.cu": ["--fmad=false"],
     "mixed.cu": ["--fmad=true"],
     "pb.cu": ["--fmad=false"],
+    "devmem.cu": ["--fmad=false"],
 }
 HEADERS = ["mzb_common.cuh", "engine.cuh", "particles.cuh", "fft.cuh", "tma.cuh", "mixed.cuh", "pb.cuh"]
 

@@ -115,6 +115,7 @@ EXTENSION_SYMBOLS = {
     "mzb_last_solve_ms": (_c.c_double, []),
     "mzb_last_solve_result": (_c.c_int, []),
     "mzb_kernel_launches": (_c.c_uint64, []),
+    "mzb_sm_count": (_c.c_int, []),
     "mzb_set_precision": (None, [_c.c_int, _c.c_double]),
     "mzb_get_precision": (_c.c_int, []),
     "mzb_conj_grad_noalloc": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_double, _c.c_int,
@@ -124,8 +125,10 @@ EXTENSION_SYMBOLS = {
     "mzb_system_current": (_c.c_int, []),
     "mzb_system_destroy": (_c.c_int, [_c.c_int]),
     "mzb_batch_step": (_c.c_int, [_i32_1, _c.c_int, _c.c_int]),
+    "mzb_batch_classes": (_c.c_int, [_i32_1, _i32_1, _c.c_int, _i32_1, _i32_1, _c.c_int]),
     "mzb_batch_autotune": (_c.c_int, [_i32_1, _c.c_int, _f64_1]),
     "mzb_system_footprint": (_c.c_double, [_c.c_int, _c.c_int]),
+    "mzb_trim_device_cache": (_c.c_size_t, []),
     "mzb_snapshot_begin": (_c.c_int, [_c.c_int]),
     "mzb_snapshot_fetch": (_c.c_int, [_c.c_int] + [_c.c_void_p] * 8),
     "mzb_snapshot_host": (_c.POINTER(_c.c_double), [_c.c_int]),

@@ -63,15 +63,14 @@ void copy_d2d(void* d, const void* src, size_t bytes) {
 
 template <class T>
 T* dalloc(size_t count) {
-    T* p = nullptr;
     if (count == 0) count = 1;
-    MZB_CHECK(cudaMalloc(&p, sizeof(T) * count));
+    T* p = static_cast<T*>(dev_alloc(sizeof(T) * count));
     zero_fill(p, sizeof(T) * count);
     return p;
 }
 template <class T>
 void dfree(T*& p) {
-    if (p) cudaFree(p);
+    dev_free(p);
     p = nullptr;
 }
 
@@ -166,15 +165,13 @@ void free_grid(GridState& G) {
     G.pbg = PbGrid{};
     G.pb = false;
     for (int l = 0; l < kMixedMaxLevels; l++) {
-        if (G.lev_x[l]) cudaFree(G.lev_x[l]);
-        if (G.lev_b[l]) cudaFree(G.lev_b[l]);
-        if (G.lev_r[l]) cudaFree(G.lev_r[l]);
+        dev_free(G.lev_x[l]);
+        dev_free(G.lev_b[l]);
+        dev_free(G.lev_r[l]);
         G.lev_x[l] = G.lev_b[l] = G.lev_r[l] = nullptr;
     }
-    if (G.lev_g) {
-        cudaFree(G.lev_g);
-        G.lev_g = nullptr;
-    }
+    dev_free(G.lev_g);
+    G.lev_g = nullptr;
     G.nlev = 0;
     G.ready = false;
 }
@@ -192,16 +189,16 @@ void ensure_mixed_levels(GridState& G) {
     G.nlev = mixed_levels(G.n, G.lev_n);
     for (int l = 0; l < G.nlev; l++) {
         const size_t m = (size_t)G.lev_n[l] * G.lev_n[l] * G.lev_n[l];
-        MZB_CHECK(cudaMalloc(&G.lev_x[l], m * sizeof(float)));
-        MZB_CHECK(cudaMalloc(&G.lev_b[l], m * sizeof(float)));
-        MZB_CHECK(cudaMalloc(&G.lev_r[l], m * sizeof(float)));
+        G.lev_x[l] = static_cast<float*>(dev_alloc(m * sizeof(float)));
+        G.lev_b[l] = static_cast<float*>(dev_alloc(m * sizeof(float)));
+        G.lev_r[l] = static_cast<float*>(dev_alloc(m * sizeof(float)));
         zero_fill(G.lev_x[l], m * sizeof(float));
     }
     const int nc = G.lev_n[G.nlev - 1];
     if (nc <= kMixedDirectN && mixed_small_level(G.nlev, G.lev_n) < G.nlev) {
         std::vector<float> g((size_t)nc * nc * nc);
         mixed_coarse_green(nc, g.data());
-        MZB_CHECK(cudaMalloc(&G.lev_g, g.size() * sizeof(float)));
+        G.lev_g = static_cast<float*>(dev_alloc(g.size() * sizeof(float)));
         upload(G.lev_g, g.data(), g.size() * sizeof(float));
     }
 }
@@ -1495,6 +1492,7 @@ int mzb_last_solve_result(void) { return sys().last_solve_iters; }
 
 // Kernels launched by this library since it was loaded.
 uint64_t mzb_kernel_launches(void) { return g_kernel_launches; }
+int mzb_sm_count(void) { return mixed_grid_blocks(); }
 uint64_t mzb_get_ocalls(void) { return sys().I.ocalls; }
 
 // n_steps iterations of SolverMD.md_loop_iter (maze_poisson/solver.py:483-492) with both
@@ -1531,6 +1529,8 @@ int solver_md_step(int n_steps) {
 // own range of CTAs (mixed_batch_kernel), and forks again for field + pair + total forces
 // and integrator part 2. The graph bakes in each system's buffer pointers, which rotate
 // with period 3 after every solve, so up to three graphs per membership are cached.
+// mzb_batch_classes runs several such batches (size classes) side by side, each on its
+// own stream with its own share of the CTAs and its own number of steps per call.
 // ====================================================================================
 namespace mzb {
 namespace {
@@ -1547,26 +1547,30 @@ __global__ void k_solve_check(const int* result, int* err) {
 
 struct BatchGraph {
     std::vector<uint64_t> key;
+    std::vector<int> handles;
     cudaGraphExec_t exec = nullptr;
     MixedArgs* list_d = nullptr;
     int* start_d = nullptr;
     unsigned long long launches = 0;
+    unsigned long long used = 0;  // call counter of the last use (least recently used goes first)
 };
 
 struct Batch {
     int device = -1;
-    cudaStream_t stream = nullptr;
     cudaEvent_t fork1 = nullptr, fork2 = nullptr, t0 = nullptr, t1 = nullptr;
+    std::vector<cudaStream_t> streams;  // one per size class; streams[0] also serves mzb_batch_step
     std::vector<cudaEvent_t> join1, join2;
     std::vector<BatchGraph> graphs;
+    size_t capacity = 6;
+    unsigned long long calls = 0;
     double alpha = 1.0;  // team size ~ (grid points)^alpha (autotuned)
 };
 Batch g_batchst;
 
 void release_graph(BatchGraph& bg) {
     if (bg.exec) cudaGraphExecDestroy(bg.exec);
-    if (bg.list_d) cudaFree(bg.list_d);
-    if (bg.start_d) cudaFree(bg.start_d);
+    dev_free(bg.list_d);
+    dev_free(bg.start_d);
     bg = BatchGraph{};
 }
 
@@ -1575,17 +1579,34 @@ void batch_clear_graphs() {
     g_batchst.graphs.clear();
 }
 
-void batch_events(int nsys) {
+// Release the graphs that step system `handle` (the others stay valid).
+void batch_drop_graphs(int handle) {
+    auto& gs = g_batchst.graphs;
+    for (size_t i = 0; i < gs.size();) {
+        if (std::find(gs[i].handles.begin(), gs[i].handles.end(), handle) != gs[i].handles.end()) {
+            release_graph(gs[i]);
+            gs.erase(gs.begin() + i);
+        } else {
+            i++;
+        }
+    }
+}
+
+void batch_events(int nsys, int nclass = 1) {
     Batch& B = g_batchst;
     int dev;
     MZB_CHECK(cudaGetDevice(&dev));
     if (B.device != dev) {
-        MZB_CHECK(cudaStreamCreateWithFlags(&B.stream, cudaStreamNonBlocking));
         MZB_CHECK(cudaEventCreateWithFlags(&B.fork1, cudaEventDisableTiming));
         MZB_CHECK(cudaEventCreateWithFlags(&B.fork2, cudaEventDisableTiming));
         MZB_CHECK(cudaEventCreate(&B.t0));
         MZB_CHECK(cudaEventCreate(&B.t1));
         B.device = dev;
+    }
+    while ((int)B.streams.size() < nclass) {
+        cudaStream_t st;
+        MZB_CHECK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        B.streams.push_back(st);
     }
     while ((int)B.join1.size() < nsys) {
         cudaEvent_t e1, e2;
@@ -1669,21 +1690,31 @@ void stage_particles_after_solve(System& s) {
     integrator_part2(P, s.I, s.stream);
 }
 
-// Build (or find) the graph of one batched MD step for the systems' current state.
-BatchGraph& batch_graph(const std::vector<int>& handles, const std::vector<System*>& ss) {
+// Build (or find) the graph of one batched MD step for the systems' current state, its
+// field solves on `nblocks` CTAs, captured on `stream` (any stream may launch it). `first`
+// is the index of the systems' first join events (each system of a call has its own).
+BatchGraph& batch_graph(const std::vector<int>& handles, const std::vector<System*>& ss, int nblocks,
+                        cudaStream_t stream, int first) {
     Batch& B = g_batchst;
     std::vector<uint64_t> key;
     key.push_back((uint64_t)(B.alpha * 1e6));
+    key.push_back((uint64_t)nblocks);
     for (size_t r = 0; r < ss.size(); r++) {
         key.push_back((uint64_t)handles[r]);
         key.push_back(ss[r]->epoch);
         key.push_back((uint64_t)ss[r]->G.iphi);
     }
     for (auto& bg : B.graphs)
-        if (bg.key == key) return bg;
-    if (B.graphs.size() >= 6) {
-        release_graph(B.graphs.front());
-        B.graphs.erase(B.graphs.begin());
+        if (bg.key == key) {
+            bg.used = B.calls;
+            return bg;
+        }
+    while (B.graphs.size() >= B.capacity) {  // least recently used first
+        size_t v = 0;
+        for (size_t i = 1; i < B.graphs.size(); i++)
+            if (B.graphs[i].used < B.graphs[v].used) v = i;
+        release_graph(B.graphs[v]);
+        B.graphs.erase(B.graphs.begin() + v);
     }
     const int nsys = (int)ss.size();
     std::vector<MixedArgs> list(nsys);
@@ -1694,35 +1725,36 @@ BatchGraph& batch_graph(const std::vector<int>& handles, const std::vector<Syste
         list[r] = mixed_args(*ss[r], prog, cst);
         smem = std::max(smem, mixed_smem_bytes(list[r]));
     }
-    const int nblocks = mixed_grid_blocks();
     const std::vector<int> start = team_starts(ss, nblocks, B.alpha);
     BatchGraph bg;
     bg.key = key;
-    MZB_CHECK(cudaMalloc(&bg.list_d, sizeof(MixedArgs) * nsys));
-    MZB_CHECK(cudaMalloc(&bg.start_d, sizeof(int) * (nsys + 1)));
+    bg.handles = handles;
+    bg.used = B.calls;
+    bg.list_d = static_cast<MixedArgs*>(dev_alloc(sizeof(MixedArgs) * nsys));
+    bg.start_d = static_cast<int*>(dev_alloc(sizeof(int) * (nsys + 1)));
     upload(bg.list_d, list.data(), sizeof(MixedArgs) * nsys);
     upload(bg.start_d, start.data(), sizeof(int) * (nsys + 1));
 
     const unsigned long long l0 = g_kernel_launches;
     cudaGraph_t graph = nullptr;
-    MZB_CHECK(cudaStreamBeginCapture(B.stream, cudaStreamCaptureModeThreadLocal));
-    MZB_CHECK(cudaEventRecord(B.fork1, B.stream));
+    MZB_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    MZB_CHECK(cudaEventRecord(B.fork1, stream));
     for (int r = 0; r < nsys; r++) {
         MZB_CHECK(cudaStreamWaitEvent(ss[r]->stream, B.fork1, 0));
         stage_particles_before_solve(*ss[r]);
-        MZB_CHECK(cudaEventRecord(B.join1[r], ss[r]->stream));
-        MZB_CHECK(cudaStreamWaitEvent(B.stream, B.join1[r], 0));
+        MZB_CHECK(cudaEventRecord(B.join1[first + r], ss[r]->stream));
+        MZB_CHECK(cudaStreamWaitEvent(stream, B.join1[first + r], 0));
     }
-    for (int r = 0; r < nsys; r++) MZB_CHECK(cudaMemsetAsync(ss[r]->bar, 0, sizeof(GridBarrier), B.stream));
-    mixed_batch_launch(bg.list_d, bg.start_d, nsys, nblocks, smem, B.stream);
-    MZB_CHECK(cudaEventRecord(B.fork2, B.stream));
+    for (int r = 0; r < nsys; r++) MZB_CHECK(cudaMemsetAsync(ss[r]->bar, 0, sizeof(GridBarrier), stream));
+    mixed_batch_launch(bg.list_d, bg.start_d, nsys, nblocks, smem, stream);
+    MZB_CHECK(cudaEventRecord(B.fork2, stream));
     for (int r = 0; r < nsys; r++) {
         MZB_CHECK(cudaStreamWaitEvent(ss[r]->stream, B.fork2, 0));
         stage_particles_after_solve(*ss[r]);
-        MZB_CHECK(cudaEventRecord(B.join2[r], ss[r]->stream));
-        MZB_CHECK(cudaStreamWaitEvent(B.stream, B.join2[r], 0));
+        MZB_CHECK(cudaEventRecord(B.join2[first + r], ss[r]->stream));
+        MZB_CHECK(cudaStreamWaitEvent(stream, B.join2[first + r], 0));
     }
-    MZB_CHECK(cudaStreamEndCapture(B.stream, &graph));
+    MZB_CHECK(cudaStreamEndCapture(stream, &graph));
     bg.launches = g_kernel_launches - l0;
     g_kernel_launches = l0;  // counted when the graph runs
     MZB_CHECK(cudaGraphInstantiate(&bg.exec, graph, 0));
@@ -1745,8 +1777,9 @@ std::vector<System*> batch_systems(const int* handles, int nsys) {
 }
 
 // Wait for the systems' own streams, set up their device-side state.
-void batch_begin(std::vector<System*>& ss) {
-    batch_events((int)ss.size());
+void batch_begin(std::vector<System*>& ss, int nclass = 1) {
+    batch_events((int)ss.size(), nclass);
+    g_batchst.calls++;
     for (System* s : ss) {
         MZB_CHECK(cudaStreamSynchronize(s->stream));
         batch_prepare(*s);
@@ -1755,8 +1788,8 @@ void batch_begin(std::vector<System*>& ss) {
 
 // Wait for the batch, copy the device-side state back and report errors the way the
 // per-call path does (solver_md.c:98-102 exits on a charge error).
-int batch_end(std::vector<System*>& ss, const int* handles) {
-    MZB_CHECK(cudaStreamSynchronize(g_batchst.stream));
+int batch_end(std::vector<System*>& ss, const int* handles, int nclass = 1) {
+    for (int c = 0; c < nclass; c++) MZB_CHECK(cudaStreamSynchronize(g_batchst.streams[c]));
     int status = 0;
     for (size_t r = 0; r < ss.size(); r++) {
         System& s = *ss[r];
@@ -1775,6 +1808,51 @@ int batch_end(std::vector<System*>& ss, const int* handles) {
         zero_fill(s.err_d, 4 * sizeof(int));
     }
     return status;
+}
+
+void rotate_fields(const std::vector<System*>& ss) {  // phi_prev <- old phi, phi <- the solve's output
+    for (System* s : ss) {
+        GridState& G = s->G;
+        const int old = G.iphi;
+        G.iphi = G.ispare;
+        G.ispare = G.iprev;
+        G.iprev = old;
+    }
+}
+
+// Class c takes steps[c] graph launches on its own stream, interleaved across the classes
+// so that every stream has work queued early. All graphs of the call (at most three
+// buffer rotations per class) are built first: building one allocates device memory and
+// copies on the legacy stream, which would otherwise stop the classes from overlapping.
+void batch_run(const std::vector<std::vector<int>>& hv, const std::vector<std::vector<System*>>& cs,
+               const std::vector<int>& ctas, const std::vector<int>& steps) {
+    Batch& B = g_batchst;
+    const int nclass = (int)cs.size();
+    int most = 0, first = 0;
+    std::vector<int> firsts(nclass);
+    for (int c = 0; c < nclass; c++) {
+        most = std::max(most, steps[c]);
+        firsts[c] = first;
+        first += (int)cs[c].size();
+    }
+    B.capacity = std::max<size_t>(B.capacity, 3 * (size_t)nclass + 3);
+    for (int c = 0; c < nclass; c++) {
+        const int k = std::min(steps[c], 3);
+        for (int t = 0; t < k; t++) {
+            batch_graph(hv[c], cs[c], ctas[c], B.streams[c], firsts[c]);
+            rotate_fields(cs[c]);
+        }
+        for (int t = k; t < 3 && k > 0; t++) rotate_fields(cs[c]);  // back to the starting rotation
+    }
+    for (int k = 0; k < most; k++) {
+        for (int c = 0; c < nclass; c++) {
+            if (k >= steps[c]) continue;
+            BatchGraph& bg = batch_graph(hv[c], cs[c], ctas[c], B.streams[c], firsts[c]);
+            MZB_CHECK(cudaGraphLaunch(bg.exec, B.streams[c]));
+            g_kernel_launches += bg.launches;
+            rotate_fields(cs[c]);
+        }
+    }
 }
 
 void release_snapshots(int handle);  // output snapshots of a system (defined below)
@@ -1812,7 +1890,7 @@ int mzb_system_destroy(int handle) {
     g = g_systems[handle];
     solver_finalize();
     System& s = *g;
-    batch_clear_graphs();
+    batch_drop_graphs(handle);
     if (s.stream) cudaStreamDestroy(s.stream);
     if (s.ev0) cudaEventDestroy(s.ev0);
     if (s.ev1) cudaEventDestroy(s.ev1);
@@ -1845,19 +1923,42 @@ int mzb_batch_step(const int* handles, int nsys, int n_steps) {
     std::vector<System*> ss = batch_systems(handles, nsys);
     batch_begin(ss);
     std::vector<int> hv(handles, handles + nsys);
-    for (int k = 0; k < n_steps; k++) {
-        BatchGraph& bg = batch_graph(hv, ss);
-        MZB_CHECK(cudaGraphLaunch(bg.exec, g_batchst.stream));
-        g_kernel_launches += bg.launches;
-        for (System* s : ss) {  // phi_prev <- old phi, phi <- the solve's output
-            GridState& G = s->G;
-            const int old = G.iphi;
-            G.iphi = G.ispare;
-            G.ispare = G.iprev;
-            G.iprev = old;
-        }
-    }
+    batch_run({hv}, {ss}, {mixed_grid_blocks()}, {n_steps});
     return batch_end(ss, handles);
+}
+
+// Size classes side by side: system r belongs to class cls[r] (0 <= cls[r] < nclass);
+// class c advances class_steps[c] MD steps (at least 0) on its own stream, its systems'
+// field solves sharing class_ctas[c] CTAs (at least one per system), while the other
+// classes run theirs: the classes' kernels overlap on the device, each class at its own
+// pace. The CTA counts must add up to at most the SM count, so that every class's
+// cooperative solve can be resident together with the others'. Each class runs the steps
+// of mzb_batch_step (the same graphs, the same results); returns when all classes are
+// done: 0, or -1 if any field solve did not converge.
+int mzb_batch_classes(const int* handles, const int* cls, int nsys, const int* class_ctas, const int* class_steps,
+                      int nclass) {
+    if (nclass < 1) fatal("batched classes: no classes");
+    std::vector<System*> ss = batch_systems(handles, nsys);
+    std::vector<std::vector<int>> hv(nclass);
+    std::vector<std::vector<System*>> cs(nclass);
+    for (int r = 0; r < nsys; r++) {
+        if (cls[r] < 0 || cls[r] >= nclass) fatal("batched classes: class index out of range");
+        hv[cls[r]].push_back(handles[r]);
+        cs[cls[r]].push_back(ss[r]);
+    }
+    std::vector<int> ctas(nclass), steps(nclass);
+    long total = 0;
+    for (int c = 0; c < nclass; c++) {
+        ctas[c] = class_ctas[c];
+        steps[c] = cs[c].empty() ? 0 : class_steps[c];
+        if (steps[c] < 0) fatal("batched classes: negative step count");
+        if (!cs[c].empty() && ctas[c] < (int)cs[c].size()) fatal("batched classes: fewer CTAs than systems in a class");
+        if (!cs[c].empty()) total += ctas[c];
+    }
+    if (total > mixed_grid_blocks()) fatal("batched classes: more CTAs than SMs");
+    batch_begin(ss, nclass);
+    batch_run(hv, cs, ctas, steps);
+    return batch_end(ss, handles, nclass);
 }
 
 // Choose the batched step's team partition exponent (CTAs per system ~ points^alpha)
@@ -1869,6 +1970,7 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
     std::vector<System*> ss = batch_systems(handles, nsys);
     batch_begin(ss);
     Batch& B = g_batchst;
+    cudaStream_t st = B.streams[0];
     const int nblocks = mixed_grid_blocks();
     std::vector<MixedArgs> list(nsys);
     size_t smem = 0;
@@ -1896,7 +1998,7 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
         for (int r = 0; r < nsys; r++)
             if (ysave[r])
                 MZB_CHECK(cudaMemcpyAsync(ss[r]->G.y, ysave[r], sizeof(double) * ss[r]->G.m, cudaMemcpyDeviceToDevice,
-                                          B.stream));
+                                          st));
     };
     const double alphas[] = {1.0, 0.8, 0.6, 0.4};
     double best_alpha = B.alpha, best_solve = 1e30;
@@ -1906,11 +2008,11 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
         float tot = 0.f;
         for (int rep = 0; rep < 3; rep++) {
             restore_y();
-            for (int r = 0; r < nsys; r++) MZB_CHECK(cudaMemsetAsync(ss[r]->bar, 0, sizeof(GridBarrier), B.stream));
-            MZB_CHECK(cudaEventRecord(B.t0, B.stream));
-            mixed_batch_launch(list_d, start_d, nsys, nblocks, smem, B.stream);
-            MZB_CHECK(cudaEventRecord(B.t1, B.stream));
-            MZB_CHECK(cudaStreamSynchronize(B.stream));
+            for (int r = 0; r < nsys; r++) MZB_CHECK(cudaMemsetAsync(ss[r]->bar, 0, sizeof(GridBarrier), st));
+            MZB_CHECK(cudaEventRecord(B.t0, st));
+            mixed_batch_launch(list_d, start_d, nsys, nblocks, smem, st);
+            MZB_CHECK(cudaEventRecord(B.t1, st));
+            MZB_CHECK(cudaStreamSynchronize(st));
             float ms = 0.f;
             MZB_CHECK(cudaEventElapsedTime(&ms, B.t0, B.t1));
             if (rep > 0) tot += ms;
@@ -1921,7 +2023,7 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
         }
     }
     restore_y();
-    MZB_CHECK(cudaStreamSynchronize(B.stream));
+    MZB_CHECK(cudaStreamSynchronize(st));
     for (double* p : ysave)
         if (p) cudaFree(p);
     cudaFree(list_d);
@@ -1935,17 +2037,17 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
     {
         float tot = 0.f;
         for (int rep = 0; rep < 3; rep++) {
-            MZB_CHECK(cudaEventRecord(B.t0, B.stream));
-            MZB_CHECK(cudaEventRecord(B.fork1, B.stream));
+            MZB_CHECK(cudaEventRecord(B.t0, st));
+            MZB_CHECK(cudaEventRecord(B.fork1, st));
             for (int r = 0; r < nsys; r++) {
                 MZB_CHECK(cudaStreamWaitEvent(ss[r]->stream, B.fork1, 0));
                 build_cells(ss[r]->P, ss[r]->stream);
                 tf_forces(ss[r]->P, ss[r]->stream);
                 MZB_CHECK(cudaEventRecord(B.join1[r], ss[r]->stream));
-                MZB_CHECK(cudaStreamWaitEvent(B.stream, B.join1[r], 0));
+                MZB_CHECK(cudaStreamWaitEvent(st, B.join1[r], 0));
             }
-            MZB_CHECK(cudaEventRecord(B.t1, B.stream));
-            MZB_CHECK(cudaStreamSynchronize(B.stream));
+            MZB_CHECK(cudaEventRecord(B.t1, st));
+            MZB_CHECK(cudaStreamSynchronize(st));
             float ms = 0.f;
             MZB_CHECK(cudaEventElapsedTime(&ms, B.t0, B.t1));
             if (rep > 0) tot += ms;

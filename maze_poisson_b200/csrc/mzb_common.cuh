@@ -23,6 +23,14 @@ constexpr double kBoltzmannHartree = 3.1668e-6;  // Hartree / K
 extern unsigned long long g_kernel_launches;
 inline void count_launch(unsigned long long k = 1) { g_kernel_launches += k; }
 
+// Device blocks for the systems' arrays, reused across systems (devmem.cu): dev_free
+// keeps a block for a later dev_alloc of the same size class once the device has
+// synchronised; dev_trim releases every kept block.
+void* dev_alloc(size_t bytes);
+void dev_free(void* p);
+void dev_trim();
+size_t dev_cached_bytes();
+
 }  // namespace mzb
 
 #define MZB_CHECK(x)                                                       \

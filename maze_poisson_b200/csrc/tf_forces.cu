@@ -233,12 +233,12 @@ __global__ void k_tf_energy(ParticleDev P) {
 }
 
 void tf_plan(ParticleDev& P) {
-    cudaFree(P.tf_st);
-    cudaFree(P.tf_gstart);
-    cudaFree(P.tf_gent);
-    cudaFree(P.tf_box);
-    cudaFree(P.fpart);
-    cudaFree(P.epart);
+    dev_free(P.tf_st);
+    dev_free(P.tf_gstart);
+    dev_free(P.tf_gent);
+    dev_free(P.tf_box);
+    dev_free(P.fpart);
+    dev_free(P.epart);
     const int nblk = (P.np + 31) / 32 > 0 ? (P.np + 31) / 32 : 1;
     const int nsb = (nblk + kTfSb - 1) / kTfSb;
     std::vector<int> st;
@@ -265,16 +265,16 @@ void tf_plan(ParticleDev& P) {
         gstart[b + 1] = (int)gent.size();
     }
     auto up = [](void** d, const void* h, size_t bytes) {
-        MZB_CHECK(cudaMalloc(d, bytes));
+        *d = dev_alloc(bytes);
         MZB_CHECK(cudaMemcpy(*d, h, bytes, cudaMemcpyHostToDevice));
         MZB_CHECK(cudaStreamSynchronize(cudaStreamLegacy));  // landed before any later kernel
     };
     up((void**)&P.tf_st, st.data(), sizeof(int) * st.size());
     up((void**)&P.tf_gstart, gstart.data(), sizeof(int) * gstart.size());
     up((void**)&P.tf_gent, gent.data(), sizeof(int) * gent.size());
-    MZB_CHECK(cudaMalloc(&P.tf_box, sizeof(double) * 6 * nblk));
-    MZB_CHECK(cudaMalloc(&P.fpart, sizeof(double) * (size_t)P.tf_nst * 2 * kTfSb * 32 * 3));
-    MZB_CHECK(cudaMalloc(&P.epart, sizeof(double) * P.tf_nst));
+    P.tf_box = static_cast<double*>(dev_alloc(sizeof(double) * 6 * nblk));
+    P.fpart = static_cast<double*>(dev_alloc(sizeof(double) * (size_t)P.tf_nst * 2 * kTfSb * 32 * 3));
+    P.epart = static_cast<double*>(dev_alloc(sizeof(double) * P.tf_nst));
     static unsigned long long attr_done = 0;  // devices whose kernels allow kTfSmem
     int dev = 0;
     MZB_CHECK(cudaGetDevice(&dev));

@@ -5,17 +5,33 @@ integrator) arrive as a seeded Poisson stream. The loop admits them in arrival o
 slots and device memory free up (the footprint of mzb_system_footprint against an HBM
 budget), bootstraps each admitted job through the reference calls (SolverMD.initialize
 and initialize_md, maze_poisson/solver.py:96-108, 371-409), keeps its fields and
-particle state on the device, and advances all active jobs together in chunks of
-mzb_batch_step (continuous batching: membership changes between chunks, never within
-one). A job's latency runs from its arrival to the end of its last step.
+particle state on the device, and advances the active jobs together in calls of the
+batched step (continuous batching: membership changes between calls, never within one).
+
+Two policies:
+
+* ``shared`` (default): every active job is its own class of mzb_batch_classes, with its
+  own stream and its own share of the SMs for its cooperative field solve, so jobs of
+  different sizes run side by side, each at its own pace. A calibrated cost model gives
+  each job's step time on c CTAs, t(c) = a + b / c (a: latency-bound part, b: the part
+  that scales with the SMs), fitted from two timed runs of the job's configuration alone.
+  The shares are water-filled to equalise the predicted slowdown t(c_j) / t(all SMs)
+  across jobs, and a job is admitted only while the predicted slowdown of every active
+  job, times the measured interference factor of recent calls, stays within ``beta``.
+  Each call gives job j about ``call_ms`` / t(c_j) steps.
+* ``lockstep``: all active jobs in ONE batched step per MD step (mzb_batch_step after
+  mzb_batch_autotune), admitted by slots and memory only; every job moves at the pace of
+  the slowest.
+
+A job's latency runs from its admission to the end of its last step (its bootstrap
+included); the queueing wait before admission is reported on its own. The slowdown of a
+job is its latency over the same job run alone on the whole GPU (bootstrap + steps x its
+step time alone, from the calibration).
 
     python -m maze_poisson_b200.serve --rate 20 --duration 5 --seed 7
 
-prints one JSON line: p50/p99 latency, p50/p99 slowdown against the same job run alone
-(from per-configuration step times measured alone), aggregate steps/s, the steps/s of
-running the same jobs one after another alone, and occupancy.
-With --precision 0 the jobs use the reference's FP64 solvers and are stepped one after
-another (solver_md_step), the plain baseline of the served form.
+prints one JSON line. With --precision 0 the jobs use the reference's FP64 solvers and
+are stepped one after another in chunks (solver_md_step), the plain baseline.
 """
 import argparse
 import dataclasses
@@ -55,6 +71,10 @@ class Job:
     def n_ions(self):
         return 2 * self.ncell ** 3
 
+    @property
+    def key(self):
+        return (self.n_grid, self.ncell)
+
 
 def grid_for(n_ions, density, spacing_ang=0.3):
     """The allowed grid closest to a spacing of `spacing_ang` for this box."""
@@ -90,25 +110,160 @@ def make_run(capi, job, precision, tol):
                  thermostat=job.integrator == "OVRVO", precision=precision)
 
 
+# -- cost model and CTA shares ---------------------------------------------------------
+
+@dataclasses.dataclass
+class Cost:
+    """Seconds: bootstrap, and one MD step on c CTAs, t(c) = a + b / c."""
+    boot: float
+    a: float
+    b: float
+    sms: int
+
+    @property
+    def alone(self):
+        return self.step(self.sms)
+
+    def step(self, ctas):
+        return self.a + self.b / ctas
+
+    def ctas_for(self, slowdown):
+        """Fewest CTAs with t(c) <= slowdown x t(all SMs), or None if none is enough."""
+        room = slowdown * self.alone - self.a
+        if self.b <= 0:  # no part that scales with the SMs
+            return 1 if room >= -1e-15 * self.a else None
+        if room <= 0:
+            return None
+        c = max(1, math.ceil(self.b / room - 1e-12))
+        return c if c <= self.sms else None
+
+
+def fit_cost(boot, t_all, t_low, sms, low):
+    """a, b of t(c) = a + b / c through (sms, t_all) and (low, t_low), b >= 0, a >= 0."""
+    b = max(0.0, (t_low - t_all) / (1.0 / low - 1.0 / sms))
+    a = max(0.0, t_all - b / sms)
+    return Cost(boot=boot, a=a, b=b, sms=sms)
+
+
+def plan_shares(costs, sms):
+    """CTA shares that minimise the largest predicted slowdown t(c_j) / t(sms): bisection
+    on the slowdown for the fewest CTAs each job needs, then leftover CTAs one at a time to
+    the job that is slowest. Returns (predicted slowdowns, shares), or (None, None) when
+    the jobs need more than one CTA each than there are SMs."""
+    n = len(costs)
+    if n == 0:
+        return [], []
+    if n > sms:
+        return None, None
+
+    def need(sd):
+        cs = [c.ctas_for(sd) for c in costs]
+        return None if any(c is None for c in cs) else cs
+
+    lo, hi = 1.0, 2.0
+    while need(hi) is None or sum(need(hi)) > sms:
+        hi *= 2.0
+        if hi > 1e7:
+            return None, None
+    for _ in range(60):
+        mid = 0.5 * (lo + hi)
+        cs = need(mid)
+        if cs is not None and sum(cs) <= sms:
+            hi = mid
+        else:
+            lo = mid
+    shares = need(hi)
+    left = sms - sum(shares)
+    while left > 0:
+        j = max(range(n), key=lambda i: costs[i].step(shares[i]) / costs[i].alone)
+        shares[j] += 1
+        left -= 1
+    return [c.step(s) / c.alone for c, s in zip(costs, shares)], shares
+
+
+def calibrate(capi, keys, precision, tol, steps=6, low=12):
+    """Cost per (grid, ncell): each configuration alone on the GPU, bootstrapped through
+    the same calls the loop makes, then timed on all SMs and (FP32+refine) on `low` CTAs.
+    The first system only warms up the library."""
+    sms = capi.mzb_sm_count()
+    out = {}
+    order = [min(keys)] + sorted(keys)
+    for i, key in enumerate(order):
+        n_grid, ncell = key
+        job = Job(jid=-1, arrival=0, ncell=ncell, n_grid=n_grid, density=1.35, steps=steps,
+                  integrator="VERLET", seed=1)
+        h = capi.mzb_system_create()
+        run = make_run(capi, job, precision, tol)
+        t0 = time.perf_counter()
+        run.initialize()
+        boot = time.perf_counter() - t0
+        if precision == 1:
+            hs, cls, one = (np.array([h], dtype=np.int32), np.zeros(1, dtype=np.int32),
+                            np.ones(1, dtype=np.int32))
+            timed = []
+            for ctas in (sms, low):
+                c = np.array([ctas], dtype=np.int32)
+                capi.mzb_batch_classes(hs, cls, 1, c, 3 * one, 1)  # the three graphs of this share
+                t1 = time.perf_counter()
+                capi.mzb_batch_classes(hs, cls, 1, c, steps * one, 1)
+                timed.append((time.perf_counter() - t1) / steps)
+            cost = fit_cost(boot, timed[0], timed[1], sms, low)
+        else:
+            capi.solver_md_step(1)
+            t1 = time.perf_counter()
+            capi.solver_md_step(steps)
+            t_all = (time.perf_counter() - t1) / steps
+            cost = Cost(boot=boot, a=t_all, b=0.0, sms=sms)
+        capi.mzb_system_destroy(h)
+        if i > 0:
+            out[key] = cost
+    return out
+
+
+# -- the loop --------------------------------------------------------------------------
+
 class Server:
     """Admission + continuous batching over one library instance (see module doc)."""
 
-    def __init__(self, capi, budget_gb=150.0, max_slots=64, chunk=10, precision=1, tol=1e-10, collect=False):
+    def __init__(self, capi, costs=None, budget_gb=150.0, max_slots=64, chunk=10, precision=1, tol=1e-10,
+                 policy="shared", beta=1.5, call_ms=25.0, admit_per_call=1, collect=False):
         self.capi = capi
+        self.costs = costs or {}
         self.collect = collect  # keep each job's final positions/velocities/forces
         self.budget = budget_gb * 1e9
         self.max_slots = max_slots
         self.chunk = chunk
         self.precision = precision
         self.tol = tol
+        self.policy = policy if precision == 1 else "sequential"
+        self.beta = beta
+        self.call_s = call_ms * 1e-3
+        # bootstraps run between calls and stall every active job: at most this many per
+        # call (0 = no limit), so that a job admitted starts stepping promptly
+        self.admit_per_call = admit_per_call
+        self.sms = capi.mzb_sm_count()
+        self.interference = 1.0  # measured call time / predicted, smoothed over calls
         self.active = []
         self.used = 0.0
         self.steps_done = 0
-        self.occupancy = []   # active jobs per chunk
+        self.occupancy = []      # active jobs per call
+        self.queued = []         # jobs waiting for admission per call
+        self.predicted = []      # largest predicted slowdown per call
         self.autotuned = {}
+        self.seconds = {"calls": 0.0, "admit": 0.0, "retire": 0.0, "plan": 0.0}
+
+    def cost(self, job):
+        if job.key not in self.costs:
+            raise KeyError(f"no calibrated cost for grid {job.n_grid}, ncell {job.ncell}")
+        return self.costs[job.key]
 
     def fits(self, job):
-        return len(self.active) < self.max_slots and self.used + job.footprint <= self.budget
+        if len(self.active) >= self.max_slots or self.used + job.footprint > self.budget:
+            return False
+        if self.policy != "shared" or not self.active:
+            return True
+        sd, _ = plan_shares([self.cost(j) for j in self.active + [job]], self.sms)
+        return sd is not None and max(sd) * self.interference <= self.beta
 
     def admit(self, job, now):
         c = self.capi
@@ -129,25 +284,53 @@ class Server:
         self.active.remove(job)
         self.used -= job.footprint
 
-    def advance(self, k):
+    def plan(self):
+        """Shares and step counts of the next call (policy shared)."""
+        costs = [self.cost(j) for j in self.active]
+        sd, shares = plan_shares(costs, self.sms)
+        if sd is None:
+            raise RuntimeError("more active jobs than SMs")
+        times = [c.step(s) for c, s in zip(costs, shares)]
+        span = max(self.call_s, 2.0 * max(times))
+        steps = [max(1, min(j.steps - j.done, int(round(span / t)))) for j, t in zip(self.active, times)]
+        return sd, shares, steps, max(n * t for n, t in zip(steps, times))
+
+    def advance(self):
         c = self.capi
-        if self.precision == 1:
-            handles = np.array([j.handle for j in self.active], dtype=np.int32)
-            # re-tune when the batch's shape (job count to a power of two, largest grid) is new
+        handles = np.array([j.handle for j in self.active], dtype=np.int32)
+        t0 = time.perf_counter()
+        if self.policy == "shared":
+            sd, shares, steps, expect = self.plan()
+            t1 = time.perf_counter()
+            self.seconds["plan"] += t1 - t0
+            rc = c.mzb_batch_classes(handles, np.arange(len(handles), dtype=np.int32), len(handles),
+                                     np.array(shares, dtype=np.int32), np.array(steps, dtype=np.int32),
+                                     len(handles))
+            wall = time.perf_counter() - t1
+            self.interference = 0.7 * self.interference + 0.3 * max(1.0, wall / expect)
+            self.predicted.append(max(sd))
+        elif self.policy == "lockstep":
+            k = min(self.chunk, min(j.steps - j.done for j in self.active))
             key = (1 << len(self.active).bit_length(), max(j.n_grid for j in self.active))
             if key not in self.autotuned and len(self.active) > 1:
                 out = np.zeros(4)
                 c.mzb_batch_autotune(handles, len(handles), out)
                 self.autotuned[key] = out.tolist()
-            if c.mzb_batch_step(handles, len(handles), k) != 0:
-                raise RuntimeError("a field solve did not converge")
+            rc = c.mzb_batch_step(handles, len(handles), k)
+            steps = [k] * len(self.active)
         else:
+            k = min(self.chunk, min(j.steps - j.done for j in self.active))
+            rc = 0
             for j in self.active:
                 c.mzb_system_select(j.handle)
                 c.solver_md_step(k)
-        for j in self.active:
+            steps = [k] * len(self.active)
+        self.seconds["calls"] += time.perf_counter() - t0
+        if rc != 0:
+            raise RuntimeError("a field solve did not converge")
+        for j, k in zip(self.active, steps):
             j.done += k
-        self.steps_done += k * len(self.active)
+        self.steps_done += sum(steps)
         self.occupancy.append(len(self.active))
 
     def serve(self, jobs):
@@ -160,63 +343,62 @@ class Server:
         t0 = time.perf_counter()
         while pending or self.active:
             now = time.perf_counter() - t0
-            while pending and pending[0].arrival <= now and self.fits(pending[0]):
+            ta = time.perf_counter()
+            n_adm = 0
+            while (pending and pending[0].arrival <= now and self.fits(pending[0])
+                   and (self.admit_per_call <= 0 or n_adm < self.admit_per_call)):
                 self.admit(pending.pop(0), time.perf_counter() - t0)
+                n_adm += 1
+            self.seconds["admit"] += time.perf_counter() - ta
             if not self.active:
                 time.sleep(max(0.0, min(pending[0].arrival - now, 0.05)))
                 continue
-            k = min(self.chunk, min(j.steps - j.done for j in self.active))
-            self.advance(k)
+            self.queued.append(sum(1 for j in pending if j.arrival <= now))
+            self.advance()
             now = time.perf_counter() - t0
+            tr = time.perf_counter()
             for j in [j for j in self.active if j.done >= j.steps]:
                 self.retire(j, now)
+            self.seconds["retire"] += time.perf_counter() - tr
         return jobs
 
 
-def isolated_step_times(capi, jobs, precision, tol, steps=5):
-    """Per (grid, ncell, integrator): seconds of the bootstrap and of one step, the job
-    alone on the GPU through the same calls the loop makes."""
-    out = {}
-    for key in sorted({(j.n_grid, j.ncell, j.integrator) for j in jobs}):
-        n_grid, ncell, itg = key
-        job = Job(jid=-1, arrival=0, ncell=ncell, n_grid=n_grid, density=1.35, steps=steps,
-                  integrator=itg, seed=1)
-        h = capi.mzb_system_create()
-        run = make_run(capi, job, precision, tol)
-        t0 = time.perf_counter()
-        run.initialize()
-        t1 = time.perf_counter()
-        hs = np.array([h], dtype=np.int32)
-        if precision == 1:
-            capi.mzb_batch_step(hs, 1, 3)  # the three step graphs of this system
-            t1b = time.perf_counter()
-            capi.mzb_batch_step(hs, 1, steps)
-        else:
-            capi.solver_md_step(1)
-            t1b = time.perf_counter()
-            capi.solver_md_step(steps)
-        t2 = time.perf_counter()
-        capi.mzb_system_destroy(h)
-        out[key] = (t1 - t0, (t2 - t1b) / steps)  # the warm-up steps are in neither
-    return out
-
-
-def summarize(jobs, server, iso, wall):
-    lat = np.array([j.finished - j.arrival for j in jobs])
-    alone = np.array([iso[(j.n_grid, j.ncell, j.integrator)][0] + j.steps * iso[(j.n_grid, j.ncell, j.integrator)][1]
-                      for j in jobs])
+def summarize(jobs, server, costs, wall):
+    lat = np.array([j.finished - j.admitted for j in jobs])
+    lat_q = np.array([j.finished - j.arrival for j in jobs])
+    alone = np.array([costs[j.key].boot + j.steps * costs[j.key].alone for j in jobs])
     slow = lat / alone
     total_steps = sum(j.steps for j in jobs)
+    occ = np.array(server.occupancy) if server.occupancy else np.zeros(1)
+    queued = np.array(server.queued) if server.queued else np.zeros(1)
     return {
+        "jobs": len(jobs), "job_steps": total_steps, "wall_s": wall,
+        "steps_per_s": total_steps / wall,
         "sequential_alone_steps_per_s": total_steps / float(alone.sum()),
-        "jobs": len(jobs),
         "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
         "p50_slowdown_vs_alone": float(np.percentile(slow, 50)),
         "p99_slowdown_vs_alone": float(np.percentile(slow, 99)),
-        "steps_per_s": total_steps / wall, "job_steps": total_steps, "wall_s": wall,
-        "mean_active_jobs": float(np.mean(server.occupancy)) if server.occupancy else 0.0,
-        "max_active_jobs": int(max(server.occupancy)) if server.occupancy else 0,
+        "max_slowdown_vs_alone": float(slow.max()),
+        "p50_latency_with_queue_s": float(np.percentile(lat_q, 50)),
+        "p99_latency_with_queue_s": float(np.percentile(lat_q, 99)),
+        "mean_active_jobs": float(occ.mean()), "max_active_jobs": int(occ.max()),
+        "calls_with_jobs_waiting": float(np.mean(queued > 0)),
+        "latency_from": "admission (bootstrap included); queueing reported apart",
+        "calls": len(server.occupancy),
+        "seconds_in": {k: round(v, 3) for k, v in server.seconds.items()},
     }
+
+
+def job_records(jobs, costs):
+    """Per job: configuration, timestamps, time alone and slowdown."""
+    out = []
+    for j in jobs:
+        alone = costs[j.key].boot + j.steps * costs[j.key].alone
+        out.append({"jid": j.jid, "grid": j.n_grid, "n_ions": j.n_ions, "steps": j.steps,
+                    "integrator": j.integrator, "arrival": j.arrival, "admitted": j.admitted,
+                    "finished": j.finished, "boot_alone_s": costs[j.key].boot, "alone_s": alone,
+                    "slowdown": (j.finished - j.admitted) / alone})
+    return out
 
 
 def main():
@@ -230,25 +412,39 @@ def main():
     ap.add_argument("--steps-max", type=int, default=500)
     ap.add_argument("--budget-gb", type=float, default=150.0)
     ap.add_argument("--slots", type=int, default=64)
-    ap.add_argument("--chunk", type=int, default=10)
+    ap.add_argument("--chunk", type=int, default=10, help="steps per call (lockstep, sequential)")
     ap.add_argument("--precision", type=int, default=1, choices=[0, 1])
     ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--policy", default="shared", choices=["shared", "lockstep"])
+    ap.add_argument("--beta", type=float, default=1.5, help="admission bound on predicted slowdown (shared)")
+    ap.add_argument("--call-ms", type=float, default=25.0, help="target length of one call (shared)")
+    ap.add_argument("--admit-per-call", type=int, default=1, help="bootstraps between two calls (0: no limit)")
+    ap.add_argument("--jobs-out", default=None, help="write per-job records (JSON) to this file")
     args = ap.parse_args()
     os.environ.setdefault("MZB_QUIET", "1")
     capi = CAPI()
     jobs = job_stream(args.seed, args.rate, args.duration, args.n_min, args.n_max,
                       (args.steps_min, args.steps_max))
-    server = Server(capi, args.budget_gb, args.slots, args.chunk, args.precision, args.tol)
+    t0 = time.perf_counter()
+    costs = calibrate(capi, {j.key for j in jobs}, args.precision, args.tol)
+    calib_s = time.perf_counter() - t0
+    server = Server(capi, costs, args.budget_gb, args.slots, args.chunk, args.precision, args.tol,
+                    policy=args.policy, beta=args.beta, call_ms=args.call_ms, admit_per_call=args.admit_per_call)
     t0 = time.perf_counter()
     server.serve(jobs)
     wall = time.perf_counter() - t0
-    iso = isolated_step_times(capi, jobs, args.precision, args.tol)
     line = {"form": "served", "precision": "fp32_refine" if args.precision else "fp64",
+            "policy": server.policy, "beta": args.beta if server.policy == "shared" else None,
+            "call_ms": args.call_ms, "admit_per_call": args.admit_per_call,
             "rate_per_s": args.rate, "arrival_window_s": args.duration, "seed": args.seed,
-            "budget_gb": args.budget_gb, "slots": args.slots, "chunk": args.chunk,
-            **summarize(jobs, server, iso, wall),
-            "autotuned": {str(k): v for k, v in list(server.autotuned.items())[:4]}}
+            "budget_gb": args.budget_gb, "slots": args.slots, "calibration_s": calib_s,
+            **summarize(jobs, server, costs, wall),
+            "mean_predicted_slowdown": float(np.mean(server.predicted)) if server.predicted else None,
+            "interference": server.interference}
     print(json.dumps(line), flush=True)
+    if args.jobs_out:
+        with open(args.jobs_out, "w") as f:
+            json.dump(job_records(jobs, costs), f)
 
 
 if __name__ == "__main__":

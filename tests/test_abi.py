@@ -9,7 +9,7 @@ import re
 from conftest import ROOT
 from maze_poisson_b200.c_api import EXTENSION_SYMBOLS, REFERENCE_SYMBOLS, CAPI
 
-DECL = re.compile(r"^\s*(?:int|void|double|char\s*\*|uint64_t)\s*\*?\s*([a-z_0-9]+)\s*\(", re.M)
+DECL = re.compile(r"^\s*(?:int|void|double|char\s*\*|uint64_t|size_t)\s*\*?\s*([a-z_0-9]+)\s*\(", re.M)
 
 
 def declared():

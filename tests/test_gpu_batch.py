@@ -94,3 +94,35 @@ def test_batch_of_one_matches_per_call(prod):
             assert rel(st[key], ref[key]) < TOL, (key, rel(st[key], ref[key]))
     finally:
         prod.mzb_system_destroy(h1)
+
+
+def test_classes_match_alone(prod):
+    """Size classes side by side (mzb_batch_classes): the 32^3 and 48^3 systems form one
+    class on 6 CTAs, the 64^3 system another on 20; over two calls the first class takes
+    4 + 2 steps and the second 2 + 1, and each result equals the system stepped alone for
+    its own step count."""
+    class_of = [0, 0, 1]
+    totals = [6, 3]
+    alone = []
+    for k, spec in enumerate(SPECS):
+        h, run = new_run(prod, k, spec)
+        for _ in range(totals[class_of[k]]):
+            run.step()
+        alone.append(run.state(fields=False))
+        assert prod.mzb_system_destroy(h) == 0
+
+    runs = [new_run(prod, k, spec) for k, spec in enumerate(SPECS)]
+    handles = np.array([h for h, _ in runs], dtype=np.int32)
+    cls = np.array(class_of, dtype=np.int32)
+    ctas = np.array([6, 20], dtype=np.int32)
+    try:
+        for steps in ([4, 2], [2, 1]):
+            assert prod.mzb_batch_classes(handles, cls, len(handles), ctas, np.array(steps, dtype=np.int32), 2) == 0
+        for (h, run), ref in zip(runs, alone):
+            assert prod.mzb_system_select(h) == 0
+            st = run.state(fields=False)
+            for key in ("pos", "vel", "fcs_tot", "fcs_elec", "fcs_noel"):
+                assert rel(st[key], ref[key]) < TOL, (h, key, rel(st[key], ref[key]))
+    finally:
+        for h, _ in runs:
+            prod.mzb_system_destroy(h)
