@@ -206,7 +206,7 @@ void ensure_mixed_levels(GridState& G) {
 void free_particles(ParticleDev& P) {
     dfree(P.types); dfree(P.pos); dfree(P.vel); dfree(P.fe); dfree(P.fn); dfree(P.ft);
     dfree(P.mass); dfree(P.chg); dfree(P.tab); dfree(P.base);
-    dfree(P.tile_count); dfree(P.tile_start); dfree(P.tile_fill); dfree(P.tile_ions);
+    dfree(P.tile_count); dfree(P.tile_start); dfree(P.tile_fill); dfree(P.tile_ions); dfree(P.tile_part);
     dfree(P.cell_of); dfree(P.cell_count); dfree(P.cell_start); dfree(P.cell_fill);
     dfree(P.cell_ions); dfree(P.srank); dfree(P.spos); dfree(P.stype); dfree(P.fpart);
     dfree(P.epart); dfree(P.red); dfree(P.flags); dfree(P.partial);
@@ -650,6 +650,7 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
     P.tile_count = dalloc<int32_t>(P.ntiles);
     P.tile_start = dalloc<int32_t>(P.ntiles + 1);
     P.tile_fill = dalloc<int32_t>(P.ntiles);
+    P.tile_part = dalloc<int32_t>((P.ntiles + 1023) / 1024);
     P.tile_ions = dalloc<int32_t>(n_p);
     // linked cells
     P.cell_of = dalloc<int32_t>(n_p);

@@ -1,4 +1,6 @@
 // Particle-side kernels (see particles.cuh). FP64, compiled with --fmad=false.
+#include <climits>
+
 #include "particles.cuh"
 
 namespace mzb {
@@ -63,9 +65,10 @@ __device__ __forceinline__ void corner_offsets(int c, int& di, int& dj, int& dk)
 
 // ------------------------------------------------------------------------------------
 // Exclusive scan of count[0..m) into start[0..m] (start[m] = total); start is also copied
-// into fill[0..m) as a scatter cursor. One block of 1024 threads taking the counts in
-// coalesced rounds of 1024 with a running carry. Optionally sums `part[0..np_part)` in
-// index order into *sum_out.
+// into fill[0..m) as a scatter cursor. One block of 1024 threads: thread t takes the
+// contiguous chunk [t C, (t + 1) C) (C a multiple of 4, read as int4 where the chunk is
+// whole), so every load is issued before the one block-wide scan of the chunk totals.
+// Optionally sums `part[0..np_part)` in index order into *sum_out.
 // ------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(1024) k_scan(const int32_t* __restrict__ count, int m,
                                                int32_t* __restrict__ start, int32_t* __restrict__ fill,
@@ -73,37 +76,52 @@ __global__ void __launch_bounds__(1024) k_scan(const int32_t* __restrict__ count
                                                double* __restrict__ sum_out) {
     __shared__ int32_t wsum[32];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
-    int32_t carry = 0;
-    for (int base = 0; base < m; base += blockDim.x) {
-        const int x = base + t;
-        const int32_t v = x < m ? count[x] : 0;
-        int32_t incl = v;
+    const int C = (((m + (int)blockDim.x - 1) / (int)blockDim.x) + 3) & ~3;
+    const int lo = min(m, t * C), hi = min(m, lo + C);
+    const int hv = lo + ((hi - lo) & ~3);  // end of the whole int4 groups
+    int32_t tot = 0;
+    for (int x = lo; x < hv; x += 4) {
+        const int4 v = *reinterpret_cast<const int4*>(count + x);
+        tot += v.x + v.y + v.z + v.w;
+    }
+    for (int x = hv; x < hi; x++) tot += count[x];
+    int32_t incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int32_t y = lane < nw ? wsum[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int32_t u = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += u;
+            const int32_t u = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += u;
         }
-        if (lane == 31) wsum[w] = incl;
-        __syncthreads();
-        if (w == 0) {
-            int32_t y = lane < nw ? wsum[lane] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int32_t u = __shfl_up_sync(0xffffffffu, y, o);
-                if (lane >= o) y += u;
-            }
-            wsum[lane] = y;
-        }
-        __syncthreads();
-        const int32_t excl = carry + incl - v + (w > 0 ? wsum[w - 1] : 0);
-        if (x < m) {
-            start[x] = excl;
-            fill[x] = excl;
-        }
-        carry += wsum[nw - 1];
-        __syncthreads();
+        wsum[lane] = y;
     }
-    if (t == 0) start[m] = carry;
+    __syncthreads();
+    int32_t run = incl - tot + (w > 0 ? wsum[w - 1] : 0);
+    for (int x = lo; x < hv; x += 4) {
+        const int4 v = *reinterpret_cast<const int4*>(count + x);
+        int4 o;
+        o.x = run;
+        o.y = o.x + v.x;
+        o.z = o.y + v.y;
+        o.w = o.z + v.z;
+        run = o.w + v.w;
+        *reinterpret_cast<int4*>(start + x) = o;
+        *reinterpret_cast<int4*>(fill + x) = o;
+    }
+    for (int x = hv; x < hi; x++) {
+        const int32_t v = count[x];
+        start[x] = run;
+        fill[x] = run;
+        run += v;
+    }
+    if (t == (int)blockDim.x - 1) start[m] = run;
     if (sum_out != nullptr && t == 0) {
         double s = 0.0;
         for (int x = 0; x < np_part; x++) s += part[x];
@@ -111,17 +129,113 @@ __global__ void __launch_bounds__(1024) k_scan(const int32_t* __restrict__ count
     }
 }
 
+// The same scan over many blocks (large m): k_scan_reduce sums the counts of each block
+// of 1024, k_scan_apply scans each block from the sum of the blocks before it (read in
+// block order), coalesced, one count per thread.
+__global__ void __launch_bounds__(1024) k_scan_reduce(const int32_t* __restrict__ count, int m,
+                                                      int32_t* __restrict__ blk) {
+    __shared__ int32_t wsum[32];
+    const int x = blockIdx.x * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int32_t v = x < m ? count[x] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) wsum[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        int32_t y = wsum[lane];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+        if (lane == 0) blk[blockIdx.x] = y;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_scan_apply(const int32_t* __restrict__ count, int m,
+                                                     const int32_t* __restrict__ blk, int32_t* __restrict__ start,
+                                                     int32_t* __restrict__ fill, const double* __restrict__ part,
+                                                     int np_part, double* __restrict__ sum_out) {
+    __shared__ int32_t wsum[32];
+    __shared__ int32_t base_s;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int x = blockIdx.x * 1024 + t;
+    if (w == 0) {
+        int32_t b = 0;
+        for (int u = lane; u < (int)blockIdx.x; u += 32) b += blk[u];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
+        if (lane == 0) base_s = b;
+    }
+    const int32_t v = x < m ? count[x] : 0;
+    int32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int32_t y = wsum[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t u = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += u;
+        }
+        wsum[lane] = y;
+    }
+    __syncthreads();
+    const int32_t excl = base_s + incl - v + (w > 0 ? wsum[w - 1] : 0);
+    if (x < m) {
+        start[x] = excl;
+        fill[x] = excl;
+    }
+    if (x == m - 1) start[m] = excl + v;
+    if (m == 0 && blockIdx.x == 0 && t == 0) start[0] = 0;
+    if (sum_out != nullptr && blockIdx.x == 0 && t == 0) {
+        double s = 0.0;
+        for (int y = 0; y < np_part; y++) s += part[y];
+        *sum_out = s;
+    }
+}
+
+// Exclusive scan of count[0..m) into start (and fill): one block for small m, else the
+// two-kernel form with per-block totals in blk ([ceil(m / 1024)]).
+void scan_counts(const int32_t* count, int m, int32_t* start, int32_t* fill, int32_t* blk, const double* part,
+                 int np_part, double* sum_out, cudaStream_t s) {
+    if (m <= 4096 || blk == nullptr) {
+        count_launch();
+        k_scan<<<1, 1024, 0, s>>>(count, m, start, fill, part, np_part, sum_out);
+        return;
+    }
+    const int nblk = (m + 1023) / 1024;
+    count_launch(2);
+    k_scan_reduce<<<nblk, 1024, 0, s>>>(count, m, blk);
+    k_scan_apply<<<nblk, 1024, 0, s>>>(count, m, blk, start, fill, part, np_part, sum_out);
+}
+
 // ------------------------------------------------------------------------------------
 // Charge spreading
 // ------------------------------------------------------------------------------------
 
 // Per ion: base cell floor(pos/h) (wrapped), tile histogram and the ion's total spread
-// charge (block partial, summed later in block order).
+// charge (block partial, summed later in block order). With q_old non-null (a CIC grid
+// whose only nonzeros are the corners of the bases being replaced) the ion first zeroes
+// the 8 corners of its old base cell.
 template <int CAS>
-__global__ void k_spread_bin(ParticleDev P, int n, double h, double* __restrict__ part) {
+__global__ void k_spread_bin(ParticleDev P, int n, double h, double* __restrict__ part, double* __restrict__ q_old) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     double u = 0.0;
     if (p < P.np) {
+        if (q_old != nullptr) {
+            const int o0 = P.base[3 * p], o1 = P.base[3 * p + 1], o2 = P.base[3 * p + 2];
+            const long n2 = (long)n * n;
+#pragma unroll
+            for (int o = 0; o < 8; o++) {
+                const int i = o0 + (o >> 2) == n ? 0 : o0 + (o >> 2);
+                const int j = o1 + ((o >> 1) & 1) == n ? 0 : o1 + ((o >> 1) & 1);
+                const int k = o2 + (o & 1) == n ? 0 : o2 + (o & 1);
+                q_old[(long)i * n2 + (long)j * n + k] = 0.0;
+            }
+        }
         int b[3];
 #pragma unroll
         for (int d = 0; d < 3; d++) {
@@ -163,9 +277,10 @@ __device__ __forceinline__ bool in_stencil(int g, int b, int n) {
     return (d >= 0 && d <= 3) || (d + n >= 0 && d + n <= 3) || (d - n >= 0 && d - n <= 3);
 }
 
-// One warp per tile (grid-stride over warps): gather the ions whose stencil can reach the
-// tile (base cell in this tile or the 7 tiles below it for CIC, whose +1 corners reach
-// up; in the 27 tiles around it for the splines, whose offsets run -1..2), sort them by
+// Spline spreading (CIC takes k_spread_ions below). One warp per tile (grid-stride over
+// warps): gather the ions whose stencil can reach the tile (base cell in this tile or the
+// 7 tiles below it for CIC, whose +1 corners reach up; in the 27 tiles around it for the
+// splines, whose offsets run -1..2), sort them by
 // ion index, and let every lane sum the contributions of its TI x TJ points (one k column)
 // over those ions in ascending ion order -- for each point the order of the reference's
 // serial scatter (charges.c:123-141), with the same weight expression -- then write the
@@ -295,30 +410,177 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) k_spread_tiles(ParticleDev 
     }
 }
 
+// CIC spreading by ion, into a q that is zero away from the corners written here. Ion
+// p's stencil covers the corners P = b + o, o in {0,1}^3, of its base cell b; the ions
+// that contribute to a corner are those whose base cell is P - {0,1}^3, so every
+// contributor to any of p's corners has its base within one cell of b, in the (at most
+// eight) tiles around b. For each corner the contributor of lowest index writes the
+// corner's value: the contributions summed from 0 in ascending ion order -- the order of
+// the reference's serial scatter (charges.c:123-141), with the same weight expression as
+// k_spread_tiles -- so each point is written once and no atomics touch q.
+//
+// Eight lanes per ion: lane l scans tile l for near ions (base within one cell of b along
+// every axis; usually p alone) into the ion's list in shared memory, then handles corner
+// l. A crowd of more than kNear near ions takes a slower exact path that scans the tiles
+// for each corner.
+constexpr int kNear = 16;
+constexpr int kIonLanes = 8;
+constexpr int kSpreadIonThreads = 128;
+constexpr int kIonsPerCta = kSpreadIonThreads / kIonLanes;
+
+__device__ __forceinline__ int wrap_delta(int d, int n) {  // d in (-n, n) -> (-n/2, n/2]
+    if (2 * d > n) return d - n;
+    if (2 * d <= -n) return d + n;
+    return d;
+}
+
+__device__ __forceinline__ double cic_contrib(const ParticleDev& P, int c, int i, int j, int k, double L, double h) {
+    const double wx = w_cas<CAS_CIC>(P.pos[3 * c] - i * h, L, h);
+    double wgt = wx * w_cas<CAS_CIC>(P.pos[3 * c + 1] - j * h, L, h);
+    wgt = wgt * w_cas<CAS_CIC>(P.pos[3 * c + 2] - k * h, L, h);
+    return P.chg[c] * wgt;
+}
+
+__global__ void __launch_bounds__(kSpreadIonThreads) k_spread_ions(ParticleDev P, double* __restrict__ q, int n,
+                                                                   double h) {
+    __shared__ int near_id_s[kIonsPerCta][kNear];
+    __shared__ int near_o_s[kIonsPerCta][kNear];  // offset code (di+1)*9 + (dj+1)*3 + (dk+1)
+    __shared__ int near_n_s[kIonsPerCta];
+    const int g = threadIdx.x / kIonLanes, sub = threadIdx.x % kIonLanes;
+    const int p = blockIdx.x * kIonsPerCta + g;
+    if (p >= P.np) return;  // whole groups of eight lanes leave together
+    const unsigned gmask = 0xffu << (threadIdx.x & 24);
+    const double L = n * h;
+    const int b0 = P.base[3 * p], b1 = P.base[3 * p + 1], b2 = P.base[3 * p + 2];
+    // the distinct tiles holding the cells b - 1 .. b + 1 (at most two per axis)
+    int ts[2][3], nt[3];
+    {
+        const int bb[3] = {b0, b1, b2}, tsz[3] = {kTileI, kTileJ, kTileK}, ntl[3] = {P.nti, P.ntj, P.ntk};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const int lo = wrapi(bb[d] - 1, n) / tsz[d], hi = wrapi(bb[d] + 1, n) / tsz[d];
+            ts[0][d] = lo;
+            ts[1][d] = hi;
+            nt[d] = lo == hi || ntl[d] == 1 ? 1 : 2;
+        }
+    }
+    auto near_code = [&](int c) {  // offset code of ion c, or -1 if its base is not within one cell
+        const int di = wrap_delta(P.base[3 * c] - b0, n), dj = wrap_delta(P.base[3 * c + 1] - b1, n),
+                  dk = wrap_delta(P.base[3 * c + 2] - b2, n);
+        if (di < -1 || di > 1 || dj < -1 || dj > 1 || dk < -1 || dk > 1) return -1;
+        return (di + 1) * 9 + (dj + 1) * 3 + (dk + 1);
+    };
+    auto tile_of = [&](int l) { return (ts[l >> 2][0] * P.ntj + ts[(l >> 1) & 1][1]) * P.ntk + ts[l & 1][2]; };
+    auto tile_valid = [&](int l) { return (l >> 2) < nt[0] && ((l >> 1) & 1) < nt[1] && (l & 1) < nt[2]; };
+    if (sub == 0) near_n_s[g] = 0;
+    __syncwarp(gmask);
+    if (tile_valid(sub)) {
+        const int tile = tile_of(sub);
+        for (int x = P.tile_start[tile], e1 = P.tile_start[tile + 1]; x < e1; x++) {
+            const int c = P.tile_ions[x];
+            const int code = near_code(c);
+            if (code < 0) continue;
+            const int slot = atomicAdd(&near_n_s[g], 1);
+            if (slot < kNear) {
+                near_id_s[g][slot] = c;
+                near_o_s[g][slot] = code;
+            }
+        }
+    }
+    __syncwarp(gmask);
+    const int nn_all = near_n_s[g];
+    const bool crowd = nn_all > kNear;
+    const int nn = crowd ? kNear : nn_all;
+    const int* near_id = near_id_s[g];
+    const int* near_o = near_o_s[g];
+    // corner o = sub; c contributes to it iff o - (base_c - b) is in {0,1}^3
+    const int oi = sub >> 2, oj = (sub >> 1) & 1, ok = sub & 1;
+    const int i = b0 + oi == n ? 0 : b0 + oi, j = b1 + oj == n ? 0 : b1 + oj, k = b2 + ok == n ? 0 : b2 + ok;
+    auto contributes = [&](int code) {
+        const int ei = oi - (code / 9 - 1), ej = oj - ((code / 3) % 3 - 1), ek = ok - (code % 3 - 1);
+        return ei >= 0 && ei <= 1 && ej >= 0 && ej <= 1 && ek >= 0 && ek <= 1;
+    };
+    double acc = 0.0;
+    if (!crowd) {
+        int owner = p, m = 0;
+        for (int x = 0; x < nn; x++)
+            if (contributes(near_o[x])) {
+                owner = min(owner, near_id[x]);
+                m++;
+            }
+        if (owner != p) return;
+        int last = -1;
+        for (int t = 0; t < m; t++) {  // contributors in ascending ion order
+            int next = INT_MAX;
+            for (int x = 0; x < nn; x++)
+                if (near_id[x] > last && near_id[x] < next && contributes(near_o[x])) next = near_id[x];
+            acc += cic_contrib(P, next, i, j, k, L, h);
+            last = next;
+        }
+    } else {  // the same, scanning the tiles for every contributor
+        auto for_contrib = [&](auto&& f) {
+            for (int l = 0; l < 8; l++) {
+                if (!tile_valid(l)) continue;
+                const int tile = tile_of(l);
+                for (int x = P.tile_start[tile]; x < P.tile_start[tile + 1]; x++) {
+                    const int c = P.tile_ions[x];
+                    const int code = near_code(c);
+                    if (code >= 0 && contributes(code)) f(c);
+                }
+            }
+        };
+        int owner = p;
+        for_contrib([&](int c) { owner = min(owner, c); });
+        if (owner != p) return;
+        int last = -1;
+        while (true) {
+            int next = INT_MAX;
+            for_contrib([&](int c) {
+                if (c > last && c < next) next = c;
+            });
+            if (next == INT_MAX) break;
+            acc += cic_contrib(P, next, i, j, k, L, h);
+            last = next;
+        }
+    }
+    q[((long)i * n + j) * n + k] = acc;
+}
+
 void spread_charges(ParticleDev& P, double* q, int n, double h, cudaStream_t s) {
     const int nb = (P.np + 127) / 128;
     MZB_CHECK(cudaMemsetAsync(P.tile_count, 0, sizeof(int32_t) * P.ntiles, s));
+    // CIC: q keeps zeros away from the ions' corners, so only the old corners need
+    // clearing when q holds the last CIC spreading of these ions; otherwise clear it all
+    const bool sparse = P.cas == CAS_CIC && P.q_sparse == q;
+    if (P.cas == CAS_CIC && !sparse) MZB_CHECK(cudaMemsetAsync(q, 0, sizeof(double) * (size_t)n * n * n, s));
     count_launch();
     if (P.cas == CAS_CIC)
-        k_spread_bin<CAS_CIC><<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial);
+        k_spread_bin<CAS_CIC><<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial, sparse ? q : nullptr);
     else if (P.cas == CAS_SPL_QUADR)
-        k_spread_bin<CAS_SPL_QUADR><<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial);
+        k_spread_bin<CAS_SPL_QUADR><<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial, nullptr);
     else
-        k_spread_bin<CAS_SPL_CUBIC><<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial);
-    count_launch();
-    k_scan<<<1, 1024, 0, s>>>(P.tile_count, P.ntiles, P.tile_start, P.tile_fill, P.partial,
-                              nb > 0 ? nb : 1, P.red + 0);
+        k_spread_bin<CAS_SPL_CUBIC><<<nb > 0 ? nb : 1, 128, 0, s>>>(P, n, h, P.partial, nullptr);
+    scan_counts(P.tile_count, P.ntiles, P.tile_start, P.tile_fill, P.tile_part, P.partial, nb > 0 ? nb : 1,
+                P.red + 0, s);
     if (nb > 0) count_launch();
     if (nb > 0) k_spread_fill<<<nb, 128, 0, s>>>(P);
+    if (P.cas == CAS_CIC) {  // the corners the ions reach (q is zero elsewhere)
+        if (P.np > 0) {
+            count_launch();
+            k_spread_ions<<<(P.np + kIonsPerCta - 1) / kIonsPerCta, kSpreadIonThreads, 0, s>>>(P, q, n, h);
+        }
+        MZB_CHECK(cudaGetLastError());
+        P.q_sparse = q;
+        return;
+    }
+    P.q_sparse = nullptr;  // the tile kernel writes every point
     int dev, sms;
     MZB_CHECK(cudaGetDevice(&dev));
     MZB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const int ctas = (P.ntiles + kSpreadWarps - 1) / kSpreadWarps;
     const int grid = ctas < sms * 12 ? ctas : sms * 12;
     count_launch();
-    if (P.cas == CAS_CIC)
-        k_spread_tiles<CAS_CIC><<<grid, kSpreadWarps * 32, 0, s>>>(P, q, n, h);
-    else if (P.cas == CAS_SPL_QUADR)
+    if (P.cas == CAS_SPL_QUADR)
         k_spread_tiles<CAS_SPL_QUADR><<<grid, kSpreadWarps * 32, 0, s>>>(P, q, n, h);
     else
         k_spread_tiles<CAS_SPL_CUBIC><<<grid, kSpreadWarps * 32, 0, s>>>(P, q, n, h);
@@ -328,18 +590,28 @@ void spread_charges(ParticleDev& P, double* q, int n, double h, cudaStream_t s) 
 // ------------------------------------------------------------------------------------
 // Field forces: central differences of phi at the stencil points (forces.c:26-100).
 // ------------------------------------------------------------------------------------
+// Eight lanes per ion: lane l takes the stencil points c = l, l + 8, ... (one for CIC, 8
+// for the splines) and the ion's sums are then formed from 0 in the stencil's order c = 0,
+// 1, 2, ... by shuffling each term to the lanes in turn -- the reference's order, so the
+// forces are bit-exact -- and written by the first lane.
+constexpr int kForceLanes = 8;
+
 template <int CAS>
-__global__ void k_field_forces(ParticleDev P, const double* __restrict__ phi, int n, double h) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= P.np) return;
+__global__ void __launch_bounds__(128) k_field_forces(ParticleDev P, const double* __restrict__ phi, int n, double h) {
+    constexpr int S = stencil_size<CAS>(), T = S / kForceLanes;
+    const int p = (blockIdx.x * blockDim.x + threadIdx.x) / kForceLanes, sub = threadIdx.x % kForceLanes;
+    if (p >= P.np) return;  // whole groups of eight lanes leave together
+    const unsigned gmask = 0xffu << (threadIdx.x & 24);
+    const int g0 = threadIdx.x & 31 & ~(kForceLanes - 1);
     const double L = n * h, h2 = 2.0 * h;
     const long n2 = (long)n * n;
     const int* b = P.base + 3 * p;
     const double px = P.pos[3 * p], py = P.pos[3 * p + 1], pz = P.pos[3 * p + 2], chg = P.chg[p];
-    double fx = 0.0, fy = 0.0, fz = 0.0;
-    for (int c = 0; c < stencil_size<CAS>(); c++) {
+    double tx[T], ty[T], tz[T];
+#pragma unroll
+    for (int u = 0; u < T; u++) {
         int i, j, k;
-        stencil_point<CAS>(c, b, n, i, j, k);
+        stencil_point<CAS>(u * kForceLanes + sub, b, n, i, j, k);
         double qc = chg * w_cas<CAS>(px - i * h, L, h);
         qc = qc * w_cas<CAS>(py - j * h, L, h);
         qc = qc * w_cas<CAS>(pz - k * h, L, h);
@@ -347,19 +619,30 @@ __global__ void k_field_forces(ParticleDev P, const double* __restrict__ phi, in
         const long ip = (long)wrap_inc(i, n) * n2, im = (long)wrap_dec(i, n) * n2;
         const long jp = (long)wrap_inc(j, n) * n, jm = (long)wrap_dec(j, n) * n;
         const int kp = wrap_inc(k, n), km = wrap_dec(k, n);
-        fx += qc * ((phi[im + j0 + k] - phi[ip + j0 + k]) / h2);
-        fy += qc * ((phi[i0 + jm + k] - phi[i0 + jp + k]) / h2);
-        fz += qc * ((phi[i0 + j0 + km] - phi[i0 + j0 + kp]) / h2);
+        tx[u] = qc * ((phi[im + j0 + k] - phi[ip + j0 + k]) / h2);
+        ty[u] = qc * ((phi[i0 + jm + k] - phi[i0 + jp + k]) / h2);
+        tz[u] = qc * ((phi[i0 + j0 + km] - phi[i0 + j0 + kp]) / h2);
     }
-    P.fe[3 * p] = fx;
-    P.fe[3 * p + 1] = fy;
-    P.fe[3 * p + 2] = fz;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+#pragma unroll
+    for (int u = 0; u < T; u++)
+#pragma unroll
+        for (int l = 0; l < kForceLanes; l++) {
+            fx += __shfl_sync(gmask, tx[u], g0 + l);
+            fy += __shfl_sync(gmask, ty[u], g0 + l);
+            fz += __shfl_sync(gmask, tz[u], g0 + l);
+        }
+    if (sub == 0) {
+        P.fe[3 * p] = fx;
+        P.fe[3 * p + 1] = fy;
+        P.fe[3 * p + 2] = fz;
+    }
 }
 
 void field_forces(ParticleDev& P, const double* phi, int n, double h, cudaStream_t s) {
     if (P.np == 0) return;
     count_launch();
-    const int nb = (P.np + 127) / 128;
+    const int nb = (P.np * kForceLanes + 127) / 128;
     if (P.cas == CAS_CIC)
         k_field_forces<CAS_CIC><<<nb, 128, 0, s>>>(P, phi, n, h);
     else if (P.cas == CAS_SPL_QUADR)
@@ -400,22 +683,41 @@ __global__ void k_cell_fill(ParticleDev P) {
     P.cell_ions[slot] = p;
 }
 
-// One thread per cell: restore ascending ion order inside the cell (the scatter above is
-// unordered), then gather positions/types into cell order and record each ion's rank.
-__global__ void k_cell_sort_gather(ParticleDev P) {
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per cell: restore ascending ion order inside the cell (the scatter above is
+// unordered) by ranking each ion against the cell's others (ion indices are distinct, so
+// the ranks are a permutation; a cell of more than kCellStage ions is insertion-sorted by
+// one lane), then gather positions/types into cell order and record each ion's rank.
+constexpr int kCellStage = 256;
+
+__global__ void __launch_bounds__(128) k_cell_sort_gather(ParticleDev P) {
+    __shared__ int stage_all[4][kCellStage];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cell = blockIdx.x * 4 + w;
     if (cell >= P.ncell) return;
-    const int b = P.cell_start[cell], e = P.cell_start[cell + 1];
-    for (int x = b + 1; x < e; x++) {
-        const int v = P.cell_ions[x];
-        int y = x - 1;
-        while (y >= b && P.cell_ions[y] > v) {
-            P.cell_ions[y + 1] = P.cell_ions[y];
-            y--;
+    const int b = P.cell_start[cell], e = P.cell_start[cell + 1], m = e - b;
+    int* st = stage_all[w];
+    if (m <= kCellStage) {
+        for (int x = lane; x < m; x += 32) st[x] = P.cell_ions[b + x];
+        __syncwarp();
+        for (int x = lane; x < m; x += 32) {
+            const int v = st[x];
+            int r = 0;
+            for (int y = 0; y < m; y++) r += st[y] < v;
+            P.cell_ions[b + r] = v;
         }
-        P.cell_ions[y + 1] = v;
+    } else if (lane == 0) {
+        for (int x = b + 1; x < e; x++) {
+            const int v = P.cell_ions[x];
+            int y = x - 1;
+            while (y >= b && P.cell_ions[y] > v) {
+                P.cell_ions[y + 1] = P.cell_ions[y];
+                y--;
+            }
+            P.cell_ions[y + 1] = v;
+        }
     }
-    for (int x = b; x < e; x++) {
+    __syncwarp();
+    for (int x = b + lane; x < e; x += 32) {
         const int p = P.cell_ions[x];
         P.spos[3 * x] = P.pos[3 * p];
         P.spos[3 * x + 1] = P.pos[3 * p + 1];
@@ -435,7 +737,7 @@ void build_cells(ParticleDev& P, cudaStream_t s) {
     if (P.np > 0) count_launch();
     if (P.np > 0) k_cell_fill<<<(P.np + 127) / 128, 128, 0, s>>>(P);
     count_launch();
-    k_cell_sort_gather<<<(P.ncell + 127) / 128, 128, 0, s>>>(P);
+    k_cell_sort_gather<<<(P.ncell + 3) / 4, 128, 0, s>>>(P);
     MZB_CHECK(cudaGetLastError());
 }
 

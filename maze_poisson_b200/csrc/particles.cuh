@@ -32,6 +32,10 @@ struct ParticleDev {
     double* tab = nullptr;   // [ntyp*ntyp][7] pair-potential constants per type pair
     int32_t* base = nullptr; // [np][3] base cell floor(pos/h) (wrapped)
     int cas = CAS_CIC;       // charge assignment scheme
+    // the charge grid whose only nonzeros are the CIC corners of `base` (left by the last
+    // CIC spreading into it), or null: the next CIC spreading into it zeroes those corners
+    // instead of the whole grid
+    const double* q_sparse = nullptr;
     int pot = POT_TF;        // pair potential
 
     // spreading bins
@@ -40,6 +44,7 @@ struct ParticleDev {
     int32_t* tile_start = nullptr;   // [ntiles+1]
     int32_t* tile_fill = nullptr;    // [ntiles]
     int32_t* tile_ions = nullptr;    // [np]
+    int32_t* tile_part = nullptr;    // [ceil(ntiles / 1024)] per-block totals of the tile scan
 
     // linked cells (Tosi-Fumi)
     int nc = 0, ncell = 0;
