@@ -63,6 +63,21 @@ __device__ __forceinline__ void corner_offsets(int c, int& di, int& dj, int& dk)
     dk = (c == 3 || c == 5 || c == 6 || c == 7);
 }
 
+// part[0] + part[1] + ... + part[n-1], added from 0 in index order, by one whole warp: the
+// lanes load 32 values at a time and lane 0's running sum takes them in turn by shuffles
+// (the result of a serial loop, without its chain of dependent loads). Every lane
+// returns the sum.
+__device__ __forceinline__ double warp_ordered_sum(const double* part, int n) {
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int c = 0; c < n; c += 32) {
+        const double v = c + lane < n ? part[c + lane] : 0.0;
+        const int k = min(32, n - c);
+        for (int y = 0; y < k; y++) s += __shfl_sync(0xffffffffu, v, y);
+    }
+    return s;
+}
+
 // ------------------------------------------------------------------------------------
 // Exclusive scan of count[0..m) into start[0..m] (start[m] = total); start is also copied
 // into fill[0..m) as a scatter cursor. One block of 1024 threads: thread t takes the
@@ -122,10 +137,9 @@ __global__ void __launch_bounds__(1024) k_scan(const int32_t* __restrict__ count
         run += v;
     }
     if (t == (int)blockDim.x - 1) start[m] = run;
-    if (sum_out != nullptr && t == 0) {
-        double s = 0.0;
-        for (int x = 0; x < np_part; x++) s += part[x];
-        *sum_out = s;
+    if (sum_out != nullptr && w == 0) {
+        const double s = warp_ordered_sum(part, np_part);
+        if (lane == 0) *sum_out = s;
     }
 }
 
@@ -190,10 +204,9 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const int32_t* __restrict__
     }
     if (x == m - 1) start[m] = excl + v;
     if (m == 0 && blockIdx.x == 0 && t == 0) start[0] = 0;
-    if (sum_out != nullptr && blockIdx.x == 0 && t == 0) {
-        double s = 0.0;
-        for (int y = 0; y < np_part; y++) s += part[y];
-        *sum_out = s;
+    if (sum_out != nullptr && blockIdx.x == 0 && w == 0) {
+        const double s = warp_ordered_sum(part, np_part);
+        if (lane == 0) *sum_out = s;
     }
 }
 

@@ -206,12 +206,15 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
 }
 
 // Each ion's force: its super-tile partials in list order, scattered back to ion order.
+// A warp per block of 32 cell-ordered ions: the block's list is walked once for all 32
+// lanes (one ion each), whose partials lie side by side.
 __global__ void k_tf_gather(ParticleDev P) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= P.np) return;
-    const int s = P.srank[p], b = s >> 5, lane = s & 31;
+    const int b = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (b >= (P.np + 31) / 32) return;
     double f[3] = {0.0, 0.0, 0.0};
-    for (int e = P.tf_gstart[b]; e < P.tf_gstart[b + 1]; e++) {
+    const int e1 = P.tf_gstart[b + 1];
+#pragma unroll 4
+    for (int e = P.tf_gstart[b]; e < e1; e++) {
         const int ent = P.tf_gent[e];
         const int st = ent >> 4, side = (ent >> 3) & 1, slot = ent & 7;
         const double* o = P.fpart + (((size_t)st * 2 + side) * kTfSb + slot) * 32 * 3 + lane * 3;
@@ -219,6 +222,9 @@ __global__ void k_tf_gather(ParticleDev P) {
         f[1] += o[1];
         f[2] += o[2];
     }
+    const int s = b * 32 + lane;
+    if (s >= P.np) return;
+    const int p = P.cell_ions[s];
     P.fn[3 * p] = f[0];
     P.fn[3 * p + 1] = f[1];
     P.fn[3 * p + 2] = f[2];
@@ -304,7 +310,7 @@ void tf_forces(ParticleDev& P, cudaStream_t s) {
     else
         k_tf<POT_TF><<<P.tf_nst, kTfThreads, kTfSmem, s>>>(P);
     count_launch();
-    k_tf_gather<<<(P.np + 127) / 128, 128, 0, s>>>(P);
+    k_tf_gather<<<(nblk * 32 + 127) / 128, 128, 0, s>>>(P);
     count_launch();
     k_tf_energy<<<1, 1024, 0, s>>>(P);
     MZB_CHECK(cudaGetLastError());
