@@ -217,6 +217,20 @@ void free_particles(ParticleDev& P) {
 
 // Linked cells that order the ions for the pair-force kernel: about 16 ions per cell, at
 // least one cell per side.
+// r^2 beyond which the Born-Mayer terms of a Tosi-Fumi pair, A B exp(B (sigma - r)) in
+// the force and A exp(B (sigma - r)) in the energy, are both below 1e-21 hartree (/bohr),
+// so the pair-force kernel leaves the exponential out beyond it. Summed over all of an
+// ion's partners (N = 16000: < 2e-17 hartree/bohr) that stays below the rounding of the
+// ion's force sum (~1e-16 for forces of 1e-2 over thousands of pairs); for NaCl it is
+// r ~ 31 bohr of r_cut = 78 at N = 16000.
+double tf_exp_r2_limit(double A, double B, double sg) {
+    const double m = std::max(fabs(A * B), fabs(A));
+    if (m == 0.0) return 0.0;
+    if (!(B > 0.0)) return INFINITY;
+    const double r = sg - log(1e-21 / m) / B;
+    return r > 0.0 ? r * r : 0.0;
+}
+
 void set_cells(ParticleDev& P, int nc) {
     dfree(P.cell_count); dfree(P.cell_start); dfree(P.cell_fill);
     P.nc = nc < 1 ? 1 : nc;
@@ -609,13 +623,13 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
         upload(P.mass, mass, sizeof(double) * n_p);
         upload(P.chg, charges, sizeof(double) * n_p);
     }
-    // pair-potential constants per type pair, 7 doubles each, with the shifted-force
-    // constants at r_cut = L/2
+    // pair-potential constants per type pair, kPairConsts doubles each, with the
+    // shifted-force constants at r_cut = L/2
     P.pot = pot_type;
-    std::vector<double> tab((size_t)n_typ * n_typ * 7, 0.0);
+    std::vector<double> tab((size_t)n_typ * n_typ * kPairConsts, 0.0);
     const double rc = L / 2.0, rc6 = pow(rc, 6), rc7 = rc6 * rc, rc8 = rc7 * rc, rc9 = rc8 * rc;
     for (int t = 0; t < n_typ * n_typ; t++) {
-        double* o = &tab[7 * t];
+        double* o = &tab[kPairConsts * t];
         if (pot_type == POT_TF) {  // particles.c:181-228: [A, B, C, D, sigma, alpha, beta]
             const double A = pot_params[5 * t], B = pot_params[5 * t + 1], C = pot_params[5 * t + 2],
                          D = pot_params[5 * t + 3], sg = pot_params[5 * t + 4];
@@ -624,6 +638,7 @@ void solver_initialize_particles(int n, int n_typ, double L, double h, int n_p, 
             const double al = A * B * ea - 6 * C / rc7 - 8 * D / rc9;
             const double be = -vs - al * rc;
             o[0] = A; o[1] = B; o[2] = C; o[3] = D; o[4] = sg; o[5] = al; o[6] = be;
+            o[7] = tf_exp_r2_limit(A, B, sg);
         } else if (pot_type == POT_LJ) {
             // particles.c:230-266: [sigma, epsilon, alpha, beta]. pot_params holds [sigma,
             // epsilon] per type pair as solver.py:241-270 passes it; the reference reads

@@ -18,6 +18,11 @@ enum CasType { CAS_CIC = 0, CAS_SPL_QUADR = 1, CAS_SPL_CUBIC = 2 };
 // Pair potentials (particles.c:17): Tosi-Fumi, Lennard-Jones, soft-core repulsion.
 enum PotType { POT_TF = 0, POT_LJ = 1, POT_SC = 2 };
 
+// Pair-potential constants per type pair in ParticleDev::tab: Tosi-Fumi [A, B, C, D,
+// sigma, alpha, beta, r^2 beyond which the exponential terms are dropped], Lennard-Jones
+// [sigma, epsilon, alpha, beta], soft core [nu, d, B, alpha, beta].
+constexpr int kPairConsts = 8;
+
 struct ParticleDev {
     int np = 0, ntyp = 0, n = 0;
     double L = 0, h = 0, rcut = 0;
@@ -29,7 +34,7 @@ struct ParticleDev {
     double* ft = nullptr;
     double* mass = nullptr;
     double* chg = nullptr;
-    double* tab = nullptr;   // [ntyp*ntyp][7] pair-potential constants per type pair
+    double* tab = nullptr;   // [ntyp*ntyp][kPairConsts] pair-potential constants per type pair
     int32_t* base = nullptr; // [np][3] base cell floor(pos/h) (wrapped)
     int cas = CAS_CIC;       // charge assignment scheme
     // the charge grid whose only nonzeros are the CIC corners of `base` (left by the last

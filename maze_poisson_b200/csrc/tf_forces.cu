@@ -33,7 +33,7 @@ namespace mzb {
 
 constexpr int kTfSb = 8;                  // blocks of 32 ions per super-block
 constexpr int kTfThreads = kTfSb * 32;    // one warp per I block of a super-block
-constexpr int kTfTab = 64 * 7;            // pair-constant table (up to 8 types)
+constexpr int kTfTab = 64 * kPairConsts;  // pair-constant table (up to 8 types)
 constexpr size_t kTfSmem =
     sizeof(double) * (kTfTab + 2 * kTfSb * 32 * 4 + kTfSb * kTfSb * 32 * 3);
 
@@ -58,7 +58,7 @@ __device__ __forceinline__ void pair_terms(const double* t, double r2, double ir
         const double a = t[0], b = t[1], c = t[2], d = t[3], sg = t[4], al = t[5], be = t[6];
         const double ir2 = ir * ir, ir6 = ir2 * ir2 * ir2;
         const double ir7 = ir6 * ir, ir8 = ir6 * ir2, ir9 = ir8 * ir;
-        const double ex = exp(b * (sg - r));
+        const double ex = r2 < t[7] ? exp(b * (sg - r)) : 0.0;  // negligible beyond (tf_exp_r2_limit)
         const double fm = b * a * ex - 6 * c * ir7 - 8 * d * ir9 - al;
         vm = a * ex - c * ir6 - d * ir8 + al * r + be;
         fr = fm * ir;
@@ -103,7 +103,7 @@ __global__ void k_tf_boxes(ParticleDev P) {
 template <int POT>
 __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
     extern __shared__ double sm[];
-    double* tab = sm;                              // [64 * 7]
+    double* tab = sm;                              // [64 * kPairConsts]
     double* ipos = tab + kTfTab;                   // [256][4]: x, y, z, type
     double* jpos = ipos + kTfSb * 32 * 4;          // [256][4]
     double* fjw = jpos + kTfSb * 32 * 4;           // [8 warps][8 J blocks][32][3]
@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
     const double prune2 = rc2 * (1.0 + 1e-9);
     const bool prune = P.flags[1] == 0;
 
-    for (int x = threadIdx.x; x < ntyp * ntyp * 7; x += blockDim.x) tab[x] = P.tab[x];
+    for (int x = threadIdx.x; x < ntyp * ntyp * kPairConsts; x += blockDim.x) tab[x] = P.tab[x];
     for (int q = threadIdx.x; q < kTfSb * 32; q += blockDim.x) {
         const int gi = SI * kTfSb * 32 + q, gj = SJ * kTfSb * 32 + q;
         const bool vi = gi < np, vj = gj < np;
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
                 const double r2 = dx * dx + dy * dy + dz * dz;
                 if (r2 > rc2) continue;
                 double fr, vm;
-                pair_terms<POT>(tab + 7 * (ti * ntyp + tj), r2, rsqrt(r2), fr, vm);
+                pair_terms<POT>(tab + kPairConsts * (ti * ntyp + tj), r2, rsqrt(r2), fr, vm);
                 const double ax = fr * dx, ay = fr * dy, az = fr * dz;
                 fx += ax;
                 fy += ay;
