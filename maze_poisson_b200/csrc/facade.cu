@@ -80,6 +80,7 @@ struct GridState {
     double L = 0, h = 0, tol = 0, eps_s = 1, eps_int = 1;
     long m = 0;
     double* q = nullptr;
+    uint32_t* qmask = nullptr;  // spreading's nonzero-charge segments (n % 64 == 0; spread_charges)
     double* buf[3] = {nullptr, nullptr, nullptr};  // phi / phi_prev / spare (renamed)
     int iphi = 0, iprev = 1, ispare = 2;
     double* y = nullptr;
@@ -154,6 +155,7 @@ void sync() { MZB_CHECK(cudaStreamSynchronize(sys().stream)); }
 
 void free_grid(GridState& G) {
     dfree(G.q);
+    dfree(G.qmask);
     for (auto& b : G.buf) dfree(b);
     dfree(G.y);
     dfree(G.r); dfree(G.p0); dfree(G.p1); dfree(G.Ap); dfree(G.v); dfree(G.rf); dfree(G.tmp);
@@ -346,6 +348,7 @@ MixedArgs mixed_args(System& s, int prog, double cst) {
         m.lev_r[l] = G.lev_r[l];
     }
     m.q = G.q;
+    m.qmask = G.qmask;
     m.phi_old = G.phi();
     m.phi_prev = G.phi_prev();
     m.phi_new = G.buf[G.ispare];
@@ -527,6 +530,7 @@ void solver_initialize_grid(int n, double L, double h, double tol, double eps, d
         G.precision = (pm && strcmp(pm, "mixed") == 0) ? 1 : 0;
     }
     G.q = dalloc<double>(G.m);
+    if (n % 64 == 0) G.qmask = dalloc<uint32_t>(((size_t)G.m / 64 + 31) / 32);
     G.buf[0] = dalloc<double>(G.m);
     if (grid_type == G_FFT) {
         G.fft.init(n, L, h);
@@ -727,7 +731,7 @@ int solver_update_charges(void) {
     System& s = sys();
     GridState& G = grid();
     ParticleDev& P = parts();
-    spread_charges(P, G.q, G.n, G.h, s.stream);
+    spread_charges(P, G.q, G.qmask, G.n, G.h, s.stream);
     MZB_CHECK(cudaMemcpyAsync(s.red_h, P.red, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     int flag = 0;
     MZB_CHECK(cudaMemcpyAsync(s.result_h, P.flags, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
@@ -1690,7 +1694,7 @@ std::vector<int> team_starts(const std::vector<System*>& ss, int nblocks, double
 void stage_particles_before_solve(System& s) {
     ParticleDev& P = s.P;
     integrator_part1(P, s.I, s.stream);
-    spread_charges(P, s.G.q, s.G.n, s.G.h, s.stream);
+    spread_charges(P, s.G.q, s.G.qmask, s.G.n, s.G.h, s.stream);
     count_launch();
     k_charge_check<<<1, 1, 0, s.stream>>>(P.red, s.qtot_d, s.err_d, P.flags);
 }

@@ -1003,10 +1003,13 @@ __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedA
             const int k = k0 + 2 * lane;
             double r0, r1;
             double2 bq;
-            if (RHS_Q) {
-                bq = *reinterpret_cast<const double2*>(a.q + row + k);
-                bq.x = bq.x * a.c;
-                bq.y = bq.y * a.c;
+            if (RHS_Q) {  // q is read only in segments the spreading marked (0 * c elsewhere)
+                const int seg = (row >> 6) + (k0 >> 6);
+                double2 qv = make_double2(0.0, 0.0);
+                if (a.qmask == nullptr || ((a.qmask[seg >> 5] >> (seg & 31)) & 1u))
+                    qv = *reinterpret_cast<const double2*>(a.q + row + k);
+                bq.x = qv.x * a.c;
+                bq.y = qv.y * a.c;
             } else {
                 bq = *reinterpret_cast<const double2*>(a.tmp + row + k);
             }

@@ -26,6 +26,7 @@ struct MixedArgs {
     float* lev_b[kMixedMaxLevels];
     float* lev_r[kMixedMaxLevels];
     const double* q;
+    const uint32_t* qmask;  // segments of 64 k where q may be nonzero (spread_charges), or null
     const double* phi_old;
     const double* phi_prev;
     double* phi_new;

@@ -454,8 +454,8 @@ __device__ __forceinline__ double cic_contrib(const ParticleDev& P, int c, int i
     return P.chg[c] * wgt;
 }
 
-__global__ void __launch_bounds__(kSpreadIonThreads) k_spread_ions(ParticleDev P, double* __restrict__ q, int n,
-                                                                   double h) {
+__global__ void __launch_bounds__(kSpreadIonThreads) k_spread_ions(ParticleDev P, double* __restrict__ q,
+                                                                   uint32_t* __restrict__ qmask, int n, double h) {
     __shared__ int near_id_s[kIonsPerCta][kNear];
     __shared__ int near_o_s[kIonsPerCta][kNear];  // offset code (di+1)*9 + (dj+1)*3 + (dk+1)
     __shared__ int near_n_s[kIonsPerCta];
@@ -557,9 +557,13 @@ __global__ void __launch_bounds__(kSpreadIonThreads) k_spread_ions(ParticleDev P
         }
     }
     q[((long)i * n + j) * n + k] = acc;
+    if (qmask != nullptr) {
+        const long seg = ((long)i * n + j) * (n >> 6) + (k >> 6);
+        atomicOr(qmask + (seg >> 5), 1u << (seg & 31));
+    }
 }
 
-void spread_charges(ParticleDev& P, double* q, int n, double h, cudaStream_t s) {
+void spread_charges(ParticleDev& P, double* q, uint32_t* qmask, int n, double h, cudaStream_t s) {
     const int nb = (P.np + 127) / 128;
     MZB_CHECK(cudaMemsetAsync(P.tile_count, 0, sizeof(int32_t) * P.ntiles, s));
     // CIC: q keeps zeros away from the ions' corners, so only the old corners need
@@ -577,16 +581,19 @@ void spread_charges(ParticleDev& P, double* q, int n, double h, cudaStream_t s) 
                 P.red + 0, s);
     if (nb > 0) count_launch();
     if (nb > 0) k_spread_fill<<<nb, 128, 0, s>>>(P);
+    const size_t mask_bytes = qmask != nullptr ? sizeof(uint32_t) * (((size_t)n * n * (n >> 6) + 31) / 32) : 0;
     if (P.cas == CAS_CIC) {  // the corners the ions reach (q is zero elsewhere)
+        if (qmask != nullptr) MZB_CHECK(cudaMemsetAsync(qmask, 0, mask_bytes, s));
         if (P.np > 0) {
             count_launch();
-            k_spread_ions<<<(P.np + kIonsPerCta - 1) / kIonsPerCta, kSpreadIonThreads, 0, s>>>(P, q, n, h);
+            k_spread_ions<<<(P.np + kIonsPerCta - 1) / kIonsPerCta, kSpreadIonThreads, 0, s>>>(P, q, qmask, n, h);
         }
         MZB_CHECK(cudaGetLastError());
         P.q_sparse = q;
         return;
     }
     P.q_sparse = nullptr;  // the tile kernel writes every point
+    if (qmask != nullptr) MZB_CHECK(cudaMemsetAsync(qmask, 0xff, mask_bytes, s));
     int dev, sms;
     MZB_CHECK(cudaGetDevice(&dev));
     MZB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

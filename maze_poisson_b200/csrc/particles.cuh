@@ -88,7 +88,9 @@ struct ParticleDev {
 
 // Build the CIC base cells, the tile bins and q (bit-identical to the reference's serial
 // update_charges). Writes the spread total charge to red[0].
-void spread_charges(ParticleDev& P, double* q, int n, double h, cudaStream_t s);
+// qmask (n % 64 == 0, else null): one bit per run of 64 consecutive k of a grid row, set
+// where the spreading may have written a nonzero charge (readers may skip the others).
+void spread_charges(ParticleDev& P, double* q, uint32_t* qmask, int n, double h, cudaStream_t s);
 // Forces from -grad(phi) at the 8 CIC corners (forces.c:26-100) into P.fe.
 void field_forces(ParticleDev& P, const double* phi, int n, double h, cudaStream_t s);
 // Linked cells (counting sort, stable by ion index) + Tosi-Fumi forces into P.fn;
