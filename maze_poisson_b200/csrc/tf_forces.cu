@@ -13,10 +13,12 @@
 // blocks into super-blocks of 8 (256 ions). A CTA of 8 warps takes one super-block pair
 // (SI, SJ) of a half shell (SJ = SI + d, d = 0 .. nsb/2, the middle distance only once):
 // warp w owns block I = 8 SI + w -- one ion per lane, its forces in registers -- and
-// walks the J blocks of SJ; in step s lane l pairs its ion with ion (l + s) mod 32 of the
-// J block, so the 32 lanes touch 32 distinct J ions and add the reactions into a
-// warp-private shared array without atomics. On the diagonal super-tile each unordered
-// block pair is taken once (and each pair inside a block once). A tile whose bounding
+// walks the J blocks of SJ; in step s (0..15) lane l pairs its ion with ions (l + s) and
+// (l + s + 16) mod 32 of the J block, two independent chains, so the 32 lanes touch 32
+// distinct J ions at a time and add the reactions into a warp-private shared array
+// (structure of arrays, conflict-free) without atomics, with a __syncwarp between the two
+// halves. On the diagonal super-tile each unordered block pair is taken once (and each
+// pair inside a block once, 16 steps of one partner). A tile whose bounding
 // boxes are farther apart than r_cut (minimum image, 1e-9 relative margin) is skipped;
 // pruning is off when a coordinate lies outside [0, L).
 //
@@ -100,13 +102,35 @@ __global__ void k_tf_boxes(ParticleDev P) {
     }
 }
 
+// One pair (i, partner j at x, y, z of type tj) for the lane's ion: whether it is inside
+// r_cut (and both ions exist), and its force times the separation and energy.
+template <int POT>
+__device__ __forceinline__ bool pair_eval(const double* tab, int ntyp, double L, double invL, double rc2, double xi,
+                                          double yi, double zi, int ti, double xj, double yj, double zj, int tj,
+                                          double& ax, double& ay, double& az, double& vm) {
+    double dx = xi - xj, dy = yi - yj, dz = zi - zj;
+    dx -= L * round(dx * invL);
+    dy -= L * round(dy * invL);
+    dz -= L * round(dz * invL);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    const bool in = ti >= 0 && tj >= 0 && r2 <= rc2;
+    const double r2s = in ? r2 : rc2;  // a harmless value for lanes whose pair is not taken
+    double fr;
+    pair_terms<POT>(tab + kPairConsts * ((in ? ti : 0) * ntyp + (in ? tj : 0)), r2s, rsqrt(r2s), fr, vm);
+    ax = fr * dx;
+    ay = fr * dy;
+    az = fr * dz;
+    return in;
+}
+
 template <int POT>
 __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
     extern __shared__ double sm[];
     double* tab = sm;                              // [64 * kPairConsts]
-    double* ipos = tab + kTfTab;                   // [256][4]: x, y, z, type
-    double* jpos = ipos + kTfSb * 32 * 4;          // [256][4]
-    double* fjw = jpos + kTfSb * 32 * 4;           // [8 warps][8 J blocks][32][3]
+    double* ipos = tab + kTfTab;                   // [4][256]: x, y, z, type (structure of arrays)
+    double* jpos = ipos + kTfSb * 32 * 4;          // [4][256]
+    double* fjw = jpos + kTfSb * 32 * 4;           // [8 warps][8 J blocks][3][32]
+    constexpr int NQ = kTfSb * 32;
     const int st = blockIdx.x;
     const int SI = P.tf_st[2 * st], SJ = P.tf_st[2 * st + 1];
     const bool diag = SI == SJ;
@@ -117,17 +141,17 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
     const bool prune = P.flags[1] == 0;
 
     for (int x = threadIdx.x; x < ntyp * ntyp * kPairConsts; x += blockDim.x) tab[x] = P.tab[x];
-    for (int q = threadIdx.x; q < kTfSb * 32; q += blockDim.x) {
-        const int gi = SI * kTfSb * 32 + q, gj = SJ * kTfSb * 32 + q;
+    for (int q = threadIdx.x; q < NQ; q += blockDim.x) {
+        const int gi = SI * NQ + q, gj = SJ * NQ + q;
         const bool vi = gi < np, vj = gj < np;
-        ipos[4 * q] = vi ? P.spos[3 * gi] : 0.0;
-        ipos[4 * q + 1] = vi ? P.spos[3 * gi + 1] : 0.0;
-        ipos[4 * q + 2] = vi ? P.spos[3 * gi + 2] : 0.0;
-        ipos[4 * q + 3] = vi ? (double)P.stype[gi] : -1.0;
-        jpos[4 * q] = vj ? P.spos[3 * gj] : 0.0;
-        jpos[4 * q + 1] = vj ? P.spos[3 * gj + 1] : 0.0;
-        jpos[4 * q + 2] = vj ? P.spos[3 * gj + 2] : 0.0;
-        jpos[4 * q + 3] = vj ? (double)P.stype[gj] : -1.0;
+        ipos[q] = vi ? P.spos[3 * gi] : 0.0;
+        ipos[NQ + q] = vi ? P.spos[3 * gi + 1] : 0.0;
+        ipos[2 * NQ + q] = vi ? P.spos[3 * gi + 2] : 0.0;
+        ipos[3 * NQ + q] = vi ? (double)P.stype[gi] : -1.0;
+        jpos[q] = vj ? P.spos[3 * gj] : 0.0;
+        jpos[NQ + q] = vj ? P.spos[3 * gj + 1] : 0.0;
+        jpos[2 * NQ + q] = vj ? P.spos[3 * gj + 2] : 0.0;
+        jpos[3 * NQ + q] = vj ? (double)P.stype[gj] : -1.0;
     }
     for (int x = threadIdx.x; x < kTfSb * kTfSb * 32 * 3; x += blockDim.x) fjw[x] = 0.0;
     __syncthreads();
@@ -135,9 +159,9 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
     double fx = 0.0, fy = 0.0, fz = 0.0, e_acc = 0.0;
     const int I = SI * kTfSb + w;
     if (I < nblk) {
-        const double* me = ipos + 4 * (w * 32 + lane);
-        const double xi = me[0], yi = me[1], zi = me[2];
-        const int ti = (int)me[3];  // -1: no ion in this lane
+        const int me = w * 32 + lane;
+        const double xi = ipos[me], yi = ipos[NQ + me], zi = ipos[2 * NQ + me];
+        const int ti = (int)ipos[3 * NQ + me];  // -1: no ion in this lane
         const double* bI = P.tf_box + 6 * I;
         for (int t = 0; t < kTfSb; t++) {
             const int d = (t - w) & (kTfSb - 1);
@@ -152,32 +176,64 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
                 const double gz = axis_gap(bI[2], bI[5], bJ[2], bJ[5] - bJ[2], L);
                 if (gx * gx + gy * gy + gz * gz > prune2) continue;
             }
-            const double* jb = jpos + 4 * (t * 32);
-            double* fj = fjw + ((w * kTfSb + t) * 32) * 3;
-            // self tile: partners (l + s) mod 32 for s = 1..16, the last step by half the
-            // lanes, so every pair inside the block comes once
-            const int s0 = self ? 1 : 0, s1 = self ? 16 : 31;
-            for (int s = s0; s <= s1; s++) {
-                const int jj = (lane + s) & 31;
-                const double* pj = jb + 4 * jj;
-                const int tj = (int)pj[3];
-                if (ti < 0 || tj < 0 || (self && s == 16 && lane >= 16)) continue;
-                double dx = xi - pj[0], dy = yi - pj[1], dz = zi - pj[2];
-                dx -= L * round(dx * invL);
-                dy -= L * round(dy * invL);
-                dz -= L * round(dz * invL);
-                const double r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 > rc2) continue;
-                double fr, vm;
-                pair_terms<POT>(tab + kPairConsts * (ti * ntyp + tj), r2, rsqrt(r2), fr, vm);
-                const double ax = fr * dx, ay = fr * dy, az = fr * dz;
-                fx += ax;
-                fy += ay;
-                fz += az;
-                fj[3 * jj] -= ax;
-                fj[3 * jj + 1] -= ay;
-                fj[3 * jj + 2] -= az;
-                e_acc += vm;
+            const double* jx = jpos + t * 32;
+            const double* jy = jx + NQ;
+            const double* jz = jx + 2 * NQ;
+            const double* jt = jx + 3 * NQ;
+            double* fjx = fjw + (w * kTfSb + t) * 3 * 32;
+            double* fjy = fjx + 32;
+            double* fjz = fjx + 64;
+            if (self) {
+                // partners (l + s) mod 32 for s = 1..16, the last step by half the lanes, so
+                // every pair inside the block comes once
+                for (int s = 1; s <= 16; s++) {
+                    const int jj = (lane + s) & 31;
+                    double ax, ay, az, vm;
+                    const bool in = pair_eval<POT>(tab, ntyp, L, invL, rc2, xi, yi, zi, ti, jx[jj], jy[jj], jz[jj],
+                                                   (int)jt[jj], ax, ay, az, vm);
+                    if (in && !(s == 16 && lane >= 16)) {
+                        fx += ax;
+                        fy += ay;
+                        fz += az;
+                        fjx[jj] -= ax;
+                        fjy[jj] -= ay;
+                        fjz[jj] -= az;
+                        e_acc += vm;
+                    }
+                    __syncwarp();
+                }
+                continue;
+            }
+            // two partners per step, (l + s) and (l + s + 16) mod 32, as two independent
+            // chains; their reactions go in one after the other (each a permutation of the
+            // 32 entries)
+            for (int s = 0; s < 16; s++) {
+                const int ja = (lane + s) & 31, jb = (lane + s + 16) & 31;
+                double ax, ay, az, va, bx, by, bz, vb;
+                const bool ina = pair_eval<POT>(tab, ntyp, L, invL, rc2, xi, yi, zi, ti, jx[ja], jy[ja], jz[ja],
+                                                (int)jt[ja], ax, ay, az, va);
+                const bool inb = pair_eval<POT>(tab, ntyp, L, invL, rc2, xi, yi, zi, ti, jx[jb], jy[jb], jz[jb],
+                                                (int)jt[jb], bx, by, bz, vb);
+                if (ina) {
+                    fx += ax;
+                    fy += ay;
+                    fz += az;
+                    fjx[ja] -= ax;
+                    fjy[ja] -= ay;
+                    fjz[ja] -= az;
+                    e_acc += va;
+                }
+                __syncwarp();
+                if (inb) {
+                    fx += bx;
+                    fy += by;
+                    fz += bz;
+                    fjx[jb] -= bx;
+                    fjy[jb] -= by;
+                    fjz[jb] -= bz;
+                    e_acc += vb;
+                }
+                __syncwarp();
             }
         }
     }
@@ -194,8 +250,10 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
     if (lane == 0) esh[w] = e_acc;
     __syncthreads();
     for (int x = threadIdx.x; x < kTfSb * 32 * 3; x += blockDim.x) {
+        const int t = x / 96, jj = (x / 3) % 32, dd = x % 3;  // out layout [J block][32][3]
+        const int y = (t * 3 + dd) * 32 + jj;                  // warp arrays [J block][3][32]
         double v = 0.0;
-        for (int q = 0; q < kTfSb; q++) v += fjw[q * kTfSb * 32 * 3 + x];
+        for (int q = 0; q < kTfSb; q++) v += fjw[q * kTfSb * 32 * 3 + y];
         out[kTfSb * 32 * 3 + x] = v;
     }
     if (threadIdx.x == 0) {
