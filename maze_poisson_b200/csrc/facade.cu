@@ -97,6 +97,7 @@ struct GridState {
     float* lev_b[kMixedMaxLevels] = {};
     float* lev_r[kMixedMaxLevels] = {};
     float* lev_g = nullptr;   // Green's function of the coarsest level (direct solve) or null
+    bool coarse_team = false; // the coarsest level (n <= kMixedTeamDirectN) is solved by the whole team
     double* bj_inv = nullptr;  // block-Jacobi block inverse (1000 x 1000) on BLOCKJACOBI grids
     // Poisson-Boltzmann (solver_initialize_grid_pois_boltz, grid_general.c:84-100)
     bool pb = false;
@@ -175,6 +176,7 @@ void free_grid(GridState& G) {
     dev_free(G.lev_g);
     G.lev_g = nullptr;
     G.nlev = 0;
+    G.coarse_team = false;
     G.ready = false;
 }
 
@@ -189,6 +191,13 @@ bool mixed_supported(const GridState& G) {
 void ensure_mixed_levels(GridState& G) {
     if (G.nlev) return;
     G.nlev = mixed_levels(G.n, G.lev_n);
+    G.coarse_team = false;
+    for (int l = 1; l < G.nlev; l++)  // stop at the first level the team solves directly
+        if (G.lev_n[l] <= kMixedTeamDirectN) {
+            G.nlev = l + 1;
+            G.coarse_team = true;
+            break;
+        }
     for (int l = 0; l < G.nlev; l++) {
         const size_t m = (size_t)G.lev_n[l] * G.lev_n[l] * G.lev_n[l];
         G.lev_x[l] = static_cast<float*>(dev_alloc(m * sizeof(float)));
@@ -197,7 +206,7 @@ void ensure_mixed_levels(GridState& G) {
         zero_fill(G.lev_x[l], m * sizeof(float));
     }
     const int nc = G.lev_n[G.nlev - 1];
-    if (nc <= kMixedDirectN && mixed_small_level(G.nlev, G.lev_n) < G.nlev) {
+    if (G.coarse_team || (nc <= kMixedDirectN && mixed_small_level(G.nlev, G.lev_n) < G.nlev)) {
         std::vector<float> g((size_t)nc * nc * nc);
         mixed_coarse_green(nc, g.data());
         G.lev_g = static_cast<float*>(dev_alloc(g.size() * sizeof(float)));
@@ -339,8 +348,9 @@ MixedArgs mixed_args(System& s, int prog, double cst) {
     m.nu2 = 2;
     m.coarse_sweeps = 16;
     m.nlev = G.nlev;
-    m.lsmall = mixed_small_level(G.nlev, G.lev_n);
+    m.lsmall = G.coarse_team ? G.nlev : mixed_small_level(G.nlev, G.lev_n);
     m.coarse_g = G.lev_g;
+    m.coarse_team = G.coarse_team ? 1 : 0;
     for (int l = 0; l < G.nlev; l++) {
         m.lev_n[l] = G.lev_n[l];
         m.lev_x[l] = G.lev_x[l];

@@ -24,6 +24,8 @@
 // pass that writes the level's right-hand side (the FP64 residual pass, the
 // restrictions), and the sum of the finest correction, whose mean is removed, is taken in
 // the last two half-sweeps instead of by another pass.
+#include <vector>
+
 #include "engine.cuh"
 #include "mixed.cuh"
 #include "tma.cuh"
@@ -889,6 +891,53 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above
     cta_pts(nl, [&](int i, int j, int k) { dst[split_idx(nl, i, j, k)] = xs[(i * nl + j) * nl + k]; });
 }
 
+// The coarsest level l (n <= kMixedTeamDirectN, rhs in lev_b[l]) solved exactly by the
+// whole team: x = G * b, the circular convolution with the pseudo-inverse of the unscaled
+// periodic 7-point Laplacian (coarse_g, precomputed on the host), i.e. the zero-mean
+// solution of L x = b - mean(b). Every CTA stages G and b in shared memory; a warp forms
+// one point's sum, its lanes taking the (j, k) columns r = lane + 32 t of every i plane.
+__device__ void team_direct(const MixedArgs& a, const Team& tm, float* sm, int l) {
+    const int n = a.lev_n[l], n2 = n * n, N = n2 * n;
+    float* gs = sm;
+    float* bs = sm + N;
+    const float* b = a.lev_b[l];  // split layout
+    for (int p = threadIdx.x; p < N; p += blockDim.x) {
+        gs[p] = a.coarse_g[p];
+        const int i = p / n2, j = (p / n) % n, k = p % n;
+        bs[p] = b[split_idx(n, i, j, k)];
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int TM = (kMixedTeamDirectN * kMixedTeamDirectN + 31) / 32;
+    float* x = a.lev_x[l];
+    for (int p = tm.b * nw + w; p < N; p += tm.nblk * nw) {
+        const int pi = p / n2, pj = (p / n) % n, pk = p % n;
+        int ro[TM], go[TM];  // b offset (j n + k) and G offset of the lane's columns
+#pragma unroll
+        for (int t = 0; t < TM; t++) {
+            const int r = lane + 32 * t;
+            const int qj = r / n, qk = r - qj * n;
+            int dj = pj - qj, dk = pk - qk;
+            dj += dj < 0 ? n : 0;
+            dk += dk < 0 ? n : 0;
+            ro[t] = r < n2 ? r : -1;
+            go[t] = dj * n + dk;
+        }
+        float acc = 0.0f;
+        for (int qi = 0; qi < n; qi++) {
+            int di = pi - qi;
+            di += di < 0 ? n : 0;
+            const float* gp = gs + di * n2;
+            const float* bp = bs + qi * n2;
+#pragma unroll
+            for (int t = 0; t < TM; t++)
+                if (ro[t] >= 0) acc = fmaf(gp[go[t]], bp[ro[t]], acc);
+        }
+        acc = warp_sumf(acc);
+        if (lane == 0) x[split_idx(n, pi, pj, pk)] = acc;
+    }
+}
+
 // Grid-wide red-black sweeps of level l: `half_sweeps` colours starting at first_colour,
 // a grid barrier after each except (when skip_last_barrier) the last. When esum is not
 // null the values written in the last two half-sweeps are summed into it.
@@ -925,6 +974,9 @@ __device__ bool vcycle(const MixedArgs& a, const Team& tm, float* sm, unsigned& 
     stamp_outer(a, outer, 2);
     if (ls < L) {
         if (tm.b == 0) small_vcycle(a, sm, R(ls - 1));
+        if (!team_sync(tm, epoch)) return false;
+    } else if (a.coarse_team) {
+        team_direct(a, tm, sm, L - 1);
         if (!team_sync(tm, epoch)) return false;
     } else {
         if (!grid_smooth(a, tm, L - 1, X(L - 1), 1, 2 * a.coarse_sweeps - 1, epoch, nullptr, false)) return false;
@@ -1237,6 +1289,10 @@ int g_batch_device = -1;
 size_t g_batch_smem_set = 0;
 
 size_t small_smem_bytes(const MixedArgs& a) {
+    if (a.coarse_team) {  // G and b of the coarsest level in every CTA
+        const size_t nc = (size_t)a.lev_n[a.nlev - 1];
+        return 2 * nc * nc * nc * sizeof(float);
+    }
     size_t v = 0;
     for (int m = a.lsmall; m < a.nlev; m++) v += 3 * (size_t)a.lev_n[m] * a.lev_n[m] * a.lev_n[m];
     if (a.coarse_g != nullptr) v += (size_t)a.lev_n[a.nlev - 1] * a.lev_n[a.nlev - 1] * a.lev_n[a.nlev - 1];
@@ -1257,18 +1313,39 @@ int mixed_levels(int n, int* sizes) {
 }
 
 void mixed_coarse_green(int n, float* g) {
+    // g[d] = (1/N) sum_k e^{i w k.d} / lambda(k) over k != 0 (real: 1/lambda is even),
+    // as three 1-D inverse transforms of 1/lambda, one axis at a time.
     const int N = n * n * n;
     const double w = 2.0 * 3.14159265358979323846 / n;
-    for (int d = 0; d < N; d++) {
-        const int di = d / (n * n), dj = (d / n) % n, dk = d % n;
-        double s = 0.0;
-        for (int k = 1; k < N; k++) {
-            const int ki = k / (n * n), kj = (k / n) % n, kk = k % n;
-            const double lam = 2 * cos(w * ki) + 2 * cos(w * kj) + 2 * cos(w * kk) - 6.0;
-            s += cos(w * (ki * di + kj * dj + kk * dk)) / lam;
-        }
-        g[d] = (float)(s / N);
+    std::vector<double> re((size_t)N), im((size_t)N, 0.0), tr((size_t)N), ti((size_t)N), c(n), sn(n);
+    for (int k = 0; k < n; k++) {
+        c[k] = cos(w * k);
+        sn[k] = sin(w * k);
     }
+    for (int k = 0; k < N; k++) {
+        const int ki = k / (n * n), kj = (k / n) % n, kk = k % n;
+        const double lam = 2 * c[ki] + 2 * c[kj] + 2 * c[kk] - 6.0;
+        re[k] = k == 0 ? 0.0 : 1.0 / lam;
+    }
+    const int stride[3] = {n * n, n, 1};
+    for (int ax = 0; ax < 3; ax++) {
+        const int st = stride[ax];
+        for (int q = 0; q < N; q++) {
+            const int pos = (q / st) % n, base = q - pos * st;
+            double sr = 0.0, si = 0.0;
+            for (int k = 0; k < n; k++) {
+                const int m = (k * pos) % n;  // e^{i w k pos}
+                const double xr = re[base + k * st], xi = im[base + k * st];
+                sr += xr * c[m] - xi * sn[m];
+                si += xr * sn[m] + xi * c[m];
+            }
+            tr[q] = sr;
+            ti[q] = si;
+        }
+        re.swap(tr);
+        im.swap(ti);
+    }
+    for (int d = 0; d < N; d++) g[d] = (float)(re[d] / N);
 }
 
 int mixed_small_level(int nlev, const int* sizes) {

@@ -19,6 +19,7 @@ struct MixedArgs {
     int nu1, nu2;       // red-black GS sweeps before / after the coarse correction (>= 1)
     int coarse_sweeps;  // sweeps on the coarsest level (>= 1) when coarse_g is null
     const float* coarse_g;  // Green's function of the coarsest level (mixed_coarse_green) or null
+    int coarse_team;        // 1: the coarsest level is solved by every CTA of the team with coarse_g
     int nlev;
     int lsmall;         // first level held in shared memory (nlev if none; >= 1)
     int lev_n[kMixedMaxLevels];
@@ -42,8 +43,13 @@ struct MixedArgs {
 int mixed_levels(int n, int* sizes);
 // First level with n <= kMixedSmallN (nlev if none).
 int mixed_small_level(int nlev, const int* sizes);
-// Largest coarsest level solved directly (n^3 values of its Green's function).
+// Largest coarsest level solved directly in CTA 0's shared memory (n^3 values of its
+// Green's function).
 constexpr int kMixedDirectN = 6;
+// The hierarchy stops at the first level of at most this many points per side, which
+// every CTA of the team solves directly: a slice of the convolution with its Green's
+// function each (see mixed.cu).
+constexpr int kMixedTeamDirectN = 16;
 // Pseudo-inverse kernel of the unscaled periodic 7-point Laplacian on an n^3 grid:
 // g[d] = (1/n^3) sum_{k != 0} cos(2 pi k.d / n) / lambda(k),
 // lambda(k) = 2 cos(2 pi k1/n) + 2 cos(2 pi k2/n) + 2 cos(2 pi k3/n) - 6.
