@@ -38,6 +38,17 @@ __device__ __forceinline__ void for_points(const Team& t, int n, F&& f) {
         for (int k = t.lane; k < n; k += 32) f(i, j, k);
     }
 }
+// The same visit for n % 64 == 0 with two points per lane per step, k and k + 32: f(i, j,
+// k0, k1) computes both before storing either, so their loads are in flight together; a
+// lane still meets its points in ascending k.
+template <class F>
+__device__ __forceinline__ void for_point_pairs(const Team& t, int n, F&& f) {
+    const long rows = (long)n * n;
+    for (long row = t.gw; row < rows; row += t.nw) {
+        const int i = (int)(row / n), j = (int)(row - (long)i * n);
+        for (int k = t.lane; k < n; k += 64) f(i, j, k, k + 32);
+    }
+}
 // Visit the points of one colour ((i+j+k) % 2 == colour) of an n^3 grid (n even).
 template <class F>
 __device__ __forceinline__ void for_colour(const Team& t, int n, int colour, F&& f) {
@@ -45,6 +56,17 @@ __device__ __forceinline__ void for_colour(const Team& t, int n, int colour, F&&
     for (long row = t.gw; row < rows; row += t.nw) {
         const int i = (int)(row / n), j = (int)(row - (long)i * n);
         for (int k = ((i + j + colour) & 1) + 2 * t.lane; k < n; k += 64) f(i, j, k);
+    }
+}
+
+// The colour visit for n % 128 == 0 with two points per lane per step, k and k + 64 (the
+// same colour, so neither reads the other): f(i, j, k0, k1) computes both before storing.
+template <class F>
+__device__ __forceinline__ void for_colour_pairs(const Team& t, int n, int colour, F&& f) {
+    const long rows = (long)n * n;
+    for (long row = t.gw; row < rows; row += t.nw) {
+        const int i = (int)(row / n), j = (int)(row - (long)i * n);
+        for (int k = ((i + j + colour) & 1) + 2 * t.lane; k < n; k += 128) f(i, j, k, k + 64);
     }
 }
 
@@ -179,19 +201,31 @@ __device__ bool rbgs(const Team& t, const double* rhs, double* x, int n, const E
 // x-, y+, y-, z+, z- times their neighbours, minus rhs_c) / max(dg_c, 1e-14).
 __device__ bool rbgs_pb(const Team& t, const double* rhs, double* x, int n, const PbOp& op,
                         const EngineArgs& a) {
+    auto value = [&](const Nb& o) {
+        double d = op.dg[o.c];
+        if (d < 1e-14) d = 1e-14;
+        double s = op.ex[o.c] * x[o.ip] + op.ex[o.im] * x[o.im];
+        s = s + op.ey[o.c] * x[o.jp];
+        s = s + op.ey[o.jm] * x[o.jm];
+        s = s + op.ez[o.c] * x[o.kp];
+        s = s + op.ez[o.km] * x[o.km];
+        s = s - rhs[o.c];
+        return s / d;
+    };
     for (int colour = 0; colour < 2; colour++) {
-        for_colour(t, n, colour, [&](int i, int j, int k) {
-            const Nb o = neighbours(n, i, j, k);
-            double d = op.dg[o.c];
-            if (d < 1e-14) d = 1e-14;
-            double s = op.ex[o.c] * x[o.ip] + op.ex[o.im] * x[o.im];
-            s = s + op.ey[o.c] * x[o.jp];
-            s = s + op.ey[o.jm] * x[o.jm];
-            s = s + op.ez[o.c] * x[o.kp];
-            s = s + op.ez[o.km] * x[o.km];
-            s = s - rhs[o.c];
-            x[o.c] = s / d;
-        });
+        if (n % 128 == 0) {
+            for_colour_pairs(t, n, colour, [&](int i, int j, int k0, int k1) {
+                const Nb o0 = neighbours(n, i, j, k0), o1 = neighbours(n, i, j, k1);
+                const double v0 = value(o0), v1 = value(o1);
+                x[o0.c] = v0;
+                x[o1.c] = v1;
+            });
+        } else {
+            for_colour(t, n, colour, [&](int i, int j, int k) {
+                const Nb o = neighbours(n, i, j, k);
+                x[o.c] = value(o);
+            });
+        }
         if (!grid_sync(a.bar)) return false;
     }
     return true;
@@ -446,29 +480,60 @@ __device__ int cg_run(const Team& t, const CgSpec& s, const OP& op, const Engine
         };
         auto pf = [&](long q) { return first ? zf(q) : pold[q] * beta + zf(q); };
         double pap[1] = {0.0}, m0[1];
-        for_points(t, n, [&](int i, int j, int k) {
-            const Nb o = neighbours(n, i, j, k);
-            const double pc = pf(o.c);
-            const double ap = op.apply(o, pf);
-            pnew[o.c] = pc;
-            s.Ap[o.c] = ap;
-            pap[0] += pc * ap;
-        });
+        if (n % 64 == 0) {
+            for_point_pairs(t, n, [&](int i, int j, int k0, int k1) {
+                const Nb o0 = neighbours(n, i, j, k0), o1 = neighbours(n, i, j, k1);
+                const double pc0 = pf(o0.c), pc1 = pf(o1.c);
+                const double ap0 = op.apply(o0, pf), ap1 = op.apply(o1, pf);
+                pnew[o0.c] = pc0;
+                s.Ap[o0.c] = ap0;
+                pnew[o1.c] = pc1;
+                s.Ap[o1.c] = ap1;
+                pap[0] += pc0 * ap0;
+                pap[0] += pc1 * ap1;
+            });
+        } else {
+            for_points(t, n, [&](int i, int j, int k) {
+                const Nb o = neighbours(n, i, j, k);
+                const double pc = pf(o.c);
+                const double ap = op.apply(o, pf);
+                pnew[o.c] = pc;
+                s.Ap[o.c] = ap;
+                pap[0] += pc * ap;
+            });
+        }
         ok = grid_reduce<1, 0>(pap, m0, a, seq);
         if (!ok) return -1;
         if (COARSE && fabs(pap[0]) < 1e-300) { res = (int)iter; break; }
         const double alpha = rv / pap[0];
         // phase B: x += alpha p; r += alpha Ap; <r,r>, |r|_inf (+ <r, P r> for Jacobi)
         double sums[2] = {0.0, 0.0}, rmax[1] = {0.0};
-        for_points(t, n, [&](int i, int j, int k) {
-            const long c = ((long)i * n + j) * n + k;
-            s.x[c] = s.x[c] + alpha * pnew[c];
-            const double rn = s.r[c] + alpha * s.Ap[c];
-            s.r[c] = rn;
+        auto upd = [&](double rn) {
             sums[0] += rn * rn;
             if (KIND == PC_JACOBI) sums[1] += rn * (-rn / 6.0);
             rmax[0] = fmax(rmax[0], fabs(rn));
-        });
+        };
+        if (n % 64 == 0) {
+            for_point_pairs(t, n, [&](int i, int j, int k0, int k1) {
+                const long c0 = ((long)i * n + j) * n + k0, c1 = c0 + (k1 - k0);
+                const double x0 = s.x[c0] + alpha * pnew[c0], x1 = s.x[c1] + alpha * pnew[c1];
+                const double rn0 = s.r[c0] + alpha * s.Ap[c0], rn1 = s.r[c1] + alpha * s.Ap[c1];
+                s.x[c0] = x0;
+                s.x[c1] = x1;
+                s.r[c0] = rn0;
+                s.r[c1] = rn1;
+                upd(rn0);
+                upd(rn1);
+            });
+        } else {
+            for_points(t, n, [&](int i, int j, int k) {
+                const long c = ((long)i * n + j) * n + k;
+                s.x[c] = s.x[c] + alpha * pnew[c];
+                const double rn = s.r[c] + alpha * s.Ap[c];
+                s.r[c] = rn;
+                upd(rn);
+            });
+        }
         ok = grid_reduce<2, 1>(sums, rmax, a, seq);
         if (!ok) return -1;
         if (COARSE) {
