@@ -144,6 +144,10 @@ double mzb_last_solve_ms(void);            /* device ms of the last field-solver
 int mzb_last_solve_result(void);           /* its return value (iterations or -1) */
 uint64_t mzb_kernel_launches(void);        /* kernels this library has launched */
 int mzb_sm_count(void);                    /* SMs of the current device (CTA shares of the batched step) */
+/* Green's function of the unscaled periodic 7-point Laplacian on an n^3 grid (2 <= n <= 16),
+   g[d] = (1/n^3) sum_{k != 0} cos(2 pi k.d / n) / lambda(k): the mixed solver's exact
+   coarsest-level solve. Host-only; returns 0, or -1 for an n out of range. */
+int mzb_coarse_green(int n, float *g);
 
 #ifdef __cplusplus
 }

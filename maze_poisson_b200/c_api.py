@@ -116,6 +116,7 @@ EXTENSION_SYMBOLS = {
     "mzb_last_solve_result": (_c.c_int, []),
     "mzb_kernel_launches": (_c.c_uint64, []),
     "mzb_sm_count": (_c.c_int, []),
+    "mzb_coarse_green": (_c.c_int, [_c.c_int, _c.c_void_p]),
     "mzb_set_precision": (None, [_c.c_int, _c.c_double]),
     "mzb_get_precision": (_c.c_int, []),
     "mzb_conj_grad_noalloc": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_double, _c.c_int,

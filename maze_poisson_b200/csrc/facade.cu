@@ -1523,6 +1523,13 @@ int mzb_last_solve_result(void) { return sys().last_solve_iters; }
 // Kernels launched by this library since it was loaded.
 uint64_t mzb_kernel_launches(void) { return g_kernel_launches; }
 int mzb_sm_count(void) { return mixed_grid_blocks(); }
+// Green's function of the unscaled periodic 7-point Laplacian on an n^3 grid (its
+// pseudo-inverse; the mixed solver's coarsest level is solved with it): g[0..n^3).
+int mzb_coarse_green(int n, float* g) {
+    if (n < 2 || n > kMixedTeamDirectN || !g) return -1;
+    mixed_coarse_green(n, g);
+    return 0;
+}
 uint64_t mzb_get_ocalls(void) { return sys().I.ocalls; }
 
 // n_steps iterations of SolverMD.md_loop_iter (maze_poisson/solver.py:483-492) with both
