@@ -610,11 +610,20 @@ __device__ bool vcycle_pb(const Team& t, const double* rhs, double* x, int n, in
     const PbOp fine{a.ex, a.ey, a.ez, a.dg}, coarse{a.cex, a.cey, a.cez, a.cdg};
     for (int it = 0; it < sm; it++)
         if (!rbgs_pb(t, rhs, x, n, fine, a)) return false;
-    for_points(t, n, [&](int i, int j, int k) {
-        const Nb o = neighbours(n, i, j, k);
-        const double lx = fine.apply(o, [&](long q) { return x[q]; });
-        a.rf[o.c] = -lx + 1.0 * rhs[o.c];
-    });
+    auto res = [&](const Nb& o) { return -fine.apply(o, [&](long q) { return x[q]; }) + 1.0 * rhs[o.c]; };
+    if (n % 64 == 0) {
+        for_point_pairs(t, n, [&](int i, int j, int k0, int k1) {
+            const Nb o0 = neighbours(n, i, j, k0), o1 = neighbours(n, i, j, k1);
+            const double r0 = res(o0), r1 = res(o1);
+            a.rf[o0.c] = r0;
+            a.rf[o1.c] = r1;
+        });
+    } else {
+        for_points(t, n, [&](int i, int j, int k) {
+            const Nb o = neighbours(n, i, j, k);
+            a.rf[o.c] = res(o);
+        });
+    }
     if (!grid_sync(a.bar)) return false;
     restrict27(t, a.rf, a.rc, n);
     for_points(t, nc, [&](int i, int j, int k) { a.ec[((long)i * nc + j) * nc + k] = 0.0; });
@@ -626,10 +635,20 @@ __device__ bool vcycle_pb(const Team& t, const double* rhs, double* x, int n, in
     bool ok = true;
     cg_run<PC_NONE, true>(t, cs, coarse, a, seq, ok);
     if (!ok) return false;
-    for_points(t, n, [&](int i, int j, int k) {
-        const long c = ((long)i * n + j) * n + k;
-        x[c] = x[c] + 1.0 * prolong_at(a.ec, nc, i, j, k);
-    });
+    if (n % 64 == 0) {
+        for_point_pairs(t, n, [&](int i, int j, int k0, int k1) {
+            const long c0 = ((long)i * n + j) * n + k0, c1 = c0 + (k1 - k0);
+            const double v0 = x[c0] + 1.0 * prolong_at(a.ec, nc, i, j, k0);
+            const double v1 = x[c1] + 1.0 * prolong_at(a.ec, nc, i, j, k1);
+            x[c0] = v0;
+            x[c1] = v1;
+        });
+    } else {
+        for_points(t, n, [&](int i, int j, int k) {
+            const long c = ((long)i * n + j) * n + k;
+            x[c] = x[c] + 1.0 * prolong_at(a.ec, nc, i, j, k);
+        });
+    }
     if (!grid_sync(a.bar)) return false;
     for (int it = 0; it < sm; it++)
         if (!rbgs_pb(t, rhs, x, n, fine, a)) return false;
