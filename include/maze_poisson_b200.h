@@ -54,8 +54,11 @@ void mzb_get_pb_grids(double *ex, double *ey, double *ez, double *k2);
 
 /* precision of the field solve: 0 = the reference's FP64 algorithms (default), 1 = FP32
    multigrid V-cycles with FP64 iterative refinement until the FP64 residual meets the
-   grid's tol (or tol_override when > 0). Also selected by MZB_PRECISION=mixed at
-   solver_initialize_grid. FFT grids and grids that cannot be halved twice stay FP64. */
+   grid's tol (or tol_override when > 0), 2 = the same multigrid and refinement loop with
+   every value in FP64 (the FP64 multigrid form, the fair FP64 comparator of mode 1). Also
+   selected by MZB_PRECISION=mixed / fp64mg at solver_initialize_grid. FFT grids and grids
+   that cannot be halved twice stay on the reference's algorithms. No counterpart in the
+   reference. */
 void mzb_set_precision(int mode, double tol_override);
 int mzb_get_precision(void);      /* precision in effect for the current grid */
 
@@ -70,12 +73,16 @@ uint64_t mzb_get_ocalls(void);             /* O-blocks applied so far */
 /* CG solve that allocates no device memory, for callers that cannot call cudaMalloc
    (a host framework that owns all device allocations, a loop that must not take an
    allocation's implicit synchronisation). No counterpart in the reference. b, x0, x are
-   caller-owned device buffers of n^3 doubles, 2 <= n <= 64; the work arrays live in a
-   static ~8.4 MB device array that every GPU loading this library holds until exit and
-   that all calls share (overlapping calls race). The first call per device looks up that
-   array's address; make it before any stream capture. Returns iterations or -1 as
-   conj_grad does, -2 for unsupported arguments, -3 if the solver aborted, -4 if the work
-   area's address is unavailable. precond: 0 implicit Jacobi, 1 Jacobi. */
+   caller-owned buffers of n^3 doubles on the current device, 2 <= n <= 64; the work arrays
+   live in a static ~8.4 MB device array that every GPU loading this library holds until
+   exit and that all calls share (overlapping calls race). The first call per device looks
+   up that array's address. The call is synchronous (it waits for the solve and reads the
+   result on the host), so it must not be called while its stream -- or, in global capture
+   mode, any stream -- is being captured. Returns iterations or -1 as conj_grad does, -2 for
+   unsupported arguments (including pointers that are not memory of the current device),
+   -3 if the solver aborted, -4 if the work area's address is unavailable, -5 for a CUDA
+   error already pending or in reading the result; a kernel that cannot be launched ends
+   the process, as elsewhere in this library. precond: 0 implicit Jacobi, 1 Jacobi. */
 int mzb_conj_grad_noalloc(const double *b, const double *x0, double *x, double tol, int n,
                           int precond, void *stream);
 

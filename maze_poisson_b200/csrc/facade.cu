@@ -88,15 +88,17 @@ struct GridState {
            *tmp = nullptr;
     double *rc = nullptr, *ec = nullptr, *cr = nullptr, *cp0 = nullptr, *cp1 = nullptr, *cAp = nullptr;
     FftPoisson fft;
-    // mixed precision (FP32 multigrid + FP64 refinement)
-    int precision = 0;        // 0: FP64 reference algorithms, 1: mixed
+    // field-solve form: 0 the reference's FP64 algorithms, 1 mixed precision (FP32
+    // multigrid + FP64 refinement), 2 FP64 multigrid (the same V-cycle in FP64)
+    int precision = 0;
     double mixed_tol = 0.0;   // > 0 overrides tol for the mixed solve
     int nlev = 0;
     int lev_n[kMixedMaxLevels] = {};
-    float* lev_x[kMixedMaxLevels] = {};
-    float* lev_b[kMixedMaxLevels] = {};
-    float* lev_r[kMixedMaxLevels] = {};
-    float* lev_g = nullptr;   // Green's function of the coarsest level (direct solve) or null
+    void* lev_x[kMixedMaxLevels] = {};  // float (precision 1) or double (precision 2)
+    void* lev_b[kMixedMaxLevels] = {};
+    void* lev_r[kMixedMaxLevels] = {};
+    void* lev_g = nullptr;    // Green's function of the coarsest level (direct solve) or null
+    int lev_fp64 = 0;         // the levels above hold doubles
     bool coarse_team = false; // the coarsest level (n <= kMixedTeamDirectN) is solved by the whole team
     double* bj_inv = nullptr;  // block-Jacobi block inverse (1000 x 1000) on BLOCKJACOBI grids
     // Poisson-Boltzmann (solver_initialize_grid_pois_boltz, grid_general.c:84-100)
@@ -188,8 +190,25 @@ bool mixed_supported(const GridState& G) {
     return G.type != 1 && !G.pb && G.n <= kMixedMaxN && L >= 3 && mixed_small_level(L, sizes) >= 1;
 }
 
+void free_mixed_levels(GridState& G) {
+    for (int l = 0; l < kMixedMaxLevels; l++) {
+        dev_free(G.lev_x[l]);
+        dev_free(G.lev_b[l]);
+        dev_free(G.lev_r[l]);
+        G.lev_x[l] = G.lev_b[l] = G.lev_r[l] = nullptr;
+    }
+    dev_free(G.lev_g);
+    G.lev_g = nullptr;
+    G.nlev = 0;
+    G.coarse_team = false;
+}
+
 void ensure_mixed_levels(GridState& G) {
+    const int fp64 = G.precision == 2 ? 1 : 0;
+    if (G.nlev && G.lev_fp64 != fp64) free_mixed_levels(G);  // the form changed: levels of the other type
     if (G.nlev) return;
+    G.lev_fp64 = fp64;
+    const size_t w = fp64 ? sizeof(double) : sizeof(float);
     G.nlev = mixed_levels(G.n, G.lev_n);
     G.coarse_team = false;
     for (int l = 1; l < G.nlev; l++)  // stop at the first level the team solves directly
@@ -200,17 +219,24 @@ void ensure_mixed_levels(GridState& G) {
         }
     for (int l = 0; l < G.nlev; l++) {
         const size_t m = (size_t)G.lev_n[l] * G.lev_n[l] * G.lev_n[l];
-        G.lev_x[l] = static_cast<float*>(dev_alloc(m * sizeof(float)));
-        G.lev_b[l] = static_cast<float*>(dev_alloc(m * sizeof(float)));
-        G.lev_r[l] = static_cast<float*>(dev_alloc(m * sizeof(float)));
-        zero_fill(G.lev_x[l], m * sizeof(float));
+        G.lev_x[l] = dev_alloc(m * w);
+        G.lev_b[l] = dev_alloc(m * w);
+        G.lev_r[l] = dev_alloc(m * w);
+        zero_fill(G.lev_x[l], m * w);
     }
     const int nc = G.lev_n[G.nlev - 1];
     if (G.coarse_team || (nc <= kMixedDirectN && mixed_small_level(G.nlev, G.lev_n) < G.nlev)) {
-        std::vector<float> g((size_t)nc * nc * nc);
-        mixed_coarse_green(nc, g.data());
-        G.lev_g = static_cast<float*>(dev_alloc(g.size() * sizeof(float)));
-        upload(G.lev_g, g.data(), g.size() * sizeof(float));
+        const size_t N = (size_t)nc * nc * nc;
+        G.lev_g = dev_alloc(N * w);
+        if (fp64) {
+            std::vector<double> g(N);
+            mixed_coarse_green(nc, g.data());
+            upload(G.lev_g, g.data(), N * w);
+        } else {
+            std::vector<float> g(N);
+            mixed_coarse_green(nc, g.data());
+            upload(G.lev_g, g.data(), N * w);
+        }
     }
 }
 
@@ -350,6 +376,7 @@ MixedArgs mixed_args(System& s, int prog, double cst) {
     m.nlev = G.nlev;
     m.lsmall = G.coarse_team ? G.nlev : mixed_small_level(G.nlev, G.lev_n);
     m.coarse_g = G.lev_g;
+    m.fp64 = G.lev_fp64;
     m.coarse_team = G.coarse_team ? 1 : 0;
     for (int l = 0; l < G.nlev; l++) {
         m.lev_n[l] = G.lev_n[l];
@@ -537,7 +564,7 @@ void solver_initialize_grid(int n, double L, double h, double tol, double eps, d
     G.iphi = 0; G.iprev = 1; G.ispare = 2;
     {
         const char* pm = getenv("MZB_PRECISION");
-        G.precision = (pm && strcmp(pm, "mixed") == 0) ? 1 : 0;
+        G.precision = (pm && strcmp(pm, "mixed") == 0) ? 1 : (pm && strcmp(pm, "fp64mg") == 0) ? 2 : 0;
     }
     G.q = dalloc<double>(G.m);
     if (n % 64 == 0) G.qmask = dalloc<uint32_t>(((size_t)G.m / 64 + 31) / 32);
@@ -767,7 +794,7 @@ void solver_init_field(void) {
         sync();
         return;
     }
-    if (G.precision == 1 && mixed_supported(G)) {
+    if (G.precision >= 1 && mixed_supported(G)) {
         run_mixed(s, PROG_INIT_FIELD, rhs_const(G));
         return;
     }
@@ -785,23 +812,16 @@ void solver_init_field(void) {
     G.iprev = old;
 }
 
-int solver_update_field(void) {
-    System& s = sys();
-    GridState& G = grid();
-    if (G.type == G_FFT) {  // grid_fft.c:139-143
-        G.fft.solve(G.q, G.phi(), s.stream);
-        sync();
-        return 0;
-    }
-    if (G.precision == 1 && mixed_supported(G)) {
-        if (G.type == G_MAZE_MG && G.precond != P_NONE) {  // grid_maze_multigrid.c:138-141
-            fprintf(stderr, "Maze Multigrid with preconditioner not implemented yet.\n");
-            exit(1);
-        }
-        if (G.type == G_LCG) return run_mixed(s, PROG_LCG_UPDATE, rhs_const(G));
-        if (G.type == G_MG) return run_mixed(s, PROG_MG_UPDATE, rhs_const(G));
-        return run_mixed(s, G.type == G_MAZE_LCG ? PROG_MAZE_LCG : PROG_MAZE_MG, maze_const(G));
-    }
+}  // extern "C"
+
+namespace mzb {
+namespace {
+int md_steps_deferred(System& s, int n_steps);
+
+// Engine arguments of an MD-step field update on an FP64 grid (the engine branch of
+// solver_update_field): the new field goes into the spare buffer.
+EngineArgs update_engine_args(System& s) {
+    GridState& G = s.G;
     EngineArgs a = engine_base(s);
     a.phi_old = G.phi();
     a.phi_prev = G.phi_prev();
@@ -837,6 +857,31 @@ int solver_update_field(void) {
         a.c = maze_const(G);
         break;
     }
+    return a;
+}
+}  // namespace
+}  // namespace mzb
+
+extern "C" {
+
+int solver_update_field(void) {
+    System& s = sys();
+    GridState& G = grid();
+    if (G.type == G_FFT) {  // grid_fft.c:139-143
+        G.fft.solve(G.q, G.phi(), s.stream);
+        sync();
+        return 0;
+    }
+    if (G.precision >= 1 && mixed_supported(G)) {
+        if (G.type == G_MAZE_MG && G.precond != P_NONE) {  // grid_maze_multigrid.c:138-141
+            fprintf(stderr, "Maze Multigrid with preconditioner not implemented yet.\n");
+            exit(1);
+        }
+        if (G.type == G_LCG) return run_mixed(s, PROG_LCG_UPDATE, rhs_const(G));
+        if (G.type == G_MG) return run_mixed(s, PROG_MG_UPDATE, rhs_const(G));
+        return run_mixed(s, G.type == G_MAZE_LCG ? PROG_MAZE_LCG : PROG_MAZE_MG, maze_const(G));
+    }
+    EngineArgs a = update_engine_args(s);
     const int res = run_engine(s, a);
     const int old = G.iphi;
     G.iphi = G.ispare;
@@ -1497,18 +1542,19 @@ void mzb_set_seed(uint64_t seed) {
     touch(sys());
 }
 
-// Field-solve precision of the current grid: 0 = the reference's FP64 algorithms,
-// 1 = FP32 multigrid with FP64 iterative refinement to the same (or an overriding)
-// tolerance. Grids that cannot be coarsened three times, and FFT, stay FP64.
+// Field-solve form of the current grid: 0 = the reference's FP64 algorithms, 1 = FP32
+// multigrid with FP64 iterative refinement to the same (or an overriding) tolerance, 2 =
+// the same multigrid with every value in FP64 (the FP64 multigrid form). Grids that cannot
+// be coarsened three times, and FFT, stay on the reference's algorithms.
 void mzb_set_precision(int mode, double tol_override) {
     GridState& G = grid();
     touch(sys());
-    G.precision = mode == 1 ? 1 : 0;
+    G.precision = (mode == 1 || mode == 2) ? mode : 0;
     G.mixed_tol = tol_override;
 }
 int mzb_get_precision(void) {
     GridState& G = grid();
-    return (G.precision == 1 && mixed_supported(G)) ? 1 : 0;
+    return (G.precision >= 1 && mixed_supported(G)) ? G.precision : 0;
 }
 
 // The CUDA stream all work of the current system is queued on (for callers that time
@@ -1534,8 +1580,19 @@ uint64_t mzb_get_ocalls(void) { return sys().I.ocalls; }
 
 // n_steps iterations of SolverMD.md_loop_iter (maze_poisson/solver.py:483-492) with both
 // electrostatic and non-electrostatic forces (and the PB coefficient update and forces on
-// a Poisson-Boltzmann grid); returns the last solver_update_field value.
+// a Poisson-Boltzmann grid); returns the last solver_update_field value. Poisson grids
+// solved by CG, multigrid or the mixed solver run the steps without a host round trip:
+// the charge check and the solve status stay on the device and are read after the last
+// step (md_steps_deferred); a charge error still prints the reference's message and exits.
 int solver_md_step(int n_steps) {
+    if (n_steps <= 0) return 0;
+    {
+        System& s = sys();
+        GridState& G = grid();
+        if (G.type != G_FFT && !G.pb && !(G.type == G_MAZE_MG && G.precond != P_NONE) && s.parts_ready &&
+            s.integ_ready)
+            return md_steps_deferred(s, n_steps);
+    }
     int res = 0;
     for (int i = 0; i < n_steps; i++) {
         const bool pb = grid().pb;
@@ -1725,6 +1782,83 @@ void stage_particles_after_solve(System& s) {
     tf_forces(P, s.stream);
     total_forces(P, s.stream);
     integrator_part2(P, s.I, s.stream);
+}
+
+__global__ void k_md_charge_check(const double* red, double* qtot, int* err, const int* flags, double* bad) {
+    const double q = red[0];
+    if (fabs(*qtot - q) > 1e-6 && !err[0]) {  // solver_md.c:98-102, first failing step kept
+        err[0] = 1;
+        bad[0] = *qtot;
+        bad[1] = q;
+    }
+    *qtot = q;
+    if (flags[0]) err[1] = 1;
+}
+
+// solver_md_step on a Poisson grid without host round trips: per step integrator part 1,
+// spreading with the charge check on the device, the field solve launched without reading
+// its result (the buffers rotate as solver_update_field rotates them), field, pair and
+// total forces, integrator part 2. One synchronisation at the end reads the error words,
+// the charge total and the last solve's result and time.
+int md_steps_deferred(System& s, int n_steps) {
+    GridState& G = s.G;
+    ParticleDev& P = s.P;
+    batch_prepare(s);  // device charge total, error words, Philox counter
+    double* bad = s.scratch_d + 4094;  // the last two words of the 4096-double scratch
+    static const bool generic_only = getenv("MZB_ENGINE") && strcmp(getenv("MZB_ENGINE"), "generic") == 0;
+    for (int i = 0; i < n_steps; i++) {
+        integrator_part1(P, s.I, s.stream);
+        spread_charges(P, G.q, G.qmask, G.n, G.h, s.stream);
+        count_launch();
+        k_md_charge_check<<<1, 1, 0, s.stream>>>(P.red, s.qtot_d, s.err_d, P.flags, bad);
+        MZB_CHECK(cudaEventRecord(s.ev0, s.stream));
+        if (G.precision >= 1 && mixed_supported(G)) {
+            double cst = 0.0;
+            const int prog = mixed_update_prog(G, cst);
+            mixed_launch(mixed_args(s, prog, cst), s.stream);
+        } else {
+            const EngineArgs a = update_engine_args(s);
+            if (generic_only || !cg_fast_launch(a, s.stream)) engine_launch(a, s.stream);
+        }
+        MZB_CHECK(cudaEventRecord(s.ev1, s.stream));
+        const int old = G.iphi;
+        G.iphi = G.ispare;
+        G.ispare = G.iprev;
+        G.iprev = old;
+        count_launch();
+        k_solve_check<<<1, 1, 0, s.stream>>>(s.result, s.err_d);
+        field_forces(P, G.phi(), G.n, G.h, s.stream);
+        build_cells(P, s.stream);
+        tf_forces(P, s.stream);
+        total_forces(P, s.stream);
+        integrator_part2(P, s.I, s.stream);
+    }
+    int err[4];
+    double q = 0.0, qbad[2] = {0.0, 0.0};
+    MZB_CHECK(cudaMemcpyAsync(s.result_h, s.result, 2 * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    MZB_CHECK(cudaStreamSynchronize(s.stream));
+    MZB_CHECK(cudaMemcpy(err, s.err_d, sizeof(err), cudaMemcpyDeviceToHost));
+    MZB_CHECK(cudaMemcpy(&q, s.qtot_d, sizeof(double), cudaMemcpyDeviceToHost));
+    MZB_CHECK(cudaMemcpy(qbad, bad, sizeof(qbad), cudaMemcpyDeviceToHost));
+    MZB_CHECK(cudaEventElapsedTime(&s.last_solve_ms, s.ev0, s.ev1));
+    s.last_solve_iters = s.result_h[0];
+    if (err[1]) fatal("charge spreading: more than 1024 ions reach one 2x8x32 grid tile");
+    if (err[0]) {
+        printf("Charge conservation error: q_tot = %.6f, q_tot_loc = %.6f\n", qbad[0], qbad[1]);
+        exit(1);
+    }
+    s.q_tot = q;
+    int res = s.result_h[0];
+    if (s.result_h[1] != 0) {
+        fprintf(stderr, "maze_poisson_b200: field solver aborted (grid barrier timeout)\n");
+        res = -1;
+    } else if (err[2]) {
+        res = -1;  // an earlier step's solve did not converge
+    }
+    if (res == -1 && G.type == G_MAZE_MG)
+        fprintf(stderr, "Warning: Multigrid did not converge after 1000 iterations.\n");
+    if (err[2]) zero_fill(s.err_d, 4 * sizeof(int));
+    return res;
 }
 
 // Build (or find) the graph of one batched MD step for the systems' current state, its

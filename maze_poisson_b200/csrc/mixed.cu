@@ -187,68 +187,88 @@ __device__ bool reduce_sum_max(double& s, double& mx, const Team& tm, unsigned& 
     return ok;
 }
 
-// ---- FP32 multigrid point operations (pointers may be global or shared) ----
+// ---- multigrid point operations (pointers may be global or shared) ----
+//
+// The V-cycle is written once for the level scalar S: float for the mixed-precision form
+// (FP32 levels inside FP64 refinement), double for the FP64 multigrid form (the same
+// V-cycle and refinement loop with every value in FP64).
+
+template <class S> __device__ __forceinline__ S neg_sixth();
+template <> __device__ __forceinline__ float neg_sixth<float>() { return -1.0f / 6.0f; }
+template <> __device__ __forceinline__ double neg_sixth<double>() { return -1.0 / 6.0; }
+__device__ __forceinline__ float fma_s(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_s(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float warp_sum_s(float v) { return warp_sumf(v); }
+__device__ __forceinline__ double warp_sum_s(double v) { return warp_sum(v); }
+// level arrays of the hierarchy, stored as S
+template <class S> __device__ __forceinline__ S* lev_x(const MixedArgs& a, int l) { return static_cast<S*>(a.lev_x[l]); }
+template <class S> __device__ __forceinline__ S* lev_b(const MixedArgs& a, int l) { return static_cast<S*>(a.lev_b[l]); }
+template <class S> __device__ __forceinline__ S* lev_r(const MixedArgs& a, int l) { return static_cast<S*>(a.lev_r[l]); }
 
 // red-black Gauss-Seidel update of one point; returns the new value
-__device__ __forceinline__ float gs_point(int n, const float* b, float* x, int i, int j, int k) {
+template <class S>
+__device__ __forceinline__ S gs_point(int n, const S* b, S* x, int i, int j, int k) {
     const Nb o = nb_of(n, i, j, k);
-    float s = x[o.im] + x[o.ip];
+    S s = x[o.im] + x[o.ip];
     s += x[o.jm];
     s += x[o.jp];
     s += x[o.km];
     s += x[o.kp];
-    const float v = (b[o.c] - s) * (-1.0f / 6.0f);
+    const S v = (b[o.c] - s) * neg_sixth<S>();
     x[o.c] = v;
     return v;
 }
 
-__device__ __forceinline__ void resid_point(int n, const float* b, const float* x, float* r, int i, int j, int k) {
+template <class S>
+__device__ __forceinline__ void resid_point(int n, const S* b, const S* x, S* r, int i, int j, int k) {
     const Nb o = nb_of(n, i, j, k);
-    float s = x[o.ip] + x[o.im];
+    S s = x[o.ip] + x[o.im];
     s += x[o.jp];
     s += x[o.jm];
     s += x[o.kp];
     s += x[o.km];
-    r[o.c] = b[o.c] - (s - 6.0f * x[o.c]);
+    r[o.c] = b[o.c] - (s - S(6) * x[o.c]);
 }
 
 // Coarse point (I,J,K) of bc = 4 * R27(r) with its first red half-sweep from x = 0:
 // xc = -bc/6 on red (I+J+K even) points, 0 on black ones.
-__device__ __forceinline__ void restrict_point(int n, const float* r, float* bc, float* xc, int I, int J, int K) {
+template <class S>
+__device__ __forceinline__ void restrict_point(int n, const S* r, S* bc, S* xc, int I, int J, int K) {
     const int nc = n / 2;
     const long n2 = (long)n * n;
     const int i = 2 * I, j = 2 * J, k = 2 * K;
     const long i0 = (long)i * n2, i1 = (long)(i + 1 == n ? 0 : i + 1) * n2, i2 = (long)(i == 0 ? n - 1 : i - 1) * n2;
     const long j0 = (long)j * n, j1 = (long)(j + 1 == n ? 0 : j + 1) * n, j2 = (long)(j == 0 ? n - 1 : j - 1) * n;
     const long k0 = k, k1 = (k + 1 == n ? 0 : k + 1), k2 = (k == 0 ? n - 1 : k - 1);
-    const float f = r[i2 + j0 + k0] + r[i1 + j0 + k0] + r[i0 + j2 + k0] + r[i0 + j1 + k0] + r[i0 + j0 + k2] +
+    const S f = r[i2 + j0 + k0] + r[i1 + j0 + k0] + r[i0 + j2 + k0] + r[i0 + j1 + k0] + r[i0 + j0 + k2] +
                     r[i0 + j0 + k1];
-    const float e = r[i1 + j0 + k2] + r[i1 + j0 + k1] + r[i2 + j0 + k2] + r[i2 + j0 + k1] + r[i1 + j2 + k0] +
+    const S e = r[i1 + j0 + k2] + r[i1 + j0 + k1] + r[i2 + j0 + k2] + r[i2 + j0 + k1] + r[i1 + j2 + k0] +
                     r[i1 + j1 + k0] + r[i2 + j2 + k0] + r[i2 + j1 + k0] + r[i0 + j2 + k2] + r[i0 + j2 + k1] +
                     r[i0 + j1 + k2] + r[i0 + j1 + k1];
-    const float c = r[i1 + j1 + k2] + r[i1 + j1 + k1] + r[i1 + j2 + k2] + r[i1 + j2 + k1] + r[i2 + j1 + k2] +
+    const S c = r[i1 + j1 + k2] + r[i1 + j1 + k1] + r[i1 + j2 + k2] + r[i1 + j2 + k1] + r[i2 + j1 + k2] +
                     r[i2 + j1 + k1] + r[i2 + j2 + k2] + r[i2 + j2 + k1];
     const long cc = ((long)I * nc + J) * nc + K;
-    const float bv = (8.0f * r[i0 + j0 + k0] + 4.0f * f + 2.0f * e + c) * (4.0f / 64.0f);
+    const S bv = (S(8) * r[i0 + j0 + k0] + S(4) * f + S(2) * e + c) * (S(0.0625));
     bc[cc] = bv;
-    xc[cc] = ((I + J + K) & 1) == 0 ? bv * (-1.0f / 6.0f) : 0.0f;
+    xc[cc] = ((I + J + K) & 1) == 0 ? bv * neg_sixth<S>() : S(0);
 }
 
 // fine x += P(coarse x) at (i,j,k), trilinear
-__device__ __forceinline__ void prolong_point(int n, const float* xc, float* x, int i, int j, int k) {
+template <class S>
+__device__ __forceinline__ void prolong_point(int n, const S* xc, S* x, int i, int j, int k) {
     const int nc = n / 2;
     const long n2c = (long)nc * nc;
     const int ci = i >> 1, cj = j >> 1, ck = k >> 1;
     const long i0 = (long)ci * n2c, i1 = (long)(ci + 1 == nc ? 0 : ci + 1) * n2c;
     const long j0 = (long)cj * nc, j1 = (long)(cj + 1 == nc ? 0 : cj + 1) * nc;
     const long k0 = ck, k1 = (ck + 1 == nc ? 0 : ck + 1);
-    const float wi = (i & 1) ? 0.5f : 0.0f, wj = (j & 1) ? 0.5f : 0.0f, wk = (k & 1) ? 0.5f : 0.0f;
-    const float a00 = xc[i0 + j0 + k0] * (1.0f - wk) + xc[i0 + j0 + k1] * wk;
-    const float a01 = xc[i0 + j1 + k0] * (1.0f - wk) + xc[i0 + j1 + k1] * wk;
-    const float a10 = xc[i1 + j0 + k0] * (1.0f - wk) + xc[i1 + j0 + k1] * wk;
-    const float a11 = xc[i1 + j1 + k0] * (1.0f - wk) + xc[i1 + j1 + k1] * wk;
-    const float b0 = a00 * (1.0f - wj) + a01 * wj, b1 = a10 * (1.0f - wj) + a11 * wj;
-    x[((long)i * n + j) * n + k] += b0 * (1.0f - wi) + b1 * wi;
+    const S wi = (i & 1) ? S(0.5) : S(0), wj = (j & 1) ? S(0.5) : S(0), wk = (k & 1) ? S(0.5) : S(0);
+    const S a00 = xc[i0 + j0 + k0] * (S(1) - wk) + xc[i0 + j0 + k1] * wk;
+    const S a01 = xc[i0 + j1 + k0] * (S(1) - wk) + xc[i0 + j1 + k1] * wk;
+    const S a10 = xc[i1 + j0 + k0] * (S(1) - wk) + xc[i1 + j0 + k1] * wk;
+    const S a11 = xc[i1 + j1 + k0] * (S(1) - wk) + xc[i1 + j1 + k1] * wk;
+    const S b0 = a00 * (S(1) - wj) + a01 * wj, b1 = a10 * (S(1) - wj) + a11 * wj;
+    x[((long)i * n + j) * n + k] += b0 * (S(1) - wi) + b1 * wi;
 }
 
 // ---- grid levels: red-black split layout ----
@@ -304,17 +324,17 @@ __device__ __forceinline__ void grid_rows(const Team& tm, int n, F&& f) {
 // in-row value at kk are loaded for all chunks first; the in-row neighbour on the other
 // side (kk - 1 for s = 0, kk + 1 for s = 1) comes from the adjacent lane by a shuffle,
 // and only at a chunk or row boundary from memory.
-template <int T>
-__device__ __forceinline__ void split_nb_sums(const float* xo, const Rows& o, int h, int s, int k0, float (&sum)[T]) {
+template <int T, class S>
+__device__ __forceinline__ void split_nb_sums(const S* xo, const Rows& o, int h, int s, int k0, S (&sum)[T]) {
     const int lane = threadIdx.x & 31;
-    float cen[T];
+    S cen[T];
 #pragma unroll
     for (int t = 0; t < T; t++) {
         const int kk = k0 + lane + 32 * t;
-        sum[t] = 0.0f;
-        cen[t] = 0.0f;
+        sum[t] = S(0);
+        cen[t] = S(0);
         if (kk < h) {
-            const float a0 = xo[o.im + kk], a1 = xo[o.ip + kk], a2 = xo[o.jm + kk], a3 = xo[o.jp + kk];
+            const S a0 = xo[o.im + kk], a1 = xo[o.ip + kk], a2 = xo[o.jm + kk], a3 = xo[o.jp + kk];
             cen[t] = xo[o.c + kk];
             sum[t] = ((a0 + a1) + a2) + a3;
         }
@@ -322,12 +342,12 @@ __device__ __forceinline__ void split_nb_sums(const float* xo, const Rows& o, in
 #pragma unroll
     for (int t = 0; t < T; t++) {
         const int kk = k0 + lane + 32 * t;
-        const float up = __shfl_up_sync(0xffffffffu, cen[t], 1);
-        const float dn = __shfl_down_sync(0xffffffffu, cen[t], 1);
-        const float last_prev = __shfl_sync(0xffffffffu, cen[t > 0 ? t - 1 : 0], 31);
-        const float first_next = __shfl_sync(0xffffffffu, cen[t + 1 < T ? t + 1 : t], 0);
+        const S up = __shfl_up_sync(0xffffffffu, cen[t], 1);
+        const S dn = __shfl_down_sync(0xffffffffu, cen[t], 1);
+        const S last_prev = __shfl_sync(0xffffffffu, cen[t > 0 ? t - 1 : 0], 31);
+        const S first_next = __shfl_sync(0xffffffffu, cen[t + 1 < T ? t + 1 : t], 0);
         if (kk < h) {
-            float side;
+            S side;
             if (s == 0) {
                 if (lane > 0)
                     side = up;
@@ -351,29 +371,30 @@ __device__ __forceinline__ void split_nb_sums(const float* xo, const Rows& o, in
 }
 
 // half-sweep of colour c; when acc is not null the new values are summed into it
-__device__ void split_gs_scalar(const Team& tm, int n, int c, const float* b, float* x, double* acc) {
+template <class S>
+__device__ void split_gs_scalar(const Team& tm, int n, int c, const S* b, S* x, double* acc) {
     const int lane = threadIdx.x & 31, h = n >> 1;
     const int hp = h * n * n;
-    const float* xo = x + (1 - c) * hp;
-    float* xc = x + c * hp;
-    const float* bc = b + c * hp;
+    const S* xo = x + (1 - c) * hp;
+    S* xc = x + c * hp;
+    const S* bc = b + c * hp;
     double s_acc = 0.0;
     grid_rows(tm, n, [&](int i, int j) {
         const Rows o = rows_of(n, i, j);
         const int s = (i + j + c) & 1;
         for (int k0 = 0; k0 < h; k0 += 32 * kBatchSweep) {
-            float bv[kBatchSweep], sum[kBatchSweep];
+            S bv[kBatchSweep], sum[kBatchSweep];
 #pragma unroll
             for (int t = 0; t < kBatchSweep; t++) {
                 const int kk = k0 + lane + 32 * t;
-                bv[t] = kk < h ? bc[o.c + kk] : 0.0f;
+                bv[t] = kk < h ? bc[o.c + kk] : S(0);
             }
             split_nb_sums<kBatchSweep>(xo, o, h, s, k0, sum);
 #pragma unroll
             for (int t = 0; t < kBatchSweep; t++) {
                 const int kk = k0 + lane + 32 * t;
                 if (kk < h) {
-                    const float v = (bv[t] - sum[t]) * (-1.0f / 6.0f);
+                    const S v = (bv[t] - sum[t]) * neg_sixth<S>();
                     xc[o.c + kk] = v;
                     s_acc += (double)v;
                 }
@@ -384,26 +405,27 @@ __device__ void split_gs_scalar(const Team& tm, int n, int c, const float* b, fl
 }
 
 // red residual r_red = b_red - L x at the red points (black residuals are zero)
-__device__ void split_resid_red_scalar(const Team& tm, int n, const float* b, const float* x, float* r) {
+template <class S>
+__device__ void split_resid_red_scalar(const Team& tm, int n, const S* b, const S* x, S* r) {
     const int lane = threadIdx.x & 31, h = n >> 1;
     const int hp = h * n * n;
-    const float* x1 = x + hp;
+    const S* x1 = x + hp;
     grid_rows(tm, n, [&](int i, int j) {
         const Rows o = rows_of(n, i, j);
         const int s = (i + j) & 1;
         for (int k0 = 0; k0 < h; k0 += 32 * kBatchSweep) {
-            float bv[kBatchSweep], xv[kBatchSweep], sum[kBatchSweep];
+            S bv[kBatchSweep], xv[kBatchSweep], sum[kBatchSweep];
 #pragma unroll
             for (int t = 0; t < kBatchSweep; t++) {
                 const int kk = k0 + lane + 32 * t;
-                bv[t] = kk < h ? b[o.c + kk] : 0.0f;
-                xv[t] = kk < h ? x[o.c + kk] : 0.0f;
+                bv[t] = kk < h ? b[o.c + kk] : S(0);
+                xv[t] = kk < h ? x[o.c + kk] : S(0);
             }
             split_nb_sums<kBatchSweep>(x1, o, h, s, k0, sum);
 #pragma unroll
             for (int t = 0; t < kBatchSweep; t++) {
                 const int kk = k0 + lane + 32 * t;
-                if (kk < h) r[o.c + kk] = bv[t] - (sum[t] - 6.0f * xv[t]);
+                if (kk < h) r[o.c + kk] = bv[t] - (sum[t] - S(6) * xv[t]);
             }
         }
     });
@@ -411,13 +433,14 @@ __device__ void split_resid_red_scalar(const Team& tm, int n, const float* b, co
 
 // 4 x R27(r) at coarse point (I,J,K) from the red residual half of a split level n
 // (the 13 red taps of the 27-point full weighting)
-__device__ __forceinline__ float split_restrict_value(int n, const float* r, int I, int J, int K) {
+template <class S>
+__device__ __forceinline__ S split_restrict_value(int n, const S* r, int I, int J, int K) {
     const int h = n >> 1;
     const int i = 2 * I, j = 2 * J;
     const int ip = i + 1, im = i == 0 ? n - 1 : i - 1, jp = j + 1, jm = j == 0 ? n - 1 : j - 1;
     auto R = [&](int fi, int fj) { return (fi * n + fj) * h; };
     const int Km = K == 0 ? h - 1 : K - 1;
-    float e = r[R(ip, jp) + K] + r[R(ip, jm) + K];
+    S e = r[R(ip, jp) + K] + r[R(ip, jm) + K];
     e += r[R(im, jp) + K];
     e += r[R(im, jm) + K];
     e += r[R(ip, j) + K];
@@ -428,16 +451,17 @@ __device__ __forceinline__ float split_restrict_value(int n, const float* r, int
     e += r[R(i, jp) + Km];
     e += r[R(i, jm) + K];
     e += r[R(i, jm) + Km];
-    return (8.0f * r[R(i, j) + K] + 2.0f * e) * (4.0f / 64.0f);
+    return (S(8) * r[R(i, j) + K] + S(2) * e) * (S(0.0625));
 }
 
 // coarse b = 4 R27(r), coarse x = its first red half-sweep from 0 (both split layout)
-__device__ void split_restrict_scalar(const Team& tm, int n, const float* r, float* bc, float* xc) {
+template <class S>
+__device__ void split_restrict_scalar(const Team& tm, int n, const S* r, S* bc, S* xc) {
     const int lane = threadIdx.x & 31, nc = n / 2, hc = nc >> 1;
     const int hpc = hc * nc * nc;
     grid_rows(tm, nc, [&](int I, int J) {
         for (int k0 = 0; k0 < nc; k0 += 32 * kBatch) {
-            float v[kBatch];
+            S v[kBatch];
 #pragma unroll
             for (int t = 0; t < kBatch; t++) {
                 const int K = k0 + lane + 32 * t;
@@ -450,7 +474,7 @@ __device__ void split_restrict_scalar(const Team& tm, int n, const float* r, flo
                     const int C = (I + J + K) & 1;
                     const int idx = C * hpc + (I * nc + J) * hc + (K >> 1);
                     bc[idx] = v[t];
-                    xc[idx] = C == 0 ? v[t] * (-1.0f / 6.0f) : 0.0f;
+                    xc[idx] = C == 0 ? v[t] * neg_sixth<S>() : S(0);
                 }
             }
         }
@@ -458,10 +482,11 @@ __device__ void split_restrict_scalar(const Team& tm, int n, const float* r, flo
 }
 
 // fine black x += P(coarse x), trilinear (both split layout)
-__device__ void split_prolong_black_scalar(const Team& tm, int n, const float* xc, float* x) {
+template <class S>
+__device__ void split_prolong_black_scalar(const Team& tm, int n, const S* xc, S* x) {
     const int lane = threadIdx.x & 31, h = n >> 1, nc = n / 2, hc = nc >> 1;
     const int hp = h * n * n, hpc = hc * nc * nc;
-    float* x1 = x + hp;
+    S* x1 = x + hp;
     grid_rows(tm, n, [&](int i, int j) {
         const int s1 = (i + j + 1) & 1;  // black points of row (i,j) sit at k = 2 kk + s1
         const int ci = i >> 1, cj = j >> 1;
@@ -471,23 +496,23 @@ __device__ void split_prolong_black_scalar(const Team& tm, int n, const float* x
             return ((CI + CJ + CK) & 1) * hpc + (CI * nc + CJ) * hc + (CK >> 1);
         };
         auto line = [&](int CI, int CJ, int ck, int ck1) {
-            const float a = xc[C(CI, CJ, ck)];
-            return ok ? 0.5f * (a + xc[C(CI, CJ, ck1)]) : a;
+            const S a = xc[C(CI, CJ, ck)];
+            return ok ? S(0.5) * (a + xc[C(CI, CJ, ck1)]) : a;
         };
         const int rowx = (i * n + j) * h;
         for (int k0 = 0; k0 < h; k0 += 32 * kBatch) {
-            float v[kBatch], old[kBatch];
+            S v[kBatch], old[kBatch];
 #pragma unroll
             for (int t = 0; t < kBatch; t++) {
                 const int kk = k0 + lane + 32 * t;
                 if (kk < h) {
                     const int ck = kk, ck1 = kk + 1 == nc ? 0 : kk + 1;
-                    float p = line(ci, cj, ck, ck1);
-                    if (oj) p = 0.5f * (p + line(ci, cj1, ck, ck1));
+                    S p = line(ci, cj, ck, ck1);
+                    if (oj) p = S(0.5) * (p + line(ci, cj1, ck, ck1));
                     if (oi) {
-                        float q = line(ci1, cj, ck, ck1);
-                        if (oj) q = 0.5f * (q + line(ci1, cj1, ck, ck1));
-                        p = 0.5f * (p + q);
+                        S q = line(ci1, cj, ck, ck1);
+                        if (oj) q = S(0.5) * (q + line(ci1, cj1, ck, ck1));
+                        p = S(0.5) * (p + q);
                     }
                     v[t] = p;
                     old[t] = x1[rowx + kk];
@@ -511,61 +536,70 @@ __device__ void split_prolong_black_scalar(const Team& tm, int n, const float* x
 // the adjacent lane by a shuffle, wrapping from lane 0 to lane 31 as the periodic row
 // does. Every sum keeps the scalar versions' order, so results are identical.
 
-template <int V>
-__device__ __forceinline__ void ldv(const float* p, float (&v)[V]) {
-    if constexpr (V == 4) {
+template <int V, class S>
+__device__ __forceinline__ void ldv(const S* p, S (&v)[V]) {
+    if constexpr (sizeof(S) == 4 && V == 4) {
         const float4 t = *reinterpret_cast<const float4*>(p);
         v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-    } else {
+    } else if constexpr (sizeof(S) == 4) {
         const float2 t = *reinterpret_cast<const float2*>(p);
         v[0] = t.x; v[1] = t.y;
+    } else {  // double: one 16-byte load per pair
+#pragma unroll
+        for (int e = 0; e < V; e += 2) {
+            const double2 t = *reinterpret_cast<const double2*>(p + e);
+            v[e] = t.x; v[e + 1] = t.y;
+        }
     }
 }
-template <int V>
-__device__ __forceinline__ void stv(float* p, const float (&v)[V]) {
-    if constexpr (V == 4)
+template <int V, class S>
+__device__ __forceinline__ void stv(S* p, const S (&v)[V]) {
+    if constexpr (sizeof(S) == 4 && V == 4)
         *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-    else
+    else if constexpr (sizeof(S) == 4)
         *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    else
+#pragma unroll
+        for (int e = 0; e < V; e += 2) *reinterpret_cast<double2*>(p + e) = make_double2(v[e], v[e + 1]);
 }
 
 // sum of the six other-colour neighbours of the lane's V points in row o (s as in
 // split_nb_sums), from full-row vector loads
-template <int V>
-__device__ __forceinline__ void vec_nb_sums(const float* xo, const Rows& o, int s, float (&sum)[V]) {
+template <int V, class S>
+__device__ __forceinline__ void vec_nb_sums(const S* xo, const Rows& o, int s, S (&sum)[V]) {
     const int lane = threadIdx.x & 31;
-    float a0[V], a1[V], a2[V], a3[V], cen[V];
+    S a0[V], a1[V], a2[V], a3[V], cen[V];
     ldv<V>(xo + o.im + V * lane, a0);
     ldv<V>(xo + o.ip + V * lane, a1);
     ldv<V>(xo + o.jm + V * lane, a2);
     ldv<V>(xo + o.jp + V * lane, a3);
     ldv<V>(xo + o.c + V * lane, cen);
-    const float prev = __shfl_sync(0xffffffffu, cen[V - 1], (lane + 31) & 31);
-    const float next = __shfl_sync(0xffffffffu, cen[0], (lane + 1) & 31);
+    const S prev = __shfl_sync(0xffffffffu, cen[V - 1], (lane + 31) & 31);
+    const S next = __shfl_sync(0xffffffffu, cen[0], (lane + 1) & 31);
 #pragma unroll
     for (int e = 0; e < V; e++) {
-        const float side = s == 0 ? (e == 0 ? prev : cen[e - 1]) : (e == V - 1 ? next : cen[e + 1]);
-        float t = ((a0[e] + a1[e]) + a2[e]) + a3[e];
+        const S side = s == 0 ? (e == 0 ? prev : cen[e - 1]) : (e == V - 1 ? next : cen[e + 1]);
+        S t = ((a0[e] + a1[e]) + a2[e]) + a3[e];
         sum[e] = (t + cen[e]) + side;
     }
 }
 
-template <int V>
-__device__ void split_gs_vec(const Team& tm, int n, int c, const float* b, float* x, double* acc) {
+template <int V, class S>
+__device__ void split_gs_vec(const Team& tm, int n, int c, const S* b, S* x, double* acc) {
     const int lane = threadIdx.x & 31, h = n >> 1;
     const int hp = h * n * n;
-    const float* xo = x + (1 - c) * hp;
-    float* xc = x + c * hp;
-    const float* bc = b + c * hp;
+    const S* xo = x + (1 - c) * hp;
+    S* xc = x + c * hp;
+    const S* bc = b + c * hp;
     double s_acc = 0.0;
     grid_rows(tm, n, [&](int i, int j) {
         const Rows o = rows_of(n, i, j);
-        float bv[V], sum[V], v[V];
+        S bv[V], sum[V], v[V];
         ldv<V>(bc + o.c + V * lane, bv);
         vec_nb_sums<V>(xo, o, (i + j + c) & 1, sum);
 #pragma unroll
         for (int e = 0; e < V; e++) {
-            v[e] = (bv[e] - sum[e]) * (-1.0f / 6.0f);
+            v[e] = (bv[e] - sum[e]) * neg_sixth<S>();
             s_acc += (double)v[e];
         }
         stv<V>(xc + o.c + V * lane, v);
@@ -573,33 +607,33 @@ __device__ void split_gs_vec(const Team& tm, int n, int c, const float* b, float
     if (acc != nullptr) *acc += s_acc;
 }
 
-template <int V>
-__device__ void split_resid_red_vec(const Team& tm, int n, const float* b, const float* x, float* r) {
+template <int V, class S>
+__device__ void split_resid_red_vec(const Team& tm, int n, const S* b, const S* x, S* r) {
     const int lane = threadIdx.x & 31, h = n >> 1;
     const int hp = h * n * n;
-    const float* x1 = x + hp;
+    const S* x1 = x + hp;
     grid_rows(tm, n, [&](int i, int j) {
         const Rows o = rows_of(n, i, j);
-        float bv[V], xv[V], sum[V], v[V];
+        S bv[V], xv[V], sum[V], v[V];
         ldv<V>(b + o.c + V * lane, bv);
         ldv<V>(x + o.c + V * lane, xv);
         vec_nb_sums<V>(x1, o, (i + j) & 1, sum);
 #pragma unroll
-        for (int e = 0; e < V; e++) v[e] = bv[e] - (sum[e] - 6.0f * xv[e]);
+        for (int e = 0; e < V; e++) v[e] = bv[e] - (sum[e] - S(6) * xv[e]);
         stv<V>(r + o.c + V * lane, v);
     });
 }
 
 // restriction with coarse rows of nc = h = 32 V points: lane l computes K = V l .. V l + V - 1
-template <int V>
-__device__ void split_restrict_vec(const Team& tm, int n, const float* r, float* bc, float* xc) {
+template <int V, class S>
+__device__ void split_restrict_vec(const Team& tm, int n, const S* r, S* bc, S* xc) {
     const int lane = threadIdx.x & 31, nc = n / 2, hc = nc >> 1, h = n >> 1;
     const int hpc = hc * nc * nc;
     grid_rows(tm, nc, [&](int I, int J) {
         const int i = 2 * I, j = 2 * J;
         const int ip = i + 1, im = i == 0 ? n - 1 : i - 1, jp = j + 1, jm = j == 0 ? n - 1 : j - 1;
         auto R = [&](int fi, int fj) { return r + (fi * n + fj) * h + V * lane; };
-        float dpp[V], dpm[V], dmp[V], dmm[V], p0[V], m0[V], q0p[V], q0m[V], cc[V];
+        S dpp[V], dpm[V], dmp[V], dmm[V], p0[V], m0[V], q0p[V], q0m[V], cc[V];
         ldv<V>(R(ip, jp), dpp);
         ldv<V>(R(ip, jm), dpm);
         ldv<V>(R(im, jp), dmp);
@@ -610,14 +644,14 @@ __device__ void split_restrict_vec(const Team& tm, int n, const float* r, float*
         ldv<V>(R(i, jm), q0m);
         ldv<V>(R(i, j), cc);
         // values at K - 1: the previous element, or the previous lane's last one
-        const float p0m = __shfl_sync(0xffffffffu, p0[V - 1], (lane + 31) & 31);
-        const float m0m = __shfl_sync(0xffffffffu, m0[V - 1], (lane + 31) & 31);
-        const float q0pm = __shfl_sync(0xffffffffu, q0p[V - 1], (lane + 31) & 31);
-        const float q0mm = __shfl_sync(0xffffffffu, q0m[V - 1], (lane + 31) & 31);
-        float bv[V];
+        const S p0m = __shfl_sync(0xffffffffu, p0[V - 1], (lane + 31) & 31);
+        const S m0m = __shfl_sync(0xffffffffu, m0[V - 1], (lane + 31) & 31);
+        const S q0pm = __shfl_sync(0xffffffffu, q0p[V - 1], (lane + 31) & 31);
+        const S q0mm = __shfl_sync(0xffffffffu, q0m[V - 1], (lane + 31) & 31);
+        S bv[V];
 #pragma unroll
         for (int e = 0; e < V; e++) {
-            float ee = dpp[e] + dpm[e];
+            S ee = dpp[e] + dpm[e];
             ee += dmp[e];
             ee += dmm[e];
             ee += p0[e];
@@ -628,7 +662,7 @@ __device__ void split_restrict_vec(const Team& tm, int n, const float* r, float*
             ee += e == 0 ? q0pm : q0p[e - 1];
             ee += q0m[e];
             ee += e == 0 ? q0mm : q0m[e - 1];
-            bv[e] = (8.0f * cc[e] + 2.0f * ee) * (4.0f / 64.0f);
+            bv[e] = (S(8) * cc[e] + S(2) * ee) * (S(0.0625));
         }
         // K = V lane + e has colour (I + J + e) & 1 and sits at K >> 1 of its half
         const int rowc = (I * nc + J) * hc;
@@ -638,16 +672,16 @@ __device__ void split_restrict_vec(const Team& tm, int n, const float* r, float*
             const int C = (c0 + e) & 1;
             const int idx = C * hpc + rowc + ((V * lane + e) >> 1);
             bc[idx] = bv[e];
-            xc[idx] = C == 0 ? bv[e] * (-1.0f / 6.0f) : 0.0f;
+            xc[idx] = C == 0 ? bv[e] * neg_sixth<S>() : S(0);
         }
     });
 }
 
-template <int V>
-__device__ void split_prolong_black_vec(const Team& tm, int n, const float* xc, float* x) {
+template <int V, class S>
+__device__ void split_prolong_black_vec(const Team& tm, int n, const S* xc, S* x) {
     const int lane = threadIdx.x & 31, h = n >> 1, nc = n / 2, hc = nc >> 1;
     const int hp = h * n * n, hpc = hc * nc * nc;
-    float* x1 = x + hp;
+    S* x1 = x + hp;
     grid_rows(tm, n, [&](int i, int j) {
         const int s1 = (i + j + 1) & 1;
         const int ci = i >> 1, cj = j >> 1;
@@ -657,22 +691,22 @@ __device__ void split_prolong_black_vec(const Team& tm, int n, const float* xc, 
             return ((CI + CJ + CK) & 1) * hpc + (CI * nc + CJ) * hc + (CK >> 1);
         };
         auto line = [&](int CI, int CJ, int ck, int ck1) {
-            const float a = xc[C(CI, CJ, ck)];
-            return ok ? 0.5f * (a + xc[C(CI, CJ, ck1)]) : a;
+            const S a = xc[C(CI, CJ, ck)];
+            return ok ? S(0.5) * (a + xc[C(CI, CJ, ck1)]) : a;
         };
         const int rowx = (i * n + j) * h + V * lane;
-        float old[V], v[V];
+        S old[V], v[V];
         ldv<V>(x1 + rowx, old);
 #pragma unroll
         for (int e = 0; e < V; e++) {
             const int kk = V * lane + e;
             const int ck = kk, ck1 = kk + 1 == nc ? 0 : kk + 1;
-            float p = line(ci, cj, ck, ck1);
-            if (oj) p = 0.5f * (p + line(ci, cj1, ck, ck1));
+            S p = line(ci, cj, ck, ck1);
+            if (oj) p = S(0.5) * (p + line(ci, cj1, ck, ck1));
             if (oi) {
-                float q = line(ci1, cj, ck, ck1);
-                if (oj) q = 0.5f * (q + line(ci1, cj1, ck, ck1));
-                p = 0.5f * (p + q);
+                S q = line(ci1, cj, ck, ck1);
+                if (oj) q = S(0.5) * (q + line(ci1, cj1, ck, ck1));
+                p = S(0.5) * (p + q);
             }
             v[e] = old[e] + p;
         }
@@ -681,22 +715,26 @@ __device__ void split_prolong_black_vec(const Team& tm, int n, const float* xc, 
 }
 
 // dispatch: rows of 128 floats (n = 256) as float4, of 64 (n = 128) as float2
-__device__ __forceinline__ void split_gs(const Team& tm, int n, int c, const float* b, float* x, double* acc) {
+template <class S>
+__device__ __forceinline__ void split_gs(const Team& tm, int n, int c, const S* b, S* x, double* acc) {
     if (n == 256) split_gs_vec<4>(tm, n, c, b, x, acc);
     else if (n == 128) split_gs_vec<2>(tm, n, c, b, x, acc);
     else split_gs_scalar(tm, n, c, b, x, acc);
 }
-__device__ __forceinline__ void split_resid_red(const Team& tm, int n, const float* b, const float* x, float* r) {
+template <class S>
+__device__ __forceinline__ void split_resid_red(const Team& tm, int n, const S* b, const S* x, S* r) {
     if (n == 256) split_resid_red_vec<4>(tm, n, b, x, r);
     else if (n == 128) split_resid_red_vec<2>(tm, n, b, x, r);
     else split_resid_red_scalar(tm, n, b, x, r);
 }
-__device__ __forceinline__ void split_restrict(const Team& tm, int n, const float* r, float* bc, float* xc) {
+template <class S>
+__device__ __forceinline__ void split_restrict(const Team& tm, int n, const S* r, S* bc, S* xc) {
     if (n == 256) split_restrict_vec<4>(tm, n, r, bc, xc);
     else if (n == 128) split_restrict_vec<2>(tm, n, r, bc, xc);
     else split_restrict_scalar(tm, n, r, bc, xc);
 }
-__device__ __forceinline__ void split_prolong_black(const Team& tm, int n, const float* xc, float* x) {
+template <class S>
+__device__ __forceinline__ void split_prolong_black(const Team& tm, int n, const S* xc, S* x) {
     if (n == 256) split_prolong_black_vec<4>(tm, n, xc, x);
     else if (n == 128) split_prolong_black_vec<2>(tm, n, xc, x);
     else split_prolong_black_scalar(tm, n, xc, x);
@@ -706,7 +744,8 @@ __device__ __forceinline__ void split_prolong_black(const Team& tm, int n, const
 //
 // Shared memory holds x, b, r of levels lsmall..nlev-1 back to back, then (when the
 // coarsest level is solved directly) the coarsest level's Green's function.
-__device__ __forceinline__ float* small_arr(const MixedArgs& a, float* sm, int m, int which) {
+template <class S>
+__device__ __forceinline__ S* small_arr(const MixedArgs& a, S* sm, int m, int which) {
     int off = 0;
     for (int l = a.lsmall; l < m; l++) off += 3 * a.lev_n[l] * a.lev_n[l] * a.lev_n[l];
     return sm + off + which * a.lev_n[m] * a.lev_n[m] * a.lev_n[m];
@@ -714,22 +753,23 @@ __device__ __forceinline__ float* small_arr(const MixedArgs& a, float* sm, int m
 
 // Coarsest level solved exactly: x = G * b (circular convolution with the pseudo-inverse
 // of the unscaled periodic 7-point Laplacian, precomputed on the host), i.e. the
-// zero-mean solution of L x = b - mean(b). S lanes share one output point.
-__device__ void coarse_direct(int n, const float* g, const float* b, float* x) {
+// zero-mean solution of L x = b - mean(b). Several lanes share one output point.
+template <class S>
+__device__ void coarse_direct(int n, const S* g, const S* b, S* x) {
     const int N = n * n * n;
-    int S = 1;
-    while (S < 32 && 2 * S * N <= (int)blockDim.x) S *= 2;
-    const int p = threadIdx.x / S, sub = threadIdx.x % S;
-    float acc = 0.0f;
+    int lanes = 1;  // lanes that share one output point
+    while (lanes < 32 && 2 * lanes * N <= (int)blockDim.x) lanes *= 2;
+    const int p = threadIdx.x / lanes, sub = threadIdx.x % lanes;
+    S acc = S(0);
     if (p < N) {
         const int pi = p / (n * n), pj = (p / n) % n, pk = p % n;
-        for (int q = sub; q < N; q += S) {
+        for (int q = sub; q < N; q += lanes) {
             const int qi = q / (n * n), qj = (q / n) % n, qk = q % n;
             const int d = (((pi - qi + n) % n) * n + ((pj - qj + n) % n)) * n + ((pk - qk + n) % n);
             acc += g[d] * b[q];
         }
     }
-    for (int o = S >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    for (int o = lanes >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
     if (p < N && sub == 0) x[p] = acc;
 }
 
@@ -738,8 +778,8 @@ __device__ void coarse_direct(int n, const float* g, const float* b, float* x) {
 // restrict_point and prolong_point, with the size known at compile time: 32-bit indices
 // and periodic wraps by masks instead of the general helpers' divisions and 64-bit
 // arithmetic, which on one CTA made each pass of these small levels instruction-bound.
-template <int N>
-__device__ __forceinline__ void sm_smooth(const float* b, float* x, int first_colour, int half_sweeps) {
+template <int N, class S>
+__device__ __forceinline__ void sm_smooth(const S* b, S* x, int first_colour, int half_sweeps) {
     constexpr int H = N / 2, M = N - 1, TOT = N * N * H;
     for (int hs = 0; hs < half_sweeps; hs++) {
         const int colour = (first_colour + hs) & 1;
@@ -747,32 +787,32 @@ __device__ __forceinline__ void sm_smooth(const float* b, float* x, int first_co
             const int i = p / (N * H), j = (p / H) % N, kk = p % H;
             const int k = 2 * kk + ((i + j + colour) & 1);
             const int c = (i * N + j) * N + k;
-            float s = x[(((i - 1) & M) * N + j) * N + k] + x[(((i + 1) & M) * N + j) * N + k];
+            S s = x[(((i - 1) & M) * N + j) * N + k] + x[(((i + 1) & M) * N + j) * N + k];
             s += x[(i * N + ((j - 1) & M)) * N + k];
             s += x[(i * N + ((j + 1) & M)) * N + k];
             s += x[(i * N + j) * N + ((k - 1) & M)];
             s += x[(i * N + j) * N + ((k + 1) & M)];
-            x[c] = (b[c] - s) * (-1.0f / 6.0f);
+            x[c] = (b[c] - s) * neg_sixth<S>();
         }
         __syncthreads();
     }
 }
-template <int N>
-__device__ __forceinline__ void sm_resid(const float* b, const float* x, float* r) {
+template <int N, class S>
+__device__ __forceinline__ void sm_resid(const S* b, const S* x, S* r) {
     constexpr int M = N - 1, TOT = N * N * N;
     for (int p = threadIdx.x; p < TOT; p += blockDim.x) {
         const int i = p / (N * N), j = (p / N) % N, k = p % N;
-        float s = x[(((i + 1) & M) * N + j) * N + k] + x[(((i - 1) & M) * N + j) * N + k];
+        S s = x[(((i + 1) & M) * N + j) * N + k] + x[(((i - 1) & M) * N + j) * N + k];
         s += x[(i * N + ((j + 1) & M)) * N + k];
         s += x[(i * N + ((j - 1) & M)) * N + k];
         s += x[(i * N + j) * N + ((k + 1) & M)];
         s += x[(i * N + j) * N + ((k - 1) & M)];
-        r[p] = b[p] - (s - 6.0f * x[p]);
+        r[p] = b[p] - (s - S(6) * x[p]);
     }
     __syncthreads();
 }
-template <int N>
-__device__ __forceinline__ void sm_restrict(const float* r, float* bc, float* xc) {
+template <int N, class S>
+__device__ __forceinline__ void sm_restrict(const S* r, S* bc, S* xc) {
     constexpr int NC = N / 2, M = N - 1, N2 = N * N, TOT = NC * NC * NC;
     for (int p = threadIdx.x; p < TOT; p += blockDim.x) {
         const int I = p / (NC * NC), J = (p / NC) % NC, K = p % NC;
@@ -780,21 +820,21 @@ __device__ __forceinline__ void sm_restrict(const float* r, float* bc, float* xc
         const int i0 = i * N2, i1 = ((i + 1) & M) * N2, i2 = ((i - 1) & M) * N2;
         const int j0 = j * N, j1 = ((j + 1) & M) * N, j2 = ((j - 1) & M) * N;
         const int k0 = k, k1 = (k + 1) & M, k2 = (k - 1) & M;
-        const float f = r[i2 + j0 + k0] + r[i1 + j0 + k0] + r[i0 + j2 + k0] + r[i0 + j1 + k0] + r[i0 + j0 + k2] +
+        const S f = r[i2 + j0 + k0] + r[i1 + j0 + k0] + r[i0 + j2 + k0] + r[i0 + j1 + k0] + r[i0 + j0 + k2] +
                         r[i0 + j0 + k1];
-        const float e = r[i1 + j0 + k2] + r[i1 + j0 + k1] + r[i2 + j0 + k2] + r[i2 + j0 + k1] + r[i1 + j2 + k0] +
+        const S e = r[i1 + j0 + k2] + r[i1 + j0 + k1] + r[i2 + j0 + k2] + r[i2 + j0 + k1] + r[i1 + j2 + k0] +
                         r[i1 + j1 + k0] + r[i2 + j2 + k0] + r[i2 + j1 + k0] + r[i0 + j2 + k2] + r[i0 + j2 + k1] +
                         r[i0 + j1 + k2] + r[i0 + j1 + k1];
-        const float c = r[i1 + j1 + k2] + r[i1 + j1 + k1] + r[i1 + j2 + k2] + r[i1 + j2 + k1] + r[i2 + j1 + k2] +
+        const S c = r[i1 + j1 + k2] + r[i1 + j1 + k1] + r[i1 + j2 + k2] + r[i1 + j2 + k1] + r[i2 + j1 + k2] +
                         r[i2 + j1 + k1] + r[i2 + j2 + k2] + r[i2 + j2 + k1];
-        const float bv = (8.0f * r[i0 + j0 + k0] + 4.0f * f + 2.0f * e + c) * (4.0f / 64.0f);
+        const S bv = (S(8) * r[i0 + j0 + k0] + S(4) * f + S(2) * e + c) * (S(0.0625));
         bc[p] = bv;
-        xc[p] = ((I + J + K) & 1) == 0 ? bv * (-1.0f / 6.0f) : 0.0f;
+        xc[p] = ((I + J + K) & 1) == 0 ? bv * neg_sixth<S>() : S(0);
     }
     __syncthreads();
 }
-template <int N>
-__device__ __forceinline__ void sm_prolong(const float* xc, float* x) {
+template <int N, class S>
+__device__ __forceinline__ void sm_prolong(const S* xc, S* x) {
     constexpr int NC = N / 2, MC = NC - 1, NC2 = NC * NC, TOT = N * N * N;
     for (int p = threadIdx.x; p < TOT; p += blockDim.x) {
         const int i = p / (N * N), j = (p / N) % N, k = p % N;
@@ -802,13 +842,13 @@ __device__ __forceinline__ void sm_prolong(const float* xc, float* x) {
         const int i0 = ci * NC2, i1 = ((ci + 1) & MC) * NC2;
         const int j0 = cj * NC, j1 = ((cj + 1) & MC) * NC;
         const int k0 = ck, k1 = (ck + 1) & MC;
-        const float wi = (i & 1) ? 0.5f : 0.0f, wj = (j & 1) ? 0.5f : 0.0f, wk = (k & 1) ? 0.5f : 0.0f;
-        const float a00 = xc[i0 + j0 + k0] * (1.0f - wk) + xc[i0 + j0 + k1] * wk;
-        const float a01 = xc[i0 + j1 + k0] * (1.0f - wk) + xc[i0 + j1 + k1] * wk;
-        const float a10 = xc[i1 + j0 + k0] * (1.0f - wk) + xc[i1 + j0 + k1] * wk;
-        const float a11 = xc[i1 + j1 + k0] * (1.0f - wk) + xc[i1 + j1 + k1] * wk;
-        const float b0 = a00 * (1.0f - wj) + a01 * wj, b1 = a10 * (1.0f - wj) + a11 * wj;
-        x[p] += b0 * (1.0f - wi) + b1 * wi;
+        const S wi = (i & 1) ? S(0.5) : S(0), wj = (j & 1) ? S(0.5) : S(0), wk = (k & 1) ? S(0.5) : S(0);
+        const S a00 = xc[i0 + j0 + k0] * (S(1) - wk) + xc[i0 + j0 + k1] * wk;
+        const S a01 = xc[i0 + j1 + k0] * (S(1) - wk) + xc[i0 + j1 + k1] * wk;
+        const S a10 = xc[i1 + j0 + k0] * (S(1) - wk) + xc[i1 + j0 + k1] * wk;
+        const S a11 = xc[i1 + j1 + k0] * (S(1) - wk) + xc[i1 + j1 + k1] * wk;
+        const S b0 = a00 * (S(1) - wj) + a01 * wj, b1 = a10 * (S(1) - wj) + a11 * wj;
+        x[p] += b0 * (S(1) - wi) + b1 * wi;
     }
     __syncthreads();
 }
@@ -816,12 +856,13 @@ __device__ __forceinline__ bool sm_fixed(int n) { return n == 4 || n == 8 || n =
 
 // Restricts the residual of level lsmall-1 (global) into shared memory, runs the rest of
 // the V-cycle there and writes level lsmall's correction back to lev_x[lsmall].
-__device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above) {
+template <class S>
+__device__ void small_vcycle(const MixedArgs& a, S* sm, const S* r_above) {
     const int L = a.nlev, ls = a.lsmall;
     auto smooth = [&](int m, int first_colour, int half_sweeps) {
         const int n = a.lev_n[m];
-        float* x = small_arr(a, sm, m, 0);
-        const float* b = small_arr(a, sm, m, 1);
+        S* x = small_arr(a, sm, m, 0);
+        const S* b = small_arr(a, sm, m, 1);
         if (n == 16) return sm_smooth<16>(b, x, first_colour, half_sweeps);
         if (n == 8) return sm_smooth<8>(b, x, first_colour, half_sweeps);
         if (n == 4) return sm_smooth<4>(b, x, first_colour, half_sweeps);
@@ -830,32 +871,32 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above
             __syncthreads();
         }
     };
-    float* gsm = small_arr(a, sm, L, 0);  // just past the last level
+    S* gsm = small_arr(a, sm, L, 0);  // just past the last level
     if (a.coarse_g != nullptr) {
         const int N = a.lev_n[L - 1] * a.lev_n[L - 1] * a.lev_n[L - 1];
-        for (int p = threadIdx.x; p < N; p += blockDim.x) gsm[p] = a.coarse_g[p];
+        for (int p = threadIdx.x; p < N; p += blockDim.x) gsm[p] = static_cast<const S*>(a.coarse_g)[p];
     }
     {
-        const float* r = r_above;  // red residual of level ls - 1, split layout
+        const S* r = r_above;  // red residual of level ls - 1, split layout
         const int nf = a.lev_n[ls - 1], nc = a.lev_n[ls];
-        float* bs = small_arr(a, sm, ls, 1);
-        float* xs = small_arr(a, sm, ls, 0);
+        S* bs = small_arr(a, sm, ls, 1);
+        S* xs = small_arr(a, sm, ls, 0);
         cta_pts(nc, [&](int I, int J, int K) {
-            const float bv = split_restrict_value(nf, r, I, J, K);
+            const S bv = split_restrict_value(nf, r, I, J, K);
             const int cc = (I * nc + J) * nc + K;
             bs[cc] = bv;
-            xs[cc] = ((I + J + K) & 1) == 0 ? bv * (-1.0f / 6.0f) : 0.0f;
+            xs[cc] = ((I + J + K) & 1) == 0 ? bv * neg_sixth<S>() : S(0);
         });
         __syncthreads();
     }
     for (int m = ls; m < L - 1; m++) {
         const int n = a.lev_n[m];
         smooth(m, 1, 2 * a.nu1 - 1);
-        float* x = small_arr(a, sm, m, 0);
-        float* b = small_arr(a, sm, m, 1);
-        float* r = small_arr(a, sm, m, 2);
-        float* bc = small_arr(a, sm, m + 1, 1);
-        float* xc = small_arr(a, sm, m + 1, 0);
+        S* x = small_arr(a, sm, m, 0);
+        S* b = small_arr(a, sm, m, 1);
+        S* r = small_arr(a, sm, m, 2);
+        S* bc = small_arr(a, sm, m + 1, 1);
+        S* xc = small_arr(a, sm, m + 1, 0);
         if (sm_fixed(n)) {
             if (n == 16) { sm_resid<16>(b, x, r); sm_restrict<16>(r, bc, xc); }
             else if (n == 8) { sm_resid<8>(b, x, r); sm_restrict<8>(r, bc, xc); }
@@ -875,8 +916,8 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above
     }
     for (int m = L - 2; m >= ls; m--) {
         const int n = a.lev_n[m];
-        const float* xc = small_arr(a, sm, m + 1, 0);
-        float* x = small_arr(a, sm, m, 0);
+        const S* xc = small_arr(a, sm, m + 1, 0);
+        S* x = small_arr(a, sm, m, 0);
         if (n == 16) sm_prolong<16>(xc, x);
         else if (n == 8) sm_prolong<8>(xc, x);
         else {
@@ -886,8 +927,8 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above
         smooth(m, 0, 2 * a.nu2);
     }
     const int nl = a.lev_n[ls];
-    const float* xs = small_arr(a, sm, ls, 0);
-    float* dst = a.lev_x[ls];  // split layout
+    const S* xs = small_arr(a, sm, ls, 0);
+    S* dst = lev_x<S>(a, ls);  // split layout
     cta_pts(nl, [&](int i, int j, int k) { dst[split_idx(nl, i, j, k)] = xs[(i * nl + j) * nl + k]; });
 }
 
@@ -896,20 +937,21 @@ __device__ void small_vcycle(const MixedArgs& a, float* sm, const float* r_above
 // periodic 7-point Laplacian (coarse_g, precomputed on the host), i.e. the zero-mean
 // solution of L x = b - mean(b). Every CTA stages G and b in shared memory; a warp forms
 // one point's sum, its lanes taking the (j, k) columns r = lane + 32 t of every i plane.
-__device__ void team_direct(const MixedArgs& a, const Team& tm, float* sm, int l) {
+template <class S>
+__device__ void team_direct(const MixedArgs& a, const Team& tm, S* sm, int l) {
     const int n = a.lev_n[l], n2 = n * n, N = n2 * n;
-    float* gs = sm;
-    float* bs = sm + N;
-    const float* b = a.lev_b[l];  // split layout
+    S* gs = sm;
+    S* bs = sm + N;
+    const S* b = lev_b<S>(a, l);  // split layout
     for (int p = threadIdx.x; p < N; p += blockDim.x) {
-        gs[p] = a.coarse_g[p];
+        gs[p] = static_cast<const S*>(a.coarse_g)[p];
         const int i = p / n2, j = (p / n) % n, k = p % n;
         bs[p] = b[split_idx(n, i, j, k)];
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     constexpr int TM = (kMixedTeamDirectN * kMixedTeamDirectN + 31) / 32;
-    float* x = a.lev_x[l];
+    S* x = lev_x<S>(a, l);
     for (int p = tm.b * nw + w; p < N; p += tm.nblk * nw) {
         const int pi = p / n2, pj = (p / n) % n, pk = p % n;
         int ro[TM], go[TM];  // b offset (j n + k) and G offset of the lane's columns
@@ -923,17 +965,17 @@ __device__ void team_direct(const MixedArgs& a, const Team& tm, float* sm, int l
             ro[t] = r < n2 ? r : -1;
             go[t] = dj * n + dk;
         }
-        float acc = 0.0f;
+        S acc = S(0);
         for (int qi = 0; qi < n; qi++) {
             int di = pi - qi;
             di += di < 0 ? n : 0;
-            const float* gp = gs + di * n2;
-            const float* bp = bs + qi * n2;
+            const S* gp = gs + di * n2;
+            const S* bp = bs + qi * n2;
 #pragma unroll
             for (int t = 0; t < TM; t++)
-                if (ro[t] >= 0) acc = fmaf(gp[go[t]], bp[ro[t]], acc);
+                if (ro[t] >= 0) acc = fma_s(gp[go[t]], bp[ro[t]], acc);
         }
-        acc = warp_sumf(acc);
+        acc = warp_sum_s(acc);
         if (lane == 0) x[split_idx(n, pi, pj, pk)] = acc;
     }
 }
@@ -941,10 +983,11 @@ __device__ void team_direct(const MixedArgs& a, const Team& tm, float* sm, int l
 // Grid-wide red-black sweeps of level l: `half_sweeps` colours starting at first_colour,
 // a grid barrier after each except (when skip_last_barrier) the last. When esum is not
 // null the values written in the last two half-sweeps are summed into it.
-__device__ bool grid_smooth(const MixedArgs& a, const Team& tm, int l, float* x, int first_colour, int half_sweeps,
+template <class S>
+__device__ bool grid_smooth(const MixedArgs& a, const Team& tm, int l, S* x, int first_colour, int half_sweeps,
                             unsigned& epoch, double* esum, bool skip_last_barrier) {
     for (int h = 0; h < half_sweeps; h++) {
-        split_gs(tm, a.lev_n[l], (first_colour + h) & 1, a.lev_b[l], x,
+        split_gs(tm, a.lev_n[l], (first_colour + h) & 1, lev_b<S>(a, l), x,
                  esum != nullptr && h >= half_sweeps - 2 ? esum : nullptr);
         if (h == half_sweeps - 1 && skip_last_barrier) break;
         if (!team_sync(tm, epoch)) return false;
@@ -956,18 +999,19 @@ __device__ bool grid_smooth(const MixedArgs& a, const Team& tm, int l, float* x,
 // lev_b[0], whose first red half-sweep has been done by the residual pass. Ends after
 // the last half-sweep of level 0 without a barrier, with this thread's share of sum(x0)
 // in esum.
-__device__ bool vcycle(const MixedArgs& a, const Team& tm, float* sm, unsigned& epoch, double& esum, int outer,
-                       float* x0, float* r0) {
+template <class S>
+__device__ bool vcycle(const MixedArgs& a, const Team& tm, S* sm, unsigned& epoch, double& esum, int outer,
+                       S* x0, S* r0) {
     const int L = a.nlev, ls = a.lsmall;
     const int lg = ls < L ? ls : L - 1;  // levels 0..lg-1 are smoothed and restricted on the grid
-    auto X = [&](int l) { return l == 0 ? x0 : a.lev_x[l]; };
-    auto R = [&](int l) { return l == 0 ? r0 : a.lev_r[l]; };
+    auto X = [&](int l) { return l == 0 ? x0 : lev_x<S>(a, l); };
+    auto R = [&](int l) { return l == 0 ? r0 : lev_r<S>(a, l); };
     for (int l = 0; l < lg; l++) {
         if (!grid_smooth(a, tm, l, X(l), 1, 2 * a.nu1 - 1, epoch, nullptr, false)) return false;
-        split_resid_red(tm, a.lev_n[l], a.lev_b[l], X(l), R(l));
+        split_resid_red(tm, a.lev_n[l], lev_b<S>(a, l), X(l), R(l));
         if (!team_sync(tm, epoch)) return false;
         if (l + 1 < ls) {
-            split_restrict(tm, a.lev_n[l], R(l), a.lev_b[l + 1], X(l + 1));
+            split_restrict(tm, a.lev_n[l], R(l), lev_b<S>(a, l + 1), X(l + 1));
             if (!team_sync(tm, epoch)) return false;
         }
     }
@@ -995,9 +1039,9 @@ __device__ bool vcycle(const MixedArgs& a, const Team& tm, float* sm, unsigned& 
 // (START_ZERO), X[] (START_X) or the extrapolation 2 X[] - Xp[] (START_EXTRAP); B is c q
 // when RHS_Q, else tmp.
 enum StartKind { START_ZERO, START_X, START_EXTRAP };
-template <int START, bool RHS_Q>
+template <int START, bool RHS_Q, class S>
 __device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs& a, const double* X,
-                                                const double* Xp, float* e, float* rb) {
+                                                const double* Xp, S* e, S* rb) {
     const int n = a.n;
     double rmax = 0.0;
     grid_pts(tm, n, [&](int i, int j, int k) {
@@ -1014,10 +1058,10 @@ __device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs&
             s = s + x(o.km);
             r = (RHS_Q ? a.q[o.c] * a.c : a.tmp[o.c]) - (s - x(o.c) * 6.0);
         }
-        const float rf = (float)r;
+        const S rf = (S)r;
         const int sx = split_idx(n, i, j, k);
         rb[sx] = rf;
-        e[sx] = ((i + j + k) & 1) == 0 ? rf * (-1.0f / 6.0f) : 0.0f;
+        e[sx] = ((i + j + k) & 1) == 0 ? rf * neg_sixth<S>() : S(0);
         rmax = fmax(rmax, fabs(r));
     });
     return rmax;
@@ -1026,9 +1070,9 @@ __device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs&
 // Vectorised residual pass for n % 64 == 0: a warp covers 64 consecutive k of a row with
 // one double2 per lane; k - 1 / k + 1 come from the adjacent lane by a shuffle, from memory
 // at the ends of the 64. Same sums, in the same order, as residual_pass.
-template <int START, bool RHS_Q>
+template <int START, bool RHS_Q, class S>
 __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedArgs& a, const double* X,
-                                                    const double* Xp, float* e, float* rb) {
+                                                    const double* Xp, S* e, S* rb) {
     const int n = a.n, h = n >> 1, lane = threadIdx.x & 31;
     const int hp = h * n * n;
     double rmax = 0.0;
@@ -1088,29 +1132,29 @@ __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedA
                 r0 = bq.x - (s0 - xc.x * 6.0);
                 r1 = bq.y - (s1 - xc.y * 6.0);
             }
-            const float rf0 = (float)r0, rf1 = (float)r1;
+            const S rf0 = (S)r0, rf1 = (S)r1;
             const int p0 = cA * hp + srow + (k >> 1), p1 = (cA ^ 1) * hp + srow + (k >> 1);
             rb[p0] = rf0;
             rb[p1] = rf1;
-            e[p0] = cA == 0 ? rf0 * (-1.0f / 6.0f) : 0.0f;
-            e[p1] = cA == 1 ? rf1 * (-1.0f / 6.0f) : 0.0f;
+            e[p0] = cA == 0 ? rf0 * neg_sixth<S>() : S(0);
+            e[p1] = cA == 1 ? rf1 * neg_sixth<S>() : S(0);
             rmax = fmax(rmax, fmax(fabs(r0), fabs(r1)));
         }
     });
     return rmax;
 }
 
-template <int START, bool RHS_Q>
+template <int START, bool RHS_Q, class S>
 __device__ __forceinline__ double residual_any(const Team& tm, const MixedArgs& a, const double* X,
-                                               const double* Xp, float* e, float* rb) {
+                                               const double* Xp, S* e, S* rb) {
     if (a.n % 64 == 0) return residual_pass_vec<START, RHS_Q>(tm, a, X, Xp, e, rb);
     return residual_pass<START, RHS_Q>(tm, a, X, Xp, e, rb);
 }
 
 // home = X + (e - emean) with X as residual_pass reads it (0, X[], 2 X[] - phi_prev[]).
-template <int START>
+template <int START, class S>
 __device__ __forceinline__ void update_pass(const Team& tm, const MixedArgs& a, const double* X, double* home,
-                                            const float* e, double emean) {
+                                            const S* e, double emean) {
     const int n = a.n;
     if (n % 64 == 0) {  // double2 per lane, e from both colour halves
         const int h = n >> 1, lane = threadIdx.x & 31, hp = h * n * n;
@@ -1126,7 +1170,7 @@ __device__ __forceinline__ void update_pass(const Team& tm, const MixedArgs& a, 
                     xo.x = 2 * xo.x - p.x;
                     xo.y = 2 * xo.y - p.y;
                 }
-                const float e0 = e[cA * hp + srow + (k >> 1)], e1 = e[(cA ^ 1) * hp + srow + (k >> 1)];
+                const S e0 = e[cA * hp + srow + (k >> 1)], e1 = e[(cA ^ 1) * hp + srow + (k >> 1)];
                 *reinterpret_cast<double2*>(home + row + k) =
                     make_double2(xo.x + ((double)e0 - emean), xo.y + ((double)e1 - emean));
             }
@@ -1141,7 +1185,8 @@ __device__ __forceinline__ void update_pass(const Team& tm, const MixedArgs& a, 
 }
 
 // The solve of one system by one team of CTAs.
-__device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, float* sm) {
+template <class S>
+__device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, S* sm) {
     const int n = a.n;
     unsigned epoch = 0;
     int seq = 0;
@@ -1191,8 +1236,8 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
     // with the correction's first red half-sweep from e = 0; e = V-cycle; X += e - mean(e).
     // X starts as X0 (read-only; zero for INIT) and lives in `home` from the first update.
     const double* Xs = X0;
-    float* e = a.lev_x[0];
-    float* rb = a.lev_b[0];
+    S* e = lev_x<S>(a, 0);
+    S* rb = lev_b<S>(a, 0);
     int outer = 0;
     while (ok) {
         stamp_outer(a, outer, 0);
@@ -1217,7 +1262,7 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
         }
         if (outer >= a.max_outer) break;
         double esum = 0.0, m0 = 0.0;
-        ok = vcycle(a, tm, sm, epoch, esum, outer, e, a.lev_r[0]);
+        ok = vcycle(a, tm, sm, epoch, esum, outer, e, lev_r<S>(a, 0));
         if (!ok) break;
         stamp_outer(a, outer, 4);
         // mean of the correction (the periodic Laplacian's null space)
@@ -1256,16 +1301,21 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, f
     }
 }
 
-__global__ void __launch_bounds__(kThreads, 1) mixed_kernel(MixedArgs a) {
-    extern __shared__ float sm[];
+// Threads per CTA: 1024 with FP32 levels; 512 with FP64 levels, whose vectorised passes
+// hold twice the registers per value (64 registers per thread at 1024 threads would spill).
+template <class S> constexpr int threads_of() { return sizeof(S) == 8 ? 512 : kThreads; }
+
+template <class S>
+__global__ void __launch_bounds__(threads_of<S>(), 1) mixed_kernel(MixedArgs a) {
+    extern __shared__ __align__(16) unsigned char sm_raw[];
     const Team tm{(int)gridDim.x, (int)blockIdx.x, a.bar, a.partials};
-    mixed_body(a, tm, sm);
+    mixed_body(a, tm, reinterpret_cast<S*>(sm_raw));
 }
 
-// Many systems in one launch: system r is worked by CTAs [start[r], start[r+1]).
+// Many systems in one launch (FP32 levels): system r is worked by CTAs [start[r], start[r+1]).
 __global__ void __launch_bounds__(kThreads, 1)
     mixed_batch_kernel(const MixedArgs* __restrict__ list, const int* __restrict__ start, int nsys) {
-    extern __shared__ float sm[];
+    extern __shared__ __align__(16) unsigned char sm_raw[];
     int lo = 0, hi = nsys - 1;  // last r with start[r] <= blockIdx.x
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -1279,24 +1329,29 @@ __global__ void __launch_bounds__(kThreads, 1)
         reinterpret_cast<int*>(&a)[w] = reinterpret_cast<const int*>(list + lo)[w];
     __syncthreads();
     const Team tm{b1 - b0, (int)blockIdx.x - b0, a.bar, a.partials};
-    mixed_body(a, tm, sm);
+    mixed_body(a, tm, reinterpret_cast<float*>(sm_raw));
 }
 
-int g_mixed_device = -1;
-int g_mixed_blocks = 0;
-size_t g_mixed_smem_set = 0;
+// Launch configuration of one kernel variant, set up once per device.
+struct Variant {
+    int device = -1;
+    int blocks = 0;
+    size_t smem_set = 0;
+};
+Variant g_mixed_f32, g_mixed_f64;
 int g_batch_device = -1;
 size_t g_batch_smem_set = 0;
 
 size_t small_smem_bytes(const MixedArgs& a) {
+    const size_t w = a.fp64 ? sizeof(double) : sizeof(float);
     if (a.coarse_team) {  // G and b of the coarsest level in every CTA
         const size_t nc = (size_t)a.lev_n[a.nlev - 1];
-        return 2 * nc * nc * nc * sizeof(float);
+        return 2 * nc * nc * nc * w;
     }
     size_t v = 0;
     for (int m = a.lsmall; m < a.nlev; m++) v += 3 * (size_t)a.lev_n[m] * a.lev_n[m] * a.lev_n[m];
     if (a.coarse_g != nullptr) v += (size_t)a.lev_n[a.nlev - 1] * a.lev_n[a.nlev - 1] * a.lev_n[a.nlev - 1];
-    return v * sizeof(float);
+    return v * w;
 }
 
 }  // namespace
@@ -1312,7 +1367,7 @@ int mixed_levels(int n, int* sizes) {
     return L;
 }
 
-void mixed_coarse_green(int n, float* g) {
+void mixed_coarse_green(int n, double* g) {
     // g[d] = (1/N) sum_k e^{i w k.d} / lambda(k) over k != 0 (real: 1/lambda is even),
     // as three 1-D inverse transforms of 1/lambda, one axis at a time.
     const int N = n * n * n;
@@ -1345,7 +1400,13 @@ void mixed_coarse_green(int n, float* g) {
         re.swap(tr);
         im.swap(ti);
     }
-    for (int d = 0; d < N; d++) g[d] = (float)(re[d] / N);
+    for (int d = 0; d < N; d++) g[d] = re[d] / N;
+}
+
+void mixed_coarse_green(int n, float* g) {
+    std::vector<double> gd((size_t)n * n * n);
+    mixed_coarse_green(n, gd.data());
+    for (size_t d = 0; d < gd.size(); d++) g[d] = (float)gd[d];
 }
 
 int mixed_small_level(int nlev, const int* sizes) {
@@ -1383,29 +1444,40 @@ void mixed_batch_launch(const MixedArgs* list, const int* start, int nsys, int n
                                           stream));
 }
 
-void mixed_launch(const MixedArgs& a, cudaStream_t stream) {
-    if (a.lsmall < 1 || a.lsmall > a.nlev || a.nlev < 2 || a.nu1 < 1 || a.nu2 < 1 || a.coarse_sweeps < 1)
-        fatal("mixed solver: invalid level plan");
-    const size_t smem = small_smem_bytes(a);
+namespace {
+template <class S>
+void launch_variant(Variant& v, const MixedArgs& a, size_t smem, cudaStream_t stream) {
+    const void* fn = (const void*)mixed_kernel<S>;
+    constexpr int threads = threads_of<S>();
     int dev;
     MZB_CHECK(cudaGetDevice(&dev));
-    if (g_mixed_device != dev || smem > g_mixed_smem_set) {
+    if (v.device != dev || smem > v.smem_set) {
         int sms = 0, per_sm = 0;
         if (smem > 48 * 1024)
-            MZB_CHECK(cudaFuncSetAttribute(mixed_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            MZB_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         MZB_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        MZB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mixed_kernel, kThreads, smem));
+        MZB_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
         if (per_sm < 1) fatal("mixed solver: kernel cannot be resident on this device");
-        g_mixed_device = dev;
-        g_mixed_blocks = sms;
-        g_mixed_smem_set = smem > g_mixed_smem_set ? smem : g_mixed_smem_set;
+        v.device = dev;
+        v.blocks = sms;
+        v.smem_set = smem > v.smem_set ? smem : v.smem_set;
     }
     MZB_CHECK(cudaMemsetAsync(a.bar, 0, sizeof(GridBarrier), stream));
     MixedArgs copy = a;
     void* params[] = {&copy};
     count_launch();
-    MZB_CHECK(cudaLaunchCooperativeKernel((const void*)mixed_kernel, dim3(g_mixed_blocks), dim3(kThreads), params,
-                                          smem, stream));
+    MZB_CHECK(cudaLaunchCooperativeKernel(fn, dim3(v.blocks), dim3(threads), params, smem, stream));
+}
+}  // namespace
+
+void mixed_launch(const MixedArgs& a, cudaStream_t stream) {
+    if (a.lsmall < 1 || a.lsmall > a.nlev || a.nlev < 2 || a.nu1 < 1 || a.nu2 < 1 || a.coarse_sweeps < 1)
+        fatal("mixed solver: invalid level plan");
+    const size_t smem = small_smem_bytes(a);
+    if (a.fp64)
+        launch_variant<double>(g_mixed_f64, a, smem, stream);
+    else
+        launch_variant<float>(g_mixed_f32, a, smem, stream);
 }
 
 }  // namespace mzb

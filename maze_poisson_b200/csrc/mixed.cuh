@@ -1,4 +1,5 @@
-// Mixed-precision field solve (see mixed.cu).
+// Multigrid field solve with FP64 refinement (see mixed.cu): FP32 levels (the
+// mixed-precision form) or FP64 levels (the FP64 multigrid form).
 #pragma once
 
 #include "mzb_common.cuh"
@@ -18,14 +19,16 @@ struct MixedArgs {
     int max_outer;      // refinement steps before giving up (-1 returned)
     int nu1, nu2;       // red-black GS sweeps before / after the coarse correction (>= 1)
     int coarse_sweeps;  // sweeps on the coarsest level (>= 1) when coarse_g is null
-    const float* coarse_g;  // Green's function of the coarsest level (mixed_coarse_green) or null
+    int fp64;               // 1: level arrays and V-cycle in FP64, 0: in FP32
+    const void* coarse_g;   // Green's function of the coarsest level (mixed_coarse_green), stored
+                            // like the levels (float or double), or null
     int coarse_team;        // 1: the coarsest level is solved by every CTA of the team with coarse_g
     int nlev;
     int lsmall;         // first level held in shared memory (nlev if none; >= 1)
     int lev_n[kMixedMaxLevels];
-    float* lev_x[kMixedMaxLevels];
-    float* lev_b[kMixedMaxLevels];
-    float* lev_r[kMixedMaxLevels];
+    void* lev_x[kMixedMaxLevels];  // level arrays: float, or double when fp64
+    void* lev_b[kMixedMaxLevels];
+    void* lev_r[kMixedMaxLevels];
     const double* q;
     const uint32_t* qmask;  // segments of 64 k where q may be nonzero (spread_charges), or null
     const double* phi_old;
@@ -53,13 +56,14 @@ constexpr int kMixedTeamDirectN = 16;
 // Pseudo-inverse kernel of the unscaled periodic 7-point Laplacian on an n^3 grid:
 // g[d] = (1/n^3) sum_{k != 0} cos(2 pi k.d / n) / lambda(k),
 // lambda(k) = 2 cos(2 pi k1/n) + 2 cos(2 pi k2/n) + 2 cos(2 pi k3/n) - 6.
+void mixed_coarse_green(int n, double* g);
 void mixed_coarse_green(int n, float* g);
 void mixed_launch(const MixedArgs& a, cudaStream_t stream);
 // Dynamic shared memory one system's solve needs.
 size_t mixed_smem_bytes(const MixedArgs& a);
 // CTAs of a full (one per SM) launch on the current device.
 int mixed_grid_blocks();
-// Solve nsys systems in one cooperative launch of nblocks CTAs: system r (list[r], in
+// Solve nsys systems (FP32 levels) in one cooperative launch of nblocks CTAs: system r (list[r], in
 // device memory) is worked by CTAs [start[r], start[r+1]), start[nsys] = nblocks, each
 // team on its own barrier (zeroed by the caller) and partials. smem is the largest
 // mixed_smem_bytes of the list.

@@ -36,15 +36,20 @@ using namespace mzb;
 // with precond = 1) on an n^3 grid with 2 <= n <= 64, on device buffers the caller owns.
 // No device memory is allocated or freed by this call.
 //
-//  * b, x0, x: device pointers to n^3 doubles (x may equal x0); stream: the cudaStream_t
-//    to run on (NULL = the default stream). The call returns after the solve finished.
+//  * b, x0, x: device pointers to n^3 doubles on the current device (x may equal x0);
+//    stream: the cudaStream_t to run on (NULL = the default stream).
+//  * Synchronous: the call waits for the solve on `stream` and copies the result word to
+//    the host, so it must not be called while `stream` (or, in global capture mode, any
+//    stream) is being captured into a CUDA graph.
 //  * Returns the reference's value (0-based iteration of convergence, or -1 when not
 //    converged), -2 for arguments it cannot serve (n outside [2, 64], precond not 0/1,
-//    null pointers), -3 when the solver aborted, -4 when the work area's address could
-//    not be obtained.
+//    null pointers or pointers that are not memory of the current device), -3 when the
+//    solver aborted, -4 when the work area's address could not be obtained, -5 when the
+//    CUDA context already holds an error or the copy or synchronisation of the result
+//    fails (the message is printed). A kernel that cannot be launched ends the process,
+//    as in every other entry point of this library.
 //  * The first call on each device looks up the work area's device address
-//    (cudaGetSymbolAddress) and sets kernel attributes; make that first call before any
-//    stream capture.
+//    (cudaGetSymbolAddress) and sets kernel attributes.
 //  * Every call shares the one work area, which keeps the last call's contents; the
 //    solver clears what must start at zero (the barrier words) itself. Calls that overlap
 //    on the GPU -- on different streams or threads -- race on it and must not be issued.
@@ -63,8 +68,22 @@ extern "C" int mzb_conj_grad_noalloc(const double* b, const double* x0, double* 
         fprintf(stderr, "mzb_conj_grad_noalloc: null buffer\n");
         return -2;
     }
+    const cudaError_t sticky = cudaPeekAtLastError();
+    if (sticky != cudaSuccess) {
+        fprintf(stderr, "mzb_conj_grad_noalloc: CUDA error before the call: %s\n", cudaGetErrorString(sticky));
+        return -5;
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return -4;
+    for (const void* ptr : {static_cast<const void*>(b), static_cast<const void*>(x0), static_cast<const void*>(x)}) {
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess || at.device != dev ||
+            (at.type != cudaMemoryTypeDevice && at.type != cudaMemoryTypeManaged)) {
+            cudaGetLastError();  // clear the lookup's error, if any
+            fprintf(stderr, "mzb_conj_grad_noalloc: %p is not memory of device %d\n", ptr, dev);
+            return -2;
+        }
+    }
     if (g_noalloc_addr[dev] == nullptr) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_work);
@@ -98,8 +117,12 @@ extern "C" int mzb_conj_grad_noalloc(const double* b, const double* x0, double* 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (!cg_fast_launch(a, s)) engine_launch(a, s);
     int res[2] = {0, 0};
-    MZB_CHECK(cudaMemcpyAsync(res, a.result, sizeof(res), cudaMemcpyDeviceToHost, s));
-    MZB_CHECK(cudaStreamSynchronize(s));
+    cudaError_t e = cudaMemcpyAsync(res, a.result, sizeof(res), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "mzb_conj_grad_noalloc: %s\n", cudaGetErrorString(e));
+        return -5;
+    }
     if (res[1] != 0) return -3;
     return res[0];
 }

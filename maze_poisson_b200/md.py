@@ -35,7 +35,8 @@ class MDRun:
         self.cas = cas.upper()  # charge assignment: CIC, SPL_QUADR, SPL_CUBIC
         self.pot = pot.upper()  # pair potential: TF, LJ, SC (system.pot_params to match)
         # field-solve precision (this build's extension): 0 FP64 reference algorithms,
-        # 1 FP32 multigrid + FP64 refinement to mixed_tol (or tol when 0)
+        # 1 FP32 multigrid + FP64 refinement to mixed_tol (or tol when 0), 2 the same
+        # multigrid and refinement with every value in FP64
         self.precision = precision
         self.mixed_tol = mixed_tol
         # Poisson-Boltzmann implicit solvent (systems.PBSettings) or None
@@ -74,6 +75,36 @@ class MDRun:
         c.integrator_part_2()
         if self.rescale:
             c.solver_rescale_velocities()
+
+    # -- solver.py:371-409 with a restart field -------------------------------------------
+    def restart(self, pos, vel, field, field_prev):
+        """Start from a saved state the way the reference's restart path does: the particles
+        from the restart positions and velocities, solver_set_field / solver_set_field_prev
+        in place of the two bootstrap steps; then the forces of that state are computed,
+        so that the first step integrates with them."""
+        c = self.capi
+        s = self.sys
+        s.pos = np.ascontiguousarray(pos, dtype=np.float64)
+        s.vel = np.ascontiguousarray(vel, dtype=np.float64)
+        c.solver_initialize()
+        maps = c.type_maps()
+        c.solver_initialize_grid(s.n_grid, s.L, s.h, self.tol, self.eps_s, self.eps_int,
+                                 maps["method"][self.method], maps["precond"][self.precond])
+        if self.pb is not None:
+            c.solver_initialize_grid_pois_boltz(self.pb.w, self.pb.kbar2, int(self.pb.nonpolar))
+        if self.precision:
+            c.mzb_set_precision(int(self.precision), float(self.mixed_tol))
+        c.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, maps["potential"][self.pot],
+                                      maps["cas"][self.cas], s.types, s.pos, s.vel, s.mass, s.charges,
+                                      s.pot_params)
+        if self.pb is not None:
+            c.solver_initialize_particles_pois_boltz(self.pb.gamma_np, self.pb.beta_np, self.pb.radii)
+        c.solver_initialize_integrator(s.n_ions, self.dt, self.T, self.gamma,
+                                       maps["integrator"][self.integrator], 1 if self.thermostat else 0)
+        self.update_charges()
+        c.solver_set_field(np.ascontiguousarray(field, dtype=np.float64))
+        c.solver_set_field_prev(np.ascontiguousarray(field_prev, dtype=np.float64))
+        self.compute_forces()
 
     def update_charges(self):
         if self.capi.solver_update_charges() != 0:

@@ -253,4 +253,5 @@ def write_reference_inputs(system, directory, name="input.csv"):
     with open(os.path.join(directory, name), "w") as f:
         f.write("type,x,y,z,vx,vy,vz\n")
         for t, p, v in zip(system.types, system.pos * A0, system.vel):
-            f.write(f"{names[t]},{p[0]!r},{p[1]!r},{p[2]!r},{v[0]!r},{v[1]!r},{v[2]!r}\n")
+            vals = ",".join(repr(float(x)) for x in (*p, *v))  # shortest round-trip decimal
+            f.write(f"{names[t]},{vals}\n")
