@@ -16,7 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmaze_poisson_ref.so")
 REF_FAST_SO = os.path.join(HERE, "_ref", "libmaze_poisson_ref_fast.so")
-REF_TREE = "/root/reference"
+# Source tree of the reference project (Crivella/MaZe_Poisson): MAZE_REFERENCE_ROOT, else
+# the read-only checkout this build was made against.
+REF_TREE = os.environ.get("MAZE_REFERENCE_ROOT", "/root/reference")
 
 
 def build(ref=True):

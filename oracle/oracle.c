@@ -10,8 +10,15 @@
  *  - every sum is accumulated in the reference's order, products are rounded before they
  *    are added (built with -ffp-contract=off, see Makefile);
  *  - reductions are serial, i.e. the reference run with OMP_NUM_THREADS=1.
+ *
+ * Pointwise passes (the stencils, BLAS-1 updates, one colour of a red-black sweep on an
+ * even grid, the grid transfers, the pair forces of each ion) run on several host threads
+ * (ORACLE_THREADS, default all cores).  Each output value is still computed by one thread
+ * in the serial order, and every sum across points (dot products, the pair energy) stays
+ * serial in index order, so the results do not depend on the thread count.
  */
 #include <math.h>
+#include <omp.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -22,6 +29,20 @@
 #define KB_HARTREE 3.1668e-6 /* library/include/constants.h:10 */
 
 static inline long wrap(long a, long n) { a %= n; return a < 0 ? a + n : a; }
+
+/* Host threads for the pointwise passes: ORACLE_THREADS, else every core. */
+static int orc_threads(void) {
+    static int nt = 0;
+    if (nt == 0) {
+        const char *e = getenv("ORACLE_THREADS");
+        int v = e ? atoi(e) : 0;
+        nt = v > 0 ? v : omp_get_num_procs();
+        if (nt < 1) nt = 1;
+    }
+    return nt;
+}
+/* Parallel only where the pass is large enough to pay for the threads. */
+#define PAR_MIN 32768L
 static inline long gidx(long i, long j, long k, long n) {
     return (wrap(i, n) * n + wrap(j, n)) * n + wrap(k, n);
 }
@@ -34,17 +55,26 @@ static double dot(const double *a, const double *b, long m) {
     for (long t = 0; t < m; t++) s += a[t] * b[t];
     return s;
 }
+/* max |a|: exact, so the order of the comparisons does not matter */
 static double amax(const double *a, long m) {
     double s = 0.0;
+#pragma omp parallel for reduction(max : s) num_threads(orc_threads()) if (m >= PAR_MIN)
     for (long t = 0; t < m; t++) { double v = fabs(a[t]); if (v > s) s = v; }
     return s;
 }
 /* u += alpha * v  (linalg.c:153-159) */
 static void axpy(double *u, const double *v, double alpha, long m) {
+#pragma omp parallel for num_threads(orc_threads()) if (m >= PAR_MIN)
     for (long t = 0; t < m; t++) u[t] += alpha * v[t];
 }
 static void scal(double *x, double alpha, long m) {
+#pragma omp parallel for num_threads(orc_threads()) if (m >= PAR_MIN)
     for (long t = 0; t < m; t++) x[t] *= alpha;
+}
+/* out = in * a, pointwise */
+static void scaled_copy(double *out, const double *in, double a, long m) {
+#pragma omp parallel for num_threads(orc_threads()) if (m >= PAR_MIN)
+    for (long t = 0; t < m; t++) out[t] = in[t] * a;
 }
 
 /* ------------------------------------------------------------------------------------
@@ -52,16 +82,25 @@ static void scal(double *x, double alpha, long m) {
  * Sum order: x+1, x-1, y+1, y-1, z+1, z-1, then minus 6*centre.
  * ---------------------------------------------------------------------------------- */
 void orc_laplace(const double *u, double *out, int n) {
-    for (long i = 0; i < n; i++)
-        for (long j = 0; j < n; j++)
+    long nn = (long)n * n;
+#pragma omp parallel for num_threads(orc_threads()) if (nn * n >= PAR_MIN)
+    for (long i = 0; i < n; i++) {
+        const double *up = u + wrap(i + 1, n) * nn, *um = u + wrap(i - 1, n) * nn;
+        const double *uc = u + i * nn;
+        for (long j = 0; j < n; j++) {
+            const double *rp = uc + wrap(j + 1, n) * n, *rm = uc + wrap(j - 1, n) * n;
+            const double *r0 = uc + j * n;
             for (long k = 0; k < n; k++) {
-                double s = u[gidx(i + 1, j, k, n)] + u[gidx(i - 1, j, k, n)];
-                s = s + u[gidx(i, j + 1, k, n)];
-                s = s + u[gidx(i, j - 1, k, n)];
-                s = s + u[gidx(i, j, k + 1, n)];
-                s = s + u[gidx(i, j, k - 1, n)];
-                out[(i * n + j) * n + k] = s - u[(i * n + j) * n + k] * 6.0;
+                long kp = k + 1 < n ? k + 1 : 0, km = k > 0 ? k - 1 : n - 1;
+                double s = up[j * n + k] + um[j * n + k];
+                s = s + rp[k];
+                s = s + rm[k];
+                s = s + r0[kp];
+                s = s + r0[km];
+                out[i * nn + j * n + k] = s - r0[k] * 6.0;
             }
+        }
+    }
 }
 
 /* ------------------------------------------------------------------------------------
@@ -77,7 +116,7 @@ int orc_conj_grad(const double *b, const double *x0, double *x, double tol, int 
     orc_laplace(x0, r, n);
     axpy(r, b, -1.0, m);                       /* r = A x0 - b */
     if (x != x0) memcpy(x, x0, m * sizeof(double));
-    for (long t = 0; t < m; t++) p[t] = r[t] * (1.0 / 6.0);
+    scaled_copy(p, r, 1.0 / 6.0, m);
     double rv = -dot(r, p, m);
     while (iter < limit) {
         orc_laplace(p, Ap, n);
@@ -103,8 +142,13 @@ int orc_conj_grad(const double *b, const double *x0, double *x, double tol, int 
 /* Red-black Gauss-Seidel, red = (i+j+k) even first (multigrid.c:636-729). */
 void orc_smooth_rbgs(const double *rhs, double *x, int n, int iters) {
     const double inv_diag = -1.0 / 6.0;
+    /* on an even grid a point's six neighbours all have the other colour, so the points
+       of one colour are independent; on an odd grid the wrap joins equal colours and the
+       sweep stays serial */
+    int par = (n % 2 == 0) && (long)n * n * n >= PAR_MIN;
     for (int it = 0; it < iters; it++)
         for (int colour = 0; colour < 2; colour++)
+#pragma omp parallel for num_threads(orc_threads()) if (par)
             for (long i = 0; i < n; i++)
                 for (long j = 0; j < n; j++)
                     for (long k = (i + j + colour) & 1; k < n; k += 2) {
@@ -123,6 +167,7 @@ void orc_smooth_rbgs(const double *rhs, double *x, int n, int iters) {
 void orc_restrict27(const double *in, double *out, int n) {
     int nc = n / 2;
 #define F(a, b, c) in[gidx(i + (a), j + (b), k + (c), n)]
+#pragma omp parallel for num_threads(orc_threads()) if ((long)nc * nc * nc >= PAR_MIN / 8)
     for (long I = 0; I < nc; I++)
         for (long J = 0; J < nc; J++)
             for (long K = 0; K < nc; K++) {
@@ -153,6 +198,7 @@ void orc_restrict27(const double *in, double *out, int n) {
    reference's order. */
 void orc_prolong_trilinear(const double *in, double *out, int nc) {
     long nf = 2L * nc;
+#pragma omp parallel for num_threads(orc_threads()) if (nf * nf * nf >= PAR_MIN)
     for (long i = 0; i < nf; i++) {
         double wi0 = (i & 1) ? 0.5 : 1.0, wi1 = (i & 1) ? 0.5 : 0.0;
         long i0 = i / 2, i1 = i0 + 1;
@@ -185,7 +231,7 @@ int orc_cg_coarse(const double *b, double *x, int n, int maxit, double rtol) {
     int k;
     orc_laplace(x, r, n);
     axpy(r, b, -1.0, m);
-    for (long t = 0; t < m; t++) p[t] = r[t] * (1.0 / 6.0);
+    scaled_copy(p, r, 1.0 / 6.0, m);
     double r0 = amax(r, m);
     if (r0 == 0.0) { free(r); free(p); free(Ap); return 0; }
     double rv = -dot(r, p, m);
@@ -238,7 +284,10 @@ void orc_mg_apply(const double *rhs, double *x, int n, int sm) {
  * ---------------------------------------------------------------------------------- */
 static void apply_precond(int kind, const double *in, double *out, int n) {
     long m = (long)n * n * n;
-    if (kind == 1) { for (long t = 0; t < m; t++) out[t] = -in[t] / 6.0; }
+    if (kind == 1) {
+#pragma omp parallel for num_threads(orc_threads()) if (m >= PAR_MIN)
+        for (long t = 0; t < m; t++) out[t] = -in[t] / 6.0;
+    }
     else if (kind == 3) orc_ssor_apply(in, out, n);
     else if (kind == 4) orc_blockjacobi_apply(in, out, n);
     else orc_mg_apply(in, out, n, 5);
@@ -254,7 +303,7 @@ static int conj_grad_precond(const double *b, const double *x0, double *x, doubl
     axpy(r, b, -1.0, m);
     if (x != x0) memcpy(x, x0, m * sizeof(double));
     apply_precond(kind, r, v, n);
-    for (long t = 0; t < m; t++) p[t] = v[t] * -1.0;
+    scaled_copy(p, v, -1.0, m);
     double rv = dot(r, v, m);
     while (iter < limit) {
         orc_laplace(p, Ap, n);
@@ -491,7 +540,7 @@ int orc_conj_grad_pb(const double *b, const double *x0, double *x, double tol, i
     orc_laplace_pb(x0, r, ex, ey, ez, k2, n);
     axpy(r, b, -1.0, m);
     if (x != x0) memcpy(x, x0, m * sizeof(double));
-    for (long t = 0; t < m; t++) p[t] = r[t] * (1.0 / 6.0);
+    scaled_copy(p, r, 1.0 / 6.0, m);
     double rv = -dot(r, p, m);
     while (iter < limit) {
         orc_laplace_pb(p, Ap, ex, ey, ez, k2, n);
@@ -907,34 +956,52 @@ void orc_tf_table(const double *pp, int ntyp, double L, double *tab) {
 }
 
 /* All-pairs shifted-force Tosi-Fumi, minimum image, skip r > r_cut, both orders summed
-   over j ascending (forces.c:112-186). Returns half the summed pair energy. */
+   over j ascending (forces.c:112-186). Returns half the summed pair energy.
+   Each ion's force is its own serial sum over j, so ions run on several threads; the
+   pair energies of a block of rows are kept in row order and added to the running total
+   serially, ion by ion and j ascending, which is the reference's single-thread order. */
 double orc_tf_forces(const double *pos, const int32_t *types, const double *tab, int ntyp, int np,
                      double L, double rcut, double *f) {
+    const long rows = 64;
     double en = 0.0;
-    for (long i = 0; i < np; i++) {
-        double fx = 0.0, fy = 0.0, fz = 0.0;
-        for (long j = 0; j < np; j++) {
-            if (i == j) continue;
-            double d[3], r = 0.0;
-            for (int a = 0; a < 3; a++) {
-                double x = pos[3 * i + a] - pos[3 * j + a];
-                x -= L * round(x / L);
-                d[a] = x;
-                r = (a == 0) ? x * x : r + x * x;
+    double *ebuf = malloc((size_t)rows * (np > 0 ? np : 1) * sizeof(double));
+    long *ecnt = malloc(rows * sizeof(long));
+    for (long i0 = 0; i0 < np; i0 += rows) {
+        long i1 = i0 + rows < np ? i0 + rows : np;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(orc_threads()) if ((long)np >= 512)
+        for (long i = i0; i < i1; i++) {
+            double fx = 0.0, fy = 0.0, fz = 0.0;
+            double *erow = ebuf + (i - i0) * np;
+            long ne = 0;
+            for (long j = 0; j < np; j++) {
+                if (i == j) continue;
+                double d[3], r = 0.0;
+                for (int a = 0; a < 3; a++) {
+                    double x = pos[3 * i + a] - pos[3 * j + a];
+                    x -= L * round(x / L);
+                    d[a] = x;
+                    r = (a == 0) ? x * x : r + x * x;
+                }
+                r = sqrt(r);
+                if (r > rcut) continue;
+                const double *t = tab + 7 * (types[i] * ntyp + types[j]);
+                double a = t[0], b = t[1], c = t[2], dd = t[3], s = t[4], al = t[5], be = t[6];
+                double fm = b * a * exp(b * (s - r)) - 6 * c / pow(r, 7) - 8 * dd / pow(r, 9) - al;
+                double vm = a * exp(b * (s - r)) - c / pow(r, 6) - dd / pow(r, 8) + al * r + be;
+                fx += fm * (d[0] / r);
+                fy += fm * (d[1] / r);
+                fz += fm * (d[2] / r);
+                erow[ne++] = vm;
             }
-            r = sqrt(r);
-            if (r > rcut) continue;
-            const double *t = tab + 7 * (types[i] * ntyp + types[j]);
-            double a = t[0], b = t[1], c = t[2], dd = t[3], s = t[4], al = t[5], be = t[6];
-            double fm = b * a * exp(b * (s - r)) - 6 * c / pow(r, 7) - 8 * dd / pow(r, 9) - al;
-            double vm = a * exp(b * (s - r)) - c / pow(r, 6) - dd / pow(r, 8) + al * r + be;
-            fx += fm * (d[0] / r);
-            fy += fm * (d[1] / r);
-            fz += fm * (d[2] / r);
-            en += vm;
+            ecnt[i - i0] = ne;
+            f[3 * i] = fx; f[3 * i + 1] = fy; f[3 * i + 2] = fz;
         }
-        f[3 * i] = fx; f[3 * i + 1] = fy; f[3 * i + 2] = fz;
+        for (long i = i0; i < i1; i++) {
+            const double *erow = ebuf + (i - i0) * np;
+            for (long e = 0; e < ecnt[i - i0]; e++) en += erow[e];
+        }
     }
+    free(ebuf); free(ecnt);
     return en / 2;
 }
 
@@ -1178,13 +1245,14 @@ void solver_init_field(void) {
     double c = rhs_const();
     memset(G.y, 0, G.m * sizeof(double));
     memcpy(G.phi_prev, G.phi, G.m * sizeof(double));
-    for (long t = 0; t < G.m; t++) G.phi[t] = G.q[t] * c;
+    scaled_copy(G.phi, G.q, c, G.m);
     if (G.pb) orc_conj_grad_pb(G.phi, G.y, G.phi, G.tol, G.n, G.ex, G.ey, G.ez, G.k2);
     else orc_conj_grad(G.phi, G.y, G.phi, G.tol, G.n);
 }
 
 /* phi <- 2 phi - phi_prev, phi_prev <- old phi (verlet.c:46-51, grid_multigrid.c:124-129) */
 static void extrapolate(void) {
+#pragma omp parallel for num_threads(orc_threads()) if (G.m >= PAR_MIN)
     for (long t = 0; t < G.m; t++) {
         double a = G.phi[t];
         G.phi[t] = 2 * a - G.phi_prev[t];
@@ -1198,7 +1266,7 @@ int solver_update_field(void) {
     if (G.type == G_LCG) {                                 /* grid_lcg.c:126-149 */
         double c = rhs_const();
         memcpy(G.phi_prev, G.phi, m * sizeof(double));
-        for (long t = 0; t < m; t++) G.y[t] = G.q[t] * c;
+        scaled_copy(G.y, G.q, c, m);
         if (G.pb) return orc_conj_grad_pb(G.y, G.phi_prev, G.phi, G.tol, n, G.ex, G.ey, G.ez, G.k2);
         return orc_conj_grad(G.y, G.phi_prev, G.phi, G.tol, n);
     }
@@ -1218,7 +1286,7 @@ int solver_update_field(void) {
         extrapolate();
         if (G.type == G_MG) {
             double c = rhs_const();
-            for (long t = 0; t < m; t++) tmp[t] = G.q[t] * c;
+            scaled_copy(tmp, G.q, c, m);
             while (it < 1000) {
                 orc_mg_pb_apply(tmp, G.phi, n, 4, G.ex, G.ey, G.ez, G.k2);
                 lap_pb(G.phi, tmp2);
@@ -1261,7 +1329,7 @@ int solver_update_field(void) {
     if (G.type == G_MG) {                                  /* grid_multigrid.c:110-212 */
         extrapolate();
         double c = rhs_const();
-        for (long t = 0; t < m; t++) tmp[t] = G.q[t] * c;
+        scaled_copy(tmp, G.q, c, m);
         while (it < 1000) {
             orc_mg_apply(tmp, G.phi, n, 3);
             orc_laplace(G.phi, tmp2, n);

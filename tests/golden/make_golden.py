@@ -29,7 +29,7 @@ from maze_poisson_b200.systems import make_pb_system, make_system, pair_system, 
 from oracle import loader  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
-REF_TREE = "/root/reference"
+REF_TREE = loader.REF_TREE  # MAZE_REFERENCE_ROOT, with the default in oracle/loader.py
 
 
 def sha(a):

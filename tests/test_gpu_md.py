@@ -16,6 +16,7 @@ import sys
 import numpy as np
 import pytest
 
+import mdparity
 from conftest import GOLDEN, ROOT
 from maze_poisson_b200.c_api import CAPI
 from maze_poisson_b200.md import MDRun
@@ -23,11 +24,7 @@ from maze_poisson_b200.systems import make_system, pair_system
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-10
-
-
-def rel(a, b):
-    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
-    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+rel = mdparity.rel
 
 
 @pytest.fixture(scope="module")
@@ -41,41 +38,7 @@ def orc(oracle_path):
 
 
 def run_pair(prod, orc, system, steps, check_each=True, noise=False, **kw):
-    """Run the same MD on product and oracle; compare after init and every step."""
-    a = MDRun(prod, system.copy(), **kw)
-    b = MDRun(orc, system.copy(), **kw)
-    a.initialize()
-    if noise:
-        from oracle.loader import load_kernels
-        ok = load_kernels()
-        calls = 2 + 2 * steps
-        z = np.empty((calls, system.n_ions, 3))
-        for c in range(calls):
-            prod.mzb_philox_normals(c, z[c])
-        ok.orc_set_noise(np.ascontiguousarray(z.reshape(-1)), z.size)
-    b.initialize()
-    try:
-        sa, sb = a.state(), b.state()
-        # q is bit-exact for identical positions (test_particle_kernels_bitexact); here the
-        # positions already went through one force evaluation, so compare to tolerance
-        assert rel(sa["q"], sb["q"]) < TOL
-        assert rel(sa["field"], sb["field"]) < TOL
-        for key in ("fcs_elec", "fcs_noel", "fcs_tot", "pos", "vel"):
-            assert rel(sa[key], sb[key]) < TOL, key
-        assert abs(sa["potential_notelec"] - sb["potential_notelec"]) <= TOL * abs(sb["potential_notelec"])
-        for s in range(steps):
-            a.step()
-            b.step()
-            if check_each or s == steps - 1:
-                sa, sb = a.state(), b.state()
-                assert abs(sa["n_iters"] - sb["n_iters"]) <= 1, (s, sa["n_iters"], sb["n_iters"])
-                for key in ("field", "fcs_tot", "pos", "vel"):
-                    assert rel(sa[key], sb[key]) < TOL, (s, key, rel(sa[key], sb[key]))
-                assert abs(sa["kinetic"] - sb["kinetic"]) <= TOL * sb["kinetic"]
-        return sa, sb
-    finally:
-        a.finalize()
-        b.finalize()
+    return mdparity.run_pair(prod, orc, system, steps, check_each=check_each, noise=noise, bound=TOL, **kw)[:2]
 
 
 SCEN = json.load(open(os.path.join(GOLDEN, "scenarios.json")))
@@ -265,6 +228,54 @@ print("not reached")
     assert r.returncode == 1
     assert "Charge conservation error" in r.stdout
     assert "not reached" not in r.stdout
+
+
+def test_charge_conservation_failure_exits_in_md_step():
+    """solver_md_step keeps the charge check on the device and reads it after the steps;
+    a non-neutral system still prints the reference's message and exits 1."""
+    code = f"""
+import sys; sys.path.insert(0, {ROOT!r})
+from maze_poisson_b200.c_api import CAPI
+from maze_poisson_b200.systems import make_system
+s = make_system(2, 16, seed=1)
+s.charges[0] = 3.0
+c = CAPI(); c.solver_initialize()
+c.solver_initialize_grid(16, s.L, s.h, 1e-7, 1.0, 1.0, 0, 0)
+c.solver_initialize_particles(16, 2, s.L, s.h, s.n_ions, 0, 0, s.types, s.pos, s.vel, s.mass, s.charges, s.pot_params)
+c.solver_initialize_integrator(s.n_ions, 40.0, 1200.0, 0.0, 1, 0)
+c.solver_md_step(3)
+print("not reached")
+"""
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300,
+                       env=dict(os.environ, MZB_QUIET="1"))
+    assert r.returncode == 1, (r.returncode, r.stdout, r.stderr[-2000:])
+    assert "Charge conservation error: q_tot = 0.000000, q_tot_loc = 2.000000" in r.stdout
+    assert "not reached" not in r.stdout
+
+
+def test_md_step_matches_per_call_sequence(prod):
+    """solver_md_step(n) (device-side checks, one synchronisation) gives the same state as
+    the reference's per-call sequence, FP64 and mixed forms."""
+    for precision in (0, 1):
+        out = []
+        for batched in (False, True):
+            run = MDRun(prod, make_system(5, 64, seed=3), method="LCG", tol=1e-9, precision=precision)
+            run.initialize()
+            try:
+                if batched:
+                    res = prod.solver_md_step(4)
+                else:
+                    for _ in range(4):
+                        res = run.step()
+                st = run.state()
+                st["res"] = res
+                out.append(st)
+            finally:
+                run.finalize()
+        a, b = out
+        assert a["res"] == b["res"]
+        for key in ("field", "field_prev", "q", "fcs_tot", "pos", "vel"):
+            assert np.array_equal(a[key], b[key]), (precision, key)
 
 
 @pytest.mark.parametrize("cas", ["SPL_QUADR", "SPL_CUBIC"])

@@ -1,5 +1,6 @@
-"""Mixed-precision field solve (FP32 multigrid V-cycles with FP64 iterative refinement):
-solves the same systems to the same FP64 residual tolerance as the reference's FP64
+"""Multigrid field solve with FP64 refinement, in its two forms: mixed precision (FP32
+V-cycles, precision 1) and FP64 multigrid (the same V-cycles in FP64, precision 2). Both
+solve the same systems to the same FP64 residual tolerance as the reference's FP64
 solvers, with a different inner algorithm. Checked against the CPU oracle's FP64 path
 solved to the same tolerance; the bound is the one the mixed form is specified to meet,
 force error below 1e-6 relative (max-norm ratio; much tighter in practice)."""
@@ -28,6 +29,9 @@ def orc(oracle_path):
 
 
 class MixedRun(MDRun):
+    def __init__(self, *args, precision=1, **kw):
+        super().__init__(*args, precision=precision, **kw)
+
     def initialize(self):
         c = self.capi
         c.solver_initialize()
@@ -35,8 +39,8 @@ class MixedRun(MDRun):
         s = self.sys
         c.solver_initialize_grid(s.n_grid, s.L, s.h, self.tol, self.eps_s, self.eps_int,
                                  maps["method"][self.method], maps["precond"][self.precond])
-        c.mzb_set_precision(1, 0.0)
-        assert c.mzb_get_precision() == 1
+        c.mzb_set_precision(self.precision, 0.0)
+        assert c.mzb_get_precision() == self.precision
         c.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, maps["potential"]["TF"],
                                       maps["cas"]["CIC"], s.types, s.pos, s.vel, s.mass, s.charges,
                                       s.pot_params)
@@ -52,18 +56,21 @@ class MixedRun(MDRun):
         c.integrator_part_2()
 
 
+@pytest.mark.parametrize("precision", [1, 2])
 @pytest.mark.parametrize("method", ["LCG", "MAZE-LCG", "MULTIGRID", "MAZE-MULTIGRID"])
-def test_mixed_matches_fp64_oracle(prod, orc, method):
+def test_mixed_matches_fp64_oracle(prod, orc, method, precision):
     system = make_system(5, 64, seed=21)
-    a = MixedRun(prod, system.copy(), method=method, tol=1e-10)
+    a = MixedRun(prod, system.copy(), method=method, tol=1e-10, precision=precision)
     b = MDRun(orc, system.copy(), method=method, tol=1e-10)
     a.initialize()
     b.initialize()
     try:
         for step in range(3):
             sa, sb = a.state(), b.state()
-            assert rel(sa["fcs_elec"], sb["fcs_elec"]) < 1e-6, (step, rel(sa["fcs_elec"], sb["fcs_elec"]))
-            assert rel(sa["fcs_tot"], sb["fcs_tot"]) < 1e-6
+            e_elec, e_tot = rel(sa["fcs_elec"], sb["fcs_elec"]), rel(sa["fcs_tot"], sb["fcs_tot"])
+            print(f"{method} precision {precision} step {step}: fcs_elec {e_elec:.3e} fcs_tot {e_tot:.3e}")
+            assert e_elec < 1e-7, (step, e_elec)
+            assert e_tot < 1e-7, (step, e_tot)
             assert rel(sa["pos"], sb["pos"]) < 1e-10
             a.step()
             b.step()
@@ -73,10 +80,11 @@ def test_mixed_matches_fp64_oracle(prod, orc, method):
         b.finalize()
 
 
-def test_mixed_solution_residual_meets_tol(prod, oracle_lib):
+@pytest.mark.parametrize("precision", [1, 2])
+def test_mixed_solution_residual_meets_tol(prod, oracle_lib, precision):
     """The returned field satisfies |L phi - b|_inf <= tol in FP64."""
     system = make_system(10, 128, density=1.329, seed=5)
-    run = MixedRun(prod, system, method="LCG", tol=1e-9)
+    run = MixedRun(prod, system, method="LCG", tol=1e-9, precision=precision)
     run.initialize()
     try:
         run.step()
