@@ -19,9 +19,12 @@ Forms, each from the same initial state (`modes` in the JSON line):
   fp64_multigrid_ref, fp64_maze_multigrid_ref : the reference's MULTIGRID and
                 MAZE-MULTIGRID algorithms (2-level V-cycle, coarse CG) in FP64;
   fp64_mg     : the fair FP64 comparator of fp32_refine -- the same V(2,2) multigrid and
-                refinement loop with every value in FP64.
+                refinement loop with every value in FP64;
+  fft         : the reference's FFT Poisson method (a spectral discretisation, so it is
+                timed beside the others but not counted among the FP64 comparators).
 `speedup_fp32_refine_over_fp64` sets fp32_refine against the CG form;
-`speedup_fp32_refine_over_best_fp64` against the fastest FP64 form.
+`speedup_fp32_refine_over_best_fp64` against the fastest FP64 form that solves the same
+7-point problem.
 After the same steps the forces, energies and positions of fp32_refine and fp64_mg are
 compared with fp64 (`errors_vs_fp64`). Then one MD step restarted from the FP64 state
 (solver_set_field / solver_set_field_prev) is run by the reference's C on the host (the
@@ -184,14 +187,28 @@ FORMS = {
     "fp64_multigrid_ref": ("MULTIGRID", 0),
     "fp64_maze_multigrid_ref": ("MAZE-MULTIGRID", 0),
     "fp64_mg": ("LCG", 2),
+    "fft": ("FFT", 0),
 }
+# forms that solve the same 7-point discretisation as fp32_refine (FFT solves the
+# spectral one, so it is timed beside them but not counted as an FP64 comparator)
+SAME_PROBLEM_FP64 = ("fp64", "fp64_multigrid_ref", "fp64_maze_multigrid_ref", "fp64_mg")
 FORM_DTYPE = {
     "fp32_refine": "f32 multigrid bulk + f64 residual/refinement/energies/positions",
     "fp64": "f64 (the reference's LCG algorithm)",
     "fp64_multigrid_ref": "f64 (the reference's MULTIGRID algorithm)",
     "fp64_maze_multigrid_ref": "f64 (the reference's MAZE-MULTIGRID algorithm)",
     "fp64_mg": "f64 (the V(2,2) multigrid + refinement loop of fp32_refine, every value in FP64)",
+    "fft": "f64 (the reference's FFT Poisson solve, continuous k^2; hand-written shared-memory FFT)",
 }
+
+
+def fft_solve_bytes(n):
+    """Algorithmic HBM bytes of one FFT solve (five passes): r2c along k reads q (8 B per
+    point) and writes the n x n x (n/2+1) complex spectrum (16 B per value); the three column
+    passes (forward j; forward i, multiply, inverse i; inverse j) read and write it; c2r
+    reads it and writes phi."""
+    spec = n * n * (n // 2 + 1) * 16
+    return 2 * 8 * n ** 3 + 8 * spec
 
 
 def make_run(capi, rank, precision=0, method=None):
@@ -345,8 +362,12 @@ def bench_b200(args, rank, world, dist):
         modes[name] = m
     modes["fp32_refine"]["errors_vs_fp64"] = errors
     modes["fp64_mg"]["errors_vs_fp64"] = errors_mg
-    fp64_names = [k for k in forms if k != "fp32_refine"]
-    best = min(fp64_names, key=lambda k: forms[k]["ms"])
+    best = min(SAME_PROBLEM_FP64, key=lambda k: forms[k]["ms"])
+    fft_s = statistics.mean(forms["fft"]["solve_ms"]) / 1e3
+    modes["fft"]["roofline"] = {"kernel": "FFT passes (k_pass_k_fwd, k_pass_cols x3, k_pass_k_inv)", "bound": "hbm",
+                                "alg_bytes_per_solve": fft_solve_bytes(n),
+                                "achieved": round(fft_solve_bytes(n) / fft_s / 1e9, 1), "peak": peak,
+                                "unit": "GB/s", "frac": round(fft_solve_bytes(n) / fft_s / 1e9 / peak, 4)}
     modes["speedup_fp32_refine_over_fp64"] = round(f64["ms"] / mix["ms"], 3)
     modes["speedup_fp32_refine_over_best_fp64"] = round(forms[best]["ms"] / mix["ms"], 3)
     modes["best_fp64_form"] = best
@@ -621,6 +642,157 @@ def bench_pb(args):
     print(json.dumps(line), flush=True)
 
 
+# Batched workload (--workload batch64): 64 resident +-1 melts, N log-uniform in
+# [128, 4000] (even), density from {1.329, 1.379} g/cm^3, grid from {32, 64, 96, 128}^3
+# closest to 0.3 A spacing, FP32+refine to 1e-10, OVRVO at 1200 K with 1 ps^-1 friction,
+# dt 1 fs, 300 steps, all replicas advanced by mzb_batch_step (a CUDA graph per MD step,
+# one cooperative launch for all field solves) after mzb_batch_autotune.
+BATCH = dict(count=64, seed=2026, steps=300)
+BATCH_SOLVER = dict(method="LCG", tol=1e-10, integrator="OVRVO", thermostat=True, T=1200.0, gamma_per_ps=1.0,
+                    dt_fs=1.0)
+
+
+def make_replica(capi, spec, precision=1, method=None):
+    from maze_poisson_b200.md import MDRun
+    from maze_poisson_b200.systems import make_melt
+    n, g, rho, seed = spec
+    kw = dict(BATCH_SOLVER)
+    if method is not None:
+        kw["method"] = method
+    return MDRun(capi, make_melt(n, g, density=rho, seed=seed), precision=precision, **kw)
+
+
+def bench_batch(args):
+    """One JSON line: replica-steps/s of the 64 replicas advanced together, beside the same
+    replicas stepped one at a time alone on the GPU (each 3 warm-up + 10 timed steps,
+    CUDA events, scaled to the batch's step count) and the reference's C on a sample of
+    them on the host cores."""
+    import numpy as np
+    import torch
+    from maze_poisson_b200.c_api import CAPI
+    from maze_poisson_b200.systems import replica_set
+    os.environ.setdefault("MZB_QUIET", "1")
+    torch.cuda.set_device(0)
+    capi = CAPI()
+    reps = replica_set(BATCH["count"], BATCH["seed"])
+    steps = args.batch_steps
+    # alone: one replica resident at a time
+    alone_ms = []
+    for spec in reps:
+        h = capi.mzb_system_create()
+        run = make_replica(capi, spec)
+        run.initialize()
+        for _ in range(3):
+            capi.solver_md_step(1)
+        stream = torch.cuda.ExternalStream(capi.mzb_get_stream(), device=0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        capi.solver_md_step(10)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        torch.cuda.synchronize()
+        alone_ms.append(e0.elapsed_time(e1) / 10)
+        run.finalize()
+        capi.mzb_system_destroy(h)
+    # together
+    handles, runs = [], []
+    for spec in reps:
+        handles.append(capi.mzb_system_create())
+        run = make_replica(capi, spec)
+        run.initialize()
+        runs.append(run)
+    hs = np.array(handles, dtype=np.int32)
+    tuned = np.zeros(4)
+    t0 = time.perf_counter()
+    capi.mzb_batch_autotune(hs, len(hs), tuned)
+    tune_s = time.perf_counter() - t0
+    capi.mzb_batch_step(hs, len(hs), args.warmup)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    l0 = capi.mzb_kernel_launches()
+    t0 = time.perf_counter()
+    rc = capi.mzb_batch_step(hs, len(hs), steps)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    launches = capi.mzb_kernel_launches() - l0
+    clk = clocks.stop()
+    for h in handles:
+        capi.mzb_system_select(h)
+        capi.solver_finalize()
+        capi.mzb_system_destroy(h)
+    value = len(reps) * steps / wall
+    alone_s = sum(alone_ms) / 1e3 * steps
+    points = [g ** 3 for _, g, _, _ in reps]
+    line = {
+        "metric": "replica MD steps/s, 64 replicas advanced together (FP32+refine, OVRVO)",
+        "value": round(value, 2), "unit": "replica-steps/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": round(wall / steps * 1e3, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 multigrid bulk + f64 residual/refinement/energies/positions",
+        "data": f"synthetic (seeded: replica_set(count={BATCH['count']}, seed={BATCH['seed']}), make_melt)",
+        "config": {"workload": "batch64", "replicas": len(reps), "ions_total": int(sum(n for n, _, _, _ in reps)),
+                   "grids": {str(g): sum(1 for _, x, _, _ in reps if x == g) for g in (32, 64, 96, 128)},
+                   "grid_points_total": int(sum(points)), **BATCH_SOLVER, "tol": 1e-10,
+                   "l2": "not flushed (a batched step moves several GB)"},
+        "batch_rc": rc, "autotune": {"alpha": tuned[0], "ctas": tuned[1], "solve_ms": tuned[2],
+                                      "forces_ms": tuned[3], "seconds": round(tune_s, 3)},
+        "alone_gpu": {"value": round(len(reps) * steps / alone_s, 2), "unit": "replica-steps/s",
+                      "sum_ms_per_step": round(sum(alone_ms), 4),
+                      "sample": "each replica alone on the whole GPU, 10 timed steps after 3 warm-up steps"},
+        "speedup_over_alone": round(alone_s / wall, 3),
+        "gpu_launches": int(launches), "clocks": clk,
+    }
+    if not args.no_cpu_baseline and reference_lib() is not None:
+        line["cpu_baseline"] = batch_cpu_sample(reps)
+    print(json.dumps(line), flush=True)
+
+
+BATCH_CPU = r"""
+import json, sys, time
+sys.path.insert(0, {root!r})
+from maze_poisson_b200.c_api import CAPI
+import bench
+capi = CAPI({lib!r}, extensions=False)
+out = []
+for spec in {sample!r}:
+    run = bench.make_replica(capi, tuple(spec), 0, "MAZE-MULTIGRID")
+    run.initialize()
+    run.step()
+    t0 = time.perf_counter()
+    run.step()
+    out.append(time.perf_counter() - t0)
+    run.finalize()
+print(json.dumps(out))
+"""
+
+
+def batch_cpu_sample(reps):
+    """The reference's C (MAZE-MULTIGRID, its fastest method; OpenMP on every host core)
+    on one replica of each grid size in the set (the median N of that size), one timed step
+    after the bootstrap and a warm-up step; the sum over all replicas is estimated as
+    each size's sample time times the number of replicas of that size."""
+    cores = os.cpu_count() or 1
+    by_grid = {}
+    for spec in reps:
+        by_grid.setdefault(spec[1], []).append(spec)
+    sample = []
+    for g, specs in sorted(by_grid.items()):
+        specs = sorted(specs)
+        sample.append(specs[len(specs) // 2])
+    code = BATCH_CPU.format(root=ROOT, lib=reference_lib(), sample=[list(x) for x in sample])
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, timeout=1800)
+    if r.returncode != 0:
+        return {"unavailable": (r.stderr.strip().splitlines() or ["cpu sample failed"])[-1][:200]}
+    times = json.loads(r.stdout.strip().splitlines()[-1])
+    est = sum(t * len(by_grid[spec[1]]) for t, spec in zip(times, sample))
+    return {"value": round(len(reps) / est, 4), "unit": "replica-steps/s", "cores": cores, "kind": "reference",
+            "sample": f"reference C (MAZE-MULTIGRID, OpenMP {cores} threads), one step per grid size "
+                      f"({', '.join(f'N={n} {g}^3: {t:.3f} s' for (n, g, _, _), t in zip(sample, times))}); "
+                      f"all replicas one after another estimated as size sample x count = {est:.2f} s per step"}
+
+
 def bench_reference(args):
     """The reference's C on the host cores through its facade, with its own bootstrap, on
     its two methods for this workload: MAZE-MULTIGRID (its fastest here; the line's value)
@@ -691,13 +863,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["nacl16000_256", "pb_solute32_128"], default="nacl16000_256",
-                    help="pb_solute32_128: the Poisson-Boltzmann workload (one GPU, its own JSON line)")
+    ap.add_argument("--workload", choices=["nacl16000_256", "pb_solute32_128", "batch64"], default="nacl16000_256",
+                    help="pb_solute32_128: the Poisson-Boltzmann workload; batch64: the batched form "
+                         "(one GPU each, their own JSON line)")
+    ap.add_argument("--batch-steps", type=int, default=BATCH["steps"], help="timed batched steps of batch64")
     ap.add_argument("--method", default="MAZE-LCG", help="field method of the PB workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.workload == "pb_solute32_128":
         bench_pb(args)
+        return
+    if args.workload == "batch64":
+        bench_batch(args)
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -455,6 +455,18 @@ int run_mixed(System& s, int prog, double cst) {
     return s.result_h[0];
 }
 
+// FFT Poisson solve of the current charge grid into phi (in place; FFT grids keep no
+// previous field), timed like the iterative solves.
+void run_fft(System& s) {
+    GridState& G = s.G;
+    MZB_CHECK(cudaEventRecord(s.ev0, s.stream));
+    G.fft.solve(G.q, G.phi(), s.stream);
+    MZB_CHECK(cudaEventRecord(s.ev1, s.stream));
+    MZB_CHECK(cudaStreamSynchronize(s.stream));
+    MZB_CHECK(cudaEventElapsedTime(&s.last_solve_ms, s.ev0, s.ev1));
+    s.last_solve_iters = 0;
+}
+
 void require_mg_size(int n) {
     // multigrid.c:114-121: at least one level of recursion, n/2 >= 16
     if (n / 2 < 16 || n % 2) fatal("Multigrid: requires an even grid with n/2 >= 16");
@@ -790,8 +802,7 @@ void solver_init_field(void) {
     System& s = sys();
     GridState& G = grid();
     if (G.type == G_FFT) {  // grid_fft.c:135-137
-        G.fft.solve(G.q, G.phi(), s.stream);
-        sync();
+        run_fft(s);
         return;
     }
     if (G.precision >= 1 && mixed_supported(G)) {
@@ -868,8 +879,7 @@ int solver_update_field(void) {
     System& s = sys();
     GridState& G = grid();
     if (G.type == G_FFT) {  // grid_fft.c:139-143
-        G.fft.solve(G.q, G.phi(), s.stream);
-        sync();
+        run_fft(s);
         return 0;
     }
     if (G.precision >= 1 && mixed_supported(G)) {
@@ -1581,7 +1591,7 @@ uint64_t mzb_get_ocalls(void) { return sys().I.ocalls; }
 // n_steps iterations of SolverMD.md_loop_iter (maze_poisson/solver.py:483-492) with both
 // electrostatic and non-electrostatic forces (and the PB coefficient update and forces on
 // a Poisson-Boltzmann grid); returns the last solver_update_field value. Poisson grids
-// solved by CG, multigrid or the mixed solver run the steps without a host round trip:
+// (every method and form) run the steps without a host round trip:
 // the charge check and the solve status stay on the device and are read after the last
 // step (md_steps_deferred); a charge error still prints the reference's message and exits.
 int solver_md_step(int n_steps) {
@@ -1589,8 +1599,7 @@ int solver_md_step(int n_steps) {
     {
         System& s = sys();
         GridState& G = grid();
-        if (G.type != G_FFT && !G.pb && !(G.type == G_MAZE_MG && G.precond != P_NONE) && s.parts_ready &&
-            s.integ_ready)
+        if (!G.pb && !(G.type == G_MAZE_MG && G.precond != P_NONE) && s.parts_ready && s.integ_ready)
             return md_steps_deferred(s, n_steps);
     }
     int res = 0;
@@ -1812,21 +1821,26 @@ int md_steps_deferred(System& s, int n_steps) {
         count_launch();
         k_md_charge_check<<<1, 1, 0, s.stream>>>(P.red, s.qtot_d, s.err_d, P.flags, bad);
         MZB_CHECK(cudaEventRecord(s.ev0, s.stream));
-        if (G.precision >= 1 && mixed_supported(G)) {
-            double cst = 0.0;
-            const int prog = mixed_update_prog(G, cst);
-            mixed_launch(mixed_args(s, prog, cst), s.stream);
+        if (G.type == G_FFT) {  // in place, no previous field, no status word
+            G.fft.solve(G.q, G.phi(), s.stream);
+            MZB_CHECK(cudaEventRecord(s.ev1, s.stream));
         } else {
-            const EngineArgs a = update_engine_args(s);
-            if (generic_only || !cg_fast_launch(a, s.stream)) engine_launch(a, s.stream);
+            if (G.precision >= 1 && mixed_supported(G)) {
+                double cst = 0.0;
+                const int prog = mixed_update_prog(G, cst);
+                mixed_launch(mixed_args(s, prog, cst), s.stream);
+            } else {
+                const EngineArgs a = update_engine_args(s);
+                if (generic_only || !cg_fast_launch(a, s.stream)) engine_launch(a, s.stream);
+            }
+            MZB_CHECK(cudaEventRecord(s.ev1, s.stream));
+            const int old = G.iphi;
+            G.iphi = G.ispare;
+            G.ispare = G.iprev;
+            G.iprev = old;
+            count_launch();
+            k_solve_check<<<1, 1, 0, s.stream>>>(s.result, s.err_d);
         }
-        MZB_CHECK(cudaEventRecord(s.ev1, s.stream));
-        const int old = G.iphi;
-        G.iphi = G.ispare;
-        G.ispare = G.iprev;
-        G.iprev = old;
-        count_launch();
-        k_solve_check<<<1, 1, 0, s.stream>>>(s.result, s.err_d);
         field_forces(P, G.phi(), G.n, G.h, s.stream);
         build_cells(P, s.stream);
         tf_forces(P, s.stream);
@@ -1835,7 +1849,12 @@ int md_steps_deferred(System& s, int n_steps) {
     }
     int err[4];
     double q = 0.0, qbad[2] = {0.0, 0.0};
-    MZB_CHECK(cudaMemcpyAsync(s.result_h, s.result, 2 * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    if (G.type == G_FFT) {
+        s.result_h[0] = 0;
+        s.result_h[1] = 0;
+    } else {
+        MZB_CHECK(cudaMemcpyAsync(s.result_h, s.result, 2 * sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    }
     MZB_CHECK(cudaStreamSynchronize(s.stream));
     MZB_CHECK(cudaMemcpy(err, s.err_d, sizeof(err), cudaMemcpyDeviceToHost));
     MZB_CHECK(cudaMemcpy(&q, s.qtot_d, sizeof(double), cudaMemcpyDeviceToHost));

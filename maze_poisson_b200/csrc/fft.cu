@@ -5,8 +5,9 @@
 //   I  : forward along i, multiply by ig2, inverse along i (one read, one write)
 //   J' : inverse along j
 //   K' : c2r along k
-// Each 1-D transform runs in shared memory as a mixed-radix (4, 2, 3) Stockham FFT with
-// an accurate twiddle table (sincospi). Reference semantics (library/src/grid_fft.c:65-125,
+// For n = 64, 128 and 256 each 1-D transform runs in registers (see solve_reg); other
+// sizes run each 1-D transform in shared memory as a mixed-radix (4, 2, 3) Stockham FFT.
+// Both use an accurate twiddle table (sincospi). Reference semantics (library/src/grid_fft.c:65-125,
 // fftw_wrap.c:166-189): ig2 = 4 pi / (h^3 n^3) / (k^2 + 1e-10) with continuous
 // k = 2 pi m / L, the unnormalised inverse transform, and the DC term left unmultiplied.
 #include "fft.cuh"
@@ -252,6 +253,278 @@ __global__ void __launch_bounds__(kFftThreads) k_pass_cols(double2* __restrict__
     }
 }
 
+// ---- register-resident transforms for n = 64, 128, 256 ----
+//
+// A length-N transform is split N = N1 x N2 (Cooley-Tukey, four-step): N2 threads work it,
+// thread t holding x[n1 N2 + t] for n1 < N1; each forms a length-N1 DFT in registers,
+// multiplies by W_N^(t k1), the partial results are exchanged through shared memory, and
+// each thread forms the length-N2 DFTs of its k1 = t + N2 a, ending with X[k1 + N1 k2].
+// That output set is again {m : m = t mod N2}, the input distribution, so an inverse can
+// start from registers. Small DFTs are radix-2 decimation-in-time with compile-time
+// indices; every twiddle comes from the accurate table W (exp(-2 pi i m / N), sincospi).
+// The passes move each value once each way with whole 128-byte segments per warp, and no
+// integer division is left in the butterflies.
+template <int N> struct Split;
+template <> struct Split<256> { static constexpr int N1 = 16, N2 = 16; };
+template <> struct Split<128> { static constexpr int N1 = 16, N2 = 8; };
+template <> struct Split<64> { static constexpr int N1 = 8, N2 = 8; };
+// exchange buffer of one sequence: N1 rows of N2 + 1 doubles, plus 4 so that consecutive
+// sequences' buffers start 8 banks apart
+template <int N> constexpr int XchLen = Split<N>::N1 * (Split<N>::N2 + 1) + 4;
+
+__host__ __device__ constexpr int ilog2(int v) { return v >= 16 ? 4 : v >= 8 ? 3 : v >= 4 ? 2 : v >= 2 ? 1 : 0; }
+// bit reversal of v in `bits` (<= 4) bits
+__host__ __device__ constexpr int bitrev(int v, int bits) {
+    const int r4 = ((v & 1) << 3) | ((v & 2) << 1) | ((v & 4) >> 1) | ((v & 8) >> 3);
+    return r4 >> (4 - bits);
+}
+
+// In-register DFT of length R on (xr, xi) (natural order in and out); w holds W_N^m and
+// W_R^j = w[j * (N / R)].
+// one radix-2 stage of span M = 2^S over the R registers (compile-time indices)
+template <int R, int N, bool INV, int M>
+__device__ __forceinline__ void dit_stage(double (&xr)[R], double (&xi)[R], const double2* w) {
+    constexpr int H = M / 2;
+#pragma unroll
+    for (int k = 0; k < R; k += M) {
+#pragma unroll
+        for (int j = 0; j < H; j++) {
+            const double br = xr[k + j + H], bi = xi[k + j + H];
+            double tr = br, ti = bi;
+            if (j != 0) {
+                const double2 tw = w[j * (N / M)];
+                const double c = tw.x, sn = INV ? -tw.y : tw.y;
+                tr = fma(br, c, -bi * sn);
+                ti = fma(br, sn, bi * c);
+            }
+            const double ur = xr[k + j], ui = xi[k + j];
+            xr[k + j] = ur + tr;
+            xi[k + j] = ui + ti;
+            xr[k + j + H] = ur - tr;
+            xi[k + j + H] = ui - ti;
+        }
+    }
+}
+
+template <int R, int N, bool INV>
+__device__ __forceinline__ void dft_reg(double (&xr)[R], double (&xi)[R], const double2* w) {
+    constexpr int B = ilog2(R);
+#pragma unroll
+    for (int q = 0; q < R; q++) {  // bit-reversal permutation, in place
+        const int p = bitrev(q, B);
+        if (q < p) {
+            const double tr = xr[q], ti = xi[q];
+            xr[q] = xr[p];
+            xi[q] = xi[p];
+            xr[p] = tr;
+            xi[p] = ti;
+        }
+    }
+    dit_stage<R, N, INV, 2>(xr, xi, w);
+    dit_stage<R, N, INV, 4>(xr, xi, w);
+    dit_stage<R, N, INV, 8>(xr, xi, w);
+    if constexpr (R >= 16) dit_stage<R, N, INV, 16>(xr, xi, w);
+}
+
+// The distributed length-N transform of one sequence by its N2 threads (t = this thread's
+// rank): in, xr[n1] = x[n1 N2 + t]; out, xr[a N2 + k2] = X[(t + N2 a) + N1 k2]. (xre, xim)
+// is the sequence's exchange buffer (XchLen<N> doubles each: N1 rows of N2 + 1, the pad
+// spreading a warp's accesses over the banks); `sync` makes the writes of all N2 threads
+// visible (a warp or block barrier, whichever spans them).
+template <int N, bool INV, class Sync>
+__device__ __forceinline__ void fft_dist(double (&xr)[Split<N>::N1], double (&xi)[Split<N>::N1], int t,
+                                         const double2* w, double* xre, double* xim, Sync sync) {
+    constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+    dft_reg<N1, N, INV>(xr, xi, w);
+#pragma unroll
+    for (int k1 = 0; k1 < N1; k1++) {
+        const double2 tw = w[(t * k1) & (N - 1)];
+        const double c = tw.x, sn = INV ? -tw.y : tw.y;
+        const double r = xr[k1], i = xi[k1];
+        xre[k1 * (N2 + 1) + t] = k1 == 0 ? r : fma(r, c, -i * sn);
+        xim[k1 * (N2 + 1) + t] = k1 == 0 ? i : fma(r, sn, i * c);
+    }
+    sync();
+#pragma unroll
+    for (int a = 0; a < N1 / N2; a++) {
+        double yr[N2], yi[N2];
+        const int k1 = t + N2 * a;
+#pragma unroll
+        for (int n2 = 0; n2 < N2; n2++) {
+            yr[n2] = xre[k1 * (N2 + 1) + n2];
+            yi[n2] = xim[k1 * (N2 + 1) + n2];
+        }
+        dft_reg<N2, N, INV>(yr, yi, w);
+#pragma unroll
+        for (int k2 = 0; k2 < N2; k2++) {
+            xr[a * N2 + k2] = yr[k2];
+            xi[a * N2 + k2] = yi[k2];
+        }
+    }
+    sync();  // the buffer is free again
+}
+
+// Index, in the sequence, of register q after fft_dist (thread t): (t + N2 a) + N1 k2 for
+// q = a N2 + k2. It is also the input index n1 N2 + t of register n1 = q' for the inverse:
+// X[m] with m = t + N2 n1' sits in register q where n1' = a + (N1 / N2) k2.
+template <int N>
+__device__ __forceinline__ int out_index(int t, int q) {
+    constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2;
+    return (t + N2 * (q / N2)) + N1 * (q % N2);
+}
+
+constexpr int kRegRows = 8;  // sequences per CTA in the row and column passes
+
+// pass K forward: real rows of N (q) -> spectrum rows of N/2+1; a CTA of kRegRows x N2
+// threads takes kRegRows consecutive rows, thread (r, t) = r N2 + t (a row's threads in one
+// warp, reading consecutive values)
+template <int N>
+__global__ void __launch_bounds__(kRegRows * Split<N>::N2) k_rows_fwd(const double* __restrict__ in,
+                                                                    double2* __restrict__ spec,
+                                                                    const double2* __restrict__ W, long rows) {
+    constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, NH = N / 2 + 1;
+    __shared__ double2 w[N];
+    __shared__ double xre[kRegRows][XchLen<N>], xim[kRegRows][XchLen<N>];
+    for (int m = threadIdx.x; m < N; m += blockDim.x) w[m] = W[m];
+    __syncthreads();
+    const int r = threadIdx.x / N2, t = threadIdx.x % N2;
+    const long row = (long)blockIdx.x * kRegRows + r;
+    const bool live = row < rows;
+    double xr[N1], xi[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; n1++) {
+        xr[n1] = live ? in[row * N + n1 * N2 + t] : 0.0;
+        xi[n1] = 0.0;
+    }
+    fft_dist<N, false>(xr, xi, t, w, xre[r], xim[r], [] { __syncwarp(); });
+    if (!live) return;
+#pragma unroll
+    for (int q = 0; q < N1; q++) {
+        const int m = out_index<N>(t, q);
+        if (m < NH) spec[row * NH + m] = make_double2(xr[q], xi[q]);
+    }
+}
+
+// pass K': spectrum rows (Hermitian, N/2+1 stored) -> real rows of N
+template <int N>
+__global__ void __launch_bounds__(kRegRows * Split<N>::N2) k_rows_inv(const double2* __restrict__ spec,
+                                                                    double* __restrict__ out,
+                                                                    const double2* __restrict__ W, long rows) {
+    constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, NH = N / 2 + 1;
+    __shared__ double2 w[N];
+    __shared__ double xre[kRegRows][XchLen<N>], xim[kRegRows][XchLen<N>];
+    for (int m = threadIdx.x; m < N; m += blockDim.x) w[m] = W[m];
+    __syncthreads();
+    const int r = threadIdx.x / N2, t = threadIdx.x % N2;
+    const long row = (long)blockIdx.x * kRegRows + r;
+    const bool live = row < rows;
+    double xr[N1], xi[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; n1++) {
+        const int m = n1 * N2 + t;
+        double2 v = make_double2(0.0, 0.0);
+        if (live) {
+            if (m < NH) v = spec[row * NH + m];
+            else {
+                v = spec[row * NH + (N - m)];
+                v.y = -v.y;
+            }
+        }
+        xr[n1] = v.x;
+        xi[n1] = v.y;
+    }
+    fft_dist<N, true>(xr, xi, t, w, xre[r], xim[r], [] { __syncwarp(); });
+    if (!live) return;
+#pragma unroll
+    for (int q = 0; q < N1; q++) out[row * N + out_index<N>(t, q)] = xr[q];
+}
+
+// passes J / I: columns of the spectrum (MODE 0 forward along j, 1 inverse along j, 2
+// forward along i, ig2 multiply, inverse along i). A CTA takes kRegRows consecutive kh of
+// one i (MODE 0/1) or one j (MODE 2); thread (t, f) = t kRegRows + f, so a warp reads whole
+// 128-byte runs of kh; a column's threads span warps and exchange through the block.
+template <int N, int MODE>
+__global__ void __launch_bounds__(kRegRows * Split<N>::N2) k_cols_reg(double2* __restrict__ spec,
+                                                                    const double2* __restrict__ W,
+                                                                    const double* __restrict__ freq,
+                                                                    const double* __restrict__ rfreq, double cst) {
+    constexpr int N1 = Split<N>::N1, N2 = Split<N>::N2, NH = N / 2 + 1;
+    constexpr int NT = (NH + kRegRows - 1) / kRegRows;
+    __shared__ double2 w[N];
+    __shared__ double xre[kRegRows][XchLen<N>], xim[kRegRows][XchLen<N>];
+    for (int m = threadIdx.x; m < N; m += blockDim.x) w[m] = W[m];
+    __syncthreads();
+    const int t = threadIdx.x / kRegRows, f = threadIdx.x % kRegRows;
+    const int fixed = blockIdx.x / NT, kh = (blockIdx.x % NT) * kRegRows + f;
+    const bool live = kh < NH;
+    const long nnh = (long)N * NH;
+    // element e of the column: (i = fixed, j = e) for MODE 0/1, (i = e, j = fixed) for MODE 2
+    auto addr = [&](int e) -> long { return MODE == 2 ? (long)e * nnh + (long)fixed * NH + kh
+                                                      : (long)fixed * nnh + (long)e * NH + kh; };
+    double xr[N1], xi[N1];
+#pragma unroll
+    for (int n1 = 0; n1 < N1; n1++) {
+        const double2 v = live ? spec[addr(n1 * N2 + t)] : make_double2(0.0, 0.0);
+        xr[n1] = v.x;
+        xi[n1] = v.y;
+    }
+    auto bar = [] { __syncthreads(); };
+    if (MODE == 1)
+        fft_dist<N, true>(xr, xi, t, w, xre[f], xim[f], bar);
+    else
+        fft_dist<N, false>(xr, xi, t, w, xre[f], xim[f], bar);
+    if (MODE == 2) {
+        // ig2(i, j, kh) = cst / ((freq_i^2 + freq_j^2) + rfreq_kh^2 + 1e-10), DC untouched
+        const double fj = freq[fixed], rk = live ? rfreq[kh] : 0.0;
+        double yr[N1], yi[N1];
+#pragma unroll
+        for (int q = 0; q < N1; q++) {
+            const int e = out_index<N>(t, q);
+            double g = 1.0;
+            if (!(e == 0 && fixed == 0 && kh == 0)) {
+                const double fi = freq[e];
+                const double f1 = fi * fi;
+                const double f2 = f1 + fj * fj;
+                g = cst / (f2 + rk * rk + 1E-10);
+            }
+            // register q holds X[e], e - t = N2 (q / N2) + N1 (q % N2): the inverse's input
+            // n1' = (e - t) / N2
+            const int n1p = q / N2 + (N1 / N2) * (q % N2);
+            yr[n1p] = xr[q] * g;
+            yi[n1p] = xi[q] * g;
+        }
+        fft_dist<N, true>(yr, yi, t, w, xre[f], xim[f], bar);
+#pragma unroll
+        for (int q = 0; q < N1; q++) {
+            xr[q] = yr[q];
+            xi[q] = yi[q];
+        }
+    }
+    if (!live) return;
+#pragma unroll
+    for (int q = 0; q < N1; q++) spec[addr(out_index<N>(t, q))] = make_double2(xr[q], xi[q]);
+}
+
+template <int N>
+void solve_reg(const double* q, double* phi, double2* spec, const double2* W, const double* freq, const double* rfreq,
+               double cst, cudaStream_t s) {
+    constexpr int T = kRegRows * Split<N>::N2, NH = N / 2 + 1;
+    constexpr int NT = (NH + kRegRows - 1) / kRegRows;
+    const long rows = (long)N * N;
+    const int rblocks = (int)((rows + kRegRows - 1) / kRegRows);
+    count_launch();
+    k_rows_fwd<N><<<rblocks, T, 0, s>>>(q, spec, W, rows);
+    count_launch();
+    k_cols_reg<N, 0><<<N * NT, T, 0, s>>>(spec, W, freq, rfreq, cst);
+    count_launch();
+    k_cols_reg<N, 2><<<N * NT, T, 0, s>>>(spec, W, freq, rfreq, cst);
+    count_launch();
+    k_cols_reg<N, 1><<<N * NT, T, 0, s>>>(spec, W, freq, rfreq, cst);
+    count_launch();
+    k_rows_inv<N><<<rblocks, T, 0, s>>>(spec, phi, W, rows);
+    MZB_CHECK(cudaGetLastError());
+}
+
 }  // namespace
 
 void FftPoisson::init(int n_, double L_, double h_) {
@@ -292,6 +565,11 @@ void FftPoisson::release() {
 }
 
 void FftPoisson::solve(const double* q, double* phi, cudaStream_t s) const {
+    // constant = 4 pi / (h h h) / (n n n)   (grid_fft.c:105)
+    const double cst0 = 4 * kPi / (h * h * h) / (double)(n * n * n);
+    if (n == 256) return solve_reg<256>(q, phi, spec, W, freq, rfreq, cst0, s);
+    if (n == 128) return solve_reg<128>(q, phi, spec, W, freq, rfreq, cst0, s);
+    if (n == 64) return solve_reg<64>(q, phi, spec, W, freq, rfreq, cst0, s);
     const Radices rd = plan_radices(n);
     const long rows = (long)n * n;
     const int rblocks = (int)((rows + kRowsPerBlock - 1) / kRowsPerBlock);

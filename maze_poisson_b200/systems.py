@@ -114,6 +114,55 @@ def make_system(ncell, n_grid, density=1.379, T=1200.0, seed=0, jitter=0.1):
                       pot_params=tf_params_au())
 
 
+def make_melt(n_ions, n_grid, density=1.379, T=1200.0, seed=0, jitter=0.1):
+    """A +-1 ionic melt of any even n_ions: the 2-ion cells of the smallest cubic lattice
+    that holds n_ions/2 of them, n_ions/2 cells drawn at random (seeded), each with its Na+
+    at the corner and Cl- at the body centre, jittered as make_system; the box holds the
+    n_ions at `density`."""
+    if n_ions < 2 or n_ions % 2:
+        raise ValueError("n_ions must be even and positive")
+    rng = np.random.default_rng(seed)
+    pairs = n_ions // 2
+    ncell = int(np.ceil(pairs ** (1.0 / 3.0) - 1e-9))
+    L = box_length_ang(n_ions, density) / A0
+    a = L / ncell
+    cells = np.stack(np.meshgrid(np.arange(ncell), np.arange(ncell), np.arange(ncell),
+                                 indexing="ij"), axis=-1).reshape(-1, 3).astype(np.float64)
+    cells = cells[np.sort(rng.choice(len(cells), size=pairs, replace=False))]
+    pos = np.empty((n_ions, 3))
+    pos[0::2] = cells * a
+    pos[1::2] = (cells + 0.5) * a
+    pos += rng.uniform(-jitter * a, jitter * a, size=pos.shape)
+    pos = np.mod(pos, L)
+    pos = np.where(pos >= L, pos - L, pos)
+    types = np.tile(np.array([0, 1], dtype=np.int32), pairs)
+    charges = np.array([SPECIES[t][1] for t in types], dtype=np.float64)
+    mass = np.array([SPECIES[t][2] for t in types], dtype=np.float64) * CONV_MASS
+    vel = rng.normal(0.0, 1.0, size=(n_ions, 3)) * np.sqrt(KB * T / mass)[:, None]
+    vel -= (mass[:, None] * vel).sum(axis=0) / mass.sum()
+    return MoltenSalt(ncell=ncell, n_grid=n_grid, density=density, T=T, seed=seed, L=L,
+                      h=L / n_grid, types=np.ascontiguousarray(types),
+                      pos=np.ascontiguousarray(pos), vel=np.ascontiguousarray(vel),
+                      mass=np.ascontiguousarray(mass), charges=np.ascontiguousarray(charges),
+                      pot_params=tf_params_au())
+
+
+def replica_set(count=64, seed=2026, n_min=128, n_max=4000, densities=(1.329, 1.379), grids=(32, 64, 96, 128),
+                spacing_ang=0.3):
+    """The replicas of the batched configuration: N log-uniform in [n_min, n_max] rounded to
+    an even count, density drawn from `densities`, grid from `grids` closest to a spacing
+    of `spacing_ang`; returns (n_ions, n_grid, density, seed) per replica."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max))) / 2)) * 2
+        rho = float(rng.choice(densities))
+        target = box_length_ang(n, rho) / spacing_ang
+        g = min(grids, key=lambda x: abs(x - target))
+        out.append((n, g, rho, int(rng.integers(1 << 30))))
+    return out
+
+
 # Lennard-Jones Na+/Cl- pairs: (type1, type2, sigma [A], epsilon [kJ/mol])
 LENNARD_JONES = (("Na", "Na", 2.350, 0.544), ("Na", "Cl", 3.370, 0.477), ("Cl", "Cl", 4.400, 0.418))
 

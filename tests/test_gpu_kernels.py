@@ -133,7 +133,7 @@ def test_cg_coarse_and_vcycle(lib, oracle_lib, K):
     assert rel(xc, xco) < 1e-10
 
 
-@pytest.mark.parametrize("n", [32, 48, 64, 96])
+@pytest.mark.parametrize("n", [32, 48, 64, 96, 128, 192, 256])
 def test_fft_poisson_vs_numpy(lib, n):
     from oracle.fft_oracle import fft_poisson
     rng = np.random.default_rng(n)
