@@ -101,25 +101,40 @@ def level_sizes(n):
     return sizes
 
 
+def fft_coarse_level(n):
+    """The coarse level the mixed solver solves by FFT (n/2 when that is 32, 64 or 128 points
+    per side), or None when its hierarchy ends at a level of at most 16 points per side."""
+    m = n // 2
+    return m if n % 2 == 0 and m in (32, 64, 128) else None
+
+
 def mixed_solve_bytes(n, refinements, nu1=2, nu2=2, small_n=16):
     """Algorithmic HBM bytes of one mixed solve (MD update, LCG form) that took
     `refinements` V-cycles, with 8 B per FP64 and 4 B per FP32 value, per grid point:
       set-up          read q, phi_old; write y, rhs, phi                     40 B
-      residual check  read X, rhs; write FP32 rhs, e            24 B, refinements + 1 times
+      residual check  read X, rhs; write FP32 rhs, red e        22 B, refinements + 1 times
       update          read X, e; write X                                     20 B
-      V-cycle, per point of each level worked by the whole grid (n > small_n), with the
-      red-black split layout (a half-sweep reads the other colour, this colour's rhs and
-      writes this colour: 3 x 4 B x 1/2):
+      V-cycle, per point of each level swept by the whole grid, with the red-black split
+      layout (a half-sweep reads the other colour, this colour's rhs and writes this
+      colour: 3 x 4 B x 1/2):
         2 nu1 - 1 + 2 nu2 half-sweeps                                   6 B each
         red residual: read both colours of x, red rhs; write red r       8 B
         restriction (13 red taps): read red r; write coarse rhs, x       2 + 1 B
         prolongation into black points: read coarse x; read/write black  0.5 + 4 B
-    Levels of at most small_n^3 points live in shared memory and move no HBM bytes."""
+      coarse level of m points per side solved by FFT (fft_coarse_level): read its rhs,
+        write x (4 B each), the half spectrum m^2 (m/2 + 1) complex (8 B) written by the
+        first pass, read and written by the second, read by the third:  8 m^3 + 32 m^2 (m/2 + 1)
+    Otherwise levels of at most small_n^3 points are solved in shared memory or from a
+    staged Green's function and move no HBM bytes."""
     P = n ** 3
     per_level = (2 * nu1 - 1 + 2 * nu2) * 6 + 8 + 3 + 4.5
-    grid_levels = [m for m in level_sizes(n) if m > small_n]
-    vcycle = sum(m ** 3 * per_level for m in grid_levels)
-    return P * 40 + (refinements + 1) * P * 24 + refinements * (vcycle + P * 20)
+    m = fft_coarse_level(n)
+    if m is not None:
+        vcycle = P * per_level + 8 * m ** 3 + 32 * m * m * (m // 2 + 1)
+    else:
+        grid_levels = [k for k in level_sizes(n) if k > small_n]
+        vcycle = sum(k ** 3 * per_level for k in grid_levels)
+    return P * 40 + (refinements + 1) * P * 22 + refinements * (vcycle + P * 20)
 
 
 class ClockSampler:

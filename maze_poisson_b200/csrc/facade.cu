@@ -100,6 +100,8 @@ struct GridState {
     void* lev_g = nullptr;    // Green's function of the coarsest level (direct solve) or null
     int lev_fp64 = 0;         // the levels above hold doubles
     bool coarse_team = false; // the coarsest level (n <= kMixedTeamDirectN) is solved by the whole team
+    bool coarse_fft = false;  // the coarsest level (mixed_fft_coarse_ok) is solved by the team by FFT
+    void* lev_spec = nullptr; // its half spectrum
     double* bj_inv = nullptr;  // block-Jacobi block inverse (1000 x 1000) on BLOCKJACOBI grids
     // Poisson-Boltzmann (solver_initialize_grid_pois_boltz, grid_general.c:84-100)
     bool pb = false;
@@ -177,8 +179,11 @@ void free_grid(GridState& G) {
     }
     dev_free(G.lev_g);
     G.lev_g = nullptr;
+    dev_free(G.lev_spec);
+    G.lev_spec = nullptr;
     G.nlev = 0;
     G.coarse_team = false;
+    G.coarse_fft = false;
     G.ready = false;
 }
 
@@ -199,8 +204,24 @@ void free_mixed_levels(GridState& G) {
     }
     dev_free(G.lev_g);
     G.lev_g = nullptr;
+    dev_free(G.lev_spec);
+    G.lev_spec = nullptr;
     G.nlev = 0;
     G.coarse_team = false;
+    G.coarse_fft = false;
+}
+
+// First level that may be solved by FFT: 1, or from MZB_MIXED_COARSE (a tuning aid) "fft2"
+// -> 2, "levels" -> none (the hierarchy down to kMixedTeamDirectN).
+int mixed_fft_level() {
+    static const int lf = [] {
+        const char* e = getenv("MZB_MIXED_COARSE");
+        if (e == nullptr) return 1;
+        if (strcmp(e, "fft2") == 0) return 2;
+        if (strcmp(e, "levels") == 0) return kMixedMaxLevels;
+        return 1;
+    }();
+    return lf;
 }
 
 void ensure_mixed_levels(GridState& G) {
@@ -211,12 +232,24 @@ void ensure_mixed_levels(GridState& G) {
     const size_t w = fp64 ? sizeof(double) : sizeof(float);
     G.nlev = mixed_levels(G.n, G.lev_n);
     G.coarse_team = false;
-    for (int l = 1; l < G.nlev; l++)  // stop at the first level the team solves directly
-        if (G.lev_n[l] <= kMixedTeamDirectN) {
+    G.coarse_fft = false;
+    // Stop at the first level the team solves exactly: by FFT when one of n/2, n/4, ... has
+    // an FFT size (from level mixed_fft_level(), 1 unless MZB_MIXED_COARSE=fft2 / levels),
+    // else by the Green's function at <= kMixedTeamDirectN points per side.
+    const int lf = mixed_fft_level();
+    for (int l = lf; l < G.nlev; l++)
+        if (mixed_fft_coarse_ok(G.lev_n[l])) {
             G.nlev = l + 1;
-            G.coarse_team = true;
+            G.coarse_fft = true;
             break;
         }
+    if (!G.coarse_fft)
+        for (int l = 1; l < G.nlev; l++)
+            if (G.lev_n[l] <= kMixedTeamDirectN) {
+                G.nlev = l + 1;
+                G.coarse_team = true;
+                break;
+            }
     for (int l = 0; l < G.nlev; l++) {
         const size_t m = (size_t)G.lev_n[l] * G.lev_n[l] * G.lev_n[l];
         G.lev_x[l] = dev_alloc(m * w);
@@ -225,6 +258,7 @@ void ensure_mixed_levels(GridState& G) {
         zero_fill(G.lev_x[l], m * w);
     }
     const int nc = G.lev_n[G.nlev - 1];
+    if (G.coarse_fft) G.lev_spec = dev_alloc((size_t)nc * nc * (nc / 2 + 1) * 2 * w);
     if (G.coarse_team || (nc <= kMixedDirectN && mixed_small_level(G.nlev, G.lev_n) < G.nlev)) {
         const size_t N = (size_t)nc * nc * nc;
         G.lev_g = dev_alloc(N * w);
@@ -374,8 +408,11 @@ MixedArgs mixed_args(System& s, int prog, double cst) {
     m.nu2 = 2;
     m.coarse_sweeps = 16;
     m.nlev = G.nlev;
-    m.lsmall = G.coarse_team ? G.nlev : mixed_small_level(G.nlev, G.lev_n);
+    m.lsmall = G.coarse_team || G.coarse_fft ? G.nlev : mixed_small_level(G.nlev, G.lev_n);
     m.coarse_g = G.lev_g;
+    m.coarse_fft = G.coarse_fft ? 1 : 0;
+
+    m.coarse_spec = G.lev_spec;
     m.fp64 = G.lev_fp64;
     m.coarse_team = G.coarse_team ? 1 : 0;
     for (int l = 0; l < G.nlev; l++) {
@@ -436,6 +473,12 @@ int run_mixed(System& s, int prog, double cst) {
             if (!t[6]) break;
             fprintf(stderr, " down %.2f small %.2f up %.2f esum %.2f upd %.2f |", (t[2] - t[1]) * 1e-3,
                     (t[3] - t[2]) * 1e-3, (t[4] - t[3]) * 1e-3, (t[5] - t[4]) * 1e-3, (t[6] - t[5]) * 1e-3);
+        }
+        const unsigned long long* f = h + 2 + 8 * 8;
+        if (f[0] && f[7]) {
+            fprintf(stderr, "[coarse FFT us, refinement 1] twiddles %.2f planes-i %.2f sync %.2f planes-kj %.2f sync %.2f planes-i %.2f sync %.2f",
+                    (f[1] - f[0]) * 1e-3, (f[2] - f[1]) * 1e-3, (f[3] - f[2]) * 1e-3, (f[4] - f[3]) * 1e-3,
+                    (f[5] - f[4]) * 1e-3, (f[6] - f[5]) * 1e-3, (f[7] - f[6]) * 1e-3);
         }
         fprintf(stderr, "\n");
     }
@@ -2264,6 +2307,7 @@ double mzb_system_footprint(int n, int n_p) {
     int sizes[kMixedMaxLevels];
     const int L = mixed_levels(n, sizes);
     for (int l = 0; l < L; l++) levels += 3.0 * 4.0 * (double)sizes[l] * sizes[l] * sizes[l];
+    levels += 8.0 * (double)(n / 2) * (n / 2) * (n / 4 + 1);  // half spectrum of an FFT-solved coarse level
     const double grid = 8.0 * m * 10.0;  // q, phi x3, y, r, p0, p1, Ap, tmp
     const int nblk = (n_p + 31) / 32 > 0 ? (n_p + 31) / 32 : 1;
     const double nsb = std::ceil(nblk / 8.0);

@@ -9,17 +9,22 @@
 //   repeat: r = b - L x            (FP64, residual checked against tol in FP64)
 //           e = V-cycle(r)         (FP32: red-black GS V(nu1,nu2), 27-point full
 //                                   weighting scaled by 4 = (2h/h)^2 for the unscaled
-//                                   Laplacian, trilinear prolongation, levels down to
-//                                   4^3)
+//                                   Laplacian, trilinear prolongation, down to a coarse
+//                                   level solved exactly)
 //           x += e - mean(e)       (FP64; the periodic Laplacian's null space is the
 //                                   constants, and dropping e's mean keeps x's mean
 //                                   where it started, as CG does)
 //
-// Work placement. Levels with n > 16 are swept by every CTA with a grid barrier between
-// passes. Levels with n <= 16 (at most 3 x 4 x (16^3 + 8^3 + 4^3) B = 55 KB) are loaded
-// into CTA 0's shared memory and worked there while the other CTAs wait at the next grid
-// barrier; a coarsest level of at most 6^3 points is solved exactly by a convolution with
-// its Green's function instead of by sweeps. Every V-cycle starts a level from
+// Work placement. Levels are swept by every CTA with a grid barrier between passes. When
+// n/2 is 32, 64 or 128 the hierarchy has two levels and the coarse one is solved exactly by
+// FFT (team_fft: three passes, each CTA transforming whole planes in its shared memory),
+// which replaces the barrier-bound passes of the levels below. Otherwise levels go down to
+// the first one of at most 16 points per side, which every CTA solves by its Green's
+// function (team_direct). A plan kept for hierarchies that end at neither (mixed_small_level)
+// loads the levels with n <= 16 (at most 3 x 4 x (16^3 + 8^3 + 4^3) B = 55 KB) into CTA 0's
+// shared memory and works them there while the other CTAs wait at the next grid barrier;
+// a coarsest level of at most 6^3 points is solved exactly by a convolution with its
+// Green's function instead of by sweeps. Every V-cycle starts a level from
 // x = 0, so the first red half-sweep (x_red = -b/6, no neighbour reads) is folded into the
 // pass that writes the level's right-hand side (the FP64 residual pass, the
 // restrictions), and the sum of the finest correction, whose mean is removed, is taken in
@@ -980,6 +985,254 @@ __device__ void team_direct(const MixedArgs& a, const Team& tm, S* sm, int l) {
     }
 }
 
+// ---- the coarse level by FFT (whole team) ----
+//
+// A coarse level of nc = 32, 64 or 128 points per side is solved exactly, like
+// team_direct: x = the zero-mean solution of L x = b - mean(b) for the unscaled periodic
+// 7-point Laplacian, whose eigenvalues on the DFT basis are
+// lambda(k) = 2 cos(2 pi k1/nc) + 2 cos(2 pi k2/nc) + 2 cos(2 pi k3/nc) - 6. Five passes
+// over a half spectrum T[i][j][kk] (kk = 0..nc/2, complex), a team barrier after each:
+//   1. rows along k, real to complex, two rows per warp (packed as re + i im);
+//   2. lines along j, forward;
+//   3. lines along i: forward, times 1/(lambda nc^3) (0 at k = 0), inverse;
+//   4. lines along j, inverse;
+//   5. rows along k, complex to real, two rows per warp, into x (split layout).
+// A warp transforms a line of N = 32 R points, lane t holding points 32 r + t: a length-R
+// DFT in registers, twiddles W_N^(t k1), then a length-32 radix-2 decimation in
+// frequency across the lanes by shuffles, which leaves X[k1 + R brev5(t)] in lane t,
+// register k1. The inverse applies the adjoint of each step in reverse order (the
+// transposed butterflies with conjugate twiddles), so forward then inverse is N times
+// the identity in any distribution of the frequencies over the lanes.
+constexpr int kFftCoarseMax = 128;
+
+template <class S> struct CxT;
+template <> struct CxT<float> { using T = float2; };
+template <> struct CxT<double> { using T = double2; };
+template <class S> using Cx = typename CxT<S>::T;
+
+template <class C> __device__ __forceinline__ C cx(decltype(C::x) re, decltype(C::x) im) { C c; c.x = re; c.y = im; return c; }
+template <class C> __device__ __forceinline__ C cadd(C a, C b) { return cx<C>(a.x + b.x, a.y + b.y); }
+template <class C> __device__ __forceinline__ C csub(C a, C b) { return cx<C>(a.x - b.x, a.y - b.y); }
+template <class C> __device__ __forceinline__ C cmul(C a, C w) { return cx<C>(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x); }
+template <class C> __device__ __forceinline__ C cmulc(C a, C w) { return cx<C>(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y); }  // a conj(w)
+template <class C> __device__ __forceinline__ C cshfl_xor(C a, int m) {
+    return cx<C>(__shfl_xor_sync(0xffffffffu, a.x, m), __shfl_xor_sync(0xffffffffu, a.y, m));
+}
+template <class C> __device__ __forceinline__ C cshfl(C a, int src) {
+    return cx<C>(__shfl_sync(0xffffffffu, a.x, src), __shfl_sync(0xffffffffu, a.y, src));
+}
+__device__ __forceinline__ float fast_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double fast_div(double a, double b) { return a / b; }
+__device__ __forceinline__ int brev5(int t) { return (int)(__brev((unsigned)t) >> 27); }
+
+// forward DFT of the warp's line (tw[e] = W_N^e = exp(-2 pi i e / N))
+template <int R, class C>
+__device__ __forceinline__ void wfft_fwd(C (&v)[R], const C* tw, int t) {
+    if constexpr (R == 2) {
+        const C a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        const C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]), s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
+        v[0] = cadd(s02, s13);
+        v[2] = csub(s02, s13);
+        v[1] = cx<C>(d02.x + d13.y, d02.y - d13.x);  // d02 - i d13
+        v[3] = cx<C>(d02.x - d13.y, d02.y + d13.x);  // d02 + i d13
+    }
+#pragma unroll
+    for (int k1 = 1; k1 < R; k1++) v[k1] = cmul(v[k1], tw[t * k1]);
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+        const bool bottom = (t & d) != 0;
+        const C w = tw[(t & (d - 1)) * (16 / d) * R];
+#pragma unroll
+        for (int k1 = 0; k1 < R; k1++) {
+            const C p = cshfl_xor(v[k1], d);
+            v[k1] = bottom ? cmul(csub(p, v[k1]), w) : cadd(v[k1], p);
+        }
+    }
+}
+
+// N times the inverse of wfft_fwd (the adjoint of its steps, last first)
+template <int R, class C>
+__device__ __forceinline__ void wfft_inv(C (&v)[R], const C* tw, int t) {
+#pragma unroll
+    for (int d = 1; d <= 16; d <<= 1) {
+        const bool bottom = (t & d) != 0;
+        const C w = tw[(t & (d - 1)) * (16 / d) * R];
+#pragma unroll
+        for (int k1 = 0; k1 < R; k1++) {
+            const C p = cshfl_xor(v[k1], d);
+            v[k1] = bottom ? csub(p, cmulc(v[k1], w)) : cadd(v[k1], cmulc(p, w));
+        }
+    }
+#pragma unroll
+    for (int k1 = 1; k1 < R; k1++) v[k1] = cmulc(v[k1], tw[t * k1]);
+    if constexpr (R == 2) {
+        const C a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (R == 4) {
+        const C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]), s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
+        v[0] = cadd(s02, s13);
+        v[2] = csub(s02, s13);
+        v[1] = cx<C>(d02.x - d13.y, d02.y + d13.x);  // d02 + i d13
+        v[3] = cx<C>(d02.x + d13.y, d02.y - d13.x);  // d02 - i d13
+    }
+}
+
+template <int R, class S>
+__device__ bool team_fft_r(const MixedArgs& a, const Team& tm, unsigned& epoch, int l, Cx<S>* tw, Cx<S>* P, int outer) {
+    auto pstamp = [&](int k) { if (outer == 1) stamp(a, 2 + 8 * 8 + k); };
+    pstamp(0);
+    using C = Cx<S>;
+    constexpr int N = 32 * R, H = N / 2 + 1, NH = N * H;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nwc = blockDim.x >> 5;
+    const int bl = brev5(lane), src0 = brev5((32 - bl) & 31);
+    C* T = static_cast<C*>(a.coarse_spec);
+    const S* b = lev_b<S>(a, l);
+    S* x = lev_x<S>(a, l);
+    for (int e = threadIdx.x; e < N; e += blockDim.x) {
+        double sv, cv;
+        sincospi(2.0 * e / N, &sv, &cv);
+        tw[e] = cx<C>((S)cv, (S)-sv);
+    }
+    __syncthreads();
+    pstamp(1);
+    // A. each CTA takes whole planes i: rows along k (two real rows per warp as one complex
+    //    row), then lines along j, in its shared plane P[j][kk]; the plane goes to T[i].
+    for (int i = tm.b; i < N; i += tm.nblk) {
+        for (int pr = w; pr < N / 2; pr += nwc) {
+            const int jA = 2 * pr, jB = jA + 1;
+            C v[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int k = 32 * r + lane;
+                v[r] = cx<C>(b[split_idx(N, i, jA, k)], b[split_idx(N, i, jB, k)]);
+            }
+            wfft_fwd<R>(v, tw, lane);
+#pragma unroll
+            for (int k1 = 0; k1 < R; k1++) {  // X_A = (Z[k] + conj Z[N-k]) / 2, X_B = (Z[k] - conj Z[N-k]) / 2i
+                const C z = v[k1];
+                const C zc = k1 == 0 ? cshfl(v[0], src0) : cshfl(v[R - k1], lane ^ 31);
+                const int k = k1 + R * bl;
+                if (k < H) {
+                    P[jA * H + k] = cx<C>(S(0.5) * (z.x + zc.x), S(0.5) * (z.y - zc.y));
+                    P[jB * H + k] = cx<C>(S(0.5) * (z.y + zc.y), S(0.5) * (zc.x - z.x));
+                }
+            }
+        }
+        __syncthreads();
+        for (int kk = w; kk < H; kk += nwc) {
+            C v[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = P[(32 * r + lane) * H + kk];
+            wfft_fwd<R>(v, tw, lane);
+#pragma unroll
+            for (int k1 = 0; k1 < R; k1++) P[(k1 + R * bl) * H + kk] = v[k1];
+        }
+        __syncthreads();
+        C* Ti = T + (size_t)i * NH;
+        for (int e = threadIdx.x; e < NH; e += blockDim.x) Ti[e] = P[e];
+        __syncthreads();
+    }
+    pstamp(2);
+    if (!team_sync(tm, epoch)) return false;
+    pstamp(3);
+    // B. each CTA takes whole planes kj: lines along i forward, times 1/(lambda N^3), inverse
+    const S inv_n3 = S(1) / (S(N) * S(N) * S(N));
+    for (int kj = tm.b; kj < N; kj += tm.nblk) {
+        for (int e = threadIdx.x; e < NH; e += blockDim.x) {
+            const int ii = e / H, kk = e - ii * H;
+            P[e] = T[((size_t)ii * N + kj) * H + kk];
+        }
+        __syncthreads();
+        const S lj = S(2) * tw[kj].x - S(6);
+        for (int kk = w; kk < H; kk += nwc) {
+            C v[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = P[(32 * r + lane) * H + kk];
+            wfft_fwd<R>(v, tw, lane);
+            const S ljk = lj + S(2) * tw[kk].x;
+#pragma unroll
+            for (int k1 = 0; k1 < R; k1++) {
+                const int ki = k1 + R * bl;
+                const S f = (ki | kj | kk) == 0 ? S(0) : fast_div(inv_n3, S(2) * tw[ki].x + ljk);
+                v[k1] = cx<C>(v[k1].x * f, v[k1].y * f);
+            }
+            wfft_inv<R>(v, tw, lane);
+#pragma unroll
+            for (int r = 0; r < R; r++) P[(32 * r + lane) * H + kk] = v[r];
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < NH; e += blockDim.x) {
+            const int ii = e / H, kk = e - ii * H;
+            T[((size_t)ii * N + kj) * H + kk] = P[e];
+        }
+        __syncthreads();
+    }
+    pstamp(4);
+    if (!team_sync(tm, epoch)) return false;
+    pstamp(5);
+    // C. planes i again: lines along j inverse, then rows along k complex to real
+    //    (Z = X_A + i X_B, X[k] = conj X[N - k] above N/2) into x
+    for (int i = tm.b; i < N; i += tm.nblk) {
+        const C* Ti = T + (size_t)i * NH;
+        for (int e = threadIdx.x; e < NH; e += blockDim.x) P[e] = Ti[e];
+        __syncthreads();
+        for (int kk = w; kk < H; kk += nwc) {
+            C v[R];
+#pragma unroll
+            for (int k1 = 0; k1 < R; k1++) v[k1] = P[(k1 + R * bl) * H + kk];
+            wfft_inv<R>(v, tw, lane);
+#pragma unroll
+            for (int r = 0; r < R; r++) P[(32 * r + lane) * H + kk] = v[r];
+        }
+        __syncthreads();
+        for (int pr = w; pr < N / 2; pr += nwc) {
+            const int jA = 2 * pr, jB = jA + 1;
+            C v[R];
+#pragma unroll
+            for (int k1 = 0; k1 < R; k1++) {
+                const int k = k1 + R * bl;
+                const bool up = k >= H;
+                const int kr = up ? N - k : k;
+                C xa = P[jA * H + kr], xb = P[jB * H + kr];
+                if (up) {
+                    xa.y = -xa.y;
+                    xb.y = -xb.y;
+                }
+                v[k1] = cx<C>(xa.x - xb.y, xa.y + xb.x);
+            }
+            wfft_inv<R>(v, tw, lane);
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int k = 32 * r + lane;
+                x[split_idx(N, i, jA, k)] = v[r].x;
+                x[split_idx(N, i, jB, k)] = v[r].y;
+            }
+        }
+        __syncthreads();
+    }
+    pstamp(6);
+    const bool ok = team_sync(tm, epoch);
+    pstamp(7);
+    return ok;
+}
+
+// Shared memory of the FFT-solved coarse level: one plane of the half spectrum.
+__host__ __device__ constexpr size_t fft_plane_bytes(int nc, size_t scalar) { return (size_t)nc * (nc / 2 + 1) * 2 * scalar; }
+
+template <class S>
+__device__ bool team_fft(const MixedArgs& a, const Team& tm, unsigned& epoch, S* sm, int l, int outer) {
+    __shared__ Cx<S> tw[kFftCoarseMax];
+    Cx<S>* P = reinterpret_cast<Cx<S>*>(sm);
+    const int n = a.lev_n[l];
+    if (n == 128) return team_fft_r<4, S>(a, tm, epoch, l, tw, P, outer);
+    if (n == 64) return team_fft_r<2, S>(a, tm, epoch, l, tw, P, outer);
+    return team_fft_r<1, S>(a, tm, epoch, l, tw, P, outer);
+}
+
 // Grid-wide red-black sweeps of level l: `half_sweeps` colours starting at first_colour,
 // a grid barrier after each except (when skip_last_barrier) the last. When esum is not
 // null the values written in the last two half-sweeps are summed into it.
@@ -1019,6 +1272,8 @@ __device__ bool vcycle(const MixedArgs& a, const Team& tm, S* sm, unsigned& epoc
     if (ls < L) {
         if (tm.b == 0) small_vcycle(a, sm, R(ls - 1));
         if (!team_sync(tm, epoch)) return false;
+    } else if (a.coarse_fft) {
+        if (!team_fft<S>(a, tm, epoch, sm, L - 1, outer)) return false;
     } else if (a.coarse_team) {
         team_direct(a, tm, sm, L - 1);
         if (!team_sync(tm, epoch)) return false;
@@ -1061,7 +1316,7 @@ __device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs&
         const S rf = (S)r;
         const int sx = split_idx(n, i, j, k);
         rb[sx] = rf;
-        e[sx] = ((i + j + k) & 1) == 0 ? rf * neg_sixth<S>() : S(0);
+        if (((i + j + k) & 1) == 0) e[sx] = rf * neg_sixth<S>();  // black e: written by the first half-sweep
         rmax = fmax(rmax, fabs(r));
     });
     return rmax;
@@ -1136,8 +1391,9 @@ __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedA
             const int p0 = cA * hp + srow + (k >> 1), p1 = (cA ^ 1) * hp + srow + (k >> 1);
             rb[p0] = rf0;
             rb[p1] = rf1;
-            e[p0] = cA == 0 ? rf0 * neg_sixth<S>() : S(0);
-            e[p1] = cA == 1 ? rf1 * neg_sixth<S>() : S(0);
+            // red e only: the first half-sweep (black) writes the black values without reading them
+            if (cA == 0) e[p0] = rf0 * neg_sixth<S>();
+            else e[p1] = rf1 * neg_sixth<S>();
             rmax = fmax(rmax, fmax(fabs(r0), fabs(r1)));
         }
     });
@@ -1344,6 +1600,7 @@ size_t g_batch_smem_set = 0;
 
 size_t small_smem_bytes(const MixedArgs& a) {
     const size_t w = a.fp64 ? sizeof(double) : sizeof(float);
+    if (a.coarse_fft) return fft_plane_bytes(a.lev_n[a.nlev - 1], w);  // one spectrum plane
     if (a.coarse_team) {  // G and b of the coarsest level in every CTA
         const size_t nc = (size_t)a.lev_n[a.nlev - 1];
         return 2 * nc * nc * nc * w;

@@ -9,7 +9,7 @@ namespace mzb {
 constexpr int kMixedMaxLevels = 10;
 constexpr int kMixedSmallN = 16;     // levels with n <= this live in CTA 0's shared memory
 constexpr int kMixedMaxN = 1024;     // largest grid of the mixed solver (32-bit offsets in a level)
-constexpr int kMixedStampSlots = 2 + 8 * 8;
+constexpr int kMixedStampSlots = 2 + 8 * 8 + 8;  // + coarse-FFT pass stamps of refinement 1
 
 struct MixedArgs {
     int prog;           // PROG_INIT_FIELD, PROG_LCG_UPDATE, PROG_MAZE_LCG, PROG_MG_UPDATE, PROG_MAZE_MG
@@ -23,6 +23,9 @@ struct MixedArgs {
     const void* coarse_g;   // Green's function of the coarsest level (mixed_coarse_green), stored
                             // like the levels (float or double), or null
     int coarse_team;        // 1: the coarsest level is solved by every CTA of the team with coarse_g
+    int coarse_fft;         // 1: the coarsest level (32, 64 or 128 per side) is solved by every CTA
+                            // of the team by FFT, in coarse_spec
+    void* coarse_spec;      // n (n/2 + 1) n complex values (float2, or double2 when fp64)
     int nlev;
     int lsmall;         // first level held in shared memory (nlev if none; >= 1)
     int lev_n[kMixedMaxLevels];
@@ -53,6 +56,8 @@ constexpr int kMixedDirectN = 6;
 // every CTA of the team solves directly: a slice of the convolution with its Green's
 // function each (see mixed.cu).
 constexpr int kMixedTeamDirectN = 16;
+// Coarse levels the team solves by FFT (mixed_fft_coarse_ok): 32, 64 or 128 points per side.
+inline bool mixed_fft_coarse_ok(int nc) { return nc == 32 || nc == 64 || nc == 128; }
 // Pseudo-inverse kernel of the unscaled periodic 7-point Laplacian on an n^3 grid:
 // g[d] = (1/n^3) sum_{k != 0} cos(2 pi k.d / n) / lambda(k),
 // lambda(k) = 2 cos(2 pi k1/n) + 2 cos(2 pi k2/n) + 2 cos(2 pi k3/n) - 6.
