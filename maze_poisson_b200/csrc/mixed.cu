@@ -1025,9 +1025,36 @@ __device__ __forceinline__ float fast_div(float a, float b) { return __fdividef(
 __device__ __forceinline__ double fast_div(double a, double b) { return a / b; }
 __device__ __forceinline__ int brev5(int t) { return (int)(__brev((unsigned)t) >> 27); }
 
-// forward DFT of the warp's line (tw[e] = W_N^e = exp(-2 pi i e / N))
+// The lane's twiddles of the five across-lane stages: forward, W_{2d}^m on the bottom
+// lane of a pair and 1 on the top one (m = t mod d); inverse, +-conj(W_{2d}^m) (+ top,
+// - bottom).
+template <class C>
+struct LaneTw {
+    C f[5], i[5];
+};
 template <int R, class C>
-__device__ __forceinline__ void wfft_fwd(C (&v)[R], const C* tw, int t) {
+__device__ __forceinline__ LaneTw<C> lane_tw(const C* tw, int t) {
+    LaneTw<C> L;
+#pragma unroll
+    for (int s = 0; s < 5; s++) {
+        const int d = 16 >> s;
+        const C w = tw[(t & (d - 1)) * (16 / d) * R];
+        const bool bottom = (t & d) != 0;
+        L.f[s] = bottom ? w : cx<C>(1, 0);
+        const int di = 1 << s;
+        const C wi = tw[(t & (di - 1)) * (16 / di) * R];
+        L.i[s] = (t & di) != 0 ? cx<C>(-wi.x, wi.y) : cx<C>(wi.x, -wi.y);
+    }
+    return L;
+}
+
+// forward DFT of the warp's line: a length-R DFT in registers, twiddles W_N^(t k1)
+// (tq[k1 * 32 + t], W_N^e = exp(-2 pi i e / N)), then the across-lane stages d = 16 .. 1, each
+// (u, v) -> (u + v, (u - v) W_{2d}^m) on the pair of lanes t, t + d: on either lane
+// (+-own + partner) times the lane's twiddle.
+template <int R, class C>
+__device__ __forceinline__ void wfft_fwd(C (&v)[R], const C* tq, const LaneTw<C>& L, int t) {
+    using S = decltype(C::x);
     if constexpr (R == 2) {
         const C a = v[0], b = v[1];
         v[0] = cadd(a, b);
@@ -1040,34 +1067,37 @@ __device__ __forceinline__ void wfft_fwd(C (&v)[R], const C* tw, int t) {
         v[3] = cx<C>(d02.x - d13.y, d02.y + d13.x);  // d02 + i d13
     }
 #pragma unroll
-    for (int k1 = 1; k1 < R; k1++) v[k1] = cmul(v[k1], tw[t * k1]);
+    for (int k1 = 1; k1 < R; k1++) v[k1] = cmul(v[k1], tq[k1 * 32 + t]);
 #pragma unroll
-    for (int d = 16; d >= 1; d >>= 1) {
-        const bool bottom = (t & d) != 0;
-        const C w = tw[(t & (d - 1)) * (16 / d) * R];
+    for (int s = 0; s < 5; s++) {
+        const int d = 16 >> s;
+        const S sg = (t & d) != 0 ? S(-1) : S(1);
 #pragma unroll
         for (int k1 = 0; k1 < R; k1++) {
             const C p = cshfl_xor(v[k1], d);
-            v[k1] = bottom ? cmul(csub(p, v[k1]), w) : cadd(v[k1], p);
+            v[k1] = cmul(cx<C>(fma_s(sg, v[k1].x, p.x), fma_s(sg, v[k1].y, p.y)), L.f[s]);
         }
     }
 }
 
-// N times the inverse of wfft_fwd (the adjoint of its steps, last first)
+// N times the inverse of wfft_fwd: the adjoint of each step, last first; the adjoint of a
+// stage maps the pair (a, b) on lanes (t, t + d) to (a + conj(w) b, a - conj(w) b).
 template <int R, class C>
-__device__ __forceinline__ void wfft_inv(C (&v)[R], const C* tw, int t) {
+__device__ __forceinline__ void wfft_inv(C (&v)[R], const C* tq, const LaneTw<C>& L, int t) {
 #pragma unroll
-    for (int d = 1; d <= 16; d <<= 1) {
-        const bool bottom = (t & d) != 0;
-        const C w = tw[(t & (d - 1)) * (16 / d) * R];
+    for (int s = 0; s < 5; s++) {
+        const int d = 1 << s;
+        const bool top = (t & d) == 0;
 #pragma unroll
         for (int k1 = 0; k1 < R; k1++) {
             const C p = cshfl_xor(v[k1], d);
-            v[k1] = bottom ? csub(p, cmulc(v[k1], w)) : cadd(v[k1], cmulc(p, w));
+            const C a = top ? v[k1] : p, b = top ? p : v[k1];
+            const C w = L.i[s];
+            v[k1] = cx<C>(fma_s(w.x, b.x, fma_s(-w.y, b.y, a.x)), fma_s(w.x, b.y, fma_s(w.y, b.x, a.y)));
         }
     }
 #pragma unroll
-    for (int k1 = 1; k1 < R; k1++) v[k1] = cmulc(v[k1], tw[t * k1]);
+    for (int k1 = 1; k1 < R; k1++) v[k1] = cmulc(v[k1], tq[k1 * 32 + t]);
     if constexpr (R == 2) {
         const C a = v[0], b = v[1];
         v[0] = cadd(a, b);
@@ -1081,12 +1111,19 @@ __device__ __forceinline__ void wfft_inv(C (&v)[R], const C* tw, int t) {
     }
 }
 
+// Z[N - k] for each register of wfft_fwd's output (lane t, register k1 <-> k = k1 + R brev5(t))
+template <int R, class C>
+__device__ __forceinline__ C mirror(const C (&v)[R], int k1, int lane, int src0) {
+    return k1 == 0 ? cshfl(v[0], src0) : cshfl(v[R - k1], lane ^ 31);
+}
+
 template <int R, class S>
-__device__ bool team_fft_r(const MixedArgs& a, const Team& tm, unsigned& epoch, int l, Cx<S>* tw, Cx<S>* P, int outer) {
+__device__ bool team_fft_r(const MixedArgs& a, const Team& tm, unsigned& epoch, int l, Cx<S>* tw, Cx<S>* tq, S* tc,
+                           Cx<S>* P, int outer) {
+    using C = Cx<S>;
+    constexpr int N = 32 * R, H = N / 2 + 1, NH = N * H, NQ = N / 2;
     auto pstamp = [&](int k) { if (outer == 1) stamp(a, 2 + 8 * 8 + k); };
     pstamp(0);
-    using C = Cx<S>;
-    constexpr int N = 32 * R, H = N / 2 + 1, NH = N * H;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nwc = blockDim.x >> 5;
     const int bl = brev5(lane), src0 = brev5((32 - bl) & 31);
     C* T = static_cast<C*>(a.coarse_spec);
@@ -1098,7 +1135,18 @@ __device__ bool team_fft_r(const MixedArgs& a, const Team& tm, unsigned& epoch, 
         tw[e] = cx<C>((S)cv, (S)-sv);
     }
     __syncthreads();
+    // lane-indexed tables (no bank conflicts): tq[k1][t] = W_N^(t k1), and tc[k1][t] =
+    // 2 cos(2 pi ki / N) of the frequency ki = k1 + R brev5(t) a lane holds after wfft_fwd
+    for (int e = threadIdx.x; e < 32 * R; e += blockDim.x) {
+        const int k1 = e >> 5, t = e & 31;
+        tq[e] = tw[t * k1];
+        tc[e] = S(2) * tw[k1 + R * brev5(t)].x;
+    }
+    __syncthreads();
+    const LaneTw<C> L = lane_tw<R>(tw, lane);
     pstamp(1);
+    // The line tasks of a plane along j: kk = 1 .. N/2 - 1, and task 0 for the DC and Nyquist
+    // columns (kk = 0, N/2), both real after the row transforms, as one complex column.
     // A. each CTA takes whole planes i: rows along k (two real rows per warp as one complex
     //    row), then lines along j, in its shared plane P[j][kk]; the plane goes to T[i].
     for (int i = tm.b; i < N; i += tm.nblk) {
@@ -1110,11 +1158,10 @@ __device__ bool team_fft_r(const MixedArgs& a, const Team& tm, unsigned& epoch, 
                 const int k = 32 * r + lane;
                 v[r] = cx<C>(b[split_idx(N, i, jA, k)], b[split_idx(N, i, jB, k)]);
             }
-            wfft_fwd<R>(v, tw, lane);
+            wfft_fwd<R>(v, tq, L, lane);
 #pragma unroll
             for (int k1 = 0; k1 < R; k1++) {  // X_A = (Z[k] + conj Z[N-k]) / 2, X_B = (Z[k] - conj Z[N-k]) / 2i
-                const C z = v[k1];
-                const C zc = k1 == 0 ? cshfl(v[0], src0) : cshfl(v[R - k1], lane ^ 31);
+                const C z = v[k1], zc = mirror(v, k1, lane, src0);
                 const int k = k1 + R * bl;
                 if (k < H) {
                     P[jA * H + k] = cx<C>(S(0.5) * (z.x + zc.x), S(0.5) * (z.y - zc.y));
@@ -1123,13 +1170,36 @@ __device__ bool team_fft_r(const MixedArgs& a, const Team& tm, unsigned& epoch, 
             }
         }
         __syncthreads();
-        for (int kk = w; kk < H; kk += nwc) {
+        for (int kk = w; kk < NQ; kk += nwc) {
             C v[R];
+            if (kk == 0) {
 #pragma unroll
-            for (int r = 0; r < R; r++) v[r] = P[(32 * r + lane) * H + kk];
-            wfft_fwd<R>(v, tw, lane);
+                for (int r = 0; r < R; r++) {
+                    const int j = 32 * r + lane;
+                    v[r] = cx<C>(P[j * H].x, P[j * H + NQ].x);
+                }
+            } else {
 #pragma unroll
-            for (int k1 = 0; k1 < R; k1++) P[(k1 + R * bl) * H + kk] = v[k1];
+                for (int r = 0; r < R; r++) v[r] = P[(32 * r + lane) * H + kk];
+            }
+            wfft_fwd<R>(v, tq, L, lane);
+            if (kk == 0) {  // separate the two real columns' spectra (every kj)
+                C c0[R], cq[R];
+#pragma unroll
+                for (int k1 = 0; k1 < R; k1++) {
+                    const C z = v[k1], zc = mirror(v, k1, lane, src0);
+                    c0[k1] = cx<C>(S(0.5) * (z.x + zc.x), S(0.5) * (z.y - zc.y));
+                    cq[k1] = cx<C>(S(0.5) * (z.y + zc.y), S(0.5) * (zc.x - z.x));
+                }
+#pragma unroll
+                for (int k1 = 0; k1 < R; k1++) {
+                    P[(k1 + R * bl) * H] = c0[k1];
+                    P[(k1 + R * bl) * H + NQ] = cq[k1];
+                }
+            } else {
+#pragma unroll
+                for (int k1 = 0; k1 < R; k1++) P[(k1 + R * bl) * H + kk] = v[k1];
+            }
         }
         __syncthreads();
         C* Ti = T + (size_t)i * NH;
@@ -1139,54 +1209,89 @@ __device__ bool team_fft_r(const MixedArgs& a, const Team& tm, unsigned& epoch, 
     pstamp(2);
     if (!team_sync(tm, epoch)) return false;
     pstamp(3);
-    // B. each CTA takes whole planes kj: lines along i forward, times 1/(lambda N^3), inverse
+    // B. each CTA takes whole planes kj: lines along i forward, times 1/(lambda N^3), inverse.
+    //    With more CTAs than planes, the extra CTAs take the lines kk = N/2 of every plane.
     const S inv_n3 = S(1) / (S(N) * S(N) * S(N));
+    const bool offload = tm.nblk > N;
+    const int kk_end = offload ? NQ : H;
+    auto line_i = [&](C (&v)[R], int kj, int kk) {
+        wfft_fwd<R>(v, tq, L, lane);
+        const S ljk = S(2) * tw[kj].x + S(2) * tw[kk].x - S(6);
+#pragma unroll
+        for (int k1 = 0; k1 < R; k1++) {
+            const int ki = k1 + R * bl;
+            const S f = (ki | kj | kk) == 0 ? S(0) : fast_div(inv_n3, tc[k1 * 32 + lane] + ljk);
+            v[k1] = cx<C>(v[k1].x * f, v[k1].y * f);
+        }
+        wfft_inv<R>(v, tq, L, lane);
+    };
     for (int kj = tm.b; kj < N; kj += tm.nblk) {
         for (int e = threadIdx.x; e < NH; e += blockDim.x) {
             const int ii = e / H, kk = e - ii * H;
-            P[e] = T[((size_t)ii * N + kj) * H + kk];
+            if (kk < kk_end) P[e] = T[((size_t)ii * N + kj) * H + kk];
         }
         __syncthreads();
-        const S lj = S(2) * tw[kj].x - S(6);
-        for (int kk = w; kk < H; kk += nwc) {
+        for (int kk = w; kk < kk_end; kk += nwc) {
             C v[R];
 #pragma unroll
             for (int r = 0; r < R; r++) v[r] = P[(32 * r + lane) * H + kk];
-            wfft_fwd<R>(v, tw, lane);
-            const S ljk = lj + S(2) * tw[kk].x;
-#pragma unroll
-            for (int k1 = 0; k1 < R; k1++) {
-                const int ki = k1 + R * bl;
-                const S f = (ki | kj | kk) == 0 ? S(0) : fast_div(inv_n3, S(2) * tw[ki].x + ljk);
-                v[k1] = cx<C>(v[k1].x * f, v[k1].y * f);
-            }
-            wfft_inv<R>(v, tw, lane);
+            line_i(v, kj, kk);
 #pragma unroll
             for (int r = 0; r < R; r++) P[(32 * r + lane) * H + kk] = v[r];
         }
         __syncthreads();
         for (int e = threadIdx.x; e < NH; e += blockDim.x) {
             const int ii = e / H, kk = e - ii * H;
-            T[((size_t)ii * N + kj) * H + kk] = P[e];
+            if (kk < kk_end) T[((size_t)ii * N + kj) * H + kk] = P[e];
         }
         __syncthreads();
+    }
+    if (offload && tm.b >= N) {
+        const int nx = (tm.nblk - N) * nwc;
+        for (int kj = (tm.b - N) * nwc + w; kj < N; kj += nx) {
+            C* line = T + (size_t)kj * H + NQ;
+            C v[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) v[r] = line[(size_t)(32 * r + lane) * NH];
+            line_i(v, kj, NQ);
+#pragma unroll
+            for (int r = 0; r < R; r++) line[(size_t)(32 * r + lane) * NH] = v[r];
+        }
     }
     pstamp(4);
     if (!team_sync(tm, epoch)) return false;
     pstamp(5);
-    // C. planes i again: lines along j inverse, then rows along k complex to real
+    // C. planes i again: lines along j inverse (the DC and Nyquist columns as one complex
+    //    column, whose inverse is real in both parts), then rows along k complex to real
     //    (Z = X_A + i X_B, X[k] = conj X[N - k] above N/2) into x
     for (int i = tm.b; i < N; i += tm.nblk) {
         const C* Ti = T + (size_t)i * NH;
         for (int e = threadIdx.x; e < NH; e += blockDim.x) P[e] = Ti[e];
         __syncthreads();
-        for (int kk = w; kk < H; kk += nwc) {
+        for (int kk = w; kk < NQ; kk += nwc) {
             C v[R];
+            if (kk == 0) {
 #pragma unroll
-            for (int k1 = 0; k1 < R; k1++) v[k1] = P[(k1 + R * bl) * H + kk];
-            wfft_inv<R>(v, tw, lane);
+                for (int k1 = 0; k1 < R; k1++) {
+                    const C c0 = P[(k1 + R * bl) * H], cq = P[(k1 + R * bl) * H + NQ];
+                    v[k1] = cx<C>(c0.x - cq.y, c0.y + cq.x);
+                }
+            } else {
 #pragma unroll
-            for (int r = 0; r < R; r++) P[(32 * r + lane) * H + kk] = v[r];
+                for (int k1 = 0; k1 < R; k1++) v[k1] = P[(k1 + R * bl) * H + kk];
+            }
+            wfft_inv<R>(v, tq, L, lane);
+            if (kk == 0) {
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    const int j = 32 * r + lane;
+                    P[j * H] = cx<C>(v[r].x, S(0));
+                    P[j * H + NQ] = cx<C>(v[r].y, S(0));
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; r++) P[(32 * r + lane) * H + kk] = v[r];
+            }
         }
         __syncthreads();
         for (int pr = w; pr < N / 2; pr += nwc) {
@@ -1204,7 +1309,7 @@ __device__ bool team_fft_r(const MixedArgs& a, const Team& tm, unsigned& epoch, 
                 }
                 v[k1] = cx<C>(xa.x - xb.y, xa.y + xb.x);
             }
-            wfft_inv<R>(v, tw, lane);
+            wfft_inv<R>(v, tq, L, lane);
 #pragma unroll
             for (int r = 0; r < R; r++) {
                 const int k = 32 * r + lane;
@@ -1225,12 +1330,13 @@ __host__ __device__ constexpr size_t fft_plane_bytes(int nc, size_t scalar) { re
 
 template <class S>
 __device__ bool team_fft(const MixedArgs& a, const Team& tm, unsigned& epoch, S* sm, int l, int outer) {
-    __shared__ Cx<S> tw[kFftCoarseMax];
+    __shared__ Cx<S> tw[kFftCoarseMax], tq[kFftCoarseMax];
+    __shared__ S tc[kFftCoarseMax];
     Cx<S>* P = reinterpret_cast<Cx<S>*>(sm);
     const int n = a.lev_n[l];
-    if (n == 128) return team_fft_r<4, S>(a, tm, epoch, l, tw, P, outer);
-    if (n == 64) return team_fft_r<2, S>(a, tm, epoch, l, tw, P, outer);
-    return team_fft_r<1, S>(a, tm, epoch, l, tw, P, outer);
+    if (n == 128) return team_fft_r<4, S>(a, tm, epoch, l, tw, tq, tc, P, outer);
+    if (n == 64) return team_fft_r<2, S>(a, tm, epoch, l, tw, tq, tc, P, outer);
+    return team_fft_r<1, S>(a, tm, epoch, l, tw, tq, tc, P, outer);
 }
 
 // Grid-wide red-black sweeps of level l: `half_sweeps` colours starting at first_colour,

@@ -20,7 +20,10 @@
 // halves. On the diagonal super-tile each unordered block pair is taken once (and each
 // pair inside a block once, 16 steps of one partner). A tile whose bounding
 // boxes are farther apart than r_cut (minimum image, 1e-9 relative margin) is skipped;
-// pruning is off when a coordinate lies outside [0, L).
+// pruning is off when a coordinate lies outside [0, L). Inside a tile, a step in which no
+// lane's two partners lie inside r_cut skips the pair terms (a warp vote). 1/r is an FP32
+// seed refined by two FP64 Newton steps; types sit in the shared position arrays as integer
+// bits; the pair-constant rows have an odd stride (no bank conflicts between type pairs).
 //
 // Determinism. Registers and warp arrays accumulate in step order; the warps' J partials
 // are summed in warp order; each ion's force is the sum of its super-tile partials in a
@@ -35,7 +38,11 @@ namespace mzb {
 
 constexpr int kTfSb = 8;                  // blocks of 32 ions per super-block
 constexpr int kTfThreads = kTfSb * 32;    // one warp per I block of a super-block
-constexpr int kTfTab = 64 * kPairConsts;  // pair-constant table (up to 8 types)
+// Pair-constant table in shared memory, up to 8 types, one row of kTfTabStride doubles per
+// type pair: the odd stride puts the rows a warp reads at once (lanes of different type
+// pairs) on different banks.
+constexpr int kTfTabStride = kPairConsts + 1;
+constexpr int kTfTab = 64 * kTfTabStride;
 constexpr size_t kTfSmem =
     sizeof(double) * (kTfTab + 2 * kTfSb * 32 * 4 + kTfSb * kTfSb * 32 * 3);
 
@@ -102,31 +109,65 @@ __global__ void k_tf_boxes(ParticleDev P) {
     }
 }
 
+// The ion type stored in a double slot of the shared position arrays as its integer bits
+// (read back without a conversion).
+__device__ __forceinline__ double type_bits(int t) { return __longlong_as_double((long long)t); }
+__device__ __forceinline__ int type_of(double v) { return (int)__double_as_longlong(v); }
+
 // One pair (i, partner j at x, y, z of type tj) for the lane's ion: whether it is inside
 // r_cut (and both ions exist), and its force times the separation and energy.
+// 1/sqrt(x) for x in the range of squared pair distances (normal FP32 numbers): an FP32
+// seed (relative error below 2^-22) refined by two Newton-Raphson steps for x^(-1/2),
+// y <- y (3/2 - x y^2 / 2), each of which squares the relative error, so the result is
+// within a few ulp of the FP64 value.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+    double y = (double)rsqrtf((float)x);
+    const double h = 0.5 * x;
+    y = y * fma(-h * y, y, 1.5);
+    y = y * fma(-h * y, y, 1.5);
+    return y;
+}
+
+struct PairSep {
+    double dx, dy, dz, r2;
+    bool in;
+};
+__device__ __forceinline__ PairSep pair_sep(double L, double invL, double rc2, double xi, double yi, double zi, int ti,
+                                            double xj, double yj, double zj, int tj) {
+    PairSep p;
+    p.dx = xi - xj;
+    p.dy = yi - yj;
+    p.dz = zi - zj;
+    p.dx -= L * round(p.dx * invL);
+    p.dy -= L * round(p.dy * invL);
+    p.dz -= L * round(p.dz * invL);
+    p.r2 = p.dx * p.dx + p.dy * p.dy + p.dz * p.dz;
+    p.in = ti >= 0 && tj >= 0 && p.r2 <= rc2;
+    return p;
+}
+template <int POT>
+__device__ __forceinline__ void pair_force(const double* tab, int ntyp, double rc2, int ti, int tj, const PairSep& p,
+                                           double& ax, double& ay, double& az, double& vm) {
+    const double r2s = p.in ? p.r2 : rc2;  // a harmless value for lanes whose pair is not taken
+    double fr;
+    pair_terms<POT>(tab + kTfTabStride * ((p.in ? ti : 0) * ntyp + (p.in ? tj : 0)), r2s, rsqrt_nr(r2s), fr, vm);
+    ax = fr * p.dx;
+    ay = fr * p.dy;
+    az = fr * p.dz;
+}
 template <int POT>
 __device__ __forceinline__ bool pair_eval(const double* tab, int ntyp, double L, double invL, double rc2, double xi,
                                           double yi, double zi, int ti, double xj, double yj, double zj, int tj,
                                           double& ax, double& ay, double& az, double& vm) {
-    double dx = xi - xj, dy = yi - yj, dz = zi - zj;
-    dx -= L * round(dx * invL);
-    dy -= L * round(dy * invL);
-    dz -= L * round(dz * invL);
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    const bool in = ti >= 0 && tj >= 0 && r2 <= rc2;
-    const double r2s = in ? r2 : rc2;  // a harmless value for lanes whose pair is not taken
-    double fr;
-    pair_terms<POT>(tab + kPairConsts * ((in ? ti : 0) * ntyp + (in ? tj : 0)), r2s, rsqrt(r2s), fr, vm);
-    ax = fr * dx;
-    ay = fr * dy;
-    az = fr * dz;
-    return in;
+    const PairSep p = pair_sep(L, invL, rc2, xi, yi, zi, ti, xj, yj, zj, tj);
+    pair_force<POT>(tab, ntyp, rc2, ti, tj, p, ax, ay, az, vm);
+    return p.in;
 }
 
 template <int POT>
 __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
     extern __shared__ double sm[];
-    double* tab = sm;                              // [64 * kPairConsts]
+    double* tab = sm;                              // [64][kTfTabStride]
     double* ipos = tab + kTfTab;                   // [4][256]: x, y, z, type (structure of arrays)
     double* jpos = ipos + kTfSb * 32 * 4;          // [4][256]
     double* fjw = jpos + kTfSb * 32 * 4;           // [8 warps][8 J blocks][3][32]
@@ -140,18 +181,19 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
     const double prune2 = rc2 * (1.0 + 1e-9);
     const bool prune = P.flags[1] == 0;
 
-    for (int x = threadIdx.x; x < ntyp * ntyp * kPairConsts; x += blockDim.x) tab[x] = P.tab[x];
+    for (int x = threadIdx.x; x < ntyp * ntyp * kPairConsts; x += blockDim.x)
+        tab[(x / kPairConsts) * kTfTabStride + x % kPairConsts] = P.tab[x];
     for (int q = threadIdx.x; q < NQ; q += blockDim.x) {
         const int gi = SI * NQ + q, gj = SJ * NQ + q;
         const bool vi = gi < np, vj = gj < np;
         ipos[q] = vi ? P.spos[3 * gi] : 0.0;
         ipos[NQ + q] = vi ? P.spos[3 * gi + 1] : 0.0;
         ipos[2 * NQ + q] = vi ? P.spos[3 * gi + 2] : 0.0;
-        ipos[3 * NQ + q] = vi ? (double)P.stype[gi] : -1.0;
+        ipos[3 * NQ + q] = type_bits(vi ? P.stype[gi] : -1);
         jpos[q] = vj ? P.spos[3 * gj] : 0.0;
         jpos[NQ + q] = vj ? P.spos[3 * gj + 1] : 0.0;
         jpos[2 * NQ + q] = vj ? P.spos[3 * gj + 2] : 0.0;
-        jpos[3 * NQ + q] = vj ? (double)P.stype[gj] : -1.0;
+        jpos[3 * NQ + q] = type_bits(vj ? P.stype[gj] : -1);
     }
     for (int x = threadIdx.x; x < kTfSb * kTfSb * 32 * 3; x += blockDim.x) fjw[x] = 0.0;
     __syncthreads();
@@ -161,7 +203,7 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
     if (I < nblk) {
         const int me = w * 32 + lane;
         const double xi = ipos[me], yi = ipos[NQ + me], zi = ipos[2 * NQ + me];
-        const int ti = (int)ipos[3 * NQ + me];  // -1: no ion in this lane
+        const int ti = type_of(ipos[3 * NQ + me]);  // -1: no ion in this lane
         const double* bI = P.tf_box + 6 * I;
         for (int t = 0; t < kTfSb; t++) {
             const int d = (t - w) & (kTfSb - 1);
@@ -190,7 +232,7 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
                     const int jj = (lane + s) & 31;
                     double ax, ay, az, vm;
                     const bool in = pair_eval<POT>(tab, ntyp, L, invL, rc2, xi, yi, zi, ti, jx[jj], jy[jj], jz[jj],
-                                                   (int)jt[jj], ax, ay, az, vm);
+                                                   type_of(jt[jj]), ax, ay, az, vm);
                     if (in && !(s == 16 && lane >= 16)) {
                         fx += ax;
                         fy += ay;
@@ -210,10 +252,13 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
             for (int s = 0; s < 16; s++) {
                 const int ja = (lane + s) & 31, jb = (lane + s + 16) & 31;
                 double ax, ay, az, va, bx, by, bz, vb;
-                const bool ina = pair_eval<POT>(tab, ntyp, L, invL, rc2, xi, yi, zi, ti, jx[ja], jy[ja], jz[ja],
-                                                (int)jt[ja], ax, ay, az, va);
-                const bool inb = pair_eval<POT>(tab, ntyp, L, invL, rc2, xi, yi, zi, ti, jx[jb], jy[jb], jz[jb],
-                                                (int)jt[jb], bx, by, bz, vb);
+                const int tja = type_of(jt[ja]), tjb = type_of(jt[jb]);
+                const PairSep pa = pair_sep(L, invL, rc2, xi, yi, zi, ti, jx[ja], jy[ja], jz[ja], tja);
+                const PairSep pb = pair_sep(L, invL, rc2, xi, yi, zi, ti, jx[jb], jy[jb], jz[jb], tjb);
+                if (!__any_sync(0xffffffffu, pa.in || pb.in)) continue;  // no pair of this step inside r_cut
+                pair_force<POT>(tab, ntyp, rc2, ti, tja, pa, ax, ay, az, va);
+                pair_force<POT>(tab, ntyp, rc2, ti, tjb, pb, bx, by, bz, vb);
+                const bool ina = pa.in, inb = pb.in;
                 if (ina) {
                     fx += ax;
                     fy += ay;
