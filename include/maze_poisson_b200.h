@@ -62,6 +62,13 @@ void mzb_get_pb_grids(double *ex, double *ey, double *ez, double *k2);
 void mzb_set_precision(int mode, double tol_override);
 int mzb_get_precision(void);      /* precision in effect for the current grid */
 
+/* coarse-level plan of the current grid's multigrid forms (precision 1 and 2): 0 = levels
+   down to the first of at most 16 points per side, solved by its Green's function; 1 or 2 =
+   the first level from level 1 or 2 on with 32, 64 or 128 points per side is solved by FFT;
+   -1 = default (1). Returns -1 for an unknown plan. No counterpart in the reference. */
+int mzb_set_mixed_plan(int plan);
+int mzb_get_mixed_plan(void);     /* the level solved by FFT (1, 2) or 0 when none is */
+
 /* state accessors of the current system */
 void mzb_get_cic_neighbors(int64_t *out);  /* (n_p,8,3) CIC corners, particles.c:297-346 */
 void mzb_set_cell_grid(int nc);            /* linked cells per side for the pair forces */
@@ -114,9 +121,14 @@ int mzb_batch_step(const int *handles, int nsys, int n_steps);
 int mzb_batch_classes(const int *handles, const int *cls, int nsys, const int *class_ctas,
                       const int *class_steps, int nclass);
 
-/* Time candidate team partitions of the batched field solve on the listed systems and keep
-   the fastest, and time their pair forces; out[0..3] = {partition exponent, pair-force
-   CTAs, solve ms, forces ms}. Leaves the systems' state unchanged. */
+/* Tune the batched field solve on the listed systems, timing batched solves of every
+   system's current charges from its previous field (an MD-step update): per size class
+   (systems of one grid size) alone, each distinct coarse-level plan (mzb_set_mixed_plan),
+   keeping the fastest and its time per grid point; then, on the whole set, team partitions
+   with CTAs per system ~ grid points^alpha x that class time per point (alpha in {1.2, 1.0,
+   0.8, 0.6, 0.4}), keeping the fastest; and the pair forces. out[0..3] = {partition
+   exponent, pair-force CTAs, solve ms, forces ms}. Leaves the systems' state unchanged
+   except for the plans and shares chosen. */
 int mzb_batch_autotune(const int *handles, int nsys, double *out);
 
 /* Device bytes one FP32+refine system with an n^3 grid and n_p ions holds (admission

@@ -102,6 +102,9 @@ struct GridState {
     bool coarse_team = false; // the coarsest level (n <= kMixedTeamDirectN) is solved by the whole team
     bool coarse_fft = false;  // the coarsest level (mixed_fft_coarse_ok) is solved by the team by FFT
     void* lev_spec = nullptr; // its half spectrum
+    int plan = -1;            // first level that may be solved by FFT (mzb_set_mixed_plan; -1: default)
+    double batch_cost = 1.0;  // batched-solve time per grid point relative to other sizes (mzb_batch_autotune)
+    int lev_plan = -1;        // the plan the current levels were built for
     double* bj_inv = nullptr;  // block-Jacobi block inverse (1000 x 1000) on BLOCKJACOBI grids
     // Poisson-Boltzmann (solver_initialize_grid_pois_boltz, grid_general.c:84-100)
     bool pb = false;
@@ -226,17 +229,19 @@ int mixed_fft_level() {
 
 void ensure_mixed_levels(GridState& G) {
     const int fp64 = G.precision == 2 ? 1 : 0;
-    if (G.nlev && G.lev_fp64 != fp64) free_mixed_levels(G);  // the form changed: levels of the other type
+    const int lf = G.plan >= 0 ? (G.plan == 0 ? kMixedMaxLevels : G.plan) : mixed_fft_level();
+    if (G.nlev && (G.lev_fp64 != fp64 || G.lev_plan != lf)) free_mixed_levels(G);  // another form or plan
     if (G.nlev) return;
     G.lev_fp64 = fp64;
+    G.lev_plan = lf;
     const size_t w = fp64 ? sizeof(double) : sizeof(float);
     G.nlev = mixed_levels(G.n, G.lev_n);
     G.coarse_team = false;
     G.coarse_fft = false;
-    // Stop at the first level the team solves exactly: by FFT when one of n/2, n/4, ... has
-    // an FFT size (from level mixed_fft_level(), 1 unless MZB_MIXED_COARSE=fft2 / levels),
-    // else by the Green's function at <= kMixedTeamDirectN points per side.
-    const int lf = mixed_fft_level();
+    // Stop at the first level the team solves exactly: by FFT when one of the levels from lf
+    // on has an FFT size (lf: the grid's plan, else mixed_fft_level(), 1 unless
+    // MZB_MIXED_COARSE=fft2 / levels), else by the Green's function at <= kMixedTeamDirectN
+    // points per side.
     for (int l = lf; l < G.nlev; l++)
         if (mixed_fft_coarse_ok(G.lev_n[l])) {
             G.nlev = l + 1;
@@ -1610,6 +1615,27 @@ int mzb_get_precision(void) {
     return (G.precision >= 1 && mixed_supported(G)) ? G.precision : 0;
 }
 
+// Coarse-level plan of the current grid's multigrid forms (precision 1 and 2): 0 = the
+// levels go down to the first one of at most 16 points per side, solved by its Green's
+// function; 1 or 2 = the first level from level 1 or 2 on with 32, 64 or 128 points per side
+// is the coarse level, solved by FFT; -1 = the default (1). mzb_batch_autotune sets it per
+// size class. Returns -1 for an unknown plan.
+int mzb_set_mixed_plan(int plan) {
+    if (plan < -1 || plan > 2) return -1;
+    GridState& G = grid();
+    touch(sys());
+    G.plan = plan;
+    return 0;
+}
+// The level the current grid's multigrid forms solve by FFT (1, 2), or 0 when the coarsest
+// level is solved by its Green's function (or the grid has no multigrid form).
+int mzb_get_mixed_plan(void) {
+    GridState& G = grid();
+    if (!(G.precision >= 1 && mixed_supported(G))) return 0;
+    ensure_mixed_levels(G);
+    return G.coarse_fft ? G.nlev - 1 : 0;
+}
+
 // The CUDA stream all work of the current system is queued on (for callers that time
 // it with their own events or order their own kernels against it).
 void* mzb_get_stream(void) { return (void*)sys().stream; }
@@ -1788,13 +1814,14 @@ void batch_prepare(System& s) {
 }
 
 // Team partition of nblocks CTAs: at least one per system, the rest in proportion to
-// (grid points)^alpha by largest remainder.
+// (grid points)^alpha times the system's cost factor (1 without the tuner's factors) by
+// largest remainder.
 std::vector<int> team_starts(const std::vector<System*>& ss, int nblocks, double alpha) {
     const int n = (int)ss.size();
     std::vector<double> w(n);
     double tot = 0.0;
     for (int r = 0; r < n; r++) {
-        w[r] = pow((double)ss[r]->G.m, alpha);
+        w[r] = pow((double)ss[r]->G.m, alpha) * ss[r]->G.batch_cost;
         tot += w[r];
     }
     const int rem = nblocks - n;
@@ -2205,19 +2232,10 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
     Batch& B = g_batchst;
     cudaStream_t st = B.streams[0];
     const int nblocks = mixed_grid_blocks();
-    std::vector<MixedArgs> list(nsys);
-    size_t smem = 0;
-    for (int r = 0; r < nsys; r++) {
-        double cst = 0.0;
-        const int prog = mixed_update_prog(ss[r]->G, cst);
-        list[r] = mixed_args(*ss[r], prog, cst);
-        smem = std::max(smem, mixed_smem_bytes(list[r]));
-    }
     MixedArgs* list_d = nullptr;
     int* start_d = nullptr;
     MZB_CHECK(cudaMalloc(&list_d, sizeof(MixedArgs) * nsys));
     MZB_CHECK(cudaMalloc(&start_d, sizeof(int) * (nsys + 1)));
-    upload(list_d, list.data(), sizeof(MixedArgs) * nsys);
     std::vector<double*> ysave(nsys, nullptr);
     MZB_CHECK(cudaDeviceSynchronize());  // the systems' streams have written y
     for (int r = 0; r < nsys; r++) {
@@ -2233,35 +2251,110 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
                 MZB_CHECK(cudaMemcpyAsync(ss[r]->G.y, ysave[r], sizeof(double) * ss[r]->G.m, cudaMemcpyDeviceToDevice,
                                           st));
     };
-    const double alphas[] = {1.0, 0.8, 0.6, 0.4};
-    double best_alpha = B.alpha, best_solve = 1e30;
-    for (double alpha : alphas) {
-        const std::vector<int> start = team_starts(ss, nblocks, alpha);
-        upload(start_d, start.data(), sizeof(int) * (nsys + 1));
+    // One batched solve of every system's current charges from its previous field (the
+    // work of an MD-step update; the solves write only the spare field buffer, the
+    // multigrid levels and, restored here, the MaZe unknown), under the team partition of
+    // exponent alpha; the mean of two timed launches after one untimed.
+    auto time_set = [&](const std::vector<System*>& set, double alpha) {
+        const int ns = (int)set.size();
+        std::vector<MixedArgs> list(ns);
+        size_t smem = 0;
+        for (int r = 0; r < ns; r++) {
+            double cst = 0.0;
+            const int prog = mixed_update_prog(set[r]->G, cst);
+            list[r] = mixed_args(*set[r], prog, cst);
+            list[r].phi_old = set[r]->G.phi_prev();
+            smem = std::max(smem, mixed_smem_bytes(list[r]));
+        }
+        upload(list_d, list.data(), sizeof(MixedArgs) * ns);
+        const std::vector<int> start = team_starts(set, nblocks, alpha);
+        upload(start_d, start.data(), sizeof(int) * (ns + 1));
         float tot = 0.f;
         for (int rep = 0; rep < 3; rep++) {
             restore_y();
-            for (int r = 0; r < nsys; r++) MZB_CHECK(cudaMemsetAsync(ss[r]->bar, 0, sizeof(GridBarrier), st));
+            for (int r = 0; r < ns; r++) MZB_CHECK(cudaMemsetAsync(set[r]->bar, 0, sizeof(GridBarrier), st));
             MZB_CHECK(cudaEventRecord(B.t0, st));
-            mixed_batch_launch(list_d, start_d, nsys, nblocks, smem, st);
+            mixed_batch_launch(list_d, start_d, ns, nblocks, smem, st);
             MZB_CHECK(cudaEventRecord(B.t1, st));
             MZB_CHECK(cudaStreamSynchronize(st));
             float ms = 0.f;
             MZB_CHECK(cudaEventElapsedTime(&ms, B.t0, B.t1));
             if (rep > 0) tot += ms;
         }
-        if (tot / 2 < best_solve) {
-            best_solve = tot / 2;
-            best_alpha = alpha;
+        return (double)tot / 2;
+    };
+    auto time_solves = [&](double alpha) { return time_set(ss, alpha); };
+    // team partition: CTAs per system ~ (grid points)^alpha
+    const double alphas[] = {1.2, 1.0, 0.8, 0.6, 0.4};
+    auto tune_alpha = [&](double& best_solve) {
+        double best_alpha = B.alpha;
+        best_solve = 1e30;
+        for (double alpha : alphas) {
+            const double ms = time_solves(alpha);
+            if (ms < best_solve) {
+                best_solve = ms;
+                best_alpha = alpha;
+            }
         }
+        return best_alpha;
+    };
+    // Per size class (systems of one grid size), timed alone on all CTAs: the coarse-level
+    // plan (each distinct one of mzb_set_mixed_plan; the FFT-solved coarse level pays off
+    // with many CTAs per team, the levels down to 16^3 with few) and the time per grid
+    // point of the fastest. The classes' shares of the mix are then weighted by that time
+    // (the small grids' passes are latency-bound), so that the teams finish together, and
+    // the exponent of the partition is tuned on the whole set.
+    std::vector<int> sizes;
+    for (System* s : ss)
+        if (std::find(sizes.begin(), sizes.end(), s->G.n) == sizes.end()) sizes.push_back(s->G.n);
+    std::vector<double> per_point(sizes.size(), 1.0);
+    for (System* s : ss) s->G.batch_cost = 1.0;
+    for (size_t c = 0; c < sizes.size(); c++) {
+        std::vector<System*> cls;
+        double pts = 0.0;
+        for (System* s : ss)
+            if (s->G.n == sizes[c]) {
+                cls.push_back(s);
+                pts += (double)s->G.m;
+            }
+        int best_plan = cls[0]->G.plan;
+        double best_ms = 1e30;
+        std::vector<std::pair<int, int>> seen;  // (levels, FFT coarse) of the plans timed
+        for (int plan : {1, 2, 0}) {
+            for (System* s : cls) {
+                s->G.plan = plan;
+                touch(*s);
+                ensure_mixed_levels(s->G);
+            }
+            const std::pair<int, int> shape{cls[0]->G.nlev, cls[0]->G.coarse_fft ? 1 : 0};
+            if (std::find(seen.begin(), seen.end(), shape) != seen.end()) continue;
+            seen.push_back(shape);
+            const double ms = time_set(cls, 1.0);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best_plan = plan;
+            }
+        }
+        for (System* s : cls) {
+            s->G.plan = best_plan;
+            touch(*s);
+            ensure_mixed_levels(s->G);
+        }
+        per_point[c] = best_ms / pts;
     }
+    double ref = per_point[0];
+    for (double v : per_point) ref = std::min(ref, v);
+    for (System* s : ss)
+        for (size_t c = 0; c < sizes.size(); c++)
+            if (s->G.n == sizes[c]) s->G.batch_cost = per_point[c] / ref;
+    double best_solve = 0.0;
+    B.alpha = tune_alpha(best_solve);
     restore_y();
     MZB_CHECK(cudaStreamSynchronize(st));
     for (double* p : ysave)
         if (p) cudaFree(p);
     cudaFree(list_d);
     cudaFree(start_d);
-    B.alpha = best_alpha;
 
     // pair forces of all systems together (their work division is fixed by N; timed only)
     double best_forces = 0.0;
@@ -2290,7 +2383,7 @@ int mzb_batch_autotune(const int* handles, int nsys, double* out) {
     for (System* s : ss) touch(*s);
     batch_clear_graphs();
     if (out) {
-        out[0] = best_alpha;
+        out[0] = B.alpha;
         out[1] = (double)force_ctas;
         out[2] = best_solve;
         out[3] = best_forces;

@@ -71,6 +71,11 @@ struct Team {
 // counter's release sequence, and the exit __syncthreads extends that to the whole CTA.
 __device__ __forceinline__ bool team_sync(const Team& t, unsigned int& epoch) {
     __shared__ int ok_sh;
+    if (t.nblk == 1) {  // a team of one CTA: the block barrier orders its global writes too
+        __syncthreads();
+        epoch++;
+        return true;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
@@ -719,17 +724,118 @@ __device__ void split_prolong_black_vec(const Team& tm, int n, const S* xc, S* x
     });
 }
 
-// dispatch: rows of 128 floats (n = 256) as float4, of 64 (n = 128) as float2
+// Rows shorter than a warp's 32 V values (h = n/2 per colour, h % V == 0, h / V <= 32): a
+// warp takes R = 32 / (h / V) consecutive rows at once, h / V lanes per row (the other
+// lanes idle), each lane V values of its row. The in-row neighbours across a lane's ends
+// come from the adjacent lanes of the same row, wrapping inside the row as the periodic
+// row does. Same sums, in the same order, as the scalar and one-row versions.
+struct RowLanes {
+    int L, R, sub, q;  // lanes per row, rows per warp, this lane's row slot and chunk in it
+    int lp, ln;        // lanes holding the previous and the next chunk of this lane's row
+};
+template <int V>
+__device__ __forceinline__ RowLanes row_lanes(int h) {
+    RowLanes t;
+    const int lane = threadIdx.x & 31;
+    t.L = h / V;
+    t.R = 32 / t.L;
+    t.sub = lane / t.L;
+    t.q = lane - t.sub * t.L;
+    t.lp = t.q == 0 ? lane + t.L - 1 : lane - 1;
+    t.ln = t.q == t.L - 1 ? lane - (t.L - 1) : lane + 1;
+    return t;
+}
+// warp per R rows of an n x n set of rows: f(i, j, active) for the lane's row (a clamped
+// row of the warp's first when the lane idles, so that every lane takes the shuffles)
+template <class F>
+__device__ __forceinline__ void grid_row_groups(const Team& tm, int n, const RowLanes& t, F&& f) {
+    const int gw = tm.b * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int nw = tm.nblk * (blockDim.x >> 5);
+    const int rows = n * n;
+    for (int r0 = gw * t.R; r0 < rows; r0 += nw * t.R) {
+        const int row = r0 + t.sub;
+        const bool act = t.sub < t.R && row < rows;
+        const int rr = act ? row : r0;
+        const int i = rr / n;
+        f(i, rr - i * n, act);
+    }
+}
+template <int V, class S>
+__device__ __forceinline__ void rows_nb_sums(const S* xo, const Rows& o, int s, int kk0, const RowLanes& t,
+                                             S (&sum)[V]) {
+    S a0[V], a1[V], a2[V], a3[V], cen[V];
+    ldv<V>(xo + o.im + kk0, a0);
+    ldv<V>(xo + o.ip + kk0, a1);
+    ldv<V>(xo + o.jm + kk0, a2);
+    ldv<V>(xo + o.jp + kk0, a3);
+    ldv<V>(xo + o.c + kk0, cen);
+    const S prev = __shfl_sync(0xffffffffu, cen[V - 1], t.lp);
+    const S next = __shfl_sync(0xffffffffu, cen[0], t.ln);
+#pragma unroll
+    for (int e = 0; e < V; e++) {
+        const S side = s == 0 ? (e == 0 ? prev : cen[e - 1]) : (e == V - 1 ? next : cen[e + 1]);
+        S u = ((a0[e] + a1[e]) + a2[e]) + a3[e];
+        sum[e] = (u + cen[e]) + side;
+    }
+}
+template <int V, class S>
+__device__ void split_gs_rows(const Team& tm, int n, int c, const S* b, S* x, double* acc) {
+    const int h = n >> 1, hp = h * n * n;
+    const RowLanes t = row_lanes<V>(h);
+    const S* xo = x + (1 - c) * hp;
+    S* xc = x + c * hp;
+    const S* bc = b + c * hp;
+    const int kk0 = t.q * V;
+    double s_acc = 0.0;
+    grid_row_groups(tm, n, t, [&](int i, int j, bool act) {
+        const Rows o = rows_of(n, i, j);
+        S bv[V], sum[V], v[V];
+        ldv<V>(bc + o.c + kk0, bv);
+        rows_nb_sums<V>(xo, o, (i + j + c) & 1, kk0, t, sum);
+#pragma unroll
+        for (int e = 0; e < V; e++) v[e] = (bv[e] - sum[e]) * neg_sixth<S>();
+        if (act) {
+            stv<V>(xc + o.c + kk0, v);
+#pragma unroll
+            for (int e = 0; e < V; e++) s_acc += (double)v[e];
+        }
+    });
+    if (acc != nullptr) *acc += s_acc;
+}
+template <int V, class S>
+__device__ void split_resid_red_rows(const Team& tm, int n, const S* b, const S* x, S* r) {
+    const int h = n >> 1, hp = h * n * n;
+    const RowLanes t = row_lanes<V>(h);
+    const S* x1 = x + hp;
+    const int kk0 = t.q * V;
+    grid_row_groups(tm, n, t, [&](int i, int j, bool act) {
+        const Rows o = rows_of(n, i, j);
+        S bv[V], xv[V], sum[V], v[V];
+        ldv<V>(b + o.c + kk0, bv);
+        ldv<V>(x + o.c + kk0, xv);
+        rows_nb_sums<V>(x1, o, (i + j) & 1, kk0, t, sum);
+#pragma unroll
+        for (int e = 0; e < V; e++) v[e] = bv[e] - (sum[e] - S(6) * xv[e]);
+        if (act) stv<V>(r + o.c + kk0, v);
+    });
+}
+
+// dispatch: rows of 128 floats (n = 256) as float4 and of 64 (n = 128) as float2, one row
+// per warp; shorter rows several per warp (n % 8 == 0 as float4, n % 4 == 0 as float2)
 template <class S>
 __device__ __forceinline__ void split_gs(const Team& tm, int n, int c, const S* b, S* x, double* acc) {
     if (n == 256) split_gs_vec<4>(tm, n, c, b, x, acc);
     else if (n == 128) split_gs_vec<2>(tm, n, c, b, x, acc);
+    else if (n < 256 && n % 8 == 0) split_gs_rows<4>(tm, n, c, b, x, acc);
+    else if (n < 128 && n % 4 == 0) split_gs_rows<2>(tm, n, c, b, x, acc);
     else split_gs_scalar(tm, n, c, b, x, acc);
 }
 template <class S>
 __device__ __forceinline__ void split_resid_red(const Team& tm, int n, const S* b, const S* x, S* r) {
     if (n == 256) split_resid_red_vec<4>(tm, n, b, x, r);
     else if (n == 128) split_resid_red_vec<2>(tm, n, b, x, r);
+    else if (n < 256 && n % 8 == 0) split_resid_red_rows<4>(tm, n, b, x, r);
+    else if (n < 128 && n % 4 == 0) split_resid_red_rows<2>(tm, n, b, x, r);
     else split_resid_red_scalar(tm, n, b, x, r);
 }
 template <class S>

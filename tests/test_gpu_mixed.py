@@ -29,8 +29,9 @@ def orc(oracle_path):
 
 
 class MixedRun(MDRun):
-    def __init__(self, *args, precision=1, **kw):
+    def __init__(self, *args, precision=1, plan=-1, **kw):
         super().__init__(*args, precision=precision, **kw)
+        self.plan = plan
 
     def initialize(self):
         c = self.capi
@@ -41,6 +42,7 @@ class MixedRun(MDRun):
                                  maps["method"][self.method], maps["precond"][self.precond])
         c.mzb_set_precision(self.precision, 0.0)
         assert c.mzb_get_precision() == self.precision
+        assert c.mzb_set_mixed_plan(self.plan) == 0
         c.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, maps["potential"]["TF"],
                                       maps["cas"]["CIC"], s.types, s.pos, s.vel, s.mass, s.charges,
                                       s.pot_params)
@@ -56,14 +58,18 @@ class MixedRun(MDRun):
         c.integrator_part_2()
 
 
+@pytest.mark.parametrize("plan", [1, 0])
 @pytest.mark.parametrize("precision", [1, 2])
 @pytest.mark.parametrize("method", ["LCG", "MAZE-LCG", "MULTIGRID", "MAZE-MULTIGRID"])
-def test_mixed_matches_fp64_oracle(prod, orc, method, precision):
+def test_mixed_matches_fp64_oracle(prod, orc, method, precision, plan):
+    """Coarse-level plan 1: the 32^3 coarse level solved by FFT; plan 0: levels down to 16^3,
+    solved by the Green's function."""
     system = make_system(5, 64, seed=21)
-    a = MixedRun(prod, system.copy(), method=method, tol=1e-10, precision=precision)
+    a = MixedRun(prod, system.copy(), method=method, tol=1e-10, precision=precision, plan=plan)
     b = MDRun(orc, system.copy(), method=method, tol=1e-10)
     a.initialize()
     b.initialize()
+    assert prod.mzb_get_mixed_plan() == plan
     try:
         for step in range(3):
             sa, sb = a.state(), b.state()
@@ -80,12 +86,15 @@ def test_mixed_matches_fp64_oracle(prod, orc, method, precision):
         b.finalize()
 
 
+@pytest.mark.parametrize("plan", [1, 2, 0])
 @pytest.mark.parametrize("precision", [1, 2])
-def test_mixed_solution_residual_meets_tol(prod, oracle_lib, precision):
-    """The returned field satisfies |L phi - b|_inf <= tol in FP64."""
+def test_mixed_solution_residual_meets_tol(prod, oracle_lib, precision, plan):
+    """The returned field satisfies |L phi - b|_inf <= tol in FP64, with the 64^3 or the
+    32^3 level solved by FFT, or the levels down to 16^3."""
     system = make_system(10, 128, density=1.329, seed=5)
-    run = MixedRun(prod, system, method="LCG", tol=1e-9, precision=precision)
+    run = MixedRun(prod, system, method="LCG", tol=1e-9, precision=precision, plan=plan)
     run.initialize()
+    assert prod.mzb_get_mixed_plan() == plan
     try:
         run.step()
         st = run.state()
