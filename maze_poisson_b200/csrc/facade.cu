@@ -1723,6 +1723,7 @@ struct BatchGraph {
     cudaGraphExec_t exec = nullptr;
     MixedArgs* list_d = nullptr;
     int* start_d = nullptr;
+    StageTable stages;  // replica table of the particle stages (nsys 0: per-system branches)
     unsigned long long launches = 0;
     unsigned long long used = 0;  // call counter of the last use (least recently used goes first)
 };
@@ -1738,11 +1739,15 @@ struct Batch {
     double alpha = 1.0;  // team size ~ (grid points)^alpha (autotuned)
 };
 Batch g_batchst;
+// MZB_BATCH_BRANCHES=1 (a comparison aid): the particle stages as one graph branch per
+// system instead of replica tables
+const bool g_batch_branches = getenv("MZB_BATCH_BRANCHES") != nullptr && strcmp(getenv("MZB_BATCH_BRANCHES"), "0") != 0;
 
 void release_graph(BatchGraph& bg) {
     if (bg.exec) cudaGraphExecDestroy(bg.exec);
     dev_free(bg.list_d);
     dev_free(bg.start_d);
+    if (bg.stages.nsys) stage_table_free(bg.stages);
     bg = BatchGraph{};
 }
 
@@ -1842,6 +1847,25 @@ std::vector<int> team_starts(const std::vector<System*>& ss, int nblocks, double
     std::vector<int> start(n + 1, 0);
     for (int r = 0; r < n; r++) start[r + 1] = start[r] + cnt[r];
     return start;
+}
+
+// The particle stages' arguments of system s in a batched step (replica tables).
+StageArgs stage_args(System& s) {
+    StageArgs a;
+    a.P = s.P;
+    a.I = s.I;
+    a.q = s.G.q;
+    a.qmask = s.G.qmask;
+    a.n = s.G.n;
+    a.h = s.G.h;
+    a.mask_words = s.G.qmask != nullptr ? (int)(((size_t)s.G.n * s.G.n * (s.G.n >> 6) + 31) / 32) : 0;
+    a.q_sparse = s.P.cas == CAS_CIC && s.P.q_sparse == s.G.q ? 1 : 0;
+    a.phi = s.G.buf[s.G.ispare];  // the field the solve writes
+    a.qtot = s.qtot_d;
+    a.err = s.err_d;
+    a.result = s.result;
+    a.bar = s.bar;
+    return a;
 }
 
 void stage_particles_before_solve(System& s) {
@@ -1995,24 +2019,41 @@ BatchGraph& batch_graph(const std::vector<int>& handles, const std::vector<Syste
     upload(bg.list_d, list.data(), sizeof(MixedArgs) * nsys);
     upload(bg.start_d, start.data(), sizeof(int) * (nsys + 1));
 
+    // CIC systems take the particle stages as replica tables: one launch per stage for
+    // all of them; otherwise each system's stages run as a branch of the graph
+    std::vector<StageArgs> sargs;
+    bool tables = !g_batch_branches;
+    for (int r = 0; r < nsys && tables; r++) {
+        sargs.push_back(stage_args(*ss[r]));
+        tables = stage_table_ok(sargs.back());
+    }
+    if (tables) bg.stages = stage_table_build(sargs);
+
     const unsigned long long l0 = g_kernel_launches;
     cudaGraph_t graph = nullptr;
     MZB_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    MZB_CHECK(cudaEventRecord(B.fork1, stream));
-    for (int r = 0; r < nsys; r++) {
-        MZB_CHECK(cudaStreamWaitEvent(ss[r]->stream, B.fork1, 0));
-        stage_particles_before_solve(*ss[r]);
-        MZB_CHECK(cudaEventRecord(B.join1[first + r], ss[r]->stream));
-        MZB_CHECK(cudaStreamWaitEvent(stream, B.join1[first + r], 0));
-    }
-    for (int r = 0; r < nsys; r++) MZB_CHECK(cudaMemsetAsync(ss[r]->bar, 0, sizeof(GridBarrier), stream));
-    mixed_batch_launch(bg.list_d, bg.start_d, nsys, nblocks, smem, stream);
-    MZB_CHECK(cudaEventRecord(B.fork2, stream));
-    for (int r = 0; r < nsys; r++) {
-        MZB_CHECK(cudaStreamWaitEvent(ss[r]->stream, B.fork2, 0));
-        stage_particles_after_solve(*ss[r]);
-        MZB_CHECK(cudaEventRecord(B.join2[first + r], ss[r]->stream));
-        MZB_CHECK(cudaStreamWaitEvent(stream, B.join2[first + r], 0));
+    if (tables) {
+        stages_before_solve(bg.stages, stream);  // also zeroes the solve's barriers
+        mixed_batch_launch(bg.list_d, bg.start_d, nsys, nblocks, smem, stream);
+        stages_after_solve(bg.stages, stream);
+        for (System* sp : ss) sp->P.q_sparse = sp->G.q;  // as spread_charges leaves it
+    } else {
+        MZB_CHECK(cudaEventRecord(B.fork1, stream));
+        for (int r = 0; r < nsys; r++) {
+            MZB_CHECK(cudaStreamWaitEvent(ss[r]->stream, B.fork1, 0));
+            stage_particles_before_solve(*ss[r]);
+            MZB_CHECK(cudaEventRecord(B.join1[first + r], ss[r]->stream));
+            MZB_CHECK(cudaStreamWaitEvent(stream, B.join1[first + r], 0));
+        }
+        for (int r = 0; r < nsys; r++) MZB_CHECK(cudaMemsetAsync(ss[r]->bar, 0, sizeof(GridBarrier), stream));
+        mixed_batch_launch(bg.list_d, bg.start_d, nsys, nblocks, smem, stream);
+        MZB_CHECK(cudaEventRecord(B.fork2, stream));
+        for (int r = 0; r < nsys; r++) {
+            MZB_CHECK(cudaStreamWaitEvent(ss[r]->stream, B.fork2, 0));
+            stage_particles_after_solve(*ss[r]);
+            MZB_CHECK(cudaEventRecord(B.join2[first + r], ss[r]->stream));
+            MZB_CHECK(cudaStreamWaitEvent(stream, B.join2[first + r], 0));
+        }
     }
     MZB_CHECK(cudaStreamEndCapture(stream, &graph));
     bg.launches = g_kernel_launches - l0;

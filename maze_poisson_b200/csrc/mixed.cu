@@ -1534,9 +1534,10 @@ __device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs&
     return rmax;
 }
 
-// Vectorised residual pass for n % 64 == 0: a warp covers 64 consecutive k of a row with
-// one double2 per lane; k - 1 / k + 1 come from the adjacent lane by a shuffle, from memory
-// at the ends of the 64. Same sums, in the same order, as residual_pass.
+// Vectorised residual pass (n even): a warp covers 64 consecutive k of a row with one
+// double2 per lane (the last chunk of a row shorter when 64 does not divide n, its lanes
+// past the row idle); k - 1 / k + 1 come from the adjacent lane by a shuffle, from memory
+// at the ends of the chunk. Same sums, in the same order, as residual_pass.
 template <int START, bool RHS_Q, class S>
 __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedArgs& a, const double* X,
                                                     const double* Xp, S* e, S* rb) {
@@ -1563,10 +1564,11 @@ __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedA
         const int cA = (i + j) & 1;  // colour of even k in this row
         const int srow = (i * n + j) * h;
         for (int k0 = 0; k0 < n; k0 += 64) {
-            const int k = k0 + 2 * lane;
+            const bool act = k0 + 2 * lane < n;
+            const int k = act ? k0 + 2 * lane : n - 2;  // idle lanes read a valid pair, store nothing
             double r0, r1;
             double2 bq;
-            if (RHS_Q) {  // q is read only in segments the spreading marked (0 * c elsewhere)
+            if (RHS_Q) {  // q is read only in segments the spreading marked (0 * c elsewhere; n % 64 == 0)
                 const int seg = (row >> 6) + (k0 >> 6);
                 double2 qv = make_double2(0.0, 0.0);
                 if (a.qmask == nullptr || ((a.qmask[seg >> 5] >> (seg & 31)) & 1u))
@@ -1585,7 +1587,7 @@ __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedA
                 double km0 = __shfl_sync(0xffffffffu, xc.y, (lane + 31) & 31);
                 double kp1 = __shfl_sync(0xffffffffu, xc.x, (lane + 1) & 31);
                 if (lane == 0) km0 = x1(row + (k0 == 0 ? n - 1 : k0 - 1));
-                if (lane == 31) kp1 = x1(row + (k0 + 64 == n ? 0 : k0 + 64));
+                if (lane == 31 || k + 2 >= n) kp1 = x1(row + (k + 2 >= n ? 0 : k + 2));
                 double s0 = xip.x + xim.x;
                 s0 = s0 + xjp.x;
                 s0 = s0 + xjm.x;
@@ -1599,14 +1601,16 @@ __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedA
                 r0 = bq.x - (s0 - xc.x * 6.0);
                 r1 = bq.y - (s1 - xc.y * 6.0);
             }
-            const S rf0 = (S)r0, rf1 = (S)r1;
-            const int p0 = cA * hp + srow + (k >> 1), p1 = (cA ^ 1) * hp + srow + (k >> 1);
-            rb[p0] = rf0;
-            rb[p1] = rf1;
-            // red e only: the first half-sweep (black) writes the black values without reading them
-            if (cA == 0) e[p0] = rf0 * neg_sixth<S>();
-            else e[p1] = rf1 * neg_sixth<S>();
-            rmax = fmax(rmax, fmax(fabs(r0), fabs(r1)));
+            if (act) {
+                const S rf0 = (S)r0, rf1 = (S)r1;
+                const int p0 = cA * hp + srow + (k >> 1), p1 = (cA ^ 1) * hp + srow + (k >> 1);
+                rb[p0] = rf0;
+                rb[p1] = rf1;
+                // red e only: the first half-sweep (black) writes the black values without reading them
+                if (cA == 0) e[p0] = rf0 * neg_sixth<S>();
+                else e[p1] = rf1 * neg_sixth<S>();
+                rmax = fmax(rmax, fmax(fabs(r0), fabs(r1)));
+            }
         }
     });
     return rmax;
@@ -1615,7 +1619,7 @@ __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedA
 template <int START, bool RHS_Q, class S>
 __device__ __forceinline__ double residual_any(const Team& tm, const MixedArgs& a, const double* X,
                                                const double* Xp, S* e, S* rb) {
-    if (a.n % 64 == 0) return residual_pass_vec<START, RHS_Q>(tm, a, X, Xp, e, rb);
+    if (a.n % 2 == 0) return residual_pass_vec<START, RHS_Q>(tm, a, X, Xp, e, rb);
     return residual_pass<START, RHS_Q>(tm, a, X, Xp, e, rb);
 }
 
@@ -1624,13 +1628,14 @@ template <int START, class S>
 __device__ __forceinline__ void update_pass(const Team& tm, const MixedArgs& a, const double* X, double* home,
                                             const S* e, double emean) {
     const int n = a.n;
-    if (n % 64 == 0) {  // double2 per lane, e from both colour halves
+    if (n % 2 == 0) {  // double2 per lane, e from both colour halves (lanes past the row idle)
         const int h = n >> 1, lane = threadIdx.x & 31, hp = h * n * n;
         grid_rows(tm, n, [&](int i, int j) {
             const int row = (i * n + j) * n, srow = (i * n + j) * h;
             const int cA = (i + j) & 1;
             for (int k0 = 0; k0 < n; k0 += 64) {
                 const int k = k0 + 2 * lane;
+                if (k >= n) break;
                 double2 xo = make_double2(0.0, 0.0);
                 if (START != START_ZERO) xo = *reinterpret_cast<const double2*>(X + row + k);
                 if (START == START_EXTRAP) {

@@ -85,10 +85,7 @@ __device__ __forceinline__ double warp_ordered_sum(const double* part, int n) {
 // whole), so every load is issued before the one block-wide scan of the chunk totals.
 // Optionally sums `part[0..np_part)` in index order into *sum_out.
 // ------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_scan(const int32_t* __restrict__ count, int m,
-                                               int32_t* __restrict__ start, int32_t* __restrict__ fill,
-                                               const double* __restrict__ part, int np_part,
-                                               double* __restrict__ sum_out) {
+__device__ __forceinline__ void k_scan_body(const int32_t* __restrict__ count, int m, int32_t* __restrict__ start, int32_t* __restrict__ fill, const double* __restrict__ part, int np_part, double* __restrict__ sum_out, int bx) {
     __shared__ int32_t wsum[32];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
     const int C = (((m + (int)blockDim.x - 1) / (int)blockDim.x) + 3) & ~3;
@@ -142,14 +139,17 @@ __global__ void __launch_bounds__(1024) k_scan(const int32_t* __restrict__ count
         if (lane == 0) *sum_out = s;
     }
 }
+__global__ void __launch_bounds__(1024) k_scan(const int32_t* __restrict__ count, int m,
+                                               int32_t* __restrict__ start, int32_t* __restrict__ fill,
+                                               const double* __restrict__ part, int np_part,
+                                               double* __restrict__ sum_out) { k_scan_body(count, m, start, fill, part, np_part, sum_out, blockIdx.x); }
 
 // The same scan over many blocks (large m): k_scan_reduce sums the counts of each block
 // of 1024, k_scan_apply scans each block from the sum of the blocks before it (read in
 // block order), coalesced, one count per thread.
-__global__ void __launch_bounds__(1024) k_scan_reduce(const int32_t* __restrict__ count, int m,
-                                                      int32_t* __restrict__ blk) {
+__device__ __forceinline__ void k_scan_reduce_body(const int32_t* __restrict__ count, int m, int32_t* __restrict__ blk, int bx) {
     __shared__ int32_t wsum[32];
-    const int x = blockIdx.x * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int x = bx * 1024 + threadIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int32_t v = x < m ? count[x] : 0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -159,21 +159,20 @@ __global__ void __launch_bounds__(1024) k_scan_reduce(const int32_t* __restrict_
         int32_t y = wsum[lane];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
-        if (lane == 0) blk[blockIdx.x] = y;
+        if (lane == 0) blk[bx] = y;
     }
 }
+__global__ void __launch_bounds__(1024) k_scan_reduce(const int32_t* __restrict__ count, int m,
+                                                      int32_t* __restrict__ blk) { k_scan_reduce_body(count, m, blk, blockIdx.x); }
 
-__global__ void __launch_bounds__(1024) k_scan_apply(const int32_t* __restrict__ count, int m,
-                                                     const int32_t* __restrict__ blk, int32_t* __restrict__ start,
-                                                     int32_t* __restrict__ fill, const double* __restrict__ part,
-                                                     int np_part, double* __restrict__ sum_out) {
+__device__ __forceinline__ void k_scan_apply_body(const int32_t* __restrict__ count, int m, const int32_t* __restrict__ blk, int32_t* __restrict__ start, int32_t* __restrict__ fill, const double* __restrict__ part, int np_part, double* __restrict__ sum_out, int bx) {
     __shared__ int32_t wsum[32];
     __shared__ int32_t base_s;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    const int x = blockIdx.x * 1024 + t;
+    const int x = bx * 1024 + t;
     if (w == 0) {
         int32_t b = 0;
-        for (int u = lane; u < (int)blockIdx.x; u += 32) b += blk[u];
+        for (int u = lane; u < (int)bx; u += 32) b += blk[u];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
         if (lane == 0) base_s = b;
@@ -203,12 +202,16 @@ __global__ void __launch_bounds__(1024) k_scan_apply(const int32_t* __restrict__
         fill[x] = excl;
     }
     if (x == m - 1) start[m] = excl + v;
-    if (m == 0 && blockIdx.x == 0 && t == 0) start[0] = 0;
-    if (sum_out != nullptr && blockIdx.x == 0 && w == 0) {
+    if (m == 0 && bx == 0 && t == 0) start[0] = 0;
+    if (sum_out != nullptr && bx == 0 && w == 0) {
         const double s = warp_ordered_sum(part, np_part);
         if (lane == 0) *sum_out = s;
     }
 }
+__global__ void __launch_bounds__(1024) k_scan_apply(const int32_t* __restrict__ count, int m,
+                                                     const int32_t* __restrict__ blk, int32_t* __restrict__ start,
+                                                     int32_t* __restrict__ fill, const double* __restrict__ part,
+                                                     int np_part, double* __restrict__ sum_out) { k_scan_apply_body(count, m, blk, start, fill, part, np_part, sum_out, blockIdx.x); }
 
 // Exclusive scan of count[0..m) into start (and fill): one block for small m, else the
 // two-kernel form with per-block totals in blk ([ceil(m / 1024)]).
@@ -234,8 +237,8 @@ void scan_counts(const int32_t* count, int m, int32_t* start, int32_t* fill, int
 // whose only nonzeros are the corners of the bases being replaced) the ion first zeroes
 // the 8 corners of its old base cell.
 template <int CAS>
-__global__ void k_spread_bin(ParticleDev P, int n, double h, double* __restrict__ part, double* __restrict__ q_old) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_spread_bin_body(const ParticleDev& P, int n, double h, double* __restrict__ part, double* __restrict__ q_old, int bx) {
+    const int p = bx * blockDim.x + threadIdx.x;
     double u = 0.0;
     if (p < P.np) {
         if (q_old != nullptr) {
@@ -269,17 +272,20 @@ __global__ void k_spread_bin(ParticleDev P, int n, double h, double* __restrict_
     __shared__ double sh[4 * 32];
     double v[1] = {u};
     block_sum<1>(v, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    if (threadIdx.x == 0) part[bx] = v[0];
 }
+template <int CAS>
+__global__ void k_spread_bin(ParticleDev P, int n, double h, double* __restrict__ part, double* __restrict__ q_old) { k_spread_bin_body<CAS>(P, n, h, part, q_old, blockIdx.x); }
 
-__global__ void k_spread_fill(ParticleDev P) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_spread_fill_body(const ParticleDev& P, int bx) {
+    const int p = bx * blockDim.x + threadIdx.x;
     if (p >= P.np) return;
     const int* b = P.base + 3 * p;
     const int tile = ((b[0] / kTileI) * P.ntj + b[1] / kTileJ) * P.ntk + b[2] / kTileK;
     const int slot = atomicAdd(&P.tile_fill[tile], 1);
     P.tile_ions[slot] = p;
 }
+__global__ void k_spread_fill(ParticleDev P) { k_spread_fill_body(P, blockIdx.x); }
 
 // Is grid index g one of the stencil's indices along an axis with base index b (wrapped)?
 // CIC: b, b+1; splines: b-1 .. b+2 (particles.c:297-385).
@@ -454,13 +460,12 @@ __device__ __forceinline__ double cic_contrib(const ParticleDev& P, int c, int i
     return P.chg[c] * wgt;
 }
 
-__global__ void __launch_bounds__(kSpreadIonThreads) k_spread_ions(ParticleDev P, double* __restrict__ q,
-                                                                   uint32_t* __restrict__ qmask, int n, double h) {
+__device__ __forceinline__ void k_spread_ions_body(const ParticleDev& P, double* __restrict__ q, uint32_t* __restrict__ qmask, int n, double h, int bx) {
     __shared__ int near_id_s[kIonsPerCta][kNear];
     __shared__ int near_o_s[kIonsPerCta][kNear];  // offset code (di+1)*9 + (dj+1)*3 + (dk+1)
     __shared__ int near_n_s[kIonsPerCta];
     const int g = threadIdx.x / kIonLanes, sub = threadIdx.x % kIonLanes;
-    const int p = blockIdx.x * kIonsPerCta + g;
+    const int p = bx * kIonsPerCta + g;
     if (p >= P.np) return;  // whole groups of eight lanes leave together
     const unsigned gmask = 0xffu << (threadIdx.x & 24);
     const double L = n * h;
@@ -562,6 +567,8 @@ __global__ void __launch_bounds__(kSpreadIonThreads) k_spread_ions(ParticleDev P
         atomicOr(qmask + (seg >> 5), 1u << (seg & 31));
     }
 }
+__global__ void __launch_bounds__(kSpreadIonThreads) k_spread_ions(ParticleDev P, double* __restrict__ q,
+                                                                   uint32_t* __restrict__ qmask, int n, double h) { k_spread_ions_body(P, q, qmask, n, h, blockIdx.x); }
 
 void spread_charges(ParticleDev& P, double* q, uint32_t* qmask, int n, double h, cudaStream_t s) {
     const int nb = (P.np + 127) / 128;
@@ -617,9 +624,9 @@ void spread_charges(ParticleDev& P, double* q, uint32_t* qmask, int n, double h,
 constexpr int kForceLanes = 8;
 
 template <int CAS>
-__global__ void __launch_bounds__(128) k_field_forces(ParticleDev P, const double* __restrict__ phi, int n, double h) {
+__device__ __forceinline__ void k_field_forces_body(const ParticleDev& P, const double* __restrict__ phi, int n, double h, int bx) {
     constexpr int S = stencil_size<CAS>(), T = S / kForceLanes;
-    const int p = (blockIdx.x * blockDim.x + threadIdx.x) / kForceLanes, sub = threadIdx.x % kForceLanes;
+    const int p = (bx * blockDim.x + threadIdx.x) / kForceLanes, sub = threadIdx.x % kForceLanes;
     if (p >= P.np) return;  // whole groups of eight lanes leave together
     const unsigned gmask = 0xffu << (threadIdx.x & 24);
     const int g0 = threadIdx.x & 31 & ~(kForceLanes - 1);
@@ -658,6 +665,8 @@ __global__ void __launch_bounds__(128) k_field_forces(ParticleDev P, const doubl
         P.fe[3 * p + 2] = fz;
     }
 }
+template <int CAS>
+__global__ void __launch_bounds__(128) k_field_forces(ParticleDev P, const double* __restrict__ phi, int n, double h) { k_field_forces_body<CAS>(P, phi, n, h, blockIdx.x); }
 
 void field_forces(ParticleDev& P, const double* phi, int n, double h, cudaStream_t s) {
     if (P.np == 0) return;
@@ -676,8 +685,8 @@ void field_forces(ParticleDev& P, const double* phi, int n, double h, cudaStream
 // Linked cells by counting sort, stable in ion index: cell (IX,IY,IZ) with
 // IX = int((nc/L) * x) (maze_poisson/linkedcell.py:18-26), clamped into the box.
 // ------------------------------------------------------------------------------------
-__global__ void k_cell_count(ParticleDev P) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_cell_count_body(const ParticleDev& P, int bx) {
+    const int p = bx * blockDim.x + threadIdx.x;
     if (p >= P.np) return;
     const double rel = P.nc / P.L;
     int c[3];
@@ -695,13 +704,15 @@ __global__ void k_cell_count(ParticleDev P) {
     P.cell_of[p] = cell;
     atomicAdd(&P.cell_count[cell], 1);
 }
+__global__ void k_cell_count(ParticleDev P) { k_cell_count_body(P, blockIdx.x); }
 
-__global__ void k_cell_fill(ParticleDev P) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_cell_fill_body(const ParticleDev& P, int bx) {
+    const int p = bx * blockDim.x + threadIdx.x;
     if (p >= P.np) return;
     const int slot = atomicAdd(&P.cell_fill[P.cell_of[p]], 1);
     P.cell_ions[slot] = p;
 }
+__global__ void k_cell_fill(ParticleDev P) { k_cell_fill_body(P, blockIdx.x); }
 
 // One warp per cell: restore ascending ion order inside the cell (the scatter above is
 // unordered) by ranking each ion against the cell's others (ion indices are distinct, so
@@ -709,10 +720,10 @@ __global__ void k_cell_fill(ParticleDev P) {
 // one lane), then gather positions/types into cell order and record each ion's rank.
 constexpr int kCellStage = 256;
 
-__global__ void __launch_bounds__(128) k_cell_sort_gather(ParticleDev P) {
+__device__ __forceinline__ void k_cell_sort_gather_body(const ParticleDev& P, int bx) {
     __shared__ int stage_all[4][kCellStage];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int cell = blockIdx.x * 4 + w;
+    const int cell = bx * 4 + w;
     if (cell >= P.ncell) return;
     const int b = P.cell_start[cell], e = P.cell_start[cell + 1], m = e - b;
     int* st = stage_all[w];
@@ -746,6 +757,7 @@ __global__ void __launch_bounds__(128) k_cell_sort_gather(ParticleDev P) {
         P.srank[p] = x;
     }
 }
+__global__ void __launch_bounds__(128) k_cell_sort_gather(ParticleDev P) { k_cell_sort_gather_body(P, blockIdx.x); }
 
 void build_cells(ParticleDev& P, cudaStream_t s) {
     MZB_CHECK(cudaMemsetAsync(P.cell_count, 0, sizeof(int32_t) * P.ncell, s));
@@ -764,8 +776,8 @@ void build_cells(ParticleDev& P, cudaStream_t s) {
 // ------------------------------------------------------------------------------------
 // fcs_tot = (0 + 1*fcs_elec) + 1*fcs_noel (particles.c:777-795)
 // ------------------------------------------------------------------------------------
-__global__ void k_total_forces(ParticleDev P) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_total_forces_body(const ParticleDev& P, int bx) {
+    const int t = bx * blockDim.x + threadIdx.x;
     if (t >= 3 * P.np) return;
     double v = 0.0;
     v += 1.0 * P.fe[t];
@@ -777,6 +789,7 @@ __global__ void k_total_forces(ParticleDev P) {
     }
     P.ft[t] = v;
 }
+__global__ void k_total_forces(ParticleDev P) { k_total_forces_body(P, blockIdx.x); }
 
 void total_forces(ParticleDev& P, cudaStream_t s) {
     if (P.np == 0) return;
@@ -789,8 +802,8 @@ void total_forces(ParticleDev& P, cudaStream_t s) {
 // Kinetic energy, momentum, temperature (particles.c:798-839). Block partials are summed
 // in block order by one thread: deterministic for a given N.
 // ------------------------------------------------------------------------------------
-__global__ void k_ke_partial(ParticleDev P) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_ke_partial_body(const ParticleDev& P, int bx) {
+    const int p = bx * blockDim.x + threadIdx.x;
     double v[4] = {0.0, 0.0, 0.0, 0.0};
     if (p < P.np) {
         const double m = P.mass[p], vx = P.vel[3 * p], vy = P.vel[3 * p + 1], vz = P.vel[3 * p + 2];
@@ -806,11 +819,12 @@ __global__ void k_ke_partial(ParticleDev P) {
     __shared__ double sh[4 * 32];
     block_sum<4>(v, sh);
     if (threadIdx.x == 0)
-        for (int q = 0; q < 4; q++) P.partial[4 * blockIdx.x + q] = v[q];
+        for (int q = 0; q < 4; q++) P.partial[4 * bx + q] = v[q];
 }
+__global__ void k_ke_partial(ParticleDev P) { k_ke_partial_body(P, blockIdx.x); }
 
 // red[2] = KE, red[3..5] = momentum, red[6] = T, red[7] = sqrt(T_target / T)
-__global__ void k_ke_final(ParticleDev P, int nblocks, double T_target) {
+__device__ __forceinline__ void k_ke_final_body(const ParticleDev& P, int nblocks, double T_target, int bx) {
     double s[4] = {0.0, 0.0, 0.0, 0.0};
     for (int b = 0; b < nblocks; b++)
         for (int q = 0; q < 4; q++) s[q] += P.partial[4 * b + q];
@@ -823,6 +837,7 @@ __global__ void k_ke_final(ParticleDev P, int nblocks, double T_target) {
     P.red[6] = T;
     P.red[7] = sqrt(T_target / T);
 }
+__global__ void k_ke_final(ParticleDev P, int nblocks, double T_target) { k_ke_final_body(P, nblocks, T_target, blockIdx.x); }
 
 static void ke_reduce(ParticleDev& P, double T_target, cudaStream_t s) {
     const int nb = P.np > 0 ? (P.np + 255) / 256 : 1;
@@ -900,8 +915,8 @@ __device__ __forceinline__ double wrap_box(double a, double L) {
 }
 
 // Velocity Verlet part 1: optional rescale to the target T, half kick, drift, wrap.
-__global__ void k_verlet1(ParticleDev P, double dt, int rescale) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_verlet1_body(const ParticleDev& P, double dt, int rescale, int bx) {
+    const int t = bx * blockDim.x + threadIdx.x;
     if (t >= 3 * P.np) return;
     const int p = t / 3;
     double v = P.vel[t];
@@ -910,15 +925,17 @@ __global__ void k_verlet1(ParticleDev P, double dt, int rescale) {
     P.vel[t] = v;
     P.pos[t] = wrap_box(P.pos[t] + dt * v, P.L);
 }
-__global__ void k_verlet2(ParticleDev P, double dt) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_verlet1(ParticleDev P, double dt, int rescale) { k_verlet1_body(P, dt, rescale, blockIdx.x); }
+__device__ __forceinline__ void k_verlet2_body(const ParticleDev& P, double dt, int bx) {
+    const int t = bx * blockDim.x + threadIdx.x;
     if (t >= 3 * P.np) return;
     P.vel[t] += 0.5 * dt * P.ft[t] / P.mass[t / 3];
 }
+__global__ void k_verlet2(ParticleDev P, double dt) { k_verlet2_body(P, dt, blockIdx.x); }
 
 // OVRVO: part1 = [O] V R, part2 = V [O]; O uses Philox normals for call `call`.
-__global__ void k_ovrvo(ParticleDev P, IntegratorDev I, int part, uint64_t call) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_ovrvo_body(const ParticleDev& P, const IntegratorDev& I, int part, uint64_t call, int bx) {
+    const int p = bx * blockDim.x + threadIdx.x;
     if (p >= P.np) return;
     if (I.ocalls_d != nullptr) call = *I.ocalls_d;
     const double m = P.mass[p];
@@ -946,8 +963,10 @@ __global__ void k_ovrvo(ParticleDev P, IntegratorDev I, int part, uint64_t call)
     }
     for (int d = 0; d < 3; d++) P.vel[3 * p + d] = v[d];
 }
+__global__ void k_ovrvo(ParticleDev P, IntegratorDev I, int part, uint64_t call) { k_ovrvo_body(P, I, part, call, blockIdx.x); }
 
-__global__ void k_advance_counter(uint64_t* c) { *c += 1; }
+__device__ __forceinline__ void k_advance_counter_body(uint64_t* c, int bx) { *c += 1; }
+__global__ void k_advance_counter(uint64_t* c) { k_advance_counter_body(c, blockIdx.x); }
 
 static void advance_ocalls(IntegratorDev& I, cudaStream_t s) {
     if (!I.enabled) return;
@@ -1011,6 +1030,190 @@ void rescale_velocities(ParticleDev& P, cudaStream_t s) {
     count_launch();
     k_rescale_apply<<<(3 * P.np + 255) / 256, 256, 0, s>>>(P, P.partial);
     MZB_CHECK(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------------------------
+// Replica tables (particles.cuh): the particle stages of a batched MD step, one launch per
+// stage over all systems, each CTA running the per-system kernel's body for its system.
+// ------------------------------------------------------------------------------------
+namespace {
+
+// The step's zeroing for one system, over one run of units: tile counts, the charge
+// bitmap, cell counts, the bad-cell flag and the field solve's barrier words (and the whole
+// charge grid when it does not hold only the last corners) -- what the per-system path
+// clears with memsets.
+constexpr int kZeroThreads = 256;
+long zero_units(const StageArgs& a) {
+    return (long)a.P.ntiles + a.mask_words + a.P.ncell + 1 + 4 + (a.q_sparse ? 0 : (long)a.n * a.n * a.n);
+}
+__device__ __forceinline__ void zero_body(const StageArgs& a, int bx) {
+    long u = (long)bx * blockDim.x + threadIdx.x;
+    const ParticleDev& P = a.P;
+    if (u < P.ntiles) {
+        P.tile_count[u] = 0;
+        return;
+    }
+    u -= P.ntiles;
+    if (u < a.mask_words) {
+        a.qmask[u] = 0u;
+        return;
+    }
+    u -= a.mask_words;
+    if (u < P.ncell) {
+        P.cell_count[u] = 0;
+        return;
+    }
+    u -= P.ncell;
+    if (u == 0) {
+        P.flags[1] = 0;
+        return;
+    }
+    u -= 1;
+    if (u < 4) {
+        reinterpret_cast<unsigned int*>(a.bar)[u] = 0u;
+        return;
+    }
+    u -= 4;
+    if (!a.q_sparse && u < (long)a.n * a.n * a.n) a.q[u] = 0.0;
+}
+
+__device__ __forceinline__ int blocks_of(long units, int per) { return (int)((units + per - 1) / per); }
+// CTAs of the per-ion spreading kernel (their partial charge sums are summed by the scan)
+__device__ __forceinline__ int spread_bin_blocks(const StageArgs& a) { return a.P.np > 0 ? blocks_of(a.P.np, 128) : 1; }
+
+// CTAs of every stage for system a (the per-system launches' grids), into c[SK_COUNT]
+void stage_blocks(const StageArgs& a, int* c) {
+    const ParticleDev& P = a.P;
+    const long np = P.np, nblk32 = (np + 31) / 32;
+    const bool verlet = a.I.type == 1, has = np > 0;
+    auto cdiv = [](long u, long per) { return (int)((u + per - 1) / per); };
+    for (int k = 0; k < SK_COUNT; k++) c[k] = 0;
+    c[SK_ZERO] = cdiv(zero_units(a), kZeroThreads);
+    c[SK_KE] = has && verlet && a.I.enabled ? cdiv(np, 256) : 0;
+    c[SK_KEF] = has && verlet && a.I.enabled ? 1 : 0;
+    c[SK_INT1] = c[SK_INT2] = has ? cdiv(verlet ? 3 * np : np, 128) : 0;
+    c[SK_ADV1] = c[SK_ADV2] = has && !verlet && a.I.enabled ? 1 : 0;
+    c[SK_BIN] = has ? cdiv(np, 128) : 1;  // spread_bin_blocks
+    c[SK_SCANR] = c[SK_SCANA] = cdiv(P.ntiles, 1024);
+    c[SK_FILL] = has ? cdiv(np, 128) : 0;
+    c[SK_IONS] = has ? cdiv(np, kIonsPerCta) : 0;
+    c[SK_QCHK] = c[SK_SCHK] = 1;
+    c[SK_FF] = has ? cdiv(8 * np, 128) : 0;
+    c[SK_CCOUNT] = c[SK_CFILL] = has ? cdiv(np, 128) : 0;
+    c[SK_CSCAN] = 1;
+    c[SK_CSORT] = cdiv(P.ncell, 4);
+    c[SK_TFBOX] = has ? cdiv(32 * nblk32, 256) : 0;
+    c[SK_TF_TF] = has && P.pot == POT_TF ? P.tf_nst : 0;
+    c[SK_TF_LJ] = has && P.pot == POT_LJ ? P.tf_nst : 0;
+    c[SK_TF_SC] = has && P.pot == POT_SC ? P.tf_nst : 0;
+    c[SK_TFG] = has ? cdiv(32 * nblk32, 128) : 0;
+    c[SK_TFE] = 1;
+    c[SK_TOT] = has ? cdiv(3 * np, 256) : 0;
+}
+
+#define MZB_TABLE_KERNEL(name, threads, ...)                                                                \
+    __global__ void __launch_bounds__(threads) name(const StageArgs* __restrict__ A,                        \
+                                                    const int* __restrict__ start, int nsys) {               \
+        table_run(A, start, nsys, [&](const StageArgs& a, int b) { __VA_ARGS__; });                         \
+    }
+
+MZB_TABLE_KERNEL(kt_zero, kZeroThreads, zero_body(a, b))
+MZB_TABLE_KERNEL(kt_ke, 256, k_ke_partial_body(a.P, b))
+MZB_TABLE_KERNEL(kt_kef, 32, if (threadIdx.x == 0) k_ke_final_body(a.P, blocks_of(a.P.np, 256), a.I.T, b))
+MZB_TABLE_KERNEL(kt_int1, 128,
+                 if (a.I.type == 1) k_verlet1_body(a.P, a.I.dt, a.I.enabled, b);
+                 else k_ovrvo_body(a.P, a.I, 1, a.I.ocalls, b))
+MZB_TABLE_KERNEL(kt_int2, 128,
+                 if (a.I.type == 1) k_verlet2_body(a.P, a.I.dt, b);
+                 else k_ovrvo_body(a.P, a.I, 2, a.I.ocalls, b))
+MZB_TABLE_KERNEL(kt_adv, 32, if (threadIdx.x == 0) k_advance_counter_body(a.I.ocalls_d, b))
+MZB_TABLE_KERNEL(kt_bin, 128, k_spread_bin_body<CAS_CIC>(a.P, a.n, a.h, a.P.partial, a.q_sparse ? a.q : nullptr, b))
+MZB_TABLE_KERNEL(kt_scanr, 1024, k_scan_reduce_body(a.P.tile_count, a.P.ntiles, a.P.tile_part, b))
+MZB_TABLE_KERNEL(kt_scana, 1024,
+                 k_scan_apply_body(a.P.tile_count, a.P.ntiles, a.P.tile_part, a.P.tile_start, a.P.tile_fill,
+                                   a.P.partial, spread_bin_blocks(a), a.P.red + 0, b))
+MZB_TABLE_KERNEL(kt_fill, 128, k_spread_fill_body(a.P, b))
+MZB_TABLE_KERNEL(kt_ions, kSpreadIonThreads, k_spread_ions_body(a.P, a.q, a.qmask, a.n, a.h, b))
+// the charge check of solver_update_charges (solver_md.c:98-102) and the solve's status,
+// kept on the device and read after the call
+MZB_TABLE_KERNEL(kt_qchk, 32, if (threadIdx.x == 0) {
+    const double q = a.P.red[0];
+    if (fabs(*a.qtot - q) > 1e-6) a.err[0] = 1;
+    *a.qtot = q;
+    if (a.P.flags[0]) a.err[1] = 1;
+})
+MZB_TABLE_KERNEL(kt_schk, 32, if (threadIdx.x == 0 && (a.result[0] < 0 || a.result[1] != 0)) a.err[2] = 1)
+MZB_TABLE_KERNEL(kt_ff, 128, k_field_forces_body<CAS_CIC>(a.P, a.phi, a.n, a.h, b))
+MZB_TABLE_KERNEL(kt_ccount, 128, k_cell_count_body(a.P, b))
+MZB_TABLE_KERNEL(kt_cscan, 1024,
+                 k_scan_body(a.P.cell_count, a.P.ncell, a.P.cell_start, a.P.cell_fill, nullptr, 0, nullptr, b))
+MZB_TABLE_KERNEL(kt_cfill, 128, k_cell_fill_body(a.P, b))
+MZB_TABLE_KERNEL(kt_csort, 128, k_cell_sort_gather_body(a.P, b))
+MZB_TABLE_KERNEL(kt_tot, 256, k_total_forces_body(a.P, b))
+
+#undef MZB_TABLE_KERNEL
+
+void tlaunch(const StageTable& t, int k, void (*kernel)(const StageArgs*, const int*, int), int threads,
+             cudaStream_t s) {
+    if (t.total[k] <= 0) return;
+    count_launch();
+    kernel<<<t.total[k], threads, 0, s>>>(t.args, t.start + k * (t.nsys + 1), t.nsys);
+    MZB_CHECK(cudaGetLastError());
+}
+
+}  // namespace
+
+bool stage_table_ok(const StageArgs& a) { return a.P.cas == CAS_CIC && a.P.fdb == nullptr; }
+
+StageTable stage_table_build(const std::vector<StageArgs>& a) {
+    StageTable t;
+    t.nsys = (int)a.size();
+    const int w = t.nsys + 1;
+    std::vector<int> start((size_t)SK_COUNT * w, 0);
+    int c[SK_COUNT];
+    for (int r = 0; r < t.nsys; r++) {
+        stage_blocks(a[r], c);
+        for (int k = 0; k < SK_COUNT; k++) start[(size_t)k * w + r + 1] = start[(size_t)k * w + r] + c[k];
+    }
+    for (int k = 0; k < SK_COUNT; k++) t.total[k] = start[(size_t)k * w + t.nsys];
+    t.args = static_cast<StageArgs*>(dev_alloc(sizeof(StageArgs) * a.size()));
+    t.start = static_cast<int*>(dev_alloc(sizeof(int) * start.size()));
+    MZB_CHECK(cudaMemcpy(t.args, a.data(), sizeof(StageArgs) * a.size(), cudaMemcpyHostToDevice));
+    MZB_CHECK(cudaMemcpy(t.start, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice));
+    return t;
+}
+
+void stage_table_free(StageTable& t) {
+    dev_free(t.args);
+    dev_free(t.start);
+    t = StageTable{};
+}
+
+void stages_before_solve(const StageTable& t, cudaStream_t s) {
+    tlaunch(t, SK_ZERO, kt_zero, kZeroThreads, s);
+    tlaunch(t, SK_KE, kt_ke, 256, s);
+    tlaunch(t, SK_KEF, kt_kef, 32, s);
+    tlaunch(t, SK_INT1, kt_int1, 128, s);
+    tlaunch(t, SK_ADV1, kt_adv, 32, s);
+    tlaunch(t, SK_BIN, kt_bin, 128, s);
+    tlaunch(t, SK_SCANR, kt_scanr, 1024, s);
+    tlaunch(t, SK_SCANA, kt_scana, 1024, s);
+    tlaunch(t, SK_FILL, kt_fill, 128, s);
+    tlaunch(t, SK_IONS, kt_ions, kSpreadIonThreads, s);
+    tlaunch(t, SK_QCHK, kt_qchk, 32, s);
+}
+
+void stages_after_solve(const StageTable& t, cudaStream_t s) {
+    tlaunch(t, SK_SCHK, kt_schk, 32, s);
+    tlaunch(t, SK_FF, kt_ff, 128, s);
+    tlaunch(t, SK_CCOUNT, kt_ccount, 128, s);
+    tlaunch(t, SK_CSCAN, kt_cscan, 1024, s);
+    tlaunch(t, SK_CFILL, kt_cfill, 128, s);
+    tlaunch(t, SK_CSORT, kt_csort, 128, s);
+    tf_stages(t, s);
+    tlaunch(t, SK_TOT, kt_tot, 256, s);
+    tlaunch(t, SK_INT2, kt_int2, 128, s);
+    tlaunch(t, SK_ADV2, kt_adv, 32, s);
 }
 
 }  // namespace mzb

@@ -2,6 +2,8 @@
 // interpolation, Tosi-Fumi pair forces, integrators and reductions.
 #pragma once
 
+#include <vector>
+
 #include "mzb_common.cuh"
 
 namespace mzb {
@@ -122,5 +124,79 @@ void rescale_velocities(ParticleDev& P, cudaStream_t s);
 // Philox4x32-10 standard normals of the O-block (O-block call `call`, ion `ion`,
 // components 0..2) written to out[3*ion + d] for ion < np.
 void philox_normals(uint64_t seed, uint64_t call, int np, double* out, cudaStream_t s);
+
+// ------------------------------------------------------------------------------------
+// Replica tables: each particle stage of the batched MD step as ONE launch over all the
+// systems of the batch. The launch's CTAs are the systems' own grids of that stage laid
+// end to end (start[r] .. start[r + 1] for system r, per stage); every CTA finds its
+// system, stages that system's StageArgs in shared memory and runs the stage's kernel
+// body with its block index inside the system's grid -- the same body, block for block,
+// as the per-system launch, so the results are the same.
+// ------------------------------------------------------------------------------------
+struct StageArgs {
+    ParticleDev P;
+    IntegratorDev I;            // ocalls_d set: the Philox counter lives on the device
+    double* q = nullptr;        // charge grid (n^3)
+    uint32_t* qmask = nullptr;  // its bitmap of runs of 64 k (n % 64 == 0), or null
+    int mask_words = 0;
+    int n = 0;
+    double h = 0;
+    int q_sparse = 1;           // q holds only the CIC corners of the ions' base cells (else cleared whole)
+    const double* phi = nullptr;  // the field the step's solve writes
+    double* qtot = nullptr;       // device charge total of the last step
+    int* err = nullptr;           // device error words ([0] charge drift, [1] spread overflow, [2] solve)
+    const int* result = nullptr;  // the solve's result words
+    GridBarrier* bar = nullptr;   // the solve team's barrier (zeroed at the start of the step)
+};
+
+// The system of this CTA in a launch over a replica table (the last r with start[r] <=
+// blockIdx.x: systems without CTAs in the launch have start[r] == start[r + 1]), its
+// arguments staged in shared memory, and f(args, block index inside the system's grid).
+template <class F>
+__device__ __forceinline__ void table_run(const StageArgs* __restrict__ A, const int* __restrict__ start, int nsys,
+                                          F&& f) {
+    // raw storage: StageArgs has default member initialisers, and a __shared__ object of it
+    // would have every thread store them at its declaration, racing with the copy below
+    __shared__ __align__(16) unsigned char a_raw[sizeof(StageArgs)];
+    StageArgs& a = *reinterpret_cast<StageArgs*>(a_raw);
+    int lo = 0, hi = nsys - 1;
+    const int b = (int)blockIdx.x;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (start[mid] <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    const int* src = reinterpret_cast<const int*>(A + lo);
+    int* dst = reinterpret_cast<int*>(a_raw);
+    for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    f(a, b - start[lo]);
+}
+
+enum StageKind {
+    SK_ZERO, SK_KE, SK_KEF, SK_INT1, SK_ADV1, SK_BIN, SK_SCANR, SK_SCANA, SK_FILL, SK_IONS, SK_QCHK,
+    SK_SCHK, SK_FF, SK_CCOUNT, SK_CSCAN, SK_CFILL, SK_CSORT, SK_TFBOX, SK_TF_TF, SK_TF_LJ, SK_TF_SC, SK_TFG,
+    SK_TFE, SK_TOT, SK_INT2, SK_ADV2, SK_COUNT
+};
+
+struct StageTable {
+    int nsys = 0;
+    StageArgs* args = nullptr;  // device [nsys]
+    int* start = nullptr;       // device [SK_COUNT][nsys + 1]
+    int total[SK_COUNT] = {};   // CTAs of each stage's launch (0: not launched)
+};
+
+// Whether a system can be stepped through the tables (CIC charge assignment).
+bool stage_table_ok(const StageArgs& a);
+// Per-stage CTA counts of every system and the device copies of the table.
+StageTable stage_table_build(const std::vector<StageArgs>& a);
+void stage_table_free(StageTable& t);
+// The stages before the field solve (integrator part 1, charge spreading, charge check,
+// zeroing of the step's counters and the solve's barriers), and after it (solve check,
+// field forces, linked cells, pair forces, total forces, integrator part 2).
+void stages_before_solve(const StageTable& t, cudaStream_t s);
+void stages_after_solve(const StageTable& t, cudaStream_t s);
+// The pair-force stages (tf_forces.cu): boxes, pair forces, gather, energy.
+void tf_stages(const StageTable& t, cudaStream_t s);
 
 }  // namespace mzb

@@ -87,9 +87,9 @@ __device__ __forceinline__ void pair_terms(const double* t, double r2, double ir
 }
 
 // Bounding box of each block of 32 cell-ordered ions: [lo x, lo y, lo z, hi x, hi y, hi z].
-__global__ void k_tf_boxes(ParticleDev P) {
+__device__ __forceinline__ void k_tf_boxes_body(const ParticleDev& P, int bx) {
     const int lane = threadIdx.x & 31;
-    const int b = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+    const int b = (int)((bx * (long)blockDim.x + threadIdx.x) >> 5);
     const int nblk = (P.np + 31) / 32;
     if (b >= nblk) return;
     const int s = b * 32 + lane < P.np ? b * 32 + lane : b * 32;  // idle lanes mirror lane 0
@@ -108,6 +108,7 @@ __global__ void k_tf_boxes(ParticleDev P) {
         P.tf_box[6 * b + 3 + lane] = hi[lane];
     }
 }
+__global__ void k_tf_boxes(ParticleDev P) { k_tf_boxes_body(P, blockIdx.x); }
 
 // The ion type stored in a double slot of the shared position arrays as its integer bits
 // (read back without a conversion).
@@ -165,14 +166,14 @@ __device__ __forceinline__ bool pair_eval(const double* tab, int ntyp, double L,
 }
 
 template <int POT>
-__global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
+__device__ __forceinline__ void k_tf_body(const ParticleDev& P, int bx) {
     extern __shared__ double sm[];
     double* tab = sm;                              // [64][kTfTabStride]
     double* ipos = tab + kTfTab;                   // [4][256]: x, y, z, type (structure of arrays)
     double* jpos = ipos + kTfSb * 32 * 4;          // [4][256]
     double* fjw = jpos + kTfSb * 32 * 4;           // [8 warps][8 J blocks][3][32]
     constexpr int NQ = kTfSb * 32;
-    const int st = blockIdx.x;
+    const int st = bx;
     const int SI = P.tf_st[2 * st], SJ = P.tf_st[2 * st + 1];
     const bool diag = SI == SJ;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -307,12 +308,14 @@ __global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) {
         P.epart[st] = e;
     }
 }
+template <int POT>
+__global__ void __launch_bounds__(kTfThreads, 3) k_tf(ParticleDev P) { k_tf_body<POT>(P, blockIdx.x); }
 
 // Each ion's force: its super-tile partials in list order, scattered back to ion order.
 // A warp per block of 32 cell-ordered ions: the block's list is walked once for all 32
 // lanes (one ion each), whose partials lie side by side.
-__global__ void k_tf_gather(ParticleDev P) {
-    const int b = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+__device__ __forceinline__ void k_tf_gather_body(const ParticleDev& P, int bx) {
+    const int b = (int)((bx * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
     if (b >= (P.np + 31) / 32) return;
     double f[3] = {0.0, 0.0, 0.0};
     const int e1 = P.tf_gstart[b + 1];
@@ -332,14 +335,16 @@ __global__ void k_tf_gather(ParticleDev P) {
     P.fn[3 * p + 1] = f[1];
     P.fn[3 * p + 2] = f[2];
 }
+__global__ void k_tf_gather(ParticleDev P) { k_tf_gather_body(P, blockIdx.x); }
 
-__global__ void k_tf_energy(ParticleDev P) {
+__device__ __forceinline__ void k_tf_energy_body(const ParticleDev& P, int bx) {
     double v[1] = {0.0};
     for (int x = threadIdx.x; x < P.tf_nst; x += blockDim.x) v[0] += P.epart[x];
     __shared__ double sh[4 * 32];
     block_sum<1>(v, sh);
     if (threadIdx.x == 0) P.red[1] = v[0];
 }
+__global__ void k_tf_energy(ParticleDev P) { k_tf_energy_body(P, blockIdx.x); }
 
 void tf_plan(ParticleDev& P) {
     dev_free(P.tf_st);
@@ -417,6 +422,53 @@ void tf_forces(ParticleDev& P, cudaStream_t s) {
     count_launch();
     k_tf_energy<<<1, 1024, 0, s>>>(P);
     MZB_CHECK(cudaGetLastError());
+}
+
+// The pair-force stages of a batched step over a replica table (particles.cuh): boxes,
+// pair forces (one launch per potential present), gather, energy.
+namespace {
+__global__ void __launch_bounds__(256) kt_tfbox(const StageArgs* __restrict__ A, const int* __restrict__ start,
+                                                int nsys) {
+    table_run(A, start, nsys, [&](const StageArgs& a, int b) { k_tf_boxes_body(a.P, b); });
+}
+template <int POT>
+__global__ void __launch_bounds__(kTfThreads, 3) kt_tf(const StageArgs* __restrict__ A, const int* __restrict__ start,
+                                                       int nsys) {
+    table_run(A, start, nsys, [&](const StageArgs& a, int b) { k_tf_body<POT>(a.P, b); });
+}
+__global__ void __launch_bounds__(128) kt_tfg(const StageArgs* __restrict__ A, const int* __restrict__ start,
+                                              int nsys) {
+    table_run(A, start, nsys, [&](const StageArgs& a, int b) { k_tf_gather_body(a.P, b); });
+}
+__global__ void __launch_bounds__(1024) kt_tfe(const StageArgs* __restrict__ A, const int* __restrict__ start,
+                                               int nsys) {
+    table_run(A, start, nsys, [&](const StageArgs& a, int b) { k_tf_energy_body(a.P, b); });
+}
+void tf_tlaunch(const StageTable& t, int k, void (*kernel)(const StageArgs*, const int*, int), int threads,
+                size_t smem, cudaStream_t s) {
+    if (t.total[k] <= 0) return;
+    count_launch();
+    kernel<<<t.total[k], threads, smem, s>>>(t.args, t.start + k * (t.nsys + 1), t.nsys);
+    MZB_CHECK(cudaGetLastError());
+}
+}  // namespace
+
+void tf_stages(const StageTable& t, cudaStream_t s) {
+    static unsigned long long attr_done = 0;  // devices whose table kernels allow kTfSmem
+    int dev = 0;
+    MZB_CHECK(cudaGetDevice(&dev));
+    if (!(attr_done >> (dev & 63) & 1ull)) {
+        MZB_CHECK(cudaFuncSetAttribute(kt_tf<POT_TF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTfSmem));
+        MZB_CHECK(cudaFuncSetAttribute(kt_tf<POT_LJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTfSmem));
+        MZB_CHECK(cudaFuncSetAttribute(kt_tf<POT_SC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTfSmem));
+        attr_done |= 1ull << (dev & 63);
+    }
+    tf_tlaunch(t, SK_TFBOX, kt_tfbox, 256, 0, s);
+    tf_tlaunch(t, SK_TF_TF, kt_tf<POT_TF>, kTfThreads, kTfSmem, s);
+    tf_tlaunch(t, SK_TF_LJ, kt_tf<POT_LJ>, kTfThreads, kTfSmem, s);
+    tf_tlaunch(t, SK_TF_SC, kt_tf<POT_SC>, kTfThreads, kTfSmem, s);
+    tf_tlaunch(t, SK_TFG, kt_tfg, 128, 0, s);
+    tf_tlaunch(t, SK_TFE, kt_tfe, 1024, 0, s);
 }
 
 }  // namespace mzb

@@ -72,7 +72,10 @@ def test_batch_matches_alone(prod):
         assert prod.mzb_system_destroy(h) == 0
     launches0 = prod.mzb_kernel_launches()
     assert prod.mzb_batch_step(handles, len(handles), STEPS) == 0
-    assert prod.mzb_kernel_launches() > launches0
+    # each particle stage is one launch over the replica table, whatever the number of
+    # systems: about 20 kernels per batched step (the field solves are one of them)
+    per_step = (prod.mzb_kernel_launches() - launches0) / STEPS
+    assert 0 < per_step <= 24, per_step
     try:
         for (h, run), ref in zip(runs, alone):
             assert prod.mzb_system_select(h) == 0
