@@ -134,7 +134,7 @@ struct System {
     uint64_t epoch = 0;           // bumped by host-side changes that batched-step graphs bake in
     double* qtot_d = nullptr;     // device copy of q_tot (batched steps check charge on the device)
     std::vector<double> pb_radii; // host copy of the PB solvation radii
-    int* err_d = nullptr;         // batched steps: [0] charge error, [1] spread overflow, [2] solve failure
+    int* err_d = nullptr;         // batched steps: [0] charge error, [2] solve failure
 };
 
 System* g = nullptr;             // the selected system
@@ -830,11 +830,7 @@ int solver_update_charges(void) {
     ParticleDev& P = parts();
     spread_charges(P, G.q, G.qmask, G.n, G.h, s.stream);
     MZB_CHECK(cudaMemcpyAsync(s.red_h, P.red, sizeof(double), cudaMemcpyDeviceToHost, s.stream));
-    int flag = 0;
-    MZB_CHECK(cudaMemcpyAsync(s.result_h, P.flags, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
     sync();
-    flag = s.result_h[0];
-    if (flag) fatal("charge spreading: more than 1024 ions reach one 2x8x32 grid tile");
     const double q_loc = s.red_h[0];
     int res = 0;
     if (fabs(s.q_tot - q_loc) > 1e-6) {
@@ -1707,11 +1703,10 @@ int solver_md_step(int n_steps) {
 namespace mzb {
 namespace {
 
-__global__ void k_charge_check(const double* red, double* qtot, int* err, const int* flags) {
+__global__ void k_charge_check(const double* red, double* qtot, int* err) {
     const double q = red[0];
     if (fabs(*qtot - q) > 1e-6) err[0] = 1;  // solver_md.c:98-102
     *qtot = q;
-    if (flags[0]) err[1] = 1;
 }
 __global__ void k_solve_check(const int* result, int* err) {
     if (result[0] < 0 || result[1] != 0) err[2] = 1;
@@ -1873,7 +1868,7 @@ void stage_particles_before_solve(System& s) {
     integrator_part1(P, s.I, s.stream);
     spread_charges(P, s.G.q, s.G.qmask, s.G.n, s.G.h, s.stream);
     count_launch();
-    k_charge_check<<<1, 1, 0, s.stream>>>(P.red, s.qtot_d, s.err_d, P.flags);
+    k_charge_check<<<1, 1, 0, s.stream>>>(P.red, s.qtot_d, s.err_d);
 }
 
 void stage_particles_after_solve(System& s) {
@@ -1887,7 +1882,7 @@ void stage_particles_after_solve(System& s) {
     integrator_part2(P, s.I, s.stream);
 }
 
-__global__ void k_md_charge_check(const double* red, double* qtot, int* err, const int* flags, double* bad) {
+__global__ void k_md_charge_check(const double* red, double* qtot, int* err, double* bad) {
     const double q = red[0];
     if (fabs(*qtot - q) > 1e-6 && !err[0]) {  // solver_md.c:98-102, first failing step kept
         err[0] = 1;
@@ -1895,7 +1890,6 @@ __global__ void k_md_charge_check(const double* red, double* qtot, int* err, con
         bad[1] = q;
     }
     *qtot = q;
-    if (flags[0]) err[1] = 1;
 }
 
 // solver_md_step on a Poisson grid without host round trips: per step integrator part 1,
@@ -1913,7 +1907,7 @@ int md_steps_deferred(System& s, int n_steps) {
         integrator_part1(P, s.I, s.stream);
         spread_charges(P, G.q, G.qmask, G.n, G.h, s.stream);
         count_launch();
-        k_md_charge_check<<<1, 1, 0, s.stream>>>(P.red, s.qtot_d, s.err_d, P.flags, bad);
+        k_md_charge_check<<<1, 1, 0, s.stream>>>(P.red, s.qtot_d, s.err_d, bad);
         MZB_CHECK(cudaEventRecord(s.ev0, s.stream));
         if (G.type == G_FFT) {  // in place, no previous field, no status word
             G.fft.solve(G.q, G.phi(), s.stream);
@@ -1955,7 +1949,6 @@ int md_steps_deferred(System& s, int n_steps) {
     MZB_CHECK(cudaMemcpy(qbad, bad, sizeof(qbad), cudaMemcpyDeviceToHost));
     MZB_CHECK(cudaEventElapsedTime(&s.last_solve_ms, s.ev0, s.ev1));
     s.last_solve_iters = s.result_h[0];
-    if (err[1]) fatal("charge spreading: more than 1024 ions reach one 2x8x32 grid tile");
     if (err[0]) {
         printf("Charge conservation error: q_tot = %.6f, q_tot_loc = %.6f\n", qbad[0], qbad[1]);
         exit(1);
@@ -2099,7 +2092,6 @@ int batch_end(std::vector<System*>& ss, const int* handles, int nclass = 1) {
         MZB_CHECK(cudaMemcpy(err, s.err_d, sizeof(err), cudaMemcpyDeviceToHost));
         MZB_CHECK(cudaMemcpy(&q, s.qtot_d, sizeof(double), cudaMemcpyDeviceToHost));
         MZB_CHECK(cudaMemcpy(&s.I.ocalls, s.I.ocalls_d, sizeof(uint64_t), cudaMemcpyDeviceToHost));
-        if (err[1]) fatal("charge spreading: more than 1024 ions reach one 2x8x32 grid tile");
         if (err[0]) {
             printf("Charge conservation error in system %d: q_tot = %.6f\n", handles[r], s.q_tot);
             exit(1);

@@ -300,7 +300,8 @@ __device__ __forceinline__ bool in_stencil(int g, int b, int n) {
 // warps): gather the ions whose stencil can reach the tile (base cell in this tile or the
 // 7 tiles below it for CIC, whose +1 corners reach up; in the 27 tiles around it for the
 // splines, whose offsets run -1..2), sort them by
-// ion index, and let every lane sum the contributions of its TI x TJ points (one k column)
+// ion index (beyond kTileCap candidates, take them in the same order by repeated warp
+// minima over the source tiles' lists instead), and let every lane sum the contributions of its TI x TJ points (one k column)
 // over those ions in ascending ion order -- for each point the order of the reference's
 // serial scatter (charges.c:123-141), with the same weight expression -- then write the
 // tile, zeros included, 32 consecutive k per store. q is written once; no atomics touch
@@ -317,12 +318,15 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) k_spread_tiles(ParticleDev 
     __shared__ double spos_all[kSpreadWarps][kSpreadStage][4];  // x, y, z, charge (rank order)
     __shared__ int sbase_all[kSpreadWarps][kSpreadStage][3];
     __shared__ int srcs_all[kSpreadWarps][32];
+    __shared__ int lfirst_all[kSpreadWarps][32], lcnt_all[kSpreadWarps][32];  // source lists (overflow path)
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int* cand = cand_all[w];
     int* sorted = sorted_all[w];
     double (*spos)[4] = spos_all[w];
     int (*sbase)[3] = sbase_all[w];
     int* srcs = srcs_all[w];
+    int* lfirst = lfirst_all[w];
+    int* lcnt = lcnt_all[w];
     const double L = n * h;
     const long n2 = (long)n * n;
     const long nwarps = (long)gridDim.x * kSpreadWarps;
@@ -366,9 +370,44 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) k_spread_tiles(ParticleDev 
         for (int a = 0; a < kTileI; a++)
 #pragma unroll
             for (int r = 0; r < kTileJ; r++) acc[a][r] = 0.0;
-        if (nc > kTileCap) {
-            if (lane == 0) atomicOr(&P.flags[0], 1);
-        } else {
+        // one round: lane l stages ion p (or nothing, p < 0), then every lane adds the
+        // round's cn ions, in lane order, to its points
+        auto stage_and_add = [&](int p, int cn) {
+            if (p >= 0) {
+                spos[lane][0] = P.pos[3 * p];
+                spos[lane][1] = P.pos[3 * p + 1];
+                spos[lane][2] = P.pos[3 * p + 2];
+                spos[lane][3] = P.chg[p];
+                sbase[lane][0] = P.base[3 * p];
+                sbase[lane][1] = P.base[3 * p + 1];
+                sbase[lane][2] = P.base[3 * p + 2];
+            }
+            __syncwarp();
+            if (k < n) {
+                for (int x = 0; x < cn; x++) {
+                    if (!in_stencil<CAS>(k, sbase[x][2], n)) continue;
+                    const double zk = w_cas<CAS>(spos[x][2] - k * h, L, h);
+                    const double cq = spos[x][3];
+#pragma unroll
+                    for (int a = 0; a < kTileI; a++) {
+                        const int i = i0 + a;
+                        if (i >= n || !in_stencil<CAS>(i, sbase[x][0], n)) continue;
+                        const double wx = w_cas<CAS>(spos[x][0] - i * h, L, h);
+#pragma unroll
+                        for (int r = 0; r < kTileJ; r++) {
+                            const int j = j0 + r;
+                            if (j < n && in_stencil<CAS>(j, sbase[x][1], n)) {
+                                double wgt = wx * w_cas<CAS>(spos[x][1] - j * h, L, h);
+                                wgt = wgt * zk;
+                                acc[a][r] += cq * wgt;
+                            }
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+        };
+        if (nc <= kTileCap) {
             for (int x = 0; x < cnt; x++) cand[incl - cnt + x] = P.tile_ions[first + x];
             __syncwarp();
             for (int x = lane; x < nc; x += 32) {
@@ -380,40 +419,34 @@ __global__ void __launch_bounds__(kSpreadWarps * 32) k_spread_tiles(ParticleDev 
             __syncwarp();
             for (int c0 = 0; c0 < nc; c0 += kSpreadStage) {
                 const int cn = min(kSpreadStage, nc - c0);
-                if (lane < cn) {
-                    const int p = sorted[c0 + lane];
-                    spos[lane][0] = P.pos[3 * p];
-                    spos[lane][1] = P.pos[3 * p + 1];
-                    spos[lane][2] = P.pos[3 * p + 2];
-                    spos[lane][3] = P.chg[p];
-                    sbase[lane][0] = P.base[3 * p];
-                    sbase[lane][1] = P.base[3 * p + 1];
-                    sbase[lane][2] = P.base[3 * p + 2];
-                }
-                __syncwarp();
-                if (k < n) {
-                    for (int x = 0; x < cn; x++) {
-                        if (!in_stencil<CAS>(k, sbase[x][2], n)) continue;
-                        const double zk = w_cas<CAS>(spos[x][2] - k * h, L, h);
-                        const double cq = spos[x][3];
-#pragma unroll
-                        for (int a = 0; a < kTileI; a++) {
-                            const int i = i0 + a;
-                            if (i >= n || !in_stencil<CAS>(i, sbase[x][0], n)) continue;
-                            const double wx = w_cas<CAS>(spos[x][0] - i * h, L, h);
-#pragma unroll
-                            for (int r = 0; r < kTileJ; r++) {
-                                const int j = j0 + r;
-                                if (j < n && in_stencil<CAS>(j, sbase[x][1], n)) {
-                                    double wgt = wx * w_cas<CAS>(spos[x][1] - j * h, L, h);
-                                    wgt = wgt * zk;
-                                    acc[a][r] += cq * wgt;
-                                }
-                            }
+                stage_and_add(lane < cn ? sorted[c0 + lane] : -1, cn);
+            }
+        } else {
+            // more candidates than the shared lists hold (crowded ions, or small grids
+            // whose 27 source tiles cover much of the box): the same rounds in the same
+            // ascending ion order, each ion found as the warp minimum of the source lists
+            // above the last one taken (an ion lies in one tile, so the indices differ)
+            lfirst[lane] = first;
+            lcnt[lane] = cnt;
+            __syncwarp();
+            int last = -1;
+            for (int c0 = 0; c0 < nc; c0 += kSpreadStage) {
+                const int cn = min(kSpreadStage, nc - c0);
+                int mine = -1;
+                for (int t = 0; t < cn; t++) {
+                    int best = INT_MAX;
+                    for (int src = 0; src < NSRC; src++) {
+                        const int f = lfirst[src], c = lcnt[src];
+                        for (int x = lane; x < c; x += 32) {
+                            const int id = P.tile_ions[f + x];
+                            if (id > last && id < best) best = id;
                         }
                     }
+                    best = __reduce_min_sync(0xffffffffu, best);
+                    if (lane == t) mine = best;
+                    last = best;
                 }
-                __syncwarp();
+                stage_and_add(mine, cn);
             }
         }
         if (k < n) {
@@ -1140,7 +1173,6 @@ MZB_TABLE_KERNEL(kt_qchk, 32, if (threadIdx.x == 0) {
     const double q = a.P.red[0];
     if (fabs(*a.qtot - q) > 1e-6) a.err[0] = 1;
     *a.qtot = q;
-    if (a.P.flags[0]) a.err[1] = 1;
 })
 MZB_TABLE_KERNEL(kt_schk, 32, if (threadIdx.x == 0 && (a.result[0] < 0 || a.result[1] != 0)) a.err[2] = 1)
 MZB_TABLE_KERNEL(kt_ff, 128, k_field_forces_body<CAS_CIC>(a.P, a.phi, a.n, a.h, b))

@@ -12,7 +12,7 @@ namespace mzb {
 // points per lane); TI >= 2 so the splines' -1..2 stencils reach at most one tile either
 // way.
 constexpr int kTileI = 2, kTileJ = 8, kTileK = 32;
-constexpr int kTileCap = 1024;  // candidate ions one tile's warp can hold (see spread_tiles)
+constexpr int kTileCap = 1024;  // candidate ions one tile's warp sorts in shared memory (more take a slower path)
 
 // Charge assignment schemes (particles.c:28): CIC (8 points), quadratic and cubic
 // B-splines (4 x 4 x 4 = 64 points, offsets -1..2 around floor(pos/h)).
@@ -84,7 +84,7 @@ struct ParticleDev {
 
     // scalars
     double* red = nullptr;           // reduction outputs (device)
-    int* flags = nullptr;            // [0] spread overflow, [1] bad cell index
+    int* flags = nullptr;            // [0] unused, [1] a coordinate outside [0, L) (cell clamping)
     double* partial = nullptr;       // block partials
 };
 
@@ -144,7 +144,7 @@ struct StageArgs {
     int q_sparse = 1;           // q holds only the CIC corners of the ions' base cells (else cleared whole)
     const double* phi = nullptr;  // the field the step's solve writes
     double* qtot = nullptr;       // device charge total of the last step
-    int* err = nullptr;           // device error words ([0] charge drift, [1] spread overflow, [2] solve)
+    int* err = nullptr;           // device error words ([0] charge drift, [2] solve failure)
     const int* result = nullptr;  // the solve's result words
     GridBarrier* bar = nullptr;   // the solve team's barrier (zeroed at the start of the step)
 };

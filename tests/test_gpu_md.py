@@ -327,6 +327,49 @@ def test_spline_kernels(prod, oracle_lib, cas):
 
 
 @pytest.mark.parametrize("cas", ["SPL_QUADR", "SPL_CUBIC"])
+def test_spline_crowded_tile(prod, oracle_lib, cas):
+    """More than 1024 ions reach one 2 x 8 x 32 spreading tile (1100 ions packed around
+    the box corner, wrapping across it): the tile kernel takes its slower path, which adds
+    the ions in the same ascending order, so q stays bit-exact for the quadratic spline
+    and within 1e-14 for the cubic one, and the field forces likewise."""
+    code = {"SPL_QUADR": 1, "SPL_CUBIC": 2}[cas]
+    s = make_system(10, 64, density=1.329, seed=37)
+    rng = np.random.default_rng(5)
+    box = np.array([1.5, 5.0, 20.0]) * s.h
+    s.pos[:1100] = np.mod(rng.uniform(-box, box, (1100, 3)), s.L)
+    s.pos[:1100] = np.where(s.pos[:1100] >= s.L, 0.0, s.pos[:1100])
+    prod.solver_initialize()
+    maps = prod.type_maps()
+    prod.solver_initialize_grid(s.n_grid, s.L, s.h, 1e-6, 1.0, 1.0, maps["method"]["LCG"], 0)
+    prod.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, 0, code, s.types, s.pos, s.vel,
+                                     s.mass, s.charges, s.pot_params)
+    prod.solver_initialize_integrator(s.n_ions, 1.0, 1200.0, 0.0, 1, 0)
+    try:
+        assert prod.solver_update_charges() == 0
+        q = np.empty((64, 64, 64))
+        prod.get_q(q)
+        qo = np.empty_like(q)
+        oracle_lib.orc_spread_scheme(s.pos, s.charges, s.n_ions, 64, s.h, code, qo, None)
+        if code == 1:
+            assert np.array_equal(q, qo)
+        else:
+            assert rel(q, qo) < 1e-14
+        phi = np.random.default_rng(6).standard_normal((64, 64, 64))
+        prod.solver_set_field(phi)
+        prod.solver_compute_forces_elec()
+        fe = np.empty((s.n_ions, 3))
+        prod.get_fcs_elec(fe)
+        feo = np.empty_like(fe)
+        oracle_lib.orc_force_scheme(phi, s.charges, s.pos, s.n_ions, 64, s.h, code, feo)
+        if code == 1:
+            assert np.array_equal(fe, feo)
+        else:
+            assert rel(fe, feo) < 1e-14
+    finally:
+        prod.solver_finalize()
+
+
+@pytest.mark.parametrize("cas", ["SPL_QUADR", "SPL_CUBIC"])
 def test_spline_md_250(prod, orc, cas):
     run_pair(prod, orc, make_system(5, 64, seed=13), 4, method="LCG", tol=1e-7, cas=cas)
 
