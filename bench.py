@@ -18,7 +18,7 @@ Forms, each from the same initial state (`modes` in the JSON line):
                 within 1e-10 of the CPU oracle per step;
   fp64_multigrid_ref, fp64_maze_multigrid_ref : the reference's MULTIGRID and
                 MAZE-MULTIGRID algorithms (2-level V-cycle, coarse CG) in FP64;
-  fp64_mg     : the fair FP64 comparator of fp32_refine -- the same V(2,2) multigrid and
+  fp64_mg     : the fair FP64 comparator of fp32_refine -- the same V(3,2) multigrid and
                 refinement loop with every value in FP64;
   fft         : the reference's FFT Poisson method (a spectral discretisation, so it is
                 timed beside the others but not counted among the FP64 comparators).
@@ -108,33 +108,41 @@ def fft_coarse_level(n):
     return m if n % 2 == 0 and m in (32, 64, 128) else None
 
 
-def mixed_solve_bytes(n, refinements, nu1=2, nu2=2, small_n=16):
+def mixed_solve_bytes(n, refinements, nu1=3, nu2=2, small_n=16, w0=None):
     """Algorithmic HBM bytes of one mixed solve (MD update, LCG form) that took
-    `refinements` V-cycles, with 8 B per FP64 and 4 B per FP32 value, per grid point:
+    `refinements` V(nu1, nu2)-cycles (the library's default V(3,2)), with 8 B per FP64 value,
+    4 B per FP32 value of the coarser levels and w0 B per value of level 0's correction,
+    rhs and residual (2: FP16, which the library takes at n = 256; else 4), per grid point:
       set-up          read q, phi_old; write y, rhs, phi                     40 B
-      residual check  read X, rhs; write FP32 rhs, red e        22 B, refinements + 1 times
-      update          read X, e; write X                                     20 B
+      residual check  read X, q; write level-0 rhs, red e      16 + 1.5 w0 B, refinements + 1 times
+      update          read X, e; write X                             16 + w0 B
       V-cycle, per point of each level swept by the whole grid, with the red-black split
       layout (a half-sweep reads the other colour, this colour's rhs and writes this
-      colour: 3 x 4 B x 1/2):
-        2 nu1 - 1 + 2 nu2 half-sweeps                                   6 B each
-        red residual: read both colours of x, red rhs; write red r       8 B
-        restriction (13 red taps): read red r; write coarse rhs, x       2 + 1 B
-        prolongation into black points: read coarse x; read/write black  0.5 + 4 B
+      colour: 3 x w x 1/2):
+        2 nu1 - 1 + 2 nu2 half-sweeps                              1.5 w each
+        red residual: read both colours of x, red rhs; write red r       2 w
+        restriction (13 red taps): read red r; write coarse rhs, x     w / 2 + 2 w_c / 8
+        prolongation into black points: read coarse x; read/write black  w_c / 8 + w
+      (w the level's value size, w_c the next level's, 4 B)
       coarse level of m points per side solved by FFT (fft_coarse_level): read its rhs,
         write x (4 B each), the half spectrum m^2 (m/2 + 1) complex (8 B) written by the
         first pass, read and written by the second, read by the third:  8 m^3 + 32 m^2 (m/2 + 1)
     Otherwise levels of at most small_n^3 points are solved in shared memory or from a
     staged Green's function and move no HBM bytes."""
+    if w0 is None:
+        w0 = 2 if n == 256 else 4
     P = n ** 3
-    per_level = (2 * nu1 - 1 + 2 * nu2) * 6 + 8 + 3 + 4.5
+
+    def per_level(w):
+        return (2 * nu1 - 1 + 2 * nu2) * 1.5 * w + 2 * w + (w / 2 + 1) + (0.5 + w)
+
     m = fft_coarse_level(n)
     if m is not None:
-        vcycle = P * per_level + 8 * m ** 3 + 32 * m * m * (m // 2 + 1)
+        vcycle = P * per_level(w0) + 8 * m ** 3 + 32 * m * m * (m // 2 + 1)
     else:
         grid_levels = [k for k in level_sizes(n) if k > small_n]
-        vcycle = sum(k ** 3 * per_level for k in grid_levels)
-    return P * 40 + (refinements + 1) * P * 22 + refinements * (vcycle + P * 20)
+        vcycle = sum(k ** 3 * per_level(w0 if k == n else 4) for k in grid_levels)
+    return P * 40 + (refinements + 1) * P * (16 + 1.5 * w0) + refinements * (vcycle + P * (16 + w0))
 
 
 class ClockSampler:
@@ -212,7 +220,7 @@ FORM_DTYPE = {
     "fp64": "f64 (the reference's LCG algorithm)",
     "fp64_multigrid_ref": "f64 (the reference's MULTIGRID algorithm)",
     "fp64_maze_multigrid_ref": "f64 (the reference's MAZE-MULTIGRID algorithm)",
-    "fp64_mg": "f64 (the V(2,2) multigrid + refinement loop of fp32_refine, every value in FP64)",
+    "fp64_mg": "f64 (the V(3,2) multigrid + refinement loop of fp32_refine, every value in FP64)",
     "fft": "f64 (the reference's FFT Poisson solve, continuous k^2; hand-written shared-memory FFT)",
 }
 

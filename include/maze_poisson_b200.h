@@ -69,6 +69,13 @@ int mzb_get_precision(void);      /* precision in effect for the current grid */
 int mzb_set_mixed_plan(int plan);
 int mzb_get_mixed_plan(void);     /* the level solved by FFT (1, 2) or 0 when none is */
 
+/* red-black Gauss-Seidel sweeps before (nu1) and after (nu2) the coarse correction in the
+   V-cycle of the current grid's multigrid forms (precision 1 and 2); 1 .. 16 each, default
+   V(3,2); returns -1 outside that range. No counterpart in the reference (its multigrid,
+   library/src/multigrid.c:111-124, takes 3 sweeps on 2 levels). */
+int mzb_set_mixed_sweeps(int nu1, int nu2);
+void mzb_get_mixed_sweeps(int *nu1, int *nu2);
+
 /* state accessors of the current system */
 void mzb_get_cic_neighbors(int64_t *out);  /* (n_p,8,3) CIC corners, particles.c:297-346 */
 void mzb_set_cell_grid(int nc);            /* linked cells per side for the pair forces */

@@ -121,6 +121,8 @@ EXTENSION_SYMBOLS = {
     "mzb_get_precision": (_c.c_int, []),
     "mzb_set_mixed_plan": (_c.c_int, [_c.c_int]),
     "mzb_get_mixed_plan": (_c.c_int, []),
+    "mzb_set_mixed_sweeps": (_c.c_int, [_c.c_int, _c.c_int]),
+    "mzb_get_mixed_sweeps": (None, [_c.POINTER(_c.c_int), _c.POINTER(_c.c_int)]),
     "mzb_conj_grad_noalloc": (_c.c_int, [_c.c_void_p, _c.c_void_p, _c.c_void_p, _c.c_double, _c.c_int,
                                          _c.c_int, _c.c_void_p]),
     "mzb_system_create": (_c.c_int, []),

@@ -102,7 +102,12 @@ struct GridState {
     bool coarse_team = false; // the coarsest level (n <= kMixedTeamDirectN) is solved by the whole team
     bool coarse_fft = false;  // the coarsest level (mixed_fft_coarse_ok) is solved by the team by FFT
     void* lev_spec = nullptr; // its half spectrum
+    double* lev_hint = nullptr;  // the last solve's first residual max (scale of an FP16 level 0)
     int plan = -1;            // first level that may be solved by FFT (mzb_set_mixed_plan; -1: default)
+    // red-black GS sweeps before / after the coarse correction of the multigrid forms
+    // (mzb_set_mixed_sweeps): V(3,2) needs one refinement fewer than V(2,2) at tol 1e-8 to
+    // 1e-10 on 64^3 to 256^3 grids, for less time in all
+    int nu1 = 3, nu2 = 2;
     double batch_cost = 1.0;  // batched-solve time per grid point relative to other sizes (mzb_batch_autotune)
     int lev_plan = -1;        // the plan the current levels were built for
     double* bj_inv = nullptr;  // block-Jacobi block inverse (1000 x 1000) on BLOCKJACOBI grids
@@ -184,6 +189,8 @@ void free_grid(GridState& G) {
     G.lev_g = nullptr;
     dev_free(G.lev_spec);
     G.lev_spec = nullptr;
+    dev_free(G.lev_hint);
+    G.lev_hint = nullptr;
     G.nlev = 0;
     G.coarse_team = false;
     G.coarse_fft = false;
@@ -209,6 +216,8 @@ void free_mixed_levels(GridState& G) {
     G.lev_g = nullptr;
     dev_free(G.lev_spec);
     G.lev_spec = nullptr;
+    dev_free(G.lev_hint);
+    G.lev_hint = nullptr;
     G.nlev = 0;
     G.coarse_team = false;
     G.coarse_fft = false;
@@ -264,6 +273,8 @@ void ensure_mixed_levels(GridState& G) {
     }
     const int nc = G.lev_n[G.nlev - 1];
     if (G.coarse_fft) G.lev_spec = dev_alloc((size_t)nc * nc * (nc / 2 + 1) * 2 * w);
+    G.lev_hint = static_cast<double*>(dev_alloc(sizeof(double)));
+    zero_fill(G.lev_hint, sizeof(double));
     if (G.coarse_team || (nc <= kMixedDirectN && mixed_small_level(G.nlev, G.lev_n) < G.nlev)) {
         const size_t N = (size_t)nc * nc * nc;
         G.lev_g = dev_alloc(N * w);
@@ -409,8 +420,8 @@ MixedArgs mixed_args(System& s, int prog, double cst) {
     m.tol = G.mixed_tol > 0 ? G.mixed_tol : G.tol;
     m.c = cst;
     m.max_outer = 100;
-    m.nu1 = 2;
-    m.nu2 = 2;
+    m.nu1 = G.nu1;
+    m.nu2 = G.nu2;
     m.coarse_sweeps = 16;
     m.nlev = G.nlev;
     m.lsmall = G.coarse_team || G.coarse_fft ? G.nlev : mixed_small_level(G.nlev, G.lev_n);
@@ -419,6 +430,12 @@ MixedArgs mixed_args(System& s, int prog, double cst) {
 
     m.coarse_spec = G.lev_spec;
     m.fp64 = G.lev_fp64;
+    // FP16 storage of level 0 at 256^3, where the level-0 passes stream from HBM (at 128^3
+    // they run from L2 and FP16 measured slower). The correction only has to cut the
+    // residual by the V-cycle's factor each refinement; the FP64 residual and update keep
+    // the solution's accuracy. The batched solve keeps FP32 (mixed_batch_kernel).
+    m.level0_fp16 = !m.fp64 && G.n == 256 ? 1 : 0;
+    m.scale_hint = G.lev_hint;
     m.coarse_team = G.coarse_team ? 1 : 0;
     for (int l = 0; l < G.nlev; l++) {
         m.lev_n[l] = G.lev_n[l];
@@ -1630,6 +1647,22 @@ int mzb_get_mixed_plan(void) {
     if (!(G.precision >= 1 && mixed_supported(G))) return 0;
     ensure_mixed_levels(G);
     return G.coarse_fft ? G.nlev - 1 : 0;
+}
+
+// Red-black Gauss-Seidel sweeps before (nu1) and after (nu2) the coarse correction of the
+// current grid's multigrid forms; 1 .. 16 each.
+int mzb_set_mixed_sweeps(int nu1, int nu2) {
+    if (nu1 < 1 || nu1 > 16 || nu2 < 1 || nu2 > 16) return -1;
+    GridState& G = grid();
+    touch(sys());
+    G.nu1 = nu1;
+    G.nu2 = nu2;
+    return 0;
+}
+void mzb_get_mixed_sweeps(int* nu1, int* nu2) {
+    GridState& G = grid();
+    if (nu1) *nu1 = G.nu1;
+    if (nu2) *nu2 = G.nu2;
 }
 
 // The CUDA stream all work of the current system is queued on (for callers that time

@@ -29,6 +29,9 @@
 // pass that writes the level's right-hand side (the FP64 residual pass, the
 // restrictions), and the sum of the finest correction, whose mean is removed, is taken in
 // the last two half-sweeps instead of by another pass.
+#include <cuda_fp16.h>
+
+#include <type_traits>
 #include <vector>
 
 #include "engine.cuh"
@@ -572,11 +575,49 @@ __device__ __forceinline__ void stv(S* p, const S (&v)[V]) {
 #pragma unroll
         for (int e = 0; e < V; e += 2) *reinterpret_cast<double2*>(p + e) = make_double2(v[e], v[e + 1]);
 }
+// FP16 storage with FP32 arithmetic (level 0 of the mixed form): V = 4 values per 8-byte
+// access, V = 2 per 4-byte access; stores round to nearest.
+template <int V>
+__device__ __forceinline__ void ldv(const __half* p, float (&v)[V]) {
+    static_assert(V == 2 || V == 4, "FP16 rows take 2 or 4 values per lane");
+    if constexpr (V == 4) {
+        const uint2 t = *reinterpret_cast<const uint2*>(p);
+        const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&t.x));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&t.y));
+        v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+    } else {
+        const float2 a = __half22float2(*reinterpret_cast<const __half2*>(p));
+        v[0] = a.x; v[1] = a.y;
+    }
+}
+template <int V>
+__device__ __forceinline__ void stv(__half* p, const float (&v)[V]) {
+    static_assert(V == 2 || V == 4, "FP16 rows take 2 or 4 values per lane");
+    if constexpr (V == 4) {
+        const __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
+        uint2 t;
+        t.x = *reinterpret_cast<const unsigned*>(&a);
+        t.y = *reinterpret_cast<const unsigned*>(&b);
+        *reinterpret_cast<uint2*>(p) = t;
+    } else {
+        *reinterpret_cast<__half2*>(p) = __floats2half2_rn(v[0], v[1]);
+    }
+}
+// arithmetic type of a storage type, and scalar conversions
+template <class T> struct Calc { using type = T; };
+template <> struct Calc<__half> { using type = float; };
+__device__ __forceinline__ float to_calc(__half v) { return __half2float(v); }
+__device__ __forceinline__ float to_calc(float v) { return v; }
+__device__ __forceinline__ double to_calc(double v) { return v; }
+template <class T> __device__ __forceinline__ T from_calc(typename Calc<T>::type v) {
+    if constexpr (std::is_same<T, __half>::value) return __float2half_rn(v);
+    else return v;
+}
 
 // sum of the six other-colour neighbours of the lane's V points in row o (s as in
 // split_nb_sums), from full-row vector loads
-template <int V, class S>
-__device__ __forceinline__ void vec_nb_sums(const S* xo, const Rows& o, int s, S (&sum)[V]) {
+template <int V, class T, class S>
+__device__ __forceinline__ void vec_nb_sums(const T* xo, const Rows& o, int s, S (&sum)[V]) {
     const int lane = threadIdx.x & 31;
     S a0[V], a1[V], a2[V], a3[V], cen[V];
     ldv<V>(xo + o.im + V * lane, a0);
@@ -594,13 +635,14 @@ __device__ __forceinline__ void vec_nb_sums(const S* xo, const Rows& o, int s, S
     }
 }
 
-template <int V, class S>
-__device__ void split_gs_vec(const Team& tm, int n, int c, const S* b, S* x, double* acc) {
+template <int V, class T>
+__device__ void split_gs_vec(const Team& tm, int n, int c, const T* b, T* x, double* acc) {
+    using S = typename Calc<T>::type;
     const int lane = threadIdx.x & 31, h = n >> 1;
     const int hp = h * n * n;
-    const S* xo = x + (1 - c) * hp;
-    S* xc = x + c * hp;
-    const S* bc = b + c * hp;
+    const T* xo = x + (1 - c) * hp;
+    T* xc = x + c * hp;
+    const T* bc = b + c * hp;
     double s_acc = 0.0;
     grid_rows(tm, n, [&](int i, int j) {
         const Rows o = rows_of(n, i, j);
@@ -609,7 +651,7 @@ __device__ void split_gs_vec(const Team& tm, int n, int c, const S* b, S* x, dou
         vec_nb_sums<V>(xo, o, (i + j + c) & 1, sum);
 #pragma unroll
         for (int e = 0; e < V; e++) {
-            v[e] = (bv[e] - sum[e]) * neg_sixth<S>();
+            v[e] = to_calc(from_calc<T>((bv[e] - sum[e]) * neg_sixth<S>()));  // the value stored
             s_acc += (double)v[e];
         }
         stv<V>(xc + o.c + V * lane, v);
@@ -617,11 +659,12 @@ __device__ void split_gs_vec(const Team& tm, int n, int c, const S* b, S* x, dou
     if (acc != nullptr) *acc += s_acc;
 }
 
-template <int V, class S>
-__device__ void split_resid_red_vec(const Team& tm, int n, const S* b, const S* x, S* r) {
+template <int V, class T>
+__device__ void split_resid_red_vec(const Team& tm, int n, const T* b, const T* x, T* r) {
+    using S = typename Calc<T>::type;
     const int lane = threadIdx.x & 31, h = n >> 1;
     const int hp = h * n * n;
-    const S* x1 = x + hp;
+    const T* x1 = x + hp;
     grid_rows(tm, n, [&](int i, int j) {
         const Rows o = rows_of(n, i, j);
         S bv[V], xv[V], sum[V], v[V];
@@ -635,8 +678,8 @@ __device__ void split_resid_red_vec(const Team& tm, int n, const S* b, const S* 
 }
 
 // restriction with coarse rows of nc = h = 32 V points: lane l computes K = V l .. V l + V - 1
-template <int V, class S>
-__device__ void split_restrict_vec(const Team& tm, int n, const S* r, S* bc, S* xc) {
+template <int V, class T, class S>
+__device__ void split_restrict_vec(const Team& tm, int n, const T* r, S* bc, S* xc) {
     const int lane = threadIdx.x & 31, nc = n / 2, hc = nc >> 1, h = n >> 1;
     const int hpc = hc * nc * nc;
     grid_rows(tm, nc, [&](int I, int J) {
@@ -687,11 +730,11 @@ __device__ void split_restrict_vec(const Team& tm, int n, const S* r, S* bc, S* 
     });
 }
 
-template <int V, class S>
-__device__ void split_prolong_black_vec(const Team& tm, int n, const S* xc, S* x) {
+template <int V, class S, class T>
+__device__ void split_prolong_black_vec(const Team& tm, int n, const S* xc, T* x) {
     const int lane = threadIdx.x & 31, h = n >> 1, nc = n / 2, hc = nc >> 1;
     const int hp = h * n * n, hpc = hc * nc * nc;
-    S* x1 = x + hp;
+    T* x1 = x + hp;
     grid_rows(tm, n, [&](int i, int j) {
         const int s1 = (i + j + 1) & 1;
         const int ci = i >> 1, cj = j >> 1;
@@ -822,33 +865,54 @@ __device__ void split_resid_red_rows(const Team& tm, int n, const S* b, const S*
 
 // dispatch: rows of 128 floats (n = 256) as float4 and of 64 (n = 128) as float2, one row
 // per warp; shorter rows several per warp (n % 8 == 0 as float4, n % 4 == 0 as float2)
+// FP16 storage (level 0 of the mixed form) is taken for n = 256 and 128 only.
 template <class S>
 __device__ __forceinline__ void split_gs(const Team& tm, int n, int c, const S* b, S* x, double* acc) {
-    if (n == 256) split_gs_vec<4>(tm, n, c, b, x, acc);
-    else if (n == 128) split_gs_vec<2>(tm, n, c, b, x, acc);
-    else if (n < 256 && n % 8 == 0) split_gs_rows<4>(tm, n, c, b, x, acc);
-    else if (n < 128 && n % 4 == 0) split_gs_rows<2>(tm, n, c, b, x, acc);
-    else split_gs_scalar(tm, n, c, b, x, acc);
+    if constexpr (std::is_same<S, __half>::value) {
+        if (n == 256) split_gs_vec<4>(tm, n, c, b, x, acc);
+        else split_gs_vec<2>(tm, n, c, b, x, acc);
+    } else {
+        if (n == 256) split_gs_vec<4>(tm, n, c, b, x, acc);
+        else if (n == 128) split_gs_vec<2>(tm, n, c, b, x, acc);
+        else if (n < 256 && n % 8 == 0) split_gs_rows<4>(tm, n, c, b, x, acc);
+        else if (n < 128 && n % 4 == 0) split_gs_rows<2>(tm, n, c, b, x, acc);
+        else split_gs_scalar(tm, n, c, b, x, acc);
+    }
 }
 template <class S>
 __device__ __forceinline__ void split_resid_red(const Team& tm, int n, const S* b, const S* x, S* r) {
-    if (n == 256) split_resid_red_vec<4>(tm, n, b, x, r);
-    else if (n == 128) split_resid_red_vec<2>(tm, n, b, x, r);
-    else if (n < 256 && n % 8 == 0) split_resid_red_rows<4>(tm, n, b, x, r);
-    else if (n < 128 && n % 4 == 0) split_resid_red_rows<2>(tm, n, b, x, r);
-    else split_resid_red_scalar(tm, n, b, x, r);
+    if constexpr (std::is_same<S, __half>::value) {
+        if (n == 256) split_resid_red_vec<4>(tm, n, b, x, r);
+        else split_resid_red_vec<2>(tm, n, b, x, r);
+    } else {
+        if (n == 256) split_resid_red_vec<4>(tm, n, b, x, r);
+        else if (n == 128) split_resid_red_vec<2>(tm, n, b, x, r);
+        else if (n < 256 && n % 8 == 0) split_resid_red_rows<4>(tm, n, b, x, r);
+        else if (n < 128 && n % 4 == 0) split_resid_red_rows<2>(tm, n, b, x, r);
+        else split_resid_red_scalar(tm, n, b, x, r);
+    }
 }
-template <class S>
-__device__ __forceinline__ void split_restrict(const Team& tm, int n, const S* r, S* bc, S* xc) {
-    if (n == 256) split_restrict_vec<4>(tm, n, r, bc, xc);
-    else if (n == 128) split_restrict_vec<2>(tm, n, r, bc, xc);
-    else split_restrict_scalar(tm, n, r, bc, xc);
+template <class T, class S>
+__device__ __forceinline__ void split_restrict(const Team& tm, int n, const T* r, S* bc, S* xc) {
+    if constexpr (std::is_same<T, __half>::value) {
+        if (n == 256) split_restrict_vec<4>(tm, n, r, bc, xc);
+        else split_restrict_vec<2>(tm, n, r, bc, xc);
+    } else {
+        if (n == 256) split_restrict_vec<4>(tm, n, r, bc, xc);
+        else if (n == 128) split_restrict_vec<2>(tm, n, r, bc, xc);
+        else split_restrict_scalar(tm, n, r, bc, xc);
+    }
 }
-template <class S>
-__device__ __forceinline__ void split_prolong_black(const Team& tm, int n, const S* xc, S* x) {
-    if (n == 256) split_prolong_black_vec<4>(tm, n, xc, x);
-    else if (n == 128) split_prolong_black_vec<2>(tm, n, xc, x);
-    else split_prolong_black_scalar(tm, n, xc, x);
+template <class S, class T>
+__device__ __forceinline__ void split_prolong_black(const Team& tm, int n, const S* xc, T* x) {
+    if constexpr (std::is_same<T, __half>::value) {
+        if (n == 256) split_prolong_black_vec<4>(tm, n, xc, x);
+        else split_prolong_black_vec<2>(tm, n, xc, x);
+    } else {
+        if (n == 256) split_prolong_black_vec<4>(tm, n, xc, x);
+        else if (n == 128) split_prolong_black_vec<2>(tm, n, xc, x);
+        else split_prolong_black_scalar(tm, n, xc, x);
+    }
 }
 
 // ---- the shared-memory part of the V-cycle (CTA 0) ----
@@ -1448,41 +1512,49 @@ __device__ bool team_fft(const MixedArgs& a, const Team& tm, unsigned& epoch, S*
 // Grid-wide red-black sweeps of level l: `half_sweeps` colours starting at first_colour,
 // a grid barrier after each except (when skip_last_barrier) the last. When esum is not
 // null the values written in the last two half-sweeps are summed into it.
-template <class S>
-__device__ bool grid_smooth(const MixedArgs& a, const Team& tm, int l, S* x, int first_colour, int half_sweeps,
+template <class T>
+__device__ bool grid_smooth(const Team& tm, int n, const T* b, T* x, int first_colour, int half_sweeps,
                             unsigned& epoch, double* esum, bool skip_last_barrier) {
     for (int h = 0; h < half_sweeps; h++) {
-        split_gs(tm, a.lev_n[l], (first_colour + h) & 1, lev_b<S>(a, l), x,
-                 esum != nullptr && h >= half_sweeps - 2 ? esum : nullptr);
+        split_gs(tm, n, (first_colour + h) & 1, b, x, esum != nullptr && h >= half_sweeps - 2 ? esum : nullptr);
         if (h == half_sweeps - 1 && skip_last_barrier) break;
         if (!team_sync(tm, epoch)) return false;
     }
     return true;
 }
 
-// One V-cycle for the correction x0 (level 0's x; r0 is level 0's residual buffer) of rhs
-// lev_b[0], whose first red half-sweep has been done by the residual pass. Ends after
-// the last half-sweep of level 0 without a barrier, with this thread's share of sum(x0)
-// in esum.
-template <class S>
+// One V-cycle for the correction x0 of rhs b0 (level 0; r0 is its residual buffer), whose
+// first red half-sweep has been done by the residual pass. Level 0 is stored as T0 (S, or
+// FP16 for n = 128 and 256 with FP32 levels), the coarser levels as S. Ends after the last
+// half-sweep of level 0 without a barrier, with this thread's share of sum(x0) in esum.
+template <class S, class T0>
 __device__ bool vcycle(const MixedArgs& a, const Team& tm, S* sm, unsigned& epoch, double& esum, int outer,
-                       S* x0, S* r0) {
-    const int L = a.nlev, ls = a.lsmall;
+                       T0* x0, const T0* b0, T0* r0) {
+    const int L = a.nlev, ls = a.lsmall, n0 = a.lev_n[0];
     const int lg = ls < L ? ls : L - 1;  // levels 0..lg-1 are smoothed and restricted on the grid
-    auto X = [&](int l) { return l == 0 ? x0 : lev_x<S>(a, l); };
-    auto R = [&](int l) { return l == 0 ? r0 : lev_r<S>(a, l); };
-    for (int l = 0; l < lg; l++) {
-        if (!grid_smooth(a, tm, l, X(l), 1, 2 * a.nu1 - 1, epoch, nullptr, false)) return false;
-        split_resid_red(tm, a.lev_n[l], lev_b<S>(a, l), X(l), R(l));
+    if (!grid_smooth(tm, n0, b0, x0, 1, 2 * a.nu1 - 1, epoch, nullptr, false)) return false;
+    split_resid_red(tm, n0, b0, x0, r0);
+    if (!team_sync(tm, epoch)) return false;
+    if (1 < ls) {
+        split_restrict(tm, n0, r0, lev_b<S>(a, 1), lev_x<S>(a, 1));
+        if (!team_sync(tm, epoch)) return false;
+    }
+    for (int l = 1; l < lg; l++) {
+        if (!grid_smooth(tm, a.lev_n[l], lev_b<S>(a, l), lev_x<S>(a, l), 1, 2 * a.nu1 - 1, epoch, nullptr, false))
+            return false;
+        split_resid_red(tm, a.lev_n[l], lev_b<S>(a, l), lev_x<S>(a, l), lev_r<S>(a, l));
         if (!team_sync(tm, epoch)) return false;
         if (l + 1 < ls) {
-            split_restrict(tm, a.lev_n[l], R(l), lev_b<S>(a, l + 1), X(l + 1));
+            split_restrict(tm, a.lev_n[l], lev_r<S>(a, l), lev_b<S>(a, l + 1), lev_x<S>(a, l + 1));
             if (!team_sync(tm, epoch)) return false;
         }
     }
     stamp_outer(a, outer, 2);
     if (ls < L) {
-        if (tm.b == 0) small_vcycle(a, sm, R(ls - 1));
+        if (tm.b == 0) {
+            if constexpr (std::is_same<T0, S>::value) small_vcycle(a, sm, ls == 1 ? r0 : lev_r<S>(a, ls - 1));
+            else small_vcycle(a, sm, lev_r<S>(a, ls - 1));  // FP16 level 0 implies ls >= 2
+        }
         if (!team_sync(tm, epoch)) return false;
     } else if (a.coarse_fft) {
         if (!team_fft<S>(a, tm, epoch, sm, L - 1, outer)) return false;
@@ -1490,15 +1562,20 @@ __device__ bool vcycle(const MixedArgs& a, const Team& tm, S* sm, unsigned& epoc
         team_direct(a, tm, sm, L - 1);
         if (!team_sync(tm, epoch)) return false;
     } else {
-        if (!grid_smooth(a, tm, L - 1, X(L - 1), 1, 2 * a.coarse_sweeps - 1, epoch, nullptr, false)) return false;
+        if (!grid_smooth(tm, a.lev_n[L - 1], lev_b<S>(a, L - 1), lev_x<S>(a, L - 1), 1, 2 * a.coarse_sweeps - 1,
+                         epoch, nullptr, false))
+            return false;
     }
     stamp_outer(a, outer, 3);
-    for (int l = lg - 1; l >= 0; l--) {
-        split_prolong_black(tm, a.lev_n[l], X(l + 1), X(l));
+    for (int l = lg - 1; l >= 1; l--) {
+        split_prolong_black(tm, a.lev_n[l], lev_x<S>(a, l + 1), lev_x<S>(a, l));
         if (!team_sync(tm, epoch)) return false;
-        if (!grid_smooth(a, tm, l, X(l), 0, 2 * a.nu2, epoch, l == 0 ? &esum : nullptr, l == 0)) return false;
+        if (!grid_smooth(tm, a.lev_n[l], lev_b<S>(a, l), lev_x<S>(a, l), 0, 2 * a.nu2, epoch, nullptr, false))
+            return false;
     }
-    return true;
+    split_prolong_black(tm, n0, lev_x<S>(a, 1), x0);
+    if (!team_sync(tm, epoch)) return false;
+    return grid_smooth(tm, n0, b0, x0, 0, 2 * a.nu2, epoch, &esum, true);
 }
 
 // FP64 residual r = B - L X written as the FP32 rhs of the inner solve together with that
@@ -1537,10 +1614,13 @@ __device__ __forceinline__ double residual_pass(const Team& tm, const MixedArgs&
 // Vectorised residual pass (n even): a warp covers 64 consecutive k of a row with one
 // double2 per lane (the last chunk of a row shorter when 64 does not divide n, its lanes
 // past the row idle); k - 1 / k + 1 come from the adjacent lane by a shuffle, from memory
-// at the ends of the chunk. Same sums, in the same order, as residual_pass.
-template <int START, bool RHS_Q, class S>
+// at the ends of the chunk. Same sums, in the same order, as residual_pass. The rhs and e
+// are stored as T (FP32, FP64, or FP16 for level 0 of the mixed form) in units of
+// 1 / inv; WRITE false only returns the max |r|.
+template <int START, bool RHS_Q, class T, bool WRITE = true>
 __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedArgs& a, const double* X,
-                                                    const double* Xp, S* e, S* rb) {
+                                                    const double* Xp, T* e, T* rb, double inv) {
+    using S = typename Calc<T>::type;
     const int n = a.n, h = n >> 1, lane = threadIdx.x & 31;
     const int hp = h * n * n;
     double rmax = 0.0;
@@ -1602,13 +1682,15 @@ __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedA
                 r1 = bq.y - (s1 - xc.y * 6.0);
             }
             if (act) {
-                const S rf0 = (S)r0, rf1 = (S)r1;
-                const int p0 = cA * hp + srow + (k >> 1), p1 = (cA ^ 1) * hp + srow + (k >> 1);
-                rb[p0] = rf0;
-                rb[p1] = rf1;
-                // red e only: the first half-sweep (black) writes the black values without reading them
-                if (cA == 0) e[p0] = rf0 * neg_sixth<S>();
-                else e[p1] = rf1 * neg_sixth<S>();
+                if (WRITE) {
+                    const T rf0 = from_calc<T>((S)(r0 * inv)), rf1 = from_calc<T>((S)(r1 * inv));
+                    const int p0 = cA * hp + srow + (k >> 1), p1 = (cA ^ 1) * hp + srow + (k >> 1);
+                    rb[p0] = rf0;
+                    rb[p1] = rf1;
+                    // red e only: the first half-sweep (black) writes the black values without reading them
+                    if (cA == 0) e[p0] = from_calc<T>(to_calc(rf0) * neg_sixth<S>());
+                    else e[p1] = from_calc<T>(to_calc(rf1) * neg_sixth<S>());
+                }
                 rmax = fmax(rmax, fmax(fabs(r0), fabs(r1)));
             }
         }
@@ -1616,17 +1698,31 @@ __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedA
     return rmax;
 }
 
-template <int START, bool RHS_Q, class S>
+template <int START, bool RHS_Q, class T, bool WRITE>
 __device__ __forceinline__ double residual_any(const Team& tm, const MixedArgs& a, const double* X,
-                                               const double* Xp, S* e, S* rb) {
-    if (a.n % 2 == 0) return residual_pass_vec<START, RHS_Q>(tm, a, X, Xp, e, rb);
-    return residual_pass<START, RHS_Q>(tm, a, X, Xp, e, rb);
+                                               const double* Xp, T* e, T* rb, double inv) {
+    if constexpr (std::is_same<T, __half>::value || !WRITE) {  // FP16: n = 128 or 256
+        return residual_pass_vec<START, RHS_Q, T, WRITE>(tm, a, X, Xp, e, rb, inv);
+    } else {
+        if (a.n % 2 == 0) return residual_pass_vec<START, RHS_Q, T, WRITE>(tm, a, X, Xp, e, rb, inv);
+        return residual_pass<START, RHS_Q>(tm, a, X, Xp, e, rb);
+    }
+}
+// the residual pass of refinement start st (rhs c q, or tmp when !rhs_q)
+template <bool WRITE, class T>
+__device__ __forceinline__ double residual_of(const Team& tm, const MixedArgs& a, int st, bool rhs_q,
+                                              const double* X, T* e, T* rb, double inv) {
+    if (st == START_ZERO) return residual_any<START_ZERO, true, T, WRITE>(tm, a, X, a.phi_prev, e, rb, inv);
+    if (st == START_EXTRAP) return residual_any<START_EXTRAP, true, T, WRITE>(tm, a, X, a.phi_prev, e, rb, inv);
+    if (rhs_q) return residual_any<START_X, true, T, WRITE>(tm, a, X, a.phi_prev, e, rb, inv);
+    return residual_any<START_X, false, T, WRITE>(tm, a, X, a.phi_prev, e, rb, inv);
 }
 
-// home = X + (e - emean) with X as residual_pass reads it (0, X[], 2 X[] - phi_prev[]).
-template <int START, class S>
+// home = X + (e - emean) scale with X as residual_pass reads it (0, X[], 2 X[] - phi_prev[])
+// and e stored as T in units of 1 / scale.
+template <int START, class T>
 __device__ __forceinline__ void update_pass(const Team& tm, const MixedArgs& a, const double* X, double* home,
-                                            const S* e, double emean) {
+                                            const T* e, double emean, double scale) {
     const int n = a.n;
     if (n % 2 == 0) {  // double2 per lane, e from both colour halves (lanes past the row idle)
         const int h = n >> 1, lane = threadIdx.x & 31, hp = h * n * n;
@@ -1643,9 +1739,9 @@ __device__ __forceinline__ void update_pass(const Team& tm, const MixedArgs& a, 
                     xo.x = 2 * xo.x - p.x;
                     xo.y = 2 * xo.y - p.y;
                 }
-                const S e0 = e[cA * hp + srow + (k >> 1)], e1 = e[(cA ^ 1) * hp + srow + (k >> 1)];
+                const double e0 = to_calc(e[cA * hp + srow + (k >> 1)]), e1 = to_calc(e[(cA ^ 1) * hp + srow + (k >> 1)]);
                 *reinterpret_cast<double2*>(home + row + k) =
-                    make_double2(xo.x + ((double)e0 - emean), xo.y + ((double)e1 - emean));
+                    make_double2(xo.x + (e0 - emean) * scale, xo.y + (e1 - emean) * scale);
             }
         });
         return;
@@ -1653,12 +1749,99 @@ __device__ __forceinline__ void update_pass(const Team& tm, const MixedArgs& a, 
     grid_pts(tm, n, [&](int i, int j, int k) {
         const long c = ((long)i * n + j) * n + k;
         const double xo = START == START_ZERO ? 0.0 : (START == START_EXTRAP ? 2 * X[c] - a.phi_prev[c] : X[c]);
-        home[c] = xo + ((double)e[split_idx(n, i, j, k)] - emean);
+        home[c] = xo + ((double)to_calc(e[split_idx(n, i, j, k)]) - emean) * scale;
     });
 }
 
-// The solve of one system by one team of CTAs.
-template <class S>
+template <class T>
+__device__ __forceinline__ void update_of(const Team& tm, const MixedArgs& a, int st, const double* X, double* home,
+                                          const T* e, double emean, double scale) {
+    if (st == START_ZERO) update_pass<START_ZERO>(tm, a, X, home, e, emean, scale);
+    else if (st == START_EXTRAP) update_pass<START_EXTRAP>(tm, a, X, home, e, emean, scale);
+    else update_pass<START_X>(tm, a, X, home, e, emean, scale);
+}
+
+// The refinement loop: r = B - L X in FP64 (checked against tol) -> rhs of the inner solve
+// with the correction's first red half-sweep from e = 0; e = V-cycle; X += e - mean(e).
+// X starts as Xs (read-only; zero for INIT) and lives in `home` from the first update.
+// Level 0 is stored as T0. With FP16 (T0 = __half) its values are kept in units of a scale:
+// the max |r| of the first residual (found by a pass that writes nothing), then of the last
+// refinement's, so that the rhs stays within [-1, 1] and the correction well inside the
+// FP16 range (a residual that leaves [1e-4, 4] times the scale is written again with its own
+// max). The first scale is the grid's hint (the last solve's first residual max) when it
+// has one, which spares the pass that only measures. The first red half-sweep, the V-cycle
+// and the mean of the correction all work in those units; the update multiplies back.
+template <class S, class T0>
+__device__ __forceinline__ void refine(const MixedArgs& a, const Team& tm, S* sm, unsigned& epoch, int& seq,
+                                       int start, bool rhs_q, const double*& Xs, double* home, int& result,
+                                       bool& ok) {
+    constexpr bool half0 = std::is_same<T0, __half>::value;
+    const int n = a.n;
+    T0* e = static_cast<T0*>(a.lev_x[0]);
+    T0* rb = static_cast<T0*>(a.lev_b[0]);
+    T0* r0 = static_cast<T0*>(a.lev_r[0]);
+    double scale = 1.0;
+    int outer = 0;
+    while (ok) {
+        stamp_outer(a, outer, 0);
+        const int st = outer == 0 ? start : START_X;
+        double s0 = 0.0, rmax = 0.0;
+        if (half0 && outer == 0) {
+            const double hint = a.scale_hint != nullptr ? *a.scale_hint : 0.0;
+            if (hint > 0.0) {
+                scale = hint;
+            } else {
+                rmax = residual_of<false>(tm, a, st, rhs_q, Xs, e, rb, 1.0);
+                ok = reduce_sum_max(s0, rmax, tm, epoch, seq);
+                if (!ok) break;
+                if (rmax <= a.tol) {
+                    result = 0;
+                    break;
+                }
+                scale = rmax;
+                s0 = rmax = 0.0;
+            }
+        }
+        rmax = residual_of<true>(tm, a, st, rhs_q, Xs, e, rb, 1.0 / scale);
+        ok = reduce_sum_max(s0, rmax, tm, epoch, seq);
+        if (half0 && ok && rmax > a.tol && (rmax > 4.0 * scale || rmax < 1e-4 * scale)) {
+            scale = rmax;
+            s0 = rmax = 0.0;
+            rmax = residual_of<true>(tm, a, st, rhs_q, Xs, e, rb, 1.0 / scale);
+            ok = reduce_sum_max(s0, rmax, tm, epoch, seq);
+        }
+        // every CTA has read the hint before the reductions above
+        if (half0 && outer == 0 && ok && a.scale_hint != nullptr && tm.b == 0 && threadIdx.x == 0)
+            *a.scale_hint = rmax;
+        stamp_outer(a, outer, 1);
+        if (a.stamps != nullptr && outer < 8 && tm.b == 0 && threadIdx.x == 0)
+            a.stamps[2 + 8 * outer + 7] = (unsigned long long)__double_as_longlong(rmax);
+        if (!ok) break;
+        if (rmax <= a.tol) {
+            result = outer;
+            break;
+        }
+        if (outer >= a.max_outer) break;
+        double esum = 0.0, m0 = 0.0;
+        ok = vcycle<S, T0>(a, tm, sm, epoch, esum, outer, e, rb, r0);
+        if (!ok) break;
+        stamp_outer(a, outer, 4);
+        // mean of the correction (the periodic Laplacian's null space)
+        ok = reduce_sum_max(esum, m0, tm, epoch, seq);
+        if (!ok) break;
+        stamp_outer(a, outer, 5);
+        const double emean = esum / ((double)n * n * n);
+        update_of(tm, a, st, Xs, home, e, emean, scale);
+        Xs = home;
+        ok = team_sync(tm, epoch);
+        stamp_outer(a, outer, 6);
+        if (half0) scale = rmax;  // the next residual is a fraction of this one
+        outer++;
+    }
+}
+
+// The solve of one system by one team of CTAs, level 0 stored as T0.
+template <class S, class T0>
 __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, S* sm) {
     const int n = a.n;
     unsigned epoch = 0;
@@ -1705,55 +1888,8 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, S
     if (a.prog != PROG_LCG_UPDATE) ok = team_sync(tm, epoch);
     stamp(a, 1);
 
-    // Refinement: r = B - L X in FP64 (checked against tol) -> FP32 rhs of the inner solve
-    // with the correction's first red half-sweep from e = 0; e = V-cycle; X += e - mean(e).
-    // X starts as X0 (read-only; zero for INIT) and lives in `home` from the first update.
     const double* Xs = X0;
-    S* e = lev_x<S>(a, 0);
-    S* rb = lev_b<S>(a, 0);
-    int outer = 0;
-    while (ok) {
-        stamp_outer(a, outer, 0);
-        const int st = outer == 0 ? start : START_X;
-        double s0 = 0.0, rmax = 0.0;
-        if (st == START_ZERO)
-            rmax = residual_any<START_ZERO, true>(tm, a, Xs, a.phi_prev, e, rb);
-        else if (st == START_EXTRAP)
-            rmax = residual_any<START_EXTRAP, true>(tm, a, Xs, a.phi_prev, e, rb);
-        else if (rhs_q)
-            rmax = residual_any<START_X, true>(tm, a, Xs, a.phi_prev, e, rb);
-        else
-            rmax = residual_any<START_X, false>(tm, a, Xs, a.phi_prev, e, rb);
-        ok = reduce_sum_max(s0, rmax, tm, epoch, seq);
-        stamp_outer(a, outer, 1);
-        if (a.stamps != nullptr && outer < 8 && tm.b == 0 && threadIdx.x == 0)
-            a.stamps[2 + 8 * outer + 7] = (unsigned long long)__double_as_longlong(rmax);
-        if (!ok) break;
-        if (rmax <= a.tol) {
-            result = outer;
-            break;
-        }
-        if (outer >= a.max_outer) break;
-        double esum = 0.0, m0 = 0.0;
-        ok = vcycle(a, tm, sm, epoch, esum, outer, e, lev_r<S>(a, 0));
-        if (!ok) break;
-        stamp_outer(a, outer, 4);
-        // mean of the correction (the periodic Laplacian's null space)
-        ok = reduce_sum_max(esum, m0, tm, epoch, seq);
-        if (!ok) break;
-        stamp_outer(a, outer, 5);
-        const double emean = esum / ((double)n * n * n);
-        if (st == START_ZERO)
-            update_pass<START_ZERO>(tm, a, Xs, home, e, emean);
-        else if (st == START_EXTRAP)
-            update_pass<START_EXTRAP>(tm, a, Xs, home, e, emean);
-        else
-            update_pass<START_X>(tm, a, Xs, home, e, emean);
-        Xs = home;
-        ok = team_sync(tm, epoch);
-        stamp_outer(a, outer, 6);
-        outer++;
-    }
+    refine<S, T0>(a, tm, sm, epoch, seq, start, rhs_q, Xs, home, result, ok);
     // converged before any update: the solution is the start itself
     if (ok && Xs != home) {
         grid_pts(tm, n, [&](int i, int j, int k) {
@@ -1778,11 +1914,13 @@ __device__ __forceinline__ void mixed_body(const MixedArgs& a, const Team& tm, S
 // hold twice the registers per value (64 registers per thread at 1024 threads would spill).
 template <class S> constexpr int threads_of() { return sizeof(S) == 8 ? 512 : kThreads; }
 
-template <class S>
+// One kernel per level-0 storage type (S, or FP16 with FP32 levels), each with one
+// refinement loop.
+template <class S, class T0>
 __global__ void __launch_bounds__(threads_of<S>(), 1) mixed_kernel(MixedArgs a) {
     extern __shared__ __align__(16) unsigned char sm_raw[];
     const Team tm{(int)gridDim.x, (int)blockIdx.x, a.bar, a.partials};
-    mixed_body(a, tm, reinterpret_cast<S*>(sm_raw));
+    mixed_body<S, T0>(a, tm, reinterpret_cast<S*>(sm_raw));
 }
 
 // Many systems in one launch (FP32 levels): system r is worked by CTAs [start[r], start[r+1]).
@@ -1802,7 +1940,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         reinterpret_cast<int*>(&a)[w] = reinterpret_cast<const int*>(list + lo)[w];
     __syncthreads();
     const Team tm{b1 - b0, (int)blockIdx.x - b0, a.bar, a.partials};
-    mixed_body(a, tm, reinterpret_cast<float*>(sm_raw));
+    mixed_body<float, float>(a, tm, reinterpret_cast<float*>(sm_raw));  // level 0 in FP32 (level0_fp16 unused)
 }
 
 // Launch configuration of one kernel variant, set up once per device.
@@ -1811,7 +1949,7 @@ struct Variant {
     int blocks = 0;
     size_t smem_set = 0;
 };
-Variant g_mixed_f32, g_mixed_f64;
+Variant g_mixed_f32, g_mixed_f64, g_mixed_f16;
 int g_batch_device = -1;
 size_t g_batch_smem_set = 0;
 
@@ -1919,9 +2057,9 @@ void mixed_batch_launch(const MixedArgs* list, const int* start, int nsys, int n
 }
 
 namespace {
-template <class S>
+template <class S, class T0>
 void launch_variant(Variant& v, const MixedArgs& a, size_t smem, cudaStream_t stream) {
-    const void* fn = (const void*)mixed_kernel<S>;
+    const void* fn = (const void*)mixed_kernel<S, T0>;
     constexpr int threads = threads_of<S>();
     int dev;
     MZB_CHECK(cudaGetDevice(&dev));
@@ -1947,11 +2085,15 @@ void launch_variant(Variant& v, const MixedArgs& a, size_t smem, cudaStream_t st
 void mixed_launch(const MixedArgs& a, cudaStream_t stream) {
     if (a.lsmall < 1 || a.lsmall > a.nlev || a.nlev < 2 || a.nu1 < 1 || a.nu2 < 1 || a.coarse_sweeps < 1)
         fatal("mixed solver: invalid level plan");
+    if (a.level0_fp16 && (a.fp64 || (a.n != 128 && a.n != 256) || a.lsmall < 2))
+        fatal("mixed solver: FP16 level 0 needs FP32 levels, n = 128 or 256 and no shared-memory level 1");
     const size_t smem = small_smem_bytes(a);
     if (a.fp64)
-        launch_variant<double>(g_mixed_f64, a, smem, stream);
+        launch_variant<double, double>(g_mixed_f64, a, smem, stream);
+    else if (a.level0_fp16)
+        launch_variant<float, __half>(g_mixed_f16, a, smem, stream);
     else
-        launch_variant<float>(g_mixed_f32, a, smem, stream);
+        launch_variant<float, float>(g_mixed_f32, a, smem, stream);
 }
 
 }  // namespace mzb

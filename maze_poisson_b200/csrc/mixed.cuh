@@ -26,6 +26,10 @@ struct MixedArgs {
     int coarse_fft;         // 1: the coarsest level (32, 64 or 128 per side) is solved by every CTA
                             // of the team by FFT, in coarse_spec
     void* coarse_spec;      // n (n/2 + 1) n complex values (float2, or double2 when fp64)
+    int level0_fp16;        // 1 (FP32 levels, n = 128 or 256): level 0's x, b and r are stored as
+                            // FP16 in units of the last residual's max (lev_x/b/r[0] hold n^3 halves)
+    double* scale_hint;     // device: the first residual max of the last solve of this grid (0:
+                            // none yet), the first scale of an FP16 level 0; or null
     int nlev;
     int lsmall;         // first level held in shared memory (nlev if none; >= 1)
     int lev_n[kMixedMaxLevels];

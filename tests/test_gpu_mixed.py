@@ -4,6 +4,8 @@ solve the same systems to the same FP64 residual tolerance as the reference's FP
 solvers, with a different inner algorithm. Checked against the CPU oracle's FP64 path
 solved to the same tolerance; the bound is the one the mixed form is specified to meet,
 force error below 1e-6 relative (max-norm ratio; much tighter in practice)."""
+import ctypes
+
 import numpy as np
 import pytest
 
@@ -29,9 +31,10 @@ def orc(oracle_path):
 
 
 class MixedRun(MDRun):
-    def __init__(self, *args, precision=1, plan=-1, **kw):
+    def __init__(self, *args, precision=1, plan=-1, sweeps=None, **kw):
         super().__init__(*args, precision=precision, **kw)
         self.plan = plan
+        self.sweeps = sweeps
 
     def initialize(self):
         c = self.capi
@@ -43,6 +46,8 @@ class MixedRun(MDRun):
         c.mzb_set_precision(self.precision, 0.0)
         assert c.mzb_get_precision() == self.precision
         assert c.mzb_set_mixed_plan(self.plan) == 0
+        if self.sweeps is not None:
+            assert c.mzb_set_mixed_sweeps(*self.sweeps) == 0
         c.solver_initialize_particles(s.n_grid, 2, s.L, s.h, s.n_ions, maps["potential"]["TF"],
                                       maps["cas"]["CIC"], s.types, s.pos, s.vel, s.mass, s.charges,
                                       s.pot_params)
@@ -102,5 +107,33 @@ def test_mixed_solution_residual_meets_tol(prod, oracle_lib, precision, plan):
         oracle_lib.orc_laplace(np.ascontiguousarray(st["field"]), lphi, 128)
         b = st["q"] * (-4 * np.pi / system.h)
         assert np.max(np.abs(lphi - b)) <= 1e-9 * 1.0001
+    finally:
+        run.finalize()
+
+
+@pytest.mark.parametrize("sweeps", [None, (2, 2), (1, 1), (4, 3)])
+def test_mixed_sweeps(prod, oracle_lib, sweeps):
+    """Sweeps before / after the coarse correction (mzb_set_mixed_sweeps; V(3,2) unless
+    set): every choice solves to the same FP64 tolerance, fewer sweeps taking more
+    refinements; counts outside 1 .. 16 are refused."""
+    system = make_system(10, 128, density=1.329, seed=5)
+    run = MixedRun(prod, system, method="LCG", tol=1e-9, precision=1, sweeps=sweeps)
+    run.initialize()
+    try:
+        nu1, nu2 = ctypes.c_int(), ctypes.c_int()
+        prod.mzb_get_mixed_sweeps(ctypes.byref(nu1), ctypes.byref(nu2))
+        assert (nu1.value, nu2.value) == (sweeps or (3, 2))
+        for bad in ((0, 2), (2, 0), (17, 2), (2, 17)):
+            assert prod.mzb_set_mixed_sweeps(*bad) == -1
+        prod.mzb_get_mixed_sweeps(ctypes.byref(nu1), ctypes.byref(nu2))
+        assert (nu1.value, nu2.value) == (sweeps or (3, 2))
+        run.step()
+        st = run.state()
+        lphi = np.empty_like(st["field"])
+        oracle_lib.orc_laplace(np.ascontiguousarray(st["field"]), lphi, 128)
+        b = st["q"] * (-4 * np.pi / system.h)
+        assert np.max(np.abs(lphi - b)) <= 1e-9 * 1.0001
+        print(f"V{sweeps or (3, 2)}: {run.n_iters} refinements")
+        assert 0 <= run.n_iters < (30 if sweeps == (1, 1) else 15)
     finally:
         run.finalize()

@@ -20,7 +20,9 @@
   FP64 multigrid form within 1e-7 (max-norm) and 1e-8 (RMS) of the oracle's forces, the
   bound the mixed form is specified to meet being 1e-6.
 * 2000 ions / 128^3: one Poisson solve of the same charge grid by PCG (tol 1e-8), the
-  reference's multigrid, the FP64 4-level V(2,2) multigrid and the FP32+refine form, each
+  reference's multigrid, the FP64 4-level V(2,2) multigrid (levels 128 to 16 per side),
+  the FP64 multigrid as the step runs it (V(3,2), the 64^3 level solved by FFT) and the
+  FP32+refine form, each
   against (a) the exact solution of the same 7-point system (an FFT with the stencil's
   eigenvalues, in the test) and (b) the reference's FFT Poisson solve (continuous k^2),
   run through the product's FFT path. Against (a) they agree to the solve's tolerance: a
@@ -144,14 +146,16 @@ def test_nacl16000_256_multigrid_refine_step(prod, nacl16000_state, precision):
     assert errs["vel"] < 1e-7
 
 
-def _solve_once(prod, system, method, precision, tol=1e-8):
+def _solve_once(prod, system, method, precision, tol=1e-8, setup=None):
     """One solver_update_field from phi = phi_prev = 0 for the system's charges; returns
-    (q, phi, field forces, solver result)."""
+    (q, phi, field forces, solver result). `setup` runs after the grid is made."""
     run = MDRun(prod, system.copy(), method=method, tol=tol, precision=precision)
     g = system.n_grid
     zero = np.zeros((g, g, g))
     mdparity.restart(run, system.pos, system.vel, zero, zero)
     try:
+        if setup is not None:
+            setup()
         res = prod.solver_update_field()
         prod.solver_compute_forces_elec()
         q, phi, f = np.empty((g, g, g)), np.empty((g, g, g)), np.empty((system.n_ions, 3))
@@ -181,12 +185,17 @@ def test_nacl2000_128_solvers_vs_fft(prod, oracle_lib):
     f_7 = np.empty((system.n_ions, 3))
     oracle_lib.orc_force_fd(np.ascontiguousarray(phi_7), nbr, system.charges, system.pos, system.n_ions, n,
                             system.h, f_7)
-    for method, precision in (("LCG", 0), ("MULTIGRID", 0), ("MULTIGRID", 2), ("MULTIGRID", 1)):
-        q2, phi, f, res = _solve_once(prod, system, method, precision)
+    def four_level_v22():  # 128, 64, 32, 16 points per side, V(2,2)
+        assert prod.mzb_set_mixed_plan(0) == 0 and prod.mzb_set_mixed_sweeps(2, 2) == 0
+
+    for method, precision, setup in (("LCG", 0, None), ("MULTIGRID", 0, None), ("MULTIGRID", 2, four_level_v22),
+                                     ("MULTIGRID", 2, None), ("MULTIGRID", 1, None)):
+        q2, phi, f, res = _solve_once(prod, system, method, precision, setup=setup)
         assert np.array_equal(q2, q) and res >= 0, (method, precision, res)
         phi0 = phi - phi.mean()
         errs = {"phi_vs_7pt": rel(phi0, phi_7), "f_vs_7pt": rel(f, f_7), "f_vs_fft": rel(f, f_fft),
                 "f_rms_vs_fft": rms_rel(f, f_fft)}
-        print(f"nacl2000_128 {method} precision {precision} ({res}):", errs)
+        label = " 4-level V(2,2)" if setup is not None else ""
+        print(f"nacl2000_128 {method} precision {precision}{label} ({res}):", errs)
         assert errs["phi_vs_7pt"] < 1e-6 and errs["f_vs_7pt"] < 1e-5, (method, precision, errs)
         assert errs["f_vs_fft"] < 0.05, (method, precision, errs)
