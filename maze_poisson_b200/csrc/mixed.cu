@@ -575,12 +575,21 @@ __device__ __forceinline__ void stv(S* p, const S (&v)[V]) {
 #pragma unroll
         for (int e = 0; e < V; e += 2) *reinterpret_cast<double2*>(p + e) = make_double2(v[e], v[e + 1]);
 }
-// FP16 storage with FP32 arithmetic (level 0 of the mixed form): V = 4 values per 8-byte
-// access, V = 2 per 4-byte access; stores round to nearest.
+// FP16 storage with FP32 arithmetic (level 0 of the mixed form): V = 8 values per 16-byte
+// access, 4 per 8-byte, 2 per 4-byte access; stores round to nearest.
 template <int V>
 __device__ __forceinline__ void ldv(const __half* p, float (&v)[V]) {
-    static_assert(V == 2 || V == 4, "FP16 rows take 2 or 4 values per lane");
-    if constexpr (V == 4) {
+    static_assert(V == 2 || V == 4 || V == 8, "FP16 rows take 2, 4 or 8 values per lane");
+    if constexpr (V == 8) {
+        const uint4 t = *reinterpret_cast<const uint4*>(p);
+        const unsigned w[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[q]));
+            v[2 * q] = f.x;
+            v[2 * q + 1] = f.y;
+        }
+    } else if constexpr (V == 4) {
         const uint2 t = *reinterpret_cast<const uint2*>(p);
         const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&t.x));
         const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&t.y));
@@ -592,8 +601,16 @@ __device__ __forceinline__ void ldv(const __half* p, float (&v)[V]) {
 }
 template <int V>
 __device__ __forceinline__ void stv(__half* p, const float (&v)[V]) {
-    static_assert(V == 2 || V == 4, "FP16 rows take 2 or 4 values per lane");
-    if constexpr (V == 4) {
+    static_assert(V == 2 || V == 4 || V == 8, "FP16 rows take 2, 4 or 8 values per lane");
+    if constexpr (V == 8) {
+        unsigned w[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const __half2 h2 = __floats2half2_rn(v[2 * q], v[2 * q + 1]);
+            w[q] = *reinterpret_cast<const unsigned*>(&h2);
+        }
+        *reinterpret_cast<uint4*>(p) = make_uint4(w[0], w[1], w[2], w[3]);
+    } else if constexpr (V == 4) {
         const __half2 a = __floats2half2_rn(v[0], v[1]), b = __floats2half2_rn(v[2], v[3]);
         uint2 t;
         t.x = *reinterpret_cast<const unsigned*>(&a);
@@ -613,6 +630,26 @@ template <class T> __device__ __forceinline__ T from_calc(typename Calc<T>::type
     if constexpr (std::is_same<T, __half>::value) return __float2half_rn(v);
     else return v;
 }
+// V consecutive values of a row as one lane loads them: in the arithmetic type, or for FP16
+// packed two to a register (converted where read), so that five rows of 8 FP16 values per
+// lane fit the 64 registers of a 1024-thread CTA.
+template <class T, int V>
+struct RowVals {
+    typename Calc<T>::type v[V];
+    __device__ __forceinline__ void load(const T* p) { ldv<V>(p, v); }
+    __device__ __forceinline__ typename Calc<T>::type operator[](int e) const { return v[e]; }
+};
+template <int V>
+struct RowVals<__half, V> {
+    static_assert(V == 8, "packed FP16 rows hold 8 values");
+    uint4 w;
+    __device__ __forceinline__ void load(const __half* p) { w = *reinterpret_cast<const uint4*>(p); }
+    __device__ __forceinline__ float operator[](int e) const {
+        const unsigned u = e < 2 ? w.x : e < 4 ? w.y : e < 6 ? w.z : w.w;
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&u));
+        return (e & 1) ? f.y : f.x;
+    }
+};
 
 // sum of the six other-colour neighbours of the lane's V points in row o (s as in
 // split_nb_sums), from full-row vector loads
@@ -803,15 +840,15 @@ __device__ __forceinline__ void grid_row_groups(const Team& tm, int n, const Row
         f(i, rr - i * n, act);
     }
 }
-template <int V, class S>
-__device__ __forceinline__ void rows_nb_sums(const S* xo, const Rows& o, int s, int kk0, const RowLanes& t,
+template <int V, class T, class S>
+__device__ __forceinline__ void rows_nb_sums(const T* xo, const Rows& o, int s, int kk0, const RowLanes& t,
                                              S (&sum)[V]) {
-    S a0[V], a1[V], a2[V], a3[V], cen[V];
-    ldv<V>(xo + o.im + kk0, a0);
-    ldv<V>(xo + o.ip + kk0, a1);
-    ldv<V>(xo + o.jm + kk0, a2);
-    ldv<V>(xo + o.jp + kk0, a3);
-    ldv<V>(xo + o.c + kk0, cen);
+    RowVals<T, V> a0, a1, a2, a3, cen;
+    a0.load(xo + o.im + kk0);
+    a1.load(xo + o.ip + kk0);
+    a2.load(xo + o.jm + kk0);
+    a3.load(xo + o.jp + kk0);
+    cen.load(xo + o.c + kk0);
     const S prev = __shfl_sync(0xffffffffu, cen[V - 1], t.lp);
     const S next = __shfl_sync(0xffffffffu, cen[0], t.ln);
 #pragma unroll
@@ -821,22 +858,24 @@ __device__ __forceinline__ void rows_nb_sums(const S* xo, const Rows& o, int s, 
         sum[e] = (u + cen[e]) + side;
     }
 }
-template <int V, class S>
-__device__ void split_gs_rows(const Team& tm, int n, int c, const S* b, S* x, double* acc) {
+template <int V, class T>
+__device__ void split_gs_rows(const Team& tm, int n, int c, const T* b, T* x, double* acc) {
+    using S = typename Calc<T>::type;
     const int h = n >> 1, hp = h * n * n;
     const RowLanes t = row_lanes<V>(h);
-    const S* xo = x + (1 - c) * hp;
-    S* xc = x + c * hp;
-    const S* bc = b + c * hp;
+    const T* xo = x + (1 - c) * hp;
+    T* xc = x + c * hp;
+    const T* bc = b + c * hp;
     const int kk0 = t.q * V;
     double s_acc = 0.0;
     grid_row_groups(tm, n, t, [&](int i, int j, bool act) {
         const Rows o = rows_of(n, i, j);
-        S bv[V], sum[V], v[V];
-        ldv<V>(bc + o.c + kk0, bv);
+        RowVals<T, V> bv;
+        S sum[V], v[V];
+        bv.load(bc + o.c + kk0);
         rows_nb_sums<V>(xo, o, (i + j + c) & 1, kk0, t, sum);
 #pragma unroll
-        for (int e = 0; e < V; e++) v[e] = (bv[e] - sum[e]) * neg_sixth<S>();
+        for (int e = 0; e < V; e++) v[e] = to_calc(from_calc<T>((bv[e] - sum[e]) * neg_sixth<S>()));  // as stored
         if (act) {
             stv<V>(xc + o.c + kk0, v);
 #pragma unroll
@@ -845,17 +884,19 @@ __device__ void split_gs_rows(const Team& tm, int n, int c, const S* b, S* x, do
     });
     if (acc != nullptr) *acc += s_acc;
 }
-template <int V, class S>
-__device__ void split_resid_red_rows(const Team& tm, int n, const S* b, const S* x, S* r) {
+template <int V, class T>
+__device__ void split_resid_red_rows(const Team& tm, int n, const T* b, const T* x, T* r) {
+    using S = typename Calc<T>::type;
     const int h = n >> 1, hp = h * n * n;
     const RowLanes t = row_lanes<V>(h);
-    const S* x1 = x + hp;
+    const T* x1 = x + hp;
     const int kk0 = t.q * V;
     grid_row_groups(tm, n, t, [&](int i, int j, bool act) {
         const Rows o = rows_of(n, i, j);
-        S bv[V], xv[V], sum[V], v[V];
-        ldv<V>(b + o.c + kk0, bv);
-        ldv<V>(x + o.c + kk0, xv);
+        RowVals<T, V> bv, xv;
+        S sum[V], v[V];
+        bv.load(b + o.c + kk0);
+        xv.load(x + o.c + kk0);
         rows_nb_sums<V>(x1, o, (i + j) & 1, kk0, t, sum);
 #pragma unroll
         for (int e = 0; e < V; e++) v[e] = bv[e] - (sum[e] - S(6) * xv[e]);
@@ -865,12 +906,12 @@ __device__ void split_resid_red_rows(const Team& tm, int n, const S* b, const S*
 
 // dispatch: rows of 128 floats (n = 256) as float4 and of 64 (n = 128) as float2, one row
 // per warp; shorter rows several per warp (n % 8 == 0 as float4, n % 4 == 0 as float2)
-// FP16 storage (level 0 of the mixed form) is taken for n = 256 and 128 only.
+// FP16 storage (level 0 of the mixed form, n = 256): half-sweeps and red residuals with 8
+// values (16 bytes) per lane, several rows per warp; restriction and prolongation with 4.
 template <class S>
 __device__ __forceinline__ void split_gs(const Team& tm, int n, int c, const S* b, S* x, double* acc) {
-    if constexpr (std::is_same<S, __half>::value) {
-        if (n == 256) split_gs_vec<4>(tm, n, c, b, x, acc);
-        else split_gs_vec<2>(tm, n, c, b, x, acc);
+    if constexpr (std::is_same<S, __half>::value) {  // 8 values (16 bytes) per lane, several rows per warp
+        split_gs_rows<8>(tm, n, c, b, x, acc);
     } else {
         if (n == 256) split_gs_vec<4>(tm, n, c, b, x, acc);
         else if (n == 128) split_gs_vec<2>(tm, n, c, b, x, acc);
@@ -882,8 +923,7 @@ __device__ __forceinline__ void split_gs(const Team& tm, int n, int c, const S* 
 template <class S>
 __device__ __forceinline__ void split_resid_red(const Team& tm, int n, const S* b, const S* x, S* r) {
     if constexpr (std::is_same<S, __half>::value) {
-        if (n == 256) split_resid_red_vec<4>(tm, n, b, x, r);
-        else split_resid_red_vec<2>(tm, n, b, x, r);
+        split_resid_red_rows<8>(tm, n, b, x, r);
     } else {
         if (n == 256) split_resid_red_vec<4>(tm, n, b, x, r);
         else if (n == 128) split_resid_red_vec<2>(tm, n, b, x, r);
