@@ -1704,10 +1704,14 @@ __device__ __forceinline__ double residual_pass_vec(const Team& tm, const MixedA
             } else {
                 const double2 xip = x2(rip + k), xim = x2(rim + k), xjp = x2(rjp + k), xjm = x2(rjm + k);
                 const double2 xc = x2(row + k);
+                // the values beside the chunk (lane 0 and the chunk's last lane need them), loaded
+                // by every lane ahead of the shuffles so that no load waits on one
+                const double xl = x1(row + (k0 == 0 ? n - 1 : k0 - 1));
+                const double xr = x1(row + (k + 2 >= n ? 0 : k + 2));
                 double km0 = __shfl_sync(0xffffffffu, xc.y, (lane + 31) & 31);
                 double kp1 = __shfl_sync(0xffffffffu, xc.x, (lane + 1) & 31);
-                if (lane == 0) km0 = x1(row + (k0 == 0 ? n - 1 : k0 - 1));
-                if (lane == 31 || k + 2 >= n) kp1 = x1(row + (k + 2 >= n ? 0 : k + 2));
+                if (lane == 0) km0 = xl;
+                if (lane == 31 || k + 2 >= n) kp1 = xr;
                 double s0 = xip.x + xim.x;
                 s0 = s0 + xjp.x;
                 s0 = s0 + xjm.x;
