@@ -767,40 +767,79 @@ __device__ void split_restrict_vec(const Team& tm, int n, const T* r, S* bc, S* 
     });
 }
 
+// Coarse row (CI, CJ) of a level with nc = 32 V points per side as lane l reads it for the
+// black points kk = V l .. V l + V - 1 of a fine row: the even ck = V l + 2 t from one
+// colour half and the odd ck = V l + 2 t + 1 from the other, one vector load each.
+template <int V, class S>
+struct CoarseRun {
+    S ev[V / 2], od[V / 2];
+    __device__ __forceinline__ void load(const S* xc, int nc, int CI, int CJ) {
+        const int lane = threadIdx.x & 31, hc = nc >> 1, hpc = hc * nc * nc;
+        const int rowc = (CI * nc + CJ) * hc;
+        const int c0 = (CI + CJ) & 1;  // colour of the even ck
+        constexpr int H = V / 2;
+        if constexpr (H == 1) {
+            ev[0] = xc[c0 * hpc + rowc + lane];
+            od[0] = xc[(c0 ^ 1) * hpc + rowc + lane];
+        } else {
+            ldv<H>(xc + c0 * hpc + rowc + H * lane, ev);
+            ldv<H>(xc + (c0 ^ 1) * hpc + rowc + H * lane, od);
+        }
+    }
+    // the values along k at the lane's V black points: coarse ck, or with ok the mean of
+    // ck and ck + 1 (ck = V l + V, from the next lane, wraps to 0 at the row's end)
+    __device__ __forceinline__ void line(bool ok, S (&L)[V]) const {
+        const int lane = threadIdx.x & 31;
+        const S last = __shfl_sync(0xffffffffu, ev[0], (lane + 1) & 31);
+#pragma unroll
+        for (int e = 0; e < V; e++) {
+            const S c = (e & 1) ? od[e >> 1] : ev[e >> 1];
+            const S c1 = e + 1 == V ? last : ((e & 1) ? ev[(e + 1) >> 1] : od[e >> 1]);
+            L[e] = ok ? S(0.5) * (c + c1) : c;
+        }
+    }
+};
+
+// prolongation into the black points of rows of h = nc = 32 V values per colour: lane l adds
+// the trilinear interpolation at black points kk = V l .. V l + V - 1 (same sums, in the same
+// order, as split_prolong_black_scalar); the four coarse rows are loaded before any is used
 template <int V, class S, class T>
 __device__ void split_prolong_black_vec(const Team& tm, int n, const S* xc, T* x) {
-    const int lane = threadIdx.x & 31, h = n >> 1, nc = n / 2, hc = nc >> 1;
-    const int hp = h * n * n, hpc = hc * nc * nc;
+    const int lane = threadIdx.x & 31, h = n >> 1, nc = n / 2;
+    const int hp = h * n * n;
     T* x1 = x + hp;
     grid_rows(tm, n, [&](int i, int j) {
         const int s1 = (i + j + 1) & 1;
         const int ci = i >> 1, cj = j >> 1;
         const int ci1 = ci + 1 == nc ? 0 : ci + 1, cj1 = cj + 1 == nc ? 0 : cj + 1;
         const bool oi = i & 1, oj = j & 1, ok = s1;
-        auto C = [&](int CI, int CJ, int CK) {
-            return ((CI + CJ + CK) & 1) * hpc + (CI * nc + CJ) * hc + (CK >> 1);
-        };
-        auto line = [&](int CI, int CJ, int ck, int ck1) {
-            const S a = xc[C(CI, CJ, ck)];
-            return ok ? S(0.5) * (a + xc[C(CI, CJ, ck1)]) : a;
-        };
         const int rowx = (i * n + j) * h + V * lane;
-        S old[V], v[V];
+        S old[V], p[V], t[V], q[V];
         ldv<V>(x1 + rowx, old);
+        CoarseRun<V, S> r00, r01, r10, r11;
+        r00.load(xc, nc, ci, cj);
+        r01.load(xc, nc, ci, cj1);
+        r10.load(xc, nc, ci1, cj);
+        r11.load(xc, nc, ci1, cj1);
+        r00.line(ok, p);
+        if (oj) {
+            r01.line(ok, t);
 #pragma unroll
-        for (int e = 0; e < V; e++) {
-            const int kk = V * lane + e;
-            const int ck = kk, ck1 = kk + 1 == nc ? 0 : kk + 1;
-            S p = line(ci, cj, ck, ck1);
-            if (oj) p = S(0.5) * (p + line(ci, cj1, ck, ck1));
-            if (oi) {
-                S q = line(ci1, cj, ck, ck1);
-                if (oj) q = S(0.5) * (q + line(ci1, cj1, ck, ck1));
-                p = S(0.5) * (p + q);
-            }
-            v[e] = old[e] + p;
+            for (int e = 0; e < V; e++) p[e] = S(0.5) * (p[e] + t[e]);
         }
-        stv<V>(x1 + rowx, v);
+        if (oi) {
+            r10.line(ok, q);
+            if (oj) {
+                r11.line(ok, t);
+#pragma unroll
+                for (int e = 0; e < V; e++) q[e] = S(0.5) * (q[e] + t[e]);
+            }
+#pragma unroll
+            for (int e = 0; e < V; e++) p[e] = S(0.5) * (p[e] + q[e]);
+        }
+#pragma unroll
+        for (int e = 0; e < V; e++) p[e] = old[e] + p[e];
+        stv<V>(x1 + rowx, p);
     });
 }
 
