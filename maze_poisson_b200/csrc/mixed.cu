@@ -1808,23 +1808,39 @@ __device__ __forceinline__ void update_pass(const Team& tm, const MixedArgs& a, 
                                             const T* e, double emean, double scale) {
     const int n = a.n;
     if (n % 2 == 0) {  // double2 per lane, e from both colour halves (lanes past the row idle)
+        // U chunks of 64 k at a time, all loaded before any is stored (home may be X itself,
+        // so a store would otherwise hold the next chunk's loads back)
+        constexpr int U = 4;
         const int h = n >> 1, lane = threadIdx.x & 31, hp = h * n * n;
         grid_rows(tm, n, [&](int i, int j) {
             const int row = (i * n + j) * n, srow = (i * n + j) * h;
             const int cA = (i + j) & 1;
-            for (int k0 = 0; k0 < n; k0 += 64) {
-                const int k = k0 + 2 * lane;
-                if (k >= n) break;
-                double2 xo = make_double2(0.0, 0.0);
-                if (START != START_ZERO) xo = *reinterpret_cast<const double2*>(X + row + k);
-                if (START == START_EXTRAP) {
-                    const double2 p = *reinterpret_cast<const double2*>(a.phi_prev + row + k);
-                    xo.x = 2 * xo.x - p.x;
-                    xo.y = 2 * xo.y - p.y;
+            for (int k00 = 0; k00 < n; k00 += 64 * U) {
+                double2 xo[U];
+                double e0[U], e1[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int k = k00 + 64 * u + 2 * lane;
+                    xo[u] = make_double2(0.0, 0.0);
+                    e0[u] = e1[u] = 0.0;
+                    if (k < n) {
+                        if (START != START_ZERO) xo[u] = *reinterpret_cast<const double2*>(X + row + k);
+                        if (START == START_EXTRAP) {
+                            const double2 p = *reinterpret_cast<const double2*>(a.phi_prev + row + k);
+                            xo[u].x = 2 * xo[u].x - p.x;
+                            xo[u].y = 2 * xo[u].y - p.y;
+                        }
+                        e0[u] = to_calc(e[cA * hp + srow + (k >> 1)]);
+                        e1[u] = to_calc(e[(cA ^ 1) * hp + srow + (k >> 1)]);
+                    }
                 }
-                const double e0 = to_calc(e[cA * hp + srow + (k >> 1)]), e1 = to_calc(e[(cA ^ 1) * hp + srow + (k >> 1)]);
-                *reinterpret_cast<double2*>(home + row + k) =
-                    make_double2(xo.x + (e0 - emean) * scale, xo.y + (e1 - emean) * scale);
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int k = k00 + 64 * u + 2 * lane;
+                    if (k < n)
+                        *reinterpret_cast<double2*>(home + row + k) =
+                            make_double2(xo[u].x + (e0[u] - emean) * scale, xo[u].y + (e1[u] - emean) * scale);
+                }
             }
         });
         return;
