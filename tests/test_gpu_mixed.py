@@ -137,3 +137,50 @@ def test_mixed_sweeps(prod, oracle_lib, sweeps):
         assert 0 <= run.n_iters < (30 if sweeps == (1, 1) else 15)
     finally:
         run.finalize()
+
+
+@pytest.mark.parametrize("method", ["LCG", "MAZE-LCG", "MULTIGRID", "MAZE-MULTIGRID"])
+def test_fp16_level0_programs_256(prod, oracle_lib, method):
+    """At 256^3 the FP32+refine form stores level 0 as FP16 (scaled by the residual's max):
+    every program that takes it (the LCG and MaZe updates, the multigrid updates from the
+    extrapolated start) still returns a field with |L phi - b|_inf within the FP64 tol."""
+    system = make_system(4, 256, density=1.379, seed=9)
+    run = MixedRun(prod, system, method=method, tol=1e-9, precision=1)
+    run.initialize()
+    try:
+        for _ in range(2):
+            run.step()
+            assert 0 <= run.n_iters < 30, run.n_iters
+        st = run.state()
+        lphi = np.empty_like(st["field"])
+        oracle_lib.orc_laplace(np.ascontiguousarray(st["field"]), lphi, 256)
+        b = st["q"] * (-4 * np.pi / system.h)
+        assert np.max(np.abs(lphi - b)) <= 1e-9 * 1.0001
+    finally:
+        run.finalize()
+
+
+def test_fp16_level0_scale_guard(prod, oracle_lib):
+    """The FP16 level 0 starts in the units of the grid's last first residual. A start far
+    from the solution (the field plus noise of 1e3) and then one very close to it (noise of
+    1e-6) each leave the range those units cover: the residual is written again in its own
+    units, and both solves meet the FP64 tol."""
+    system = make_system(4, 256, density=1.379, seed=11)
+    run = MixedRun(prod, system, method="LCG", tol=1e-9, precision=1)
+    run.initialize()
+    try:
+        n = 256
+        st = run.state()
+        phi = np.ascontiguousarray(st["field"])
+        b = st["q"] * (-4 * np.pi / system.h)
+        rng = np.random.default_rng(3)
+        for amp in (1e3, 1e-6):
+            prod.solver_set_field(np.ascontiguousarray(phi + amp * rng.standard_normal(phi.shape)))
+            res = prod.solver_update_field()
+            assert 0 <= res < 30, (amp, res)
+            prod.get_field(phi)
+            lphi = np.empty_like(phi)
+            oracle_lib.orc_laplace(phi, lphi, n)
+            assert np.max(np.abs(lphi - b)) <= 1e-9 * 1.0001, amp
+    finally:
+        run.finalize()
