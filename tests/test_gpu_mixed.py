@@ -184,3 +184,24 @@ def test_fp16_level0_scale_guard(prod, oracle_lib):
             assert np.max(np.abs(lphi - b)) <= 1e-9 * 1.0001, amp
     finally:
         run.finalize()
+
+
+@pytest.mark.parametrize("plan", [2, 0])
+def test_fp16_level0_plans_256(prod, oracle_lib, plan):
+    """FP16 level 0 at 256^3 under the other coarse-level plans: the 128^3 level swept in
+    FP32 and the 64^3 level solved by FFT (plan 2), or the levels down to 16^3 solved by
+    the Green's function (plan 0); the field meets the FP64 tol."""
+    system = make_system(4, 256, density=1.379, seed=13)
+    run = MixedRun(prod, system, method="LCG", tol=1e-9, precision=1, plan=plan)
+    run.initialize()
+    assert prod.mzb_get_mixed_plan() == plan
+    try:
+        run.step()
+        assert 0 <= run.n_iters < 30, run.n_iters
+        st = run.state()
+        lphi = np.empty_like(st["field"])
+        oracle_lib.orc_laplace(np.ascontiguousarray(st["field"]), lphi, 256)
+        b = st["q"] * (-4 * np.pi / system.h)
+        assert np.max(np.abs(lphi - b)) <= 1e-9 * 1.0001
+    finally:
+        run.finalize()
